@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Headline benchmark: particle-steps/s of the 1,048,576-particle PCISPH dam
+break (eta = 1 %, min 3 / max 50 corrections) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0 (see the keys below). A "step" is one full
+simulation step over the whole particle set: grid, radix sort, neighbour
+lists, density, non-pressure forces, the eta-controlled corrector loop,
+walls and velocity interpolation.
+
+  value     particle-steps/s with the state resident in HBM, device-timed with
+            CUDA events on the simulation's stream, max over ranks;
+  e2e       the same metric through the C ABI with host buffers: each step
+            uploads positions and velocities from pinned host memory, steps,
+            and downloads positions, velocities and densities (what the
+            reference's update() copies back for its front end);
+  roofline  the dominant kernel's algorithmic bytes per launch over its mean
+            launch time, against the measured HBM copy bandwidth;
+  cpu_baseline  the FP64 oracle of the same method (OpenMP, every host core)
+            on a bounded sample of the same scene.
+Multi-GPU: each rank runs an independent replica of the scene (its own seed);
+a single dam break is not partitioned (replicas only), so there is no
+collective on the step path -- one barrier and one max-reduction of the
+timings.
+
+--impl reference times the reference's own CPU implementation: its kernels
+compiled as host code (oracle/_ref) with the reference's physics (fixed three
+corrections) on the same scene, on every host core, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s, 1M-particle PCISPH dam break at eta=1%"
+UNIT = "particle-steps/s"
+
+# Algorithmic bytes per particle of each kernel (compulsory FP32 SoA
+# traffic; neighbour re-reads and list traffic not counted).
+ALG_BYTES = {
+    "cell_keys": 24,          # pos 16 -> key + id 8
+    "radix_sort": 16,         # one read + write of the (key, value) pairs
+    "reorder": 77,            # pos, vel, pressure 36 in + 36 out, cell ranges 5
+    "build_nbr": 24,          # pos 16 + key 4 -> count 4
+    "density_x": 20,          # pos 16 -> rho 4
+    "pci_init": 132,          # non-pressure forces 52 + first prediction 80
+    "pci_density": 28,        # x* 16, p 4 -> p, rho* 8
+    "pci_force_predict": 120,  # pressure force 40 + prediction 80
+    "pci_commit": 96,         # final integrate, walls, interpolation
+    "wcsph_force": 228,       # forces 52 + integrate 80 + walls/interpolation 96
+}
+# Kernels per timed group (radix_sort is 3 kernels per 8-bit pass).
+def _kernels_per_group(name: str, sort_passes: int) -> int:
+    return 3 * sort_passes if name == "radix_sort" else 1
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scene", default="C2")
+    ap.add_argument("--warm-start", choices=["zero", "previous"], default="zero")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-steps", type=int, default=1)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sms, maxs, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sms.append(float(parts[1]))
+                    maxs.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sms)) if sms else None, "sm_max_mhz": max(maxs) if maxs else None,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-particle DRAM bytes of each kernel from the committed ncu capture summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def cpu_baseline_port(scene_name: str, steps: int) -> dict:
+    """The FP64 oracle (a C port of the same method, OpenMP on every host
+    core) on a bounded sample: `steps` steps of the same scene."""
+    import oracle
+    import psb_project_b200 as P
+    sc = P.config_scene(scene_name)
+    pos = oracle.scene_positions(sc)
+    sim = oracle.OracleSim(sc, pos)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.step()
+    dt = time.perf_counter() - t0
+    return {"value": sc.n * steps / dt, "unit": UNIT, "cores": host_cores(), "kind": "port",
+            "sample": f"{steps} step(s) of the {sc.n:,}-particle scene from rest, FP64 oracle, "
+                      f"{host_cores()} threads on {cpu_model()}"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    import psb_project_b200 as P
+    sc = P.config_scene(args.scene)
+    sc_ref = P.dam_break(sc.blocks[0].nxyz, sc.blocks[0].spacing, sc.box_max, sc.h, method=P.PCISPH,
+                         profile=P.PROFILE_REF, dt=sc.dt, mass=sc.mass, seed=sc.blocks[0].seed)
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference kernels built for the "
+                          "host) is not present: build() compiles it where the reference tree exists"}))
+        return
+    pos = oracle.scene_positions(sc_ref).astype(np.float64)
+    ref = oracle.RefSim(sc_ref, pos)
+    for _ in range(args.warmup):
+        ref.pcisph_update()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref.pcisph_update()
+    dt = time.perf_counter() - t0
+    value = sc_ref.n * args.steps / dt
+    cores = host_cores()
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{sc.name}: reference physics (3 fixed corrections)", "particles": sc_ref.n,
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{args.steps} timed steps of the {sc_ref.n:,}-particle scene, the reference's "
+                                   f"kernels run as host code on {cores} threads ({cpu_model()})"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def run_ours(args):
+    import torch
+    import psb_project_b200 as P
+    from psb_project_b200 import runtime as R
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    sc = P.config_scene(args.scene)
+    if args.warm_start == "previous":
+        sc = sc.replace(warm_start=P.WARM_PREVIOUS)
+    if world > 1:       # replicas: same scene, own seed per rank
+        sc.blocks[0].seed = sc.blocks[0].seed + 1000 * rank
+    n = sc.n
+    pos0 = P.scene_positions(sc)
+    stream = torch.cuda.current_stream()
+    sim = P.Simulation(sc)
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(pos0)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timing -------------------------------------------------
+    sim.step(args.warmup)
+    iters0 = sim.stats().iters_total
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    iters = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        sim.step(1)
+        iters.append(sim.stats().iters)
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * n * args.steps / (ms_max / 1e3)
+
+    # ---- per-kernel timing: the next K steps with CUDA events around every launch ----
+    sim.profile(True)
+    sim.profile_reset()
+    sim.step(args.steps)
+    prof = sim.profile_read()
+    sim.profile(False)
+    passes = (max(1, int(np.ceil(np.log2(np.prod(sc.dims))))) + 7) // 8
+    launches = int(sum(l * _kernels_per_group(k, passes) for k, (l, _) in prof.items()))
+    tot_ms = sum(v[1] for v in prof.values())
+    dom = max((k for k in prof if k in ALG_BYTES), key=lambda k: prof[k][1])
+    l_dom, ms_dom = prof[dom]
+    per_launch_s = ms_dom / l_dom / 1e3
+    achieved = ALG_BYTES[dom] * n / per_launch_s / 1e9
+    peak, peak_kind = peaks()
+    traffic = ncu_traffic().get(dom)
+    kernels = {k: {"launches": l, "ms": round(v, 3), "share": round(v / tot_ms, 4)} for k, (l, v) in prof.items()}
+
+    # ---- end to end through the C ABI with host buffers ------------------------------
+    pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+    h_pos, h_vel, h_vh, h_rho = pin((n, 3)), pin((n, 3)), pin((n, 3)), pin((n,))
+    sim.download({"pos": h_pos, "vel": h_vel, "vel_half": h_vh, "density": h_rho})
+    barrier()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        sim.upload(h_pos, h_vel, h_vh)
+        sim.step(1)
+        sim.download({"pos": h_pos, "vel": h_vel, "vel_half": h_vh, "density": h_rho})
+    e3.record(stream)
+    barrier()
+    ms_e2e = e2.elapsed_time(e3)
+    t = torch.tensor([ms_e2e], device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * args.steps / (float(t.item()) / 1e3)
+    launches_e2e_note = None
+    st = sim.stats()
+    sim.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_port(args.scene, args.cpu_sample_steps)
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": host_cores(), "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": sc.name, "particles": n, "eta": sc.eta, "min_iters": sc.min_iters,
+                       "max_iters": sc.max_iters, "warm_start": args.warm_start, "dt": sc.dt, "h": sc.h,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "working set > L2 (state, lists and scratch ~%d MB per GPU)" % int(n * (3 * 16 * 2 + 8 * 2 + 4 * 2 + 16 * 2 + 16 + 8 + 4 + 4 * sc.nbr_cap + 4) / 1e6),
+                       "from_rest_after_warmup_steps": args.warmup},
+            "iters_per_step": {"mean": float(np.mean(iters)), "p50": float(np.median(iters)),
+                               "p95": float(np.percentile(iters, 95)), "max": int(np.max(iters)),
+                               "min": int(np.min(iters))},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None if traffic is None else traffic * n,
+                         "alg_bytes_per_particle": ALG_BYTES[dom], "mean_launch_us": per_launch_s * 1e6},
+            "kernels": kernels,
+            "gpu_launches": launches,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 12 * n,
+                    "d2h_bytes_per_step": 3 * 12 * n + 4 * n},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,167 @@
+/*
+ * psb.h -- C ABI of the B200 particle-simulation hot path (libpsb.so).
+ *
+ * Plain C: opaque context, plain pointers and sizes, int status returns,
+ * caller-owned host buffers, library-owned device buffers, one CUDA stream
+ * per context. Everything is asynchronous on that stream except the calls
+ * that return host data (psb_download*, psb_read_field, psb_get_stats) and
+ * psb_step, which reads the corrector loop's convergence word each
+ * iteration.
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the edarles/PSB_Project tree). The reference's system classes
+ * (PCI_SPHSystem, SPHSystem) keep their class API; their update() bodies
+ * call these functions instead of the reference launchers -- the
+ * integration recipe, with the ctypes binding the Python tests use, is in
+ * INTEGRATION.md.
+ */
+#ifndef PSB_H
+#define PSB_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSB_ABI_VERSION 1
+
+/* Status codes. The reference's launchers return void and never check
+ * (src/common.cu:63-66); every call here returns one of these. */
+enum {
+    PSB_OK = 0,
+    PSB_EINVAL = 1,          /* bad argument or scene */
+    PSB_ENOMEM = 2,          /* device or host allocation failed */
+    PSB_EOVERFLOW_NBR = 3,   /* a particle had more neighbours than scene.nbr_cap */
+    PSB_ENOCONV = 4,         /* corrector loop hit max_iters above eta (state is still advanced) */
+    PSB_ECUDA = 5,           /* CUDA runtime error */
+    PSB_ESTATE = 6           /* call out of order (e.g. step before upload) */
+};
+
+/* Physics profiles. REF reproduces the reference's formulas (linear EOS,
+ * surface tension, fixed 3 corrector passes, projection walls, hard-coded
+ * -9.81 y gravity in PCISPH). CONFIG is the scene text's method (Tait EOS,
+ * penalty walls, eta loop with min/max iterations, no surface tension). */
+enum { PSB_PROFILE_REF = 0, PSB_PROFILE_CONFIG = 1 };
+enum { PSB_WCSPH = 0, PSB_PCISPH = 1 };
+/* Initial pressure of each PCISPH step (CONFIG profile). */
+enum { PSB_WARM_ZERO = 0, PSB_WARM_PREVIOUS = 1 };
+
+/* Scene: the uniform per-particle parameters the reference keeps in
+ * per-particle arrays (SimulationData_SPHSystem.cpp:5-16), the grid of
+ * UniformGrid (UniformGrid.cuh:16-33: float Min, float sizeCell, cell
+ * counts) and the container box of BoxCollision. */
+typedef struct psb_scene {
+    int32_t n_max;              /* particle capacity */
+    float box_min[3], box_max[3];
+    float grid_min[3];          /* grid corner */
+    float cell;                 /* cell edge, >= h */
+    int32_t dims[3];            /* cells per axis */
+    double h;                   /* smoothing radius = interaction radius */
+    double mass, rho0, k, mu, sigma, l;
+    float particle_radius;      /* wall offset */
+    float dt;
+    float gravity[3];           /* acceleration, CONFIG profile and WCSPH */
+    int32_t profile, method;
+    int32_t min_iters, max_iters;
+    double eta;                 /* max (rho*-rho0)/rho0 accepted by the corrector loop */
+    double wall_k, wall_c;      /* penalty walls, 1/s^2 and 1/s */
+    int32_t nbr_cap;            /* neighbour slots per particle (0: 128) */
+    int32_t warm_start;         /* PSB_WARM_* */
+    double spacing;             /* rest lattice spacing of the CONFIG-profile PCISPH prototype
+                                   (0: (mass/rho0)^(1/3)) */
+} psb_scene;
+
+#define PSB_MAX_ITERS 64
+typedef struct psb_step_stats {
+    int32_t iters;              /* pressure corrections in the last step */
+    int32_t converged;
+    int32_t nbr_max;            /* largest neighbour count (self included) */
+    int32_t clamped;            /* particles whose cell was clamped into the grid */
+    int64_t nbr_total;
+    double err[PSB_MAX_ITERS + 1];   /* max (rho*-rho0)/rho0 of each density pass, FP64 */
+    int64_t steps;              /* steps taken by this context */
+    int64_t iters_total;        /* corrections summed over all steps */
+} psb_step_stats;
+
+typedef struct psb_ctx psb_ctx;
+
+/* Fields psb_read_field can copy out, in particle-id order. */
+enum {
+    PSB_FIELD_POS = 0,          /* float x3 */
+    PSB_FIELD_VEL = 1,          /* float x3, interpolated velocity (m_dVel[1]) */
+    PSB_FIELD_VEL_HALF = 2,     /* float x3, leap-frog velocity (m_dVelInterAp) */
+    PSB_FIELD_DENSITY = 3,      /* float: last density pass */
+    PSB_FIELD_PRESSURE = 4,     /* float */
+    PSB_FIELD_DENSITY_X = 5,    /* float: density at the step's start positions */
+    PSB_FIELD_FORCE_NP = 6,     /* float x3: non-pressure force density */
+    PSB_FIELD_NBR_COUNT = 7,    /* int32: neighbours incl. self */
+    PSB_FIELD_CELL_KEY = 8,     /* uint32: cell index */
+    PSB_FIELD_SORTED_ID = 9,    /* int32: particle id at each sorted slot (slot order, not id order) */
+    PSB_FIELD_SORTED_KEY = 10   /* uint32: cell index at each sorted slot (slot order) */
+};
+
+/* Replaces SPHSystem::init/PCI_SPHSystem's constructor allocations
+ * (SphSystem.cpp:57-113, PciSphSystem.cpp:7-24) and createGrid
+ * (UniformGrid.cu:17-49): sizes every buffer from the scene, no fixed caps. */
+int psb_create(const psb_scene* scene, psb_ctx** out);
+int psb_destroy(psb_ctx* ctx);
+
+/* Launch all work on `stream` (a cudaStream_t); NULL = the legacy stream. */
+int psb_set_stream(psb_ctx* ctx, void* stream);
+
+/* Replaces the particle upload of PCI_SPHSystem::_initialize
+ * (PciSphSystem.cpp:68-138): host arrays, particle-id order, xyz stride 3.
+ * vel/vel_half may be NULL (zero). pressure may be NULL (zero). */
+int psb_upload(psb_ctx* ctx, int32_t n, const float* pos, const float* vel, const float* vel_half,
+               const float* pressure);
+
+/* Same, from the reference's AoS double3 layout (m_hPos[1], m_hVel[1],
+ * m_hVelInterAp), converted once at this boundary. on_device != 0: the
+ * pointers are device memory (the reference's m_dPos[1] etc.). */
+int psb_upload_aos_f64(psb_ctx* ctx, int32_t n, const double* pos, const double* vel, const double* vel_half,
+                       int32_t on_device);
+
+/* Replaces the per-step device-to-host copies of interpolateVelocities
+ * (SphSystem.cpp:337-345). Any pointer may be NULL. Blocks until done. */
+int psb_download(psb_ctx* ctx, float* pos, float* vel, float* vel_half, float* density, float* pressure);
+int psb_download_aos_f64(psb_ctx* ctx, double* pos, double* vel, double* vel_half, int32_t on_device);
+
+/* Replaces PCI_SPHSystem::update (PciSphSystem.cpp:163-204) and
+ * SPHSystem::update (SphSystem.cpp:273-297) minus emission: grid, sort,
+ * neighbours, the SPH/PCISPH step, walls, velocity interpolation. */
+int psb_step(psb_ctx* ctx, int32_t nsteps);
+
+/* Replaces reinitCells + storeParticles + searchNeighbooring
+ * (UniformGrid.cu:64-99, UniformGridKernel.cu:30-95): cell keys, stable
+ * sort by (cell, id), cell ranges and neighbour lists at the current
+ * positions, then the density there (compute_Density_PCI,
+ * PciSphSystem_Kernel.cu:70-85). */
+int psb_build_neighbors(psb_ctx* ctx);
+
+/* Copies one field out (see PSB_FIELD_*); `bytes` is the destination size. */
+int psb_read_field(psb_ctx* ctx, int32_t field, void* dst, size_t bytes);
+
+int psb_get_stats(psb_ctx* ctx, psb_step_stats* out);
+
+/* Per-kernel CUDA-event timing: enable, then read accumulated
+ * (launches, milliseconds) per kernel name. */
+int psb_profile_enable(psb_ctx* ctx, int32_t on);
+int psb_profile_read(psb_ctx* ctx, int32_t index, char* name, size_t name_len, int64_t* launches, double* ms);
+int psb_profile_reset(psb_ctx* ctx);
+
+/* Host-side scene generator: lattice block with ids x-fastest, positions
+ * origin + (i+0.5)*spacing + jitter, jitter uniform in [-J, J) from
+ * SplitMix64(seed ^ (3*(id+id0)+axis)), rounded once to float. xyz stride 3.
+ * Stands in for the reference's EmitterBox (EmitterBox.cpp:29-47). */
+int psb_lattice(const int32_t nxyz[3], double spacing, const double origin[3], double jitter, uint64_t seed,
+                int32_t id0, float* pos);
+
+const char* psb_status_string(int32_t status);
+const char* psb_last_error(const psb_ctx* ctx);
+int32_t psb_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSB_H */

@@ -1,0 +1,299 @@
+"""ctypes bindings of the oracle (test infrastructure only).
+
+Two checkers live under oracle/:
+  * liboracle.so -- our FP64 C restatement of the hot path (psb_oracle.c);
+  * _ref/libpsbref.so -- the reference's own device kernels compiled as host
+    code through refshim/ (built only where the reference tree exists; the
+    .so then travels with the repository).
+Only tests/, the smoke check and bench.py's CPU-baseline legs import this
+package. The product (psb_project_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libpsbref.so")
+REF_SRC = os.environ.get("PSB_REFERENCE_SRC", "/root/reference/src")
+
+ORC_MAX_ITERS = 64
+
+
+def build(with_reference: bool = True) -> None:
+    """Compile the oracle (and, where the reference tree exists, oracle/_ref)."""
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+    if with_reference and os.path.isdir(REF_SRC):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_SRC={REF_SRC}"], check=True)
+
+
+class OrcParams(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32),
+        ("box_min", ctypes.c_float * 3), ("box_max", ctypes.c_float * 3),
+        ("grid_min", ctypes.c_float * 3), ("cell", ctypes.c_float), ("dims", ctypes.c_int32 * 3),
+        ("h", ctypes.c_double), ("mass", ctypes.c_double), ("rho0", ctypes.c_double), ("k", ctypes.c_double),
+        ("mu", ctypes.c_double), ("sigma", ctypes.c_double), ("l", ctypes.c_double),
+        ("particle_radius", ctypes.c_float), ("dt", ctypes.c_float), ("gravity", ctypes.c_float * 3),
+        ("profile", ctypes.c_int32), ("method", ctypes.c_int32),
+        ("min_iters", ctypes.c_int32), ("max_iters", ctypes.c_int32),
+        ("eta", ctypes.c_double), ("wall_k", ctypes.c_double), ("wall_c", ctypes.c_double),
+        ("float_state", ctypes.c_int32), ("warm_start", ctypes.c_int32), ("spacing", ctypes.c_double),
+    ]
+
+
+class OrcState(ctypes.Structure):
+    _fields_ = [("pos", ctypes.c_void_p), ("vel", ctypes.c_void_p), ("vel_ap", ctypes.c_void_p),
+                ("rho", ctypes.c_void_p), ("p", ctypes.c_void_p)]
+
+
+class OrcStats(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int32), ("converged", ctypes.c_int32),
+                ("err", ctypes.c_double * (ORC_MAX_ITERS + 1)), ("nbr_total", ctypes.c_int64),
+                ("nbr_max", ctypes.c_int32), ("clamped", ctypes.c_int32)]
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build(with_reference=False)
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        L.orc_lattice.argtypes = [P, ctypes.c_double, P, ctypes.c_double, ctypes.c_uint64, ctypes.c_int32, P]
+        L.orc_lattice.restype = None
+        L.orc_cell_keys.argtypes = [ctypes.c_int32, P, P, ctypes.c_float, P, P, P]
+        L.orc_cell_keys.restype = None
+        L.orc_sort_perm.argtypes = [ctypes.c_int32, P, P]
+        L.orc_sort_perm.restype = None
+        L.orc_neighbors.argtypes = [ctypes.POINTER(OrcParams), P, ctypes.c_int32, P, P]
+        L.orc_neighbors.restype = ctypes.c_int64
+        L.orc_density.argtypes = [ctypes.POINTER(OrcParams), P, P, P, ctypes.c_int32, ctypes.c_int, P]
+        L.orc_density.restype = None
+        L.orc_step.argtypes = [ctypes.POINTER(OrcParams), ctypes.POINTER(OrcState), ctypes.POINTER(OrcStats), P, P, P]
+        L.orc_step.restype = ctypes.c_int
+        L.orc_pci_delta.argtypes = [ctypes.POINTER(OrcParams)]
+        L.orc_pci_delta.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_PATH)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise FileNotFoundError(f"{REF_PATH} is not built (make -C oracle ref)")
+        L = ctypes.CDLL(REF_PATH)
+        P = ctypes.c_void_p
+        L.ref_create.argtypes = [ctypes.c_int, P, ctypes.c_float, P]
+        L.ref_create.restype = P
+        L.ref_destroy.argtypes = [P]
+        L.ref_set.argtypes = [P, ctypes.c_char_p, P]
+        L.ref_get.argtypes = [P, ctypes.c_char_p, P]
+        L.ref_search.argtypes = [P]
+        L.ref_neighbors.argtypes = [P, P, P]
+        L.ref_density_pci.argtypes = [P]
+        L.ref_pcisph_update.argtypes = [P, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_float, P, P]
+        L.ref_wcsph_update.argtypes = [P, ctypes.c_float, P, ctypes.c_float, ctypes.c_int, ctypes.c_float, P, P]
+        L.ref_dem_update.argtypes = [P, ctypes.c_float, P, ctypes.c_float, ctypes.c_int, ctypes.c_float, P, P]
+        _ref = L
+    return _ref
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def lattice(nxyz, spacing, origin, jitter, seed, id0=0) -> np.ndarray:
+    n = int(nxyz[0]) * int(nxyz[1]) * int(nxyz[2])
+    out = np.empty((n, 3), np.float32)
+    nx = np.asarray(nxyz, np.int32)
+    org = np.asarray(origin, np.float64)
+    lib().orc_lattice(_ptr(nx), float(spacing), _ptr(org), float(jitter), int(seed) & (2**64 - 1), int(id0), _ptr(out))
+    return out
+
+
+def scene_positions(scene) -> np.ndarray:
+    return np.concatenate([lattice(b.nxyz, b.spacing, b.origin, b.jitter, b.seed, b.id0) for b in scene.blocks])
+
+
+def params(scene, *, float_state: bool = False, n: Optional[int] = None) -> OrcParams:
+    p = OrcParams()
+    p.n = scene.n if n is None else n
+    p.box_min[:] = list(scene.box_min)
+    p.box_max[:] = list(scene.box_max)
+    p.grid_min[:] = list(scene.grid_min)
+    p.cell = scene.cell
+    p.dims[:] = list(scene.dims)
+    p.h, p.mass, p.rho0, p.k = scene.h, scene.mass, scene.rho0, scene.k
+    p.mu, p.sigma, p.l = scene.mu, scene.sigma, scene.l
+    p.particle_radius, p.dt = scene.particle_radius, scene.dt
+    p.gravity[:] = list(scene.gravity)
+    p.profile, p.method = scene.profile, scene.method
+    p.min_iters, p.max_iters, p.eta = scene.min_iters, scene.max_iters, scene.eta
+    p.wall_k, p.wall_c = scene.wall_k, scene.wall_c
+    p.float_state = 1 if float_state else 0
+    p.warm_start = 1 if scene.warm_start else 0
+    p.spacing = scene.spacing
+    return p
+
+
+def pci_delta(scene) -> float:
+    P = params(scene)
+    return lib().orc_pci_delta(ctypes.byref(P))
+
+
+def cell_keys(scene, pos) -> np.ndarray:
+    pos = np.ascontiguousarray(pos, np.float64)
+    n = pos.shape[0]
+    keys = np.empty(n, np.uint32)
+    ncl = ctypes.c_int32(0)
+    gmin = np.asarray(scene.grid_min, np.float32)
+    dims = np.asarray(scene.dims, np.int32)
+    lib().orc_cell_keys(n, _ptr(pos), _ptr(gmin), scene.cell, _ptr(dims), _ptr(keys), ctypes.addressof(ncl))
+    return keys
+
+
+def sort_perm(keys) -> np.ndarray:
+    keys = np.ascontiguousarray(keys, np.uint32)
+    perm = np.empty(keys.shape[0], np.int32)
+    lib().orc_sort_perm(keys.shape[0], _ptr(keys), _ptr(perm))
+    return perm
+
+
+def neighbors(scene, pos, with_lists=True):
+    """(counts, lists) at pos; lists is an (n, cap) int32 array padded with -1."""
+    pos = np.ascontiguousarray(pos, np.float64)
+    P = params(scene, n=pos.shape[0])
+    counts = np.empty(pos.shape[0], np.int32)
+    lib().orc_neighbors(ctypes.byref(P), _ptr(pos), 0, _ptr(counts), None)
+    if not with_lists:
+        return counts, None
+    cap = max(1, int(counts.max()))
+    lists = np.full((pos.shape[0], cap), -1, np.int32)
+    lib().orc_neighbors(ctypes.byref(P), _ptr(pos), cap, _ptr(counts), _ptr(lists))
+    return counts, lists
+
+
+def density(scene, pos, counts, lists, clamp) -> np.ndarray:
+    pos = np.ascontiguousarray(pos, np.float64)
+    P = params(scene, n=pos.shape[0])
+    rho = np.empty(pos.shape[0], np.float64)
+    lists = np.ascontiguousarray(lists, np.int32)
+    lib().orc_density(ctypes.byref(P), _ptr(pos), _ptr(np.ascontiguousarray(counts, np.int32)), _ptr(lists),
+                      lists.shape[1], 1 if clamp else 0, _ptr(rho))
+    return rho
+
+
+class OracleSim:
+    """FP64 state in particle-id order, stepped by orc_step."""
+
+    def __init__(self, scene, pos, vel=None, vel_half=None, pressure=None, *, float_state=False):
+        n = pos.shape[0]
+        self.scene = scene
+        self.P = params(scene, float_state=float_state, n=n)
+        self.pos = np.ascontiguousarray(pos, np.float64).copy()
+        self.vel = np.zeros((n, 3)) if vel is None else np.ascontiguousarray(vel, np.float64).copy()
+        self.vel_half = np.zeros((n, 3)) if vel_half is None else np.ascontiguousarray(vel_half, np.float64).copy()
+        self.rho = np.zeros(n)
+        self.p = np.zeros(n) if pressure is None else np.ascontiguousarray(pressure, np.float64).copy()
+        self.rho_x = np.zeros(n)
+        self.f_np = np.zeros((n, 3))
+        self.nbr = np.zeros(n, np.int32)
+        self.stats = OrcStats()
+
+    def step(self):
+        S = OrcState(self.pos.ctypes.data, self.vel.ctypes.data, self.vel_half.ctypes.data,
+                     self.rho.ctypes.data, self.p.ctypes.data)
+        rc = lib().orc_step(ctypes.byref(self.P), ctypes.byref(S), ctypes.byref(self.stats),
+                            _ptr(self.rho_x), _ptr(self.f_np), _ptr(self.nbr))
+        if rc != 0:
+            raise RuntimeError(f"orc_step failed: {rc}")
+        return self.stats
+
+
+class RefSim:
+    """The reference's kernels on the CPU, AoS double state (oracle/_ref)."""
+
+    def __init__(self, scene, pos, vel=None, vel_half=None):
+        L = ref_lib()
+        n = pos.shape[0]
+        self.n = n
+        self.scene = scene
+        gmin = np.asarray(scene.grid_min, np.float32)
+        dims = np.asarray(scene.dims, np.int32)
+        self.h = L.ref_create(n, _ptr(gmin), scene.cell, _ptr(dims))
+        if not self.h:
+            raise RuntimeError("ref_create failed")
+        z3 = np.zeros((n, 3))
+        p = np.ascontiguousarray(pos, np.float64)
+        v = z3 if vel is None else np.ascontiguousarray(vel, np.float64)
+        vh = z3 if vel_half is None else np.ascontiguousarray(vel_half, np.float64)
+        # State as _initialize leaves it, with the restore buffers filled
+        # (the reference leaves some unset: PciSphSystem.cpp:93,127-130).
+        for name, arr in (("pos", p), ("pos_old", p), ("r_pos", p), ("r_pos_old", p), ("vel", v), ("vel_old", v),
+                          ("vel_ap", vh), ("vel_av", vh), ("r_vel_ap", vh), ("r_vel_av", vh)):
+            self.set(name, arr)
+        ones = np.ones(n)
+        for name, val in (("mass", scene.mass), ("radius", scene.h), ("rho0", scene.rho0), ("k", scene.k),
+                          ("mu", scene.mu), ("sigma", scene.sigma), ("threshold", scene.l), ("l", scene.l)):
+            self.set(name, ones * val)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref_lib().ref_destroy(self.h)
+            self.h = None
+
+    def set(self, name, arr):
+        arr = np.ascontiguousarray(arr, np.float64)
+        if ref_lib().ref_set(self.h, name.encode(), _ptr(arr)) != 0:
+            raise KeyError(name)
+
+    def get(self, name, width):
+        out = np.empty((self.n, width) if width > 1 else self.n, np.float64)
+        if ref_lib().ref_get(self.h, name.encode(), _ptr(out)) != 0:
+            raise KeyError(name)
+        return out
+
+    def search(self):
+        rc = ref_lib().ref_search(self.h)
+        if rc != 0:
+            raise RuntimeError(f"ref_search: {rc}")
+        counts = np.empty(self.n, np.int32)
+        ref_lib().ref_neighbors(self.h, _ptr(counts), None)
+        return counts
+
+    def density_pci(self):
+        ref_lib().ref_density_pci(self.h)
+        return self.get("density", 1)
+
+    def pcisph_update(self, iters=3, collide=True):
+        s = self.scene
+        bmin = np.asarray(s.box_min, np.float32)
+        bmax = np.asarray(s.box_max, np.float32)
+        rc = ref_lib().ref_pcisph_update(self.h, s.dt, iters, 1 if collide else 0, s.particle_radius, _ptr(bmin), _ptr(bmax))
+        if rc != 0:
+            raise RuntimeError(f"ref_pcisph_update: {rc}")
+
+    def wcsph_update(self, collide=True):
+        s = self.scene
+        bmin = np.asarray(s.box_min, np.float32)
+        bmax = np.asarray(s.box_max, np.float32)
+        g = np.asarray([0.0, -1.0, 0.0], np.float32)
+        rc = ref_lib().ref_wcsph_update(self.h, s.dt, _ptr(g), np.float32(9.81), 1 if collide else 0,
+                                        s.particle_radius, _ptr(bmin), _ptr(bmax))
+        if rc != 0:
+            raise RuntimeError(f"ref_wcsph_update: {rc}")

@@ -1,0 +1,595 @@
+/*
+ * psb_oracle.c -- FP64 CPU restatement of the PSB particle-simulation hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the GPU path and the "port" CPU
+ * baseline. Only tests/, the smoke check and bench.py's CPU-baseline leg use
+ * it; the product never links it.
+ *
+ * Reference-compatible profile (ORC_PROFILE_REF): each formula below is the
+ * reference's, restated term by term with the same association order so the
+ * results agree with the reference kernels run on the CPU (oracle/_ref) to
+ * ~1e-12 relative. Sources (paths inside the reference project):
+ *   cell index ............ src/Utils/Neighborhood/UniformGrid/UniformGridKernel.cu:43-55
+ *   neighbour test ........ UniformGridKernel.cu:58-95 (sqrt(d.d) <= h_i, self included)
+ *   WCSPH density/EOS ..... src/Kernel/System/Fluid_System/SPHSystem/SPH/SphKernel.cu:9-27
+ *   WCSPH forces .......... SphKernel.cu:32-91
+ *   gravity (force dens.) . src/Kernel/ForcesExt/Constante/ForceExt_Constante.cu:15-23
+ *   leap-frog ............. SphKernel.cu:95-124, interpolation SphKernel.cu:128-135
+ *   PCISPH density ........ .../PCISPH/PciSphSystem_Kernel.cu:70-85
+ *   PCISPH non-pressure ... PciSphSystem_Kernel.cu:117-170 (p <- 0, sigma <- 0.0728, g = -9.81 y)
+ *   PCISPH pressure update  PciSphSystem_Kernel.cu:36-67
+ *   PCISPH pressure force . PciSphSystem_Kernel.cu:88-114
+ *   PCISPH sequence ....... .../PCISPH/PciSphSystem.cu:8-68, PciSphSystem.cpp:163-204
+ *   box walls ............. src/Kernel/Collision/BoxCollision/BoxCollision_Kernel.cu:7-34
+ * The reference's predict-then-restore passes are restated as a predict that
+ * leaves the saved state untouched; the values are the same.
+ *
+ * Config profile (ORC_PROFILE_CONFIG): the scene text's method -- Tait EOS,
+ * penalty walls, eta-controlled corrector loop with min/max iterations, no
+ * surface tension, kernels cut off at r >= h. No reference counterpart.
+ */
+#include "psb_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define PI_D 3.14159265358979323846
+
+/* Storage rounding: with float_state the oracle keeps every stored array in
+ * float, at the same points the GPU path stores FP32. */
+#define RND(P, x) ((P)->float_state ? (double)(float)(x) : (x))
+
+uint64_t orc_splitmix64(uint64_t x) {
+    uint64_t z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+void orc_lattice(const int32_t nxyz[3], double spacing, const double origin[3], double jitter,
+                 uint64_t seed, int32_t id0, float* pos3) {
+    const int64_t n = (int64_t)nxyz[0] * nxyz[1] * nxyz[2];
+    for (int64_t id = 0; id < n; ++id) {
+        const int64_t ijk[3] = {id % nxyz[0], (id / nxyz[0]) % nxyz[1], id / ((int64_t)nxyz[0] * nxyz[1])};
+        for (int a = 0; a < 3; ++a) {
+            const uint64_t z = orc_splitmix64(seed ^ ((uint64_t)(id + id0) * 3u + (uint64_t)a));
+            const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);   /* [0,1) */
+            const double j = jitter * (2.0 * u - 1.0);
+            const double x = origin[a] + ((double)ijk[a] + 0.5) * spacing + j;
+            pos3[3 * id + a] = (float)x;
+        }
+    }
+}
+
+/* Clamped into [0, dim-1] in double before the conversion to int, so that
+ * infinities, NaN and huge coordinates land in the border cells. */
+static inline int cell_coord(double x, float mn, float cell, int dim, int* clamped) {
+    const double t = floor((x - (double)mn) / (double)cell);
+    if (!(t >= 0.0)) { *clamped = 1; return 0; }
+    if (t >= (double)dim) { *clamped = 1; return dim - 1; }
+    return (int)t;
+}
+
+void orc_cell_keys(int32_t n, const double* pos, const float grid_min[3], float cell, const int32_t dims[3],
+                   uint32_t* keys, int32_t* nclamped) {
+    int32_t cl = 0;
+#pragma omp parallel for reduction(+ : cl) schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+        int c = 0;
+        const int a = cell_coord(pos[3 * i + 0], grid_min[0], cell, dims[0], &c);
+        const int b = cell_coord(pos[3 * i + 1], grid_min[1], cell, dims[1], &c);
+        const int d = cell_coord(pos[3 * i + 2], grid_min[2], cell, dims[2], &c);
+        keys[i] = (uint32_t)a + (uint32_t)b * (uint32_t)dims[0] + (uint32_t)d * (uint32_t)dims[0] * (uint32_t)dims[1];
+        cl += c;
+    }
+    if (nclamped) *nclamped = cl;
+}
+
+/* Counting sort over the cell range: stable, so ties keep increasing id. */
+static void sort_by_key(int32_t n, const uint32_t* keys, uint32_t ncells, int32_t* perm, int32_t* start /* ncells+1 */) {
+    memset(start, 0, sizeof(int32_t) * ((size_t)ncells + 1));
+    for (int32_t i = 0; i < n; ++i) start[keys[i] + 1]++;
+    for (uint32_t c = 0; c < ncells; ++c) start[c + 1] += start[c];
+    int32_t* fill = (int32_t*)malloc(sizeof(int32_t) * ((size_t)ncells + 1));
+    memcpy(fill, start, sizeof(int32_t) * ((size_t)ncells + 1));
+    for (int32_t i = 0; i < n; ++i) perm[fill[keys[i]]++] = i;
+    free(fill);
+}
+
+void orc_sort_perm(int32_t n, const uint32_t* keys, int32_t* perm) {
+    uint32_t mx = 0;
+    for (int32_t i = 0; i < n; ++i) mx = keys[i] > mx ? keys[i] : mx;
+    int32_t* start = (int32_t*)malloc(sizeof(int32_t) * ((size_t)mx + 2));
+    sort_by_key(n, keys, mx + 1, perm, start);
+    free(start);
+}
+
+/* Reference neighbour test: length(x_i - x_j) <= radius_i, evaluated as
+ * sqrt((dx*dx + dy*dy) + dz*dz) in double (double3.h:15-47). */
+static inline int is_neighbor(const double* xi, const double* xj, double h) {
+    const double dx = xi[0] - xj[0], dy = xi[1] - xj[1], dz = xi[2] - xj[2];
+    return sqrt(dx * dx + dy * dy + dz * dz) <= h;
+}
+
+int64_t orc_neighbors(const orc_params* P, const double* pos, int32_t cap, int32_t* counts, int32_t* list) {
+    const int32_t n = P->n;
+    const uint32_t ncells = (uint32_t)P->dims[0] * (uint32_t)P->dims[1] * (uint32_t)P->dims[2];
+    uint32_t* keys = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)n);
+    int32_t* perm = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+    int32_t* start = (int32_t*)malloc(sizeof(int32_t) * ((size_t)ncells + 1));
+    orc_cell_keys(n, pos, P->grid_min, P->cell, P->dims, keys, NULL);
+    sort_by_key(n, keys, ncells, perm, start);
+    const int nx = P->dims[0], ny = P->dims[1], nz = P->dims[2];
+    int64_t total = 0;
+    int overflow = 0;
+#pragma omp parallel for reduction(+ : total) reduction(| : overflow) schedule(dynamic, 256)
+    for (int32_t i = 0; i < n; ++i) {
+        const uint32_t key = keys[i];
+        const int ci = (int)(key % (uint32_t)nx), cj = (int)((key / (uint32_t)nx) % (uint32_t)ny),
+                  ck = (int)(key / ((uint32_t)nx * (uint32_t)ny));
+        int32_t cnt = 0;
+        /* z outer, x inner: cells, and so candidates, come in increasing (key, id). */
+        for (int k = ck - 1; k <= ck + 1; ++k) {
+            if (k < 0 || k >= nz) continue;
+            for (int j = cj - 1; j <= cj + 1; ++j) {
+                if (j < 0 || j >= ny) continue;
+                for (int a = ci - 1; a <= ci + 1; ++a) {
+                    if (a < 0 || a >= nx) continue;
+                    const uint32_t c = (uint32_t)a + (uint32_t)j * nx + (uint32_t)k * nx * ny;
+                    for (int32_t t = start[c]; t < start[c + 1]; ++t) {
+                        const int32_t jd = perm[t];
+                        if (is_neighbor(&pos[3 * (size_t)i], &pos[3 * (size_t)jd], P->h)) {
+                            if (list) {
+                                if (cnt < cap) list[(size_t)i * cap + cnt] = jd;
+                                else overflow = 1;
+                            }
+                            cnt++;
+                        }
+                    }
+                }
+            }
+        }
+        counts[i] = cnt;
+        total += cnt;
+    }
+    free(keys);
+    free(perm);
+    free(start);
+    return overflow ? -1 : total;
+}
+
+static inline double len3(const double* v) { return sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+static inline double dmax(double a, double b) { return a > b ? a : b; }
+
+/* ---- config-profile wall boundary ---------------------------------------
+ * Each box face is backed by a half-space of virtual fluid particles on a
+ * lattice of the rest spacing s, layers at (k + 1/2) s behind the face
+ * (Harada, Koshizuka, Kawaguchi 2007: wall weight functions). Averaged over
+ * the particle's position along the face, the layer sums have closed forms:
+ *   density   sum (1 - r^2/h^2)^3          = pi h^2/(4 s^2) sum_k (1 - z_k^2/h^2)^4
+ *   gradient  sum (1 - r/h)^2 (n . x^)      = 2 pi h/(3 s^2) sum_k z_k (1 - z_k/h)^3
+ * with z_k = d + (k + 1/2) s the layer's distance and d >= 0 the particle's
+ * distance to the face. The virtual particles carry the particle's own
+ * pressure (mirror), so the wall pushes with 2 p_i/rho_i^2 times the
+ * gradient sum along the face normal. */
+static double wall_spacing(const orc_params* P) { return P->spacing > 0 ? P->spacing : cbrt(P->mass / P->rho0); }
+
+static double wall_z(double d, double h, double s) {
+    if (d < 0) d = 0;
+    double z = 0;
+    for (int k = 0;; ++k) {
+        const double zk = d + (k + 0.5) * s;
+        if (zk >= h) break;
+        const double t = 1.0 - zk * zk / (h * h);
+        z += t * t * t * t;
+    }
+    return z * PI_D * h * h / (4.0 * s * s);
+}
+
+static double wall_g(double d, double h, double s) {
+    if (d < 0) d = 0;
+    double g = 0;
+    for (int k = 0;; ++k) {
+        const double zk = d + (k + 0.5) * s;
+        if (zk >= h) break;
+        const double t = 1.0 - zk / h;
+        g += zk * t * t * t;
+    }
+    return g * 2.0 * PI_D * h / (3.0 * s * s);
+}
+
+/* Sum over the six faces: density term (normalised) and gradient vector
+ * (pointing into the box). */
+static void wall_terms(const orc_params* P, const double* x, double* z, double g[3]) {
+    const double h = P->h, s = wall_spacing(P);
+    *z = 0;
+    g[0] = g[1] = g[2] = 0;
+    for (int e = 0; e < 3; ++e) {
+        const double dl = x[e] - (double)P->box_min[e], dh = (double)P->box_max[e] - x[e];
+        if (dl < h) { *z += wall_z(dl, h, s); g[e] += wall_g(dl, h, s); }
+        if (dh < h) { *z += wall_z(dh, h, s); g[e] -= wall_g(dh, h, s); }
+    }
+}
+
+/* Poly6 density term; reference form of compute_Density_PCI (PciSphSystem_Kernel.cu:79-81). */
+void orc_density(const orc_params* P, const double* pos, const int32_t* counts, const int32_t* list, int32_t cap,
+                 int clamp, double* rho) {
+    const double h = P->h, m = P->mass;
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < P->n; ++i) {
+        double s = 0.0;
+        for (int32_t t = 0; t < counts[i]; ++t) {
+            const int32_t j = list[(size_t)i * cap + t];
+            double dv[3] = {pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1], pos[3 * i + 2] - pos[3 * j + 2]};
+            const double d = len3(dv);
+            if (clamp && d >= h) continue;
+            s += (315 / (64 * PI_D * pow(h, 9))) * pow((h * h) - (d * d), 3) * m;
+        }
+        if (clamp) {
+            double z, g[3];
+            wall_terms(P, &pos[3 * i], &z, g);
+            s += 315 * m / (64 * PI_D * h * h * h) * z;
+        }
+        rho[i] = RND(P, s);
+    }
+}
+
+/* ---- per-pair sweeps ------------------------------------------------------ */
+
+/* Non-pressure force density at (pos, vel, rho). Reference profile, PCISPH:
+ * compute_Viscosity_SurfaceTension_Force_PCI (PciSphSystem_Kernel.cu:117-170).
+ * Reference profile, WCSPH: the viscosity and surface terms of internalForces
+ * (SphKernel.cu:32-91) plus the constant force with rho as mass
+ * (ForceExt_Constante.cu:15-23). Config: viscosity + rho*g. */
+static void nonpressure_forces(const orc_params* P, const double* pos, const double* vel, const double* rho,
+                               const int32_t* counts, const int32_t* list, int32_t cap, double* f) {
+    const double h = P->h, m = P->mass, mu = P->mu;
+    const int ref = P->profile == ORC_PROFILE_REF, pci = P->method == ORC_PCISPH;
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < P->n; ++i) {
+        double fv[3] = {0, 0, 0}, nrm[3] = {0, 0, 0}, fsurf = 0.0;
+        for (int32_t t = 0; t < counts[i]; ++t) {
+            const int32_t j = list[(size_t)i * cap + t];
+            const double dv[3] = {pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1], pos[3 * i + 2] - pos[3 * j + 2]};
+            const double d = len3(dv);
+            if (!(d > 0)) continue;
+            if (!ref && d >= h) continue;
+            const double a = PI_D * pow(h, 6);
+            const double m_m = 45 * (h - d) / a;
+            const double c = (mu + mu) / 2;
+            const double inv_rho = 1.0 / rho[j];
+            for (int e = 0; e < 3; ++e) fv[e] = fv[e] + c * (vel[3 * j + e] - vel[3 * i + e]) * m * m_m * inv_rho;
+            if (ref) {
+                const double b = 32 * PI_D * (double)powf((float)h, 9.0f);
+                const double m_d = -(945 / b) * ((h * h) - (d * d)) * ((3 * h * h) - (7 * d * d));
+                fsurf += m_d * (m / rho[j]);
+                const double aN = pci ? 32 * PI_D * pow(h, 9) : b;
+                const double mk = -945 / aN;
+                const double w2 = pow((h * h) - (d * d), 2);
+                for (int e = 0; e < 3; ++e) nrm[e] = nrm[e] + dv[e] * (m / rho[j]) * w2 * mk;
+            }
+        }
+        double fs[3] = {0, 0, 0};
+        if (ref) {
+            const double lN = len3(nrm);
+            if (lN >= P->l) {
+                const double sigma = pci ? 0.0728 : P->sigma;
+                const double inv = 1.0 / lN;
+                for (int e = 0; e < 3; ++e) fs[e] = fsurf * (-sigma) * nrm[e] * inv;
+            }
+        }
+        double g[3];
+        if (ref && pci) {
+            g[0] = 0.0; g[1] = -9.81 * rho[i]; g[2] = 0.0;     /* forcesAccum, PciSphSystem_Kernel.cu:168 */
+        } else {
+            for (int e = 0; e < 3; ++e) g[e] = (double)P->gravity[e] * rho[i];
+        }
+        for (int e = 0; e < 3; ++e) f[3 * i + e] = RND(P, (g[e] + fv[e]) + fs[e]);
+    }
+}
+
+/* Symmetric spiky pressure force density -rho_i sum m (p_i/rho_i^2 + p_j/rho_j^2) gradW
+ * (SphKernel.cu:53-61,79; PciSphSystem_Kernel.cu:96-112). */
+static void pressure_forces(const orc_params* P, const double* pos, const double* rho, const double* p,
+                            const int32_t* counts, const int32_t* list, int32_t cap, double* fp) {
+    const double h = P->h, m = P->mass;
+    const int clamp = P->profile == ORC_PROFILE_CONFIG;
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < P->n; ++i) {
+        double acc[3] = {0, 0, 0};
+        const double pV1 = p[i] / (rho[i] * rho[i]);
+        for (int32_t t = 0; t < counts[i]; ++t) {
+            const int32_t j = list[(size_t)i * cap + t];
+            const double dv[3] = {pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1], pos[3 * i + 2] - pos[3 * j + 2]};
+            const double d = len3(dv);
+            if (!(d > 0)) continue;
+            if (clamp && d >= h) continue;
+            const double inv = 1.0 / d;
+            const double pV2 = p[j] / (rho[j] * rho[j]);
+            const double a = PI_D * pow(h, 6);
+            const double s = -45 * pow(h - d, 2) / a;
+            for (int e = 0; e < 3; ++e) acc[e] = acc[e] + (dv[e] * inv) * s * (pV1 + pV2) * m;
+        }
+        if (clamp) {
+            /* -sum m (2 pV1) gradW over the virtual particles = +2 pV1 m G g */
+            double z, g[3];
+            wall_terms(P, &pos[3 * i], &z, g);
+            const double G = 45 / (PI_D * h * h * h * h);
+            for (int e = 0; e < 3; ++e) acc[e] -= 2 * pV1 * m * G * g[e];
+        }
+        for (int e = 0; e < 3; ++e) fp[3 * i + e] = acc[e] * (-rho[i]);
+    }
+}
+
+double orc_pci_delta(const orc_params* P) {
+    const double h = P->h, m = P->mass, rho0 = P->rho0, dt = (double)P->dt;
+    const double s = P->spacing > 0 ? P->spacing : cbrt(m / rho0);
+    const double G = 45.0 / (PI_D * h * h * h * h);
+    const int R = (int)ceil(h / s);
+    double W1[3] = {0, 0, 0}, W2 = 0;
+    for (int k = -R; k <= R; ++k)
+        for (int j = -R; j <= R; ++j)
+            for (int i = -R; i <= R; ++i) {
+                if (!i && !j && !k) continue;
+                const double r = s * sqrt((double)(i * i + j * j + k * k));
+                if (r >= h) continue;
+                const double g = G * (1.0 - r / h) * (1.0 - r / h);
+                const double d[3] = {i * s / r, j * s / r, k * s / r};
+                for (int e = 0; e < 3; ++e) W1[e] += -g * d[e];
+                W2 += g * g;
+            }
+    const double beta = 2.0 * (m * dt / rho0) * (m * dt / rho0);
+    return 1.0 / (beta * (W1[0] * W1[0] + W1[1] * W1[1] + W1[2] * W1[2] + W2));
+}
+
+/* Config profile: p_i = max(0, p_i + delta (rho*_i - rho0)) for every
+ * particle with the prototype delta (orc_pci_delta). */
+static void pressure_update_config(const orc_params* P, const double* rho, double* p) {
+    const double delta = orc_pci_delta(P);
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < P->n; ++i) {
+        const double v = p[i] + delta * (rho[i] - P->rho0);
+        p[i] = RND(P, v > 0 ? v : 0.0);
+    }
+}
+
+/* PCISPH pressure increment (PciSphSystem_Kernel.cu:43-64): only compressed
+ * particles change, p += (rho - rho0) / (beta (|sum gradW|^2 + sum |gradW|^2)). */
+static void pressure_update(const orc_params* P, const double* pos, const double* rho, const int32_t* counts,
+                            const int32_t* list, int32_t cap, double* p) {
+    const double h = P->h, m = P->mass, rho0 = P->rho0;
+    const double dt = (double)P->dt;
+    const int clamp = P->profile == ORC_PROFILE_CONFIG;
+    if (clamp) { pressure_update_config(P, rho, p); return; }
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < P->n; ++i) {
+        if (!(rho[i] > rho0)) continue;
+        const double beta = 2 * pow(m * dt / rho0, 2);
+        double press = rho[i] - rho0;
+        double W1[3] = {0, 0, 0}, W2 = 0;
+        for (int32_t t = 0; t < counts[i]; ++t) {
+            const int32_t j = list[(size_t)i * cap + t];
+            const double dv[3] = {pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1], pos[3 * i + 2] - pos[3 * j + 2]};
+            const double d = len3(dv);
+            if (!(d > 0)) continue;
+            if (clamp && d >= h) continue;
+            const double inv = 1.0 / d;
+            const double a = PI_D * pow(h, 6);
+            const double s = -45 * pow(h - d, 2) / a;
+            double dW[3];
+            for (int e = 0; e < 3; ++e) dW[e] = (dv[e] * inv) * s;
+            W2 += dW[0] * dW[0] + dW[1] * dW[1] + dW[2] * dW[2];
+            for (int e = 0; e < 3; ++e) W1[e] = W1[e] + dW[e];
+        }
+        if (W2 > 0) {
+            press = -press / (beta * (-(W1[0] * W1[0] + W1[1] * W1[1] + W1[2] * W1[2]) - W2));
+            p[i] = RND(P, p[i] + press);
+        }
+    }
+}
+
+/* Penalty walls (config profile): a = K*depth - C*v_n along each violated
+ * wall normal, depth measured from the wall offset by the particle radius. */
+static void wall_accel(const orc_params* P, const double* x, const double* v, double* a) {
+    for (int e = 0; e < 3; ++e) {
+        a[e] = 0.0;
+        /* no-penetration backstop at the faces; the wall boundary above
+         * keeps particles off them in normal flow */
+        const float lo = P->box_min[e], hi = P->box_max[e];
+        if (x[e] < lo) a[e] += P->wall_k * (lo - x[e]) - P->wall_c * v[e];
+        if (x[e] > hi) a[e] += -P->wall_k * (x[e] - hi) - P->wall_c * v[e];
+    }
+}
+
+/* collisionBox (BoxCollision_Kernel.cu:7-34) on (pos, vel_ap): the bounds
+ * Max - r and Min + r are float expressions there. */
+static void box_project(const orc_params* P, double* x, double* v) {
+    const float r = P->particle_radius;
+    double pI[3] = {x[0], x[1], x[2]}, nI[3] = {0, 0, 0};
+    for (int e = 0; e < 3; ++e) {
+        const float hi = P->box_max[e] - r;
+        if (x[e] >= hi) { pI[e] = hi; nI[e] = -1.0; }
+    }
+    for (int e = 0; e < 3; ++e) {
+        const float lo = P->box_min[e] + r;
+        if (x[e] <= lo) { pI[e] = lo; nI[e] = 1.0; }
+    }
+    const double ln = len3(nI);
+    if (ln > 0) {
+        for (int e = 0; e < 3; ++e) nI[e] = nI[e] / ln;
+        const double vd = v[0] * nI[0] + v[1] * nI[1] + v[2] * nI[2];
+        for (int e = 0; e < 3; ++e) { x[e] = pI[e]; v[e] = v[e] - (1 + 0.0) * vd * nI[e]; }
+    }
+}
+
+/* ---- steps ---------------------------------------------------------------- */
+
+static int32_t* build_lists(const orc_params* P, const double* pos, int32_t* counts, int32_t* cap_out, orc_stats* st) {
+    orc_neighbors(P, pos, 0, counts, NULL);
+    int32_t cap = 1;
+    int64_t tot = 0;
+    for (int32_t i = 0; i < P->n; ++i) { cap = counts[i] > cap ? counts[i] : cap; tot += counts[i]; }
+    int32_t* list = (int32_t*)malloc(sizeof(int32_t) * (size_t)P->n * cap);
+    orc_neighbors(P, pos, cap, counts, list);
+    if (st) {
+        st->nbr_total = tot;
+        st->nbr_max = cap;
+        uint32_t* keys = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)P->n);
+        orc_cell_keys(P->n, pos, P->grid_min, P->cell, P->dims, keys, &st->clamped);
+        free(keys);
+    }
+    *cap_out = cap;
+    return list;
+}
+
+static int step_wcsph(const orc_params* P, orc_state* S, orc_stats* st, double* rho_x, double* f_np, int32_t* nbr_counts) {
+    const int32_t n = P->n;
+    const int ref = P->profile == ORC_PROFILE_REF;
+    int32_t* counts = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+    int32_t cap = 0;
+    int32_t* list = build_lists(P, S->pos, counts, &cap, st);
+    double* rho = S->rho;
+    double* p = S->p;
+    double* fnp = (double*)malloc(sizeof(double) * 3 * (size_t)n);
+    double* fp = (double*)malloc(sizeof(double) * 3 * (size_t)n);
+    if (ref) {
+        /* densityEvaluation (SphKernel.cu:9-27) */
+        const double h = P->h, m = P->mass;
+#pragma omp parallel for schedule(static)
+        for (int32_t i = 0; i < n; ++i) {
+            double s = 0.0;
+            for (int32_t t = 0; t < counts[i]; ++t) {
+                const int32_t j = list[(size_t)i * cap + t];
+                const double dv[3] = {S->pos[3 * i] - S->pos[3 * j], S->pos[3 * i + 1] - S->pos[3 * j + 1],
+                                      S->pos[3 * i + 2] - S->pos[3 * j + 2]};
+                const double d = len3(dv);
+                const double a = 64 * PI_D * pow(h, 9);
+                const double m_k = 315 / a;
+                const double b = pow((h * h) - (d * d), 3);
+                s += b * m_k * m;
+            }
+            rho[i] = RND(P, s);
+            p[i] = RND(P, P->k * (rho[i] - P->rho0));
+        }
+    } else {
+        orc_density(P, S->pos, counts, list, cap, 1, rho);
+        const double B = P->k * P->rho0 / 7.0;
+#pragma omp parallel for schedule(static)
+        for (int32_t i = 0; i < n; ++i) p[i] = RND(P, B * (pow(rho[i] / P->rho0, 7) - 1.0));
+    }
+    if (rho_x) memcpy(rho_x, rho, sizeof(double) * (size_t)n);
+    nonpressure_forces(P, S->pos, S->vel, rho, counts, list, cap, fnp);
+    pressure_forces(P, S->pos, rho, p, counts, list, cap, fp);
+    if (f_np) memcpy(f_np, fnp, sizeof(double) * 3 * (size_t)n);
+    const double dt = (double)P->dt;
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+        double* x = &S->pos[3 * i];
+        double* vap = &S->vel_ap[3 * i];
+        double aw[3] = {0, 0, 0};
+        if (!ref) wall_accel(P, x, vap, aw);
+        const double vav[3] = {vap[0], vap[1], vap[2]};
+        const double inv = 1.0 / rho[i];
+        for (int e = 0; e < 3; ++e) {
+            /* internalForces accumulates visc + surf + press, then the force
+             * kernel adds rho*g: F = ((fv + fs) + fp) + g */
+            const double F = fnp[3 * i + e] + fp[3 * i + e];
+            vap[e] = RND(P, vap[e] + (F * inv + aw[e]) * dt);
+            x[e] = RND(P, x[e] + vap[e] * dt);
+        }
+        if (ref) box_project(P, x, vap);
+        for (int e = 0; e < 3; ++e) {
+            x[e] = RND(P, x[e]);
+            vap[e] = RND(P, vap[e]);
+            S->vel[3 * i + e] = RND(P, (vav[e] + vap[e]) / 2);
+        }
+    }
+    if (nbr_counts) memcpy(nbr_counts, counts, sizeof(int32_t) * (size_t)n);
+    if (st) { st->iters = 0; st->converged = 1; }
+    free(counts); free(list); free(fnp); free(fp);
+    return 0;
+}
+
+static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double* rho_x, double* f_np, int32_t* nbr_counts) {
+    const int32_t n = P->n;
+    const int ref = P->profile == ORC_PROFILE_REF;
+    int32_t* counts = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+    int32_t cap = 0;
+    int32_t* list = build_lists(P, S->pos, counts, &cap, st);
+    const size_t n3 = 3 * (size_t)n;
+    double* rho = (double*)malloc(sizeof(double) * (size_t)n);
+    double* fnp = (double*)malloc(sizeof(double) * n3);
+    double* fp = (double*)calloc(n3, sizeof(double));
+    double* xs = (double*)malloc(sizeof(double) * n3);
+    double* vs = (double*)malloc(sizeof(double) * n3);
+    double* aw = (double*)calloc(n3, sizeof(double));
+    double* p = S->p;
+
+    orc_density(P, S->pos, counts, list, cap, !ref, rho);
+    if (rho_x) memcpy(rho_x, rho, sizeof(double) * (size_t)n);
+    nonpressure_forces(P, S->pos, S->vel, rho, counts, list, cap, fnp);
+    if (f_np) memcpy(f_np, fnp, sizeof(double) * n3);
+    if (!ref) {
+#pragma omp parallel for schedule(static)
+        for (int32_t i = 0; i < n; ++i) wall_accel(P, &S->pos[3 * i], &S->vel_ap[3 * i], &aw[3 * i]);
+    }
+    if (ref || !P->warm_start) memset(p, 0, sizeof(double) * (size_t)n);
+    else pressure_forces(P, S->pos, rho, p, counts, list, cap, fp);   /* warm start: f_p of the initial guess at x */
+
+    const double dt = (double)P->dt;
+    const int min_it = ref ? 3 : P->min_iters, max_it = ref ? 3 : P->max_iters;
+    int k = 0, converged = 0;
+    for (;;) {
+        /* predict (integrateSPH_LeapFrog_Forces on the saved state, SphKernel.cu:95-108) */
+#pragma omp parallel for schedule(static)
+        for (int32_t i = 0; i < n; ++i) {
+            const double inv = 1.0 / rho[i];
+            for (int e = 0; e < 3; ++e) {
+                const double F = fnp[3 * i + e] + fp[3 * i + e];
+                vs[3 * i + e] = RND(P, S->vel_ap[3 * i + e] + (F * inv + aw[3 * i + e]) * dt);
+                xs[3 * i + e] = RND(P, S->pos[3 * i + e] + vs[3 * i + e] * dt);
+            }
+        }
+        if (k >= max_it) break;
+        double* rs = (double*)malloc(sizeof(double) * (size_t)n);
+        orc_density(P, xs, counts, list, cap, !ref, rs);
+        double err = 0.0;
+        for (int32_t i = 0; i < n; ++i) {
+            const double e = (rs[i] - P->rho0) / P->rho0;
+            err = e > err ? e : err;
+        }
+        if (st && k <= ORC_MAX_ITERS) st->err[k] = err;
+        memcpy(rho, rs, sizeof(double) * (size_t)n);
+        free(rs);
+        if (!ref && k >= min_it && err <= P->eta) { converged = 1; break; }
+        pressure_update(P, xs, rho, counts, list, cap, p);
+        pressure_forces(P, xs, rho, p, counts, list, cap, fp);
+        k++;
+    }
+    /* commit the last prediction; walls; velocity interpolation (SphKernel.cu:128-135) */
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+        double* x = &S->pos[3 * i];
+        double* vap = &S->vel_ap[3 * i];
+        const double vav[3] = {vap[0], vap[1], vap[2]};
+        for (int e = 0; e < 3; ++e) { x[e] = xs[3 * i + e]; vap[e] = vs[3 * i + e]; }
+        if (ref) box_project(P, x, vap);
+        for (int e = 0; e < 3; ++e) {
+            x[e] = RND(P, x[e]);
+            vap[e] = RND(P, vap[e]);
+            S->vel[3 * i + e] = RND(P, (vav[e] + vap[e]) / 2);
+        }
+        S->rho[i] = rho[i];
+    }
+    if (nbr_counts) memcpy(nbr_counts, counts, sizeof(int32_t) * (size_t)n);
+    if (st) { st->iters = k; st->converged = ref ? 1 : converged; }
+    free(counts); free(list); free(rho); free(fnp); free(fp); free(xs); free(vs); free(aw);
+    return 0;
+}
+
+int orc_step(const orc_params* P, orc_state* S, orc_stats* st, double* rho_x, double* f_np, int32_t* nbr_counts) {
+    if (st) memset(st, 0, sizeof(*st));
+    if (P->n <= 0) return 0;
+    if (P->method == ORC_PCISPH) return step_pcisph(P, S, st, rho_x, f_np, nbr_counts);
+    return step_wcsph(P, S, st, rho_x, f_np, nbr_counts);
+}

@@ -1,0 +1,101 @@
+/*
+ * psb_oracle.h -- FP64 CPU restatement of the PSB particle-simulation hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is the checker the GPU path is compared
+ * against, and the "port" CPU baseline; the product never links it.
+ *
+ * Pinned: in the reference-compatible profile every function here is checked
+ * against the reference's own kernels executed on the CPU (oracle/_ref), see
+ * tests/test_oracle_vs_reference.py. The "config" profile follows the scene
+ * text (Tait EOS, penalty walls, eta loop) and has no reference counterpart.
+ */
+#ifndef PSB_ORACLE_H
+#define PSB_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_PROFILE_REF = 0, ORC_PROFILE_CONFIG = 1 };
+enum { ORC_WCSPH = 0, ORC_PCISPH = 1 };
+
+typedef struct orc_params {
+    int32_t n;
+    float box_min[3], box_max[3];   /* container walls */
+    float grid_min[3];              /* grid corner (UniformGrid.Min is float3) */
+    float cell;                     /* cell edge (UniformGrid.sizeCell is float) */
+    int32_t dims[3];                /* cells per axis */
+    double h, mass, rho0, k, mu, sigma, l;
+    float particle_radius;          /* wall offset */
+    float dt;
+    float gravity[3];               /* acceleration */
+    int32_t profile, method;
+    int32_t min_iters, max_iters;
+    double eta;
+    double wall_k, wall_c;          /* penalty walls: 1/s^2, 1/s */
+    int32_t float_state;            /* round stored state to float like the GPU path */
+    int32_t warm_start;             /* PCISPH: 0 start from p = 0, 1 start from the given p */
+    double spacing;                 /* config PCISPH prototype lattice spacing (0: (m/rho0)^(1/3)) */
+} orc_params;
+
+/* Config-profile PCISPH pressure factor delta = 1 / (beta (|sum gradW|^2 +
+ * sum |gradW|^2)) over the neighbours of a particle in a filled cubic
+ * lattice of the given spacing (Solenthaler & Pajarola 2009, sec. 4). */
+double orc_pci_delta(const orc_params* P);
+
+typedef struct orc_state {
+    double* pos;      /* n*3, particle-id order */
+    double* vel;      /* n*3 interpolated velocity (the reference's m_dVel[1]) */
+    double* vel_ap;   /* n*3 leap-frog half-step velocity (m_dVelInterAp) */
+    double* rho;      /* n: density at the end of the step */
+    double* p;        /* n: pressure at the end of the step */
+} orc_state;
+
+#define ORC_MAX_ITERS 64
+typedef struct orc_stats {
+    int32_t iters;                  /* pressure corrections performed */
+    int32_t converged;
+    double err[ORC_MAX_ITERS + 1];  /* max compression error per density pass */
+    int64_t nbr_total;
+    int32_t nbr_max;
+    int32_t clamped;                /* particles whose cell was clamped into the grid */
+} orc_stats;
+
+/* SplitMix64 (Steele, Lea, Flood 2014): counter-based, so every particle's
+ * jitter depends only on (seed, id, axis). */
+uint64_t orc_splitmix64(uint64_t x);
+
+/* Lattice block, ids x-fastest, positions origin + (i+0.5)*spacing + jitter
+ * with jitter uniform in [-J, J), rounded once to float. xyz stride 3. */
+void orc_lattice(const int32_t nxyz[3], double spacing, const double origin[3], double jitter,
+                 uint64_t seed, int32_t id0, float* pos3);
+
+/* Linear cell index i + j*nx + k*nx*ny with i = floor((x - Min)/cell) in
+ * double (UniformGridKernel.cu:46-49), clamped into the grid. */
+void orc_cell_keys(int32_t n, const double* pos, const float grid_min[3], float cell, const int32_t dims[3],
+                   uint32_t* keys, int32_t* nclamped);
+
+/* Stable order by (key, id): perm[t] = id of the t-th particle. */
+void orc_sort_perm(int32_t n, const uint32_t* keys, int32_t* perm);
+
+/* Neighbour lists at pos with the reference's test sqrt(d.d) <= h
+ * (UniformGridKernel.cu:58-95), self included. Each list is in sorted
+ * (key, id) order. Returns the total pair count, or -1 if a list would
+ * exceed cap (list may be NULL to count only). */
+int64_t orc_neighbors(const orc_params* P, const double* pos, int32_t cap, int32_t* counts, int32_t* list);
+
+/* Density at pos over the lists (poly6, self included). clamp != 0 drops
+ * pairs with r >= h (config profile). */
+void orc_density(const orc_params* P, const double* pos, const int32_t* counts, const int32_t* list, int32_t cap,
+                 int clamp, double* rho);
+
+/* One full step (WCSPH or PCISPH per P->method) in place. Optional outputs
+ * (NULL to skip): density at the step's start positions, the non-pressure
+ * force density, the neighbour counts. */
+int orc_step(const orc_params* P, orc_state* S, orc_stats* st, double* rho_x, double* f_np, int32_t* nbr_counts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,394 @@
+/*
+ * ref_driver.cpp -- runs the reference's own device kernels on the CPU.
+ *
+ * TEST INFRASTRUCTURE ONLY (oracle). Built by oracle/Makefile into
+ * oracle/_ref/libpsbref.so from the reference sources, where they lie, plus
+ * this driver and ref_shim.h. It is the pinned checker for the reference-
+ * compatible physics profile and the "reference" CPU baseline; the product
+ * never links it.
+ *
+ * What is the reference's and what is ours:
+ *  - every floating-point expression on the path is the reference's kernel
+ *    body, compiled unchanged: storeParticles_Kernel/searchNeighbooring_Kernel
+ *    (src/Utils/Neighborhood/UniformGrid/UniformGridKernel.cu:43-95),
+ *    densityEvaluation, internalForces, integrateSPH_LeapFrog(_Forces) and
+ *    interpolateSPH_velocities (SphKernel.cu:9-135),
+ *    the compute_..._PCI kernels and restore_Pos_Vel_PCI (PciSphSystem_Kernel.cu:36-201),
+ *    collisionBox (BoxCollision_Kernel.cu:7-34), evaluate_force_constante
+ *    (ForceExt_Constante.cu:15-23), collideParticles (CudaParticle_Kernel.cu:42-55),
+ *    integrateEuler (ParticleKernel.cu:12-20);
+ *  - this file restates, in our own code, the host launchers' call sequences
+ *    (PciSphSystem.cu:8-68, PciSphSystem.cpp:163-204, SphSystem.cpp:273-345,
+ *    SphSystem.cu:6-42, UniformGrid.cu:64-99, BoxCollision.cu:10-18,
+ *    CudaSystem.cpp:207-250, ForceExt.cu:24-34) and the launch sizing of
+ *    computeGridSize (common.cu:102-107: 256-thread blocks).
+ *
+ * Differences from running the reference on a GPU, all below the tolerances
+ * the tests use: no FMA contraction on the host (-ffp-contract=off), and
+ * glibc pow/powf/sqrt in place of CUDA's. Bucket slot order inside a cell is
+ * deterministic here (storeParticles runs on one host thread, so slots fill
+ * in increasing particle index); on a GPU it follows atomicAdd order.
+ *
+ * Safety checks the reference lacks (it writes out of bounds instead): a
+ * particle outside the grid, more than MAXPARTICLES (64) in a cell, or more
+ * than 200 neighbours makes the call return a negative code.
+ */
+#include "ref_shim.h"
+#include <UniformGrid.cuh>
+#include <UniformGridKernel.cuh>
+#include <SphKernel.cuh>
+#include <PciSphSystem_Kernel.cuh>
+#include <CudaParticle_Kernel.cuh>
+#include <vector>
+#include <string>
+#include <cstdlib>
+
+thread_local uint3 blockIdx;
+thread_local uint3 threadIdx;
+thread_local dim3 blockDim;
+thread_local dim3 gridDim;
+
+/* Kernels compiled from .cu files without an extern "C" header of their own. */
+void collisionBox(int nbBodies, double3* newPos, double3* oldVel, double3* newVel, float3 Min, float3 Max,
+                  float elast, bool container, float radiusParticles, float dt);
+void evaluate_force_constante(uint nbBodies, double3* accumForceBuff, double* mass, float3 direction, float amplitude);
+void integrateEuler(uint nbBodies, double3* newPos, double3* newVel, double3* forces, double* mass, float dt);
+
+namespace {
+
+const int kMaxNbr = 200;   /* listeVoisine stride, UniformGridKernel.cu:84 */
+
+/* Emulates kernel<<<ceil(n/256), min(256,n)>>> (computeGridSize, common.cu:102-107).
+ * Blocks are spread over host threads; the reference kernels have no
+ * intra-block communication, so any schedule gives the same results. */
+template <typename F>
+void launch1d(unsigned n, bool parallel, F body) {
+    if (n == 0) return;
+    const unsigned threads = n < 256u ? n : 256u;
+    const long blocks = (long)((n + threads - 1) / threads);
+#pragma omp parallel for schedule(static) if (parallel)
+    for (long b = 0; b < blocks; ++b) {
+        blockIdx = make_uint3((unsigned)b, 0, 0);
+        blockDim = dim3(threads, 1, 1);
+        gridDim = dim3((unsigned)blocks, 1, 1);
+        for (unsigned t = 0; t < threads; ++t) {
+            threadIdx = make_uint3(t, 0, 0);
+            body();
+        }
+    }
+}
+
+/* One host thread per cell (grid of cells, 1-thread blocks), as the
+ * reference's "3D-swapped" launches end up (UniformGrid.cu:64-77). */
+template <typename F>
+void launch_cells(int nx, int ny, int nz, F body) {
+#pragma omp parallel for schedule(static)
+    for (long z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                blockIdx = make_uint3(x, y, (unsigned)z);
+                blockDim = dim3(1, 1, 1);
+                threadIdx = make_uint3(0, 0, 0);
+                body();
+            }
+}
+
+}  // namespace
+
+struct ref_sim {
+    int n = 0;
+    UniformGrid grid{};
+    std::vector<int> cell_idx, cell_nb;
+    std::vector<int> nb_count, nb_list;
+    /* AoS double3 particle arrays (stride 3), as the reference's m_d* buffers. */
+    std::vector<double> pos_old, pos, vel_old, vel, vel_av, vel_ap;
+    std::vector<double> r_pos_old, r_pos, r_vel_av, r_vel_ap;      /* restore buffers */
+    std::vector<double> f_visc, f_surf, f_press, f_accum, normals;
+    /* per-particle scalars */
+    std::vector<double> mass, radius, rho0, k, mu, l, sigma, density, density_err, pressure, threshold;
+    /* DEM coefficients */
+    std::vector<double> spring, damping, shear, attraction;
+};
+
+static std::vector<double>* field(ref_sim* s, const char* name, int* width) {
+    struct E { const char* n; std::vector<double> ref_sim::*p; int w; };
+    static const E table[] = {
+        {"pos_old", &ref_sim::pos_old, 3}, {"pos", &ref_sim::pos, 3}, {"vel_old", &ref_sim::vel_old, 3},
+        {"vel", &ref_sim::vel, 3}, {"vel_av", &ref_sim::vel_av, 3}, {"vel_ap", &ref_sim::vel_ap, 3},
+        {"r_pos_old", &ref_sim::r_pos_old, 3}, {"r_pos", &ref_sim::r_pos, 3},
+        {"r_vel_av", &ref_sim::r_vel_av, 3}, {"r_vel_ap", &ref_sim::r_vel_ap, 3},
+        {"f_visc", &ref_sim::f_visc, 3}, {"f_surf", &ref_sim::f_surf, 3}, {"f_press", &ref_sim::f_press, 3},
+        {"f_accum", &ref_sim::f_accum, 3}, {"normals", &ref_sim::normals, 3},
+        {"mass", &ref_sim::mass, 1}, {"radius", &ref_sim::radius, 1}, {"rho0", &ref_sim::rho0, 1},
+        {"k", &ref_sim::k, 1}, {"mu", &ref_sim::mu, 1}, {"l", &ref_sim::l, 1}, {"sigma", &ref_sim::sigma, 1},
+        {"density", &ref_sim::density, 1}, {"density_err", &ref_sim::density_err, 1},
+        {"pressure", &ref_sim::pressure, 1}, {"threshold", &ref_sim::threshold, 1},
+        {"spring", &ref_sim::spring, 1}, {"damping", &ref_sim::damping, 1}, {"shear", &ref_sim::shear, 1},
+        {"attraction", &ref_sim::attraction, 1},
+    };
+    for (const E& e : table)
+        if (std::string(name) == e.n) { *width = e.w; return &(s->*(e.p)); }
+    return nullptr;
+}
+
+extern "C" {
+
+/* Grid as createGrid sets it (UniformGrid.cu:17-49), given directly by its
+ * float Min corner, float cell size and cell counts. */
+ref_sim* ref_create(int n, const float* grid_min, float cell, const int* dims) {
+    if (n <= 0 || cell <= 0.f || dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0) return nullptr;
+    ref_sim* s = new ref_sim();
+    s->n = n;
+    s->grid.Min = make_float3(grid_min[0], grid_min[1], grid_min[2]);
+    s->grid.sizeCell = cell;
+    s->grid.nbCellsX = dims[0];
+    s->grid.nbCellsY = dims[1];
+    s->grid.nbCellsZ = dims[2];
+    s->grid.Max = make_float3(grid_min[0] + dims[0] * cell, grid_min[1] + dims[1] * cell, grid_min[2] + dims[2] * cell);
+    const size_t cells = (size_t)dims[0] * dims[1] * dims[2];
+    s->cell_nb.assign(cells, 0);
+    s->cell_idx.assign(cells * MAXPARTICLES, 0);
+    s->grid.nbParticles = s->cell_nb.data();
+    s->grid.indexParticles = s->cell_idx.data();
+    s->nb_count.assign(n, 0);
+    s->nb_list.assign((size_t)n * kMaxNbr + 27 * MAXPARTICLES, 0);
+    for (auto* v : {&s->pos_old, &s->pos, &s->vel_old, &s->vel, &s->vel_av, &s->vel_ap, &s->r_pos_old, &s->r_pos,
+                    &s->r_vel_av, &s->r_vel_ap, &s->f_visc, &s->f_surf, &s->f_press, &s->f_accum, &s->normals})
+        v->assign((size_t)n * 3, 0.0);
+    for (auto* v : {&s->mass, &s->radius, &s->rho0, &s->k, &s->mu, &s->l, &s->sigma, &s->density, &s->density_err,
+                    &s->pressure, &s->threshold, &s->spring, &s->damping, &s->shear, &s->attraction})
+        v->assign((size_t)n, 0.0);
+    return s;
+}
+
+void ref_destroy(ref_sim* s) { delete s; }
+
+int ref_set(ref_sim* s, const char* name, const double* src) {
+    int w = 0;
+    std::vector<double>* v = field(s, name, &w);
+    if (!v) return -1;
+    std::memcpy(v->data(), src, sizeof(double) * v->size());
+    return 0;
+}
+
+int ref_get(ref_sim* s, const char* name, double* dst) {
+    int w = 0;
+    std::vector<double>* v = field(s, name, &w);
+    if (!v) return -1;
+    std::memcpy(dst, v->data(), sizeof(double) * v->size());
+    return 0;
+}
+
+/* reinitCells + storeParticles + searchNeighbooring (UniformGrid.cu:64-99),
+ * called as SPHSystem/PCI_SPHSystem::update do with scale 1
+ * (PciSphSystem.cpp:168-170). Returns 0, or -2 (particle outside the grid),
+ * -3 (cell over MAXPARTICLES), -4 (more than 200 neighbours). */
+int ref_search(ref_sim* s) {
+    UniformGrid* g = &s->grid;
+    /* Range check first: storeParticles_Kernel has none (UniformGridKernel.cu:46-53). */
+    for (int i = 0; i < s->n; ++i) {
+        const double* p = &s->pos[3 * (size_t)i];
+        int c[3];
+        c[0] = (int)floor((p[0] - g->Min.x) / g->sizeCell);
+        c[1] = (int)floor((p[1] - g->Min.y) / g->sizeCell);
+        c[2] = (int)floor((p[2] - g->Min.z) / g->sizeCell);
+        if (c[0] < 0 || c[1] < 0 || c[2] < 0 || c[0] >= g->nbCellsX || c[1] >= g->nbCellsY || c[2] >= g->nbCellsZ)
+            return -2;
+    }
+    launch_cells(g->nbCellsX, g->nbCellsY, g->nbCellsZ,
+                 [&] { reinitCells_Kernel(g->nbParticles, g->nbCellsX, g->nbCellsY, g->nbCellsZ); });
+    /* Counts are checked before the slots are written. */
+    {
+        std::vector<int> cnt(s->cell_nb.size(), 0);
+        for (int i = 0; i < s->n; ++i) {
+            const double* p = &s->pos[3 * (size_t)i];
+            int a = (int)floor((p[0] - g->Min.x) / g->sizeCell);
+            int b = (int)floor((p[1] - g->Min.y) / g->sizeCell);
+            int c = (int)floor((p[2] - g->Min.z) / g->sizeCell);
+            if (++cnt[(size_t)a + (size_t)b * g->nbCellsX + (size_t)c * g->nbCellsX * g->nbCellsY] > MAXPARTICLES)
+                return -3;
+        }
+    }
+    launch1d(s->n, false, [&] {
+        storeParticles_Kernel((double3*)s->pos.data(), s->n, g->nbParticles, g->indexParticles, g->sizeCell, g->Min,
+                              g->nbCellsX, g->nbCellsY, g->nbCellsZ);
+    });
+    partVoisine v{s->nb_count.data(), s->nb_list.data()};
+    /* The kernel appends without a bound (UniformGridKernel.cu:82-85). The
+     * list is padded by the most one particle can append (27 cells x 64
+     * slots), so an overflow stays inside the allocation; the count check
+     * below then rejects the call. */
+    launch1d(s->n, true, [&] {
+        searchNeighbooring_Kernel((double3*)s->pos.data(), s->radius.data(), g->indexParticles, g->nbParticles,
+                                  g->nbCellsX, g->nbCellsY, g->nbCellsZ, g->sizeCell, g->Min, 1.0, v, s->n);
+    });
+    for (int i = 0; i < s->n; ++i)
+        if (s->nb_count[i] > kMaxNbr) return -4;
+    return 0;
+}
+
+int ref_neighbors(ref_sim* s, int* counts, int* list) {
+    std::memcpy(counts, s->nb_count.data(), sizeof(int) * s->n);
+    if (list) std::memcpy(list, s->nb_list.data(), sizeof(int) * (size_t)s->n * kMaxNbr);
+    return 0;
+}
+
+int ref_cell_counts(ref_sim* s, int* counts) {
+    std::memcpy(counts, s->cell_nb.data(), sizeof(int) * s->cell_nb.size());
+    return 0;
+}
+
+/* compute_Density_PCI at the current positions over the current lists. */
+int ref_density_pci(ref_sim* s) {
+    partVoisine v{s->nb_count.data(), s->nb_list.data()};
+    launch1d(s->n, true, [&] {
+        compute_Density_PCI(s->n, (double3*)s->pos.data(), s->mass.data(), s->radius.data(), s->density.data(),
+                            s->rho0.data(), s->density_err.data(), v);
+    });
+    return 0;
+}
+
+/* pci_SPH_update (PciSphSystem.cu:8-68), kernel for kernel; `iters` is the
+ * reference's fixed 3 unless a test asks otherwise. */
+static void pci_sph_update(ref_sim* s, float dt, int iters) {
+    const uint n = s->n;
+    partVoisine v{s->nb_count.data(), s->nb_list.data()};
+    double3* pos = (double3*)s->pos.data();
+    launch1d(n, true, [&] {
+        compute_Density_PCI(n, pos, s->mass.data(), s->radius.data(), s->density.data(), s->rho0.data(),
+                            s->density_err.data(), v);
+    });
+    launch1d(n, true, [&] {
+        compute_Viscosity_SurfaceTension_Force_PCI(n, pos, (double3*)s->vel.data(), s->mass.data(), s->density.data(),
+                                                   s->pressure.data(), s->radius.data(), s->mu.data(), s->threshold.data(),
+                                                   s->sigma.data(), (double3*)s->normals.data(), (double3*)s->f_press.data(),
+                                                   (double3*)s->f_visc.data(), (double3*)s->f_surf.data(),
+                                                   (double3*)s->f_accum.data(), v);
+    });
+    for (int it = 0; it < iters; ++it) {
+        launch1d(n, true, [&] {
+            integrateSPH_LeapFrog_Forces((double3*)s->vel_av.data(), (double3*)s->vel_ap.data(), (double3*)s->pos_old.data(),
+                                         pos, (double3*)s->f_visc.data(), (double3*)s->f_surf.data(),
+                                         (double3*)s->f_press.data(), (double3*)s->f_accum.data(), s->density.data(), dt, n);
+        });
+        launch1d(n, true, [&] {
+            compute_Density_PCI(n, pos, s->mass.data(), s->radius.data(), s->density.data(), s->rho0.data(),
+                                s->density_err.data(), v);
+        });
+        launch1d(n, true, [&] {
+            compute_Pressure_PCI(n, pos, s->mass.data(), s->radius.data(), s->k.data(), 10.0, s->density.data(),
+                                 s->rho0.data(), s->density_err.data(), s->pressure.data(), v, dt);
+        });
+        launch1d(n, true, [&] {
+            compute_Pressure_Force_PCI(n, pos, s->mass.data(), s->density.data(), s->rho0.data(), s->density_err.data(),
+                                       s->pressure.data(), s->radius.data(), (double3*)s->f_press.data(), 10.0, v);
+        });
+        launch1d(n, true, [&] {
+            restore_Pos_Vel_PCI((double3*)s->r_vel_av.data(), (double3*)s->r_vel_ap.data(), (double3*)s->r_pos_old.data(),
+                                (double3*)s->r_pos.data(), (double3*)s->vel_av.data(), (double3*)s->vel_ap.data(),
+                                (double3*)s->pos_old.data(), pos, n);
+        });
+    }
+    launch1d(n, true, [&] {
+        integrateSPH_LeapFrog_Forces((double3*)s->vel_av.data(), (double3*)s->vel_ap.data(), (double3*)s->pos_old.data(),
+                                     pos, (double3*)s->f_visc.data(), (double3*)s->f_surf.data(), (double3*)s->f_press.data(),
+                                     (double3*)s->f_accum.data(), s->density.data(), dt, n);
+    });
+}
+
+static void collide_box(ref_sim* s, float particle_radius, float dt, const float* box_min, const float* box_max) {
+    /* BoxCollision::collide -> collisionSystem_Box_CUDA (BoxCollision.cpp:34-37,
+     * BoxCollision.cu:10-18), acting on (pos, vel_av, vel_ap) as
+     * SPHSystem::collide passes them (SphSystem.cpp:323-328). */
+    launch1d(s->n, true, [&] {
+        collisionBox(s->n, (double3*)s->pos.data(), (double3*)s->vel_av.data(), (double3*)s->vel_ap.data(),
+                     make_float3(box_min[0], box_min[1], box_min[2]), make_float3(box_max[0], box_max[1], box_max[2]),
+                     0.f, true, particle_radius, dt);
+    });
+}
+
+static void interpolate(ref_sim* s) {
+    launch1d(s->n, true, [&] {
+        interpolateSPH_velocities((double3*)s->vel_av.data(), (double3*)s->vel_ap.data(), (double3*)s->vel_old.data(),
+                                  (double3*)s->vel.data(), s->n);
+    });
+}
+
+/* PCI_SPHSystem::update without emission (PciSphSystem.cpp:163-204).
+ * `collide` = 0 skips the box (a scene without collision objects). */
+int ref_pcisph_update(ref_sim* s, float dt, int iters, int collide, float particle_radius,
+                      const float* box_min, const float* box_max) {
+    int rc = ref_search(s);
+    if (rc) return rc;
+    pci_sph_update(s, dt, iters);
+    if (collide) collide_box(s, particle_radius, dt, box_min, box_max);
+    interpolate(s);
+    s->r_pos_old = s->pos_old;
+    s->r_pos = s->pos;
+    s->r_vel_av = s->vel_av;
+    s->r_vel_ap = s->vel_ap;
+    return 0;
+}
+
+/* SPHSystem::update without emission (SphSystem.cpp:273-297): density and
+ * internal forces (SphSystem.cu:27-42), the constant external force with the
+ * density passed as "mass" (SphSystem.cpp:307-320, ForceExt.cu:24-34),
+ * leap-frog (SphSystem.cu:6-14), box, velocity interpolation. */
+int ref_wcsph_update(ref_sim* s, float dt, const float* gravity_dir, float gravity_amp, int collide,
+                     float particle_radius, const float* box_min, const float* box_max) {
+    int rc = ref_search(s);
+    if (rc) return rc;
+    const uint n = s->n;
+    partVoisine v{s->nb_count.data(), s->nb_list.data()};
+    double3* pos = (double3*)s->pos.data();
+    launch1d(n, true, [&] {
+        densityEvaluation(pos, s->mass.data(), s->radius.data(), s->k.data(), s->rho0.data(), n, s->density.data(),
+                          s->pressure.data(), v);
+    });
+    launch1d(n, true, [&] {
+        internalForces(pos, (double3*)s->vel.data(), s->mass.data(), s->density.data(), s->pressure.data(),
+                       s->radius.data(), s->mu.data(), s->threshold.data(), s->sigma.data(), (double3*)s->normals.data(), n,
+                       (double3*)s->f_press.data(), (double3*)s->f_visc.data(), (double3*)s->f_surf.data(),
+                       (double3*)s->f_accum.data(), v);
+    });
+    const float3 dir = make_float3(gravity_dir[0], gravity_dir[1], gravity_dir[2]);
+    launch1d(n, true, [&] { evaluate_force_constante(n, (double3*)s->f_accum.data(), s->density.data(), dir, gravity_amp); });
+    launch1d(n, true, [&] {
+        integrateSPH_LeapFrog((double3*)s->vel_av.data(), (double3*)s->vel_ap.data(), (double3*)s->pos_old.data(), pos,
+                              (double3*)s->f_accum.data(), s->density.data(), dt, n);
+    });
+    if (collide) collide_box(s, particle_radius, dt, box_min, box_max);
+    interpolate(s);
+    return 0;
+}
+
+/* CudaSystem::update without emission (CudaSystem.cpp:207-250): forces
+ * zeroed, gravity m*g, pair forces on (pos_old, vel_old), explicit Euler on
+ * (pos, vel), box. Tests call it with pos_old == pos and vel_old == vel. */
+int ref_dem_update(ref_sim* s, float dt, const float* gravity_dir, float gravity_amp, int collide,
+                   float particle_radius, const float* box_min, const float* box_max) {
+    int rc = ref_search(s);
+    if (rc) return rc;
+    const uint n = s->n;
+    partVoisine v{s->nb_count.data(), s->nb_list.data()};
+    std::fill(s->f_accum.begin(), s->f_accum.end(), 0.0);
+    const float3 dir = make_float3(gravity_dir[0], gravity_dir[1], gravity_dir[2]);
+    launch1d(n, true, [&] { evaluate_force_constante(n, (double3*)s->f_accum.data(), s->mass.data(), dir, gravity_amp); });
+    launch1d(n, true, [&] {
+        collideParticles(n, (double3*)s->pos_old.data(), (double3*)s->vel_old.data(), (double3*)s->f_accum.data(),
+                         s->radius.data(), s->spring.data(), s->damping.data(), s->shear.data(), s->attraction.data(), v);
+    });
+    launch1d(n, true, [&] {
+        integrateEuler(n, (double3*)s->pos.data(), (double3*)s->vel.data(), (double3*)s->f_accum.data(), s->mass.data(), dt);
+    });
+    if (collide) {
+        launch1d(n, true, [&] {
+            collisionBox(n, (double3*)s->pos.data(), (double3*)s->vel_old.data(), (double3*)s->vel.data(),
+                         make_float3(box_min[0], box_min[1], box_min[2]), make_float3(box_max[0], box_max[1], box_max[2]),
+                         0.f, true, particle_radius, dt);
+        });
+    }
+    return 0;
+}
+
+}  /* extern "C" */

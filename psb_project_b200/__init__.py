@@ -1,0 +1,14 @@
+"""B200-native particle-simulation hot path of PSB_Project.
+
+Uniform-grid neighbour search, SPH density and forces, the PCISPH
+predictor-corrector loop and box walls, as hand-written sm_100a CUDA
+kernels behind a C ABI (include/psb.h, lib/libpsb.so). This package is the
+Python host side: the scene description and a ctypes binding.
+"""
+from .scene import (PCISPH, PROFILE_CONFIG, PROFILE_REF, WARM_PREVIOUS, WARM_ZERO, WCSPH, Block, Scene,
+                    config_scene, dam_break, ref_scene)
+from .runtime import PsbError, Simulation, lattice, lib, scene_positions
+
+__all__ = ["Scene", "Block", "Simulation", "PsbError", "config_scene", "dam_break", "ref_scene", "lattice",
+           "scene_positions", "lib", "PCISPH", "WCSPH", "PROFILE_REF", "PROFILE_CONFIG", "WARM_ZERO",
+           "WARM_PREVIOUS"]

@@ -1,0 +1,735 @@
+// api.cu -- the C ABI (include/psb.h): context, buffers, step orchestration,
+// uploads/downloads in particle-id order, per-kernel CUDA-event profiling.
+//
+// One psb_step is, on the context's stream:
+//   reset cells of the previous sort -> cell keys -> radix sort (cell, id) ->
+//   reorder + cell ranges -> neighbour lists -> density at x ->
+//   WCSPH: forces + leap-frog + walls + interpolation (one sweep)
+//   PCISPH: non-pressure forces + first prediction, then per correction
+//           {density/pressure pass at x*, pressure-force pass + next
+//           prediction}, then commit + walls + interpolation.
+// The reference profile runs exactly three corrections with no host
+// round-trip; the config profile reads the FP64 max compression error of
+// each density pass (8 bytes) to decide convergence.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "psb.h"
+#include "psb_internal.cuh"
+
+using psb::Params;
+
+namespace {
+
+struct Profiler {
+    bool on = false;
+    std::vector<std::string> names;
+    std::vector<long long> launches;
+    std::vector<double> ms;
+    struct Pending { int k; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+
+    int index(const char* name) {
+        for (size_t i = 0; i < names.size(); ++i)
+            if (names[i] == name) return (int)i;
+        names.emplace_back(name);
+        launches.push_back(0);
+        ms.push_back(0.0);
+        return (int)names.size() - 1;
+    }
+    cudaEvent_t get() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void resolve(cudaStream_t st) {
+        if (pending.empty()) return;
+        cudaStreamSynchronize(st);
+        for (auto& p : pending) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, p.a, p.b);
+            launches[p.k] += 1;
+            ms[p.k] += t;
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    ~Profiler() {
+        for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+}  // namespace
+
+struct psb_ctx {
+    psb_scene sc{};
+    Params P{};
+    int device = 0;
+    int n = 0, n_max = 0, cap = 0;
+    cudaStream_t stream = nullptr;
+    // particle state, double-buffered for the reorder: cs indexes pos/vel/vap,
+    // cr indexes rp/ids
+    float4* pos[2] = {};
+    float4* vel[2] = {};
+    float4* vap[2] = {};
+    float2* rp[2] = {};
+    int* ids[2] = {};
+    int cs = 0, cr = 0;
+    // sort and cells
+    uint32_t* keys[2] = {};
+    uint32_t* vals[2] = {};
+    uint32_t* hist = nullptr;
+    int hist_blocks = 0, key_bits = 0;
+    int sorted = -1;          // buffer holding the last sorted keys, -1: none
+    int sorted_n = 0;
+    uint32_t* cell_start = nullptr;
+    uint32_t* cell_end = nullptr;
+    size_t ncells = 0;
+    int* nbr_count = nullptr;
+    int* nbr_list = nullptr;
+    // SPH scratch
+    float4* fnp = nullptr;
+    float4* xs[2] = {};
+    float4* vs = nullptr;
+    float2* rpc = nullptr;
+    float* rho_x = nullptr;
+    unsigned long long* err_hist = nullptr;
+    int* flags = nullptr;     // [0] overflow [1] max count [2..3] pair total [4] clamped
+    void* stage = nullptr;    // device staging for uploads/downloads
+    // host mirrors
+    unsigned long long* h_err = nullptr;
+    int* h_flags = nullptr;
+    bool uploaded = false, built = false;
+    psb_step_stats stats{};
+    Profiler prof;
+    std::string err;
+};
+
+namespace {
+
+const char* kStatus[] = {"ok", "invalid argument", "out of memory", "neighbour list overflow",
+                         "corrector did not converge", "CUDA error", "call out of order"};
+
+int fail(psb_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_check(psb_ctx* c, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return PSB_OK;
+    return fail(c, PSB_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define PSB_TRY(expr)                          \
+    do {                                       \
+        int rc__ = (expr);                     \
+        if (rc__ != PSB_OK) return rc__;       \
+    } while (0)
+
+template <typename F>
+void timed(psb_ctx* c, const char* name, F&& launch) {
+    if (!c->prof.on) { launch(); return; }
+    const int k = c->prof.index(name);
+    cudaEvent_t a = c->prof.get(), b = c->prof.get();
+    cudaEventRecord(a, c->stream);
+    launch();
+    cudaEventRecord(b, c->stream);
+    c->prof.pending.push_back({k, a, b});
+    if (c->prof.pending.size() > 8192) c->prof.resolve(c->stream);
+}
+
+template <typename T>
+int dalloc(psb_ctx* c, T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    if (cudaMalloc((void**)p, sizeof(T) * count) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, PSB_ENOMEM, "cudaMalloc of " + std::to_string(sizeof(T) * count) + " bytes failed");
+    }
+    return PSB_OK;
+}
+
+void free_all(psb_ctx* c) {
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(c->pos[i]); cudaFree(c->vel[i]); cudaFree(c->vap[i]); cudaFree(c->rp[i]); cudaFree(c->ids[i]);
+        cudaFree(c->keys[i]); cudaFree(c->vals[i]); cudaFree(c->xs[i]);
+    }
+    cudaFree(c->hist); cudaFree(c->cell_start); cudaFree(c->cell_end); cudaFree(c->nbr_count);
+    cudaFree(c->nbr_list); cudaFree(c->fnp); cudaFree(c->vs); cudaFree(c->rpc); cudaFree(c->rho_x);
+    cudaFree(c->err_hist); cudaFree(c->flags); cudaFree(c->stage);
+    cudaFreeHost(c->h_err); cudaFreeHost(c->h_flags);
+}
+
+int validate(const psb_scene* s, std::string& why) {
+    if (!s) { why = "scene is NULL"; return PSB_EINVAL; }
+    if (s->n_max <= 0) { why = "n_max must be positive"; return PSB_EINVAL; }
+    if (!(s->h > 0) || !(s->mass > 0) || !(s->rho0 > 0) || !(s->dt > 0)) { why = "h, mass, rho0, dt must be positive"; return PSB_EINVAL; }
+    if (!(s->cell > 0) || (double)s->cell < s->h * (1.0 - 1e-6)) { why = "cell must be >= h (27-cell walk)"; return PSB_EINVAL; }
+    for (int a = 0; a < 3; ++a) {
+        if (s->dims[a] <= 0) { why = "dims must be positive"; return PSB_EINVAL; }
+        if (!(s->box_max[a] > s->box_min[a])) { why = "box_max must exceed box_min"; return PSB_EINVAL; }
+    }
+    const double ncells = (double)s->dims[0] * s->dims[1] * s->dims[2];
+    if (ncells >= 4294967295.0) { why = "too many grid cells (>= 2^32 - 1)"; return PSB_EINVAL; }
+    if (s->method != PSB_WCSPH && s->method != PSB_PCISPH) { why = "unknown method"; return PSB_EINVAL; }
+    if (s->profile != PSB_PROFILE_REF && s->profile != PSB_PROFILE_CONFIG) { why = "unknown profile"; return PSB_EINVAL; }
+    if (s->min_iters < 0 || s->max_iters < s->min_iters || s->max_iters > PSB_MAX_ITERS) {
+        why = "need 0 <= min_iters <= max_iters <= PSB_MAX_ITERS";
+        return PSB_EINVAL;
+    }
+    if (s->nbr_cap < 0 || s->nbr_cap > 4096) { why = "nbr_cap out of range"; return PSB_EINVAL; }
+    if (s->warm_start != PSB_WARM_ZERO && s->warm_start != PSB_WARM_PREVIOUS) { why = "unknown warm_start"; return PSB_EINVAL; }
+    {
+        const double ws = s->spacing > 0 ? s->spacing : std::cbrt(s->mass / s->rho0);
+        if (!(ws >= s->h / 7.0)) { why = "spacing below h/7 (wall boundary layers)"; return PSB_EINVAL; }
+    }
+    if ((double)s->n_max * (s->nbr_cap ? s->nbr_cap : 128) >= 9.0e18) { why = "list too large"; return PSB_EINVAL; }
+    return PSB_OK;
+}
+
+// Scene constants in FP64 on the host, then stored as FP32.
+Params derive(const psb_scene& s) {
+    Params P{};
+    const double pi = 3.14159265358979323846;
+    const double h = s.h, m = s.mass;
+    P.g.gx = s.grid_min[0]; P.g.gy = s.grid_min[1]; P.g.gz = s.grid_min[2];
+    P.g.cell = s.cell;
+    P.g.nx = s.dims[0]; P.g.ny = s.dims[1]; P.g.nz = s.dims[2];
+    P.cap = s.nbr_cap ? s.nbr_cap : 128;
+    P.h = h;
+    const float h2f = (float)(h * h);
+    P.h2_lo = h2f * (1.f - 1e-5f);
+    P.h2_hi = h2f * (1.f + 1e-5f);
+    P.h2 = h2f;
+    P.inv_h = (float)(1.0 / h);
+    P.inv_h2 = (float)(1.0 / (h * h));
+    P.k_rho = (float)(315.0 * m / (64.0 * pi * h * h * h));
+    const double G = 45.0 / (pi * h * h * h * h);
+    P.k_grad = (float)(m * G);
+    P.k_visc = (float)(s.mu * m * 45.0 / (pi * h * h * h * h * h));
+    P.k_surf = (float)(945.0 * m / (32.0 * pi * h * h * h * h * h));
+    P.ref = s.profile == PSB_PROFILE_REF;
+    P.pci = s.method == PSB_PCISPH;
+    // The reference's PCISPH kernel sets sigma = 0.0728 (PciSphSystem_Kernel.cu:161)
+    P.sigma = (float)(P.pci ? 0.0728 : s.sigma);
+    P.l = (float)s.l;
+    P.surface = P.ref ? 1 : 0;
+    const double dt = (double)s.dt;
+    const double beta = 2.0 * (m * dt / s.rho0) * (m * dt / s.rho0);
+    P.k_press = (float)(1.0 / (beta * G * G));
+    P.rho0 = (float)s.rho0;
+    P.rho0_d = s.rho0;
+    P.eos_k = (float)(P.ref ? s.k : s.k * s.rho0 / 7.0);
+    P.dt = s.dt;
+    if (P.ref && P.pci) {            // forcesAccum = (0, -9.81 rho, 0), PciSphSystem_Kernel.cu:168
+        P.gx = 0.f; P.gy = -9.81f; P.gz = 0.f;
+    } else {
+        P.gx = s.gravity[0]; P.gy = s.gravity[1]; P.gz = s.gravity[2];
+    }
+    P.wlo_x = s.box_min[0] + s.particle_radius; P.wlo_y = s.box_min[1] + s.particle_radius;
+    P.wlo_z = s.box_min[2] + s.particle_radius;
+    P.whi_x = s.box_max[0] - s.particle_radius; P.whi_y = s.box_max[1] - s.particle_radius;
+    P.whi_z = s.box_max[2] - s.particle_radius;
+    P.wall_k = (float)s.wall_k;
+    P.wall_c = (float)s.wall_c;
+    if (!P.ref) {   // config: the penalty backstop acts at the faces themselves
+        P.wlo_x = s.box_min[0]; P.wlo_y = s.box_min[1]; P.wlo_z = s.box_min[2];
+        P.whi_x = s.box_max[0]; P.whi_y = s.box_max[1]; P.whi_z = s.box_max[2];
+    }
+    P.bx0 = s.box_min[0]; P.by0 = s.box_min[1]; P.bz0 = s.box_min[2];
+    P.bx1 = s.box_max[0]; P.by1 = s.box_max[1]; P.bz1 = s.box_max[2];
+    const double ws = s.spacing > 0 ? s.spacing : std::cbrt(m / s.rho0);
+    {   // Solenthaler & Pajarola 2009, sec. 4: delta from a particle with a filled neighbourhood
+        const int R = (int)std::ceil(h / ws);
+        double W1[3] = {0, 0, 0}, W2 = 0;
+        for (int k = -R; k <= R; ++k)
+            for (int j = -R; j <= R; ++j)
+                for (int i = -R; i <= R; ++i) {
+                    if (!i && !j && !k) continue;
+                    const double r = ws * std::sqrt((double)(i * i + j * j + k * k));
+                    if (r >= h) continue;
+                    const double gw = G * (1.0 - r / h) * (1.0 - r / h);
+                    W1[0] -= gw * i * ws / r; W1[1] -= gw * j * ws / r; W1[2] -= gw * k * ws / r;
+                    W2 += gw * gw;
+                }
+        P.k_delta = (float)(1.0 / (beta * (W1[0] * W1[0] + W1[1] * W1[1] + W1[2] * W1[2] + W2)));
+    }
+    P.hf = (float)h;
+    P.ws = (float)ws;
+    P.cz = (float)(pi * h * h / (4.0 * ws * ws));
+    P.cg = (float)(2.0 * pi * h / (3.0 * ws * ws));
+    return P;
+}
+
+// ---- small device helpers: packing and id-order scatter -------------------
+
+__global__ void k_pack3(int n, const float* __restrict__ src, float4* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src ? make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+__global__ void k_pack3d(int n, const double* __restrict__ src, float4* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        dst[i] = src ? make_float4(__double2float_rn(src[3 * i]), __double2float_rn(src[3 * i + 1]),
+                                   __double2float_rn(src[3 * i + 2]), 0.f)
+                     : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+__global__ void k_init_ids(int n, const float* __restrict__ pres, int* __restrict__ ids, float2* __restrict__ rp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { ids[i] = i; rp[i] = make_float2(0.f, pres ? pres[i] : 0.f); }
+}
+__global__ void k_scatter3(int n, const int* __restrict__ ids, const float4* __restrict__ src, float* __restrict__ dst) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) { const int id = ids[t]; const float4 v = src[t]; dst[3 * id] = v.x; dst[3 * id + 1] = v.y; dst[3 * id + 2] = v.z; }
+}
+__global__ void k_scatter3d(int n, const int* __restrict__ ids, const float4* __restrict__ src, double* __restrict__ dst) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) { const int id = ids[t]; const float4 v = src[t]; dst[3 * id] = v.x; dst[3 * id + 1] = v.y; dst[3 * id + 2] = v.z; }
+}
+__global__ void k_scatter_rp(int n, const int* __restrict__ ids, const float2* __restrict__ rp, int comp, float* __restrict__ dst) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) dst[ids[t]] = comp ? rp[t].y : rp[t].x;
+}
+__global__ void k_scatter_u32(int n, const int* __restrict__ ids, const uint32_t* __restrict__ src, uint32_t* __restrict__ dst) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) dst[ids[t]] = src[t];
+}
+
+inline int blocks(int n) { return (n + psb::kBlock - 1) / psb::kBlock; }
+
+int bits_for(size_t ncells) {
+    int b = 1;
+    while (b < 32 && ((size_t)1 << b) < ncells) ++b;
+    return b;
+}
+
+// Grid, sort, reorder, neighbour lists, density at x.
+int build(psb_ctx* c) {
+    cudaStream_t st = c->stream;
+    Params P = c->P;
+    P.n = c->n;
+    const int n = c->n;
+    if (c->sorted >= 0)
+        timed(c, "reset_cells", [&] { psb::launch_reset_cells(st, c->sorted_n, c->keys[c->sorted], c->cell_start); });
+    cudaMemsetAsync(c->flags, 0, 8 * sizeof(int), st);
+    timed(c, "cell_keys", [&] {
+        psb::launch_cell_keys(st, P, c->pos[c->cs], c->ids[c->cr], c->keys[0], c->vals[0], &c->flags[4]);
+    });
+    int res = 0;
+    timed(c, "radix_sort", [&] { res = psb::radix_sort(st, n, c->key_bits, c->keys, c->vals, c->hist, c->hist_blocks); });
+    const int ns = c->cs ^ 1, nr = c->cr ^ 1;
+    timed(c, "reorder", [&] {
+        psb::launch_reorder(st, n, c->keys[res], c->vals[res], c->pos[c->cs], c->vel[c->cs], c->vap[c->cs], c->rp[c->cr],
+                            c->ids[c->cr], c->pos[ns], c->vel[ns], c->vap[ns], c->rp[nr], c->ids[nr], c->cell_start,
+                            c->cell_end);
+    });
+    c->cs = ns;
+    c->cr = nr;
+    c->sorted = res;
+    c->sorted_n = n;
+    timed(c, "build_nbr", [&] {
+        psb::launch_build_nbr(st, P, c->pos[c->cs], c->keys[res], c->cell_start, c->cell_end, c->nbr_count, c->nbr_list,
+                              c->flags);
+    });
+    const int zero_p = P.pci && (P.ref || c->sc.warm_start == PSB_WARM_ZERO);
+    timed(c, "density_x", [&] {
+        psb::launch_density_x(st, P, c->pos[c->cs], c->nbr_count, c->nbr_list, c->rp[c->cr], c->rho_x, zero_p);
+    });
+    c->built = true;
+    return cuda_check(c, cudaGetLastError(), "launch");
+}
+
+int read_flags(psb_ctx* c) {
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->h_flags, c->flags, 8 * sizeof(int), cudaMemcpyDeviceToHost, c->stream), "flags"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "sync"));
+    c->stats.nbr_max = c->h_flags[1];
+    long long tot;
+    std::memcpy(&tot, &c->h_flags[2], 8);
+    c->stats.nbr_total = tot;
+    c->stats.clamped = c->h_flags[4];
+    if (c->h_flags[0]) return fail(c, PSB_EOVERFLOW_NBR, "a particle has " + std::to_string(c->h_flags[1]) +
+                                                             " neighbours, more than nbr_cap " + std::to_string(c->cap));
+    return PSB_OK;
+}
+
+int step_once(psb_ctx* c, bool last) {
+    PSB_TRY(build(c));
+    cudaStream_t st = c->stream;
+    Params P = c->P;
+    P.n = c->n;
+    const int s = c->cs, r = c->cr;
+    int iters = 0, converged = 1;
+    cudaMemsetAsync(c->err_hist, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1), st);
+    if (!P.pci) {
+        const int o = s ^ 1;
+        timed(c, "wcsph_force", [&] {
+            psb::launch_wcsph_force(st, P, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list,
+                                    c->pos[o], c->vel[o], c->vap[o], c->fnp);
+        });
+        c->cs = o;
+        c->stats.iters = 0;
+        c->stats.converged = 1;
+    } else {
+        const int warm = (!P.ref && c->sc.warm_start == PSB_WARM_PREVIOUS) ? 1 : 0;
+        timed(c, "pci_init", [&] {
+            psb::launch_pci_init(st, P, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list, warm,
+                                 c->fnp, c->xs[0], c->vs);
+        });
+        const int min_it = P.ref ? 3 : c->sc.min_iters;
+        const int max_it = P.ref ? 3 : c->sc.max_iters;
+        int xi = 0, k = 0, passes = 0;
+        converged = P.ref ? 1 : 0;
+        for (;;) {
+            if (k >= max_it) break;
+            timed(c, "pci_density", [&] {
+                psb::launch_pci_density(st, P, c->xs[xi], c->rp[r], c->nbr_count, c->nbr_list, c->rpc, &c->err_hist[k]);
+            });
+            ++passes;
+            if (!P.ref) {
+                PSB_TRY(cuda_check(c, cudaMemcpyAsync(&c->h_err[k], &c->err_hist[k], 8, cudaMemcpyDeviceToHost, st), "err"));
+                PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "sync"));
+                if (k >= min_it && psb::unorder_double(c->h_err[k]) <= c->sc.eta) { converged = 1; break; }
+            }
+            timed(c, "pci_force_predict", [&] {
+                psb::launch_pci_force_predict(st, P, c->pos[s], c->vap[s], c->fnp, c->xs[xi], c->rpc, c->nbr_count,
+                                              c->nbr_list, c->xs[xi ^ 1], c->vs, c->rp[r]);
+            });
+            xi ^= 1;
+            ++k;
+        }
+        timed(c, "pci_commit", [&] {
+            psb::launch_pci_commit(st, P, c->xs[xi], c->vs, c->rpc, passes > 0, c->pos[s], c->vel[s], c->vap[s], c->rp[r]);
+        });
+        iters = k;
+        c->stats.iters = iters;
+        c->stats.converged = converged;
+        if (last || !P.ref) {
+            PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->h_err, c->err_hist, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1),
+                                                  cudaMemcpyDeviceToHost, st), "err"));
+        }
+    }
+    c->stats.steps += 1;
+    c->stats.iters_total += iters;
+    PSB_TRY(cuda_check(c, cudaGetLastError(), "launch"));
+    if (last) {
+        PSB_TRY(read_flags(c));
+        for (int i = 0; i <= PSB_MAX_ITERS; ++i)
+            c->stats.err[i] = (P.pci && c->h_err[i]) ? psb::unorder_double(c->h_err[i]) : 0.0;
+        if (P.pci && !converged) return fail(c, PSB_ENOCONV, "corrector loop reached max_iters above eta");
+    } else if (P.pci && !P.ref && !converged) {
+        // keep going; the status is reported by the last step of the call
+    }
+    return PSB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t psb_abi_version(void) { return PSB_ABI_VERSION; }
+
+const char* psb_status_string(int32_t status) {
+    if (status < 0 || status > PSB_ESTATE) return "unknown status";
+    return kStatus[status];
+}
+
+const char* psb_last_error(const psb_ctx* c) { return c ? c->err.c_str() : ""; }
+
+int psb_create(const psb_scene* scene, psb_ctx** out) {
+    if (!out) return PSB_EINVAL;
+    *out = nullptr;
+    std::string why;
+    if (validate(scene, why) != PSB_OK) {
+        std::fprintf(stderr, "psb_create: %s\n", why.c_str());
+        return PSB_EINVAL;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        std::fprintf(stderr, "psb_create: no CUDA device\n");
+        return PSB_ECUDA;
+    }
+    psb_ctx* c = new psb_ctx();
+    c->sc = *scene;
+    if (c->sc.nbr_cap == 0) c->sc.nbr_cap = 128;
+    c->P = derive(c->sc);
+    c->n_max = scene->n_max;
+    c->cap = c->P.cap;
+    c->ncells = (size_t)scene->dims[0] * scene->dims[1] * scene->dims[2];
+    c->key_bits = bits_for(c->ncells);
+    c->hist_blocks = psb::radix_blocks(c->n_max);
+    cudaGetDevice(&c->device);
+    const size_t n = (size_t)c->n_max;
+    int rc = PSB_OK;
+    for (int i = 0; i < 2 && rc == PSB_OK; ++i) {
+        rc = dalloc(c, &c->pos[i], n); if (rc) break;
+        rc = dalloc(c, &c->vel[i], n); if (rc) break;
+        rc = dalloc(c, &c->vap[i], n); if (rc) break;
+        rc = dalloc(c, &c->rp[i], n); if (rc) break;
+        rc = dalloc(c, &c->ids[i], n); if (rc) break;
+        rc = dalloc(c, &c->keys[i], n); if (rc) break;
+        rc = dalloc(c, &c->vals[i], n); if (rc) break;
+        rc = dalloc(c, &c->xs[i], n); if (rc) break;
+    }
+    if (!rc) rc = dalloc(c, &c->hist, (size_t)256 * c->hist_blocks);
+    if (!rc) rc = dalloc(c, &c->cell_start, c->ncells);
+    if (!rc) rc = dalloc(c, &c->cell_end, c->ncells);
+    if (!rc) rc = dalloc(c, &c->nbr_count, n);
+    if (!rc) rc = dalloc(c, &c->nbr_list, n * (size_t)c->cap);
+    if (!rc) rc = dalloc(c, &c->fnp, n);
+    if (!rc) rc = dalloc(c, &c->vs, n);
+    if (!rc) rc = dalloc(c, &c->rpc, n);
+    if (!rc) rc = dalloc(c, &c->rho_x, n);
+    if (!rc) rc = dalloc(c, &c->err_hist, PSB_MAX_ITERS + 1);
+    if (!rc) rc = dalloc(c, &c->flags, 8);
+    if (!rc) rc = dalloc(c, (char**)&c->stage, n * 32);
+    if (!rc && cudaMallocHost((void**)&c->h_err, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1)) != cudaSuccess) rc = PSB_ENOMEM;
+    if (!rc && cudaMallocHost((void**)&c->h_flags, 8 * sizeof(int)) != cudaSuccess) rc = PSB_ENOMEM;
+    if (!rc && cudaMemset(c->cell_start, 0xFF, sizeof(uint32_t) * c->ncells) != cudaSuccess) rc = PSB_ECUDA;
+    if (!rc && cudaMemset(c->err_hist, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1)) != cudaSuccess) rc = PSB_ECUDA;
+    if (!rc && cudaDeviceSynchronize() != cudaSuccess) rc = PSB_ECUDA;
+    if (rc) {
+        std::fprintf(stderr, "psb_create: %s\n", c->err.empty() ? "allocation failed" : c->err.c_str());
+        cudaGetLastError();
+        free_all(c);
+        delete c;
+        return rc;
+    }
+    std::memset(c->h_err, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1));
+    *out = c;
+    return PSB_OK;
+}
+
+int psb_destroy(psb_ctx* c) {
+    if (!c) return PSB_EINVAL;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_all(c);
+    delete c;
+    return PSB_OK;
+}
+
+int psb_set_stream(psb_ctx* c, void* stream) {
+    if (!c) return PSB_EINVAL;
+    c->prof.resolve(c->stream);
+    c->stream = (cudaStream_t)stream;
+    return PSB_OK;
+}
+
+static int upload_common(psb_ctx* c, int32_t n) {
+    // forget the previous particle set: clear its occupied cells
+    if (c->sorted >= 0) {
+        psb::launch_reset_cells(c->stream, c->sorted_n, c->keys[c->sorted], c->cell_start);
+        c->sorted = -1;
+    }
+    c->n = n;
+    c->cs = c->cr = 0;
+    c->uploaded = true;
+    c->built = false;
+    return PSB_OK;
+}
+
+int psb_upload(psb_ctx* c, int32_t n, const float* pos, const float* vel, const float* vel_half, const float* pressure) {
+    if (!c || n <= 0 || n > c->n_max || !pos) return fail(c, PSB_EINVAL, "psb_upload: bad n or NULL pos");
+    cudaSetDevice(c->device);
+    upload_common(c, n);
+    cudaStream_t st = c->stream;
+    float* stage = (float*)c->stage;
+    const size_t b3 = sizeof(float) * 3 * (size_t)n;
+    struct { const float* src; float4* dst; } parts[3] = {{pos, c->pos[0]}, {vel, c->vel[0]}, {vel_half, c->vap[0]}};
+    for (auto& p : parts) {
+        if (p.src) PSB_TRY(cuda_check(c, cudaMemcpyAsync(stage, p.src, b3, cudaMemcpyHostToDevice, st), "upload"));
+        k_pack3<<<blocks(n), psb::kBlock, 0, st>>>(n, p.src ? stage : nullptr, p.dst);
+    }
+    if (pressure) PSB_TRY(cuda_check(c, cudaMemcpyAsync(stage, pressure, sizeof(float) * n, cudaMemcpyHostToDevice, st), "upload"));
+    k_init_ids<<<blocks(n), psb::kBlock, 0, st>>>(n, pressure ? stage : nullptr, c->ids[0], c->rp[0]);
+    return cuda_check(c, cudaGetLastError(), "upload");
+}
+
+int psb_upload_aos_f64(psb_ctx* c, int32_t n, const double* pos, const double* vel, const double* vel_half,
+                       int32_t on_device) {
+    if (!c || n <= 0 || n > c->n_max || !pos) return fail(c, PSB_EINVAL, "psb_upload_aos_f64: bad n or NULL pos");
+    cudaSetDevice(c->device);
+    upload_common(c, n);
+    cudaStream_t st = c->stream;
+    double* stage = (double*)c->stage;
+    const size_t b3 = sizeof(double) * 3 * (size_t)n;
+    struct { const double* src; float4* dst; } parts[3] = {{pos, c->pos[0]}, {vel, c->vel[0]}, {vel_half, c->vap[0]}};
+    for (auto& p : parts) {
+        const double* src = nullptr;
+        if (p.src) {
+            if (on_device) src = p.src;
+            else {
+                PSB_TRY(cuda_check(c, cudaMemcpyAsync(stage, p.src, b3, cudaMemcpyHostToDevice, st), "upload"));
+                src = stage;
+            }
+        }
+        k_pack3d<<<blocks(n), psb::kBlock, 0, st>>>(n, src, p.dst);
+    }
+    k_init_ids<<<blocks(n), psb::kBlock, 0, st>>>(n, nullptr, c->ids[0], c->rp[0]);
+    return cuda_check(c, cudaGetLastError(), "upload");
+}
+
+int psb_download(psb_ctx* c, float* pos, float* vel, float* vel_half, float* density, float* pressure) {
+    if (!c) return PSB_EINVAL;
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_download before psb_upload");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    const int n = c->n;
+    float* stage = (float*)c->stage;
+    struct { float* dst; const float4* src; } v3[3] = {{pos, c->pos[c->cs]}, {vel, c->vel[c->cs]}, {vel_half, c->vap[c->cs]}};
+    for (auto& p : v3) {
+        if (!p.dst) continue;
+        k_scatter3<<<blocks(n), psb::kBlock, 0, st>>>(n, c->ids[c->cr], p.src, stage);
+        PSB_TRY(cuda_check(c, cudaMemcpyAsync(p.dst, stage, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st), "download"));
+        PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "download"));
+    }
+    struct { float* dst; int comp; } v1[2] = {{density, 0}, {pressure, 1}};
+    for (auto& p : v1) {
+        if (!p.dst) continue;
+        k_scatter_rp<<<blocks(n), psb::kBlock, 0, st>>>(n, c->ids[c->cr], c->rp[c->cr], p.comp, stage);
+        PSB_TRY(cuda_check(c, cudaMemcpyAsync(p.dst, stage, sizeof(float) * n, cudaMemcpyDeviceToHost, st), "download"));
+        PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "download"));
+    }
+    return cuda_check(c, cudaGetLastError(), "download");
+}
+
+int psb_download_aos_f64(psb_ctx* c, double* pos, double* vel, double* vel_half, int32_t on_device) {
+    if (!c) return PSB_EINVAL;
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_download before psb_upload");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    const int n = c->n;
+    double* stage = (double*)c->stage;
+    struct { double* dst; const float4* src; } v3[3] = {{pos, c->pos[c->cs]}, {vel, c->vel[c->cs]}, {vel_half, c->vap[c->cs]}};
+    for (auto& p : v3) {
+        if (!p.dst) continue;
+        if (on_device) {
+            k_scatter3d<<<blocks(n), psb::kBlock, 0, st>>>(n, c->ids[c->cr], p.src, p.dst);
+        } else {
+            k_scatter3d<<<blocks(n), psb::kBlock, 0, st>>>(n, c->ids[c->cr], p.src, stage);
+            PSB_TRY(cuda_check(c, cudaMemcpyAsync(p.dst, stage, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st), "download"));
+        }
+    }
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "download"));
+    return cuda_check(c, cudaGetLastError(), "download");
+}
+
+int psb_step(psb_ctx* c, int32_t nsteps) {
+    if (!c || nsteps < 0) return fail(c, PSB_EINVAL, "psb_step: bad argument");
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_step before psb_upload");
+    cudaSetDevice(c->device);
+    int status = PSB_OK;
+    for (int i = 0; i < nsteps; ++i) {
+        const int rc = step_once(c, i == nsteps - 1);
+        if (rc == PSB_ENOCONV) { status = rc; continue; }
+        if (rc != PSB_OK) return rc;
+    }
+    if (c->prof.on) c->prof.resolve(c->stream);
+    return status;
+}
+
+int psb_build_neighbors(psb_ctx* c) {
+    if (!c) return PSB_EINVAL;
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_build_neighbors before psb_upload");
+    cudaSetDevice(c->device);
+    PSB_TRY(build(c));
+    return read_flags(c);
+}
+
+int psb_read_field(psb_ctx* c, int32_t field, void* dst, size_t bytes) {
+    if (!c || !dst) return PSB_EINVAL;
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_read_field before psb_upload");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    const int n = c->n;
+    const int* ids = c->ids[c->cr];
+    size_t need = 0;
+    const void* src = c->stage;
+    switch (field) {
+        case PSB_FIELD_POS: case PSB_FIELD_VEL: case PSB_FIELD_VEL_HALF: case PSB_FIELD_FORCE_NP: {
+            const float4* s = field == PSB_FIELD_POS ? c->pos[c->cs] : field == PSB_FIELD_VEL ? c->vel[c->cs]
+                            : field == PSB_FIELD_VEL_HALF ? c->vap[c->cs] : c->fnp;
+            need = sizeof(float) * 3 * n;
+            k_scatter3<<<blocks(n), psb::kBlock, 0, st>>>(n, ids, s, (float*)c->stage);
+            break;
+        }
+        case PSB_FIELD_DENSITY: case PSB_FIELD_PRESSURE:
+            need = sizeof(float) * n;
+            k_scatter_rp<<<blocks(n), psb::kBlock, 0, st>>>(n, ids, c->rp[c->cr], field == PSB_FIELD_PRESSURE, (float*)c->stage);
+            break;
+        case PSB_FIELD_DENSITY_X:
+            need = sizeof(float) * n;
+            k_scatter_u32<<<blocks(n), psb::kBlock, 0, st>>>(n, ids, (const uint32_t*)c->rho_x, (uint32_t*)c->stage);
+            break;
+        case PSB_FIELD_NBR_COUNT:
+            need = sizeof(int) * n;
+            k_scatter_u32<<<blocks(n), psb::kBlock, 0, st>>>(n, ids, (const uint32_t*)c->nbr_count, (uint32_t*)c->stage);
+            break;
+        case PSB_FIELD_CELL_KEY:
+            if (c->sorted < 0) return fail(c, PSB_ESTATE, "no sort yet");
+            need = sizeof(uint32_t) * n;
+            k_scatter_u32<<<blocks(n), psb::kBlock, 0, st>>>(n, ids, c->keys[c->sorted], (uint32_t*)c->stage);
+            break;
+        case PSB_FIELD_SORTED_ID:
+            need = sizeof(int) * n;
+            src = ids;
+            break;
+        case PSB_FIELD_SORTED_KEY:
+            if (c->sorted < 0) return fail(c, PSB_ESTATE, "no sort yet");
+            need = sizeof(uint32_t) * n;
+            src = c->keys[c->sorted];
+            break;
+        default:
+            return fail(c, PSB_EINVAL, "unknown field");
+    }
+    if (bytes < need) return fail(c, PSB_EINVAL, "destination too small");
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(dst, src, need, cudaMemcpyDeviceToHost, st), "read_field"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "read_field"));
+    return cuda_check(c, cudaGetLastError(), "read_field");
+}
+
+int psb_get_stats(psb_ctx* c, psb_step_stats* out) {
+    if (!c || !out) return PSB_EINVAL;
+    *out = c->stats;
+    return PSB_OK;
+}
+
+int psb_profile_enable(psb_ctx* c, int32_t on) {
+    if (!c) return PSB_EINVAL;
+    c->prof.resolve(c->stream);
+    c->prof.on = on != 0;
+    return PSB_OK;
+}
+
+int psb_profile_read(psb_ctx* c, int32_t index, char* name, size_t name_len, int64_t* launches, double* ms) {
+    if (!c) return PSB_EINVAL;
+    c->prof.resolve(c->stream);
+    if (index < 0 || index >= (int)c->prof.names.size()) return PSB_EINVAL;
+    if (name && name_len) {
+        std::strncpy(name, c->prof.names[index].c_str(), name_len - 1);
+        name[name_len - 1] = 0;
+    }
+    if (launches) *launches = c->prof.launches[index];
+    if (ms) *ms = c->prof.ms[index];
+    return PSB_OK;
+}
+
+int psb_profile_reset(psb_ctx* c) {
+    if (!c) return PSB_EINVAL;
+    c->prof.resolve(c->stream);
+    std::fill(c->prof.launches.begin(), c->prof.launches.end(), 0);
+    std::fill(c->prof.ms.begin(), c->prof.ms.end(), 0.0);
+    return PSB_OK;
+}
+
+}  // extern "C"

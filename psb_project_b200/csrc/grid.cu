@@ -1,0 +1,279 @@
+// grid.cu -- uniform-grid neighbour search: cell keys, stable radix sort by
+// (cell, id), cell-ordered reindexing with cell ranges, neighbour lists.
+//
+// Replaces the reference's bucket grid (64 atomically filled slots per cell,
+// src/Utils/Neighborhood/UniformGrid/UniformGridKernel.cu:30-55) and its
+// 27-cell neighbour walk writing 200-slot lists (UniformGridKernel.cu:58-95).
+// What stays identical, bit for bit:
+//   * the cell index i = floor((x - Min)/sizeCell) in FP64 from the float
+//     corner and cell edge (UniformGridKernel.cu:46-49), linearised as
+//     i + j*nx + k*nx*ny (:50);
+//   * the neighbour test length(x_i - x_j) <= h, self included (:81-82):
+//     decided in FP32 with a guard band and, inside the band, re-evaluated
+//     in FP64 with separately rounded operations in the reference's order.
+// What differs by design: particles are sorted stably by (cell, id), so the
+// neighbour order is deterministic; particles outside the grid are clamped
+// into the border cells (the reference writes out of bounds there); lists
+// are bounded (overflow raises a flag, never a trap).
+#include "psb_internal.cuh"
+
+namespace psb {
+
+namespace {
+
+__device__ __forceinline__ int cell_coord(float x, float corner, float cell, int dim, int& clamped) {
+    const double t = floor(__ddiv_rn(__dsub_rn((double)x, (double)corner), (double)cell));
+    if (!(t >= 0.0)) { clamped = 1; return 0; }          // also NaN
+    if (t >= (double)dim) { clamped = 1; return dim - 1; }
+    return (int)t;
+}
+
+// Clears the start entry of every cell the previous sort occupied.
+__global__ void k_reset_cells(int n, const uint32_t* __restrict__ sorted_keys, uint32_t* __restrict__ cell_start) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t k = sorted_keys[s];
+    if (s == 0 || sorted_keys[s - 1] != k) cell_start[k] = kEmpty;
+}
+
+// Cell key of every particle, written at its id so that a stable sort of
+// the id-ordered keys yields (cell, id) order.
+__global__ void k_cell_keys(Params P, const float4* __restrict__ pos, const int* __restrict__ ids,
+                            uint32_t* __restrict__ keys_by_id, uint32_t* __restrict__ slot_by_id,
+                            int* __restrict__ clamped) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n) return;
+    const float4 p = pos[s];
+    int c = 0;
+    const int i = cell_coord(p.x, P.g.gx, P.g.cell, P.g.nx, c);
+    const int j = cell_coord(p.y, P.g.gy, P.g.cell, P.g.ny, c);
+    const int k = cell_coord(p.z, P.g.gz, P.g.cell, P.g.nz, c);
+    const int id = ids[s];
+    keys_by_id[id] = (uint32_t)i + (uint32_t)j * (uint32_t)P.g.nx + (uint32_t)k * (uint32_t)P.g.nx * (uint32_t)P.g.ny;
+    slot_by_id[id] = (uint32_t)s;
+    const unsigned ballot = __ballot_sync(__activemask(), c);
+    if (ballot && (threadIdx.x & 31) == __ffs(ballot) - 1) atomicAdd(clamped, __popc(ballot));
+}
+
+// ---- LSD radix sort, 8-bit digits, three kernels per pass ----------------
+constexpr int kItems = 8;                      // keys per thread per tile
+constexpr int kTile = kBlock * kItems;         // 2048 keys per block
+
+__global__ void k_radix_hist(int n, int shift, int nblocks, const uint32_t* __restrict__ keys,
+                             uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kTile;
+#pragma unroll
+    for (int r = 0; r < kItems; ++r) {
+        const int i = base + r * kBlock + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of the digit-major histogram (256 * nblocks words), one block.
+__global__ void k_radix_scan(int total, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t part[1024];
+    const int t = threadIdx.x;
+    const int per = (total + 1023) / 1024;
+    const int lo = t * per, hi = min(lo + per, total);
+    uint32_t s = 0;
+    for (int i = lo; i < hi; ++i) s += hist[i];
+    part[t] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {            // Hillis-Steele inclusive scan
+        const uint32_t v = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - s;
+    for (int i = lo; i < hi; ++i) {
+        const uint32_t v = hist[i];
+        hist[i] = run;
+        run += v;
+    }
+}
+
+// Stable scatter. Tile items are ranked round by round (round r covers 256
+// consecutive keys); inside a round, lanes holding the same digit are found
+// with __match_any_sync and ranked by lane, warps by warp index.
+__global__ void __launch_bounds__(kBlock) k_radix_scatter(int n, int shift, int nblocks,
+                                                          const uint32_t* __restrict__ keys_in,
+                                                          const uint32_t* __restrict__ vals_in,
+                                                          uint32_t* __restrict__ keys_out,
+                                                          uint32_t* __restrict__ vals_out,
+                                                          const uint32_t* __restrict__ offsets) {
+    __shared__ uint32_t s_off[256];
+    __shared__ uint32_t s_wc[kBlock / 32][256];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    s_off[tid] = offsets[tid * nblocks + blockIdx.x];
+#pragma unroll
+    for (int w = 0; w < kBlock / 32; ++w) s_wc[w][tid] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kTile;
+    for (int r = 0; r < kItems; ++r) {
+        const int i = base + r * kBlock + tid;
+        const bool valid = i < n;
+        const uint32_t key = valid ? keys_in[i] : 0u;
+        const uint32_t val = valid ? vals_in[i] : 0u;
+        const uint32_t d = valid ? ((key >> shift) & 255u) : 256u;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int wrank = __popc(peers & ((1u << lane) - 1u));
+        if (valid && lane == __ffs(peers) - 1) s_wc[warp][d] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            uint32_t dst = s_off[d] + (uint32_t)wrank;
+            for (int w = 0; w < warp; ++w) dst += s_wc[w][d];
+            keys_out[dst] = key;
+            vals_out[dst] = val;
+        }
+        __syncthreads();
+        uint32_t tot = 0;
+#pragma unroll
+        for (int w = 0; w < kBlock / 32; ++w) { tot += s_wc[w][tid]; s_wc[w][tid] = 0; }
+        s_off[tid] += tot;
+        __syncthreads();
+    }
+}
+
+// Gathers the particle state into sorted order and records each occupied
+// cell's [start, end) slot range.
+__global__ void k_reorder(int n, const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                          const float4* __restrict__ pos, const float4* __restrict__ vel,
+                          const float4* __restrict__ vap, const float2* __restrict__ rp, const int* __restrict__ ids,
+                          float4* __restrict__ pos2, float4* __restrict__ vel2, float4* __restrict__ vap2,
+                          float2* __restrict__ rp2, int* __restrict__ ids2, uint32_t* __restrict__ cell_start,
+                          uint32_t* __restrict__ cell_end) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t s = vals[t];
+    pos2[t] = pos[s];
+    vel2[t] = vel[s];
+    vap2[t] = vap[s];
+    rp2[t] = rp[s];
+    ids2[t] = ids[s];
+    const uint32_t k = keys[t];
+    if (t == 0 || keys[t - 1] != k) cell_start[k] = (uint32_t)t;
+    if (t == n - 1 || keys[t + 1] != k) cell_end[k] = (uint32_t)t + 1u;
+}
+
+// The reference's test, sqrt((dx*dx + dy*dy) + dz*dz) <= h with every
+// operation rounded separately in FP64 (double3.h:15-47).
+__device__ __forceinline__ bool exact_neighbor(float4 a, float4 b, double h) {
+    const double dx = __dsub_rn((double)a.x, (double)b.x);
+    const double dy = __dsub_rn((double)a.y, (double)b.y);
+    const double dz = __dsub_rn((double)a.z, (double)b.z);
+    const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    return __dsqrt_rn(d2) <= h;
+}
+
+// One thread per sorted particle. The three cells of a grid row are
+// adjacent in sorted order, so each of the nine rows is one contiguous slot
+// range; candidates are visited in increasing slot order and the list is
+// sorted.
+__global__ void __launch_bounds__(kBlock) k_build_nbr(Params P, const float4* __restrict__ pos,
+                                                      const uint32_t* __restrict__ keys,
+                                                      const uint32_t* __restrict__ cell_start,
+                                                      const uint32_t* __restrict__ cell_end, int* __restrict__ counts,
+                                                      int* __restrict__ list, int* __restrict__ flags) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = t < P.n;       // every lane stays for the warp reductions below
+    const int n = P.n, nx = P.g.nx, ny = P.g.ny, nz = P.g.nz;
+    int cnt = 0;
+    if (valid) {
+        const float4 pi = pos[t];
+        const uint32_t key = keys[t];
+        const int ci = (int)(key % (uint32_t)nx);
+        const int cj = (int)((key / (uint32_t)nx) % (uint32_t)ny);
+        const int ck = (int)(key / ((uint32_t)nx * (uint32_t)ny));
+        const int a0 = max(ci - 1, 0), a1 = min(ci + 1, nx - 1);
+        for (int k = max(ck - 1, 0); k <= min(ck + 1, nz - 1); ++k) {
+            for (int j = max(cj - 1, 0); j <= min(cj + 1, ny - 1); ++j) {
+                const uint32_t row = (uint32_t)j * (uint32_t)nx + (uint32_t)k * (uint32_t)nx * (uint32_t)ny;
+                uint32_t lo = kEmpty, hi = 0;
+                for (int a = a0; a <= a1; ++a) {
+                    const uint32_t s = cell_start[row + a];
+                    if (s != kEmpty) {
+                        if (lo == kEmpty) lo = s;
+                        hi = cell_end[row + a];
+                    }
+                }
+                if (lo == kEmpty) continue;
+                for (uint32_t q = lo; q < hi; ++q) {
+                    const float4 pj = pos[q];
+                    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                    const float d2 = dx * dx + dy * dy + dz * dz;
+                    bool acc;
+                    if (d2 < P.h2_lo) acc = true;
+                    else if (d2 > P.h2_hi) acc = false;
+                    else acc = exact_neighbor(pi, pj, P.h);
+                    if (acc) {
+                        if (cnt < P.cap) list[(size_t)cnt * n + t] = (int)q;
+                        ++cnt;
+                    }
+                }
+            }
+        }
+        counts[t] = cnt;
+        if (cnt > P.cap) atomicOr(&flags[0], 1);
+    }
+    // flags[1]: max count, flags[2..3]: total pairs (64-bit)
+    int m = cnt;
+    unsigned long long tot = (unsigned long long)cnt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    }
+    if ((threadIdx.x & 31) == 0 && tot > 0) {
+        atomicMax(&flags[1], m);
+        atomicAdd((unsigned long long*)&flags[2], tot);
+    }
+}
+
+inline int grid_of(int n) { return (n + kBlock - 1) / kBlock; }
+
+}  // namespace
+
+void launch_reset_cells(cudaStream_t st, int n, const uint32_t* sorted_keys, uint32_t* cell_start) {
+    if (n > 0) k_reset_cells<<<grid_of(n), kBlock, 0, st>>>(n, sorted_keys, cell_start);
+}
+
+void launch_cell_keys(cudaStream_t st, const Params& P, const float4* pos, const int* ids, uint32_t* keys_by_id,
+                      uint32_t* slot_by_id, int* clamped) {
+    if (P.n > 0) k_cell_keys<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, ids, keys_by_id, slot_by_id, clamped);
+}
+
+int radix_blocks(int n) { return (n + kTile - 1) / kTile; }
+
+int radix_sort(cudaStream_t st, int n, int bits, uint32_t* keys[2], uint32_t* vals[2], uint32_t* hist, int nblocks_cap) {
+    const int nb = radix_blocks(n);
+    if (nb > nblocks_cap || n <= 0) return 0;
+    int cur = 0;
+    for (int shift = 0; shift < bits; shift += 8) {
+        k_radix_hist<<<nb, kBlock, 0, st>>>(n, shift, nb, keys[cur], hist);
+        k_radix_scan<<<1, 1024, 0, st>>>(256 * nb, hist);
+        k_radix_scatter<<<nb, kBlock, 0, st>>>(n, shift, nb, keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], hist);
+        cur ^= 1;
+    }
+    return cur;
+}
+
+void launch_reorder(cudaStream_t st, int n, const uint32_t* keys, const uint32_t* vals, const float4* pos,
+                    const float4* vel, const float4* vap, const float2* rp, const int* ids, float4* pos2, float4* vel2,
+                    float4* vap2, float2* rp2, int* ids2, uint32_t* cell_start, uint32_t* cell_end) {
+    if (n > 0)
+        k_reorder<<<grid_of(n), kBlock, 0, st>>>(n, keys, vals, pos, vel, vap, rp, ids, pos2, vel2, vap2, rp2, ids2,
+                                                 cell_start, cell_end);
+}
+
+void launch_build_nbr(cudaStream_t st, const Params& P, const float4* pos, const uint32_t* keys,
+                      const uint32_t* cell_start, const uint32_t* cell_end, int* counts, int* list, int* flags) {
+    if (P.n > 0) k_build_nbr<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, keys, cell_start, cell_end, counts, list, flags);
+}
+
+}  // namespace psb

@@ -1,0 +1,113 @@
+// psb_internal.cuh -- shared device-side types of libpsb (not part of the ABI).
+//
+// Data layout in HBM (all arrays in cell-sorted slot order after each step's
+// sort; slot s holds particle ids[s]):
+//   pos   float4  x, y, z, 0           16 B
+//   vel   float4  interpolated v       16 B   (the reference's m_dVel[1])
+//   vap   float4  leap-frog v+         16 B   (m_dVelInterAp)
+//   rp    float2  (density, pressure)   8 B   (pressure persists across steps)
+//   ids   int32   particle id           4 B
+// Per-step scratch: sort keys/values (2 x 2 x 4 B), cell_start/cell_end
+// (dense over the grid, only occupied cells are ever written or reset),
+// neighbour lists (slot-major: list[c * n + s], c < count[s]), and the
+// PCISPH predictor buffers xs[2] (float4), vs (float4), rpc (float2),
+// fnp (float4 non-pressure force density), rho_x (float).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace psb {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr int kBlock = 256;
+
+struct Grid {
+    float gx, gy, gz;   // corner (float, as UniformGrid.Min)
+    float cell;         // edge (float, as UniformGrid.sizeCell)
+    int nx, ny, nz;
+};
+
+// Uniform per-scene constants, FP32 in normalised form (q = r^2/h^2, u = r/h)
+// so that no intermediate leaves FP32 range; derived on the host in FP64.
+struct Params {
+    int n;
+    int cap;            // neighbour slots per particle
+    Grid g;
+    double h;           // exact neighbour test: sqrt(d.d) <= h in FP64
+    float h2_lo, h2_hi; // FP32 d^2 outside [h2_lo, h2_hi] is decided without the FP64 test
+    float h2, inv_h, inv_h2;
+    float k_rho;        // 315 m / (64 pi h^3):           rho = k_rho * sum (1-q)^3
+    float k_grad;       // 45 m / (pi h^4):               a_p = k_grad * sum (pV_i+pV_j)(1-u)^2 x^
+    float k_visc;       // mu m 45 / (pi h^5):            f_v = k_visc * sum (v_j-v_i)(1-u)/rho_j
+    float k_surf;       // 945 m / (32 pi h^5):           normals and surface term (reference profile)
+    float sigma, l;
+    float k_press;      // 1 / (beta G^2), beta = 2 (m dt/rho0)^2, G = 45/(pi h^4)
+    float k_delta;      // config PCISPH: prototype delta = 1/(beta (|sum gradW|^2 + sum |gradW|^2)) of a filled lattice
+    float rho0;
+    double rho0_d;
+    float eos_k;        // REF: k (p = k (rho - rho0));  CONFIG: k rho0 / 7 (Tait, gamma 7)
+    float dt;
+    float gx, gy, gz;   // gravity acceleration
+    float wlo_x, wlo_y, wlo_z, whi_x, whi_y, whi_z;   // box min + r, box max - r (float, as collisionBox)
+    float wall_k, wall_c;
+    // Config-profile wall boundary (virtual half-spaces behind the box faces):
+    float bx0, by0, bz0, bx1, by1, bz1;   // faces
+    float hf, ws;       // h and the virtual lattice spacing
+    float cz, cg;       // pi h^2/(4 s^2), 2 pi h/(3 s^2)
+    int ref;            // reference profile
+    int pci;            // PCISPH (else WCSPH)
+    int surface;        // surface tension on
+};
+
+// ---- launchers (grid.cu) -------------------------------------------------
+void launch_reset_cells(cudaStream_t st, int n, const uint32_t* sorted_keys, uint32_t* cell_start);
+void launch_cell_keys(cudaStream_t st, const Params& P, const float4* pos, const int* ids, uint32_t* keys_by_id,
+                      uint32_t* slot_by_id, int* clamped);
+// Sorts (keys, vals) by key, stably; returns the buffer index (0 or 1) holding the result.
+int radix_sort(cudaStream_t st, int n, int bits, uint32_t* keys[2], uint32_t* vals[2], uint32_t* hist, int nblocks_cap);
+int radix_blocks(int n);
+void launch_reorder(cudaStream_t st, int n, const uint32_t* keys, const uint32_t* vals, const float4* pos,
+                    const float4* vel, const float4* vap, const float2* rp, const int* ids, float4* pos2, float4* vel2,
+                    float4* vap2, float2* rp2, int* ids2, uint32_t* cell_start, uint32_t* cell_end);
+void launch_build_nbr(cudaStream_t st, const Params& P, const float4* pos, const uint32_t* keys,
+                      const uint32_t* cell_start, const uint32_t* cell_end, int* counts, int* list, int* flags);
+
+// ---- launchers (sph.cu) ---------------------------------------------------
+void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const int* counts, const int* list,
+                      float2* rp, float* rho_x, int zero_p);
+void launch_wcsph_force(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float4* vap,
+                        const float2* rp, const int* counts, const int* list, float4* pos_out, float4* vel_out,
+                        float4* vap_out, float4* fnp);
+void launch_pci_init(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float4* vap,
+                     const float2* rp, const int* counts, const int* list, int warm, float4* fnp, float4* xs,
+                     float4* vs);
+void launch_pci_density(cudaStream_t st, const Params& P, const float4* xs, const float2* rp, const int* counts,
+                        const int* list, float2* rpc, unsigned long long* err_slot);
+void launch_pci_force_predict(cudaStream_t st, const Params& P, const float4* pos, const float4* vap,
+                              const float4* fnp, const float4* xs, const float2* rpc, const int* counts,
+                              const int* list, float4* xs_next, float4* vs, float2* rp);
+void launch_pci_commit(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const float2* rpc,
+                       int have_density_pass, float4* pos, float4* vel, float4* vap, float2* rp);
+
+// Ordered encoding of doubles for atomicMax on unsigned 64-bit words.
+__host__ __device__ inline unsigned long long order_double(double v) {
+    long long b;
+#ifdef __CUDA_ARCH__
+    b = __double_as_longlong(v);
+#else
+    __builtin_memcpy(&b, &v, 8);
+#endif
+    return b >= 0 ? (unsigned long long)b ^ 0x8000000000000000ull : ~(unsigned long long)b;
+}
+__host__ __device__ inline double unorder_double(unsigned long long u) {
+    long long b = (u & 0x8000000000000000ull) ? (long long)(u ^ 0x8000000000000000ull) : (long long)~u;
+    double v;
+#ifdef __CUDA_ARCH__
+    v = __longlong_as_double(b);
+#else
+    __builtin_memcpy(&v, &b, 8);
+#endif
+    return v;
+}
+
+}  // namespace psb

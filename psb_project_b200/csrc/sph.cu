@@ -1,0 +1,455 @@
+// sph.cu -- SPH density, forces and the PCISPH predictor-corrector sweeps.
+//
+// One thread per cell-sorted particle, walking its neighbour list (slot-
+// major, so a warp's list reads are coalesced). Sums are per-particle and
+// atomic-free, in the list's fixed order; densities use Kahan-compensated
+// FP32 sums. All kernel constants are pre-scaled (q = r^2/h^2, u = r/h) so
+// FP32 never sees h^9.
+//
+// Formulas and their reference sources (paths inside the reference tree):
+//   density  rho_i = m 315/(64 pi h^9) sum (h^2-r^2)^3
+//            SphKernel.cu:9-27, PciSphSystem_Kernel.cu:70-85
+//   pressure force density -rho_i sum m (p_i/rho_i^2 + p_j/rho_j^2) gradW,
+//            gradW = -45/(pi h^6) (h-r)^2 r^     SphKernel.cu:53-61, PciSphSystem_Kernel.cu:88-114
+//   viscosity sum mu (v_j-v_i) m/rho_j 45 (h-r)/(pi h^6)
+//            SphKernel.cu:63-66, PciSphSystem_Kernel.cu:141-146
+//   surface tension and normals (reference profile only)
+//            SphKernel.cu:68-88, PciSphSystem_Kernel.cu:148-166
+//   PCISPH pressure increment (rho*-rho0)/(beta(|sum gradW|^2 + sum|gradW|^2)),
+//            compressed particles only     PciSphSystem_Kernel.cu:36-67
+//            (config profile: Solenthaler & Pajarola's prototype factor for every
+//            particle, p clamped at 0; the per-particle form diverges when
+//            iterated to an eta, see the config notes in the oracle)
+//   leap-frog v+ += a dt, x += v+ dt; v = (v- + v+)/2
+//            SphKernel.cu:95-135
+//   box walls: projection + reflection     BoxCollision_Kernel.cu:7-34
+// The reference's predict/restore passes (PciSphSystem.cu:30-61) become a
+// predictor that writes x*, v* to separate buffers and leaves the state
+// alone; the final leap-frog is the last prediction committed.
+#include "psb_internal.cuh"
+
+namespace psb {
+
+namespace {
+
+struct Kahan {
+    float s = 0.f, c = 0.f;     // sum and (negated) lost low part: true sum ~ s - c
+    __device__ __forceinline__ void add(float x) {
+        const float y = x - c;
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+};
+
+// rho - rho0 = k_rho (s - c) - rho0 with the product's low part kept by the
+// FMA: the deviation, from which every pressure is computed, keeps its full
+// relative precision instead of the ~6e-5 absolute step of an FP32 density.
+__device__ __forceinline__ float density_deviation(const Params& P, const Kahan& a) {
+    return fmaf(P.k_rho, a.s, -P.rho0) - P.k_rho * a.c;
+}
+
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+
+// Penalty walls (config profile): a = K*depth - C*v along each violated axis.
+__device__ __forceinline__ float3 wall_accel(const Params& P, float4 x, float4 v) {
+    float3 a = make_float3(0.f, 0.f, 0.f);
+    if (P.ref) return a;
+    if (x.x < P.wlo_x) a.x += P.wall_k * (P.wlo_x - x.x) - P.wall_c * v.x;
+    if (x.x > P.whi_x) a.x += -P.wall_k * (x.x - P.whi_x) - P.wall_c * v.x;
+    if (x.y < P.wlo_y) a.y += P.wall_k * (P.wlo_y - x.y) - P.wall_c * v.y;
+    if (x.y > P.whi_y) a.y += -P.wall_k * (x.y - P.whi_y) - P.wall_c * v.y;
+    if (x.z < P.wlo_z) a.z += P.wall_k * (P.wlo_z - x.z) - P.wall_c * v.z;
+    if (x.z > P.whi_z) a.z += -P.wall_k * (x.z - P.whi_z) - P.wall_c * v.z;
+    return a;
+}
+
+// Config-profile wall boundary: each box face is backed by a half-space of
+// virtual particles on the rest lattice (layers at (k+1/2) s behind the face;
+// Harada, Koshizuka, Kawaguchi 2007, wall weight functions). Averaged along
+// the face, the layer sums are closed forms:
+//   density  sum (1-q)^3          = cz sum_k (1 - z_k^2/h^2)^4
+//   gradient sum (1-u)^2 (n . x^) = cg sum_k z_k (1 - z_k/h)^3
+// with z_k = d + (k+1/2) s. The virtual particles mirror the particle's own
+// pressure, so they push with 2 pV_i times the gradient sum.
+__device__ __forceinline__ void wall_face(const Params& P, float d, float& z, float& g) {
+    d = fmaxf(d, 0.f);
+    z = 0.f;
+    g = 0.f;
+#pragma unroll 1
+    for (int k = 0; k < 8; ++k) {
+        const float zk = d + ((float)k + 0.5f) * P.ws;
+        if (zk >= P.hf) break;
+        const float q = zk * zk * P.inv_h2;
+        const float t = 1.f - q;
+        z += (t * t) * (t * t);
+        const float u = 1.f - zk * P.inv_h;
+        g += zk * u * u * u;
+    }
+    z *= P.cz;
+    g *= P.cg;
+}
+
+// Sum over the six faces: normalised density term and gradient (into the box).
+__device__ __forceinline__ float wall_terms(const Params& P, float4 x, float3& g) {
+    float zs = 0.f, z, gg;
+    g = make_float3(0.f, 0.f, 0.f);
+    if (x.x - P.bx0 < P.hf) { wall_face(P, x.x - P.bx0, z, gg); zs += z; g.x += gg; }
+    if (P.bx1 - x.x < P.hf) { wall_face(P, P.bx1 - x.x, z, gg); zs += z; g.x -= gg; }
+    if (x.y - P.by0 < P.hf) { wall_face(P, x.y - P.by0, z, gg); zs += z; g.y += gg; }
+    if (P.by1 - x.y < P.hf) { wall_face(P, P.by1 - x.y, z, gg); zs += z; g.y -= gg; }
+    if (x.z - P.bz0 < P.hf) { wall_face(P, x.z - P.bz0, z, gg); zs += z; g.z += gg; }
+    if (P.bz1 - x.z < P.hf) { wall_face(P, P.bz1 - x.z, z, gg); zs += z; g.z -= gg; }
+    return zs;
+}
+
+// collisionBox (BoxCollision_Kernel.cu:7-34) with restitution 0: clamp into
+// [Min+r, Max-r] (upper bounds tested first, lower bounds win), then remove
+// the velocity component along the normalised sum of wall normals.
+__device__ __forceinline__ void box_project(const Params& P, float3& x, float3& v) {
+    float3 pI = x, nI = make_float3(0.f, 0.f, 0.f);
+    if (x.x >= P.whi_x) { pI.x = P.whi_x; nI.x = -1.f; }
+    if (x.y >= P.whi_y) { pI.y = P.whi_y; nI.y = -1.f; }
+    if (x.z >= P.whi_z) { pI.z = P.whi_z; nI.z = -1.f; }
+    if (x.x <= P.wlo_x) { pI.x = P.wlo_x; nI.x = 1.f; }
+    if (x.y <= P.wlo_y) { pI.y = P.wlo_y; nI.y = 1.f; }
+    if (x.z <= P.wlo_z) { pI.z = P.wlo_z; nI.z = 1.f; }
+    const float l2 = nI.x * nI.x + nI.y * nI.y + nI.z * nI.z;
+    if (l2 > 0.f) {
+        const float il = rsqrtf(l2);
+        nI.x *= il; nI.y *= il; nI.z *= il;
+        const float vd = v.x * nI.x + v.y * nI.y + v.z * nI.z;
+        x = pI;
+        v.x -= vd * nI.x; v.y -= vd * nI.y; v.z -= vd * nI.z;
+    }
+}
+
+// ---- density at the step's start positions ---------------------------------
+// WCSPH: also the equation of state (reference: p = k (rho - rho0),
+// SphKernel.cu:25; config: Tait, p = k rho0/7 ((rho/rho0)^7 - 1), written as
+// k rho0/7 d (1 + x + ... + x^6) with x = 1 + d to avoid cancellation).
+// PCISPH: keeps the carried pressure (warm start) or zeroes it.
+__global__ void __launch_bounds__(kBlock) k_density_x(Params P, const float4* __restrict__ pos,
+                                                      const int* __restrict__ counts, const int* __restrict__ list,
+                                                      float2* __restrict__ rp, float* __restrict__ rho_x, int zero_p) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const float4 xi = pos[t];
+    const int cnt = min(counts[t], P.cap);
+    Kahan acc;
+    for (int c = 0; c < cnt; ++c) {
+        const float4 xj = pos[list[(size_t)c * P.n + t]];
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float q = (dx * dx + dy * dy + dz * dz) * P.inv_h2;
+        if (!P.ref && q >= 1.f) continue;
+        const float w = 1.f - q;
+        acc.add(w * w * w);
+    }
+    if (!P.ref) {
+        float3 g;
+        acc.add(wall_terms(P, xi, g));
+    }
+    const float drho = density_deviation(P, acc);
+    const float rho = P.rho0 + drho;
+    float p;
+    if (P.pci) {
+        p = zero_p ? 0.f : rp[t].y;
+    } else if (P.ref) {
+        p = P.eos_k * drho;
+    } else {
+        const float d = drho / P.rho0;
+        const float x = 1.f + d;
+        const float s = 1.f + x * (1.f + x * (1.f + x * (1.f + x * (1.f + x * (1.f + x)))));
+        p = P.eos_k * d * s;
+    }
+    rp[t] = make_float2(rho, p);
+    rho_x[t] = rho;
+}
+
+// Viscosity (+ reference surface tension) and, when with_pressure, the
+// symmetric pressure acceleration, over the list at the start positions.
+struct PairSums {
+    float3 ap;      // sum (pV_i + pV_j) (1-u)^2 x^_ij   (times k_grad: pressure acceleration)
+    float3 fv;      // sum (v_j - v_i) (1-u) / rho_j     (times k_visc: viscosity force density)
+    float3 nrm;     // sum x_ij (1-q)^2 / rho_j           (times -k_surf: surface normal)
+    float fs;       // sum (1-q)(3-7q) / rho_j           (times -k_surf: surface term)
+};
+
+template <bool WITH_PRESSURE>
+__device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi, float4 vi, float2 rpi,
+                                              const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                              const float2* __restrict__ rp, const int* __restrict__ counts,
+                                              const int* __restrict__ list) {
+    PairSums S;
+    S.ap = S.fv = S.nrm = make_float3(0.f, 0.f, 0.f);
+    S.fs = 0.f;
+    const float pVi = WITH_PRESSURE ? rpi.y / (rpi.x * rpi.x) : 0.f;
+    const int cnt = min(counts[t], P.cap);
+    for (int c = 0; c < cnt; ++c) {
+        const int j = list[(size_t)c * P.n + t];
+        const float4 xj = pos[j];
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 > 0.f)) continue;
+        const float q = r2 * P.inv_h2;
+        if (!P.ref && q >= 1.f) continue;
+        const float4 vj = vel[j];
+        const float2 rpj = rp[j];
+        const float rinv = rsqrtf(r2);
+        const float om = 1.f - r2 * rinv * P.inv_h;
+        const float inv_rj = 1.f / rpj.x;
+        const float sv = om * inv_rj;
+        S.fv.x += (vj.x - vi.x) * sv;
+        S.fv.y += (vj.y - vi.y) * sv;
+        S.fv.z += (vj.z - vi.z) * sv;
+        if (WITH_PRESSURE) {
+            const float s = (pVi + rpj.y * inv_rj * inv_rj) * om * om * rinv;
+            S.ap.x += s * dx; S.ap.y += s * dy; S.ap.z += s * dz;
+        }
+        if (P.surface) {
+            const float t1 = 1.f - q;
+            S.fs += t1 * (3.f - 7.f * q) * inv_rj;
+            const float sn = t1 * t1 * inv_rj;
+            S.nrm.x += dx * sn; S.nrm.y += dy * sn; S.nrm.z += dz * sn;
+        }
+    }
+    if (WITH_PRESSURE && !P.ref) {
+        float3 g;
+        wall_terms(P, xi, g);
+        S.ap.x += 2.f * pVi * g.x; S.ap.y += 2.f * pVi * g.y; S.ap.z += 2.f * pVi * g.z;
+    }
+    return S;
+}
+
+// Non-pressure force density f_v + f_s + rho_i g (the reference's forcesAccum
+// is (0, -9.81 rho, 0) in PCISPH, PciSphSystem_Kernel.cu:168, and rho*g from
+// ForceExt_Constante in WCSPH, SphSystem.cpp:307-320).
+__device__ __forceinline__ float3 nonpressure_force(const Params& P, const PairSums& S, float rho) {
+    float3 f = make_float3(P.k_visc * S.fv.x, P.k_visc * S.fv.y, P.k_visc * S.fv.z);
+    if (P.surface) {
+        const float3 n = make_float3(-P.k_surf * S.nrm.x, -P.k_surf * S.nrm.y, -P.k_surf * S.nrm.z);
+        const float ln = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
+        if (ln >= P.l) {
+            const float c = (-P.k_surf * S.fs) * (-P.sigma) / ln;
+            f.x += c * n.x; f.y += c * n.y; f.z += c * n.z;
+        }
+    }
+    f.x += rho * P.gx; f.y += rho * P.gy; f.z += rho * P.gz;
+    return f;
+}
+
+// WCSPH: forces, leap-frog, walls and velocity interpolation in one sweep.
+__global__ void __launch_bounds__(kBlock) k_wcsph_force(Params P, const float4* __restrict__ pos,
+                                                        const float4* __restrict__ vel, const float4* __restrict__ vap,
+                                                        const float2* __restrict__ rp, const int* __restrict__ counts,
+                                                        const int* __restrict__ list, float4* __restrict__ pos_out,
+                                                        float4* __restrict__ vel_out, float4* __restrict__ vap_out,
+                                                        float4* __restrict__ fnp) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const float4 xi = pos[t], vi = vel[t], vh = vap[t];
+    const float2 rpi = rp[t];
+    const PairSums S = pair_sums<true>(P, t, xi, vi, rpi, pos, vel, rp, counts, list);
+    const float3 f = nonpressure_force(P, S, rpi.x);
+    fnp[t] = make_float4(f.x, f.y, f.z, 0.f);
+    const float3 aw = wall_accel(P, xi, vh);
+    const float ir = 1.f / rpi.x;
+    const float3 a = make_float3(f.x * ir + P.k_grad * S.ap.x + aw.x, f.y * ir + P.k_grad * S.ap.y + aw.y,
+                                 f.z * ir + P.k_grad * S.ap.z + aw.z);
+    float3 v = make_float3(vh.x + a.x * P.dt, vh.y + a.y * P.dt, vh.z + a.z * P.dt);
+    float3 x = make_float3(xi.x + v.x * P.dt, xi.y + v.y * P.dt, xi.z + v.z * P.dt);
+    if (P.ref) box_project(P, x, v);
+    pos_out[t] = make_float4(x.x, x.y, x.z, 0.f);
+    vap_out[t] = make_float4(v.x, v.y, v.z, 0.f);
+    vel_out[t] = make_float4((vh.x + v.x) * 0.5f, (vh.y + v.y) * 0.5f, (vh.z + v.z) * 0.5f, 0.f);
+}
+
+// PCISPH set-up sweep: non-pressure forces at x (and, for a warm start, the
+// pressure acceleration of the carried pressure), then the first prediction.
+__global__ void __launch_bounds__(kBlock) k_pci_init(Params P, const float4* __restrict__ pos,
+                                                     const float4* __restrict__ vel, const float4* __restrict__ vap,
+                                                     const float2* __restrict__ rp, const int* __restrict__ counts,
+                                                     const int* __restrict__ list, int warm, float4* __restrict__ fnp,
+                                                     float4* __restrict__ xs, float4* __restrict__ vs) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const float4 xi = pos[t], vi = vel[t], vh = vap[t];
+    const float2 rpi = rp[t];
+    PairSums S;
+    if (warm) S = pair_sums<true>(P, t, xi, vi, rpi, pos, vel, rp, counts, list);
+    else S = pair_sums<false>(P, t, xi, vi, rpi, pos, vel, rp, counts, list);
+    const float3 f = nonpressure_force(P, S, rpi.x);
+    fnp[t] = make_float4(f.x, f.y, f.z, 0.f);
+    const float3 aw = wall_accel(P, xi, vh);
+    const float ir = 1.f / rpi.x;
+    const float ap = warm ? P.k_grad : 0.f;
+    const float3 a = make_float3(f.x * ir + ap * S.ap.x + aw.x, f.y * ir + ap * S.ap.y + aw.y,
+                                 f.z * ir + ap * S.ap.z + aw.z);
+    const float3 v = make_float3(vh.x + a.x * P.dt, vh.y + a.y * P.dt, vh.z + a.z * P.dt);
+    vs[t] = make_float4(v.x, v.y, v.z, 0.f);
+    xs[t] = make_float4(xi.x + v.x * P.dt, xi.y + v.y * P.dt, xi.z + v.z * P.dt, 0.f);
+}
+
+// PCISPH density pass at x*: rho*, the gradient sums of the pressure
+// increment, the candidate pressure and the FP64 max compression error.
+__global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* __restrict__ xs,
+                                                        const float2* __restrict__ rp, const int* __restrict__ counts,
+                                                        const int* __restrict__ list, float2* __restrict__ rpc,
+                                                        unsigned long long* __restrict__ err_slot) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double err = -1e300;
+    if (t < P.n) {
+        const float4 xi = xs[t];
+        const int cnt = min(counts[t], P.cap);
+        Kahan acc;
+        float3 T1 = make_float3(0.f, 0.f, 0.f);
+        float T2 = 0.f;
+        for (int c = 0; c < cnt; ++c) {
+            const float4 xj = xs[list[(size_t)c * P.n + t]];
+            const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            const float q = r2 * P.inv_h2;
+            if (!P.ref && q >= 1.f) continue;
+            const float w = 1.f - q;
+            acc.add(w * w * w);
+            if (P.ref && r2 > 0.f) {
+                const float rinv = rsqrtf(r2);
+                const float om = 1.f - r2 * rinv * P.inv_h;
+                const float g = om * om;
+                const float s = g * rinv;
+                T1.x += s * dx; T1.y += s * dy; T1.z += s * dz;
+                T2 += g * g;
+            }
+        }
+        if (!P.ref) {
+            float3 g;
+            acc.add(wall_terms(P, xi, g));
+        }
+        const float drho = density_deviation(P, acc);
+        const float rho = P.rho0 + drho;
+        float p = rp[t].y;
+        if (P.ref) {            // per-particle factor, compressed particles only
+            if (drho > 0.f && T2 > 0.f) p += P.k_press * drho / (T1.x * T1.x + T1.y * T1.y + T1.z * T1.z + T2);
+        } else {                // prototype factor, every particle, p >= 0
+            p = fmaxf(0.f, p + P.k_delta * drho);
+        }
+        rpc[t] = make_float2(rho, p);
+        err = (double)drho / P.rho0_d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
+    __shared__ double s_err[kBlock / 32];
+    if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = err;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = s_err[0];
+        for (int w = 1; w < kBlock / 32; ++w) m = fmax(m, s_err[w]);
+        if (m > -1e300) atomicMax(err_slot, order_double(m));
+    }
+}
+
+// PCISPH pressure-force pass at x* fused with the next prediction; commits
+// the candidate pressure.
+__global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const float4* __restrict__ pos,
+                                                              const float4* __restrict__ vap,
+                                                              const float4* __restrict__ fnp,
+                                                              const float4* __restrict__ xs,
+                                                              const float2* __restrict__ rpc,
+                                                              const int* __restrict__ counts,
+                                                              const int* __restrict__ list, float4* __restrict__ xs_next,
+                                                              float4* __restrict__ vs, float2* __restrict__ rp) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const float4 xi = xs[t];
+    const float2 ri = rpc[t];
+    const float pVi = ri.y / (ri.x * ri.x);
+    const int cnt = min(counts[t], P.cap);
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    for (int c = 0; c < cnt; ++c) {
+        const int j = list[(size_t)c * P.n + t];
+        const float4 xj = xs[j];
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 > 0.f)) continue;
+        if (!P.ref && r2 * P.inv_h2 >= 1.f) continue;
+        const float2 rj = rpc[j];
+        const float rinv = rsqrtf(r2);
+        const float om = 1.f - r2 * rinv * P.inv_h;
+        const float s = (pVi + rj.y / (rj.x * rj.x)) * om * om * rinv;
+        acc.x += s * dx; acc.y += s * dy; acc.z += s * dz;
+    }
+    if (!P.ref) {
+        float3 g;
+        wall_terms(P, xi, g);
+        acc.x += 2.f * pVi * g.x; acc.y += 2.f * pVi * g.y; acc.z += 2.f * pVi * g.z;
+    }
+    const float4 x0 = pos[t], vh = vap[t], f = fnp[t];
+    const float3 aw = wall_accel(P, x0, vh);
+    const float ir = 1.f / ri.x;
+    const float3 a = make_float3(f.x * ir + P.k_grad * acc.x + aw.x, f.y * ir + P.k_grad * acc.y + aw.y,
+                                 f.z * ir + P.k_grad * acc.z + aw.z);
+    const float3 v = make_float3(vh.x + a.x * P.dt, vh.y + a.y * P.dt, vh.z + a.z * P.dt);
+    vs[t] = make_float4(v.x, v.y, v.z, 0.f);
+    xs_next[t] = make_float4(x0.x + v.x * P.dt, x0.y + v.y * P.dt, x0.z + v.z * P.dt, 0.f);
+    rp[t] = ri;
+}
+
+// Commit of the last prediction, walls, velocity interpolation.
+__global__ void __launch_bounds__(kBlock) k_pci_commit(Params P, const float4* __restrict__ xs,
+                                                       const float4* __restrict__ vs, const float2* __restrict__ rpc,
+                                                       int have_density_pass, float4* __restrict__ pos,
+                                                       float4* __restrict__ vel, float4* __restrict__ vap,
+                                                       float2* __restrict__ rp) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    float3 x = f3(xs[t]), v = f3(vs[t]);
+    const float4 vh = vap[t];
+    if (P.ref) box_project(P, x, v);
+    pos[t] = make_float4(x.x, x.y, x.z, 0.f);
+    vap[t] = make_float4(v.x, v.y, v.z, 0.f);
+    vel[t] = make_float4((vh.x + v.x) * 0.5f, (vh.y + v.y) * 0.5f, (vh.z + v.z) * 0.5f, 0.f);
+    if (have_density_pass) rp[t].x = rpc[t].x;
+}
+
+inline int grid_of(int n) { return (n + kBlock - 1) / kBlock; }
+
+}  // namespace
+
+void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const int* counts, const int* list,
+                      float2* rp, float* rho_x, int zero_p) {
+    if (P.n > 0) k_density_x<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, counts, list, rp, rho_x, zero_p);
+}
+
+void launch_wcsph_force(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float4* vap,
+                        const float2* rp, const int* counts, const int* list, float4* pos_out, float4* vel_out,
+                        float4* vap_out, float4* fnp) {
+    if (P.n > 0)
+        k_wcsph_force<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, pos_out, vel_out, vap_out,
+                                                       fnp);
+}
+
+void launch_pci_init(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float4* vap,
+                     const float2* rp, const int* counts, const int* list, int warm, float4* fnp, float4* xs,
+                     float4* vs) {
+    if (P.n > 0)
+        k_pci_init<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, warm, fnp, xs, vs);
+}
+
+void launch_pci_density(cudaStream_t st, const Params& P, const float4* xs, const float2* rp, const int* counts,
+                        const int* list, float2* rpc, unsigned long long* err_slot) {
+    if (P.n > 0) k_pci_density<<<grid_of(P.n), kBlock, 0, st>>>(P, xs, rp, counts, list, rpc, err_slot);
+}
+
+void launch_pci_force_predict(cudaStream_t st, const Params& P, const float4* pos, const float4* vap,
+                              const float4* fnp, const float4* xs, const float2* rpc, const int* counts,
+                              const int* list, float4* xs_next, float4* vs, float2* rp) {
+    if (P.n > 0)
+        k_pci_force_predict<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vap, fnp, xs, rpc, counts, list, xs_next, vs, rp);
+}
+
+void launch_pci_commit(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const float2* rpc,
+                       int have_density_pass, float4* pos, float4* vel, float4* vap, float2* rp) {
+    if (P.n > 0) k_pci_commit<<<grid_of(P.n), kBlock, 0, st>>>(P, xs, vs, rpc, have_density_pass, pos, vel, vap, rp);
+}
+
+}  // namespace psb

@@ -1,0 +1,232 @@
+"""ctypes host API over libpsb.so (include/psb.h).
+
+The library is loaded from this package's lib/ directory, where
+``python -m psb_project_b200.build`` (or ``__graft_entry__.build()``) puts it.
+There is no fallback: without the compiled library every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Dict, Optional, Tuple
+
+import numpy as np
+
+from .scene import PsbScene, Scene
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libpsb.so")
+
+OK, EINVAL, ENOMEM, EOVERFLOW_NBR, ENOCONV, ECUDA, ESTATE = range(7)
+PSB_MAX_ITERS = 64
+
+FIELD_POS, FIELD_VEL, FIELD_VEL_HALF, FIELD_DENSITY, FIELD_PRESSURE, FIELD_DENSITY_X, FIELD_FORCE_NP, \
+    FIELD_NBR_COUNT, FIELD_CELL_KEY, FIELD_SORTED_ID, FIELD_SORTED_KEY = range(11)
+
+_FIELD_SPEC: Dict[int, Tuple[type, int]] = {
+    FIELD_POS: (np.float32, 3), FIELD_VEL: (np.float32, 3), FIELD_VEL_HALF: (np.float32, 3),
+    FIELD_DENSITY: (np.float32, 1), FIELD_PRESSURE: (np.float32, 1), FIELD_DENSITY_X: (np.float32, 1),
+    FIELD_FORCE_NP: (np.float32, 3), FIELD_NBR_COUNT: (np.int32, 1), FIELD_CELL_KEY: (np.uint32, 1),
+    FIELD_SORTED_ID: (np.int32, 1), FIELD_SORTED_KEY: (np.uint32, 1),
+}
+
+# Every symbol include/psb.h declares (the tests check the library exports all of them).
+EXPORTS = (
+    "psb_create", "psb_destroy", "psb_set_stream", "psb_upload", "psb_upload_aos_f64", "psb_download",
+    "psb_download_aos_f64", "psb_step", "psb_build_neighbors", "psb_read_field", "psb_get_stats",
+    "psb_profile_enable", "psb_profile_read", "psb_profile_reset", "psb_lattice", "psb_status_string",
+    "psb_last_error", "psb_abi_version",
+)
+
+
+class PsbStepStats(ctypes.Structure):
+    _fields_ = [
+        ("iters", ctypes.c_int32), ("converged", ctypes.c_int32), ("nbr_max", ctypes.c_int32),
+        ("clamped", ctypes.c_int32), ("nbr_total", ctypes.c_int64),
+        ("err", ctypes.c_double * (PSB_MAX_ITERS + 1)), ("steps", ctypes.c_int64), ("iters_total", ctypes.c_int64),
+    ]
+
+
+class PsbError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libpsb.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m psb_project_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    P, I32, I64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+    sig = {
+        "psb_create": ([ctypes.POINTER(PsbScene), ctypes.POINTER(P)], ctypes.c_int),
+        "psb_destroy": ([P], ctypes.c_int),
+        "psb_set_stream": ([P, P], ctypes.c_int),
+        "psb_upload": ([P, I32, P, P, P, P], ctypes.c_int),
+        "psb_upload_aos_f64": ([P, I32, P, P, P, I32], ctypes.c_int),
+        "psb_download": ([P, P, P, P, P, P], ctypes.c_int),
+        "psb_download_aos_f64": ([P, P, P, P, I32], ctypes.c_int),
+        "psb_step": ([P, I32], ctypes.c_int),
+        "psb_build_neighbors": ([P], ctypes.c_int),
+        "psb_read_field": ([P, I32, P, ctypes.c_size_t], ctypes.c_int),
+        "psb_get_stats": ([P, ctypes.POINTER(PsbStepStats)], ctypes.c_int),
+        "psb_profile_enable": ([P, I32], ctypes.c_int),
+        "psb_profile_read": ([P, I32, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(I64),
+                              ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+        "psb_profile_reset": ([P], ctypes.c_int),
+        "psb_lattice": ([P, ctypes.c_double, P, ctypes.c_double, ctypes.c_uint64, I32, P], ctypes.c_int),
+        "psb_status_string": ([I32], ctypes.c_char_p),
+        "psb_last_error": ([P], ctypes.c_char_p),
+        "psb_abi_version": ([], I32),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def lattice(nxyz, spacing, origin, jitter, seed, id0=0) -> np.ndarray:
+    """Lattice block positions (float32, (n, 3), ids x-fastest)."""
+    n = int(nxyz[0]) * int(nxyz[1]) * int(nxyz[2])
+    out = np.empty((n, 3), np.float32)
+    nx = np.asarray(nxyz, np.int32)
+    org = np.asarray(origin, np.float64)
+    rc = lib().psb_lattice(_ptr(nx), float(spacing), _ptr(org), float(jitter), int(seed) & (2**64 - 1), int(id0),
+                           _ptr(out))
+    if rc != OK:
+        raise PsbError(rc, "psb_lattice")
+    return out
+
+
+def scene_positions(scene: Scene) -> np.ndarray:
+    return np.concatenate([lattice(b.nxyz, b.spacing, b.origin, b.jitter, b.seed, b.id0) for b in scene.blocks])
+
+
+class Simulation:
+    """One psb_ctx: a scene's particles resident in HBM, stepped on a stream."""
+
+    def __init__(self, scene: Scene):
+        self.scene = scene
+        self._c = scene.to_c()
+        h = ctypes.c_void_p()
+        rc = lib().psb_create(ctypes.byref(self._c), ctypes.byref(h))
+        if rc != OK:
+            raise PsbError(rc, f"psb_create: {lib().psb_status_string(rc).decode()}")
+        self._h = h
+        self.n = 0
+
+    # -- lifecycle ------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().psb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int, what: str, allow=(OK,)):
+        if rc not in allow:
+            msg = lib().psb_last_error(self._h)
+            raise PsbError(rc, f"{what}: {lib().psb_status_string(rc).decode()}: {msg.decode() if msg else ''}")
+        return rc
+
+    # -- calls ----------------------------------------------------------------
+    def set_stream(self, stream_ptr: int):
+        self._check(lib().psb_set_stream(self._h, ctypes.c_void_p(stream_ptr)), "psb_set_stream")
+
+    def upload(self, pos, vel=None, vel_half=None, pressure=None):
+        pos = np.ascontiguousarray(pos, np.float32)
+        n = pos.shape[0]
+        cv = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+        vel, vel_half, pressure = cv(vel), cv(vel_half), cv(pressure)
+        self._check(lib().psb_upload(self._h, n, _ptr(pos), _ptr(vel), _ptr(vel_half), _ptr(pressure)), "psb_upload")
+        self.n = n
+
+    def upload_aos_f64(self, pos, vel=None, vel_half=None, on_device=False):
+        if on_device:
+            p = lambda a: None if a is None else ctypes.c_void_p(int(a))
+            rc = lib().psb_upload_aos_f64(self._h, self.scene.n if self.n == 0 else self.n, p(pos), p(vel), p(vel_half), 1)
+            self._check(rc, "psb_upload_aos_f64")
+            return
+        pos = np.ascontiguousarray(pos, np.float64)
+        cv = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
+        vel, vel_half = cv(vel), cv(vel_half)
+        self._check(lib().psb_upload_aos_f64(self._h, pos.shape[0], _ptr(pos), _ptr(vel), _ptr(vel_half), 0),
+                    "psb_upload_aos_f64")
+        self.n = pos.shape[0]
+
+    def step(self, nsteps: int = 1, allow_noconv: bool = True) -> int:
+        allow = (OK, ENOCONV) if allow_noconv else (OK,)
+        return self._check(lib().psb_step(self._h, int(nsteps)), "psb_step", allow)
+
+    def build_neighbors(self):
+        self._check(lib().psb_build_neighbors(self._h), "psb_build_neighbors")
+
+    def download(self, out: Optional[dict] = None) -> dict:
+        n = self.n
+        o = out if out is not None else {
+            "pos": np.empty((n, 3), np.float32), "vel": np.empty((n, 3), np.float32),
+            "vel_half": np.empty((n, 3), np.float32), "density": np.empty(n, np.float32),
+            "pressure": np.empty(n, np.float32)}
+        self._check(lib().psb_download(self._h, _ptr(o.get("pos")), _ptr(o.get("vel")), _ptr(o.get("vel_half")),
+                                       _ptr(o.get("density")), _ptr(o.get("pressure"))), "psb_download")
+        return o
+
+    def download_aos_f64(self) -> dict:
+        n = self.n
+        o = {k: np.empty((n, 3), np.float64) for k in ("pos", "vel", "vel_half")}
+        self._check(lib().psb_download_aos_f64(self._h, _ptr(o["pos"]), _ptr(o["vel"]), _ptr(o["vel_half"]), 0),
+                    "psb_download_aos_f64")
+        return o
+
+    def read_field(self, field: int) -> np.ndarray:
+        dt, w = _FIELD_SPEC[field]
+        out = np.empty((self.n, w) if w > 1 else self.n, dt)
+        self._check(lib().psb_read_field(self._h, field, _ptr(out), out.nbytes), "psb_read_field")
+        return out
+
+    def stats(self) -> PsbStepStats:
+        s = PsbStepStats()
+        self._check(lib().psb_get_stats(self._h, ctypes.byref(s)), "psb_get_stats")
+        return s
+
+    def profile(self, on: bool = True):
+        self._check(lib().psb_profile_enable(self._h, 1 if on else 0), "psb_profile_enable")
+
+    def profile_reset(self):
+        self._check(lib().psb_profile_reset(self._h), "psb_profile_reset")
+
+    def profile_read(self) -> Dict[str, Tuple[int, float]]:
+        res = {}
+        i = 0
+        buf = ctypes.create_string_buffer(64)
+        while True:
+            la = ctypes.c_int64()
+            ms = ctypes.c_double()
+            if lib().psb_profile_read(self._h, i, buf, 64, ctypes.byref(la), ctypes.byref(ms)) != OK:
+                break
+            res[buf.value.decode()] = (la.value, ms.value)
+            i += 1
+        return res

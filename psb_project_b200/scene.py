@@ -1,0 +1,241 @@
+"""Scene description: the Python mirror of ``psb_scene`` (include/psb.h) and
+the synthetic dam-break scenes the benchmarks and tests run.
+
+The reference builds scenes interactively (Qt dialogs, EmitterBox lattices:
+src/Kernel/Emitters/EmitterBox.cpp:29-47, spacing 2*particleRadius) and
+keeps material parameters in per-particle arrays filled from
+SimulationData_SPHSystem (SimulationData_SPHSystem.cpp:5-16). Here a scene
+is one uniform parameter set plus one or more lattice blocks.
+
+Conventions fixed here (the scene text leaves them open):
+  * y is up and gravity is (0, -9.81, 0), as the reference's PCISPH
+    kernel hard-codes it (PciSphSystem_Kernel.cu:168);
+  * the box spans [0, L] on each axis and the lattice block sits in the
+    (0, 0, 0) corner, first particle at spacing/2 from the walls;
+  * the grid covers the box plus one cell on each side;
+  * the cell edge is h rounded up to the next float, so the 27-cell walk
+    sees every pair within h; reference-profile parity scenes instead use
+    float(h), exactly as PCI_SPHSystem::_initialize passes
+    getInteractionRadius() to createGrid (PciSphSystem.cpp:143);
+  * where the text gives no particle mass, the mass puts a filled lattice
+    exactly at rest density (lattice_mass); rho0 * spacing^3 would leave
+    it 0.98% over rest density at h = 2 spacing, a whole eta of 1%;
+  * penalty walls: wall_k = 0.5/dt^2, wall_c = sqrt(wall_k) (damping ratio 0.5);
+  * the particle (wall) radius is spacing/2.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+PROFILE_REF = 0
+PROFILE_CONFIG = 1
+WCSPH = 0
+PCISPH = 1
+WARM_ZERO = 0
+WARM_PREVIOUS = 1
+
+
+class PsbScene(ctypes.Structure):
+    """Binary layout of ``psb_scene`` (include/psb.h)."""
+
+    _fields_ = [
+        ("n_max", ctypes.c_int32),
+        ("box_min", ctypes.c_float * 3),
+        ("box_max", ctypes.c_float * 3),
+        ("grid_min", ctypes.c_float * 3),
+        ("cell", ctypes.c_float),
+        ("dims", ctypes.c_int32 * 3),
+        ("h", ctypes.c_double),
+        ("mass", ctypes.c_double),
+        ("rho0", ctypes.c_double),
+        ("k", ctypes.c_double),
+        ("mu", ctypes.c_double),
+        ("sigma", ctypes.c_double),
+        ("l", ctypes.c_double),
+        ("particle_radius", ctypes.c_float),
+        ("dt", ctypes.c_float),
+        ("gravity", ctypes.c_float * 3),
+        ("profile", ctypes.c_int32),
+        ("method", ctypes.c_int32),
+        ("min_iters", ctypes.c_int32),
+        ("max_iters", ctypes.c_int32),
+        ("eta", ctypes.c_double),
+        ("wall_k", ctypes.c_double),
+        ("wall_c", ctypes.c_double),
+        ("nbr_cap", ctypes.c_int32),
+        ("warm_start", ctypes.c_int32),
+        ("spacing", ctypes.c_double),
+    ]
+
+
+@dataclasses.dataclass
+class Block:
+    """A lattice block: counts per axis, spacing, corner, jitter, seed, first id."""
+
+    nxyz: Tuple[int, int, int]
+    spacing: float
+    origin: Tuple[float, float, float]
+    jitter: float
+    seed: int
+    id0: int = 0
+
+    @property
+    def n(self) -> int:
+        return self.nxyz[0] * self.nxyz[1] * self.nxyz[2]
+
+
+@dataclasses.dataclass
+class Scene:
+    n: int
+    box_min: Tuple[float, float, float]
+    box_max: Tuple[float, float, float]
+    grid_min: Tuple[float, float, float]
+    cell: float
+    dims: Tuple[int, int, int]
+    h: float
+    mass: float
+    rho0: float = 1000.0
+    k: float = 3.0
+    mu: float = 0.01
+    sigma: float = 0.0
+    l: float = 7.065
+    particle_radius: float = 0.005
+    dt: float = 1e-3
+    gravity: Tuple[float, float, float] = (0.0, -9.81, 0.0)
+    profile: int = PROFILE_CONFIG
+    method: int = PCISPH
+    min_iters: int = 3
+    max_iters: int = 50
+    eta: float = 0.01
+    wall_k: float = 0.0
+    wall_c: float = 0.0
+    nbr_cap: int = 128
+    warm_start: int = WARM_ZERO
+    spacing: float = 0.0
+    blocks: List[Block] = dataclasses.field(default_factory=list)
+    name: str = ""
+    steps: int = 0
+
+    def to_c(self) -> PsbScene:
+        s = PsbScene()
+        s.n_max = self.n
+        s.box_min[:] = [float(v) for v in self.box_min]
+        s.box_max[:] = [float(v) for v in self.box_max]
+        s.grid_min[:] = [float(v) for v in self.grid_min]
+        s.cell = self.cell
+        s.dims[:] = [int(v) for v in self.dims]
+        s.h, s.mass, s.rho0, s.k = self.h, self.mass, self.rho0, self.k
+        s.mu, s.sigma, s.l = self.mu, self.sigma, self.l
+        s.particle_radius, s.dt = self.particle_radius, self.dt
+        s.gravity[:] = [float(v) for v in self.gravity]
+        s.profile, s.method = self.profile, self.method
+        s.min_iters, s.max_iters, s.eta = self.min_iters, self.max_iters, self.eta
+        s.wall_k, s.wall_c = self.wall_k, self.wall_c
+        s.nbr_cap, s.warm_start = self.nbr_cap, self.warm_start
+        s.spacing = self.spacing
+        return s
+
+    def replace(self, **kw) -> "Scene":
+        return dataclasses.replace(self, **kw)
+
+
+def f32(x: float) -> float:
+    return float(np.float32(x))
+
+
+def cell_for(h: float, exact_reference: bool) -> float:
+    """float(h), or the smallest float >= h (see module docstring)."""
+    c = np.float32(h)
+    if not exact_reference and float(c) < h:
+        c = np.nextafter(c, np.float32(np.inf), dtype=np.float32)
+    return float(c)
+
+
+def grid_for(box_min, box_max, cell: float) -> Tuple[Tuple[float, ...], Tuple[int, ...]]:
+    """Grid corner one cell outside the box, cell counts covering box + 2 cells."""
+    gmin = tuple(f32(b - cell) for b in box_min)
+    dims = tuple(int(math.ceil((hi - lo) / cell)) + 2 for lo, hi in zip(box_min, box_max))
+    return gmin, dims
+
+
+def lattice_mass(rho0: float, spacing: float, h: float) -> float:
+    """Mass that gives a filled cubic lattice of this spacing exactly the rest
+    density under the poly6 kernel (self included)."""
+    R = int(math.ceil(h / spacing))
+    acc = 0.0
+    for k in range(-R, R + 1):
+        for j in range(-R, R + 1):
+            for i in range(-R, R + 1):
+                r2 = (i * i + j * j + k * k) * spacing * spacing
+                if r2 < h * h:
+                    acc += (h * h - r2) ** 3
+    return rho0 / (315.0 / (64.0 * math.pi * h ** 9) * acc)
+
+
+def dam_break(
+    nxyz: Sequence[int],
+    spacing: float,
+    box: Sequence[float],
+    h: float,
+    *,
+    method: int = PCISPH,
+    profile: int = PROFILE_CONFIG,
+    dt: float = 1e-3,
+    mass: Optional[float] = None,
+    rho0: float = 1000.0,
+    k: float = 3.0,
+    mu: float = 0.01,
+    eta: float = 0.01,
+    min_iters: int = 3,
+    max_iters: int = 50,
+    jitter: float = 1e-4,
+    seed: int = 0,
+    steps: int = 0,
+    name: str = "",
+    nbr_cap: int = 128,
+) -> Scene:
+    box_min = (0.0, 0.0, 0.0)
+    box_max = tuple(float(b) for b in box)
+    cell = cell_for(h, exact_reference=(profile == PROFILE_REF))
+    gmin, dims = grid_for(box_min, box_max, cell)
+    n = int(nxyz[0]) * int(nxyz[1]) * int(nxyz[2])
+    m = lattice_mass(rho0, spacing, h) if mass is None else mass
+    wk = 0.5 / (dt * dt)
+    return Scene(
+        n=n, box_min=box_min, box_max=box_max, grid_min=gmin, cell=cell, dims=dims, h=h, mass=m,
+        rho0=rho0, k=k, mu=mu, sigma=0.0 if profile == PROFILE_CONFIG else 0.0728, l=7.065,
+        particle_radius=f32(spacing / 2), dt=f32(dt), method=method, profile=profile,
+        min_iters=min_iters, max_iters=max_iters, eta=eta, wall_k=wk, wall_c=math.sqrt(wk),
+        blocks=[Block(tuple(int(v) for v in nxyz), spacing, (0.0, 0.0, 0.0), jitter, seed)],
+        name=name, steps=steps, nbr_cap=nbr_cap, spacing=spacing,
+    )
+
+
+# The synthetic scenes of the benchmark configurations (sizes from the scene text).
+def config_scene(name: str) -> Scene:
+    if name == "C0":   # plain WCSPH, 16,384 particles
+        return dam_break((32, 32, 16), 0.01, (1.0, 0.5, 0.5), 0.02, method=WCSPH, dt=5e-4, mass=1e-3,
+                         seed=0, steps=200, name="C0 WCSPH dam break 16,384")
+    if name == "C1":   # PCISPH, 262,144 fluid particles (DEM spheres are a separate set)
+        return dam_break((64, 64, 64), 0.01, (2.0, 1.0, 1.0), 0.02, dt=1e-3, mass=1e-3, seed=1, steps=500,
+                         name="C1 PCISPH dam break 262,144")
+    if name == "C2":   # PCISPH, 1,048,576 particles
+        return dam_break((128, 128, 64), 0.005, (4.0, 2.0, 1.0), 0.01, dt=1e-3, seed=2, steps=1000,
+                         name="C2 PCISPH dam break 1,048,576")
+    if name == "C4":   # large PCISPH, 4,194,304 particles (obstacle not included here)
+        return dam_break((256, 128, 128), 0.004, (3.0, 1.5, 1.0), 0.008, dt=5e-4, eta=0.005, seed=4, steps=300,
+                         name="C4 PCISPH dam break 4,194,304")
+    raise ValueError(f"unknown scene {name!r}")
+
+
+def ref_scene(nxyz=(12, 10, 8), spacing=0.01, box=(0.3, 0.3, 0.3), h=0.02, method=PCISPH, dt=5e-4,
+              seed=7, jitter=1e-4) -> Scene:
+    """Small scene in the reference-compatible profile (parity tests)."""
+    s = dam_break(nxyz, spacing, box, h, method=method, profile=PROFILE_REF, dt=dt, mass=1e-3, seed=seed,
+                  jitter=jitter, name="ref-profile scene")
+    return s

@@ -1,0 +1,93 @@
+"""C ABI checks that need no GPU: the library loads, exports every entry
+point include/psb.h declares, its structs have the layout the bindings use,
+and the host-side scene generator matches the oracle's bit for bit."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+import psb_project_b200 as P
+from psb_project_b200 import runtime as R
+from psb_project_b200.scene import PsbScene
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "psb.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:int|int32_t|const char\*)\s+(psb_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 15
+    L = R.lib()
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(R.EXPORTS)
+    out = subprocess.run(["nm", "-D", "--defined-only", R.LIB_PATH], capture_output=True, text=True).stdout
+    for n in names:
+        assert re.search(rf"\bT {n}\b", out), n
+
+
+def test_struct_layout_matches_header(tmp_path):
+    c = tmp_path / "layout.c"
+    c.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "psb.h"\n'
+                 'int main(void){printf("%zu %zu %zu %zu\\n", sizeof(psb_scene), offsetof(psb_scene, spacing),'
+                 ' sizeof(psb_step_stats), offsetof(psb_step_stats, iters_total)); return 0;}\n')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(c), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
+    assert got == [ctypes.sizeof(PsbScene), PsbScene.spacing.offset, ctypes.sizeof(R.PsbStepStats),
+                   R.PsbStepStats.iters_total.offset]
+
+
+def test_abi_version_and_status_strings():
+    L = R.lib()
+    assert L.psb_abi_version() == 1
+    assert L.psb_status_string(0) == b"ok"
+    assert L.psb_status_string(3) == b"neighbour list overflow"
+    assert L.psb_status_string(99) == b"unknown status"
+
+
+@pytest.mark.parametrize("name", ["C0", "C1", "C2"])
+def test_scene_generator_matches_oracle_bitwise(name):
+    sc = P.config_scene(name)
+    a = P.scene_positions(sc)
+    b = oracle.scene_positions(sc)
+    assert a.shape == (sc.n, 3)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    # inside the box, jitter within bounds
+    blk = sc.blocks[0]
+    ideal = np.stack(np.meshgrid(*[np.arange(k) for k in blk.nxyz], indexing="ij"), -1)
+    ideal = (ideal.transpose(2, 1, 0, 3).reshape(-1, 3) + 0.5) * blk.spacing
+    assert np.max(np.abs(a - ideal)) <= blk.jitter + float(np.spacing(np.float32(ideal.max())))
+
+
+def test_lattice_rejects_bad_arguments():
+    L = R.lib()
+    out = np.empty((8, 3), np.float32)
+    nx = np.array([2, 2, 0], np.int32)
+    org = np.zeros(3)
+    assert L.psb_lattice(nx.ctypes.data_as(ctypes.c_void_p), 0.01, org.ctypes.data_as(ctypes.c_void_p), 0.0, 0, 0,
+                         out.ctypes.data_as(ctypes.c_void_p)) == R.EINVAL
+
+
+def test_create_rejects_invalid_scene():
+    sc = P.config_scene("C0").replace(max_iters=1000)
+    with pytest.raises(R.PsbError) as e:
+        P.Simulation(sc)
+    assert e.value.status == R.EINVAL
+
+
+def test_library_fails_loudly_when_missing(monkeypatch):
+    monkeypatch.setattr(R, "_lib", None)
+    monkeypatch.setattr(R, "LIB_PATH", "/nonexistent/libpsb.so")
+    with pytest.raises(ImportError):
+        R.lib()

@@ -1,0 +1,252 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Tolerances (written here, applied below):
+  * cell keys, sorted order (stable on particle id) and neighbour counts:
+    bit-exact;
+  * density: 1e-5 relative, element-wise;
+  * pressure, forces, velocities: 1e-5 relative to the field's max
+    magnitude (FP32 arithmetic against FP64; PCISPH pressure increments
+    come from rho* - rho0, a cancellation, so a norm-wise bound is the
+    meaningful one);
+  * positions: within 4 float ulps of the coordinate magnitude plus 1e-5 of
+    the step's displacement.
+The oracle runs with float_state=True (it rounds every array the GPU stores
+in FP32 at the same points) for multi-step comparisons.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import psb_project_b200 as P
+from psb_project_b200 import runtime as R
+from psb_project_b200.scene import PCISPH, PROFILE_CONFIG, PROFILE_REF, WCSPH
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def rel_norm(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def assert_positions(x_gpu, x_orc, x0):
+    ulp = np.spacing(np.float32(np.max(np.abs(x_orc))))
+    disp = np.max(np.abs(x_orc - x0))
+    err = np.max(np.abs(np.asarray(x_gpu, np.float64) - x_orc))
+    assert err <= 4 * float(ulp) + TOL * disp, (err, ulp, disp)
+
+
+def small_config_scene(method=PCISPH, nxyz=(24, 20, 16), spacing=0.005, h=0.01, box=(0.5, 0.4, 0.3), dt=1e-3, seed=11):
+    return P.dam_break(nxyz, spacing, box, h, method=method, dt=dt, seed=seed)
+
+
+def upload(sc, pos=None):
+    sim = P.Simulation(sc)
+    pos = P.scene_positions(sc) if pos is None else pos
+    sim.upload(pos)
+    return sim, pos
+
+
+# ---- grid: keys, sort, neighbours ------------------------------------------
+
+@pytest.mark.parametrize("name", ["C0", "ref"])
+def test_keys_sort_neighbours_bit_exact(name):
+    sc = P.config_scene("C0") if name == "C0" else P.ref_scene()
+    sim, pos = upload(sc)
+    sim.build_neighbors()
+    pos64 = pos.astype(np.float64)
+    keys = oracle.cell_keys(sc, pos64)
+    perm = oracle.sort_perm(keys)
+    counts, _ = oracle.neighbors(sc, pos64, with_lists=False)
+    assert np.array_equal(sim.read_field(R.FIELD_CELL_KEY), keys)
+    assert np.array_equal(sim.read_field(R.FIELD_SORTED_ID), perm)
+    assert np.array_equal(sim.read_field(R.FIELD_SORTED_KEY), keys[perm])
+    assert np.array_equal(sim.read_field(R.FIELD_NBR_COUNT), counts)
+    st = sim.stats()
+    assert st.nbr_max == counts.max() and st.nbr_total == counts.sum()
+    sim.close()
+
+
+def test_neighbour_cutoff_borderline_pairs():
+    """Pairs at float-rounded distances h*(1 +- k ulp): the FP32 guard band
+    must hand them to the FP64 test and agree with the reference's
+    sqrt(d.d) <= h on every one."""
+    sc = P.ref_scene()
+    rng = np.random.default_rng(5)
+    base = rng.uniform(0.05, 0.25, size=(400, 3))
+    d = rng.normal(size=(400, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    scale = sc.h * (1.0 + rng.integers(-8, 9, size=(400, 1)) * 1e-8)
+    pos = np.concatenate([base, base + d * scale]).astype(np.float32)
+    sc = sc.replace(n=pos.shape[0])
+    sim, _ = upload(sc, pos)
+    sim.build_neighbors()
+    counts, _ = oracle.neighbors(sc, pos.astype(np.float64), with_lists=False)
+    assert np.array_equal(sim.read_field(R.FIELD_NBR_COUNT), counts)
+    ref = oracle.RefSim(sc, pos.astype(np.float64)) if oracle.ref_available() else None
+    if ref is not None:
+        assert np.array_equal(ref.search(), counts)
+    sim.close()
+
+
+def test_particles_outside_grid_are_clamped():
+    sc = P.ref_scene()
+    pos = P.scene_positions(sc)
+    pos[:7] = np.array([[-5.0, 0.1, 0.1], [0.1, 9.0, 0.1], [0.1, 0.1, -1.0], [3, 3, 3], [np.inf, 0, 0],
+                        [0.1, -np.inf, 0.1], [0.1, 0.1, 1e30]], np.float32)
+    sim, _ = upload(sc, pos)
+    sim.build_neighbors()
+    assert sim.stats().clamped == 7
+    keys = oracle.cell_keys(sc, pos.astype(np.float64))
+    assert np.array_equal(sim.read_field(R.FIELD_CELL_KEY), keys)
+    sim.close()
+
+
+# ---- density and single steps --------------------------------------------------
+
+@pytest.mark.parametrize("profile", [PROFILE_REF, PROFILE_CONFIG])
+def test_density_at_start_positions(profile):
+    sc = P.ref_scene() if profile == PROFILE_REF else small_config_scene()
+    sim, pos = upload(sc)
+    sim.build_neighbors()
+    counts, lists = oracle.neighbors(sc, pos.astype(np.float64))
+    rho = oracle.density(sc, pos.astype(np.float64), counts, lists, clamp=(profile == PROFILE_CONFIG))
+    got = sim.read_field(R.FIELD_DENSITY_X).astype(np.float64)
+    assert np.max(np.abs(got - rho) / rho) <= TOL
+    sim.close()
+
+
+def _compare_step(sim, orc, x0):
+    out = sim.download()
+    assert_positions(out["pos"], orc.pos, x0)
+    assert rel_norm(out["vel_half"], orc.vel_half) <= TOL
+    assert rel_norm(out["vel"], orc.vel) <= TOL
+    assert np.max(np.abs(out["density"] - orc.rho) / np.abs(orc.rho)) <= TOL
+    assert rel_norm(out["pressure"], orc.p) <= TOL
+    assert rel_norm(sim.read_field(R.FIELD_FORCE_NP), orc.f_np) <= TOL
+    assert np.array_equal(sim.read_field(R.FIELD_NBR_COUNT), orc.nbr)
+
+
+@pytest.mark.parametrize("method", [PCISPH, WCSPH])
+def test_reference_profile_steps(method):
+    """Reference-compatible physics, 3 steps, against the FP64 oracle (float
+    state) and, where built, the reference's own kernels."""
+    sc = P.ref_scene(method=method)
+    sim, pos = upload(sc)
+    orc = oracle.OracleSim(sc, pos, float_state=True)
+    ref = oracle.RefSim(sc, pos.astype(np.float64)) if oracle.ref_available() else None
+    for _ in range(3):
+        x0 = orc.pos.copy()
+        sim.step(1)
+        orc.step()
+        _compare_step(sim, orc, x0)
+        if ref is not None:
+            (ref.pcisph_update() if method == PCISPH else ref.wcsph_update())
+            out = sim.download()
+            assert rel_norm(out["vel_half"], ref.get("vel_ap", 3)) <= TOL
+            assert np.max(np.abs(out["density"] - ref.get("density", 1)) / ref.get("density", 1)) <= TOL
+            assert rel_norm(out["pressure"], ref.get("pressure", 1)) <= TOL
+    if method == PCISPH:
+        assert sim.stats().iters == 3
+    sim.close()
+
+
+def test_config_pcisph_steps_and_iterations():
+    sc = small_config_scene()
+    sim, pos = upload(sc)
+    orc = oracle.OracleSim(sc, pos, float_state=True)
+    for _ in range(4):
+        x0 = orc.pos.copy()
+        sim.step(1)
+        so = orc.step()
+        sg = sim.stats()
+        assert sg.iters == so.iters
+        assert sg.converged == so.converged
+        for k in range(so.iters + 1):
+            assert abs(sg.err[k] - so.err[k]) <= 1e-5, (k, sg.err[k], so.err[k])
+        _compare_step(sim, orc, x0)
+    sim.close()
+
+
+def test_config_wcsph_steps():
+    sc = P.config_scene("C0")
+    sim, pos = upload(sc)
+    orc = oracle.OracleSim(sc, pos, float_state=True)
+    for _ in range(3):
+        x0 = orc.pos.copy()
+        sim.step(1)
+        orc.step()
+        _compare_step(sim, orc, x0)
+    sim.close()
+
+
+def test_trajectory_50_steps_wcsph():
+    """50 steps of the 16,384-particle WCSPH dam break: the trajectory stays
+    on the FP64 oracle's to 1e-4 of the travelled distance."""
+    sc = P.config_scene("C0")
+    sim, pos = upload(sc)
+    orc = oracle.OracleSim(sc, pos, float_state=False)
+    sim.step(50)
+    for _ in range(50):
+        orc.step()
+    out = sim.download()
+    travel = np.max(np.abs(orc.pos - pos))
+    err = np.max(np.abs(out["pos"] - orc.pos))
+    assert err <= 1e-4 * travel + 4 * float(np.spacing(np.float32(1.0))), (err, travel)
+    assert rel_norm(out["vel"], orc.vel) <= 1e-4
+    sim.close()
+
+
+# ---- behaviour ----------------------------------------------------------------
+
+def test_deterministic_bitwise():
+    sc = small_config_scene()
+    res = []
+    for _ in range(2):
+        sim, _ = upload(sc)
+        sim.step(3)
+        out = sim.download()
+        res.append(out)
+        sim.close()
+    for k in res[0]:
+        assert np.array_equal(res[0][k].view(np.uint32), res[1][k].view(np.uint32)), k
+
+
+def test_neighbour_overflow_is_a_status():
+    sc = small_config_scene().replace(nbr_cap=8)
+    sim, _ = upload(sc)
+    with pytest.raises(R.PsbError) as e:
+        sim.step(1)
+    assert e.value.status == R.EOVERFLOW_NBR
+    sim.close()
+
+
+def test_aos_f64_roundtrip():
+    sc = P.ref_scene()
+    pos = P.scene_positions(sc).astype(np.float64) + 1e-9
+    vel = np.random.default_rng(1).normal(size=pos.shape)
+    sim = P.Simulation(sc)
+    sim.upload_aos_f64(pos, vel, vel)
+    out = sim.download_aos_f64()
+    assert np.array_equal(out["pos"], pos.astype(np.float32).astype(np.float64))
+    assert np.array_equal(out["vel"], vel.astype(np.float32).astype(np.float64))
+    sim.close()
+
+
+def test_noconvergence_reports_status():
+    sc = small_config_scene().replace(eta=1e-9, max_iters=4)
+    sim, _ = upload(sc)
+    assert sim.step(1) == R.ENOCONV
+    st = sim.stats()
+    assert st.iters == 4 and st.converged == 0
+    sim.close()
+
+
+def test_bad_scene_rejected():
+    sc = small_config_scene().replace(max_iters=1000)
+    with pytest.raises(R.PsbError) as e:
+        P.Simulation(sc)
+    assert e.value.status == R.EINVAL
