@@ -9,7 +9,12 @@ Tolerances (written here, applied below):
     come from rho* - rho0, a cancellation, so a norm-wise bound is the
     meaningful one);
   * positions: within 4 float ulps of the coordinate magnitude plus 1e-5 of
-    the step's displacement.
+    the step's displacement;
+  * pressure after a multi-iteration config-profile PCISPH step: 1e-4 of its
+    max. The pressure accumulates delta (rho* - rho0) over the corrections;
+    an FP32 rounding of 3e-8 of a density-level term (kernel constant, wall
+    term) is 3e-5 kg/m^3 of rho* - rho0, times delta ~ 34 and 4-5
+    corrections: ~4e-5 of the pressure scale.
 The oracle runs with float_state=True (it rounds every array the GPU stores
 in FP32 at the same points) for multi-step comparisons.
 """
@@ -24,6 +29,7 @@ from psb_project_b200.scene import PCISPH, PROFILE_CONFIG, PROFILE_REF, WCSPH
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-5
+TOL_P_CONFIG_PCI = 1e-4
 
 
 def rel_norm(a, b):
@@ -119,13 +125,13 @@ def test_density_at_start_positions(profile):
     sim.close()
 
 
-def _compare_step(sim, orc, x0):
+def _compare_step(sim, orc, x0, p_tol=TOL):
     out = sim.download()
     assert_positions(out["pos"], orc.pos, x0)
     assert rel_norm(out["vel_half"], orc.vel_half) <= TOL
     assert rel_norm(out["vel"], orc.vel) <= TOL
     assert np.max(np.abs(out["density"] - orc.rho) / np.abs(orc.rho)) <= TOL
-    assert rel_norm(out["pressure"], orc.p) <= TOL
+    assert rel_norm(out["pressure"], orc.p) <= p_tol
     assert rel_norm(sim.read_field(R.FIELD_FORCE_NP), orc.f_np) <= TOL
     assert np.array_equal(sim.read_field(R.FIELD_NBR_COUNT), orc.nbr)
 
@@ -167,7 +173,7 @@ def test_config_pcisph_steps_and_iterations():
         assert sg.converged == so.converged
         for k in range(so.iters + 1):
             assert abs(sg.err[k] - so.err[k]) <= 1e-5, (k, sg.err[k], so.err[k])
-        _compare_step(sim, orc, x0)
+        _compare_step(sim, orc, x0, p_tol=TOL_P_CONFIG_PCI)
     sim.close()
 
 
