@@ -157,6 +157,27 @@ int psb_profile_reset(psb_ctx* ctx);
 int psb_lattice(const int32_t nxyz[3], double spacing, const double origin[3], double jitter, uint64_t seed,
                 int32_t id0, float* pos);
 
+/* Allocation-free sort. No counterpart in the reference: its launchers take
+ * buffers the caller allocated up front and keep no scratch.
+ *
+ * Sorts n (key, value) pairs of device memory stably by key (the same LSD
+ * radix sort psb_step uses for (cell, id) ordering), reading keys_in/vals_in
+ * and writing keys_out/vals_out; key_bits (1..32) bounds the keys. For
+ * callers that cannot allocate device memory -- hosts that give the whole
+ * GPU to their own memory pool and forbid libraries from allocating, and
+ * per-frame loops that must not stall on cudaMalloc/cudaFree, which can
+ * synchronise the device -- it calls no allocator: its scratch is a static
+ * device array inside libpsb, held by every GPU that loads the library
+ * (about 2.1 MB) until the process exits.
+ * Limit: n <= PSB_NOALLOC_MAX_N; larger n returns PSB_EINVAL (with a message
+ * on stderr). The first call on each device looks up the array's device
+ * address, so make that first call before any stream capture begins. All
+ * calls share the one array: calls that overlap on the GPU (other streams or
+ * threads on the same device) race and corrupt each other's results. */
+#define PSB_NOALLOC_MAX_N 262144
+int psb_sort_cells_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                           uint32_t* vals_out, int32_t n, int32_t key_bits, void* stream);
+
 const char* psb_status_string(int32_t status);
 const char* psb_last_error(const psb_ctx* ctx);
 int32_t psb_abi_version(void);

@@ -35,8 +35,9 @@ EXPORTS = (
     "psb_create", "psb_destroy", "psb_set_stream", "psb_upload", "psb_upload_aos_f64", "psb_download",
     "psb_download_aos_f64", "psb_step", "psb_build_neighbors", "psb_read_field", "psb_get_stats",
     "psb_profile_enable", "psb_profile_read", "psb_profile_reset", "psb_lattice", "psb_status_string",
-    "psb_last_error", "psb_abi_version",
+    "psb_last_error", "psb_abi_version", "psb_sort_cells_noalloc",
 )
+NOALLOC_MAX_N = 262144   # PSB_NOALLOC_MAX_N
 
 
 class PsbStepStats(ctypes.Structure):
@@ -85,6 +86,7 @@ def lib():
         "psb_status_string": ([I32], ctypes.c_char_p),
         "psb_last_error": ([P], ctypes.c_char_p),
         "psb_abi_version": ([], I32),
+        "psb_sort_cells_noalloc": ([P, P, P, P, I32, I32, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
