@@ -68,11 +68,11 @@ def _kernels_per_group(name: str, sort_passes: int) -> int:
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scene", default="C2")
-    ap.add_argument("--warm-start", choices=["zero", "previous"], default="zero")
+    ap.add_argument("--warm-start", choices=["zero", "previous"], default="previous")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
     return ap.parse_args()
@@ -173,21 +173,20 @@ def ncu_traffic():
         return {}
 
 
-def cpu_baseline_port(scene_name: str, steps: int) -> dict:
+def cpu_baseline_port(sc, snap, steps: int) -> dict:
     """The FP64 oracle (a C port of the same method, OpenMP on every host
-    core) on a bounded sample: `steps` steps of the same scene."""
+    core) on a bounded sample: `steps` steps of the same scene from the same
+    state the GPU's timed steps start from."""
     import oracle
-    import psb_project_b200 as P
-    sc = P.config_scene(scene_name)
-    pos = oracle.scene_positions(sc)
-    sim = oracle.OracleSim(sc, pos)
+    sim = oracle.OracleSim(sc, snap["pos"], snap["vel"], snap["vel_half"], snap["pressure"])
     t0 = time.perf_counter()
+    iters = []
     for _ in range(steps):
-        sim.step()
+        iters.append(sim.step().iters)
     dt = time.perf_counter() - t0
     return {"value": sc.n * steps / dt, "unit": UNIT, "cores": host_cores(), "kind": "port",
-            "sample": f"{steps} step(s) of the {sc.n:,}-particle scene from rest, FP64 oracle, "
-                      f"{host_cores()} threads on {cpu_model()}"}
+            "sample": f"{steps} step(s) of the {sc.n:,}-particle scene from the GPU's timed start state "
+                      f"({sum(iters)} corrections), FP64 oracle, {host_cores()} threads on {cpu_model()}"}
 
 
 def run_reference(args):
@@ -230,7 +229,6 @@ def run_reference(args):
 def run_ours(args):
     import torch
     import psb_project_b200 as P
-    from psb_project_b200 import runtime as R
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -241,52 +239,101 @@ def run_ours(args):
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
-    sc = P.config_scene(args.scene)
-    if args.warm_start == "previous":
-        sc = sc.replace(warm_start=P.WARM_PREVIOUS)
+    modes = {"zero": P.WARM_ZERO, "previous": P.WARM_PREVIOUS}
+    base = P.config_scene(args.scene)
     if world > 1:       # replicas: same scene, own seed per rank
-        sc.blocks[0].seed = sc.blocks[0].seed + 1000 * rank
+        base.blocks[0].seed = base.blocks[0].seed + 1000 * rank
+    sc = base.replace(warm_start=modes[args.warm_start])
     n = sc.n
-    pos0 = P.scene_positions(sc)
     stream = torch.cuda.current_stream()
-    sim = P.Simulation(sc)
-    sim.set_stream(stream.cuda_stream)
-    sim.upload(pos0)
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- device-resident timing -------------------------------------------------
+    def max_over_ranks(ms):
+        t = torch.tensor([ms], device="cuda")
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # Warm-up from rest, then a snapshot every timed pass restarts from, so
+    # that all passes time the same K steps.
+    sim = P.Simulation(sc)
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(P.scene_positions(sc))
     sim.step(args.warmup)
-    iters0 = sim.stats().iters_total
+    snap = sim.download()
     barrier()
+
+    def restore(s):
+        s.upload(snap["pos"], snap["vel"], snap["vel_half"], snap["pressure"])
+
+    def device_pass(s, profile=False):
+        restore(s)
+        if profile:
+            s.profile(True)
+            s.profile_reset()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        iters = []
+        e0.record(stream)
+        for _ in range(args.steps):
+            s.step(1)
+            iters.append(s.stats().iters)
+        e1.record(stream)
+        barrier()
+        prof = None
+        if profile:
+            prof = s.profile_read()
+            s.profile(False)
+        return max_over_ranks(e0.elapsed_time(e1)), iters, prof
+
     clocks = ClockSampler(local)
     clocks.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    iters = []
-    e0.record(stream)
-    for _ in range(args.steps):
-        sim.step(1)
-        iters.append(sim.stats().iters)
-    e1.record(stream)
-    barrier()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    time.sleep(0.3)
+    # ---- device-resident timing -------------------------------------------------
+    ms_max, iters, _ = device_pass(sim)
     value = world * n * args.steps / (ms_max / 1e3)
+    # ---- per-kernel timing: the same K steps with CUDA events around every launch ----
+    _, _, prof = device_pass(sim, profile=True)
+    # ---- end to end through the C ABI with host buffers ------------------------------
+    pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+    h = {"pos": pin((n, 3)), "vel": pin((n, 3)), "vel_half": pin((n, 3)), "density": pin((n,)), "pressure": pin((n,))}
+    for k in ("pos", "vel", "vel_half", "pressure"):
+        h[k][:] = snap[k]
+    warm = sc.warm_start != P.WARM_ZERO
+    barrier()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        sim.upload(h["pos"], h["vel"], h["vel_half"], h["pressure"] if warm else None)
+        sim.step(1)
+        sim.download(h if warm else {k: h[k] for k in ("pos", "vel", "vel_half", "density")})
+    e3.record(stream)
+    barrier()
+    e2e_value = world * n * args.steps / (max_over_ranks(e2.elapsed_time(e3)) / 1e3)
+    h2d = n * (36 + (4 if warm else 0))
+    d2h = n * (40 + (4 if warm else 0))
+    clk = clocks.stop()
+    # ---- plain PCISPH (pressure from zero every step) over the same steps ------------
+    comparison = {}
+    if sc.warm_start != P.WARM_ZERO:
+        plain = P.Simulation(base.replace(warm_start=P.WARM_ZERO))
+        plain.set_stream(stream.cuda_stream)
+        ms_plain, iters_plain, _ = device_pass(plain)
+        plain.close()
+        comparison["plain"] = {"iters_mean": float(np.mean(iters_plain)), "iters_max": int(np.max(iters_plain)),
+                               "ms_per_step": ms_plain / args.steps,
+                               "value": world * n * args.steps / (ms_plain / 1e3),
+                               "not_converged_steps": int(np.sum(np.asarray(iters_plain) >= sc.max_iters))}
+        comparison["iters_ratio_plain_over_this"] = float(np.mean(iters_plain) / max(np.mean(iters), 1e-9))
+        comparison["time_ratio_plain_over_this"] = float(ms_plain / ms_max)
+    sim.close()
 
-    # ---- per-kernel timing: the next K steps with CUDA events around every launch ----
-    sim.profile(True)
-    sim.profile_reset()
-    sim.step(args.steps)
-    prof = sim.profile_read()
-    sim.profile(False)
     passes = (max(1, int(np.ceil(np.log2(np.prod(sc.dims))))) + 7) // 8
     launches = int(sum(l * _kernels_per_group(k, passes) for k, (l, _) in prof.items()))
     tot_ms = sum(v[1] for v in prof.values())
@@ -298,33 +345,10 @@ def run_ours(args):
     traffic = ncu_traffic().get(dom)
     kernels = {k: {"launches": l, "ms": round(v, 3), "share": round(v / tot_ms, 4)} for k, (l, v) in prof.items()}
 
-    # ---- end to end through the C ABI with host buffers ------------------------------
-    pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
-    h_pos, h_vel, h_vh, h_rho = pin((n, 3)), pin((n, 3)), pin((n, 3)), pin((n,))
-    sim.download({"pos": h_pos, "vel": h_vel, "vel_half": h_vh, "density": h_rho})
-    barrier()
-    e2 = torch.cuda.Event(enable_timing=True)
-    e3 = torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(args.steps):
-        sim.upload(h_pos, h_vel, h_vh)
-        sim.step(1)
-        sim.download({"pos": h_pos, "vel": h_vel, "vel_half": h_vh, "density": h_rho})
-    e3.record(stream)
-    barrier()
-    ms_e2e = e2.elapsed_time(e3)
-    t = torch.tensor([ms_e2e], device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * n * args.steps / (float(t.item()) / 1e3)
-    launches_e2e_note = None
-    st = sim.stats()
-    sim.close()
-
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline_port(args.scene, args.cpu_sample_steps)
+            cpu = cpu_baseline_port(sc, snap, args.cpu_sample_steps)
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": host_cores(), "kind": "port", "sample": f"failed: {ex}"}
 
@@ -336,19 +360,20 @@ def run_ours(args):
             "config": {"workload": sc.name, "particles": n, "eta": sc.eta, "min_iters": sc.min_iters,
                        "max_iters": sc.max_iters, "warm_start": args.warm_start, "dt": sc.dt, "h": sc.h,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "working set > L2 (state, lists and scratch ~%d MB per GPU)" % int(n * (3 * 16 * 2 + 8 * 2 + 4 * 2 + 16 * 2 + 16 + 8 + 4 + 4 * sc.nbr_cap + 4) / 1e6),
-                       "from_rest_after_warmup_steps": args.warmup},
+                       "l2": "working set > L2 (state, lists and scratch ~%d MB per GPU)"
+                             % int(n * (3 * 16 * 2 + 8 * 2 + 4 * 2 + 16 * 4 + 8 + 4 + 4 * sc.nbr_cap + 4) / 1e6),
+                       "timed_steps": f"steps {args.warmup + 1}..{args.warmup + args.steps} of the dam break"},
             "iters_per_step": {"mean": float(np.mean(iters)), "p50": float(np.median(iters)),
                                "p95": float(np.percentile(iters, 95)), "max": int(np.max(iters)),
                                "min": int(np.min(iters))},
+            "comparison": comparison,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None if traffic is None else traffic * n,
                          "alg_bytes_per_particle": ALG_BYTES[dom], "mean_launch_us": per_launch_s * 1e6},
             "kernels": kernels,
             "gpu_launches": launches,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 12 * n,
-                    "d2h_bytes_per_step": 3 * 12 * n + 4 * n},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "clocks": clk,
             "cpu_baseline": cpu,
         }

@@ -132,6 +132,13 @@ int psb_download_aos_f64(psb_ctx* ctx, double* pos, double* vel, double* vel_hal
  * neighbours, the SPH/PCISPH step, walls, velocity interpolation. */
 int psb_step(psb_ctx* ctx, int32_t nsteps);
 
+/* Initial pressure for a CONFIG-profile PCISPH scene: `iters` corrector
+ * passes at the current state with eta = 0, keeping positions and
+ * velocities and only the pressure; with a warm start the following steps
+ * begin from it. The reference has no counterpart (it restarts every step
+ * from p = 0, PciSphSystem_Kernel.cu:131). stats.err[k] is pass k's error. */
+int psb_presolve(psb_ctx* ctx, int32_t iters);
+
 /* Replaces reinitCells + storeParticles + searchNeighbooring
  * (UniformGrid.cu:64-99, UniformGridKernel.cu:30-95): cell keys, stable
  * sort by (cell, id), cell ranges and neighbour lists at the current

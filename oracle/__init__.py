@@ -81,6 +81,9 @@ def lib():
         L.orc_density.restype = None
         L.orc_step.argtypes = [ctypes.POINTER(OrcParams), ctypes.POINTER(OrcState), ctypes.POINTER(OrcStats), P, P, P]
         L.orc_step.restype = ctypes.c_int
+        L.orc_presolve.argtypes = [ctypes.POINTER(OrcParams), ctypes.POINTER(OrcState), ctypes.c_int32,
+                                   ctypes.POINTER(OrcStats)]
+        L.orc_presolve.restype = ctypes.c_int
         L.orc_pci_delta.argtypes = [ctypes.POINTER(OrcParams)]
         L.orc_pci_delta.restype = ctypes.c_double
         _lib = L
@@ -214,6 +217,14 @@ class OracleSim:
         self.f_np = np.zeros((n, 3))
         self.nbr = np.zeros(n, np.int32)
         self.stats = OrcStats()
+
+    def presolve(self, iters):
+        S = OrcState(self.pos.ctypes.data, self.vel.ctypes.data, self.vel_half.ctypes.data,
+                     self.rho.ctypes.data, self.p.ctypes.data)
+        rc = lib().orc_presolve(ctypes.byref(self.P), ctypes.byref(S), int(iters), ctypes.byref(self.stats))
+        if rc != 0:
+            raise RuntimeError(f"orc_presolve failed: {rc}")
+        return self.stats
 
     def step(self):
         S = OrcState(self.pos.ctypes.data, self.vel.ctypes.data, self.vel_half.ctypes.data,

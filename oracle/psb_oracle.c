@@ -161,54 +161,39 @@ int64_t orc_neighbors(const orc_params* P, const double* pos, int32_t cap, int32
 static inline double len3(const double* v) { return sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
 static inline double dmax(double a, double b) { return a > b ? a : b; }
 
-/* ---- config-profile wall boundary ---------------------------------------
- * Each box face is backed by a half-space of virtual fluid particles on a
- * lattice of the rest spacing s, layers at (k + 1/2) s behind the face
- * (Harada, Koshizuka, Kawaguchi 2007: wall weight functions). Averaged over
- * the particle's position along the face, the layer sums have closed forms:
- *   density   sum (1 - r^2/h^2)^3          = pi h^2/(4 s^2) sum_k (1 - z_k^2/h^2)^4
- *   gradient  sum (1 - r/h)^2 (n . x^)      = 2 pi h/(3 s^2) sum_k z_k (1 - z_k/h)^3
- * with z_k = d + (k + 1/2) s the layer's distance and d >= 0 the particle's
- * distance to the face. The virtual particles carry the particle's own
- * pressure (mirror), so the wall pushes with 2 p_i/rho_i^2 times the
- * gradient sum along the face normal. */
-static double wall_spacing(const orc_params* P) { return P->spacing > 0 ? P->spacing : cbrt(P->mass / P->rho0); }
+/* ---- config-profile wall boundary: mirror ghost particles ---------------
+ * Every box face within h of a particle reflects the particle's neighbours:
+ * for each neighbour j and each non-empty set S of faces that both i and j
+ * lie within h of, the ghost x_j^S is x_j reflected across every face in S,
+ * with j's pressure and density (Libersky et al. 1993; Colagrossi &
+ * Landrini 2003). A ghost can only lie within h of i if j does (reflection
+ * moves a point away from the particles on the wall's own side), so i's
+ * neighbour list -- self included -- yields every ghost. At a flat wall the
+ * ghosts continue the fluid exactly: a uniform pressure exerts no net force
+ * and the rest lattice keeps its rest density up to the wall. */
+typedef struct { int n; int axis[3]; double plane[3]; } walls_t;
 
-static double wall_z(double d, double h, double s) {
-    if (d < 0) d = 0;
-    double z = 0;
-    for (int k = 0;; ++k) {
-        const double zk = d + (k + 0.5) * s;
-        if (zk >= h) break;
-        const double t = 1.0 - zk * zk / (h * h);
-        z += t * t * t * t;
-    }
-    return z * PI_D * h * h / (4.0 * s * s);
-}
-
-static double wall_g(double d, double h, double s) {
-    if (d < 0) d = 0;
-    double g = 0;
-    for (int k = 0;; ++k) {
-        const double zk = d + (k + 0.5) * s;
-        if (zk >= h) break;
-        const double t = 1.0 - zk / h;
-        g += zk * t * t * t;
-    }
-    return g * 2.0 * PI_D * h / (3.0 * s * s);
-}
-
-/* Sum over the six faces: density term (normalised) and gradient vector
- * (pointing into the box). */
-static void wall_terms(const orc_params* P, const double* x, double* z, double g[3]) {
-    const double h = P->h, s = wall_spacing(P);
-    *z = 0;
-    g[0] = g[1] = g[2] = 0;
+static void near_walls(const orc_params* P, const double* x, walls_t* w) {
+    const double h = P->h;
+    w->n = 0;
     for (int e = 0; e < 3; ++e) {
-        const double dl = x[e] - (double)P->box_min[e], dh = (double)P->box_max[e] - x[e];
-        if (dl < h) { *z += wall_z(dl, h, s); g[e] += wall_g(dl, h, s); }
-        if (dh < h) { *z += wall_z(dh, h, s); g[e] -= wall_g(dh, h, s); }
+        const double lo = (double)P->box_min[e], hi = (double)P->box_max[e];
+        if (x[e] - lo < h) { w->axis[w->n] = e; w->plane[w->n] = lo; w->n++; }
+        else if (hi - x[e] < h) { w->axis[w->n] = e; w->plane[w->n] = hi; w->n++; }
     }
+}
+
+/* Ghost of xj for face subset `mask` of w (bit k = face k), written to g;
+ * returns 0 when some face of the subset is h or more from xj. */
+static int ghost(const walls_t* w, int mask, const double* xj, double h, double* g) {
+    g[0] = xj[0]; g[1] = xj[1]; g[2] = xj[2];
+    for (int k = 0; k < w->n; ++k) {
+        if (!(mask >> k & 1)) continue;
+        const int e = w->axis[k];
+        if (fabs(xj[e] - w->plane[k]) >= h) return 0;
+        g[e] = 2.0 * w->plane[k] - xj[e];
+    }
+    return 1;
 }
 
 /* Poly6 density term; reference form of compute_Density_PCI (PciSphSystem_Kernel.cu:79-81). */
@@ -226,9 +211,18 @@ void orc_density(const orc_params* P, const double* pos, const int32_t* counts, 
             s += (315 / (64 * PI_D * pow(h, 9))) * pow((h * h) - (d * d), 3) * m;
         }
         if (clamp) {
-            double z, g[3];
-            wall_terms(P, &pos[3 * i], &z, g);
-            s += 315 * m / (64 * PI_D * h * h * h) * z;
+            walls_t w;
+            near_walls(P, &pos[3 * i], &w);
+            for (int mask = 1; mask < (1 << w.n); ++mask)
+                for (int32_t t = 0; t < counts[i]; ++t) {
+                    const int32_t j = list[(size_t)i * cap + t];
+                    double gx[3];
+                    if (!ghost(&w, mask, &pos[3 * j], h, gx)) continue;
+                    double dv[3] = {pos[3 * i] - gx[0], pos[3 * i + 1] - gx[1], pos[3 * i + 2] - gx[2]};
+                    const double d = len3(dv);
+                    if (d >= h) continue;
+                    s += (315 / (64 * PI_D * pow(h, 9))) * pow((h * h) - (d * d), 3) * m;
+                }
         }
         rho[i] = RND(P, s);
     }
@@ -294,10 +288,14 @@ static void pressure_forces(const orc_params* P, const double* pos, const double
                             const int32_t* counts, const int32_t* list, int32_t cap, double* fp) {
     const double h = P->h, m = P->mass;
     const int clamp = P->profile == ORC_PROFILE_CONFIG;
+    /* Config: p/rho0^2 (Solenthaler & Pajarola 2009 approximate rho by rho0
+     * in the pressure force, which keeps the corrector linear in p; with the
+     * predicted density there, the iteration diverges under tall columns). */
+    const double ir0 = 1.0 / (P->rho0 * P->rho0);
 #pragma omp parallel for schedule(static)
     for (int32_t i = 0; i < P->n; ++i) {
         double acc[3] = {0, 0, 0};
-        const double pV1 = p[i] / (rho[i] * rho[i]);
+        const double pV1 = clamp ? p[i] * ir0 : p[i] / (rho[i] * rho[i]);
         for (int32_t t = 0; t < counts[i]; ++t) {
             const int32_t j = list[(size_t)i * cap + t];
             const double dv[3] = {pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1], pos[3 * i + 2] - pos[3 * j + 2]};
@@ -305,17 +303,37 @@ static void pressure_forces(const orc_params* P, const double* pos, const double
             if (!(d > 0)) continue;
             if (clamp && d >= h) continue;
             const double inv = 1.0 / d;
-            const double pV2 = p[j] / (rho[j] * rho[j]);
+            const double pV2 = clamp ? p[j] * ir0 : p[j] / (rho[j] * rho[j]);
             const double a = PI_D * pow(h, 6);
             const double s = -45 * pow(h - d, 2) / a;
             for (int e = 0; e < 3; ++e) acc[e] = acc[e] + (dv[e] * inv) * s * (pV1 + pV2) * m;
         }
         if (clamp) {
-            /* -sum m (2 pV1) gradW over the virtual particles = +2 pV1 m G g */
-            double z, g[3];
-            wall_terms(P, &pos[3 * i], &z, g);
-            const double G = 45 / (PI_D * h * h * h * h);
-            for (int e = 0; e < 3; ++e) acc[e] -= 2 * pV1 * m * G * g[e];
+            walls_t w;
+            near_walls(P, &pos[3 * i], &w);
+            for (int mask = 1; mask < (1 << w.n); ++mask)
+                for (int32_t t = 0; t < counts[i]; ++t) {
+                    const int32_t j = list[(size_t)i * cap + t];
+                    double gx[3];
+                    if (!ghost(&w, mask, &pos[3 * j], h, gx)) continue;
+                    const double dv[3] = {pos[3 * i] - gx[0], pos[3 * i + 1] - gx[1], pos[3 * i + 2] - gx[2]};
+                    const double d = len3(dv);
+                    if (!(d > 0) || d >= h) continue;
+                    const double inv = 1.0 / d;
+                    /* the ghost continues the hydrostatic pressure across the
+                     * face: p_j + rho0 (-g . n) 2 d_j for each reflecting face */
+                    double pg = p[j];
+                    for (int k = 0; k < w.n; ++k) {
+                        if (!(mask >> k & 1)) continue;
+                        const int e = w.axis[k];
+                        const double nrm = (w.plane[k] == (double)P->box_min[e]) ? 1.0 : -1.0;
+                        pg += P->rho0 * (-(double)P->gravity[e] * nrm) * 2.0 * fabs(pos[3 * j + e] - w.plane[k]);
+                    }
+                    const double pV2 = pg * ir0;
+                    const double a = PI_D * pow(h, 6);
+                    const double sc = -45 * pow(h - d, 2) / a;
+                    for (int e = 0; e < 3; ++e) acc[e] = acc[e] + (dv[e] * inv) * sc * (pV1 + pV2) * m;
+                }
         }
         for (int e = 0; e < 3; ++e) fp[3 * i + e] = acc[e] * (-rho[i]);
     }
@@ -511,6 +529,7 @@ static int step_wcsph(const orc_params* P, orc_state* S, orc_stats* st, double* 
 }
 
 static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double* rho_x, double* f_np, int32_t* nbr_counts) {
+    if (st) memset(st, 0, sizeof(*st));
     const int32_t n = P->n;
     const int ref = P->profile == ORC_PROFILE_REF;
     int32_t* counts = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
@@ -563,7 +582,12 @@ static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double*
         free(rs);
         if (!ref && k >= min_it && err <= P->eta) { converged = 1; break; }
         pressure_update(P, xs, rho, counts, list, cap, p);
-        pressure_forces(P, xs, rho, p, counts, list, cap, fp);
+        /* reference: force at the predicted positions (PciSphSystem.cu:53-56);
+         * config: at the step's start positions, so that the corrector is a
+         * linear iteration in p (at x*, x* = x + dt^2 a(x*) is itself a
+         * fixed-point iteration that diverges once p dt^2/h^2 grows, as it
+         * does under a 0.64 m column) */
+        pressure_forces(P, ref ? xs : S->pos, rho, p, counts, list, cap, fp);
         k++;
     }
     /* commit the last prediction; walls; velocity interpolation (SphKernel.cu:128-135) */
@@ -585,6 +609,28 @@ static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double*
     if (st) { st->iters = k; st->converged = ref ? 1 : converged; }
     free(counts); free(list); free(rho); free(fnp); free(fp); free(xs); free(vs); free(aw);
     return 0;
+}
+
+int orc_presolve(const orc_params* P, orc_state* S, int32_t iters, orc_stats* st) {
+    /* The state is saved and restored around one warm-started step with
+     * exactly `iters` corrections; only the pressure is kept. */
+    orc_params Q = *P;
+    Q.min_iters = Q.max_iters = iters;
+    Q.eta = 0.0;
+    Q.warm_start = 1;
+    const size_t n3 = 3 * (size_t)P->n;
+    double* save = (double*)malloc(sizeof(double) * (3 * n3 + (size_t)P->n));
+    memcpy(save, S->pos, sizeof(double) * n3);
+    memcpy(save + n3, S->vel, sizeof(double) * n3);
+    memcpy(save + 2 * n3, S->vel_ap, sizeof(double) * n3);
+    memcpy(save + 3 * n3, S->rho, sizeof(double) * P->n);
+    const int rc = step_pcisph(&Q, S, st, NULL, NULL, NULL);
+    memcpy(S->pos, save, sizeof(double) * n3);
+    memcpy(S->vel, save + n3, sizeof(double) * n3);
+    memcpy(S->vel_ap, save + 2 * n3, sizeof(double) * n3);
+    memcpy(S->rho, save + 3 * n3, sizeof(double) * P->n);
+    free(save);
+    return rc;
 }
 
 int orc_step(const orc_params* P, orc_state* S, orc_stats* st, double* rho_x, double* f_np, int32_t* nbr_counts) {

@@ -190,7 +190,9 @@ int validate(const psb_scene* s, std::string& why) {
     if (s->warm_start != PSB_WARM_ZERO && s->warm_start != PSB_WARM_PREVIOUS) { why = "unknown warm_start"; return PSB_EINVAL; }
     {
         const double ws = s->spacing > 0 ? s->spacing : std::cbrt(s->mass / s->rho0);
-        if (!(ws >= s->h / 7.0)) { why = "spacing below h/7 (wall boundary layers)"; return PSB_EINVAL; }
+        if (!(ws > 0)) { why = "spacing must be positive"; return PSB_EINVAL; }
+        for (int a = 0; a < 3; ++a)
+            if (!((double)s->box_max[a] - s->box_min[a] > 2.0 * s->h)) { why = "box narrower than 2h"; return PSB_EINVAL; }
     }
     if ((double)s->n_max * (s->nbr_cap ? s->nbr_cap : 128) >= 9.0e18) { why = "list too large"; return PSB_EINVAL; }
     return PSB_OK;
@@ -264,9 +266,6 @@ Params derive(const psb_scene& s) {
         P.k_delta = (float)(1.0 / (beta * (W1[0] * W1[0] + W1[1] * W1[1] + W1[2] * W1[2] + W2)));
     }
     P.hf = (float)h;
-    P.ws = (float)ws;
-    P.cz = (float)(pi * h * h / (4.0 * ws * ws));
-    P.cg = (float)(2.0 * pi * h / (3.0 * ws * ws));
     return P;
 }
 
@@ -312,8 +311,9 @@ int bits_for(size_t ncells) {
     return b;
 }
 
-// Grid, sort, reorder, neighbour lists, density at x.
-int build(psb_ctx* c) {
+// Grid, sort, reorder, neighbour lists, density at x. keep_p: leave the
+// carried pressure in place even where the scene starts every step from 0.
+int build(psb_ctx* c, bool keep_p = false) {
     cudaStream_t st = c->stream;
     Params P = c->P;
     P.n = c->n;
@@ -340,7 +340,7 @@ int build(psb_ctx* c) {
         psb::launch_build_nbr(st, P, c->pos[c->cs], c->keys[res], c->cell_start, c->cell_end, c->nbr_count, c->nbr_list,
                               c->flags);
     });
-    const int zero_p = P.pci && (P.ref || c->sc.warm_start == PSB_WARM_ZERO);
+    const int zero_p = !keep_p && P.pci && (P.ref || c->sc.warm_start == PSB_WARM_ZERO);
     timed(c, "density_x", [&] {
         psb::launch_density_x(st, P, c->pos[c->cs], c->nbr_count, c->nbr_list, c->rp[c->cr], c->rho_x, zero_p);
     });
@@ -480,7 +480,7 @@ int psb_create(const psb_scene* scene, psb_ctx** out) {
         rc = dalloc(c, &c->vals[i], n); if (rc) break;
         rc = dalloc(c, &c->xs[i], n); if (rc) break;
     }
-    if (!rc) rc = dalloc(c, &c->hist, (size_t)256 * c->hist_blocks);
+    if (!rc) rc = dalloc(c, &c->hist, (size_t)256 * c->hist_blocks + 256);
     if (!rc) rc = dalloc(c, &c->cell_start, c->ncells);
     if (!rc) rc = dalloc(c, &c->cell_end, c->ncells);
     if (!rc) rc = dalloc(c, &c->nbr_count, n);
@@ -636,6 +636,41 @@ int psb_step(psb_ctx* c, int32_t nsteps) {
     }
     if (c->prof.on) c->prof.resolve(c->stream);
     return status;
+}
+
+int psb_presolve(psb_ctx* c, int32_t iters) {
+    if (!c || iters < 0) return fail(c, PSB_EINVAL, "psb_presolve: bad argument");
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_presolve before psb_upload");
+    if (!c->P.pci || c->P.ref) return fail(c, PSB_EINVAL, "psb_presolve: config-profile PCISPH scenes only");
+    cudaSetDevice(c->device);
+    PSB_TRY(build(c, /*keep_p=*/true));
+    cudaStream_t st = c->stream;
+    Params P = c->P;
+    P.n = c->n;
+    const int s = c->cs, r = c->cr;
+    cudaMemsetAsync(c->err_hist, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1), st);
+    timed(c, "pci_init", [&] {
+        psb::launch_pci_init(st, P, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list, 1, c->fnp,
+                             c->xs[0], c->vs);
+    });
+    int xi = 0;
+    for (int k = 0; k < iters; ++k) {
+        timed(c, "pci_density", [&] {
+            psb::launch_pci_density(st, P, c->xs[xi], c->rp[r], c->nbr_count, c->nbr_list, c->rpc,
+                                    &c->err_hist[k < PSB_MAX_ITERS ? k : PSB_MAX_ITERS]);
+        });
+        timed(c, "pci_force_predict", [&] {
+            psb::launch_pci_force_predict(st, P, c->pos[s], c->vap[s], c->fnp, c->xs[xi], c->rpc, c->nbr_count,
+                                          c->nbr_list, c->xs[xi ^ 1], c->vs, c->rp[r]);
+        });
+        xi ^= 1;
+    }
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->h_err, c->err_hist, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1),
+                                          cudaMemcpyDeviceToHost, st), "err"));
+    PSB_TRY(read_flags(c));
+    for (int i = 0; i <= PSB_MAX_ITERS; ++i) c->stats.err[i] = c->h_err[i] ? psb::unorder_double(c->h_err[i]) : 0.0;
+    c->stats.iters = iters;
+    return PSB_OK;
 }
 
 int psb_build_neighbors(psb_ctx* c) {

@@ -74,28 +74,49 @@ __global__ void k_radix_hist(int n, int shift, int nblocks, const uint32_t* __re
     hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of the digit-major histogram (256 * nblocks words), one block.
-__global__ void k_radix_scan(int total, uint32_t* __restrict__ hist) {
-    __shared__ uint32_t part[1024];
-    const int t = threadIdx.x;
-    const int per = (total + 1023) / 1024;
-    const int lo = t * per, hi = min(lo + per, total);
-    uint32_t s = 0;
-    for (int i = lo; i < hi; ++i) s += hist[i];
-    part[t] = s;
+// Block-wide exclusive scan of one value per thread (blockDim == 256).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s_warp, uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {            // Hillis-Steele inclusive scan
-        const uint32_t v = t >= off ? part[t - off] : 0u;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kBlock / 32 ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < kBlock / 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < kBlock / 32) s_warp[lane] = w;
     }
-    uint32_t run = part[t] - s;
-    for (int i = lo; i < hi; ++i) {
-        const uint32_t v = hist[i];
-        hist[i] = run;
-        run += v;
+    __syncthreads();
+    total = s_warp[kBlock / 32 - 1];
+    const uint32_t before = warp ? s_warp[warp - 1] : 0u;
+    __syncthreads();
+    return before + x - v;
+}
+
+// Per-digit exclusive scan of the tiles' counts: block d scans hist[d][0..nb)
+// in place and writes the digit's total.
+__global__ void __launch_bounds__(kBlock) k_radix_scan(int nb, uint32_t* __restrict__ hist,
+                                                       uint32_t* __restrict__ totals) {
+    __shared__ uint32_t s_warp[kBlock / 32];
+    uint32_t* h = hist + (size_t)blockIdx.x * nb;
+    uint32_t carry = 0;
+    for (int base = 0; base < nb; base += kBlock) {
+        const int i = base + threadIdx.x;
+        const uint32_t v = i < nb ? h[i] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan(v, s_warp, tot);
+        if (i < nb) h[i] = carry + ex;
+        carry += tot;
     }
+    if (threadIdx.x == 0) totals[blockIdx.x] = carry;
 }
 
 // Stable scatter. Tile items are ranked round by round (round r covers 256
@@ -106,11 +127,15 @@ __global__ void __launch_bounds__(kBlock) k_radix_scatter(int n, int shift, int 
                                                           const uint32_t* __restrict__ vals_in,
                                                           uint32_t* __restrict__ keys_out,
                                                           uint32_t* __restrict__ vals_out,
-                                                          const uint32_t* __restrict__ offsets) {
+                                                          const uint32_t* __restrict__ offsets,
+                                                          const uint32_t* __restrict__ totals) {
     __shared__ uint32_t s_off[256];
     __shared__ uint32_t s_wc[kBlock / 32][256];
+    __shared__ uint32_t s_warp[kBlock / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    s_off[tid] = offsets[tid * nblocks + blockIdx.x];
+    uint32_t all;
+    const uint32_t digit_base = block_exclusive_scan(totals[tid], s_warp, all);
+    s_off[tid] = digit_base + offsets[tid * nblocks + blockIdx.x];
 #pragma unroll
     for (int w = 0; w < kBlock / 32; ++w) s_wc[w][tid] = 0;
     __syncthreads();
@@ -256,8 +281,9 @@ int radix_sort(cudaStream_t st, int n, int bits, uint32_t* keys[2], uint32_t* va
     int cur = 0;
     for (int shift = 0; shift < bits; shift += 8) {
         k_radix_hist<<<nb, kBlock, 0, st>>>(n, shift, nb, keys[cur], hist);
-        k_radix_scan<<<1, 1024, 0, st>>>(256 * nb, hist);
-        k_radix_scatter<<<nb, kBlock, 0, st>>>(n, shift, nb, keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], hist);
+        k_radix_scan<<<256, kBlock, 0, st>>>(nb, hist, hist + (size_t)256 * nb);
+        k_radix_scatter<<<nb, kBlock, 0, st>>>(n, shift, nb, keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], hist,
+                                               hist + (size_t)256 * nb);
         cur ^= 1;
     }
     return cur;

@@ -35,9 +35,9 @@ namespace {
 
 constexpr int kMaxN = PSB_NOALLOC_MAX_N;
 constexpr int kMaxBlocks = (kMaxN + 2047) / 2048;                 // radix tiles of 2048 keys
-constexpr size_t kScratchWords = 2 * (size_t)kMaxN + 256 * (size_t)kMaxBlocks;
+constexpr size_t kScratchWords = 2 * (size_t)kMaxN + 256 * (size_t)kMaxBlocks + 256;
 
-// keys ping-pong | values ping-pong | digit histogram (256 x tiles)
+// keys ping-pong | values ping-pong | digit histogram (256 x tiles) | digit totals (256)
 static __device__ __align__(256) uint32_t g_sort_scratch[kScratchWords];
 
 constexpr int kMaxDevices = 64;

@@ -50,10 +50,9 @@ struct Params {
     float gx, gy, gz;   // gravity acceleration
     float wlo_x, wlo_y, wlo_z, whi_x, whi_y, whi_z;   // box min + r, box max - r (float, as collisionBox)
     float wall_k, wall_c;
-    // Config-profile wall boundary (virtual half-spaces behind the box faces):
+    // Config-profile walls (mirror ghost particles across the box faces):
     float bx0, by0, bz0, bx1, by1, bz1;   // faces
-    float hf, ws;       // h and the virtual lattice spacing
-    float cz, cg;       // pi h^2/(4 s^2), 2 pi h/(3 s^2)
+    float hf;           // h
     int ref;            // reference profile
     int pci;            // PCISPH (else WCSPH)
     int surface;        // surface tension on
@@ -64,6 +63,7 @@ void launch_reset_cells(cudaStream_t st, int n, const uint32_t* sorted_keys, uin
 void launch_cell_keys(cudaStream_t st, const Params& P, const float4* pos, const int* ids, uint32_t* keys_by_id,
                       uint32_t* slot_by_id, int* clamped);
 // Sorts (keys, vals) by key, stably; returns the buffer index (0 or 1) holding the result.
+// hist holds 256 * radix_blocks(n) + 256 words.
 int radix_sort(cudaStream_t st, int n, int bits, uint32_t* keys[2], uint32_t* vals[2], uint32_t* hist, int nblocks_cap);
 int radix_blocks(int n);
 void launch_reorder(cudaStream_t st, int n, const uint32_t* keys, const uint32_t* vals, const float4* pos,

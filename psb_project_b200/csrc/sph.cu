@@ -64,43 +64,93 @@ __device__ __forceinline__ float3 wall_accel(const Params& P, float4 x, float4 v
     return a;
 }
 
-// Config-profile wall boundary: each box face is backed by a half-space of
-// virtual particles on the rest lattice (layers at (k+1/2) s behind the face;
-// Harada, Koshizuka, Kawaguchi 2007, wall weight functions). Averaged along
-// the face, the layer sums are closed forms:
-//   density  sum (1-q)^3          = cz sum_k (1 - z_k^2/h^2)^4
-//   gradient sum (1-u)^2 (n . x^) = cg sum_k z_k (1 - z_k/h)^3
-// with z_k = d + (k+1/2) s. The virtual particles mirror the particle's own
-// pressure, so they push with 2 pV_i times the gradient sum.
-__device__ __forceinline__ void wall_face(const Params& P, float d, float& z, float& g) {
-    d = fmaxf(d, 0.f);
-    z = 0.f;
-    g = 0.f;
-#pragma unroll 1
-    for (int k = 0; k < 8; ++k) {
-        const float zk = d + ((float)k + 0.5f) * P.ws;
-        if (zk >= P.hf) break;
-        const float q = zk * zk * P.inv_h2;
-        const float t = 1.f - q;
-        z += (t * t) * (t * t);
-        const float u = 1.f - zk * P.inv_h;
-        g += zk * u * u * u;
+// Config-profile walls: mirror ghost particles (Libersky et al. 1993;
+// Colagrossi & Landrini 2003). Every box face within h of particle i
+// reflects i's neighbours (self included); for each non-empty set S of such
+// faces, the ghost of j is j reflected across every face in S, provided j is
+// itself within h of each. A ghost can only lie within h of i if j does, so
+// the neighbour list yields all of them. Ghosts carry j's pressure continued
+// hydrostatically across the faces, p_j + rho0 (-g . n) 2 d_j, so a resting
+// column is held by its bottom layer as by any interior layer.
+struct Walls {
+    int n;
+    int axis[3];
+    float plane[3], nrm[3];
+};
+
+__device__ __forceinline__ float comp(float4 v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+__device__ __forceinline__ float gcomp(const Params& P, int a) { return a == 0 ? P.gx : (a == 1 ? P.gy : P.gz); }
+
+__device__ __forceinline__ Walls near_walls(const Params& P, float4 x) {
+    Walls w;
+    w.n = 0;
+    const float lo[3] = {P.bx0, P.by0, P.bz0}, hi[3] = {P.bx1, P.by1, P.bz1};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float c = comp(x, a);
+        if (c - lo[a] < P.hf) { w.axis[w.n] = a; w.plane[w.n] = lo[a]; w.nrm[w.n] = 1.f; ++w.n; }
+        else if (hi[a] - c < P.hf) { w.axis[w.n] = a; w.plane[w.n] = hi[a]; w.nrm[w.n] = -1.f; ++w.n; }
     }
-    z *= P.cz;
-    g *= P.cg;
+    return w;
 }
 
-// Sum over the six faces: normalised density term and gradient (into the box).
-__device__ __forceinline__ float wall_terms(const Params& P, float4 x, float3& g) {
-    float zs = 0.f, z, gg;
-    g = make_float3(0.f, 0.f, 0.f);
-    if (x.x - P.bx0 < P.hf) { wall_face(P, x.x - P.bx0, z, gg); zs += z; g.x += gg; }
-    if (P.bx1 - x.x < P.hf) { wall_face(P, P.bx1 - x.x, z, gg); zs += z; g.x -= gg; }
-    if (x.y - P.by0 < P.hf) { wall_face(P, x.y - P.by0, z, gg); zs += z; g.y += gg; }
-    if (P.by1 - x.y < P.hf) { wall_face(P, P.by1 - x.y, z, gg); zs += z; g.y -= gg; }
-    if (x.z - P.bz0 < P.hf) { wall_face(P, x.z - P.bz0, z, gg); zs += z; g.z += gg; }
-    if (P.bz1 - x.z < P.hf) { wall_face(P, P.bz1 - x.z, z, gg); zs += z; g.z -= gg; }
-    return zs;
+// x_i minus the ghost of x_j across the faces in `mask`; false if a face of
+// the set is h or more from x_j. dp: the ghost's hydrostatic pressure offset.
+__device__ __forceinline__ bool ghost_delta(const Params& P, const Walls& w, int mask, float4 xi, float4 xj, float3& r,
+                                            float& dp) {
+    float d[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+    dp = 0.f;
+    for (int k = 0; k < w.n; ++k) {
+        if (!((mask >> k) & 1)) continue;
+        const int a = w.axis[k];
+        const float dj = comp(xj, a) - w.plane[k];
+        if (fabsf(dj) >= P.hf) return false;
+        d[a] = (comp(xi, a) - w.plane[k]) + dj;
+        dp += P.rho0 * (-gcomp(P, a) * w.nrm[k]) * 2.f * fabsf(dj);
+    }
+    r = make_float3(d[0], d[1], d[2]);
+    return true;
+}
+
+// Ghost density term (normalised like sum (1-q)^3) of particle t at xi.
+__device__ __forceinline__ void ghost_density(const Params& P, int t, float4 xi, const float4* __restrict__ pos,
+                                              const int* __restrict__ list, int cnt, Kahan& acc) {
+    const Walls w = near_walls(P, xi);
+    if (!w.n) return;
+    for (int mask = 1; mask < (1 << w.n); ++mask)
+        for (int c = 0; c < cnt; ++c) {
+            const float4 xj = pos[list[(size_t)c * P.n + t]];
+            float3 r;
+            float dp;
+            if (!ghost_delta(P, w, mask, xi, xj, r, dp)) continue;
+            const float q = (r.x * r.x + r.y * r.y + r.z * r.z) * P.inv_h2;
+            if (q >= 1.f) continue;
+            const float wq = 1.f - q;
+            acc.add(wq * wq * wq);
+        }
+}
+
+// Ghost pressure term: adds sum (pV_i + pV_ghost) (1-u)^2 x^ to ap.
+__device__ __forceinline__ void ghost_pressure(const Params& P, int t, float4 xi, float pVi,
+                                               const float4* __restrict__ pos, const float* __restrict__ pj_of,
+                                               int pj_stride, const int* __restrict__ list, int cnt, float3& ap) {
+    const Walls w = near_walls(P, xi);
+    if (!w.n) return;
+    const float ir0 = 1.f / (P.rho0 * P.rho0);
+    for (int mask = 1; mask < (1 << w.n); ++mask)
+        for (int c = 0; c < cnt; ++c) {
+            const int j = list[(size_t)c * P.n + t];
+            const float4 xj = pos[j];
+            float3 r;
+            float dp;
+            if (!ghost_delta(P, w, mask, xi, xj, r, dp)) continue;
+            const float r2 = r.x * r.x + r.y * r.y + r.z * r.z;
+            if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) continue;
+            const float rinv = rsqrtf(r2);
+            const float om = 1.f - r2 * rinv * P.inv_h;
+            const float s = (pVi + (pj_of[(size_t)j * pj_stride] + dp) * ir0) * om * om * rinv;
+            ap.x += s * r.x; ap.y += s * r.y; ap.z += s * r.z;
+        }
 }
 
 // collisionBox (BoxCollision_Kernel.cu:7-34) with restitution 0: clamp into
@@ -145,10 +195,7 @@ __global__ void __launch_bounds__(kBlock) k_density_x(Params P, const float4* __
         const float w = 1.f - q;
         acc.add(w * w * w);
     }
-    if (!P.ref) {
-        float3 g;
-        acc.add(wall_terms(P, xi, g));
-    }
+    if (!P.ref) ghost_density(P, t, xi, pos, list, cnt, acc);
     const float drho = density_deviation(P, acc);
     const float rho = P.rho0 + drho;
     float p;
@@ -183,7 +230,9 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
     PairSums S;
     S.ap = S.fv = S.nrm = make_float3(0.f, 0.f, 0.f);
     S.fs = 0.f;
-    const float pVi = WITH_PRESSURE ? rpi.y / (rpi.x * rpi.x) : 0.f;
+    // Config: p/rho0^2 (the PCISPH linearisation; see k_pci_force_predict).
+    const float ir0 = 1.f / (P.rho0 * P.rho0);
+    const float pVi = WITH_PRESSURE ? (P.ref ? rpi.y / (rpi.x * rpi.x) : rpi.y * ir0) : 0.f;
     const int cnt = min(counts[t], P.cap);
     for (int c = 0; c < cnt; ++c) {
         const int j = list[(size_t)c * P.n + t];
@@ -203,7 +252,8 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
         S.fv.y += (vj.y - vi.y) * sv;
         S.fv.z += (vj.z - vi.z) * sv;
         if (WITH_PRESSURE) {
-            const float s = (pVi + rpj.y * inv_rj * inv_rj) * om * om * rinv;
+            const float pVj = P.ref ? rpj.y * inv_rj * inv_rj : rpj.y * ir0;
+            const float s = (pVi + pVj) * om * om * rinv;
             S.ap.x += s * dx; S.ap.y += s * dy; S.ap.z += s * dz;
         }
         if (P.surface) {
@@ -213,11 +263,8 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
             S.nrm.x += dx * sn; S.nrm.y += dy * sn; S.nrm.z += dz * sn;
         }
     }
-    if (WITH_PRESSURE && !P.ref) {
-        float3 g;
-        wall_terms(P, xi, g);
-        S.ap.x += 2.f * pVi * g.x; S.ap.y += 2.f * pVi * g.y; S.ap.z += 2.f * pVi * g.z;
-    }
+    if (WITH_PRESSURE && !P.ref)
+        ghost_pressure(P, t, xi, pVi, pos, (const float*)rp + 1, 2, list, cnt, S.ap);
     return S;
 }
 
@@ -321,10 +368,7 @@ __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* 
                 T2 += g * g;
             }
         }
-        if (!P.ref) {
-            float3 g;
-            acc.add(wall_terms(P, xi, g));
-        }
+        if (!P.ref) ghost_density(P, t, xi, xs, list, cnt, acc);
         const float drho = density_deviation(P, acc);
         const float rho = P.rho0 + drho;
         float p = rp[t].y;
@@ -348,8 +392,14 @@ __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* 
     }
 }
 
-// PCISPH pressure-force pass at x* fused with the next prediction; commits
-// the candidate pressure.
+// PCISPH pressure-force pass fused with the next prediction; commits the
+// candidate pressure. Reference profile: at the predicted positions x*, with
+// p/rho*^2 (PciSphSystem_Kernel.cu:88-114 runs on the predicted state).
+// Config profile: at the step's start positions x, with p/rho0^2. That keeps
+// the corrector a linear iteration in p: at x*, x* = x + dt^2 a(x*) is a
+// fixed-point iteration in positions whose gain grows with p dt^2/h^2, and
+// with rho* in p/rho^2 the force feeds back on the density; under a 0.64 m
+// column either one makes the corrector diverge.
 __global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const float4* __restrict__ pos,
                                                               const float4* __restrict__ vap,
                                                               const float4* __restrict__ fnp,
@@ -360,14 +410,16 @@ __global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const fl
                                                               float4* __restrict__ vs, float2* __restrict__ rp) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= P.n) return;
-    const float4 xi = xs[t];
+    const float4* __restrict__ geo = P.ref ? xs : pos;
+    const float4 xi = geo[t];
     const float2 ri = rpc[t];
-    const float pVi = ri.y / (ri.x * ri.x);
+    const float ir0 = 1.f / (P.rho0 * P.rho0);
+    const float pVi = P.ref ? ri.y / (ri.x * ri.x) : ri.y * ir0;
     const int cnt = min(counts[t], P.cap);
     float3 acc = make_float3(0.f, 0.f, 0.f);
     for (int c = 0; c < cnt; ++c) {
         const int j = list[(size_t)c * P.n + t];
-        const float4 xj = xs[j];
+        const float4 xj = geo[j];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float r2 = dx * dx + dy * dy + dz * dz;
         if (!(r2 > 0.f)) continue;
@@ -375,14 +427,11 @@ __global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const fl
         const float2 rj = rpc[j];
         const float rinv = rsqrtf(r2);
         const float om = 1.f - r2 * rinv * P.inv_h;
-        const float s = (pVi + rj.y / (rj.x * rj.x)) * om * om * rinv;
+        const float pVj = P.ref ? rj.y / (rj.x * rj.x) : rj.y * ir0;
+        const float s = (pVi + pVj) * om * om * rinv;
         acc.x += s * dx; acc.y += s * dy; acc.z += s * dz;
     }
-    if (!P.ref) {
-        float3 g;
-        wall_terms(P, xi, g);
-        acc.x += 2.f * pVi * g.x; acc.y += 2.f * pVi * g.y; acc.z += 2.f * pVi * g.z;
-    }
+    if (!P.ref) ghost_pressure(P, t, xi, pVi, geo, (const float*)rpc + 1, 2, list, cnt, acc);
     const float4 x0 = pos[t], vh = vap[t], f = fnp[t];
     const float3 aw = wall_accel(P, x0, vh);
     const float ir = 1.f / ri.x;

@@ -35,7 +35,7 @@ EXPORTS = (
     "psb_create", "psb_destroy", "psb_set_stream", "psb_upload", "psb_upload_aos_f64", "psb_download",
     "psb_download_aos_f64", "psb_step", "psb_build_neighbors", "psb_read_field", "psb_get_stats",
     "psb_profile_enable", "psb_profile_read", "psb_profile_reset", "psb_lattice", "psb_status_string",
-    "psb_last_error", "psb_abi_version", "psb_sort_cells_noalloc",
+    "psb_last_error", "psb_abi_version", "psb_sort_cells_noalloc", "psb_presolve",
 )
 NOALLOC_MAX_N = 262144   # PSB_NOALLOC_MAX_N
 
@@ -87,6 +87,7 @@ def lib():
         "psb_last_error": ([P], ctypes.c_char_p),
         "psb_abi_version": ([], I32),
         "psb_sort_cells_noalloc": ([P, P, P, P, I32, I32, P], ctypes.c_int),
+        "psb_presolve": ([P, I32], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -182,6 +183,9 @@ class Simulation:
     def step(self, nsteps: int = 1, allow_noconv: bool = True) -> int:
         allow = (OK, ENOCONV) if allow_noconv else (OK,)
         return self._check(lib().psb_step(self._h, int(nsteps)), "psb_step", allow)
+
+    def presolve(self, iters: int):
+        self._check(lib().psb_presolve(self._h, int(iters)), "psb_presolve")
 
     def build_neighbors(self):
         self._check(lib().psb_build_neighbors(self._h), "psb_build_neighbors")
