@@ -59,6 +59,8 @@ ALG_BYTES = {
     "pci_force_predict": 120,  # pressure force 40 + prediction 80
     "pci_commit": 96,         # final integrate, walls, interpolation
     "wcsph_force": 228,       # forces 52 + integrate 80 + walls/interpolation 96
+    "features": 72,           # pos, vel 32 + rho, p 8 -> 8 features 32
+    "mlp_infer": 36,          # features 32 -> initial pressure 4
 }
 # Kernels per timed group (radix_sort is 3 kernels per 8-bit pass).
 def _kernels_per_group(name: str, sort_passes: int) -> int:
@@ -69,12 +71,16 @@ def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scene", default="C2")
-    ap.add_argument("--warm-start", choices=["zero", "previous"], default="previous")
+    ap.add_argument("--warm-start", choices=["zero", "previous", "learned"], default="learned")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
+    ap.add_argument("--presolve", type=int, default=256, help="initial-pressure corrector passes before the warm-up")
+    ap.add_argument("--train-steps", type=int, default=400, help="plain-PCISPH steps recorded for training (learned)")
+    ap.add_argument("--train-iters", type=int, default=3000, help="Adam steps (learned)")
+    ap.add_argument("--train-batch", type=int, default=16384)
     return ap.parse_args()
 
 
@@ -239,7 +245,7 @@ def run_ours(args):
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
-    modes = {"zero": P.WARM_ZERO, "previous": P.WARM_PREVIOUS}
+    modes = {"zero": P.WARM_ZERO, "previous": P.WARM_PREVIOUS, "learned": P.WARM_LEARNED}
     base = P.config_scene(args.scene)
     if world > 1:       # replicas: same scene, own seed per rank
         base.blocks[0].seed = base.blocks[0].seed + 1000 * rank
@@ -258,13 +264,43 @@ def run_ours(args):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # Warm-up from rest, then a snapshot every timed pass restarts from, so
-    # that all passes time the same K steps.
-    sim = P.Simulation(sc)
-    sim.set_stream(stream.cuda_stream)
-    sim.upload(P.scene_positions(sc))
-    sim.step(args.warmup)
-    snap = sim.download()
+    def make(mode):
+        s_ = P.Simulation(base.replace(warm_start=mode))
+        s_.set_stream(stream.cuda_stream)
+        return s_
+
+    # Set-up (untimed): the dam at rest with its initial pressure, then plain
+    # PCISPH for the recorded steps (learned: its converged pressures are the
+    # training targets), then the warm-up. The timed passes all restart from
+    # the snapshot taken after it.
+    pcisph_cfg = sc.method == P.PCISPH and sc.profile == P.PROFILE_CONFIG
+    gen = make(P.WARM_ZERO)
+    gen.upload(P.scene_positions(sc))
+    if pcisph_cfg and args.presolve > 0:
+        gen.presolve(args.presolve)      # initial pressure of the dam at rest
+    train_info = None
+    weights = None
+    if sc.warm_start == P.WARM_LEARNED:
+        t0 = time.perf_counter()
+        gen.mlp_collect(stride=64, capacity=max(1, (args.train_steps + 1) * ((n + 63) // 64)))
+        gen.step(args.train_steps)
+        gen.mlp_collect(0)
+        rows, _, _ = gen.mlp_dataset(fetch=False)
+        t1 = time.perf_counter()
+        gen.mlp_set_weights(P.mlp_init_weights(rank))
+        loss0 = gen.mlp_train(1, args.train_batch, 1e-3, seed=11)
+        loss = gen.mlp_train(args.train_iters, args.train_batch, 2e-3, seed=12)
+        loss = gen.mlp_train(args.train_iters // 2, args.train_batch, 5e-4, seed=13)
+        weights = gen.mlp_get_weights()
+        train_info = {"recorded_steps": args.train_steps, "rows": int(rows), "adam_steps": args.train_iters * 3 // 2 + 1,
+                      "batch": args.train_batch, "loss_first": loss0, "loss_last": loss,
+                      "record_s": round(t1 - t0, 2), "train_s": round(time.perf_counter() - t1, 2)}
+    gen.step(args.warmup)
+    snap = gen.download()
+    gen.close()
+    sim = make(sc.warm_start)
+    if weights is not None:
+        sim.mlp_set_weights(weights)
     barrier()
 
     def restore(s):
@@ -319,19 +355,19 @@ def run_ours(args):
     h2d = n * (36 + (4 if warm else 0))
     d2h = n * (40 + (4 if warm else 0))
     clk = clocks.stop()
-    # ---- plain PCISPH (pressure from zero every step) over the same steps ------------
+    # ---- the other warm starts over the same steps -------------------------------------
     comparison = {}
-    if sc.warm_start != P.WARM_ZERO:
-        plain = P.Simulation(base.replace(warm_start=P.WARM_ZERO))
-        plain.set_stream(stream.cuda_stream)
-        ms_plain, iters_plain, _ = device_pass(plain)
-        plain.close()
-        comparison["plain"] = {"iters_mean": float(np.mean(iters_plain)), "iters_max": int(np.max(iters_plain)),
-                               "ms_per_step": ms_plain / args.steps,
-                               "value": world * n * args.steps / (ms_plain / 1e3),
-                               "not_converged_steps": int(np.sum(np.asarray(iters_plain) >= sc.max_iters))}
-        comparison["iters_ratio_plain_over_this"] = float(np.mean(iters_plain) / max(np.mean(iters), 1e-9))
-        comparison["time_ratio_plain_over_this"] = float(ms_plain / ms_max)
+    for name, mode in (("plain", P.WARM_ZERO), ("previous", P.WARM_PREVIOUS)):
+        if mode == sc.warm_start or not pcisph_cfg:
+            continue
+        other = make(mode)
+        ms_o, iters_o, _ = device_pass(other)
+        other.close()
+        comparison[name] = {"iters_mean": float(np.mean(iters_o)), "iters_max": int(np.max(iters_o)),
+                            "ms_per_step": ms_o / args.steps, "value": world * n * args.steps / (ms_o / 1e3),
+                            "not_converged_steps": int(np.sum(np.asarray(iters_o) >= sc.max_iters)),
+                            "iters_ratio_over_this": float(np.mean(iters_o) / max(np.mean(iters), 1e-9)),
+                            "time_ratio_over_this": float(ms_o / ms_max)}
     sim.close()
 
     passes = (max(1, int(np.ceil(np.log2(np.prod(sc.dims))))) + 7) // 8
@@ -348,7 +384,9 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline_port(sc, snap, args.cpu_sample_steps)
+            # the FP64 port has no MLP: it runs the previous-pressure warm start
+            cpu_sc = sc.replace(warm_start=P.WARM_PREVIOUS) if sc.warm_start == P.WARM_LEARNED else sc
+            cpu = cpu_baseline_port(cpu_sc, snap, args.cpu_sample_steps)
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": host_cores(), "kind": "port", "sample": f"failed: {ex}"}
 
@@ -362,11 +400,15 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "working set > L2 (state, lists and scratch ~%d MB per GPU)"
                              % int(n * (3 * 16 * 2 + 8 * 2 + 4 * 2 + 16 * 4 + 8 + 4 + 4 * sc.nbr_cap + 4) / 1e6),
-                       "timed_steps": f"steps {args.warmup + 1}..{args.warmup + args.steps} of the dam break"},
+                       "timed_steps": "steps %d..%d of the dam break" % (
+                           (args.train_steps if train_info else 0) + args.warmup + 1,
+                           (args.train_steps if train_info else 0) + args.warmup + args.steps),
+                       "presolve_passes": args.presolve},
             "iters_per_step": {"mean": float(np.mean(iters)), "p50": float(np.median(iters)),
                                "p95": float(np.percentile(iters, 95)), "max": int(np.max(iters)),
                                "min": int(np.min(iters))},
             "comparison": comparison,
+            "learned_training": train_info,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None if traffic is None else traffic * n,

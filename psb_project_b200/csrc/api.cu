@@ -105,6 +105,24 @@ struct psb_ctx {
     unsigned long long* err_hist = nullptr;
     int* flags = nullptr;     // [0] overflow [1] max count [2..3] pair total [4] clamped
     void* stage = nullptr;    // device staging for uploads/downloads
+    // learned warm start
+    float* feats = nullptr;   // n_max x 8
+    float* mlp_w = nullptr;   // FP32 master weights
+    float* mlp_m1 = nullptr;
+    float* mlp_m2 = nullptr;
+    float* mlp_grad = nullptr;
+    float* mlp_loss = nullptr;
+    void* mlp_wbf = nullptr;  // BF16 copy used by the kernels
+    int mlp_step = 0;
+    bool mlp_set = false;
+    float p_scale = 1.f;
+    float* ds_X = nullptr;    // recorded rows x 8
+    float* ds_T = nullptr;
+    uint64_t ds_cap = 0, ds_rows = 0;
+    int collect_stride = 0;
+    int64_t collect_steps = 0;
+    uint32_t* sel = nullptr;
+    int sel_cap = 0;
     // host mirrors
     unsigned long long* h_err = nullptr;
     int* h_flags = nullptr;
@@ -166,6 +184,8 @@ void free_all(psb_ctx* c) {
     cudaFree(c->hist); cudaFree(c->cell_start); cudaFree(c->cell_end); cudaFree(c->nbr_count);
     cudaFree(c->nbr_list); cudaFree(c->fnp); cudaFree(c->vs); cudaFree(c->rpc); cudaFree(c->rho_x);
     cudaFree(c->err_hist); cudaFree(c->flags); cudaFree(c->stage);
+    cudaFree(c->feats); cudaFree(c->mlp_w); cudaFree(c->mlp_m1); cudaFree(c->mlp_m2); cudaFree(c->mlp_grad);
+    cudaFree(c->mlp_loss); cudaFree(c->mlp_wbf); cudaFree(c->ds_X); cudaFree(c->ds_T); cudaFree(c->sel);
     cudaFreeHost(c->h_err); cudaFreeHost(c->h_flags);
 }
 
@@ -187,7 +207,10 @@ int validate(const psb_scene* s, std::string& why) {
         return PSB_EINVAL;
     }
     if (s->nbr_cap < 0 || s->nbr_cap > 4096) { why = "nbr_cap out of range"; return PSB_EINVAL; }
-    if (s->warm_start != PSB_WARM_ZERO && s->warm_start != PSB_WARM_PREVIOUS) { why = "unknown warm_start"; return PSB_EINVAL; }
+    if (s->warm_start != PSB_WARM_ZERO && s->warm_start != PSB_WARM_PREVIOUS && s->warm_start != PSB_WARM_LEARNED) {
+        why = "unknown warm_start";
+        return PSB_EINVAL;
+    }
     {
         const double ws = s->spacing > 0 ? s->spacing : std::cbrt(s->mass / s->rho0);
         if (!(ws > 0)) { why = "spacing must be positive"; return PSB_EINVAL; }
@@ -362,7 +385,8 @@ int read_flags(psb_ctx* c) {
 }
 
 int step_once(psb_ctx* c, bool last) {
-    PSB_TRY(build(c));
+    const bool need_prev_p = !c->P.ref && c->P.pci && (c->sc.warm_start != PSB_WARM_ZERO || c->collect_stride > 0);
+    PSB_TRY(build(c, need_prev_p));
     cudaStream_t st = c->stream;
     Params P = c->P;
     P.n = c->n;
@@ -379,7 +403,20 @@ int step_once(psb_ctx* c, bool last) {
         c->stats.iters = 0;
         c->stats.converged = 1;
     } else {
-        const int warm = (!P.ref && c->sc.warm_start == PSB_WARM_PREVIOUS) ? 1 : 0;
+        const int mode = P.ref ? PSB_WARM_ZERO : c->sc.warm_start;
+        const bool collect = !P.ref && c->collect_stride > 0;
+        if (mode == PSB_WARM_LEARNED || collect) {
+            timed(c, "features", [&] {
+                psb::launch_features(st, P, c->pos[s], c->vel[s], c->rp[r], c->nbr_count, c->nbr_list, c->p_scale,
+                                     c->feats);
+            });
+        }
+        if (mode == PSB_WARM_LEARNED) {
+            timed(c, "mlp_infer", [&] { psb::launch_mlp_infer(st, c->n, c->feats, c->mlp_wbf, c->p_scale, c->rp[r]); });
+        } else if (mode == PSB_WARM_ZERO && collect) {
+            psb::launch_zero_pressure(st, c->n, c->rp[r]);   // features kept the previous pressure
+        }
+        const int warm = mode == PSB_WARM_ZERO ? 0 : 1;
         timed(c, "pci_init", [&] {
             psb::launch_pci_init(st, P, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list, warm,
                                  c->fnp, c->xs[0], c->vs);
@@ -409,6 +446,15 @@ int step_once(psb_ctx* c, bool last) {
         timed(c, "pci_commit", [&] {
             psb::launch_pci_commit(st, P, c->xs[xi], c->vs, c->rpc, passes > 0, c->pos[s], c->vel[s], c->vap[s], c->rp[r]);
         });
+        if (collect && converged) {
+            const int stride = c->collect_stride;
+            const int offset = (int)(c->collect_steps % stride);
+            const int rows = offset < c->n ? (c->n - offset + stride - 1) / stride : 0;
+            psb::launch_collect(st, c->n, stride, offset, c->ds_rows, c->ds_cap, c->feats, c->rp[r], c->p_scale, c->ds_X,
+                                c->ds_T);
+            c->ds_rows += (uint64_t)rows;
+            c->collect_steps += 1;
+        }
         iters = k;
         c->stats.iters = iters;
         c->stats.converged = converged;
@@ -492,6 +538,15 @@ int psb_create(const psb_scene* scene, psb_ctx** out) {
     if (!rc) rc = dalloc(c, &c->err_hist, PSB_MAX_ITERS + 1);
     if (!rc) rc = dalloc(c, &c->flags, 8);
     if (!rc) rc = dalloc(c, (char**)&c->stage, n * 32);
+    if (!rc) rc = dalloc(c, &c->feats, n * 8);
+    if (!rc) rc = dalloc(c, &c->mlp_w, psb::kMlpParams);
+    if (!rc) rc = dalloc(c, &c->mlp_m1, psb::kMlpParams);
+    if (!rc) rc = dalloc(c, &c->mlp_m2, psb::kMlpParams);
+    if (!rc) rc = dalloc(c, &c->mlp_grad, psb::kMlpParams);
+    if (!rc) rc = dalloc(c, &c->mlp_loss, 1);
+    if (!rc) rc = dalloc(c, (uint16_t**)&c->mlp_wbf, psb::kMlpParams);
+    if (!rc && cudaMemset(c->mlp_w, 0, sizeof(float) * psb::kMlpParams) != cudaSuccess) rc = PSB_ECUDA;
+    if (!rc && cudaMemset(c->mlp_wbf, 0, 2 * psb::kMlpParams) != cudaSuccess) rc = PSB_ECUDA;
     if (!rc && cudaMallocHost((void**)&c->h_err, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1)) != cudaSuccess) rc = PSB_ENOMEM;
     if (!rc && cudaMallocHost((void**)&c->h_flags, 8 * sizeof(int)) != cudaSuccess) rc = PSB_ENOMEM;
     if (!rc && cudaMemset(c->cell_start, 0xFF, sizeof(uint32_t) * c->ncells) != cudaSuccess) rc = PSB_ECUDA;
@@ -505,6 +560,12 @@ int psb_create(const psb_scene* scene, psb_ctx** out) {
         return rc;
     }
     std::memset(c->h_err, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1));
+    {   // pressure scale of the learned warm start: rho0 |g| 0.1 m
+        const double g = std::sqrt((double)scene->gravity[0] * scene->gravity[0] +
+                                   (double)scene->gravity[1] * scene->gravity[1] +
+                                   (double)scene->gravity[2] * scene->gravity[2]);
+        c->p_scale = (float)(scene->rho0 * (g > 0 ? g : 9.81) * 0.1);
+    }
     *out = c;
     return PSB_OK;
 }
@@ -636,6 +697,120 @@ int psb_step(psb_ctx* c, int32_t nsteps) {
     }
     if (c->prof.on) c->prof.resolve(c->stream);
     return status;
+}
+
+int psb_mlp_set_weights(psb_ctx* c, const float* w) {
+    if (!c || !w) return PSB_EINVAL;
+    cudaSetDevice(c->device);
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->mlp_w, w, sizeof(float) * psb::kMlpParams, cudaMemcpyHostToDevice, c->stream), "weights"));
+    cudaMemsetAsync(c->mlp_m1, 0, sizeof(float) * psb::kMlpParams, c->stream);
+    cudaMemsetAsync(c->mlp_m2, 0, sizeof(float) * psb::kMlpParams, c->stream);
+    psb::launch_to_bf16(c->stream, c->mlp_w, c->mlp_wbf);
+    c->mlp_step = 0;
+    c->mlp_set = true;
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "weights"));
+    return cuda_check(c, cudaGetLastError(), "weights");
+}
+
+int psb_mlp_get_weights(psb_ctx* c, float* w) {
+    if (!c || !w) return PSB_EINVAL;
+    cudaSetDevice(c->device);
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(w, c->mlp_w, sizeof(float) * psb::kMlpParams, cudaMemcpyDeviceToHost, c->stream), "weights"));
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "weights");
+}
+
+int psb_mlp_collect(psb_ctx* c, int32_t stride, int64_t capacity) {
+    if (!c || stride < 0 || (stride > 0 && capacity <= 0)) return fail(c, PSB_EINVAL, "psb_mlp_collect: bad argument");
+    cudaSetDevice(c->device);
+    c->collect_stride = stride;
+    if (stride == 0) return PSB_OK;
+    if ((uint64_t)capacity != c->ds_cap) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(c->ds_X);
+        cudaFree(c->ds_T);
+        c->ds_X = c->ds_T = nullptr;
+        c->ds_cap = 0;
+        PSB_TRY(dalloc(c, &c->ds_X, (size_t)capacity * 8));
+        PSB_TRY(dalloc(c, &c->ds_T, (size_t)capacity));
+        c->ds_cap = (uint64_t)capacity;
+        c->ds_rows = 0;
+    }
+    return PSB_OK;
+}
+
+int psb_mlp_dataset(psb_ctx* c, int64_t* rows, float* X, float* T) {
+    if (!c || !rows) return PSB_EINVAL;
+    cudaSetDevice(c->device);
+    const uint64_t r = c->ds_rows < c->ds_cap ? c->ds_rows : c->ds_cap;
+    *rows = (int64_t)r;
+    if (X && r) PSB_TRY(cuda_check(c, cudaMemcpyAsync(X, c->ds_X, sizeof(float) * 8 * r, cudaMemcpyDeviceToHost, c->stream), "dataset"));
+    if (T && r) PSB_TRY(cuda_check(c, cudaMemcpyAsync(T, c->ds_T, sizeof(float) * r, cudaMemcpyDeviceToHost, c->stream), "dataset"));
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "dataset");
+}
+
+int psb_mlp_train(psb_ctx* c, int32_t iters, int32_t batch, float lr, uint64_t seed, float* loss) {
+    if (!c || iters < 0 || batch <= 0 || !(lr > 0)) return fail(c, PSB_EINVAL, "psb_mlp_train: bad argument");
+    const uint64_t rows = c->ds_rows < c->ds_cap ? c->ds_rows : c->ds_cap;
+    if (rows == 0) return fail(c, PSB_ESTATE, "psb_mlp_train: no recorded data");
+    if (!c->mlp_set) return fail(c, PSB_ESTATE, "psb_mlp_train: set initial weights first");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    if (batch > c->sel_cap) {
+        cudaStreamSynchronize(st);
+        cudaFree(c->sel);
+        c->sel = nullptr;
+        c->sel_cap = 0;
+        PSB_TRY(dalloc(c, &c->sel, (size_t)batch));
+        c->sel_cap = batch;
+    }
+    for (int it = 0; it < iters; ++it) {
+        psb::launch_mlp_sample(st, batch, rows, seed + 0x100000001ull * (uint64_t)(c->mlp_step + 1), c->sel);
+        timed(c, "mlp_train", [&] { psb::launch_mlp_grad(st, batch, c->ds_X, c->ds_T, c->sel, c->mlp_wbf, c->mlp_grad, c->mlp_loss); });
+        ++c->mlp_step;
+        psb::launch_adam(st, c->mlp_w, c->mlp_grad, c->mlp_m1, c->mlp_m2, c->mlp_wbf, lr, c->mlp_step);
+    }
+    if (loss) {
+        PSB_TRY(cuda_check(c, cudaMemcpyAsync(loss, c->mlp_loss, sizeof(float), cudaMemcpyDeviceToHost, st), "loss"));
+    }
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "train"));
+    return cuda_check(c, cudaGetLastError(), "train");
+}
+
+static int mlp_host_call(psb_ctx* c, const float* X, const float* T, int32_t n, float* y, float* loss, float* grad) {
+    if (!c || !X || n <= 0) return fail(c, PSB_EINVAL, "psb_mlp: bad argument");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    float *dX = nullptr, *dT = nullptr, *dy = nullptr;
+    int rc = dalloc(c, &dX, (size_t)n * 8);
+    if (!rc) rc = dalloc(c, &dT, (size_t)n);
+    if (!rc) rc = dalloc(c, &dy, (size_t)n);
+    if (!rc) rc = cuda_check(c, cudaMemcpyAsync(dX, X, sizeof(float) * 8 * n, cudaMemcpyHostToDevice, st), "mlp");
+    if (!rc && T) rc = cuda_check(c, cudaMemcpyAsync(dT, T, sizeof(float) * n, cudaMemcpyHostToDevice, st), "mlp");
+    if (!rc && y) {
+        psb::launch_mlp_forward(st, n, dX, 8, c->mlp_wbf, dy);
+        rc = cuda_check(c, cudaMemcpyAsync(y, dy, sizeof(float) * n, cudaMemcpyDeviceToHost, st), "mlp");
+    }
+    if (!rc && grad) {
+        psb::launch_mlp_grad(st, n, dX, dT, nullptr, c->mlp_wbf, c->mlp_grad, c->mlp_loss);
+        rc = cuda_check(c, cudaMemcpyAsync(grad, c->mlp_grad, sizeof(float) * psb::kMlpParams, cudaMemcpyDeviceToHost, st), "mlp");
+        if (!rc && loss) rc = cuda_check(c, cudaMemcpyAsync(loss, c->mlp_loss, sizeof(float), cudaMemcpyDeviceToHost, st), "mlp");
+    }
+    if (!rc) rc = cuda_check(c, cudaStreamSynchronize(st), "mlp");
+    if (!rc) rc = cuda_check(c, cudaGetLastError(), "mlp");
+    cudaFree(dX);
+    cudaFree(dT);
+    cudaFree(dy);
+    return rc;
+}
+
+int psb_mlp_forward(psb_ctx* c, const float* X, int32_t n, float* y) {
+    if (!y) return PSB_EINVAL;
+    return mlp_host_call(c, X, nullptr, n, y, nullptr, nullptr);
+}
+
+int psb_mlp_loss_grad(psb_ctx* c, const float* X, const float* T, int32_t n, float* loss, float* grad) {
+    if (!T || !grad) return PSB_EINVAL;
+    return mlp_host_call(c, X, T, n, nullptr, loss, grad);
 }
 
 int psb_presolve(psb_ctx* c, int32_t iters) {

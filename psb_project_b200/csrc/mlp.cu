@@ -1,0 +1,326 @@
+// mlp.cu -- learned pressure warm start for the PCISPH corrector.
+//
+// A per-particle MLP, 6 -> 64 -> 64 -> 1 with SiLU, predicts each step's
+// initial pressure so that the eta-controlled corrector (unchanged; it still
+// iterates to the same eta and judges convergence) starts closer to the
+// converged pressure. The reference has no counterpart: it starts every
+// step from p = 0 (PciSphSystem_Kernel.cu:131).
+//
+// Inputs, computed at the step's start positions from the neighbour list:
+//   f0 neighbour count / 32
+//   f1 advected density (rho - dt rho div v - rho0)/rho0 * 100
+//   f2 velocity divergence div v * dt * 100, div v = sum (m/rho0)(v_j - v_i).gradW_ij
+//   f3 previous-step pressure / p_scale
+//   f4 distance to the nearest box face / h, capped at 1
+//   f5 |sum m gradW_ij| * h / rho0 (density-gradient magnitude)
+// Output y: initial pressure max(0, y) * p_scale, p_scale = rho0 |g| 0.1 m.
+//
+// Precision: weights and activations are BF16 (round-to-nearest-even at
+// every stored activation), accumulation FP32, master weights FP32 (Adam).
+// Training is on the GPU: (features, converged pressure) pairs are collected
+// from steps of the same eta-loop, then minibatch Adam on an MSE loss, with a
+// fused forward/backward kernel whose weight gradients are reduced per warp
+// with shuffles before one atomic add per warp.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "psb_internal.cuh"
+
+namespace psb {
+
+namespace {
+
+constexpr int kIn = 6, kH = 64;
+constexpr int oW1 = 0, oB1 = oW1 + kH * kIn, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH, oB3 = oW3 + kH;
+static_assert(oB3 + 1 == kMlpParams, "parameter layout");
+
+__device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ float silu(float z) { return z / (1.f + expf(-z)); }
+__device__ __forceinline__ float silu_grad(float z) {
+    const float s = 1.f / (1.f + expf(-z));
+    return s * (1.f + z * (1.f - s));
+}
+
+// ---- features ---------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_features(Params P, const float4* __restrict__ pos,
+                                                     const float4* __restrict__ vel, const float2* __restrict__ rp,
+                                                     const int* __restrict__ counts, const int* __restrict__ list,
+                                                     float p_scale, float* __restrict__ feats) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const float4 xi = pos[t], vi = vel[t];
+    const int cnt = min(counts[t], P.cap);
+    float div = 0.f;
+    float3 gr = make_float3(0.f, 0.f, 0.f);
+    for (int c = 0; c < cnt; ++c) {
+        const int j = list[(size_t)c * P.n + t];
+        const float4 xj = pos[j];
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) continue;
+        const float4 vj = vel[j];
+        const float rinv = rsqrtf(r2);
+        const float om = 1.f - r2 * rinv * P.inv_h;
+        const float s = om * om * rinv;                  // (1-u)^2 / r
+        gr.x += s * dx; gr.y += s * dy; gr.z += s * dz;  // -gradW / (m G)
+        div += s * ((vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz);
+    }
+    // gradW_ij = -G (1-u)^2 x^_ij: div v = -(k_grad/rho0) sum (1-u)^2 (v_j - v_i).x^
+    div *= -P.k_grad / P.rho0;
+    const float rho = rp[t].x;
+    float dwall = P.hf;
+    dwall = fminf(dwall, fminf(xi.x - P.bx0, P.bx1 - xi.x));
+    dwall = fminf(dwall, fminf(xi.y - P.by0, P.by1 - xi.y));
+    dwall = fminf(dwall, fminf(xi.z - P.bz0, P.bz1 - xi.z));
+    float* f = feats + (size_t)t * 8;
+    f[0] = (float)counts[t] * (1.f / 32.f);
+    f[1] = (rho - P.dt * rho * div - P.rho0) / P.rho0 * 100.f;
+    f[2] = div * P.dt * 100.f;
+    f[3] = rp[t].y / p_scale;
+    f[4] = fmaxf(dwall, 0.f) * P.inv_h;
+    f[5] = P.k_grad * sqrtf(gr.x * gr.x + gr.y * gr.y + gr.z * gr.z) * P.hf / P.rho0;
+}
+
+// ---- inference -----------------------------------------------------------------
+// One thread per particle; the BF16 weights, widened to FP32, in shared memory
+// (every lane of a warp reads the same weight: broadcast).
+__global__ void __launch_bounds__(kBlock) k_mlp_infer(int n, const float* __restrict__ feats,
+                                                      const __nv_bfloat16* __restrict__ w, float p_scale,
+                                                      float2* __restrict__ rp) {
+    __shared__ float sw[kMlpParams];
+    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) sw[i] = __bfloat162float(w[i]);
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    float x[kIn];
+#pragma unroll
+    for (int k = 0; k < kIn; ++k) x[k] = bf(feats[(size_t)t * 8 + k]);
+    float h1[kH];
+#pragma unroll
+    for (int j = 0; j < kH; ++j) {
+        float z = sw[oB1 + j];
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) z = fmaf(sw[oW1 + j * kIn + k], x[k], z);
+        h1[j] = bf(silu(z));
+    }
+    float y = sw[oB3];
+    for (int j = 0; j < kH; ++j) {
+        float z = sw[oB2 + j];
+#pragma unroll
+        for (int k = 0; k < kH; ++k) z = fmaf(sw[oW2 + j * kH + k], h1[k], z);
+        y = fmaf(sw[oW3 + j], bf(silu(z)), y);
+    }
+    rp[t].y = fmaxf(0.f, y) * p_scale;
+}
+
+// Forward on arbitrary feature rows (host-facing evaluation).
+__global__ void __launch_bounds__(kBlock) k_mlp_forward(int n, const float* __restrict__ X, int stride,
+                                                        const __nv_bfloat16* __restrict__ w, float* __restrict__ y_out) {
+    __shared__ float sw[kMlpParams];
+    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) sw[i] = __bfloat162float(w[i]);
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    float x[kIn];
+#pragma unroll
+    for (int k = 0; k < kIn; ++k) x[k] = bf(X[(size_t)t * stride + k]);
+    float h1[kH];
+#pragma unroll
+    for (int j = 0; j < kH; ++j) {
+        float z = sw[oB1 + j];
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) z = fmaf(sw[oW1 + j * kIn + k], x[k], z);
+        h1[j] = bf(silu(z));
+    }
+    float y = sw[oB3];
+    for (int j = 0; j < kH; ++j) {
+        float z = sw[oB2 + j];
+#pragma unroll
+        for (int k = 0; k < kH; ++k) z = fmaf(sw[oW2 + j * kH + k], h1[k], z);
+        y = fmaf(sw[oW3 + j], bf(silu(z)), y);
+    }
+    y_out[t] = y;
+}
+
+// ---- training ---------------------------------------------------------------------
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One thread per sample: forward (activations kept in registers, the second
+// layer recomputed per unit), MSE loss, backward. Weight gradients are summed
+// over the warp with shuffles and added to `grad` once per warp.
+// Sample b of the batch is row sel[b] of (X, T) (X stride 8, features 0..5).
+__global__ void __launch_bounds__(128) k_mlp_train(int batch, const float* __restrict__ X, const float* __restrict__ T,
+                                                   const uint32_t* __restrict__ sel,
+                                                   const __nv_bfloat16* __restrict__ w, float* __restrict__ grad,
+                                                   float* __restrict__ loss) {
+    __shared__ float sw[kMlpParams];
+    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) sw[i] = __bfloat162float(w[i]);
+    __syncthreads();
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = b < batch;
+    const uint32_t row = valid ? (sel ? sel[b] : (uint32_t)b) : 0u;
+    const float inv_b = 1.f / (float)batch;
+    float x[kIn];
+#pragma unroll
+    for (int k = 0; k < kIn; ++k) x[k] = valid ? bf(X[(size_t)row * 8 + k]) : 0.f;
+    float h1[kH];
+#pragma unroll
+    for (int j = 0; j < kH; ++j) {
+        float z = sw[oB1 + j];
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) z = fmaf(sw[oW1 + j * kIn + k], x[k], z);
+        h1[j] = bf(silu(z));
+    }
+    float y = sw[oB3];
+    for (int j = 0; j < kH; ++j) {
+        float z = sw[oB2 + j];
+#pragma unroll
+        for (int k = 0; k < kH; ++k) z = fmaf(sw[oW2 + j * kH + k], h1[k], z);
+        y = fmaf(sw[oW3 + j], bf(silu(z)), y);
+    }
+    const float e = valid ? y - T[row] : 0.f;
+    const float dy = 2.f * e * inv_b;                     // d(mean e^2)/dy
+    const float ls = warp_sum(e * e * inv_b);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, ls);
+    const float gb3 = warp_sum(dy);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&grad[oB3], gb3);
+    float dh1[kH];
+#pragma unroll
+    for (int k = 0; k < kH; ++k) dh1[k] = 0.f;
+    for (int j = 0; j < kH; ++j) {
+        float z = sw[oB2 + j];
+#pragma unroll
+        for (int k = 0; k < kH; ++k) z = fmaf(sw[oW2 + j * kH + k], h1[k], z);
+        const float h2 = bf(silu(z));
+        const float dz2 = dy * sw[oW3 + j] * silu_grad(z);
+        const float g3 = warp_sum(dy * h2);
+        const float g2b = warp_sum(dz2);
+        if ((threadIdx.x & 31) == 0) { atomicAdd(&grad[oW3 + j], g3); atomicAdd(&grad[oB2 + j], g2b); }
+#pragma unroll
+        for (int k = 0; k < kH; ++k) {
+            dh1[k] = fmaf(sw[oW2 + j * kH + k], dz2, dh1[k]);
+            const float g = warp_sum(dz2 * h1[k]);
+            if ((threadIdx.x & 31) == 0) atomicAdd(&grad[oW2 + j * kH + k], g);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kH; ++j) {
+        float z = sw[oB1 + j];
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) z = fmaf(sw[oW1 + j * kIn + k], x[k], z);
+        const float dz1 = dh1[j] * silu_grad(z);
+        const float g1b = warp_sum(dz1);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&grad[oB1 + j], g1b);
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) {
+            const float g = warp_sum(dz1 * x[k]);
+            if ((threadIdx.x & 31) == 0) atomicAdd(&grad[oW1 + j * kIn + k], g);
+        }
+    }
+}
+
+__global__ void k_adam(int np, float* __restrict__ wmaster, const float* __restrict__ grad, float* __restrict__ m1,
+                       float* __restrict__ m2, __nv_bfloat16* __restrict__ wbf, float lr, float b1, float b2,
+                       float eps, float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const float g = grad[i];
+    const float m = b1 * m1[i] + (1.f - b1) * g;
+    const float v = b2 * m2[i] + (1.f - b2) * g * g;
+    m1[i] = m;
+    m2[i] = v;
+    const float w = wmaster[i] - lr * (m / c1) / (sqrtf(v / c2) + eps);
+    wmaster[i] = w;
+    wbf[i] = __float2bfloat16_rn(w);
+}
+
+__global__ void k_to_bf16(int np, const float* __restrict__ w, __nv_bfloat16* __restrict__ wbf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < np) wbf[i] = __float2bfloat16_rn(w[i]);
+}
+
+// Samples: uniform over [0, size) from SplitMix64 of (seed, iteration, b).
+__global__ void k_sample(int batch, uint64_t size, uint64_t seed, uint32_t* __restrict__ sel) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= batch) return;
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull * (uint64_t)(b + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    sel[b] = (uint32_t)(z % size);
+}
+
+// Appends (features, converged pressure) of every stride-th slot, from
+// `offset`, to the dataset rows [base, base + ceil((n - offset)/stride)).
+__global__ void k_collect(int n, int stride, int offset, uint64_t base, uint64_t cap, const float* __restrict__ feats,
+                          const float2* __restrict__ rp, float p_scale, float* __restrict__ X, float* __restrict__ T) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = offset + i * stride;
+    if (s >= n) return;
+    const uint64_t row = (base + (uint64_t)i) % cap;
+    const float* f = feats + (size_t)s * 8;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) X[row * 8 + k] = f[k];
+    T[row] = rp[s].y / p_scale;
+}
+
+__global__ void k_zero_pressure(int n, float2* __restrict__ rp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) rp[i].y = 0.f;
+}
+
+inline int grid_of(int n, int b = kBlock) { return (n + b - 1) / b; }
+
+}  // namespace
+
+void launch_zero_pressure(cudaStream_t st, int n, float2* rp) {
+    if (n > 0) k_zero_pressure<<<grid_of(n), kBlock, 0, st>>>(n, rp);
+}
+
+void launch_features(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float2* rp,
+                     const int* counts, const int* list, float p_scale, float* feats) {
+    if (P.n > 0) k_features<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, rp, counts, list, p_scale, feats);
+}
+
+void launch_mlp_infer(cudaStream_t st, int n, const float* feats, const void* wbf, float p_scale, float2* rp) {
+    if (n > 0) k_mlp_infer<<<grid_of(n), kBlock, 0, st>>>(n, feats, (const __nv_bfloat16*)wbf, p_scale, rp);
+}
+
+void launch_mlp_forward(cudaStream_t st, int n, const float* X, int stride, const void* wbf, float* y) {
+    if (n > 0) k_mlp_forward<<<grid_of(n), kBlock, 0, st>>>(n, X, stride, (const __nv_bfloat16*)wbf, y);
+}
+
+void launch_mlp_grad(cudaStream_t st, int batch, const float* X, const float* T, const uint32_t* sel, const void* wbf,
+                     float* grad, float* loss) {
+    cudaMemsetAsync(grad, 0, sizeof(float) * kMlpParams, st);
+    cudaMemsetAsync(loss, 0, sizeof(float), st);
+    if (batch > 0) k_mlp_train<<<grid_of(batch, 128), 128, 0, st>>>(batch, X, T, sel, (const __nv_bfloat16*)wbf, grad, loss);
+}
+
+void launch_mlp_sample(cudaStream_t st, int batch, uint64_t size, uint64_t seed, uint32_t* sel) {
+    if (batch > 0) k_sample<<<grid_of(batch), kBlock, 0, st>>>(batch, size, seed, sel);
+}
+
+void launch_adam(cudaStream_t st, float* w, const float* grad, float* m1, float* m2, void* wbf, float lr, int step) {
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+    k_adam<<<grid_of(kMlpParams), kBlock, 0, st>>>(kMlpParams, w, grad, m1, m2, (__nv_bfloat16*)wbf, lr, b1, b2, 1e-8f,
+                                                   c1, c2);
+}
+
+void launch_to_bf16(cudaStream_t st, const float* w, void* wbf) {
+    k_to_bf16<<<grid_of(kMlpParams), kBlock, 0, st>>>(kMlpParams, w, (__nv_bfloat16*)wbf);
+}
+
+void launch_collect(cudaStream_t st, int n, int stride, int offset, uint64_t base, uint64_t cap, const float* feats,
+                    const float2* rp, float p_scale, float* X, float* T) {
+    const int rows = offset < n ? (n - offset + stride - 1) / stride : 0;
+    if (rows > 0) k_collect<<<grid_of(rows), kBlock, 0, st>>>(n, stride, offset, base, cap, feats, rp, p_scale, X, T);
+}
+
+}  // namespace psb

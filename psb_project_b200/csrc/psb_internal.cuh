@@ -89,6 +89,21 @@ void launch_pci_force_predict(cudaStream_t st, const Params& P, const float4* po
 void launch_pci_commit(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const float2* rpc,
                        int have_density_pass, float4* pos, float4* vel, float4* vap, float2* rp);
 
+// ---- learned warm start (mlp.cu) ---------------------------------------------------
+constexpr int kMlpParams = 4673;   // 6x64 + 64 + 64x64 + 64 + 64 + 1
+void launch_features(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float2* rp,
+                     const int* counts, const int* list, float p_scale, float* feats);
+void launch_mlp_infer(cudaStream_t st, int n, const float* feats, const void* wbf, float p_scale, float2* rp);
+void launch_mlp_forward(cudaStream_t st, int n, const float* X, int stride, const void* wbf, float* y);
+void launch_mlp_grad(cudaStream_t st, int batch, const float* X, const float* T, const uint32_t* sel, const void* wbf,
+                     float* grad, float* loss);
+void launch_mlp_sample(cudaStream_t st, int batch, uint64_t size, uint64_t seed, uint32_t* sel);
+void launch_adam(cudaStream_t st, float* w, const float* grad, float* m1, float* m2, void* wbf, float lr, int step);
+void launch_to_bf16(cudaStream_t st, const float* w, void* wbf);
+void launch_collect(cudaStream_t st, int n, int stride, int offset, uint64_t base, uint64_t cap, const float* feats,
+                    const float2* rp, float p_scale, float* X, float* T);
+void launch_zero_pressure(cudaStream_t st, int n, float2* rp);
+
 // Ordered encoding of doubles for atomicMax on unsigned 64-bit words.
 __host__ __device__ inline unsigned long long order_double(double v) {
     long long b;

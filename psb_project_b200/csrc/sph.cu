@@ -74,41 +74,57 @@ __device__ __forceinline__ float3 wall_accel(const Params& P, float4 x, float4 v
 // column is held by its bottom layer as by any interior layer.
 struct Walls {
     int n;
-    int axis[3];
-    float plane[3], nrm[3];
+    int a0, a1, a2;           // axis of each near face
+    float p0, p1, p2;         // plane
+    float n0, n1, n2;         // inward normal sign
 };
 
 __device__ __forceinline__ float comp(float4 v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
 __device__ __forceinline__ float gcomp(const Params& P, int a) { return a == 0 ? P.gx : (a == 1 ? P.gy : P.gz); }
 
+__device__ __forceinline__ void push_wall(Walls& w, int a, float plane, float nrm) {
+    if (w.n == 0) { w.a0 = a; w.p0 = plane; w.n0 = nrm; }
+    else if (w.n == 1) { w.a1 = a; w.p1 = plane; w.n1 = nrm; }
+    else { w.a2 = a; w.p2 = plane; w.n2 = nrm; }
+    ++w.n;
+}
+
 __device__ __forceinline__ Walls near_walls(const Params& P, float4 x) {
     Walls w;
     w.n = 0;
-    const float lo[3] = {P.bx0, P.by0, P.bz0}, hi[3] = {P.bx1, P.by1, P.bz1};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const float c = comp(x, a);
-        if (c - lo[a] < P.hf) { w.axis[w.n] = a; w.plane[w.n] = lo[a]; w.nrm[w.n] = 1.f; ++w.n; }
-        else if (hi[a] - c < P.hf) { w.axis[w.n] = a; w.plane[w.n] = hi[a]; w.nrm[w.n] = -1.f; ++w.n; }
-    }
+    w.a0 = w.a1 = w.a2 = 0;
+    w.p0 = w.p1 = w.p2 = 0.f;
+    w.n0 = w.n1 = w.n2 = 0.f;
+    if (x.x - P.bx0 < P.hf) push_wall(w, 0, P.bx0, 1.f);
+    else if (P.bx1 - x.x < P.hf) push_wall(w, 0, P.bx1, -1.f);
+    if (x.y - P.by0 < P.hf) push_wall(w, 1, P.by0, 1.f);
+    else if (P.by1 - x.y < P.hf) push_wall(w, 1, P.by1, -1.f);
+    if (x.z - P.bz0 < P.hf) push_wall(w, 2, P.bz0, 1.f);
+    else if (P.bz1 - x.z < P.hf) push_wall(w, 2, P.bz1, -1.f);
     return w;
+}
+
+// Reflects the offset across one face: component a of r becomes
+// (x_i - plane) + (x_j - plane). False if x_j is h or more from the face.
+__device__ __forceinline__ bool reflect(const Params& P, int a, float plane, float nrm, float4 xi, float4 xj,
+                                        float3& r, float& dp) {
+    const float dj = comp(xj, a) - plane;
+    if (fabsf(dj) >= P.hf) return false;
+    const float v = (comp(xi, a) - plane) + dj;
+    if (a == 0) r.x = v; else if (a == 1) r.y = v; else r.z = v;
+    dp += P.rho0 * (-gcomp(P, a) * nrm) * 2.f * fabsf(dj);
+    return true;
 }
 
 // x_i minus the ghost of x_j across the faces in `mask`; false if a face of
 // the set is h or more from x_j. dp: the ghost's hydrostatic pressure offset.
 __device__ __forceinline__ bool ghost_delta(const Params& P, const Walls& w, int mask, float4 xi, float4 xj, float3& r,
                                             float& dp) {
-    float d[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+    r = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
     dp = 0.f;
-    for (int k = 0; k < w.n; ++k) {
-        if (!((mask >> k) & 1)) continue;
-        const int a = w.axis[k];
-        const float dj = comp(xj, a) - w.plane[k];
-        if (fabsf(dj) >= P.hf) return false;
-        d[a] = (comp(xi, a) - w.plane[k]) + dj;
-        dp += P.rho0 * (-gcomp(P, a) * w.nrm[k]) * 2.f * fabsf(dj);
-    }
-    r = make_float3(d[0], d[1], d[2]);
+    if ((mask & 1) && !reflect(P, w.a0, w.p0, w.n0, xi, xj, r, dp)) return false;
+    if ((mask & 2) && !reflect(P, w.a1, w.p1, w.n1, xi, xj, r, dp)) return false;
+    if ((mask & 4) && !reflect(P, w.a2, w.p2, w.n2, xi, xj, r, dp)) return false;
     return true;
 }
 

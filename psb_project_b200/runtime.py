@@ -35,8 +35,12 @@ EXPORTS = (
     "psb_create", "psb_destroy", "psb_set_stream", "psb_upload", "psb_upload_aos_f64", "psb_download",
     "psb_download_aos_f64", "psb_step", "psb_build_neighbors", "psb_read_field", "psb_get_stats",
     "psb_profile_enable", "psb_profile_read", "psb_profile_reset", "psb_lattice", "psb_status_string",
-    "psb_last_error", "psb_abi_version", "psb_sort_cells_noalloc", "psb_presolve",
+    "psb_last_error", "psb_abi_version", "psb_sort_cells_noalloc", "psb_presolve", "psb_mlp_set_weights",
+    "psb_mlp_get_weights", "psb_mlp_collect", "psb_mlp_dataset", "psb_mlp_train", "psb_mlp_forward",
+    "psb_mlp_loss_grad",
 )
+MLP_PARAMS = 4673       # PSB_MLP_PARAMS
+MLP_IN, MLP_H = 6, 64
 NOALLOC_MAX_N = 262144   # PSB_NOALLOC_MAX_N
 
 
@@ -88,6 +92,13 @@ def lib():
         "psb_abi_version": ([], I32),
         "psb_sort_cells_noalloc": ([P, P, P, P, I32, I32, P], ctypes.c_int),
         "psb_presolve": ([P, I32], ctypes.c_int),
+        "psb_mlp_set_weights": ([P, P], ctypes.c_int),
+        "psb_mlp_get_weights": ([P, P], ctypes.c_int),
+        "psb_mlp_collect": ([P, I32, I64], ctypes.c_int),
+        "psb_mlp_dataset": ([P, ctypes.POINTER(I64), P, P], ctypes.c_int),
+        "psb_mlp_train": ([P, I32, I32, ctypes.c_float, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
+        "psb_mlp_forward": ([P, P, I32, P], ctypes.c_int),
+        "psb_mlp_loss_grad": ([P, P, P, I32, ctypes.POINTER(ctypes.c_float), P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -111,6 +122,30 @@ def lattice(nxyz, spacing, origin, jitter, seed, id0=0) -> np.ndarray:
                            _ptr(out))
     if rc != OK:
         raise PsbError(rc, "psb_lattice")
+    return out
+
+
+def mlp_init_weights(seed: int = 0) -> np.ndarray:
+    """He-uniform initial weights in the psb_mlp layout: W1[64][6], b1[64],
+    W2[64][64], b2[64], W3[64], b3 (biases zero)."""
+    rng = np.random.default_rng(seed)
+    w = np.zeros(MLP_PARAMS, np.float32)
+    o = 0
+    for fan_in, fan_out in ((MLP_IN, MLP_H), (MLP_H, MLP_H), (MLP_H, 1)):
+        lim = np.sqrt(6.0 / fan_in)
+        w[o:o + fan_in * fan_out] = rng.uniform(-lim, lim, fan_in * fan_out) * (0.5 if fan_out == 1 else 1.0)
+        o += fan_in * fan_out + fan_out
+    return w
+
+
+def mlp_unpack(w: np.ndarray):
+    """(W1, b1, W2, b2, W3, b3) views of a flat parameter vector."""
+    o = 0
+    out = []
+    for shape in ((MLP_H, MLP_IN), (MLP_H,), (MLP_H, MLP_H), (MLP_H,), (MLP_H,), (1,)):
+        k = int(np.prod(shape))
+        out.append(w[o:o + k].reshape(shape))
+        o += k
     return out
 
 
@@ -186,6 +221,53 @@ class Simulation:
 
     def presolve(self, iters: int):
         self._check(lib().psb_presolve(self._h, int(iters)), "psb_presolve")
+
+    # -- learned warm start -------------------------------------------------------
+    def mlp_set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        assert w.shape == (MLP_PARAMS,)
+        self._check(lib().psb_mlp_set_weights(self._h, _ptr(w)), "psb_mlp_set_weights")
+
+    def mlp_get_weights(self) -> np.ndarray:
+        w = np.empty(MLP_PARAMS, np.float32)
+        self._check(lib().psb_mlp_get_weights(self._h, _ptr(w)), "psb_mlp_get_weights")
+        return w
+
+    def mlp_collect(self, stride: int, capacity: int = 1 << 22):
+        self._check(lib().psb_mlp_collect(self._h, int(stride), int(capacity)), "psb_mlp_collect")
+
+    def mlp_dataset(self, fetch: bool = True):
+        rows = ctypes.c_int64()
+        self._check(lib().psb_mlp_dataset(self._h, ctypes.byref(rows), None, None), "psb_mlp_dataset")
+        if not fetch:
+            return rows.value, None, None
+        X = np.empty((rows.value, 8), np.float32)
+        T = np.empty(rows.value, np.float32)
+        self._check(lib().psb_mlp_dataset(self._h, ctypes.byref(rows), _ptr(X), _ptr(T)), "psb_mlp_dataset")
+        return rows.value, X, T
+
+    def mlp_train(self, iters: int, batch: int, lr: float, seed: int = 0) -> float:
+        loss = ctypes.c_float()
+        self._check(lib().psb_mlp_train(self._h, int(iters), int(batch), float(lr), int(seed), ctypes.byref(loss)),
+                    "psb_mlp_train")
+        return loss.value
+
+    def mlp_forward(self, X) -> np.ndarray:
+        X8 = np.zeros((X.shape[0], 8), np.float32)
+        X8[:, :X.shape[1]] = X
+        y = np.empty(X.shape[0], np.float32)
+        self._check(lib().psb_mlp_forward(self._h, _ptr(X8), X.shape[0], _ptr(y)), "psb_mlp_forward")
+        return y
+
+    def mlp_loss_grad(self, X, T):
+        X8 = np.zeros((X.shape[0], 8), np.float32)
+        X8[:, :X.shape[1]] = X
+        T = np.ascontiguousarray(T, np.float32)
+        g = np.empty(MLP_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        self._check(lib().psb_mlp_loss_grad(self._h, _ptr(X8), _ptr(T), X.shape[0], ctypes.byref(loss), _ptr(g)),
+                    "psb_mlp_loss_grad")
+        return loss.value, g
 
     def build_neighbors(self):
         self._check(lib().psb_build_neighbors(self._h), "psb_build_neighbors")

@@ -38,6 +38,7 @@ WCSPH = 0
 PCISPH = 1
 WARM_ZERO = 0
 WARM_PREVIOUS = 1
+WARM_LEARNED = 2
 
 
 class PsbScene(ctypes.Structure):
