@@ -70,6 +70,10 @@ typedef struct psb_scene {
     int32_t warm_start;         /* PSB_WARM_* */
     double spacing;             /* rest lattice spacing of the CONFIG-profile PCISPH prototype
                                    (0: (mass/rho0)^(1/3)) */
+    double skin;                /* CONFIG profile: neighbour lists hold every pair within (1 + skin) h,
+                                   so pairs that close in during the step's predictions are in them
+                                   (kernels still cut off at h); cell must be >= (1 + skin) h.
+                                   REF profile: must be 0 (the reference's test is r <= h). */
 } psb_scene;
 
 #define PSB_MAX_ITERS 64

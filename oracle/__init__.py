@@ -44,6 +44,7 @@ class OrcParams(ctypes.Structure):
         ("min_iters", ctypes.c_int32), ("max_iters", ctypes.c_int32),
         ("eta", ctypes.c_double), ("wall_k", ctypes.c_double), ("wall_c", ctypes.c_double),
         ("float_state", ctypes.c_int32), ("warm_start", ctypes.c_int32), ("spacing", ctypes.c_double),
+        ("skin", ctypes.c_double),
     ]
 
 
@@ -151,6 +152,7 @@ def params(scene, *, float_state: bool = False, n: Optional[int] = None) -> OrcP
     p.float_state = 1 if float_state else 0
     p.warm_start = 1 if scene.warm_start else 0
     p.spacing = scene.spacing
+    p.skin = scene.skin
     return p
 
 

@@ -120,6 +120,8 @@ int64_t orc_neighbors(const orc_params* P, const double* pos, int32_t cap, int32
     orc_cell_keys(n, pos, P->grid_min, P->cell, P->dims, keys, NULL);
     sort_by_key(n, keys, ncells, perm, start);
     const int nx = P->dims[0], ny = P->dims[1], nz = P->dims[2];
+    /* list cut-off: h, or (1 + skin) h in the config profile */
+    const double hl = P->profile == ORC_PROFILE_CONFIG ? P->h * (1.0 + P->skin) : P->h;
     int64_t total = 0;
     int overflow = 0;
 #pragma omp parallel for reduction(+ : total) reduction(| : overflow) schedule(dynamic, 256)
@@ -138,7 +140,7 @@ int64_t orc_neighbors(const orc_params* P, const double* pos, int32_t cap, int32
                     const uint32_t c = (uint32_t)a + (uint32_t)j * nx + (uint32_t)k * nx * ny;
                     for (int32_t t = start[c]; t < start[c + 1]; ++t) {
                         const int32_t jd = perm[t];
-                        if (is_neighbor(&pos[3 * (size_t)i], &pos[3 * (size_t)jd], P->h)) {
+                        if (is_neighbor(&pos[3 * (size_t)i], &pos[3 * (size_t)jd], hl)) {
                             if (list) {
                                 if (cnt < cap) list[(size_t)i * cap + cnt] = jd;
                                 else overflow = 1;
@@ -171,27 +173,39 @@ static inline double dmax(double a, double b) { return a > b ? a : b; }
  * neighbour list -- self included -- yields every ghost. At a flat wall the
  * ghosts continue the fluid exactly: a uniform pressure exerts no net force
  * and the rest lattice keeps its rest density up to the wall. */
-typedef struct { int n; int axis[3]; double plane[3]; } walls_t;
+typedef struct { int n; int axis[3]; double plane[3]; double nrm[3]; } walls_t;
 
 static void near_walls(const orc_params* P, const double* x, walls_t* w) {
     const double h = P->h;
     w->n = 0;
     for (int e = 0; e < 3; ++e) {
         const double lo = (double)P->box_min[e], hi = (double)P->box_max[e];
-        if (x[e] - lo < h) { w->axis[w->n] = e; w->plane[w->n] = lo; w->n++; }
-        else if (hi - x[e] < h) { w->axis[w->n] = e; w->plane[w->n] = hi; w->n++; }
+        if (x[e] - lo < h) { w->axis[w->n] = e; w->plane[w->n] = lo; w->nrm[w->n] = 1.0; w->n++; }
+        else if (hi - x[e] < h) { w->axis[w->n] = e; w->plane[w->n] = hi; w->nrm[w->n] = -1.0; w->n++; }
     }
 }
 
-/* Ghost of xj for face subset `mask` of w (bit k = face k), written to g;
- * returns 0 when some face of the subset is h or more from xj. */
-static int ghost(const walls_t* w, int mask, const double* xj, double h, double* g) {
-    g[0] = xj[0]; g[1] = xj[1]; g[2] = xj[2];
+/* x_i minus the ghost of x_j across the faces of subset `mask` (bit k = face
+ * k of w), written to dv. With d = n.(x - plane) the distances on the box
+ * side (n the inward normal), the reflected component is n (d_i + d_j), both
+ * clamped at 0: a particle pushed through a face still sees its ghosts on
+ * the wall side. dpg gets the ghost's hydrostatic pressure offset
+ * rho0 (-g.n) 2 d_j per face. Returns 0 when x_j is h or more inside. */
+static int ghost(const orc_params* P, const walls_t* w, int mask, const double* xi, const double* xj, double h,
+                 double* dv, double* dpg) {
+    dv[0] = xi[0] - xj[0]; dv[1] = xi[1] - xj[1]; dv[2] = xi[2] - xj[2];
+    *dpg = 0.0;
     for (int k = 0; k < w->n; ++k) {
         if (!(mask >> k & 1)) continue;
         const int e = w->axis[k];
-        if (fabs(xj[e] - w->plane[k]) >= h) return 0;
-        g[e] = 2.0 * w->plane[k] - xj[e];
+        const double nrm = w->nrm[k];
+        double dj = nrm * (xj[e] - w->plane[k]);
+        if (dj < 0) dj = 0;
+        if (dj >= h) return 0;
+        double di = nrm * (xi[e] - w->plane[k]);
+        if (di < 0) di = 0;
+        dv[e] = nrm * (di + dj);
+        *dpg += P->rho0 * (-(double)P->gravity[e] * nrm) * 2.0 * dj;
     }
     return 1;
 }
@@ -216,9 +230,8 @@ void orc_density(const orc_params* P, const double* pos, const int32_t* counts, 
             for (int mask = 1; mask < (1 << w.n); ++mask)
                 for (int32_t t = 0; t < counts[i]; ++t) {
                     const int32_t j = list[(size_t)i * cap + t];
-                    double gx[3];
-                    if (!ghost(&w, mask, &pos[3 * j], h, gx)) continue;
-                    double dv[3] = {pos[3 * i] - gx[0], pos[3 * i + 1] - gx[1], pos[3 * i + 2] - gx[2]};
+                    double dv[3], dpg;
+                    if (!ghost(P, &w, mask, &pos[3 * i], &pos[3 * j], h, dv, &dpg)) continue;
                     const double d = len3(dv);
                     if (d >= h) continue;
                     s += (315 / (64 * PI_D * pow(h, 9))) * pow((h * h) - (d * d), 3) * m;
@@ -314,22 +327,13 @@ static void pressure_forces(const orc_params* P, const double* pos, const double
             for (int mask = 1; mask < (1 << w.n); ++mask)
                 for (int32_t t = 0; t < counts[i]; ++t) {
                     const int32_t j = list[(size_t)i * cap + t];
-                    double gx[3];
-                    if (!ghost(&w, mask, &pos[3 * j], h, gx)) continue;
-                    const double dv[3] = {pos[3 * i] - gx[0], pos[3 * i + 1] - gx[1], pos[3 * i + 2] - gx[2]};
+                    double dv[3], dpg;
+                    if (!ghost(P, &w, mask, &pos[3 * i], &pos[3 * j], h, dv, &dpg)) continue;
                     const double d = len3(dv);
                     if (!(d > 0) || d >= h) continue;
                     const double inv = 1.0 / d;
-                    /* the ghost continues the hydrostatic pressure across the
-                     * face: p_j + rho0 (-g . n) 2 d_j for each reflecting face */
-                    double pg = p[j];
-                    for (int k = 0; k < w.n; ++k) {
-                        if (!(mask >> k & 1)) continue;
-                        const int e = w.axis[k];
-                        const double nrm = (w.plane[k] == (double)P->box_min[e]) ? 1.0 : -1.0;
-                        pg += P->rho0 * (-(double)P->gravity[e] * nrm) * 2.0 * fabs(pos[3 * j + e] - w.plane[k]);
-                    }
-                    const double pV2 = pg * ir0;
+                    /* the ghost continues the hydrostatic pressure across the face */
+                    const double pV2 = (p[j] + dpg) * ir0;
                     const double a = PI_D * pow(h, 6);
                     const double sc = -45 * pow(h - d, 2) / a;
                     for (int e = 0; e < 3; ++e) acc[e] = acc[e] + (dv[e] * inv) * sc * (pV1 + pV2) * m;
@@ -406,13 +410,12 @@ static void pressure_update(const orc_params* P, const double* pos, const double
     }
 }
 
-/* Penalty walls (config profile): a = K*depth - C*v_n along each violated
- * wall normal, depth measured from the wall offset by the particle radius. */
+/* Penalty walls (config profile): a = K*depth - C*v_n along each axis on
+ * which x lies outside the box faces (an uploaded state; the projection
+ * below keeps stepped particles inside). */
 static void wall_accel(const orc_params* P, const double* x, const double* v, double* a) {
     for (int e = 0; e < 3; ++e) {
         a[e] = 0.0;
-        /* no-penetration backstop at the faces; the wall boundary above
-         * keeps particles off them in normal flow */
         const float lo = P->box_min[e], hi = P->box_max[e];
         if (x[e] < lo) a[e] += P->wall_k * (lo - x[e]) - P->wall_c * v[e];
         if (x[e] > hi) a[e] += -P->wall_k * (x[e] - hi) - P->wall_c * v[e];
@@ -420,7 +423,12 @@ static void wall_accel(const orc_params* P, const double* x, const double* v, do
 }
 
 /* collisionBox (BoxCollision_Kernel.cu:7-34) on (pos, vel_ap): the bounds
- * Max - r and Min + r are float expressions there. */
+ * Max - r and Min + r are float expressions there. PCISPH in both profiles:
+ * in the config profile it keeps every particle at least r from each face,
+ * where its own ghost still pushes back (on or behind a face a particle
+ * meets its ghost at distance 0, which exerts no force, and its density
+ * error could not be corrected). Config WCSPH keeps the penalty walls its
+ * scene states. */
 static void box_project(const orc_params* P, double* x, double* v) {
     const float r = P->particle_radius;
     double pI[3] = {x[0], x[1], x[2]}, nI[3] = {0, 0, 0};
@@ -515,7 +523,7 @@ static int step_wcsph(const orc_params* P, orc_state* S, orc_stats* st, double* 
             vap[e] = RND(P, vap[e] + (F * inv + aw[e]) * dt);
             x[e] = RND(P, x[e] + vap[e] * dt);
         }
-        if (ref) box_project(P, x, vap);
+        if (ref) box_project(P, x, vap);   /* config WCSPH: penalty walls only */
         for (int e = 0; e < 3; ++e) {
             x[e] = RND(P, x[e]);
             vap[e] = RND(P, vap[e]);
@@ -597,7 +605,7 @@ static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double*
         double* vap = &S->vel_ap[3 * i];
         const double vav[3] = {vap[0], vap[1], vap[2]};
         for (int e = 0; e < 3; ++e) { x[e] = xs[3 * i + e]; vap[e] = vs[3 * i + e]; }
-        if (ref) box_project(P, x, vap);
+        box_project(P, x, vap);
         for (int e = 0; e < 3; ++e) {
             x[e] = RND(P, x[e]);
             vap[e] = RND(P, vap[e]);

@@ -37,6 +37,7 @@ typedef struct orc_params {
     int32_t float_state;            /* round stored state to float like the GPU path */
     int32_t warm_start;             /* PCISPH: 0 start from p = 0, 1 start from the given p */
     double spacing;                 /* config PCISPH prototype lattice spacing (0: (m/rho0)^(1/3)) */
+    double skin;                    /* config: lists hold pairs within (1 + skin) h */
 } orc_params;
 
 /* Config-profile PCISPH pressure factor delta = 1 / (beta (|sum gradW|^2 +

@@ -193,7 +193,11 @@ int validate(const psb_scene* s, std::string& why) {
     if (!s) { why = "scene is NULL"; return PSB_EINVAL; }
     if (s->n_max <= 0) { why = "n_max must be positive"; return PSB_EINVAL; }
     if (!(s->h > 0) || !(s->mass > 0) || !(s->rho0 > 0) || !(s->dt > 0)) { why = "h, mass, rho0, dt must be positive"; return PSB_EINVAL; }
-    if (!(s->cell > 0) || (double)s->cell < s->h * (1.0 - 1e-6)) { why = "cell must be >= h (27-cell walk)"; return PSB_EINVAL; }
+    if (!(s->skin >= 0) || (s->profile == PSB_PROFILE_REF && s->skin != 0)) { why = "skin must be >= 0 (0 in the reference profile)"; return PSB_EINVAL; }
+    if (!(s->cell > 0) || (double)s->cell < s->h * (1.0 + s->skin) * (1.0 - 1e-6)) {
+        why = "cell must be >= (1 + skin) h (27-cell walk)";
+        return PSB_EINVAL;
+    }
     for (int a = 0; a < 3; ++a) {
         if (s->dims[a] <= 0) { why = "dims must be positive"; return PSB_EINVAL; }
         if (!(s->box_max[a] > s->box_min[a])) { why = "box_max must exceed box_min"; return PSB_EINVAL; }
@@ -230,8 +234,10 @@ Params derive(const psb_scene& s) {
     P.g.cell = s.cell;
     P.g.nx = s.dims[0]; P.g.ny = s.dims[1]; P.g.nz = s.dims[2];
     P.cap = s.nbr_cap ? s.nbr_cap : 128;
-    P.h = h;
-    const float h2f = (float)(h * h);
+    // list cut-off: the reference's h, or (1 + skin) h in the config profile
+    const double hl = s.profile == PSB_PROFILE_CONFIG ? h * (1.0 + s.skin) : h;
+    P.h = hl;
+    const float h2f = (float)(hl * hl);
     P.h2_lo = h2f * (1.f - 1e-5f);
     P.h2_hi = h2f * (1.f + 1e-5f);
     P.h2 = h2f;
@@ -264,12 +270,8 @@ Params derive(const psb_scene& s) {
     P.wlo_z = s.box_min[2] + s.particle_radius;
     P.whi_x = s.box_max[0] - s.particle_radius; P.whi_y = s.box_max[1] - s.particle_radius;
     P.whi_z = s.box_max[2] - s.particle_radius;
-    P.wall_k = (float)s.wall_k;
+    P.wall_k = (float)s.wall_k;     // config: penalty outside the faces (bx0..bz1)
     P.wall_c = (float)s.wall_c;
-    if (!P.ref) {   // config: the penalty backstop acts at the faces themselves
-        P.wlo_x = s.box_min[0]; P.wlo_y = s.box_min[1]; P.wlo_z = s.box_min[2];
-        P.whi_x = s.box_max[0]; P.whi_y = s.box_max[1]; P.whi_z = s.box_max[2];
-    }
     P.bx0 = s.box_min[0]; P.by0 = s.box_min[1]; P.bz0 = s.box_min[2];
     P.bx1 = s.box_max[0]; P.by1 = s.box_max[1]; P.bz1 = s.box_max[2];
     const double ws = s.spacing > 0 ? s.spacing : std::cbrt(m / s.rho0);

@@ -23,6 +23,7 @@
 // with shuffles before one atomic add per warp.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 
 #include "psb_internal.cuh"
@@ -53,6 +54,7 @@ __global__ void __launch_bounds__(kBlock) k_features(Params P, const float4* __r
     const int cnt = min(counts[t], P.cap);
     float div = 0.f;
     float3 gr = make_float3(0.f, 0.f, 0.f);
+#pragma unroll 4
     for (int c = 0; c < cnt; ++c) {
         const int j = list[(size_t)c * P.n + t];
         const float4 xj = pos[j];
@@ -83,64 +85,126 @@ __global__ void __launch_bounds__(kBlock) k_features(Params P, const float4* __r
 }
 
 // ---- inference -----------------------------------------------------------------
-// One thread per particle; the BF16 weights, widened to FP32, in shared memory
-// (every lane of a warp reads the same weight: broadcast).
-__global__ void __launch_bounds__(kBlock) k_mlp_infer(int n, const float* __restrict__ feats,
-                                                      const __nv_bfloat16* __restrict__ w, float p_scale,
-                                                      float2* __restrict__ rp) {
-    __shared__ float sw[kMlpParams];
-    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) sw[i] = __bfloat162float(w[i]);
-    __syncthreads();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    float x[kIn];
-#pragma unroll
-    for (int k = 0; k < kIn; ++k) x[k] = bf(feats[(size_t)t * 8 + k]);
-    float h1[kH];
-#pragma unroll
-    for (int j = 0; j < kH; ++j) {
-        float z = sw[oB1 + j];
-#pragma unroll
-        for (int k = 0; k < kIn; ++k) z = fmaf(sw[oW1 + j * kIn + k], x[k], z);
-        h1[j] = bf(silu(z));
-    }
-    float y = sw[oB3];
-    for (int j = 0; j < kH; ++j) {
-        float z = sw[oB2 + j];
-#pragma unroll
-        for (int k = 0; k < kH; ++k) z = fmaf(sw[oW2 + j * kH + k], h1[k], z);
-        y = fmaf(sw[oW3 + j], bf(silu(z)), y);
-    }
-    rp[t].y = fmaxf(0.f, y) * p_scale;
+// Tensor-core inference: one warp evaluates 16 particles per pass with
+// mma.sync.m16n8k16 (BF16 inputs, FP32 accumulation). Layer 1 is a
+// [16 x 16] x [16 x 64] product (6 inputs, 10 zero pads), layer 2
+// [16 x 64] x [64 x 64]; the layer-1 accumulator fragments, rounded to BF16,
+// are exactly the A fragments of layer 2 (rows groupID and groupID + 8,
+// columns 2 tig + {0, 1} of each 8-wide tile). The output layer (64 -> 1) is
+// a per-thread dot product finished with two shuffles.
+// Shared memory: W1 and W2 as BF16 pairs, rows padded to 36 words so that
+// the eight groups of a B-fragment load fall in distinct banks.
+constexpr int kW2Stride = 36;     // 32-bit words per padded 64-wide row
+constexpr int kW1Stride = 4;      // 8 BF16 per row (6 used)
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// Forward on arbitrary feature rows (host-facing evaluation).
-__global__ void __launch_bounds__(kBlock) k_mlp_forward(int n, const float* __restrict__ X, int stride,
-                                                        const __nv_bfloat16* __restrict__ w, float* __restrict__ y_out) {
-    __shared__ float sw[kMlpParams];
-    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) sw[i] = __bfloat162float(w[i]);
+__device__ __forceinline__ void mma_bf16(float* c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ float silu_fast(float z) { return z / (1.f + __expf(-z)); }
+
+// y_raw != nullptr: write the raw output y there (host-facing evaluation)
+// instead of the initial pressure max(0, y) p_scale into rp.
+__global__ void __launch_bounds__(256) k_mlp_infer_mma(int n, const float* __restrict__ feats,
+                                                       const __nv_bfloat16* __restrict__ w, float p_scale,
+                                                       float2* __restrict__ rp, float* __restrict__ y_raw) {
+    __shared__ uint32_t sW1[kH * kW1Stride];
+    __shared__ uint32_t sW2[kH * kW2Stride];
+    __shared__ float sB1[kH], sB2[kH], sW3[kH];
+    __shared__ float sB3;
+    for (int i = threadIdx.x; i < kH * kW1Stride; i += blockDim.x) {
+        const int r = i / kW1Stride, k = 2 * (i % kW1Stride);
+        const float lo = k < kIn ? __bfloat162float(w[oW1 + r * kIn + k]) : 0.f;
+        const float hi = k + 1 < kIn ? __bfloat162float(w[oW1 + r * kIn + k + 1]) : 0.f;
+        sW1[i] = pack_bf16(lo, hi);
+    }
+    for (int i = threadIdx.x; i < kH * 32; i += blockDim.x) {
+        const int r = i / 32, k = 2 * (i % 32);
+        sW2[r * kW2Stride + i % 32] =
+            pack_bf16(__bfloat162float(w[oW2 + r * kH + k]), __bfloat162float(w[oW2 + r * kH + k + 1]));
+    }
+    for (int i = threadIdx.x; i < kH; i += blockDim.x) {
+        sB1[i] = __bfloat162float(w[oB1 + i]);
+        sB2[i] = __bfloat162float(w[oB2 + i]);
+        sW3[i] = __bfloat162float(w[oW3 + i]);
+    }
+    if (threadIdx.x == 0) sB3 = __bfloat162float(w[oB3]);
     __syncthreads();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    float x[kIn];
+
+    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const int warps_total = gridDim.x * (blockDim.x >> 5);
+    for (int tile = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tile * 16 < n; tile += warps_total) {
+        const int r0 = tile * 16 + gid, r1 = r0 + 8;
+        // layer 1: A = features (cols 0..5 real)
+        uint32_t a0 = 0u, a1 = 0u;
+        {
+            const int k = 2 * tig;
+            if (k < kIn) {
+                const float f00 = r0 < n ? feats[(size_t)r0 * 8 + k] : 0.f;
+                const float f01 = r0 < n ? feats[(size_t)r0 * 8 + k + 1] : 0.f;
+                const float f10 = r1 < n ? feats[(size_t)r1 * 8 + k] : 0.f;
+                const float f11 = r1 < n ? feats[(size_t)r1 * 8 + k + 1] : 0.f;
+                a0 = pack_bf16(f00, k + 1 < kIn ? f01 : 0.f);
+                a1 = pack_bf16(f10, k + 1 < kIn ? f11 : 0.f);
+            }
+        }
+        float z1[8][4];
 #pragma unroll
-    for (int k = 0; k < kIn; ++k) x[k] = bf(X[(size_t)t * stride + k]);
-    float h1[kH];
+        for (int nt = 0; nt < 8; ++nt) {
+            const int col = nt * 8 + 2 * tig;
+            z1[nt][0] = sB1[col]; z1[nt][1] = sB1[col + 1];
+            z1[nt][2] = sB1[col]; z1[nt][3] = sB1[col + 1];
+            const uint32_t b0 = sW1[(nt * 8 + gid) * kW1Stride + tig];   // k = 2 tig .. 2 tig + 1
+            mma_bf16(z1[nt], a0, a1, 0u, 0u, b0, 0u);
+        }
+        // layer 2: A fragments from layer 1's accumulators
+        uint32_t h1[4][4];
 #pragma unroll
-    for (int j = 0; j < kH; ++j) {
-        float z = sw[oB1 + j];
+        for (int ks = 0; ks < 4; ++ks) {
+            h1[ks][0] = pack_bf16(silu_fast(z1[2 * ks][0]), silu_fast(z1[2 * ks][1]));
+            h1[ks][1] = pack_bf16(silu_fast(z1[2 * ks][2]), silu_fast(z1[2 * ks][3]));
+            h1[ks][2] = pack_bf16(silu_fast(z1[2 * ks + 1][0]), silu_fast(z1[2 * ks + 1][1]));
+            h1[ks][3] = pack_bf16(silu_fast(z1[2 * ks + 1][2]), silu_fast(z1[2 * ks + 1][3]));
+        }
+        float y0 = 0.f, y1 = 0.f;
 #pragma unroll
-        for (int k = 0; k < kIn; ++k) z = fmaf(sw[oW1 + j * kIn + k], x[k], z);
-        h1[j] = bf(silu(z));
+        for (int nt = 0; nt < 8; ++nt) {
+            const int col = nt * 8 + 2 * tig;
+            float c[4] = {sB2[col], sB2[col + 1], sB2[col], sB2[col + 1]};
+            const uint32_t* wrow = sW2 + (nt * 8 + gid) * kW2Stride;
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks)
+                mma_bf16(c, h1[ks][0], h1[ks][1], h1[ks][2], h1[ks][3], wrow[8 * ks + tig], wrow[8 * ks + 4 + tig]);
+            // output layer on the BF16-rounded activations
+            const float w30 = sW3[col], w31 = sW3[col + 1];
+            y0 = fmaf(w30, bf(silu_fast(c[0])), y0);
+            y0 = fmaf(w31, bf(silu_fast(c[1])), y0);
+            y1 = fmaf(w30, bf(silu_fast(c[2])), y1);
+            y1 = fmaf(w31, bf(silu_fast(c[3])), y1);
+        }
+        y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
+        y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+        if (tig == 0) {
+            if (y_raw) {
+                if (r0 < n) y_raw[r0] = y0 + sB3;
+                if (r1 < n) y_raw[r1] = y1 + sB3;
+            } else {
+                if (r0 < n) rp[r0].y = fmaxf(0.f, y0 + sB3) * p_scale;
+                if (r1 < n) rp[r1].y = fmaxf(0.f, y1 + sB3) * p_scale;
+            }
+        }
     }
-    float y = sw[oB3];
-    for (int j = 0; j < kH; ++j) {
-        float z = sw[oB2 + j];
-#pragma unroll
-        for (int k = 0; k < kH; ++k) z = fmaf(sw[oW2 + j * kH + k], h1[k], z);
-        y = fmaf(sw[oW3 + j], bf(silu(z)), y);
-    }
-    y_out[t] = y;
 }
 
 // ---- training ---------------------------------------------------------------------
@@ -288,11 +352,21 @@ void launch_features(cudaStream_t st, const Params& P, const float4* pos, const 
 }
 
 void launch_mlp_infer(cudaStream_t st, int n, const float* feats, const void* wbf, float p_scale, float2* rp) {
-    if (n > 0) k_mlp_infer<<<grid_of(n), kBlock, 0, st>>>(n, feats, (const __nv_bfloat16*)wbf, p_scale, rp);
+    if (n <= 0) return;
+    const int tiles = (n + 15) / 16;
+    const int blocks = std::min((tiles + 7) / 8, 148 * 8);      // 8 warps per block, grid-stride over tiles
+    k_mlp_infer_mma<<<blocks, 256, 0, st>>>(n, feats, (const __nv_bfloat16*)wbf, p_scale, rp, nullptr);
 }
 
+
+// Host-facing forward through the tensor-core kernel the warm start uses
+// (rows of stride 8).
 void launch_mlp_forward(cudaStream_t st, int n, const float* X, int stride, const void* wbf, float* y) {
-    if (n > 0) k_mlp_forward<<<grid_of(n), kBlock, 0, st>>>(n, X, stride, (const __nv_bfloat16*)wbf, y);
+    if (n <= 0) return;
+    (void)stride;
+    const int tiles = (n + 15) / 16;
+    const int blocks = std::min((tiles + 7) / 8, 148 * 8);
+    k_mlp_infer_mma<<<blocks, 256, 0, st>>>(n, X, (const __nv_bfloat16*)wbf, 1.f, nullptr, y);
 }
 
 void launch_mlp_grad(cudaStream_t st, int batch, const float* X, const float* T, const uint32_t* sel, const void* wbf,

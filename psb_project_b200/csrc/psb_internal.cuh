@@ -33,7 +33,8 @@ struct Params {
     int n;
     int cap;            // neighbour slots per particle
     Grid g;
-    double h;           // exact neighbour test: sqrt(d.d) <= h in FP64
+    double h;           // list cut-off of the exact neighbour test sqrt(d.d) <= h in FP64
+                        // (reference: h; config: (1 + skin) h)
     float h2_lo, h2_hi; // FP32 d^2 outside [h2_lo, h2_hi] is decided without the FP64 test
     float h2, inv_h, inv_h2;
     float k_rho;        // 315 m / (64 pi h^3):           rho = k_rho * sum (1-q)^3

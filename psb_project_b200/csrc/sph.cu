@@ -51,16 +51,18 @@ __device__ __forceinline__ float density_deviation(const Params& P, const Kahan&
 
 __device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
 
-// Penalty walls (config profile): a = K*depth - C*v along each violated axis.
+// Penalty walls (config profile): a = K*depth - C*v along each axis on which
+// x lies outside the box (a state uploaded outside it; the projection below
+// keeps stepped particles inside).
 __device__ __forceinline__ float3 wall_accel(const Params& P, float4 x, float4 v) {
     float3 a = make_float3(0.f, 0.f, 0.f);
     if (P.ref) return a;
-    if (x.x < P.wlo_x) a.x += P.wall_k * (P.wlo_x - x.x) - P.wall_c * v.x;
-    if (x.x > P.whi_x) a.x += -P.wall_k * (x.x - P.whi_x) - P.wall_c * v.x;
-    if (x.y < P.wlo_y) a.y += P.wall_k * (P.wlo_y - x.y) - P.wall_c * v.y;
-    if (x.y > P.whi_y) a.y += -P.wall_k * (x.y - P.whi_y) - P.wall_c * v.y;
-    if (x.z < P.wlo_z) a.z += P.wall_k * (P.wlo_z - x.z) - P.wall_c * v.z;
-    if (x.z > P.whi_z) a.z += -P.wall_k * (x.z - P.whi_z) - P.wall_c * v.z;
+    if (x.x < P.bx0) a.x += P.wall_k * (P.bx0 - x.x) - P.wall_c * v.x;
+    if (x.x > P.bx1) a.x += -P.wall_k * (x.x - P.bx1) - P.wall_c * v.x;
+    if (x.y < P.by0) a.y += P.wall_k * (P.by0 - x.y) - P.wall_c * v.y;
+    if (x.y > P.by1) a.y += -P.wall_k * (x.y - P.by1) - P.wall_c * v.y;
+    if (x.z < P.bz0) a.z += P.wall_k * (P.bz0 - x.z) - P.wall_c * v.z;
+    if (x.z > P.bz1) a.z += -P.wall_k * (x.z - P.bz1) - P.wall_c * v.z;
     return a;
 }
 
@@ -104,15 +106,19 @@ __device__ __forceinline__ Walls near_walls(const Params& P, float4 x) {
     return w;
 }
 
-// Reflects the offset across one face: component a of r becomes
-// (x_i - plane) + (x_j - plane). False if x_j is h or more from the face.
+// Reflects the offset across one face: with d = nrm (x - plane) the
+// distances on the box side, component a of r becomes nrm (d_i + d_j), both
+// clamped at 0 so that a particle pushed through the face still sees its
+// ghosts on the wall side (unclamped, its own ghost would push it further
+// out). False if x_j is h or more inside.
 __device__ __forceinline__ bool reflect(const Params& P, int a, float plane, float nrm, float4 xi, float4 xj,
                                         float3& r, float& dp) {
-    const float dj = comp(xj, a) - plane;
-    if (fabsf(dj) >= P.hf) return false;
-    const float v = (comp(xi, a) - plane) + dj;
+    const float dj = fmaxf(nrm * (comp(xj, a) - plane), 0.f);
+    if (dj >= P.hf) return false;
+    const float di = fmaxf(nrm * (comp(xi, a) - plane), 0.f);
+    const float v = nrm * (di + dj);
     if (a == 0) r.x = v; else if (a == 1) r.y = v; else r.z = v;
-    dp += P.rho0 * (-gcomp(P, a) * nrm) * 2.f * fabsf(dj);
+    dp += P.rho0 * (-gcomp(P, a) * nrm) * 2.f * dj;
     return true;
 }
 
@@ -134,7 +140,8 @@ __device__ __forceinline__ void ghost_density(const Params& P, int t, float4 xi,
     const Walls w = near_walls(P, xi);
     if (!w.n) return;
     for (int mask = 1; mask < (1 << w.n); ++mask)
-        for (int c = 0; c < cnt; ++c) {
+    #pragma unroll 4
+    for (int c = 0; c < cnt; ++c) {
             const float4 xj = pos[list[(size_t)c * P.n + t]];
             float3 r;
             float dp;
@@ -154,7 +161,8 @@ __device__ __forceinline__ void ghost_pressure(const Params& P, int t, float4 xi
     if (!w.n) return;
     const float ir0 = 1.f / (P.rho0 * P.rho0);
     for (int mask = 1; mask < (1 << w.n); ++mask)
-        for (int c = 0; c < cnt; ++c) {
+    #pragma unroll 4
+    for (int c = 0; c < cnt; ++c) {
             const int j = list[(size_t)c * P.n + t];
             const float4 xj = pos[j];
             float3 r;
@@ -171,7 +179,12 @@ __device__ __forceinline__ void ghost_pressure(const Params& P, int t, float4 xi
 
 // collisionBox (BoxCollision_Kernel.cu:7-34) with restitution 0: clamp into
 // [Min+r, Max-r] (upper bounds tested first, lower bounds win), then remove
-// the velocity component along the normalised sum of wall normals.
+// the velocity component along the normalised sum of wall normals. PCISPH
+// in both profiles: in the config profile it keeps every particle at least r
+// from each face, where its own ghost still pushes back (a particle on or
+// behind a face meets its ghost at distance 0, which exerts no force, and
+// its density error could not be corrected). Config WCSPH keeps the penalty
+// walls its scene states.
 __device__ __forceinline__ void box_project(const Params& P, float3& x, float3& v) {
     float3 pI = x, nI = make_float3(0.f, 0.f, 0.f);
     if (x.x >= P.whi_x) { pI.x = P.whi_x; nI.x = -1.f; }
@@ -203,6 +216,7 @@ __global__ void __launch_bounds__(kBlock) k_density_x(Params P, const float4* __
     const float4 xi = pos[t];
     const int cnt = min(counts[t], P.cap);
     Kahan acc;
+#pragma unroll 4
     for (int c = 0; c < cnt; ++c) {
         const float4 xj = pos[list[(size_t)c * P.n + t]];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
@@ -250,6 +264,7 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
     const float ir0 = 1.f / (P.rho0 * P.rho0);
     const float pVi = WITH_PRESSURE ? (P.ref ? rpi.y / (rpi.x * rpi.x) : rpi.y * ir0) : 0.f;
     const int cnt = min(counts[t], P.cap);
+#pragma unroll 4
     for (int c = 0; c < cnt; ++c) {
         const int j = list[(size_t)c * P.n + t];
         const float4 xj = pos[j];
@@ -321,7 +336,7 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params P, const float4* 
                                  f.z * ir + P.k_grad * S.ap.z + aw.z);
     float3 v = make_float3(vh.x + a.x * P.dt, vh.y + a.y * P.dt, vh.z + a.z * P.dt);
     float3 x = make_float3(xi.x + v.x * P.dt, xi.y + v.y * P.dt, xi.z + v.z * P.dt);
-    if (P.ref) box_project(P, x, v);
+    if (P.ref) box_project(P, x, v);   // config WCSPH: penalty walls only
     pos_out[t] = make_float4(x.x, x.y, x.z, 0.f);
     vap_out[t] = make_float4(v.x, v.y, v.z, 0.f);
     vel_out[t] = make_float4((vh.x + v.x) * 0.5f, (vh.y + v.y) * 0.5f, (vh.z + v.z) * 0.5f, 0.f);
@@ -367,7 +382,8 @@ __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* 
         Kahan acc;
         float3 T1 = make_float3(0.f, 0.f, 0.f);
         float T2 = 0.f;
-        for (int c = 0; c < cnt; ++c) {
+    #pragma unroll 4
+    for (int c = 0; c < cnt; ++c) {
             const float4 xj = xs[list[(size_t)c * P.n + t]];
             const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
             const float r2 = dx * dx + dy * dy + dz * dz;
@@ -433,6 +449,7 @@ __global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const fl
     const float pVi = P.ref ? ri.y / (ri.x * ri.x) : ri.y * ir0;
     const int cnt = min(counts[t], P.cap);
     float3 acc = make_float3(0.f, 0.f, 0.f);
+#pragma unroll 4
     for (int c = 0; c < cnt; ++c) {
         const int j = list[(size_t)c * P.n + t];
         const float4 xj = geo[j];
@@ -469,7 +486,7 @@ __global__ void __launch_bounds__(kBlock) k_pci_commit(Params P, const float4* _
     if (t >= P.n) return;
     float3 x = f3(xs[t]), v = f3(vs[t]);
     const float4 vh = vap[t];
-    if (P.ref) box_project(P, x, v);
+    box_project(P, x, v);
     pos[t] = make_float4(x.x, x.y, x.z, 0.f);
     vap[t] = make_float4(v.x, v.y, v.z, 0.f);
     vel[t] = make_float4((vh.x + v.x) * 0.5f, (vh.y + v.y) * 0.5f, (vh.z + v.z) * 0.5f, 0.f);

@@ -39,7 +39,9 @@ def test_ghost_walls_keep_rest_density_at_faces_edges_corners():
 
 
 def test_hydrostatic_column_bottom_layer_balance():
-    sc = column().replace(warm_start=P.WARM_PREVIOUS, max_iters=0, min_iters=0)
+    # the projection bound (particle radius) below the wall layer, which sits
+    # at s/2 from the faces: the ghosts alone hold the column
+    sc = column().replace(warm_start=P.WARM_PREVIOUS, max_iters=0, min_iters=0, particle_radius=0.00125)
     pos = oracle.scene_positions(sc)
     ytop = pos[:, 1].max() + 0.0025
     o = oracle.OracleSim(sc, pos, pressure=1000 * 9.81 * (ytop - pos[:, 1]))

@@ -20,7 +20,16 @@ Tolerances (written here, applied below):
     max. The pressure accumulates delta (rho* - rho0) over the corrections;
     an FP32 rounding of 3e-8 of a density-level term (kernel constant, wall
     term) is 3e-5 kg/m^3 of rho* - rho0, times delta ~ 34 and 4-5
-    corrections: ~4e-5 of the pressure scale.
+    corrections: ~4e-5 of the pressure scale. The velocities of such a step
+    carry that pressure's error (a_p is linear in p): 1e-4 as well;
+  * reference-profile PCISPH pressure against the reference's own kernels:
+    2e-5 of its max. Those kernels keep x* in FP64; the GPU stores x* in
+    FP32, a half-ulp of 3.7e-9 m at 0.1 m. At h = 0.02, m = 1e-3 one pair
+    moves rho by 1.6e4 kg/m^3 per metre at r = h/2, so ~30 pairs with
+    independent roundings move rho* by ~5e-4 kg/m^3, 1-2e-5 of the step's
+    rho* - rho0 of a few tens of kg/m^3, which the pressure increment
+    inherits. The oracle, which rounds x* to FP32 like the GPU, agrees to
+    1e-5 on the same step.
 The oracle runs with float_state=True (it rounds every array the GPU stores
 in FP32 at the same points) for multi-step comparisons.
 """
@@ -37,6 +46,8 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-5
 TOL_V = 3e-5
 TOL_P_CONFIG_PCI = 1e-4
+TOL_V_CONFIG_PCI = 1e-4
+TOL_P_REF_FP64 = 2e-5
 
 
 def rel_norm(a, b):
@@ -132,11 +143,11 @@ def test_density_at_start_positions(profile):
     sim.close()
 
 
-def _compare_step(sim, orc, x0, p_tol=TOL):
+def _compare_step(sim, orc, x0, p_tol=TOL, v_tol=TOL_V):
     out = sim.download()
     assert_positions(out["pos"], orc.pos, x0)
-    assert rel_norm(out["vel_half"], orc.vel_half) <= TOL_V
-    assert rel_norm(out["vel"], orc.vel) <= TOL_V
+    assert rel_norm(out["vel_half"], orc.vel_half) <= v_tol
+    assert rel_norm(out["vel"], orc.vel) <= v_tol
     assert np.max(np.abs(out["density"] - orc.rho) / np.abs(orc.rho)) <= TOL
     assert rel_norm(out["pressure"], orc.p) <= p_tol
     assert rel_norm(sim.read_field(R.FIELD_FORCE_NP), orc.f_np) <= TOL
@@ -173,7 +184,7 @@ def test_reference_profile_steps(method):
             assert rel_norm(out["vel_half"], ref.get("vel_ap", 3)) <= TOL_V
             assert rel_norm(out["vel"], ref.get("vel", 3)) <= TOL_V
             assert np.max(np.abs(out["density"] - ref.get("density", 1)) / ref.get("density", 1)) <= TOL
-            assert rel_norm(out["pressure"], ref.get("pressure", 1)) <= TOL
+            assert rel_norm(out["pressure"], ref.get("pressure", 1)) <= TOL_P_REF_FP64
         _sync_oracle_from_gpu(orc, out)
         state = out
     if method == PCISPH:
@@ -200,7 +211,7 @@ def test_config_pcisph_steps_and_iterations():
             assert abs(so.err[k] - sc.eta) <= 2e-6, (sg.iters, so.iters, so.err[k])
         else:
             assert sg.converged == so.converged
-            _compare_step(sim, orc, x0, p_tol=TOL_P_CONFIG_PCI)
+            _compare_step(sim, orc, x0, p_tol=TOL_P_CONFIG_PCI, v_tol=TOL_V_CONFIG_PCI)
         _sync_oracle_from_gpu(orc, sim.download())
     sim.close()
 
@@ -314,7 +325,7 @@ def test_config_pcisph_warm_started_steps():
         so = orc.step()
         sg = sim.stats()
         if sg.iters == so.iters:
-            _compare_step(sim, orc, x0, p_tol=TOL_P_CONFIG_PCI)
+            _compare_step(sim, orc, x0, p_tol=TOL_P_CONFIG_PCI, v_tol=TOL_V_CONFIG_PCI)
         else:
             k = min(sg.iters, so.iters)
             assert abs(so.err[k] - sc.eta) <= 2e-6
