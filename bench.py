@@ -74,13 +74,17 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scene", default="C2")
-    ap.add_argument("--warm-start", choices=["zero", "previous", "learned"], default="learned")
+    ap.add_argument("--warm-start", choices=["zero", "previous", "learned"], default="learned",
+                    help="zero: plain PCISPH (each step's corrector starts from p = 0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
     ap.add_argument("--presolve", type=int, default=256, help="initial-pressure corrector passes before the warm-up")
     ap.add_argument("--train-steps", type=int, default=400, help="plain-PCISPH steps recorded for training (learned)")
     ap.add_argument("--train-iters", type=int, default=3000, help="Adam steps (learned)")
     ap.add_argument("--train-batch", type=int, default=16384)
+    ap.add_argument("--xsph", type=float, default=None, help="override the scene's XSPH velocity smoothing factor")
+    ap.add_argument("--eval-steps", type=int, default=1000,
+                    help="steps after the recorded ones over which the warm starts are compared (0: skip)")
     return ap.parse_args()
 
 
@@ -247,6 +251,8 @@ def run_ours(args):
 
     modes = {"zero": P.WARM_ZERO, "previous": P.WARM_PREVIOUS, "learned": P.WARM_LEARNED}
     base = P.config_scene(args.scene)
+    if args.xsph is not None:
+        base = base.replace(xsph=args.xsph)
     if world > 1:       # replicas: same scene, own seed per rank
         base.blocks[0].seed = base.blocks[0].seed + 1000 * rank
     sc = base.replace(warm_start=modes[args.warm_start])
@@ -355,19 +361,51 @@ def run_ours(args):
     h2d = n * (36 + (4 if warm else 0))
     d2h = n * (40 + (4 if warm else 0))
     clk = clocks.stop()
-    # ---- the other warm starts over the same steps -------------------------------------
+    # ---- warm starts compared over the evaluation window ------------------------------
+    # Every mode runs the same eval_steps steps from the snapshot (the steps
+    # after the recorded ones), device-timed; each step's final density error
+    # (the max of (rho* - rho0)/rho0 the loop stopped at) is kept so the modes
+    # are compared at the same error statistics.
+    def eval_pass(s):
+        restore(s)
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        its, errs = [], []
+        e0.record(stream)
+        for _ in range(args.eval_steps):
+            s.step(1)
+            st = s.stats()
+            its.append(st.iters)
+            errs.append(st.err[st.iters])
+        e1.record(stream)
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        its = np.asarray(its)
+        errs = np.asarray(errs)
+        return {"iters_mean": float(its.mean()), "iters_p50": float(np.median(its)), "iters_max": int(its.max()),
+                "not_converged_steps": int(np.sum(its >= sc.max_iters)), "ms_per_step": ms / len(its),
+                "value": world * n * len(its) / (ms / 1e3), "final_err_mean": float(errs.mean()),
+                "final_err_max": float(errs.max())}
+
     comparison = {}
-    for name, mode in (("plain", P.WARM_ZERO), ("previous", P.WARM_PREVIOUS)):
-        if mode == sc.warm_start or not pcisph_cfg:
-            continue
-        other = make(mode)
-        ms_o, iters_o, _ = device_pass(other)
-        other.close()
-        comparison[name] = {"iters_mean": float(np.mean(iters_o)), "iters_max": int(np.max(iters_o)),
-                            "ms_per_step": ms_o / args.steps, "value": world * n * args.steps / (ms_o / 1e3),
-                            "not_converged_steps": int(np.sum(np.asarray(iters_o) >= sc.max_iters)),
-                            "iters_ratio_over_this": float(np.mean(iters_o) / max(np.mean(iters), 1e-9)),
-                            "time_ratio_over_this": float(ms_o / ms_max)}
+    if pcisph_cfg and args.eval_steps > 0:
+        comparison["steps"] = "%d..%d of the dam break" % (
+            (args.train_steps if train_info else 0) + args.warmup + 1,
+            (args.train_steps if train_info else 0) + args.warmup + args.eval_steps)
+        comparison[args.warm_start] = eval_pass(sim)
+        for name, mode in (("zero", P.WARM_ZERO), ("previous", P.WARM_PREVIOUS)):
+            if mode == sc.warm_start:
+                continue
+            other = make(mode)
+            comparison[name] = eval_pass(other)
+            other.close()
+        this = comparison[args.warm_start]
+        for name in ("zero", "previous"):
+            if name in comparison and name != args.warm_start:
+                o = comparison[name]
+                o["iters_ratio_over_" + args.warm_start] = o["iters_mean"] / max(this["iters_mean"], 1e-9)
+                o["time_ratio_over_" + args.warm_start] = o["ms_per_step"] / this["ms_per_step"]
     sim.close()
 
     passes = (max(1, int(np.ceil(np.log2(np.prod(sc.dims))))) + 7) // 8
@@ -397,6 +435,7 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": sc.name, "particles": n, "eta": sc.eta, "min_iters": sc.min_iters,
                        "max_iters": sc.max_iters, "warm_start": args.warm_start, "dt": sc.dt, "h": sc.h,
+                       "xsph": sc.xsph,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "working set > L2 (state, lists and scratch ~%d MB per GPU)"
                              % int(n * (3 * 16 * 2 + 8 * 2 + 4 * 2 + 16 * 4 + 8 + 4 + 4 * sc.nbr_cap + 4) / 1e6),

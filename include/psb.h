@@ -74,6 +74,9 @@ typedef struct psb_scene {
                                    so pairs that close in during the step's predictions are in them
                                    (kernels still cut off at h); cell must be >= (1 + skin) h.
                                    REF profile: must be 0 (the reference's test is r <= h). */
+    double xsph;                /* CONFIG-profile PCISPH: XSPH velocity smoothing after the corrector,
+                                   v_i += xsph sum_j (m/rho0) W_ij (v_j - v_i) at the committed
+                                   positions (Monaghan 1989); 0 = off, at most 1. REF profile: 0. */
 } psb_scene;
 
 #define PSB_MAX_ITERS 64

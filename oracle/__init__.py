@@ -44,7 +44,7 @@ class OrcParams(ctypes.Structure):
         ("min_iters", ctypes.c_int32), ("max_iters", ctypes.c_int32),
         ("eta", ctypes.c_double), ("wall_k", ctypes.c_double), ("wall_c", ctypes.c_double),
         ("float_state", ctypes.c_int32), ("warm_start", ctypes.c_int32), ("spacing", ctypes.c_double),
-        ("skin", ctypes.c_double),
+        ("skin", ctypes.c_double), ("xsph", ctypes.c_double)
     ]
 
 
@@ -153,6 +153,7 @@ def params(scene, *, float_state: bool = False, n: Optional[int] = None) -> OrcP
     p.warm_start = 1 if scene.warm_start else 0
     p.spacing = scene.spacing
     p.skin = scene.skin
+    p.xsph = scene.xsph
     return p
 
 

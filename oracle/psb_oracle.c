@@ -598,6 +598,27 @@ static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double*
         pressure_forces(P, ref ? xs : S->pos, rho, p, counts, list, cap, fp);
         k++;
     }
+    /* config: XSPH smoothing of the committed velocity (Monaghan 1989),
+     * v_i + xsph sum_j (m/rho0) W_ij (v_j - v_i) at x*; positions stay */
+    if (!ref && P->xsph > 0) {
+        const double h = P->h, kw = P->xsph * 315.0 * P->mass / (64.0 * PI_D * h * h * h) / P->rho0;
+        double* vx = (double*)malloc(sizeof(double) * n3);
+#pragma omp parallel for schedule(static)
+        for (int32_t i = 0; i < n; ++i) {
+            double dv[3] = {0, 0, 0};
+            for (int32_t t = 0; t < counts[i]; ++t) {
+                const int32_t j = list[(size_t)i * cap + t];
+                const double d[3] = {xs[3 * i] - xs[3 * j], xs[3 * i + 1] - xs[3 * j + 1], xs[3 * i + 2] - xs[3 * j + 2]};
+                const double q = (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / (h * h);
+                if (q >= 1.0) continue;
+                const double w = (1 - q) * (1 - q) * (1 - q);
+                for (int e = 0; e < 3; ++e) dv[e] += w * (vs[3 * j + e] - vs[3 * i + e]);
+            }
+            for (int e = 0; e < 3; ++e) vx[3 * i + e] = RND(P, vs[3 * i + e] + kw * dv[e]);
+        }
+        memcpy(vs, vx, sizeof(double) * n3);
+        free(vx);
+    }
     /* commit the last prediction; walls; velocity interpolation (SphKernel.cu:128-135) */
 #pragma omp parallel for schedule(static)
     for (int32_t i = 0; i < n; ++i) {

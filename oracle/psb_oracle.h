@@ -38,6 +38,7 @@ typedef struct orc_params {
     int32_t warm_start;             /* PCISPH: 0 start from p = 0, 1 start from the given p */
     double spacing;                 /* config PCISPH prototype lattice spacing (0: (m/rho0)^(1/3)) */
     double skin;                    /* config: lists hold pairs within (1 + skin) h */
+    double xsph;                    /* config PCISPH: XSPH velocity smoothing factor */
 } orc_params;
 
 /* Config-profile PCISPH pressure factor delta = 1 / (beta (|sum gradW|^2 +

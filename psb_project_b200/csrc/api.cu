@@ -194,6 +194,7 @@ int validate(const psb_scene* s, std::string& why) {
     if (s->n_max <= 0) { why = "n_max must be positive"; return PSB_EINVAL; }
     if (!(s->h > 0) || !(s->mass > 0) || !(s->rho0 > 0) || !(s->dt > 0)) { why = "h, mass, rho0, dt must be positive"; return PSB_EINVAL; }
     if (!(s->skin >= 0) || (s->profile == PSB_PROFILE_REF && s->skin != 0)) { why = "skin must be >= 0 (0 in the reference profile)"; return PSB_EINVAL; }
+    if (!(s->xsph >= 0 && s->xsph <= 1) || (s->profile == PSB_PROFILE_REF && s->xsph != 0)) { why = "xsph must be in [0, 1] (0 in the reference profile)"; return PSB_EINVAL; }
     if (!(s->cell > 0) || (double)s->cell < s->h * (1.0 + s->skin) * (1.0 - 1e-6)) {
         why = "cell must be >= (1 + skin) h (27-cell walk)";
         return PSB_EINVAL;
@@ -270,6 +271,7 @@ Params derive(const psb_scene& s) {
     P.wlo_z = s.box_min[2] + s.particle_radius;
     P.whi_x = s.box_max[0] - s.particle_radius; P.whi_y = s.box_max[1] - s.particle_radius;
     P.whi_z = s.box_max[2] - s.particle_radius;
+    P.xsph_k = (float)(P.ref || !P.pci ? 0.0 : s.xsph * 315.0 * m / (64.0 * pi * h * h * h) / s.rho0);
     P.wall_k = (float)s.wall_k;     // config: penalty outside the faces (bx0..bz1)
     P.wall_c = (float)s.wall_c;
     P.bx0 = s.box_min[0]; P.by0 = s.box_min[1]; P.bz0 = s.box_min[2];
@@ -445,8 +447,16 @@ int step_once(psb_ctx* c, bool last) {
             xi ^= 1;
             ++k;
         }
+        const float4* v_commit = c->vs;
+        if (P.xsph_k != 0.f) {     // the other prediction buffer is free now
+            timed(c, "xsph", [&] {
+                psb::launch_xsph(st, P, c->xs[xi], c->vs, c->nbr_count, c->nbr_list, c->xs[xi ^ 1]);
+            });
+            v_commit = c->xs[xi ^ 1];
+        }
         timed(c, "pci_commit", [&] {
-            psb::launch_pci_commit(st, P, c->xs[xi], c->vs, c->rpc, passes > 0, c->pos[s], c->vel[s], c->vap[s], c->rp[r]);
+            psb::launch_pci_commit(st, P, c->xs[xi], v_commit, c->rpc, passes > 0, c->pos[s], c->vel[s], c->vap[s],
+                                   c->rp[r]);
         });
         if (collect && converged) {
             const int stride = c->collect_stride;

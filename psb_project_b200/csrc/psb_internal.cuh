@@ -51,6 +51,7 @@ struct Params {
     float gx, gy, gz;   // gravity acceleration
     float wlo_x, wlo_y, wlo_z, whi_x, whi_y, whi_z;   // box min + r, box max - r (float, as collisionBox)
     float wall_k, wall_c;
+    float xsph_k;       // config PCISPH XSPH: xsph * k_rho / rho0 (0: off)
     // Config-profile walls (mirror ghost particles across the box faces):
     float bx0, by0, bz0, bx1, by1, bz1;   // faces
     float hf;           // h
@@ -89,6 +90,8 @@ void launch_pci_force_predict(cudaStream_t st, const Params& P, const float4* po
                               const int* list, float4* xs_next, float4* vs, float2* rp);
 void launch_pci_commit(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const float2* rpc,
                        int have_density_pass, float4* pos, float4* vel, float4* vap, float2* rp);
+void launch_xsph(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const int* counts,
+                 const int* list, float4* vs_out);
 
 // ---- learned warm start (mlp.cu) ---------------------------------------------------
 constexpr int kMlpParams = 4673;   // 6x64 + 64 + 64x64 + 64 + 64 + 1

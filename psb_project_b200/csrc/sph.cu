@@ -493,6 +493,31 @@ __global__ void __launch_bounds__(kBlock) k_pci_commit(Params P, const float4* _
     if (have_density_pass) rp[t].x = rpc[t].x;
 }
 
+// XSPH velocity smoothing (Monaghan 1989) of the committed prediction,
+// config PCISPH: v_i + xsph sum_j (m/rho0) W_ij (v_j - v_i) over the list at
+// x*, W the poly6 kernel (m W = k_rho (1-q)^3). Positions are not moved.
+__global__ void __launch_bounds__(kBlock) k_xsph(Params P, const float4* __restrict__ xs,
+                                                 const float4* __restrict__ vs, const int* __restrict__ counts,
+                                                 const int* __restrict__ list, float4* __restrict__ vs_out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const float4 xi = xs[t], vi = vs[t];
+    const int cnt = min(counts[t], P.cap);
+    float3 dv = make_float3(0.f, 0.f, 0.f);
+#pragma unroll 4
+    for (int c = 0; c < cnt; ++c) {
+        const int j = list[(size_t)c * P.n + t];
+        const float4 xj = xs[j];
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float q = (dx * dx + dy * dy + dz * dz) * P.inv_h2;
+        if (q >= 1.f) continue;
+        const float4 vj = vs[j];
+        const float w = (1.f - q) * (1.f - q) * (1.f - q);
+        dv.x += w * (vj.x - vi.x); dv.y += w * (vj.y - vi.y); dv.z += w * (vj.z - vi.z);
+    }
+    vs_out[t] = make_float4(vi.x + P.xsph_k * dv.x, vi.y + P.xsph_k * dv.y, vi.z + P.xsph_k * dv.z, 0.f);
+}
+
 inline int grid_of(int n) { return (n + kBlock - 1) / kBlock; }
 
 }  // namespace
@@ -527,6 +552,11 @@ void launch_pci_force_predict(cudaStream_t st, const Params& P, const float4* po
                               const int* list, float4* xs_next, float4* vs, float2* rp) {
     if (P.n > 0)
         k_pci_force_predict<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vap, fnp, xs, rpc, counts, list, xs_next, vs, rp);
+}
+
+void launch_xsph(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const int* counts,
+                 const int* list, float4* vs_out) {
+    if (P.n > 0) k_xsph<<<grid_of(P.n), kBlock, 0, st>>>(P, xs, vs, counts, list, vs_out);
 }
 
 void launch_pci_commit(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const float2* rpc,

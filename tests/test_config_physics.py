@@ -10,7 +10,9 @@ GPU): each pins one property the GPU path is then checked against.
     corrector converges from a hydrostatic start in a tall column (with the
     force at x* and p/rho*^2 it diverges there);
   * the prototype pressure factor equals its closed-form definition;
-  * an isolated particle's density is m 315/(64 pi h^3) (the poly6 value at r = 0).
+  * an isolated particle's density is m 315/(64 pi h^3) (the poly6 value at r = 0);
+  * XSPH velocity smoothing moves no momentum and lowers the kinetic energy
+    of the relative motion.
 """
 import math
 
@@ -98,3 +100,24 @@ def test_lattice_mass_puts_lattice_at_rest_density():
     rho = oracle.density(sub, pos, c, l, clamp=True)
     assert sub.mass == pytest.approx(sc.mass)
     assert rho[4 + 9 * 4 + 81 * 4] == pytest.approx(1000.0, rel=1e-6)   # float32 lattice positions
+
+
+def test_xsph_conserves_momentum_and_dissipates_relative_motion():
+    """XSPH (config PCISPH) adds xsph sum_j (m/rho0) W_ij (v_j - v_i) to each
+    committed velocity: a symmetric pair exchange, so the total momentum is
+    that of the same step without it, and the kinetic energy of the relative
+    motion goes down (sum_i v_i . dv_i = -1/2 sum W |v_i - v_j|^2 <= 0)."""
+    base = P.dam_break((10, 10, 10), 0.005, (4.0, 2.0, 1.0), 0.01, seed=5, jitter=1e-4)
+    pos = oracle.scene_positions(base).astype(np.float64) + 0.2      # clear of every face
+    rng = np.random.default_rng(3)
+    vel = rng.normal(0.0, 0.3, (base.n, 3))
+    out = {}
+    for x in (0.0, 0.25):
+        sc = base.replace(xsph=x, min_iters=3, max_iters=3, eta=0.0)
+        o = oracle.OracleSim(sc, pos, vel, vel, None)
+        o.step()
+        out[x] = o.vel_half.copy()
+    d = out[0.25] - out[0.0]
+    assert np.abs(d).max() > 1e-3                      # the smoothing acts
+    assert np.abs(d.sum(0)).max() < 1e-12 * base.n     # ... and moves no momentum
+    assert (out[0.25] ** 2).sum() < (out[0.0] ** 2).sum()
