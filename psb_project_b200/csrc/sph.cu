@@ -54,9 +54,10 @@ __device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.
 // Penalty walls (config profile): a = K*depth - C*v along each axis on which
 // x lies outside the box (a state uploaded outside it; the projection below
 // keeps stepped particles inside).
+template <bool REF>
 __device__ __forceinline__ float3 wall_accel(const Params& P, float4 x, float4 v) {
     float3 a = make_float3(0.f, 0.f, 0.f);
-    if (P.ref) return a;
+    if (REF) return a;
     if (x.x < P.bx0) a.x += P.wall_k * (P.bx0 - x.x) - P.wall_c * v.x;
     if (x.x > P.bx1) a.x += -P.wall_k * (x.x - P.bx1) - P.wall_c * v.x;
     if (x.y < P.by0) a.y += P.wall_k * (P.by0 - x.y) - P.wall_c * v.y;
@@ -208,6 +209,7 @@ __device__ __forceinline__ void box_project(const Params& P, float3& x, float3& 
 // SphKernel.cu:25; config: Tait, p = k rho0/7 ((rho/rho0)^7 - 1), written as
 // k rho0/7 d (1 + x + ... + x^6) with x = 1 + d to avoid cancellation).
 // PCISPH: keeps the carried pressure (warm start) or zeroes it.
+template <bool REF>
 __global__ void __launch_bounds__(kBlock) k_density_x(Params P, const float4* __restrict__ pos,
                                                       const int* __restrict__ counts, const int* __restrict__ list,
                                                       float2* __restrict__ rp, float* __restrict__ rho_x, int zero_p) {
@@ -221,17 +223,17 @@ __global__ void __launch_bounds__(kBlock) k_density_x(Params P, const float4* __
         const float4 xj = pos[list[(size_t)c * P.n + t]];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float q = (dx * dx + dy * dy + dz * dz) * P.inv_h2;
-        if (!P.ref && q >= 1.f) continue;
+        if (!REF && q >= 1.f) continue;
         const float w = 1.f - q;
         acc.add(w * w * w);
     }
-    if (!P.ref) ghost_density(P, t, xi, pos, list, cnt, acc);
+    if (!REF) ghost_density(P, t, xi, pos, list, cnt, acc);
     const float drho = density_deviation(P, acc);
     const float rho = P.rho0 + drho;
     float p;
     if (P.pci) {
         p = zero_p ? 0.f : rp[t].y;
-    } else if (P.ref) {
+    } else if (REF) {
         p = P.eos_k * drho;
     } else {
         const float d = drho / P.rho0;
@@ -252,7 +254,7 @@ struct PairSums {
     float fs;       // sum (1-q)(3-7q) / rho_j           (times -k_surf: surface term)
 };
 
-template <bool WITH_PRESSURE>
+template <bool REF, bool WITH_PRESSURE>
 __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi, float4 vi, float2 rpi,
                                               const float4* __restrict__ pos, const float4* __restrict__ vel,
                                               const float2* __restrict__ rp, const int* __restrict__ counts,
@@ -262,7 +264,7 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
     S.fs = 0.f;
     // Config: p/rho0^2 (the PCISPH linearisation; see k_pci_force_predict).
     const float ir0 = 1.f / (P.rho0 * P.rho0);
-    const float pVi = WITH_PRESSURE ? (P.ref ? rpi.y / (rpi.x * rpi.x) : rpi.y * ir0) : 0.f;
+    const float pVi = WITH_PRESSURE ? (REF ? rpi.y / (rpi.x * rpi.x) : rpi.y * ir0) : 0.f;
     const int cnt = min(counts[t], P.cap);
 #pragma unroll 4
     for (int c = 0; c < cnt; ++c) {
@@ -272,7 +274,7 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
         const float r2 = dx * dx + dy * dy + dz * dz;
         if (!(r2 > 0.f)) continue;
         const float q = r2 * P.inv_h2;
-        if (!P.ref && q >= 1.f) continue;
+        if (!REF && q >= 1.f) continue;
         const float4 vj = vel[j];
         const float2 rpj = rp[j];
         const float rinv = rsqrtf(r2);
@@ -283,18 +285,18 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
         S.fv.y += (vj.y - vi.y) * sv;
         S.fv.z += (vj.z - vi.z) * sv;
         if (WITH_PRESSURE) {
-            const float pVj = P.ref ? rpj.y * inv_rj * inv_rj : rpj.y * ir0;
+            const float pVj = REF ? rpj.y * inv_rj * inv_rj : rpj.y * ir0;
             const float s = (pVi + pVj) * om * om * rinv;
             S.ap.x += s * dx; S.ap.y += s * dy; S.ap.z += s * dz;
         }
-        if (P.surface) {
+        if (REF) {      // surface tension and normals: reference profile only
             const float t1 = 1.f - q;
             S.fs += t1 * (3.f - 7.f * q) * inv_rj;
             const float sn = t1 * t1 * inv_rj;
             S.nrm.x += dx * sn; S.nrm.y += dy * sn; S.nrm.z += dz * sn;
         }
     }
-    if (WITH_PRESSURE && !P.ref)
+    if (WITH_PRESSURE && !REF)
         ghost_pressure(P, t, xi, pVi, pos, (const float*)rp + 1, 2, list, cnt, S.ap);
     return S;
 }
@@ -302,9 +304,10 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
 // Non-pressure force density f_v + f_s + rho_i g (the reference's forcesAccum
 // is (0, -9.81 rho, 0) in PCISPH, PciSphSystem_Kernel.cu:168, and rho*g from
 // ForceExt_Constante in WCSPH, SphSystem.cpp:307-320).
+template <bool REF>
 __device__ __forceinline__ float3 nonpressure_force(const Params& P, const PairSums& S, float rho) {
     float3 f = make_float3(P.k_visc * S.fv.x, P.k_visc * S.fv.y, P.k_visc * S.fv.z);
-    if (P.surface) {
+    if (REF) {
         const float3 n = make_float3(-P.k_surf * S.nrm.x, -P.k_surf * S.nrm.y, -P.k_surf * S.nrm.z);
         const float ln = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
         if (ln >= P.l) {
@@ -317,6 +320,7 @@ __device__ __forceinline__ float3 nonpressure_force(const Params& P, const PairS
 }
 
 // WCSPH: forces, leap-frog, walls and velocity interpolation in one sweep.
+template <bool REF>
 __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params P, const float4* __restrict__ pos,
                                                         const float4* __restrict__ vel, const float4* __restrict__ vap,
                                                         const float2* __restrict__ rp, const int* __restrict__ counts,
@@ -327,16 +331,16 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params P, const float4* 
     if (t >= P.n) return;
     const float4 xi = pos[t], vi = vel[t], vh = vap[t];
     const float2 rpi = rp[t];
-    const PairSums S = pair_sums<true>(P, t, xi, vi, rpi, pos, vel, rp, counts, list);
-    const float3 f = nonpressure_force(P, S, rpi.x);
+    const PairSums S = pair_sums<REF, true>(P, t, xi, vi, rpi, pos, vel, rp, counts, list);
+    const float3 f = nonpressure_force<REF>(P, S, rpi.x);
     fnp[t] = make_float4(f.x, f.y, f.z, 0.f);
-    const float3 aw = wall_accel(P, xi, vh);
+    const float3 aw = wall_accel<REF>(P, xi, vh);
     const float ir = 1.f / rpi.x;
     const float3 a = make_float3(f.x * ir + P.k_grad * S.ap.x + aw.x, f.y * ir + P.k_grad * S.ap.y + aw.y,
                                  f.z * ir + P.k_grad * S.ap.z + aw.z);
     float3 v = make_float3(vh.x + a.x * P.dt, vh.y + a.y * P.dt, vh.z + a.z * P.dt);
     float3 x = make_float3(xi.x + v.x * P.dt, xi.y + v.y * P.dt, xi.z + v.z * P.dt);
-    if (P.ref) box_project(P, x, v);   // config WCSPH: penalty walls only
+    if (REF) box_project(P, x, v);   // config WCSPH: penalty walls only
     pos_out[t] = make_float4(x.x, x.y, x.z, 0.f);
     vap_out[t] = make_float4(v.x, v.y, v.z, 0.f);
     vel_out[t] = make_float4((vh.x + v.x) * 0.5f, (vh.y + v.y) * 0.5f, (vh.z + v.z) * 0.5f, 0.f);
@@ -344,23 +348,22 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params P, const float4* 
 
 // PCISPH set-up sweep: non-pressure forces at x (and, for a warm start, the
 // pressure acceleration of the carried pressure), then the first prediction.
+template <bool REF, bool WARM>
 __global__ void __launch_bounds__(kBlock) k_pci_init(Params P, const float4* __restrict__ pos,
                                                      const float4* __restrict__ vel, const float4* __restrict__ vap,
                                                      const float2* __restrict__ rp, const int* __restrict__ counts,
-                                                     const int* __restrict__ list, int warm, float4* __restrict__ fnp,
+                                                     const int* __restrict__ list, float4* __restrict__ fnp,
                                                      float4* __restrict__ xs, float4* __restrict__ vs) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= P.n) return;
     const float4 xi = pos[t], vi = vel[t], vh = vap[t];
     const float2 rpi = rp[t];
-    PairSums S;
-    if (warm) S = pair_sums<true>(P, t, xi, vi, rpi, pos, vel, rp, counts, list);
-    else S = pair_sums<false>(P, t, xi, vi, rpi, pos, vel, rp, counts, list);
-    const float3 f = nonpressure_force(P, S, rpi.x);
+    const PairSums S = pair_sums<REF, WARM>(P, t, xi, vi, rpi, pos, vel, rp, counts, list);
+    const float3 f = nonpressure_force<REF>(P, S, rpi.x);
     fnp[t] = make_float4(f.x, f.y, f.z, 0.f);
-    const float3 aw = wall_accel(P, xi, vh);
+    const float3 aw = wall_accel<REF>(P, xi, vh);
     const float ir = 1.f / rpi.x;
-    const float ap = warm ? P.k_grad : 0.f;
+    const float ap = WARM ? P.k_grad : 0.f;
     const float3 a = make_float3(f.x * ir + ap * S.ap.x + aw.x, f.y * ir + ap * S.ap.y + aw.y,
                                  f.z * ir + ap * S.ap.z + aw.z);
     const float3 v = make_float3(vh.x + a.x * P.dt, vh.y + a.y * P.dt, vh.z + a.z * P.dt);
@@ -370,6 +373,7 @@ __global__ void __launch_bounds__(kBlock) k_pci_init(Params P, const float4* __r
 
 // PCISPH density pass at x*: rho*, the gradient sums of the pressure
 // increment, the candidate pressure and the FP64 max compression error.
+template <bool REF>
 __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* __restrict__ xs,
                                                         const float2* __restrict__ rp, const int* __restrict__ counts,
                                                         const int* __restrict__ list, float2* __restrict__ rpc,
@@ -388,10 +392,10 @@ __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* 
             const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
             const float r2 = dx * dx + dy * dy + dz * dz;
             const float q = r2 * P.inv_h2;
-            if (!P.ref && q >= 1.f) continue;
+            if (!REF && q >= 1.f) continue;
             const float w = 1.f - q;
             acc.add(w * w * w);
-            if (P.ref && r2 > 0.f) {
+            if (REF && r2 > 0.f) {
                 const float rinv = rsqrtf(r2);
                 const float om = 1.f - r2 * rinv * P.inv_h;
                 const float g = om * om;
@@ -400,11 +404,11 @@ __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* 
                 T2 += g * g;
             }
         }
-        if (!P.ref) ghost_density(P, t, xi, xs, list, cnt, acc);
+        if (!REF) ghost_density(P, t, xi, xs, list, cnt, acc);
         const float drho = density_deviation(P, acc);
         const float rho = P.rho0 + drho;
         float p = rp[t].y;
-        if (P.ref) {            // per-particle factor, compressed particles only
+        if (REF) {              // per-particle factor, compressed particles only
             if (drho > 0.f && T2 > 0.f) p += P.k_press * drho / (T1.x * T1.x + T1.y * T1.y + T1.z * T1.z + T2);
         } else {                // prototype factor, every particle, p >= 0
             p = fmaxf(0.f, p + P.k_delta * drho);
@@ -432,6 +436,7 @@ __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* 
 // fixed-point iteration in positions whose gain grows with p dt^2/h^2, and
 // with rho* in p/rho^2 the force feeds back on the density; under a 0.64 m
 // column either one makes the corrector diverge.
+template <bool REF>
 __global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const float4* __restrict__ pos,
                                                               const float4* __restrict__ vap,
                                                               const float4* __restrict__ fnp,
@@ -442,11 +447,11 @@ __global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const fl
                                                               float4* __restrict__ vs, float2* __restrict__ rp) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= P.n) return;
-    const float4* __restrict__ geo = P.ref ? xs : pos;
+    const float4* __restrict__ geo = REF ? xs : pos;
     const float4 xi = geo[t];
     const float2 ri = rpc[t];
     const float ir0 = 1.f / (P.rho0 * P.rho0);
-    const float pVi = P.ref ? ri.y / (ri.x * ri.x) : ri.y * ir0;
+    const float pVi = REF ? ri.y / (ri.x * ri.x) : ri.y * ir0;
     const int cnt = min(counts[t], P.cap);
     float3 acc = make_float3(0.f, 0.f, 0.f);
 #pragma unroll 4
@@ -456,17 +461,17 @@ __global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const fl
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float r2 = dx * dx + dy * dy + dz * dz;
         if (!(r2 > 0.f)) continue;
-        if (!P.ref && r2 * P.inv_h2 >= 1.f) continue;
+        if (!REF && r2 * P.inv_h2 >= 1.f) continue;
         const float2 rj = rpc[j];
         const float rinv = rsqrtf(r2);
         const float om = 1.f - r2 * rinv * P.inv_h;
-        const float pVj = P.ref ? rj.y / (rj.x * rj.x) : rj.y * ir0;
+        const float pVj = REF ? rj.y / (rj.x * rj.x) : rj.y * ir0;
         const float s = (pVi + pVj) * om * om * rinv;
         acc.x += s * dx; acc.y += s * dy; acc.z += s * dz;
     }
-    if (!P.ref) ghost_pressure(P, t, xi, pVi, geo, (const float*)rpc + 1, 2, list, cnt, acc);
+    if (!REF) ghost_pressure(P, t, xi, pVi, geo, (const float*)rpc + 1, 2, list, cnt, acc);
     const float4 x0 = pos[t], vh = vap[t], f = fnp[t];
-    const float3 aw = wall_accel(P, x0, vh);
+    const float3 aw = wall_accel<REF>(P, x0, vh);
     const float ir = 1.f / ri.x;
     const float3 a = make_float3(f.x * ir + P.k_grad * acc.x + aw.x, f.y * ir + P.k_grad * acc.y + aw.y,
                                  f.z * ir + P.k_grad * acc.z + aw.z);
@@ -524,34 +529,54 @@ inline int grid_of(int n) { return (n + kBlock - 1) / kBlock; }
 
 void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const int* counts, const int* list,
                       float2* rp, float* rho_x, int zero_p) {
-    if (P.n > 0) k_density_x<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, counts, list, rp, rho_x, zero_p);
+    if (P.n <= 0) return;
+    if (P.ref) k_density_x<true><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, counts, list, rp, rho_x, zero_p);
+    else k_density_x<false><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, counts, list, rp, rho_x, zero_p);
 }
 
 void launch_wcsph_force(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float4* vap,
                         const float2* rp, const int* counts, const int* list, float4* pos_out, float4* vel_out,
                         float4* vap_out, float4* fnp) {
-    if (P.n > 0)
-        k_wcsph_force<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, pos_out, vel_out, vap_out,
-                                                       fnp);
+    if (P.n <= 0) return;
+    if (P.ref)
+        k_wcsph_force<true><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, pos_out, vel_out,
+                                                             vap_out, fnp);
+    else
+        k_wcsph_force<false><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, pos_out, vel_out,
+                                                              vap_out, fnp);
 }
 
 void launch_pci_init(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float4* vap,
                      const float2* rp, const int* counts, const int* list, int warm, float4* fnp, float4* xs,
                      float4* vs) {
-    if (P.n > 0)
-        k_pci_init<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, warm, fnp, xs, vs);
+    if (P.n <= 0) return;
+    const dim3 g(grid_of(P.n));
+    if (P.ref) {
+        if (warm) k_pci_init<true, true><<<g, kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, fnp, xs, vs);
+        else k_pci_init<true, false><<<g, kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, fnp, xs, vs);
+    } else {
+        if (warm) k_pci_init<false, true><<<g, kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, fnp, xs, vs);
+        else k_pci_init<false, false><<<g, kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, fnp, xs, vs);
+    }
 }
 
 void launch_pci_density(cudaStream_t st, const Params& P, const float4* xs, const float2* rp, const int* counts,
                         const int* list, float2* rpc, unsigned long long* err_slot) {
-    if (P.n > 0) k_pci_density<<<grid_of(P.n), kBlock, 0, st>>>(P, xs, rp, counts, list, rpc, err_slot);
+    if (P.n <= 0) return;
+    if (P.ref) k_pci_density<true><<<grid_of(P.n), kBlock, 0, st>>>(P, xs, rp, counts, list, rpc, err_slot);
+    else k_pci_density<false><<<grid_of(P.n), kBlock, 0, st>>>(P, xs, rp, counts, list, rpc, err_slot);
 }
 
 void launch_pci_force_predict(cudaStream_t st, const Params& P, const float4* pos, const float4* vap,
                               const float4* fnp, const float4* xs, const float2* rpc, const int* counts,
                               const int* list, float4* xs_next, float4* vs, float2* rp) {
-    if (P.n > 0)
-        k_pci_force_predict<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vap, fnp, xs, rpc, counts, list, xs_next, vs, rp);
+    if (P.n <= 0) return;
+    if (P.ref)
+        k_pci_force_predict<true><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vap, fnp, xs, rpc, counts, list, xs_next,
+                                                                   vs, rp);
+    else
+        k_pci_force_predict<false><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vap, fnp, xs, rpc, counts, list, xs_next,
+                                                                    vs, rp);
 }
 
 void launch_xsph(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const int* counts,
