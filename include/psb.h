@@ -43,7 +43,10 @@ enum {
  * -9.81 y gravity in PCISPH). CONFIG is the scene text's method (Tait EOS,
  * penalty walls, eta loop with min/max iterations, no surface tension). */
 enum { PSB_PROFILE_REF = 0, PSB_PROFILE_CONFIG = 1 };
-enum { PSB_WCSPH = 0, PSB_PCISPH = 1 };
+/* PSB_DEM: the reference's discrete-element system (CudaSystem::update,
+ * CudaSystem.cpp:207-224): spheres with pairwise spring-dashpot contacts
+ * over the same grid and neighbour lists, gravity, explicit Euler, walls. */
+enum { PSB_WCSPH = 0, PSB_PCISPH = 1, PSB_DEM = 2 };
 /* Initial pressure of each PCISPH step (CONFIG profile). */
 enum { PSB_WARM_ZERO = 0, PSB_WARM_PREVIOUS = 1, PSB_WARM_LEARNED = 2 };
 
@@ -77,6 +80,16 @@ typedef struct psb_scene {
     double xsph;                /* CONFIG-profile PCISPH: XSPH velocity smoothing after the corrector,
                                    v_i += xsph sum_j (m/rho0) W_ij (v_j - v_i) at the committed
                                    positions (Monaghan 1989); 0 = off, at most 1. REF profile: 0. */
+    /* PSB_DEM contact law. REF profile: collideParticle (CudaParticle_Kernel.cu:
+     * 10-36) as it executes: -dem_spring (R - d) n for d < 2R, R = h_A + h_B
+     * with h the interaction radius, which interactionSystem passes as the
+     * sphere radius (CudaSystem.cpp:244). Its damping, shear and attraction
+     * terms are `force += ...` through a double3 operator+= that does not
+     * assign (double3.h:115-117), so they have no effect there either.
+     * CONFIG profile: linear spring-dashpot on overlaps of particle_radius
+     * spheres, dem_spring = k_n (N/m), dem_damping = normal dashpot c_n
+     * (N s/m); shear and attraction unused. mass is the sphere mass. */
+    double dem_spring, dem_damping, dem_shear, dem_attraction;
 } psb_scene;
 
 #define PSB_MAX_ITERS 64

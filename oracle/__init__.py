@@ -44,7 +44,9 @@ class OrcParams(ctypes.Structure):
         ("min_iters", ctypes.c_int32), ("max_iters", ctypes.c_int32),
         ("eta", ctypes.c_double), ("wall_k", ctypes.c_double), ("wall_c", ctypes.c_double),
         ("float_state", ctypes.c_int32), ("warm_start", ctypes.c_int32), ("spacing", ctypes.c_double),
-        ("skin", ctypes.c_double), ("xsph", ctypes.c_double)
+        ("skin", ctypes.c_double), ("xsph", ctypes.c_double),
+        ("dem_spring", ctypes.c_double), ("dem_damping", ctypes.c_double), ("dem_shear", ctypes.c_double),
+        ("dem_attraction", ctypes.c_double),
     ]
 
 
@@ -154,6 +156,8 @@ def params(scene, *, float_state: bool = False, n: Optional[int] = None) -> OrcP
     p.spacing = scene.spacing
     p.skin = scene.skin
     p.xsph = scene.xsph
+    p.dem_spring, p.dem_damping = scene.dem_spring, scene.dem_damping
+    p.dem_shear, p.dem_attraction = scene.dem_shear, scene.dem_attraction
     return p
 
 
@@ -301,6 +305,27 @@ class RefSim:
         rc = ref_lib().ref_pcisph_update(self.h, s.dt, iters, 1 if collide else 0, s.particle_radius, _ptr(bmin), _ptr(bmax))
         if rc != 0:
             raise RuntimeError(f"ref_pcisph_update: {rc}")
+
+    def dem_update(self, collide=True):
+        """CudaSystem::update (CudaSystem.cpp:207-224) on the state, the
+        step's start state serving as the old buffers (pos_old = pos,
+        vel_old = vel), with the scene's uniform contact coefficients."""
+        s = self.scene
+        ones = np.ones(self.n)
+        for name, val in (("spring", s.dem_spring), ("damping", s.dem_damping), ("shear", s.dem_shear),
+                          ("attraction", s.dem_attraction)):
+            self.set(name, ones * val)
+        self.set("pos_old", self.get("pos", 3))
+        self.set("vel_old", self.get("vel", 3))
+        bmin = np.asarray(s.box_min, np.float32)
+        bmax = np.asarray(s.box_max, np.float32)
+        g = np.asarray(s.gravity, np.float64)
+        amp = float(np.linalg.norm(g))
+        gdir = (g / amp if amp > 0 else g).astype(np.float32)
+        rc = ref_lib().ref_dem_update(self.h, s.dt, _ptr(gdir), np.float32(amp), 1 if collide else 0,
+                                      s.particle_radius, _ptr(bmin), _ptr(bmax))
+        if rc != 0:
+            raise RuntimeError(f"ref_dem_update: {rc}")
 
     def wcsph_update(self, collide=True):
         s = self.scene

@@ -21,6 +21,9 @@
  *   PCISPH pressure force . PciSphSystem_Kernel.cu:88-114
  *   PCISPH sequence ....... .../PCISPH/PciSphSystem.cu:8-68, PciSphSystem.cpp:163-204
  *   box walls ............. src/Kernel/Collision/BoxCollision/BoxCollision_Kernel.cu:7-34
+ *   DEM contacts .......... src/Kernel/System/SimpleSystem/CudaParticle_Kernel.cu:10-55 (as executed,
+ *                           see dem_pair_ref), integrateEuler ParticleKernel.cu:12-20,
+ *                           sequence CudaSystem.cpp:207-224
  * The reference's predict-then-restore passes are restated as a predict that
  * leaves the saved state untouched; the values are the same.
  *
@@ -662,9 +665,93 @@ int orc_presolve(const orc_params* P, orc_state* S, int32_t iters, orc_stats* st
     return rc;
 }
 
+/* ---- DEM (CudaSystem::update, CudaSystem.cpp:207-224) ----------------------
+ * Forces start at zero plus the constant force m g (evaluate_force_constante,
+ * ForceExt_Constante.cu:15-23: (dir amp) in float times the mass), then the
+ * pair forces over the neighbour list on the step's start state, then
+ * explicit Euler and the box. Reference profile: collideParticle
+ * (CudaParticle_Kernel.cu:10-36) as it executes -- the spring term alone,
+ * see dem_pair_ref -- with the interaction radius as the sphere radius, as
+ * interactionSystem passes it (CudaSystem.cpp:244), and
+ * integrateEuler (ParticleKernel.cu:12-20): x += v_old dt. Config profile
+ * (the scene text's linear spring-dashpot): on an overlap delta = 2r - d > 0
+ * of two particle_radius spheres, F_A = (-k_n delta + c_n (v_B - v_A).n) n
+ * with n the unit vector from A to B; semi-implicit Euler, x += v_new dt. */
+static void dem_pair_ref(const orc_params* P, const double* xa, const double* xb, const double* va, const double* vb,
+                         double* f) {
+    const double rel[3] = {xb[0] - xa[0], xb[1] - xa[1], xb[2] - xa[2]};
+    const double dist = sqrt((rel[0] * rel[0] + rel[1] * rel[1]) + rel[2] * rel[2]);
+    if (!(dist > 0)) return;
+    const float R = (float)(P->h + P->h);
+    if (!(dist < R * 2.0f)) return;
+    const double inv = 1.0 / dist;
+    const double nrm[3] = {rel[0] * inv, rel[1] * inv, rel[2] * inv};
+    (void)va; (void)vb;
+    /* force = -spring (collideDist - dist) norm (CudaParticle_Kernel.cu:28).
+     * The dashpot, shear and attraction lines (:30-34) are `force += ...`,
+     * and the reference's double3 operator+= (double3.h:115-117) takes its
+     * left operand by const reference and only returns the sum: those terms
+     * never reach the force. */
+    for (int e = 0; e < 3; ++e) f[e] = f[e] + (-P->dem_spring * ((double)R - dist) * nrm[e]);
+}
+
+static void dem_pair_config(const orc_params* P, const double* xa, const double* xb, const double* va,
+                            const double* vb, double* f) {
+    const double rel[3] = {xb[0] - xa[0], xb[1] - xa[1], xb[2] - xa[2]};
+    const double dist = sqrt(rel[0] * rel[0] + rel[1] * rel[1] + rel[2] * rel[2]);
+    const double delta = 2.0 * (double)P->particle_radius - dist;
+    if (!(dist > 0) || !(delta > 0)) return;
+    const double nrm[3] = {rel[0] / dist, rel[1] / dist, rel[2] / dist};
+    const double vn = (vb[0] - va[0]) * nrm[0] + (vb[1] - va[1]) * nrm[1] + (vb[2] - va[2]) * nrm[2];
+    const double s = -P->dem_spring * delta + P->dem_damping * vn;
+    for (int e = 0; e < 3; ++e) f[e] += s * nrm[e];
+}
+
+static int step_dem(const orc_params* P, orc_state* S, orc_stats* st, double* f_out, int32_t* nbr_counts) {
+    const int32_t n = P->n;
+    const int ref = P->profile == ORC_PROFILE_REF;
+    int32_t* counts = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+    int32_t cap = 0;
+    int32_t* list = build_lists(P, S->pos, counts, &cap, st);
+    double* f = (double*)malloc(sizeof(double) * 3 * (size_t)n);
+    const double dt = (double)P->dt;
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+        double* fi = &f[3 * (size_t)i];
+        for (int e = 0; e < 3; ++e) fi[e] = 0.0 + (double)P->gravity[e] * P->mass;
+        for (int32_t t = 0; t < counts[i]; ++t) {
+            const int32_t j = list[(size_t)i * cap + t];
+            if (ref) dem_pair_ref(P, &S->pos[3 * i], &S->pos[3 * j], &S->vel[3 * i], &S->vel[3 * j], fi);
+            else dem_pair_config(P, &S->pos[3 * i], &S->pos[3 * j], &S->vel[3 * i], &S->vel[3 * j], fi);
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+        double* x = &S->pos[3 * i];
+        double* v = &S->vel[3 * i];
+        const double v0[3] = {v[0], v[1], v[2]};
+        for (int e = 0; e < 3; ++e) {
+            v[e] = RND(P, v[e] + (f[3 * i + e] / P->mass) * dt);
+            x[e] = RND(P, x[e] + (ref ? v0[e] : v[e]) * dt);
+        }
+        box_project(P, x, v);    /* collisionBox on (pos, vel), CudaSystem::collide */
+        for (int e = 0; e < 3; ++e) {
+            x[e] = RND(P, x[e]);
+            v[e] = RND(P, v[e]);
+            S->vel_ap[3 * i + e] = v[e];
+        }
+    }
+    if (f_out) for (size_t k = 0; k < 3 * (size_t)n; ++k) f_out[k] = RND(P, f[k]);
+    if (nbr_counts) memcpy(nbr_counts, counts, sizeof(int32_t) * (size_t)n);
+    if (st) { st->iters = 0; st->converged = 1; }
+    free(counts); free(list); free(f);
+    return 0;
+}
+
 int orc_step(const orc_params* P, orc_state* S, orc_stats* st, double* rho_x, double* f_np, int32_t* nbr_counts) {
     if (st) memset(st, 0, sizeof(*st));
     if (P->n <= 0) return 0;
+    if (P->method == ORC_DEM) return step_dem(P, S, st, f_np, nbr_counts);
     if (P->method == ORC_PCISPH) return step_pcisph(P, S, st, rho_x, f_np, nbr_counts);
     return step_wcsph(P, S, st, rho_x, f_np, nbr_counts);
 }

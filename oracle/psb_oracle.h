@@ -18,7 +18,7 @@ extern "C" {
 #endif
 
 enum { ORC_PROFILE_REF = 0, ORC_PROFILE_CONFIG = 1 };
-enum { ORC_WCSPH = 0, ORC_PCISPH = 1 };
+enum { ORC_WCSPH = 0, ORC_PCISPH = 1, ORC_DEM = 2 };
 
 typedef struct orc_params {
     int32_t n;
@@ -39,6 +39,7 @@ typedef struct orc_params {
     double spacing;                 /* config PCISPH prototype lattice spacing (0: (m/rho0)^(1/3)) */
     double skin;                    /* config: lists hold pairs within (1 + skin) h */
     double xsph;                    /* config PCISPH: XSPH velocity smoothing factor */
+    double dem_spring, dem_damping, dem_shear, dem_attraction;   /* DEM contact law */
 } orc_params;
 
 /* Config-profile PCISPH pressure factor delta = 1 / (beta (|sum gradW|^2 +

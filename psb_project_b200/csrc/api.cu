@@ -205,7 +205,19 @@ int validate(const psb_scene* s, std::string& why) {
     }
     const double ncells = (double)s->dims[0] * s->dims[1] * s->dims[2];
     if (ncells >= 4294967295.0) { why = "too many grid cells (>= 2^32 - 1)"; return PSB_EINVAL; }
-    if (s->method != PSB_WCSPH && s->method != PSB_PCISPH) { why = "unknown method"; return PSB_EINVAL; }
+    if (s->method != PSB_WCSPH && s->method != PSB_PCISPH && s->method != PSB_DEM) { why = "unknown method"; return PSB_EINVAL; }
+    if (s->method == PSB_DEM) {
+        if (!(s->dem_spring >= 0) || !(s->dem_damping >= 0) || !std::isfinite(s->dem_shear) ||
+            !std::isfinite(s->dem_attraction)) { why = "DEM: spring, damping must be >= 0"; return PSB_EINVAL; }
+        if (s->profile == PSB_PROFILE_CONFIG && (!(s->particle_radius > 0) || s->h < 2.0 * s->particle_radius * (1.0 - 1e-6))) {
+            why = "DEM config: particle_radius > 0 and h >= 2 particle_radius (contacts must be listed)";
+            return PSB_EINVAL;
+        }
+        if (s->profile == PSB_PROFILE_CONFIG && (s->dem_shear != 0 || s->dem_attraction != 0)) {
+            why = "DEM config: shear and attraction are reference-profile terms";
+            return PSB_EINVAL;
+        }
+    }
     if (s->profile != PSB_PROFILE_REF && s->profile != PSB_PROFILE_CONFIG) { why = "unknown profile"; return PSB_EINVAL; }
     if (s->min_iters < 0 || s->max_iters < s->min_iters || s->max_iters > PSB_MAX_ITERS) {
         why = "need 0 <= min_iters <= max_iters <= PSB_MAX_ITERS";
@@ -272,6 +284,19 @@ Params derive(const psb_scene& s) {
     P.whi_x = s.box_max[0] - s.particle_radius; P.whi_y = s.box_max[1] - s.particle_radius;
     P.whi_z = s.box_max[2] - s.particle_radius;
     P.xsph_k = (float)(P.ref || !P.pci ? 0.0 : s.xsph * 315.0 * m / (64.0 * pi * h * h * h) / s.rho0);
+    P.dem = s.method == PSB_DEM;
+    if (P.dem) {
+        P.pci = 0;
+        P.dem_k = (float)s.dem_spring;
+        P.dem_c = (float)s.dem_damping;
+        P.dem_s = (float)s.dem_shear;
+        P.dem_a = (float)s.dem_attraction;
+        // REF: collideDist = (float)(h_A + h_B), contact while d < 2 collideDist
+        P.dem_R = P.ref ? (float)(h + h) : (float)(2.0 * s.particle_radius);
+        P.dem_range = P.ref ? 2.f * P.dem_R : P.dem_R;
+        P.dem_mass = (float)m;
+        P.dem_inv_mass = (float)(1.0 / m);
+    }
     P.wall_k = (float)s.wall_k;     // config: penalty outside the faces (bx0..bz1)
     P.wall_c = (float)s.wall_c;
     P.bx0 = s.box_min[0]; P.by0 = s.box_min[1]; P.bz0 = s.box_min[2];
@@ -367,10 +392,12 @@ int build(psb_ctx* c, bool keep_p = false) {
         psb::launch_build_nbr(st, P, c->pos[c->cs], c->keys[res], c->cell_start, c->cell_end, c->nbr_count, c->nbr_list,
                               c->flags);
     });
-    const int zero_p = !keep_p && P.pci && (P.ref || c->sc.warm_start == PSB_WARM_ZERO);
-    timed(c, "density_x", [&] {
-        psb::launch_density_x(st, P, c->pos[c->cs], c->nbr_count, c->nbr_list, c->rp[c->cr], c->rho_x, zero_p);
-    });
+    if (!P.dem) {
+        const int zero_p = !keep_p && P.pci && (P.ref || c->sc.warm_start == PSB_WARM_ZERO);
+        timed(c, "density_x", [&] {
+            psb::launch_density_x(st, P, c->pos[c->cs], c->nbr_count, c->nbr_list, c->rp[c->cr], c->rho_x, zero_p);
+        });
+    }
     c->built = true;
     return cuda_check(c, cudaGetLastError(), "launch");
 }
@@ -397,7 +424,16 @@ int step_once(psb_ctx* c, bool last) {
     const int s = c->cs, r = c->cr;
     int iters = 0, converged = 1;
     cudaMemsetAsync(c->err_hist, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1), st);
-    if (!P.pci) {
+    if (P.dem) {
+        const int o = s ^ 1;
+        timed(c, "dem_step", [&] {
+            psb::launch_dem_step(st, P, c->pos[s], c->vel[s], c->nbr_count, c->nbr_list, c->pos[o], c->vel[o], c->vap[o],
+                                 c->fnp);
+        });
+        c->cs = o;
+        c->stats.iters = 0;
+        c->stats.converged = 1;
+    } else if (!P.pci) {
         const int o = s ^ 1;
         timed(c, "wcsph_force", [&] {
             psb::launch_wcsph_force(st, P, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list,

@@ -52,6 +52,11 @@ struct Params {
     float wlo_x, wlo_y, wlo_z, whi_x, whi_y, whi_z;   // box min + r, box max - r (float, as collisionBox)
     float wall_k, wall_c;
     float xsph_k;       // config PCISPH XSPH: xsph * k_rho / rho0 (0: off)
+    // DEM: contact law constants (REF: k_s, c, s, a; CONFIG: k_n, c_n), the
+    // distance R in k (R - d) (REF: h_A + h_B as float; CONFIG: 2r), the
+    // contact range (REF: 2R; CONFIG: 2r), sphere mass and its inverse
+    float dem_k, dem_c, dem_s, dem_a, dem_R, dem_range, dem_mass, dem_inv_mass;
+    int dem;
     // Config-profile walls (mirror ghost particles across the box faces):
     float bx0, by0, bz0, bx1, by1, bz1;   // faces
     float hf;           // h
@@ -92,6 +97,8 @@ void launch_pci_commit(cudaStream_t st, const Params& P, const float4* xs, const
                        int have_density_pass, float4* pos, float4* vel, float4* vap, float2* rp);
 void launch_xsph(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const int* counts,
                  const int* list, float4* vs_out);
+void launch_dem_step(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
+                     const int* list, float4* pos_out, float4* vel_out, float4* vap_out, float4* force);
 
 // ---- learned warm start (mlp.cu) ---------------------------------------------------
 constexpr int kMlpParams = 4673;   // 6x64 + 64 + 64x64 + 64 + 64 + 1

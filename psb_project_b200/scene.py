@@ -51,6 +51,7 @@ PROFILE_REF = 0
 PROFILE_CONFIG = 1
 WCSPH = 0
 PCISPH = 1
+DEM = 2
 WARM_ZERO = 0
 WARM_PREVIOUS = 1
 WARM_LEARNED = 2
@@ -88,6 +89,10 @@ class PsbScene(ctypes.Structure):
         ("spacing", ctypes.c_double),
         ("skin", ctypes.c_double),
         ("xsph", ctypes.c_double),
+        ("dem_spring", ctypes.c_double),
+        ("dem_damping", ctypes.c_double),
+        ("dem_shear", ctypes.c_double),
+        ("dem_attraction", ctypes.c_double),
     ]
 
 
@@ -137,6 +142,10 @@ class Scene:
     spacing: float = 0.0
     skin: float = 0.0
     xsph: float = 0.0
+    dem_spring: float = 0.0
+    dem_damping: float = 0.0
+    dem_shear: float = 0.0
+    dem_attraction: float = 0.0
     blocks: List[Block] = dataclasses.field(default_factory=list)
     name: str = ""
     steps: int = 0
@@ -160,6 +169,8 @@ class Scene:
         s.spacing = self.spacing
         s.skin = self.skin
         s.xsph = self.xsph
+        s.dem_spring, s.dem_damping = self.dem_spring, self.dem_damping
+        s.dem_shear, s.dem_attraction = self.dem_shear, self.dem_attraction
         return s
 
     def replace(self, **kw) -> "Scene":
@@ -241,6 +252,63 @@ def dam_break(
         min_iters=min_iters, max_iters=max_iters, eta=eta, wall_k=wk, wall_c=math.sqrt(wk),
         blocks=[Block(tuple(int(v) for v in nxyz), spacing, (0.0, 0.0, 0.0), jitter, seed)],
         name=name, steps=steps, nbr_cap=nbr_cap, spacing=spacing, skin=skin, xsph=xsph,
+    )
+
+
+def dashpot_from_restitution(k_n: float, mass: float, restitution: float) -> float:
+    """Normal dashpot c_n of a linear spring-dashpot contact between two
+    equal spheres of this mass that gives the coefficient of restitution e:
+    c_n = 2 zeta sqrt(k_n m_eff), m_eff = m/2, zeta = -ln e / sqrt(pi^2 + ln^2 e)
+    (the damped oscillator's half-period rebound)."""
+    le = math.log(restitution)
+    zeta = -le / math.sqrt(math.pi ** 2 + le ** 2)
+    return 2.0 * zeta * math.sqrt(k_n * mass / 2.0)
+
+
+def dem_block(
+    nxyz: Sequence[int],
+    spacing: float,
+    origin: Sequence[float],
+    box: Sequence[float],
+    radius: float,
+    *,
+    profile: int = PROFILE_CONFIG,
+    density: float = 2500.0,
+    k_n: float = 1e4,
+    restitution: float = 0.3,
+    spring: float = 0.0,
+    damping: float = 0.0,
+    shear: float = 0.0,
+    attraction: float = 0.0,
+    h: Optional[float] = None,
+    dt: float = 1e-4,
+    jitter: float = 1e-4,
+    seed: int = 0,
+    name: str = "",
+) -> Scene:
+    """A lattice block of DEM spheres (PSB_DEM) in a box [0, box].
+
+    Config profile: linear spring-dashpot with k_n and the dashpot for the
+    given restitution; the lists hold every pair within h = 2 radius.
+    Reference profile: collideParticle's spring, damping, shear and
+    attraction, over lists of radius h (the interaction radius)."""
+    box_min = (0.0, 0.0, 0.0)
+    box_max = tuple(float(b) for b in box)
+    m = 4.0 / 3.0 * math.pi * radius ** 3 * density
+    if h is None:
+        h = 2.0 * radius
+    cell = cell_for(h, exact_reference=(profile == PROFILE_REF))
+    gmin, dims = grid_for(box_min, box_max, cell)
+    if profile == PROFILE_CONFIG:
+        spring, damping = k_n, dashpot_from_restitution(k_n, m, restitution)
+    n = int(nxyz[0]) * int(nxyz[1]) * int(nxyz[2])
+    return Scene(
+        n=n, box_min=box_min, box_max=box_max, grid_min=gmin, cell=cell, dims=dims, h=h, mass=m,
+        rho0=density, k=0.0, mu=0.0, sigma=0.0, l=0.0, particle_radius=f32(radius), dt=f32(dt), method=DEM,
+        profile=profile, min_iters=0, max_iters=0, eta=0.0, wall_k=0.0, wall_c=0.0,
+        blocks=[Block(tuple(int(v) for v in nxyz), spacing, tuple(float(o) for o in origin), jitter, seed)],
+        name=name, steps=0, nbr_cap=64, spacing=spacing, dem_spring=spring, dem_damping=damping,
+        dem_shear=shear, dem_attraction=attraction,
     )
 
 
