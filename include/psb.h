@@ -166,6 +166,42 @@ int psb_presolve(psb_ctx* ctx, int32_t iters);
  * PciSphSystem_Kernel.cu:70-85). */
 int psb_build_neighbors(psb_ctx* ctx);
 
+/* Node grid of the iso field and the marching cubes: dims[a] nodes along
+ * axis a at origin[a] + i spacing[a], x fastest. Replaces
+ * createGrid_MarchingCube_CUDA (MarchingCube.cu:12-27), whose nodes sit at
+ * centre - L/2 + sizeCell/2 + i sizeCell. */
+typedef struct psb_iso_grid {
+    double origin[3];
+    double spacing[3];
+    int32_t dims[3];
+    double scale;               /* REF profile: evaluateIso's scale -- influence radius h/scale over
+                                   floor(1/scale) rings of particle-grid cells (SurfaceSPH::extract
+                                   uses 0.65, SurfaceSPH.cpp:31) */
+} psb_iso_grid;
+
+/* The iso field at every node of `grid`, at the current positions (the
+ * particle grid is rebuilt first). REF profile: evaluateIso_Kernel
+ * (UniformGridKernel.cu:98-138), sum over particles within r = h/scale of
+ * (r^2 - d^2)^3 / r^6. CONFIG profile: the density-based colour field
+ * sum_j (m/rho_j) W_poly6(|x - x_j|, h). iso: host buffer of
+ * dims[0] dims[1] dims[2] doubles (NULL: leave it on the device). SPH scenes
+ * only. */
+int psb_iso_field(psb_ctx* ctx, const psb_iso_grid* grid, double* iso);
+
+/* Marching cubes at `level` over the iso field of `grid`; replaces
+ * polygonize_MarchingCube_CUDA (MarchingCube.cu:31-46) and the host vertex
+ * weld of SurfaceSPH::extract (SurfaceSPH.cpp:120-186). Corner and edge
+ * numbering, the case bit (iso <= level) and the vertex interpolation are
+ * the reference's; the triangle table is generated from the cube's faces,
+ * and every grid edge owns one vertex, so the mesh comes out welded.
+ * On entry *n_vertices and *n_triangles are the capacities of `vertices`
+ * (float x3 each) and `triangles` (int32 x3 vertex indices, normals toward
+ * iso <= level); on return they are the counts. With both buffers NULL only
+ * the counts are returned; a buffer too small gives PSB_EINVAL with the
+ * counts set. */
+int psb_extract_surface(psb_ctx* ctx, const psb_iso_grid* grid, double level, float* vertices,
+                        int64_t* n_vertices, int32_t* triangles, int64_t* n_triangles);
+
 /* Copies one field out (see PSB_FIELD_*); `bytes` is the destination size. */
 int psb_read_field(psb_ctx* ctx, int32_t field, void* dst, size_t bytes);
 

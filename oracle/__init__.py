@@ -65,6 +65,76 @@ _lib = None
 _ref = None
 
 
+class IsoGrid(ctypes.Structure):
+    """orc_iso_grid: dims[a] nodes at origin[a] + i spacing[a], x fastest."""
+    _fields_ = [("origin", ctypes.c_double * 3), ("spacing", ctypes.c_double * 3), ("dims", ctypes.c_int32 * 3),
+                ("scale", ctypes.c_double)]
+
+
+def iso_grid(origin, spacing, dims, scale=0.65) -> IsoGrid:
+    g = IsoGrid()
+    g.origin[:] = [float(v) for v in origin]
+    sp = spacing if hasattr(spacing, "__len__") else (spacing,) * 3
+    g.spacing[:] = [float(v) for v in sp]
+    g.dims[:] = [int(v) for v in dims]
+    g.scale = float(scale)
+    return g
+
+
+def grid_nodes(g: IsoGrid) -> np.ndarray:
+    """Node positions (x fastest), shape (nx*ny*nz, 3)."""
+    axes = [g.origin[a] + np.arange(g.dims[a]) * g.spacing[a] for a in range(3)]
+    z, y, x = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    return np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
+
+
+def iso_field(scene, pos, rho, g: IsoGrid) -> np.ndarray:
+    pos = np.ascontiguousarray(pos, np.float64)
+    rho = np.ascontiguousarray(rho if rho is not None else np.ones(pos.shape[0]), np.float64)
+    out = np.zeros(int(np.prod(list(g.dims))))
+    P = params(scene, n=pos.shape[0])
+    lib().orc_iso_field(ctypes.byref(P), _ptr(pos), _ptr(rho), ctypes.byref(g), _ptr(out))
+    return out
+
+
+def mc_table():
+    ntri = np.zeros(256, np.uint8)
+    tri = np.zeros((256, 30), np.int8)
+    lib().orc_mc_table(_ptr(ntri), _ptr(tri))
+    return ntri, tri
+
+
+def marching_cubes(g: IsoGrid, iso, level):
+    """(vertices (V, 3) float64, triangles (T, 3) int32)."""
+    iso = np.ascontiguousarray(iso, np.float64)
+    nv = ctypes.c_int64(0)
+    nt = ctypes.c_int64(0)
+    lib().orc_marching_cubes(ctypes.byref(g), _ptr(iso), float(level), 0, None, ctypes.byref(nv), 0, None,
+                             ctypes.byref(nt))
+    vert = np.zeros((max(nv.value, 1), 3))
+    tri = np.zeros((max(nt.value, 1), 3), np.int32)
+    rc = lib().orc_marching_cubes(ctypes.byref(g), _ptr(iso), float(level), nv.value, _ptr(vert), ctypes.byref(nv),
+                                  nt.value, _ptr(tri), ctypes.byref(nt))
+    if rc != 0:
+        raise RuntimeError("orc_marching_cubes: capacity")
+    return vert[:nv.value], tri[:nt.value]
+
+
+def ref_marching_cubes(g: IsoGrid, iso, level) -> np.ndarray:
+    """The reference's polygonize kernel on the same nodes: triangle corners
+    (3 per triangle) in cell order, shape (3T, 3)."""
+    nodes4 = np.concatenate([grid_nodes(g), np.asarray(iso, np.float64)[:, None]], 1)
+    nodes4 = np.ascontiguousarray(nodes4)
+    cap = 16 * nodes4.shape[0] + 64
+    out = np.zeros((cap, 3))
+    nv = ctypes.c_int64(0)
+    rc = ref_lib().ref_marching_cubes(_ptr(nodes4), int(g.dims[0]), int(g.dims[1]), int(g.dims[2]), float(level),
+                                      cap, _ptr(out), ctypes.byref(nv))
+    if rc != 0:
+        raise RuntimeError("ref_marching_cubes: capacity")
+    return out[:nv.value]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -89,6 +159,13 @@ def lib():
         L.orc_presolve.restype = ctypes.c_int
         L.orc_pci_delta.argtypes = [ctypes.POINTER(OrcParams)]
         L.orc_pci_delta.restype = ctypes.c_double
+        L.orc_iso_field.argtypes = [ctypes.POINTER(OrcParams), P, P, ctypes.POINTER(IsoGrid), P]
+        L.orc_iso_field.restype = None
+        L.orc_mc_table.argtypes = [P, P]
+        L.orc_mc_table.restype = None
+        L.orc_marching_cubes.argtypes = [ctypes.POINTER(IsoGrid), P, ctypes.c_double, ctypes.c_int64, P, P,
+                                         ctypes.c_int64, P, P]
+        L.orc_marching_cubes.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -115,6 +192,9 @@ def ref_lib():
         L.ref_pcisph_update.argtypes = [P, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_float, P, P]
         L.ref_wcsph_update.argtypes = [P, ctypes.c_float, P, ctypes.c_float, ctypes.c_int, ctypes.c_float, P, P]
         L.ref_dem_update.argtypes = [P, ctypes.c_float, P, ctypes.c_float, ctypes.c_int, ctypes.c_float, P, P]
+        L.ref_iso.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, P]
+        L.ref_marching_cubes.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int64,
+                                         P, P]
         _ref = L
     return _ref
 
@@ -305,6 +385,16 @@ class RefSim:
         rc = ref_lib().ref_pcisph_update(self.h, s.dt, iters, 1 if collide else 0, s.particle_radius, _ptr(bmin), _ptr(bmax))
         if rc != 0:
             raise RuntimeError(f"ref_pcisph_update: {rc}")
+
+    def iso(self, g: IsoGrid) -> np.ndarray:
+        """evaluateIso_Kernel over the nodes of g, at the current positions."""
+        nodes = np.ascontiguousarray(grid_nodes(g))
+        out = np.zeros(nodes.shape[0])
+        rc = ref_lib().ref_iso(self.h, _ptr(nodes), int(g.dims[0]), int(g.dims[1]), int(g.dims[2]), float(g.scale),
+                               _ptr(out))
+        if rc != 0:
+            raise RuntimeError(f"ref_iso: {rc}")
+        return out
 
     def dem_update(self, collide=True):
         """CudaSystem::update (CudaSystem.cpp:207-224) on the state, the

@@ -755,3 +755,214 @@ int orc_step(const orc_params* P, orc_state* S, orc_stats* st, double* rho_x, do
     if (P->method == ORC_PCISPH) return step_pcisph(P, S, st, rho_x, f_np, nbr_counts);
     return step_wcsph(P, S, st, rho_x, f_np, nbr_counts);
 }
+
+/* ---- iso field and marching cubes ------------------------------------------
+ * Iso field, reference profile: evaluateIso_Kernel (UniformGridKernel.cu:
+ * 98-138) -- the node's particle-grid cell (I, J, K) = floor((x - Min) /
+ * sizeCell), floor(1/scale) rings of cells around it, and for each particle
+ * with d = length(x - x_j) <= r = h/scale the float term
+ * (1/powf(r,6)) * powf(r*r - d*d, 3) added to a double sum. Config profile:
+ * the colour field sum_j (m/rho_j) 315/(64 pi h^9) (h^2 - d^2)^3 over the
+ * adjacent cells. Cells are walked x outer, z inner, particles within a cell
+ * in increasing id (the GPU's sorted order). */
+void orc_iso_field(const orc_params* P, const double* pos, const double* rho, const orc_iso_grid* g, double* iso) {
+    const int32_t n = P->n;
+    const uint32_t ncells = (uint32_t)P->dims[0] * (uint32_t)P->dims[1] * (uint32_t)P->dims[2];
+    uint32_t* keys = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+    int32_t* perm = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    int32_t* start = (int32_t*)malloc(sizeof(int32_t) * ((size_t)ncells + 1));
+    orc_cell_keys(n, pos, P->grid_min, P->cell, P->dims, keys, NULL);
+    sort_by_key(n, keys, ncells, perm, start);
+    const int ref = P->profile == ORC_PROFILE_REF;
+    const double h = P->h;
+    const double r = ref ? h / g->scale : h;
+    const int ring = ref ? (int)floor(1.0 / g->scale) : 1;
+    const double kc = 315.0 * P->mass / (64.0 * PI_D * h * h * h);
+    const int64_t nn = (int64_t)g->dims[0] * g->dims[1] * g->dims[2];
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t node = 0; node < nn; ++node) {
+        const int ix = (int)(node % g->dims[0]), iy = (int)((node / g->dims[0]) % g->dims[1]);
+        const int iz = (int)(node / ((int64_t)g->dims[0] * g->dims[1]));
+        const double px = g->origin[0] + ix * g->spacing[0];
+        const double py = g->origin[1] + iy * g->spacing[1];
+        const double pz = g->origin[2] + iz * g->spacing[2];
+        const int I = (int)floor((px - (double)P->grid_min[0]) / (double)P->cell);
+        const int J = (int)floor((py - (double)P->grid_min[1]) / (double)P->cell);
+        const int K = (int)floor((pz - (double)P->grid_min[2]) / (double)P->cell);
+        double acc = 0.0;
+        for (int i = I - ring; i <= I + ring; ++i) {
+            if (i < 0 || i >= P->dims[0]) continue;
+            for (int j = J - ring; j <= J + ring; ++j) {
+                if (j < 0 || j >= P->dims[1]) continue;
+                for (int k = K - ring; k <= K + ring; ++k) {
+                    if (k < 0 || k >= P->dims[2]) continue;
+                    const uint32_t c = (uint32_t)i + (uint32_t)j * P->dims[0] + (uint32_t)k * P->dims[0] * P->dims[1];
+                    for (int32_t t = start[c]; t < start[c + 1]; ++t) {
+                        const int32_t q = perm[t];
+                        const double dx = px - pos[3 * q], dy = py - pos[3 * q + 1], dz = pz - pos[3 * q + 2];
+                        const double d2 = dx * dx + dy * dy + dz * dz;
+                        if (ref) {
+                            const double d = sqrt(d2);
+                            if (!(d <= r)) continue;
+                            const float term = (1.0f / powf((float)r, 6.0f)) * powf((float)(r * r - d * d), 3.0f);
+                            acc += (double)term;
+                        } else {
+                            const double qq = d2 / (h * h);
+                            if (qq >= 1.0) continue;
+                            const double w = 1.0 - qq;
+                            acc += kc * (w * w * w) / rho[q];
+                        }
+                    }
+                }
+            }
+        }
+        iso[node] = acc;
+    }
+    free(keys); free(perm); free(start);
+}
+
+/* Corners (x, y, z offsets) and edges in the numbering of
+ * polygonize_MarchingCube_Kernel (MarchingCube_Kernel.cu:44-56, 100-124). */
+static const int MC_CORNER[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 0, 1}, {0, 0, 1}, {0, 1, 0}, {1, 1, 0}, {1, 1, 1}, {0, 1, 1}};
+static const int MC_EDGE[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+static const int MC_FACE[6][4] = {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 3, 7, 4}, {1, 2, 6, 5}, {0, 1, 5, 4}, {3, 2, 6, 7}};
+
+static int mc_edge_of(int a, int b) {
+    for (int e = 0; e < 12; ++e)
+        if ((MC_EDGE[e][0] == a && MC_EDGE[e][1] == b) || (MC_EDGE[e][0] == b && MC_EDGE[e][1] == a)) return e;
+    return -1;
+}
+
+/* The case table, generated: for case bits cs (corner c set when its value is
+ * <= level), each cube face joins its active edges into segments -- two
+ * active edges into one segment, four (two diagonal set corners) into two
+ * segments that each cut one set corner off -- and the segments close into
+ * loops over the cube surface. Each loop is oriented by comparing the Newell
+ * normal of its edge midpoints with the sum of (set - unset) corner offsets
+ * across its edges, so triangle normals point toward the set corners, and
+ * fanned from its first vertex. */
+void orc_mc_table(uint8_t* ntri, int8_t* tri) {
+    for (int cs = 0; cs < 256; ++cs) {
+        int link[12][2], deg[12] = {0}, used[12] = {0};
+        int8_t* out = &tri[cs * 30];
+        for (int k = 0; k < 30; ++k) out[k] = -1;
+        for (int f = 0; f < 6; ++f) {
+            const int* q = MC_FACE[f];
+            int act[4], na = 0;
+            for (int k = 0; k < 4; ++k) {
+                const int a = q[k], b = q[(k + 1) & 3];
+                if (((cs >> a) & 1) != ((cs >> b) & 1)) act[na++] = mc_edge_of(a, b);
+            }
+            if (na == 2) {
+                link[act[0]][deg[act[0]]++] = act[1];
+                link[act[1]][deg[act[1]]++] = act[0];
+            } else if (na == 4) {
+                for (int k = 0; k < 4; ++k) {
+                    if (!((cs >> q[k]) & 1)) continue;
+                    const int e0 = mc_edge_of(q[(k + 3) & 3], q[k]), e1 = mc_edge_of(q[k], q[(k + 1) & 3]);
+                    link[e0][deg[e0]++] = e1;
+                    link[e1][deg[e1]++] = e0;
+                }
+            }
+        }
+        int nt = 0;
+        for (int s0 = 0; s0 < 12; ++s0) {
+            if (deg[s0] != 2 || used[s0]) continue;
+            int loop[12], nl = 0, prev = -1, cur = s0;
+            do {
+                loop[nl++] = cur;
+                used[cur] = 1;
+                const int nxt = link[cur][0] != prev ? link[cur][0] : link[cur][1];
+                prev = cur;
+                cur = nxt;
+            } while (cur != s0 && nl < 12);
+            double mid[12][3], nrm[3] = {0, 0, 0}, dir[3] = {0, 0, 0};
+            for (int k = 0; k < nl; ++k) {
+                const int a = MC_EDGE[loop[k]][0], b = MC_EDGE[loop[k]][1];
+                const int sa = (cs >> a) & 1;
+                for (int d = 0; d < 3; ++d) {
+                    mid[k][d] = 0.5 * (MC_CORNER[a][d] + MC_CORNER[b][d]);
+                    dir[d] += sa ? MC_CORNER[a][d] - MC_CORNER[b][d] : MC_CORNER[b][d] - MC_CORNER[a][d];
+                }
+            }
+            for (int k = 0; k < nl; ++k) {
+                const double* p = mid[k];
+                const double* q = mid[(k + 1) % nl];
+                nrm[0] += (p[1] - q[1]) * (p[2] + q[2]);
+                nrm[1] += (p[2] - q[2]) * (p[0] + q[0]);
+                nrm[2] += (p[0] - q[0]) * (p[1] + q[1]);
+            }
+            const int flip = nrm[0] * dir[0] + nrm[1] * dir[1] + nrm[2] * dir[2] < 0;
+            for (int k = 1; k + 1 < nl; ++k) {
+                out[3 * nt] = (int8_t)loop[0];
+                out[3 * nt + 1] = (int8_t)(flip ? loop[k + 1] : loop[k]);
+                out[3 * nt + 2] = (int8_t)(flip ? loop[k] : loop[k + 1]);
+                ++nt;
+            }
+        }
+        ntri[cs] = (uint8_t)nt;
+    }
+}
+
+/* vertexInterpolate_MarchingCube (MarchingCube_Kernel.cu:143-155) */
+static double mc_interp(double level, double v1, double v2, double p1, double p2) {
+    if (fabs(level - v1) < 0.000001) return p1;
+    if (fabs(level - v2) < 0.000001) return p2;
+    if (fabs(v1 - v2) < 0.000001) return p1;
+    const double mu = (level - v1) / (v2 - v1);
+    return p1 + mu * (p2 - p1);
+}
+
+int orc_marching_cubes(const orc_iso_grid* g, const double* iso, double level, int64_t vcap, double* vert,
+                       int64_t* nv, int64_t tcap, int32_t* tri, int64_t* nt) {
+    uint8_t ntri[256];
+    int8_t table[256 * 30];
+    orc_mc_table(ntri, table);
+    const int64_t X = g->dims[0], Y = g->dims[1], Z = g->dims[2], nn = X * Y * Z;
+    int64_t* vid = (int64_t*)malloc(sizeof(int64_t) * 3 * (size_t)nn);
+    int64_t v = 0, t = 0;
+    for (int64_t node = 0; node < nn; ++node) {
+        const int64_t x = node % X, y = (node / X) % Y, z = node / (X * Y);
+        const int64_t step[3] = {1, X, X * Y};
+        const int64_t c3[3] = {x, y, z};
+        for (int a = 0; a < 3; ++a) {
+            vid[3 * node + a] = -1;
+            if (c3[a] + 1 >= g->dims[a]) continue;
+            const double v1 = iso[node], v2 = iso[node + step[a]];
+            if ((v1 <= level) == (v2 <= level)) continue;
+            if (v < vcap && vert) {
+                for (int d = 0; d < 3; ++d) {
+                    const double p = g->origin[d] + c3[d] * g->spacing[d];
+                    vert[3 * v + d] = mc_interp(level, v1, v2, p, d == a ? p + g->spacing[d] : p);
+                }
+            }
+            vid[3 * node + a] = v++;
+        }
+    }
+    for (int64_t node = 0; node < nn; ++node) {
+        const int64_t x = node % X, y = (node / X) % Y, z = node / (X * Y);
+        if (x + 1 >= X || y + 1 >= Y || z + 1 >= Z) continue;
+        int cs = 0;
+        for (int c = 0; c < 8; ++c) {
+            const int64_t o = node + MC_CORNER[c][0] + MC_CORNER[c][1] * X + MC_CORNER[c][2] * X * Y;
+            if (iso[o] <= level) cs |= 1 << c;
+        }
+        for (int k = 0; k < ntri[cs]; ++k, ++t) {
+            if (t >= tcap || !tri) continue;
+            for (int m = 0; m < 3; ++m) {
+                const int e = table[cs * 30 + 3 * k + m];
+                const int a = MC_EDGE[e][0], b = MC_EDGE[e][1];
+                const int lo = (MC_CORNER[a][0] + MC_CORNER[a][1] + MC_CORNER[a][2]) <=
+                               (MC_CORNER[b][0] + MC_CORNER[b][1] + MC_CORNER[b][2]) ? a : b;
+                const int hi = lo == a ? b : a;
+                const int axis = MC_CORNER[hi][0] != MC_CORNER[lo][0] ? 0 : (MC_CORNER[hi][1] != MC_CORNER[lo][1] ? 1 : 2);
+                const int64_t ln = node + MC_CORNER[lo][0] + MC_CORNER[lo][1] * X + MC_CORNER[lo][2] * X * Y;
+                tri[3 * t + m] = (int32_t)vid[3 * ln + axis];
+            }
+        }
+    }
+    free(vid);
+    *nv = v;
+    *nt = t;
+    return (v > vcap || t > tcap) ? -1 : 0;
+}

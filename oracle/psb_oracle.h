@@ -102,6 +102,28 @@ int orc_step(const orc_params* P, orc_state* S, orc_stats* st, double* rho_x, do
  * positions and velocities restored afterwards; only S->p changes. */
 int orc_presolve(const orc_params* P, orc_state* S, int32_t iters, orc_stats* st);
 
+/* Node grid of the iso field: dims[a] nodes at origin[a] + i spacing[a], x fastest. */
+typedef struct orc_iso_grid {
+    double origin[3];
+    double spacing[3];
+    int32_t dims[3];
+    double scale;      /* reference profile: influence radius h/scale over floor(1/scale) cell rings */
+} orc_iso_grid;
+
+/* Iso field at every node. Reference profile: evaluateIso_Kernel
+ * (UniformGridKernel.cu:98-138). Config profile: sum_j (m/rho_j) W_poly6. */
+void orc_iso_field(const orc_params* P, const double* pos, const double* rho, const orc_iso_grid* g, double* iso);
+
+/* The generated marching-cubes case table: ntri[256], tri[256][30] (cube
+ * edge numbers, -1 padded). */
+void orc_mc_table(uint8_t* ntri, int8_t* tri);
+
+/* Marching cubes at `level` over a node field: vertices on active grid edges
+ * in (node, axis) order, triangles in cube order. Returns 0, or -1 when a
+ * capacity is exceeded; the counts are always set. */
+int orc_marching_cubes(const orc_iso_grid* g, const double* iso, double level, int64_t vcap, double* vert,
+                       int64_t* nv, int64_t tcap, int32_t* tri, int64_t* nt);
+
 #ifdef __cplusplus
 }
 #endif

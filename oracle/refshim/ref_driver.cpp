@@ -39,6 +39,7 @@
 #include <SphKernel.cuh>
 #include <PciSphSystem_Kernel.cuh>
 #include <CudaParticle_Kernel.cuh>
+#include <MarchingCube.cuh>
 #include <vector>
 #include <string>
 #include <cstdlib>
@@ -53,6 +54,11 @@ void collisionBox(int nbBodies, double3* newPos, double3* oldVel, double3* newVe
                   float elast, bool container, float radiusParticles, float dt);
 void evaluate_force_constante(uint nbBodies, double3* accumForceBuff, double* mass, float3 direction, float amplitude);
 void integrateEuler(uint nbBodies, double3* newPos, double3* newVel, double3* forces, double* mass, float dt);
+/* MarchingCube_Kernel.cu:36 (its header also defines the case tables, which
+ * that file's object already holds) */
+extern "C" void polygonize_MarchingCube_Kernel(double4* grid, uint nbCellsX, uint nbCellsY, uint nbCellsZ,
+                                               double isoLevel, int* nbIndex, double3* vertexs, double3* normales,
+                                               int* indexs);
 
 namespace {
 
@@ -389,6 +395,51 @@ int ref_dem_update(ref_sim* s, float dt, const float* gravity_dir, float gravity
         });
     }
     return 0;
+}
+
+/* SPHSystem::evaluateIso -> evaluateIso_CUDA -> evaluateIso_Kernel
+ * (UniformGridKernel.cu:98-138) over the node positions `nodes` (x fastest,
+ * nx*ny*nz nodes, xyz), with the grid rebuilt at the current positions.
+ * One emulated thread per node. */
+int ref_iso(ref_sim* s, const double* nodes, int nx, int ny, int nz, double scale, double* iso) {
+    int rc = ref_search(s);
+    if (rc) return rc;
+    const size_t nn = (size_t)nx * ny * nz;
+    std::vector<double4> grid4(nn);
+    for (size_t i = 0; i < nn; ++i) grid4[i] = make_double4(nodes[3 * i], nodes[3 * i + 1], nodes[3 * i + 2], 0.0);
+    UniformGrid* g = &s->grid;
+    launch_cells(nx, ny, nz, [&] {
+        evaluateIso_Kernel(grid4.data(), nx, ny, nz, scale, g->Min, g->sizeCell, g->nbCellsX, g->nbCellsY,
+                           g->nbCellsZ, g->nbParticles, g->indexParticles, (double3*)s->pos.data(), s->radius.data(),
+                           s->n);
+    });
+    for (size_t i = 0; i < nn; ++i) iso[i] = grid4[i].w;
+    return 0;
+}
+
+/* polygonize_MarchingCube_CUDA (MarchingCube.cu:31-46) over nodes given as
+ * (x, y, z, iso), x fastest. The kernel writes each cell's triangle corners
+ * to its own slots (nbVertexMax_perCell per cell); they are returned here in
+ * cell order, three per triangle: at most `cap` vertices, the count in *nv. */
+int ref_marching_cubes(const double* nodes4, int nx, int ny, int nz, double level, int64_t cap, double* vert,
+                       int64_t* nv) {
+    const size_t size = (size_t)nx + (size_t)nx * ny + (size_t)nx * ny * nz;   /* MarchingCube.cu's allocation */
+    std::vector<double4> grid4((size_t)nx * ny * nz);
+    std::memcpy(grid4.data(), nodes4, sizeof(double4) * grid4.size());
+    std::vector<int> nb(size, 0), idx(size * nbIndexMax_perCell, 0);
+    std::vector<double3> vx(size * nbVertexMax_perCell), nm(size * nbVertexMax_perCell);
+    launch_cells(nx, ny, nz, [&] {
+        polygonize_MarchingCube_Kernel(grid4.data(), nx, ny, nz, level, nb.data(), vx.data(), nm.data(), idx.data());
+    });
+    int64_t k = 0;
+    for (size_t c = 0; c < size; ++c)
+        for (int m = 0; m < nb[c]; ++m, ++k)
+            if (k < cap) {
+                const double3 p = vx[c * nbVertexMax_perCell + m];
+                vert[3 * k] = p.x; vert[3 * k + 1] = p.y; vert[3 * k + 2] = p.z;
+            }
+    *nv = k;
+    return k > cap ? -1 : 0;
 }
 
 }  /* extern "C" */

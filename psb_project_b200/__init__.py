@@ -7,9 +7,9 @@ Python host side: the scene description and a ctypes binding.
 """
 from .scene import (DEM, PCISPH, PROFILE_CONFIG, PROFILE_REF, WARM_LEARNED, WARM_PREVIOUS, WARM_ZERO, WCSPH, Block,
                     Scene, config_scene, dam_break, dashpot_from_restitution, dem_block, ref_scene)
-from .runtime import PsbError, Simulation, lattice, lib, mlp_init_weights, mlp_unpack, scene_positions
+from .runtime import IsoGrid, PsbError, Simulation, iso_grid, lattice, lib, mlp_init_weights, mlp_unpack, scene_positions
 
 __all__ = ["Scene", "Block", "Simulation", "PsbError", "config_scene", "dam_break", "ref_scene", "lattice",
            "scene_positions", "lib", "PCISPH", "WCSPH", "PROFILE_REF", "PROFILE_CONFIG", "WARM_ZERO",
            "WARM_PREVIOUS", "WARM_LEARNED", "mlp_init_weights", "mlp_unpack", "DEM", "dem_block",
-           "dashpot_from_restitution"]
+           "dashpot_from_restitution", "IsoGrid", "iso_grid"]

@@ -123,6 +123,15 @@ struct psb_ctx {
     int64_t collect_steps = 0;
     uint32_t* sel = nullptr;
     int sel_cap = 0;
+    // iso field and marching cubes (grown on demand)
+    double* iso = nullptr;
+    uint32_t* mc_cube = nullptr;   // per-node triangle counts -> offsets
+    uint32_t* mc_edge = nullptr;   // per-edge flags -> vertex offsets
+    uint32_t* mc_scratch = nullptr;
+    float* mc_vert = nullptr;
+    int32_t* mc_tri = nullptr;
+    long long iso_cap = 0, mc_cube_cap = 0, mc_edge_cap = 0, mc_scratch_cap = 0, mc_vert_cap = 0, mc_tri_cap = 0;
+    bool mc_table = false;
     // host mirrors
     unsigned long long* h_err = nullptr;
     int* h_flags = nullptr;
@@ -186,6 +195,8 @@ void free_all(psb_ctx* c) {
     cudaFree(c->err_hist); cudaFree(c->flags); cudaFree(c->stage);
     cudaFree(c->feats); cudaFree(c->mlp_w); cudaFree(c->mlp_m1); cudaFree(c->mlp_m2); cudaFree(c->mlp_grad);
     cudaFree(c->mlp_loss); cudaFree(c->mlp_wbf); cudaFree(c->ds_X); cudaFree(c->ds_T); cudaFree(c->sel);
+    cudaFree(c->iso); cudaFree(c->mc_cube); cudaFree(c->mc_edge); cudaFree(c->mc_scratch); cudaFree(c->mc_vert);
+    cudaFree(c->mc_tri);
     cudaFreeHost(c->h_err); cudaFreeHost(c->h_flags);
 }
 
@@ -902,6 +913,120 @@ int psb_build_neighbors(psb_ctx* c) {
     cudaSetDevice(c->device);
     PSB_TRY(build(c));
     return read_flags(c);
+}
+
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+int grow(psb_ctx* c, T** p, long long* cap, long long need) {
+    if (need <= *cap) return PSB_OK;
+    cudaStreamSynchronize(c->stream);
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    PSB_TRY(dalloc(c, p, (size_t)need));
+    *cap = need;
+    return PSB_OK;
+}
+
+// Iso field of `g` into c->iso at the current positions (grid rebuilt first).
+int iso_on_device(psb_ctx* c, const psb_iso_grid* g, double level, psb::IsoParams& Q) {
+    if (!g) return fail(c, PSB_EINVAL, "iso grid is NULL");
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "iso field before psb_upload");
+    if (c->P.dem) return fail(c, PSB_EINVAL, "iso field: SPH scenes only");
+    long long nn = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (g->dims[a] < 2 || !(g->spacing[a] > 0) || !std::isfinite(g->origin[a]))
+            return fail(c, PSB_EINVAL, "iso grid: dims >= 2, spacing > 0, finite origin");
+        nn *= g->dims[a];
+    }
+    if (3 * nn + 1 >= (1LL << 30)) return fail(c, PSB_EINVAL, "iso grid: at most 2^30 / 3 nodes");
+    Q = psb::IsoParams{};
+    for (int a = 0; a < 3; ++a) {
+        Q.origin[a] = g->origin[a];
+        Q.spacing[a] = g->spacing[a];
+        Q.dims[a] = g->dims[a];
+    }
+    Q.level = level;
+    const double h = c->sc.h;
+    if (c->P.ref) {
+        if (!(g->scale > 0)) return fail(c, PSB_EINVAL, "iso grid: reference profile needs scale > 0");
+        Q.r = h / g->scale;
+        Q.ring = (int)std::floor(1.0 / g->scale);
+    } else {
+        Q.ring = 1;      // cell >= h
+        Q.inv_r2 = 1.0 / (h * h);
+        Q.k_colour = 315.0 * c->sc.mass / (64.0 * 3.14159265358979323846 * h * h * h);
+    }
+    cudaSetDevice(c->device);
+    PSB_TRY(build(c, /*keep_p=*/true));
+    PSB_TRY(grow(c, &c->iso, &c->iso_cap, nn));
+    Params P = c->P;
+    P.n = c->n;
+    timed(c, "iso_field", [&] {
+        psb::launch_iso_field(c->stream, Q, P, c->pos[c->cs], c->rp[c->cr], c->cell_start, c->cell_end, c->iso);
+    });
+    return cuda_check(c, cudaGetLastError(), "iso field");
+}
+
+}  // namespace
+
+extern "C" {
+
+int psb_iso_field(psb_ctx* c, const psb_iso_grid* g, double* iso) {
+    if (!c) return PSB_EINVAL;
+    psb::IsoParams Q;
+    PSB_TRY(iso_on_device(c, g, 0.0, Q));
+    const long long nn = (long long)Q.dims[0] * Q.dims[1] * Q.dims[2];
+    if (iso)
+        PSB_TRY(cuda_check(c, cudaMemcpyAsync(iso, c->iso, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream), "iso"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "iso"));
+    return read_flags(c);
+}
+
+int psb_extract_surface(psb_ctx* c, const psb_iso_grid* g, double level, float* vertices, int64_t* n_vertices,
+                        int32_t* triangles, int64_t* n_triangles) {
+    if (!c || !n_vertices || !n_triangles) return PSB_EINVAL;
+    psb::IsoParams Q;
+    PSB_TRY(iso_on_device(c, g, level, Q));
+    cudaStream_t st = c->stream;
+    const long long nn = (long long)Q.dims[0] * Q.dims[1] * Q.dims[2];
+    if (!c->mc_table) {
+        psb::mc_upload_table(st);
+        c->mc_table = true;
+    }
+    // counts per cube (indexed by its lowest node) and per node edge, one
+    // trailing zero each: their in-place exclusive scans end in the totals
+    const long long cube_n = nn + 1, edge_n = 3 * nn + 1;
+    PSB_TRY(grow(c, &c->mc_cube, &c->mc_cube_cap, cube_n));
+    PSB_TRY(grow(c, &c->mc_edge, &c->mc_edge_cap, edge_n));
+    PSB_TRY(grow(c, &c->mc_scratch, &c->mc_scratch_cap, psb::scan_scratch_words(edge_n)));
+    timed(c, "mc_classify", [&] { psb::launch_mc_classify(st, Q, c->iso, c->mc_cube, c->mc_edge); });
+    timed(c, "mc_scan", [&] {
+        psb::scan_exclusive_u32(st, edge_n, c->mc_edge, c->mc_scratch);
+        psb::scan_exclusive_u32(st, cube_n, c->mc_cube, c->mc_scratch);
+    });
+    uint32_t tot[2] = {0, 0};
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(&tot[0], c->mc_edge + 3 * nn, 4, cudaMemcpyDeviceToHost, st), "mc"));
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(&tot[1], c->mc_cube + nn, 4, cudaMemcpyDeviceToHost, st), "mc"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "mc"));
+    const int64_t nv = tot[0], nt = tot[1];
+    const bool fits = (!vertices || nv <= *n_vertices) && (!triangles || nt <= *n_triangles);
+    *n_vertices = nv;
+    *n_triangles = nt;
+    if (!vertices && !triangles) return PSB_OK;
+    if (!fits) return fail(c, PSB_EINVAL, "psb_extract_surface: output buffers too small (counts returned)");
+    PSB_TRY(grow(c, &c->mc_vert, &c->mc_vert_cap, 3 * (nv > 0 ? nv : 1)));
+    PSB_TRY(grow(c, &c->mc_tri, &c->mc_tri_cap, 3 * (nt > 0 ? nt : 1)));
+    timed(c, "mc_emit", [&] { psb::launch_mc_emit(st, Q, c->iso, c->mc_edge, c->mc_cube, c->mc_vert, c->mc_tri); });
+    if (vertices && nv)
+        PSB_TRY(cuda_check(c, cudaMemcpyAsync(vertices, c->mc_vert, sizeof(float) * 3 * nv, cudaMemcpyDeviceToHost, st), "mc"));
+    if (triangles && nt)
+        PSB_TRY(cuda_check(c, cudaMemcpyAsync(triangles, c->mc_tri, sizeof(int32_t) * 3 * nt, cudaMemcpyDeviceToHost, st), "mc"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "mc"));
+    return cuda_check(c, cudaGetLastError(), "mc");
 }
 
 int psb_read_field(psb_ctx* c, int32_t field, void* dst, size_t bytes) {

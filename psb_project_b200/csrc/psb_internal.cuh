@@ -100,6 +100,29 @@ void launch_xsph(cudaStream_t st, const Params& P, const float4* xs, const float
 void launch_dem_step(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
                      const int* list, float4* pos_out, float4* vel_out, float4* vap_out, float4* force);
 
+// ---- iso field and marching cubes (mc.cu) ----------------------------------------
+constexpr int kMcMaxTri = 10;       // at most 12 active edges in loops of >= 3: 12 - 2 triangles
+struct IsoParams {
+    double origin[3];   // node (0, 0, 0)
+    double spacing[3];  // node spacing per axis
+    int dims[3];        // nodes per axis
+    double level;       // iso level of the surface
+    double r;           // REF: influence radius h / scale
+    int ring;           // cells of the particle grid walked on each side of the node's cell
+    double inv_r2;      // CONFIG: 1 / h^2
+    double k_colour;    // CONFIG: m 315 / (64 pi h^3): c(x) = k_colour sum (1 - q)^3 / rho_j
+};
+void mc_build_table(uint8_t ntri[256], int8_t tri[256][kMcMaxTri * 3]);
+void mc_upload_table(cudaStream_t st);
+long long scan_scratch_words(long long n);
+void scan_exclusive_u32(cudaStream_t st, long long n, uint32_t* data, uint32_t* scratch);
+void launch_iso_field(cudaStream_t st, const IsoParams& Q, const Params& P, const float4* pos, const float2* rp,
+                      const uint32_t* cell_start, const uint32_t* cell_end, double* iso);
+void launch_mc_classify(cudaStream_t st, const IsoParams& Q, const double* iso, uint32_t* cube_tris,
+                        uint32_t* edge_flag);
+void launch_mc_emit(cudaStream_t st, const IsoParams& Q, const double* iso, const uint32_t* edge_off,
+                    const uint32_t* tri_off, float* vert, int32_t* tris);
+
 // ---- learned warm start (mlp.cu) ---------------------------------------------------
 constexpr int kMlpParams = 4673;   // 6x64 + 64 + 64x64 + 64 + 64 + 1
 void launch_features(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float2* rp,

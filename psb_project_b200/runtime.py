@@ -37,7 +37,7 @@ EXPORTS = (
     "psb_profile_enable", "psb_profile_read", "psb_profile_reset", "psb_lattice", "psb_status_string",
     "psb_last_error", "psb_abi_version", "psb_sort_cells_noalloc", "psb_presolve", "psb_mlp_set_weights",
     "psb_mlp_get_weights", "psb_mlp_collect", "psb_mlp_dataset", "psb_mlp_train", "psb_mlp_forward",
-    "psb_mlp_loss_grad",
+    "psb_mlp_loss_grad", "psb_iso_field", "psb_extract_surface",
 )
 MLP_PARAMS = 4673       # PSB_MLP_PARAMS
 MLP_IN, MLP_H = 6, 64
@@ -50,6 +50,24 @@ class PsbStepStats(ctypes.Structure):
         ("clamped", ctypes.c_int32), ("nbr_total", ctypes.c_int64),
         ("err", ctypes.c_double * (PSB_MAX_ITERS + 1)), ("steps", ctypes.c_int64), ("iters_total", ctypes.c_int64),
     ]
+
+
+class IsoGrid(ctypes.Structure):
+    """psb_iso_grid: dims[a] nodes along axis a at origin[a] + i spacing[a], x fastest."""
+    _fields_ = [("origin", ctypes.c_double * 3), ("spacing", ctypes.c_double * 3), ("dims", ctypes.c_int32 * 3),
+                ("scale", ctypes.c_double)]
+
+
+def iso_grid(origin, spacing, dims, scale: float = 0.65) -> IsoGrid:
+    """A node grid; `spacing` is one value or one per axis. `scale` is the
+    reference profile's influence-radius divisor (SurfaceSPH::extract: 0.65)."""
+    g = IsoGrid()
+    g.origin[:] = [float(v) for v in origin]
+    sp = spacing if hasattr(spacing, "__len__") else (spacing,) * 3
+    g.spacing[:] = [float(v) for v in sp]
+    g.dims[:] = [int(v) for v in dims]
+    g.scale = float(scale)
+    return g
 
 
 class PsbError(RuntimeError):
@@ -99,6 +117,9 @@ def lib():
         "psb_mlp_train": ([P, I32, I32, ctypes.c_float, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
         "psb_mlp_forward": ([P, P, I32, P], ctypes.c_int),
         "psb_mlp_loss_grad": ([P, P, P, I32, ctypes.POINTER(ctypes.c_float), P], ctypes.c_int),
+        "psb_iso_field": ([P, ctypes.POINTER(IsoGrid), P], ctypes.c_int),
+        "psb_extract_surface": ([P, ctypes.POINTER(IsoGrid), ctypes.c_double, P, ctypes.POINTER(I64), P,
+                                 ctypes.POINTER(I64)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -271,6 +292,24 @@ class Simulation:
 
     def build_neighbors(self):
         self._check(lib().psb_build_neighbors(self._h), "psb_build_neighbors")
+
+    def iso_field(self, grid: IsoGrid) -> np.ndarray:
+        """psb_iso_field: the field at every node (x fastest), float64."""
+        out = np.empty(int(grid.dims[0]) * int(grid.dims[1]) * int(grid.dims[2]), np.float64)
+        self._check(lib().psb_iso_field(self._h, ctypes.byref(grid), _ptr(out)), "psb_iso_field")
+        return out
+
+    def extract_surface(self, grid: IsoGrid, level: float):
+        """psb_extract_surface: (vertices (V, 3) float32, triangles (T, 3) int32)."""
+        nv = ctypes.c_int64(0)
+        nt = ctypes.c_int64(0)
+        self._check(lib().psb_extract_surface(self._h, ctypes.byref(grid), float(level), None, ctypes.byref(nv), None,
+                                              ctypes.byref(nt)), "psb_extract_surface")
+        vert = np.empty((max(nv.value, 1), 3), np.float32)
+        tri = np.empty((max(nt.value, 1), 3), np.int32)
+        self._check(lib().psb_extract_surface(self._h, ctypes.byref(grid), float(level), _ptr(vert), ctypes.byref(nv),
+                                              _ptr(tri), ctypes.byref(nt)), "psb_extract_surface")
+        return vert[:nv.value], tri[:nt.value]
 
     def download(self, out: Optional[dict] = None) -> dict:
         n = self.n
