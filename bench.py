@@ -88,12 +88,6 @@ def parse():
     return ap.parse_args()
 
 
-def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
-
 
 def host_cores() -> int:
     try:
@@ -200,7 +194,8 @@ def cpu_baseline_port(sc, snap, steps: int) -> dict:
 
 
 def run_reference(args):
-    rank, world, _ = dist_env()
+    from psb_project_b200.replicas import env_ranks
+    rank, world, _ = env_ranks()
     if rank != 0:
         return
     import oracle
@@ -240,35 +235,26 @@ def run_ours(args):
     import torch
     import psb_project_b200 as P
 
-    rank, world, local = dist_env()
+    from psb_project_b200 import replicas
+    rep_ = replicas.init("nccl")
+    rank, world, local = rep_.rank, rep_.world, rep_.local
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     modes = {"zero": P.WARM_ZERO, "previous": P.WARM_PREVIOUS, "learned": P.WARM_LEARNED}
     base = P.config_scene(args.scene)
     if args.xsph is not None:
         base = base.replace(xsph=args.xsph)
     if world > 1:       # replicas: same scene, own seed per rank
-        base.blocks[0].seed = base.blocks[0].seed + 1000 * rank
+        base.blocks[0].seed = rep_.seed(base.blocks[0].seed)
     sc = base.replace(warm_start=modes[args.warm_start])
     n = sc.n
     stream = torch.cuda.current_stream()
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        rep_.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(ms):
-        t = torch.tensor([ms], device="cuda")
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = rep_.max_over_ranks
 
     def make(mode):
         s_ = P.Simulation(base.replace(warm_start=mode))
@@ -459,9 +445,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
         }
         print(json.dumps(out))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep_.close()
 
 
 def main():
