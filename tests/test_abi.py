@@ -93,3 +93,15 @@ def test_library_fails_loudly_when_missing(monkeypatch):
     monkeypatch.setattr(R, "LIB_PATH", "/nonexistent/libpsb.so")
     with pytest.raises(ImportError):
         R.lib()
+
+
+def test_every_compat_launcher_is_exported():
+    """include/psb_compat.h: the reference's launchers under their own names."""
+    src = open(os.path.join(ROOT, "include", "psb_compat.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = sorted(set(re.findall(r"^\s*void\s+(\w+)\s*\(", src, flags=re.M)))
+    assert {"createGrid", "storeParticles", "searchNeighbooring", "pci_SPH_update", "interactionSystem",
+            "collisionSystem_Box_CUDA"} <= set(names)
+    out = subprocess.run(["nm", "-D", "--defined-only", R.LIB_PATH], capture_output=True, text=True).stdout
+    for n in names:
+        assert re.search(rf"\bT {n}\b", out), n
