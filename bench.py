@@ -53,13 +53,12 @@ ALG_BYTES = {
     "radix_sort": 16,         # one read + write of the (key, value) pairs
     "reorder": 77,            # pos, vel, pressure 36 in + 36 out, cell ranges 5
     "build_nbr": 24,          # pos 16 + key 4 -> count 4
-    "density_x": 20,          # pos 16 -> rho 4
+    "density_x": 20,          # pos 16 -> rho 4 (learned: + vel 16, 8 features 32)
     "pci_init": 132,          # non-pressure forces 52 + first prediction 80
     "pci_density": 28,        # x* 16, p 4 -> p, rho* 8
     "pci_force_predict": 120,  # pressure force 40 + prediction 80
     "pci_commit": 96,         # final integrate, walls, interpolation
     "wcsph_force": 228,       # forces 52 + integrate 80 + walls/interpolation 96
-    "features": 72,           # pos, vel 32 + rho, p 8 -> 8 features 32
     "mlp_infer": 36,          # features 32 -> initial pressure 4
 }
 # Kernels per timed group (radix_sort is 3 kernels per 8-bit pass).

@@ -376,7 +376,7 @@ int bits_for(size_t ncells) {
 
 // Grid, sort, reorder, neighbour lists, density at x. keep_p: leave the
 // carried pressure in place even where the scene starts every step from 0.
-int build(psb_ctx* c, bool keep_p = false) {
+int build(psb_ctx* c, bool keep_p = false, bool features = false) {
     cudaStream_t st = c->stream;
     Params P = c->P;
     P.n = c->n;
@@ -405,8 +405,11 @@ int build(psb_ctx* c, bool keep_p = false) {
     });
     if (!P.dem) {
         const int zero_p = !keep_p && P.pci && (P.ref || c->sc.warm_start == PSB_WARM_ZERO);
+        // the learned warm start and its data collection take their inputs from this pass
+        float* feats = features ? c->feats : nullptr;
         timed(c, "density_x", [&] {
-            psb::launch_density_x(st, P, c->pos[c->cs], c->nbr_count, c->nbr_list, c->rp[c->cr], c->rho_x, zero_p);
+            psb::launch_density_x(st, P, c->pos[c->cs], c->vel[c->cs], c->nbr_count, c->nbr_list, c->rp[c->cr], c->rho_x,
+                                  zero_p, c->p_scale, feats);
         });
     }
     c->built = true;
@@ -428,7 +431,8 @@ int read_flags(psb_ctx* c) {
 
 int step_once(psb_ctx* c, bool last) {
     const bool need_prev_p = !c->P.ref && c->P.pci && (c->sc.warm_start != PSB_WARM_ZERO || c->collect_stride > 0);
-    PSB_TRY(build(c, need_prev_p));
+    const bool features = !c->P.ref && c->P.pci && (c->sc.warm_start == PSB_WARM_LEARNED || c->collect_stride > 0);
+    PSB_TRY(build(c, need_prev_p, features));
     cudaStream_t st = c->stream;
     Params P = c->P;
     P.n = c->n;
@@ -456,12 +460,6 @@ int step_once(psb_ctx* c, bool last) {
     } else {
         const int mode = P.ref ? PSB_WARM_ZERO : c->sc.warm_start;
         const bool collect = !P.ref && c->collect_stride > 0;
-        if (mode == PSB_WARM_LEARNED || collect) {
-            timed(c, "features", [&] {
-                psb::launch_features(st, P, c->pos[s], c->vel[s], c->rp[r], c->nbr_count, c->nbr_list, c->p_scale,
-                                     c->feats);
-            });
-        }
         if (mode == PSB_WARM_LEARNED) {
             timed(c, "mlp_infer", [&] { psb::launch_mlp_infer(st, c->n, c->feats, c->mlp_wbf, c->p_scale, c->rp[r]); });
         } else if (mode == PSB_WARM_ZERO && collect) {

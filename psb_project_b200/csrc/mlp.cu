@@ -6,7 +6,8 @@
 // converged pressure. The reference has no counterpart: it starts every
 // step from p = 0 (PciSphSystem_Kernel.cu:131).
 //
-// Inputs, computed at the step's start positions from the neighbour list:
+// Inputs, computed at the step's start positions from the neighbour list
+// (by the density pass at x, k_density_x in sph.cu):
 //   f0 neighbour count / 32
 //   f1 advected density (rho - dt rho div v - rho0)/rho0 * 100
 //   f2 velocity divergence div v * dt * 100, div v = sum (m/rho0)(v_j - v_i).gradW_ij
@@ -43,47 +44,6 @@ __device__ __forceinline__ float silu_grad(float z) {
     return s * (1.f + z * (1.f - s));
 }
 
-// ---- features ---------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_features(Params P, const float4* __restrict__ pos,
-                                                     const float4* __restrict__ vel, const float2* __restrict__ rp,
-                                                     const int* __restrict__ counts, const int* __restrict__ list,
-                                                     float p_scale, float* __restrict__ feats) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= P.n) return;
-    const float4 xi = pos[t], vi = vel[t];
-    const int cnt = min(counts[t], P.cap);
-    float div = 0.f;
-    float3 gr = make_float3(0.f, 0.f, 0.f);
-#pragma unroll 4
-    for (int c = 0; c < cnt; ++c) {
-        const int j = list[(size_t)c * P.n + t];
-        const float4 xj = pos[j];
-        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) continue;
-        const float4 vj = vel[j];
-        const float rinv = rsqrtf(r2);
-        const float om = 1.f - r2 * rinv * P.inv_h;
-        const float s = om * om * rinv;                  // (1-u)^2 / r
-        gr.x += s * dx; gr.y += s * dy; gr.z += s * dz;  // -gradW / (m G)
-        div += s * ((vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz);
-    }
-    // gradW_ij = -G (1-u)^2 x^_ij: div v = -(k_grad/rho0) sum (1-u)^2 (v_j - v_i).x^
-    div *= -P.k_grad / P.rho0;
-    const float rho = rp[t].x;
-    float dwall = P.hf;
-    dwall = fminf(dwall, fminf(xi.x - P.bx0, P.bx1 - xi.x));
-    dwall = fminf(dwall, fminf(xi.y - P.by0, P.by1 - xi.y));
-    dwall = fminf(dwall, fminf(xi.z - P.bz0, P.bz1 - xi.z));
-    float* f = feats + (size_t)t * 8;
-    f[0] = (float)counts[t] * (1.f / 32.f);
-    f[1] = (rho - P.dt * rho * div - P.rho0) / P.rho0 * 100.f;
-    f[2] = div * P.dt * 100.f;
-    f[3] = rp[t].y / p_scale;
-    f[4] = fmaxf(dwall, 0.f) * P.inv_h;
-    f[5] = P.k_grad * sqrtf(gr.x * gr.x + gr.y * gr.y + gr.z * gr.z) * P.hf / P.rho0;
-}
-
 // ---- inference -----------------------------------------------------------------
 // Tensor-core inference: one warp evaluates 16 particles per pass with
 // mma.sync.m16n8k16 (BF16 inputs, FP32 accumulation). Layer 1 is a
@@ -110,7 +70,9 @@ __device__ __forceinline__ void mma_bf16(float* c, uint32_t a0, uint32_t a1, uin
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ float silu_fast(float z) { return z / (1.f + __expf(-z)); }
+// SiLU with the fast exponential and division (a few ulps; the activations
+// are rounded to BF16 right after)
+__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.f + __expf(-z)); }
 
 // y_raw != nullptr: write the raw output y there (host-facing evaluation)
 // instead of the initial pressure max(0, y) p_scale into rp.
@@ -346,10 +308,6 @@ void launch_zero_pressure(cudaStream_t st, int n, float2* rp) {
     if (n > 0) k_zero_pressure<<<grid_of(n), kBlock, 0, st>>>(n, rp);
 }
 
-void launch_features(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float2* rp,
-                     const int* counts, const int* list, float p_scale, float* feats) {
-    if (P.n > 0) k_features<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, rp, counts, list, p_scale, feats);
-}
 
 void launch_mlp_infer(cudaStream_t st, int n, const float* feats, const void* wbf, float p_scale, float2* rp) {
     if (n <= 0) return;

@@ -80,8 +80,9 @@ void launch_build_nbr(cudaStream_t st, const Params& P, const float4* pos, const
                       const uint32_t* cell_start, const uint32_t* cell_end, int* counts, int* list, int* flags);
 
 // ---- launchers (sph.cu) ---------------------------------------------------
-void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const int* counts, const int* list,
-                      float2* rp, float* rho_x, int zero_p);
+void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
+                      const int* list, float2* rp, float* rho_x, int zero_p, float p_scale = 1.f,
+                      float* feats = nullptr);
 void launch_wcsph_force(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float4* vap,
                         const float2* rp, const int* counts, const int* list, float4* pos_out, float4* vel_out,
                         float4* vap_out, float4* fnp);
@@ -125,8 +126,6 @@ void launch_mc_emit(cudaStream_t st, const IsoParams& Q, const double* iso, cons
 
 // ---- learned warm start (mlp.cu) ---------------------------------------------------
 constexpr int kMlpParams = 4673;   // 6x64 + 64 + 64x64 + 64 + 64 + 1
-void launch_features(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float2* rp,
-                     const int* counts, const int* list, float p_scale, float* feats);
 void launch_mlp_infer(cudaStream_t st, int n, const float* feats, const void* wbf, float p_scale, float2* rp);
 void launch_mlp_forward(cudaStream_t st, int n, const float* X, int stride, const void* wbf, float* y);
 void launch_mlp_grad(cudaStream_t st, int batch, const float* X, const float* T, const uint32_t* sel, const void* wbf,

@@ -75,45 +75,37 @@ __device__ __forceinline__ float3 wall_accel(const Params& P, float4 x, float4 v
 // the neighbour list yields all of them. Ghosts carry j's pressure continued
 // hydrostatically across the faces, p_j + rho0 (-g . n) 2 d_j, so a resting
 // column is held by its bottom layer as by any interior layer.
-struct Walls {
-    int n;
-    int a0, a1, a2;           // axis of each near face
-    float p0, p1, p2;         // plane
-    float n0, n1, n2;         // inward normal sign
-};
-
+// The faces near a particle, packed in one word: bits 0-1 hold their count
+// n (at most one face per axis), and face k takes 3 bits at 2 + 3k: its axis
+// (2 bits) and whether it is the lower face (inward normal +1).
 __device__ __forceinline__ float comp(float4 v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
 __device__ __forceinline__ float gcomp(const Params& P, int a) { return a == 0 ? P.gx : (a == 1 ? P.gy : P.gz); }
 
-__device__ __forceinline__ void push_wall(Walls& w, int a, float plane, float nrm) {
-    if (w.n == 0) { w.a0 = a; w.p0 = plane; w.n0 = nrm; }
-    else if (w.n == 1) { w.a1 = a; w.p1 = plane; w.n1 = nrm; }
-    else { w.a2 = a; w.p2 = plane; w.n2 = nrm; }
-    ++w.n;
+__device__ __forceinline__ unsigned near_walls(const Params& P, float4 x) {
+    unsigned w = 0u, n = 0u;
+    auto push = [&](unsigned axis, unsigned lower) { w |= (axis | (lower << 2)) << (2u + 3u * n); ++n; };
+    if (x.x - P.bx0 < P.hf) push(0u, 1u);
+    else if (P.bx1 - x.x < P.hf) push(0u, 0u);
+    if (x.y - P.by0 < P.hf) push(1u, 1u);
+    else if (P.by1 - x.y < P.hf) push(1u, 0u);
+    if (x.z - P.bz0 < P.hf) push(2u, 1u);
+    else if (P.bz1 - x.z < P.hf) push(2u, 0u);
+    return w | n;
 }
 
-__device__ __forceinline__ Walls near_walls(const Params& P, float4 x) {
-    Walls w;
-    w.n = 0;
-    w.a0 = w.a1 = w.a2 = 0;
-    w.p0 = w.p1 = w.p2 = 0.f;
-    w.n0 = w.n1 = w.n2 = 0.f;
-    if (x.x - P.bx0 < P.hf) push_wall(w, 0, P.bx0, 1.f);
-    else if (P.bx1 - x.x < P.hf) push_wall(w, 0, P.bx1, -1.f);
-    if (x.y - P.by0 < P.hf) push_wall(w, 1, P.by0, 1.f);
-    else if (P.by1 - x.y < P.hf) push_wall(w, 1, P.by1, -1.f);
-    if (x.z - P.bz0 < P.hf) push_wall(w, 2, P.bz0, 1.f);
-    else if (P.bz1 - x.z < P.hf) push_wall(w, 2, P.bz1, -1.f);
-    return w;
-}
-
-// Reflects the offset across one face: with d = nrm (x - plane) the
+// Reflects the offset across face k of w: with d = nrm (x - plane) the
 // distances on the box side, component a of r becomes nrm (d_i + d_j), both
 // clamped at 0 so that a particle pushed through the face still sees its
 // ghosts on the wall side (unclamped, its own ghost would push it further
 // out). False if x_j is h or more inside.
-__device__ __forceinline__ bool reflect(const Params& P, int a, float plane, float nrm, float4 xi, float4 xj,
-                                        float3& r, float& dp) {
+__device__ __forceinline__ bool reflect(const Params& P, unsigned w, int k, float4 xi, float4 xj, float3& r,
+                                        float& dp) {
+    const unsigned f = (w >> (2 + 3 * k)) & 7u;
+    const int a = (int)(f & 3u);
+    const bool lower = (f >> 2) != 0u;
+    const float plane = lower ? (a == 0 ? P.bx0 : (a == 1 ? P.by0 : P.bz0))
+                              : (a == 0 ? P.bx1 : (a == 1 ? P.by1 : P.bz1));
+    const float nrm = lower ? 1.f : -1.f;
     const float dj = fmaxf(nrm * (comp(xj, a) - plane), 0.f);
     if (dj >= P.hf) return false;
     const float di = fmaxf(nrm * (comp(xi, a) - plane), 0.f);
@@ -125,57 +117,70 @@ __device__ __forceinline__ bool reflect(const Params& P, int a, float plane, flo
 
 // x_i minus the ghost of x_j across the faces in `mask`; false if a face of
 // the set is h or more from x_j. dp: the ghost's hydrostatic pressure offset.
-__device__ __forceinline__ bool ghost_delta(const Params& P, const Walls& w, int mask, float4 xi, float4 xj, float3& r,
+__device__ __forceinline__ bool ghost_delta(const Params& P, unsigned w, int mask, float4 xi, float4 xj, float3& r,
                                             float& dp) {
     r = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
     dp = 0.f;
-    if ((mask & 1) && !reflect(P, w.a0, w.p0, w.n0, xi, xj, r, dp)) return false;
-    if ((mask & 2) && !reflect(P, w.a1, w.p1, w.n1, xi, xj, r, dp)) return false;
-    if ((mask & 4) && !reflect(P, w.a2, w.p2, w.n2, xi, xj, r, dp)) return false;
+    if ((mask & 1) && !reflect(P, w, 0, xi, xj, r, dp)) return false;
+    if ((mask & 2) && !reflect(P, w, 1, xi, xj, r, dp)) return false;
+    if ((mask & 4) && !reflect(P, w, 2, xi, xj, r, dp)) return false;
     return true;
 }
 
-// Ghost density term (normalised like sum (1-q)^3) of particle t at xi.
-__device__ __forceinline__ void ghost_density(const Params& P, int t, float4 xi, const float4* __restrict__ pos,
-                                              const int* __restrict__ list, int cnt, Kahan& acc) {
-    const Walls w = near_walls(P, xi);
-    if (!w.n) return;
-    for (int mask = 1; mask < (1 << w.n); ++mask)
-    #pragma unroll 4
-    for (int c = 0; c < cnt; ++c) {
-            const float4 xj = pos[list[(size_t)c * P.n + t]];
-            float3 r;
-            float dp;
-            if (!ghost_delta(P, w, mask, xi, xj, r, dp)) continue;
-            const float q = (r.x * r.x + r.y * r.y + r.z * r.z) * P.inv_h2;
-            if (q >= 1.f) continue;
-            const float wq = 1.f - q;
-            acc.add(wq * wq * wq);
-        }
+// The ghosts of neighbour x_j (one per non-empty subset of the near faces).
+// Density: adds (1-q)^3 of each ghost within h.
+__device__ __forceinline__ void ghost_density_pair(const Params& P, unsigned w, float4 xi, float4 xj, Kahan& acc) {
+    const int nm = 1 << (w & 3u);
+    for (int mask = 1; mask < nm; ++mask) {
+        float3 r;
+        float dp;
+        if (!ghost_delta(P, w, mask, xi, xj, r, dp)) continue;
+        const float q = (r.x * r.x + r.y * r.y + r.z * r.z) * P.inv_h2;
+        if (q >= 1.f) continue;
+        const float wq = 1.f - q;
+        acc.add(wq * wq * wq);
+    }
 }
 
-// Ghost pressure term: adds sum (pV_i + pV_ghost) (1-u)^2 x^ to ap.
+// Pressure: adds (pV_i + pV_ghost) (1-u)^2 x^ of each ghost within h, the
+// ghost carrying p_j continued hydrostatically across its faces.
+__device__ __forceinline__ void ghost_pressure_pair(const Params& P, unsigned w, float4 xi, float4 xj, float pVi,
+                                                    float pj, float3& ap) {
+    const float ir0 = 1.f / (P.rho0 * P.rho0);
+    const int nm = 1 << (w & 3u);
+    for (int mask = 1; mask < nm; ++mask) {
+        float3 r;
+        float dp;
+        if (!ghost_delta(P, w, mask, xi, xj, r, dp)) continue;
+        const float r2 = r.x * r.x + r.y * r.y + r.z * r.z;
+        if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) continue;
+        const float rinv = rsqrtf(r2);
+        const float om = 1.f - r2 * rinv * P.inv_h;
+        const float sc = (pVi + (pj + dp) * ir0) * om * om * rinv;
+        ap.x += sc * r.x; ap.y += sc * r.y; ap.z += sc * r.z;
+    }
+}
+
+// Ghost terms of particle t, in a second walk of its list that only
+// particles within h of a face take (the walls are evaluated at xi). Kept
+// out of the main walk: a per-neighbour wall test there slows every
+// particle more than the separate walk costs the few near the faces.
+__device__ __forceinline__ void ghost_density(const Params& P, int t, float4 xi, const float4* __restrict__ pos,
+                                              const int* __restrict__ list, int cnt, Kahan& acc) {
+    const unsigned wall = near_walls(P, xi);
+    if (!(wall & 3u)) return;
+    for (int c = 0; c < cnt; ++c) ghost_density_pair(P, wall, xi, pos[list[(size_t)c * P.n + t]], acc);
+}
+
 __device__ __forceinline__ void ghost_pressure(const Params& P, int t, float4 xi, float pVi,
                                                const float4* __restrict__ pos, const float* __restrict__ pj_of,
                                                int pj_stride, const int* __restrict__ list, int cnt, float3& ap) {
-    const Walls w = near_walls(P, xi);
-    if (!w.n) return;
-    const float ir0 = 1.f / (P.rho0 * P.rho0);
-    for (int mask = 1; mask < (1 << w.n); ++mask)
-    #pragma unroll 4
+    const unsigned wall = near_walls(P, xi);
+    if (!(wall & 3u)) return;
     for (int c = 0; c < cnt; ++c) {
-            const int j = list[(size_t)c * P.n + t];
-            const float4 xj = pos[j];
-            float3 r;
-            float dp;
-            if (!ghost_delta(P, w, mask, xi, xj, r, dp)) continue;
-            const float r2 = r.x * r.x + r.y * r.y + r.z * r.z;
-            if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) continue;
-            const float rinv = rsqrtf(r2);
-            const float om = 1.f - r2 * rinv * P.inv_h;
-            const float s = (pVi + (pj_of[(size_t)j * pj_stride] + dp) * ir0) * om * om * rinv;
-            ap.x += s * r.x; ap.y += s * r.y; ap.z += s * r.z;
-        }
+        const int j = list[(size_t)c * P.n + t];
+        ghost_pressure_pair(P, wall, xi, pos[j], pVi, pj_of[(size_t)j * pj_stride], ap);
+    }
 }
 
 // collisionBox (BoxCollision_Kernel.cu:7-34) with restitution 0: clamp into
@@ -209,23 +214,48 @@ __device__ __forceinline__ void box_project(const Params& P, float3& x, float3& 
 // SphKernel.cu:25; config: Tait, p = k rho0/7 ((rho/rho0)^7 - 1), written as
 // k rho0/7 d (1 + x + ... + x^6) with x = 1 + d to avoid cancellation).
 // PCISPH: keeps the carried pressure (warm start) or zeroes it.
-template <bool REF>
+// FEAT (config PCISPH, learned warm start or data collection): the same
+// neighbour walk also sums the velocity divergence and density gradient and
+// writes the MLP's six inputs (feats, stride 8):
+//   f0 neighbour count / 32
+//   f1 advected density deviation (rho - dt rho div v - rho0)/rho0 * 100
+//   f2 div v * dt * 100, div v = -(k_grad/rho0) sum (1-u)^2 (v_j - v_i).x^
+//   f3 previous-step pressure / p_scale
+//   f4 distance to the nearest box face / h, capped at 1
+//   f5 k_grad |sum (1-u)^2 x^| h / rho0 (density-gradient magnitude)
+template <bool REF, bool FEAT>
 __global__ void __launch_bounds__(kBlock) k_density_x(Params P, const float4* __restrict__ pos,
-                                                      const int* __restrict__ counts, const int* __restrict__ list,
-                                                      float2* __restrict__ rp, float* __restrict__ rho_x, int zero_p) {
+                                                      const float4* __restrict__ vel, const int* __restrict__ counts,
+                                                      const int* __restrict__ list, float2* __restrict__ rp,
+                                                      float* __restrict__ rho_x, int zero_p, float p_scale,
+                                                      float* __restrict__ feats) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= P.n) return;
     const float4 xi = pos[t];
     const int cnt = min(counts[t], P.cap);
     Kahan acc;
+    float div = 0.f;
+    float3 gr = make_float3(0.f, 0.f, 0.f);
+    float4 vi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (FEAT) vi = vel[t];
 #pragma unroll 4
     for (int c = 0; c < cnt; ++c) {
-        const float4 xj = pos[list[(size_t)c * P.n + t]];
+        const int j = list[(size_t)c * P.n + t];
+        const float4 xj = pos[j];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float q = (dx * dx + dy * dy + dz * dz) * P.inv_h2;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float q = r2 * P.inv_h2;
         if (!REF && q >= 1.f) continue;
         const float w = 1.f - q;
         acc.add(w * w * w);
+        if (FEAT && r2 > 0.f) {
+            const float4 vj = vel[j];
+            const float rinv = rsqrtf(r2);
+            const float om = 1.f - r2 * rinv * P.inv_h;
+            const float s = om * om * rinv;                  // (1-u)^2 / r
+            gr.x += s * dx; gr.y += s * dy; gr.z += s * dz;
+            div += s * ((vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz);
+        }
     }
     if (!REF) ghost_density(P, t, xi, pos, list, cnt, acc);
     const float drho = density_deviation(P, acc);
@@ -240,6 +270,20 @@ __global__ void __launch_bounds__(kBlock) k_density_x(Params P, const float4* __
         const float x = 1.f + d;
         const float s = 1.f + x * (1.f + x * (1.f + x * (1.f + x * (1.f + x * (1.f + x)))));
         p = P.eos_k * d * s;
+    }
+    if (FEAT) {
+        div *= -P.k_grad / P.rho0;
+        float dwall = P.hf;
+        dwall = fminf(dwall, fminf(xi.x - P.bx0, P.bx1 - xi.x));
+        dwall = fminf(dwall, fminf(xi.y - P.by0, P.by1 - xi.y));
+        dwall = fminf(dwall, fminf(xi.z - P.bz0, P.bz1 - xi.z));
+        float* f = feats + (size_t)t * 8;
+        f[0] = (float)counts[t] * (1.f / 32.f);
+        f[1] = (rho - P.dt * rho * div - P.rho0) / P.rho0 * 100.f;
+        f[2] = div * P.dt * 100.f;
+        f[3] = rp[t].y / p_scale;          // the carried pressure, before this pass replaces it
+        f[4] = fmaxf(dwall, 0.f) * P.inv_h;
+        f[5] = P.k_grad * sqrtf(gr.x * gr.x + gr.y * gr.y + gr.z * gr.z) * P.hf / P.rho0;
     }
     rp[t] = make_float2(rho, p);
     rho_x[t] = rho;
@@ -527,11 +571,14 @@ inline int grid_of(int n) { return (n + kBlock - 1) / kBlock; }
 
 }  // namespace
 
-void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const int* counts, const int* list,
-                      float2* rp, float* rho_x, int zero_p) {
+void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
+                      const int* list, float2* rp, float* rho_x, int zero_p, float p_scale, float* feats) {
     if (P.n <= 0) return;
-    if (P.ref) k_density_x<true><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, counts, list, rp, rho_x, zero_p);
-    else k_density_x<false><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, counts, list, rp, rho_x, zero_p);
+    const unsigned g = grid_of(P.n);
+    if (P.ref) k_density_x<true, false><<<g, kBlock, 0, st>>>(P, pos, vel, counts, list, rp, rho_x, zero_p, p_scale, feats);
+    else if (feats)
+        k_density_x<false, true><<<g, kBlock, 0, st>>>(P, pos, vel, counts, list, rp, rho_x, zero_p, p_scale, feats);
+    else k_density_x<false, false><<<g, kBlock, 0, st>>>(P, pos, vel, counts, list, rp, rho_x, zero_p, p_scale, feats);
 }
 
 void launch_wcsph_force(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float4* vap,

@@ -16,6 +16,10 @@ Tolerances (written here, applied below):
     kernels, 2.1e-5 config PCISPH against the oracle);
   * positions: within 4 float ulps of the coordinate magnitude plus 1e-5 of
     the step's displacement;
+  * PCISPH velocities of the few particles that one side clamped to a
+    projection bound (box +- r) and the other did not are not compared: the
+    projection is a threshold, a prediction within rounding of the bound
+    falls on either side, and the clamped copy loses its normal velocity;
   * pressure after a multi-iteration config-profile PCISPH step: 1e-4 of its
     max. The pressure accumulates delta (rho* - rho0) over the corrections;
     an FP32 rounding of 3e-8 of a density-level term (kernel constant, wall
@@ -143,11 +147,31 @@ def test_density_at_start_positions(profile):
     sim.close()
 
 
+def on_projection_bound(sc, x):
+    """Per particle and axis: the coordinate sits exactly on a projection
+    bound (box +- particle_radius, as float), where the projection clamps it."""
+    x = np.asarray(x, np.float64)
+    lo = (np.asarray(sc.box_min, np.float32) + np.float32(sc.particle_radius)).astype(np.float64)
+    hi = (np.asarray(sc.box_max, np.float32) - np.float32(sc.particle_radius)).astype(np.float64)
+    return (x == lo) | (x == hi)
+
+
+def projection_disagrees(sc, x_gpu, x_orc):
+    """Particles that one side clamped to a bound and the other did not: the
+    projection is a threshold, and a prediction within rounding of the
+    bound falls on either side of it; the clamped copy also loses its normal
+    velocity. Those particles are compared by position only."""
+    return np.any(on_projection_bound(sc, x_gpu) != on_projection_bound(sc, x_orc), axis=1)
+
+
 def _compare_step(sim, orc, x0, p_tol=TOL, v_tol=TOL_V):
     out = sim.download()
     assert_positions(out["pos"], orc.pos, x0)
-    assert rel_norm(out["vel_half"], orc.vel_half) <= v_tol
-    assert rel_norm(out["vel"], orc.vel) <= v_tol
+    sc = orc.scene
+    keep = ~projection_disagrees(sc, out["pos"], orc.pos) if sc.method == PCISPH else np.ones(len(orc.pos), bool)
+    assert (~keep).sum() <= max(2, 0.002 * len(keep))
+    assert rel_norm(out["vel_half"][keep], orc.vel_half[keep]) <= v_tol
+    assert rel_norm(out["vel"][keep], orc.vel[keep]) <= v_tol
     assert np.max(np.abs(out["density"] - orc.rho) / np.abs(orc.rho)) <= TOL
     assert rel_norm(out["pressure"], orc.p) <= p_tol
     assert rel_norm(sim.read_field(R.FIELD_FORCE_NP), orc.f_np) <= TOL
