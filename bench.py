@@ -79,9 +79,11 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
     ap.add_argument("--presolve", type=int, default=256, help="initial-pressure corrector passes before the warm-up")
     ap.add_argument("--train-steps", type=int, default=400, help="plain-PCISPH steps recorded for training (learned)")
-    ap.add_argument("--train-iters", type=int, default=3000, help="Adam steps (learned)")
-    ap.add_argument("--train-batch", type=int, default=16384)
+    ap.add_argument("--train-iters", type=int, default=10000, help="Adam steps (learned)")
+    ap.add_argument("--train-batch", type=int, default=65536)
+    ap.add_argument("--train-lr", type=float, default=3e-3, help="peak learning rate of the cosine schedule")
     ap.add_argument("--xsph", type=float, default=None, help="override the scene's XSPH velocity smoothing factor")
+    ap.add_argument("--no-graph", action="store_true", help="C3: launch kernel by kernel instead of CUDA graphs")
     ap.add_argument("--eval-steps", type=int, default=1000,
                     help="steps after the recorded ones over which the warm starts are compared (0: skip)")
     return ap.parse_args()
@@ -280,11 +282,11 @@ def run_ours(args):
         t1 = time.perf_counter()
         gen.mlp_set_weights(P.mlp_init_weights(rank))
         loss0 = gen.mlp_train(1, args.train_batch, 1e-3, seed=11)
-        loss = gen.mlp_train(args.train_iters, args.train_batch, 2e-3, seed=12)
-        loss = gen.mlp_train(args.train_iters // 2, args.train_batch, 5e-4, seed=13)
+        loss = gen.mlp_fit(args.train_iters, args.train_batch, args.train_lr, chunks=10, seed=12)
         weights = gen.mlp_get_weights()
-        train_info = {"recorded_steps": args.train_steps, "rows": int(rows), "adam_steps": args.train_iters * 3 // 2 + 1,
-                      "batch": args.train_batch, "loss_first": loss0, "loss_last": loss,
+        train_info = {"recorded_steps": args.train_steps, "rows": int(rows), "adam_steps": args.train_iters // 10 * 10 + 1,
+                      "batch": args.train_batch, "lr": args.train_lr, "schedule": "cosine, 10 chunks",
+                      "loss_first": loss0, "loss_last": loss,
                       "record_s": round(t1 - t0, 2), "train_s": round(time.perf_counter() - t1, 2)}
     gen.step(args.warmup)
     snap = gen.download()
@@ -447,10 +449,183 @@ def run_ours(args):
     rep_.close()
 
 
+def run_batch(args):
+    """Config C3: 64 independent PCISPH dam breaks stepped as one batch
+    (psb_create_batch), each step one CUDA-graph launch with the corrector a
+    device-side while loop, the learned warm start on. Over N GPUs the scenes
+    are split by size (replicas.assign_scenes) with no collective on the step
+    path; the total work is fixed, so the scaling is strong."""
+    import torch
+    import psb_project_b200 as P
+    from psb_project_b200 import replicas
+
+    rep_ = replicas.init("nccl")
+    rank, world, local = rep_.rank, rep_.world, rep_.local
+    torch.cuda.set_device(local)
+    modes = {"zero": P.WARM_ZERO, "previous": P.WARM_PREVIOUS, "learned": P.WARM_LEARNED}
+    all_scenes = P.batch_scenes()
+    mine = replicas.assign_scenes([s.n for s in all_scenes], world)[rank]
+    scenes = [all_scenes[i].replace(warm_start=modes[args.warm_start]) for i in mine]
+    n = sum(s.n for s in scenes)
+    n_all = sum(s.n for s in all_scenes)
+    stream = torch.cuda.current_stream()
+    max_over_ranks = rep_.max_over_ranks
+
+    def barrier():
+        rep_.barrier()
+        torch.cuda.synchronize()
+
+    def make(mode, graph=True):
+        b = P.BatchSimulation([s.replace(warm_start=mode) for s in scenes])
+        b.set_stream(stream.cuda_stream)
+        b.set_graph(graph and not args.no_graph)
+        return b
+
+    # set-up (untimed): initial pressure, plain steps recorded for training, warm-up
+    gen = make(P.WARM_ZERO, graph=False)
+    gen.upload(P.batch_positions(scenes))
+    gen.presolve(args.presolve)
+    train_info, weights = None, None
+    if args.warm_start == "learned":
+        t0 = time.perf_counter()
+        gen.mlp_collect(stride=64, capacity=(args.train_steps + 1) * ((n + 63) // 64))
+        gen.step(args.train_steps)
+        gen.mlp_collect(0)
+        rows, _, _ = gen.mlp_dataset(fetch=False)
+        t1 = time.perf_counter()
+        gen.mlp_set_weights(P.mlp_init_weights(rank))
+        loss0 = gen.mlp_train(1, args.train_batch, 1e-3, seed=11)
+        loss = gen.mlp_fit(args.train_iters, args.train_batch, args.train_lr, chunks=10, seed=12)
+        weights = gen.mlp_get_weights()
+        train_info = {"recorded_steps": args.train_steps, "rows": int(rows), "adam_steps": args.train_iters // 10 * 10 + 1,
+                      "batch": args.train_batch, "lr": args.train_lr, "schedule": "cosine, 10 chunks",
+                      "loss_first": loss0, "loss_last": loss, "record_s": round(t1 - t0, 2),
+                      "train_s": round(time.perf_counter() - t1, 2)}
+    gen.step(args.warmup)
+    snap = gen.download()
+    gen.close()
+    start = (args.train_steps if train_info else 0) + args.warmup + 1
+
+    def restore(b):
+        b.upload(snap["pos"], snap["vel"], snap["vel_half"], snap["pressure"])
+
+    def timed_pass(b, steps, profile=False):
+        restore(b)
+        b.step(2)                 # untimed: captures the graphs of both state parities on first use
+        if profile:
+            b.profile(True)
+            b.profile_reset()
+        before = b.batch_stats()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.step(steps)
+        e1.record(stream)
+        barrier()
+        after = b.batch_stats()
+        prof = None
+        if profile:
+            prof = b.profile_read()
+            b.profile(False)
+        per_scene = (after["iters_total"] - before["iters_total"]) / steps
+        unconv = after["unconverged_steps"] - before["unconverged_steps"]
+        return max_over_ranks(e0.elapsed_time(e1)), per_scene, unconv, prof
+
+    sim = make(modes[args.warm_start])
+    if weights is not None:
+        sim.mlp_set_weights(weights)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ms_max, per_scene, unconv, _ = timed_pass(sim, args.steps)
+    value = n_all * args.steps / (ms_max / 1e3)
+    _, _, _, prof = timed_pass(sim, min(args.steps, 20), profile=True)
+    # end to end: host buffers in and out every step
+    pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+    h = {"pos": pin((n, 3)), "vel": pin((n, 3)), "vel_half": pin((n, 3)), "density": pin((n,)), "pressure": pin((n,))}
+    for k in ("pos", "vel", "vel_half", "pressure"):
+        h[k][:] = snap[k]
+    barrier()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        sim.upload(h["pos"], h["vel"], h["vel_half"], h["pressure"])
+        sim.step(1)
+        sim.download(h)
+    e3.record(stream)
+    barrier()
+    e2e_value = n_all * args.steps / (max_over_ranks(e2.elapsed_time(e3)) / 1e3)
+    clk = clocks.stop()
+    # learned vs plain over the evaluation window, from the same snapshot
+    comparison = {}
+    if args.eval_steps > 0:
+        comparison["steps"] = "%d..%d of every scene" % (start + 2, start + 1 + args.eval_steps)
+        for name, mode in (("learned", P.WARM_LEARNED), ("zero", P.WARM_ZERO)):
+            if name == "learned" and weights is None:
+                continue
+            b = sim if mode == modes[args.warm_start] else make(mode)
+            if weights is not None:
+                b.mlp_set_weights(weights)
+            ms, ps, unc, _ = timed_pass(b, args.eval_steps)
+            comparison[name] = {"iters_mean": float(np.mean(ps)), "iters_mean_weighted": float(np.average(ps, weights=[s.n for s in scenes])),
+                                "unconverged_steps": int(np.sum(unc)), "ms_per_step": ms / args.eval_steps,
+                                "value": n_all * args.eval_steps / (ms / 1e3)}
+            if b is not sim:
+                b.close()
+        if "learned" in comparison:
+            z, l_ = comparison["zero"], comparison["learned"]
+            z["iters_ratio_over_learned"] = z["iters_mean"] / max(l_["iters_mean"], 1e-9)
+            z["time_ratio_over_learned"] = z["ms_per_step"] / l_["ms_per_step"]
+    sim.close()
+
+    passes = (max(1, int(np.ceil(np.log2(sum(int(np.prod(s.dims)) for s in scenes))))) + 7) // 8
+    launches = int(sum(l * _kernels_per_group(k, passes) for k, (l, _) in prof.items()))
+    tot_ms = sum(v[1] for v in prof.values())
+    dom = max((k for k in prof if k in ALG_BYTES), key=lambda k: prof[k][1])
+    l_dom, ms_dom = prof[dom]
+    per_launch_s = ms_dom / l_dom / 1e3
+    achieved = ALG_BYTES[dom] * n / per_launch_s / 1e9
+    peak, peak_kind = peaks()
+    kernels = {k: {"launches": l, "ms": round(v, 3), "share": round(v / tot_ms, 4)} for k, (l, v) in prof.items()}
+    prof_steps = min(args.steps, 20)
+    if rank == 0:
+        out = {
+            "metric": "particle-steps/s, 64 batched PCISPH dam breaks at eta=1% (C3)", "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "C3: 64 PCISPH dam breaks, N log-uniform in [4096, 131072], seed 3",
+                       "particles": n_all, "scenes": len(all_scenes), "scenes_on_rank0": len(scenes),
+                       "eta": scenes[0].eta, "warm_start": args.warm_start, "dt": scenes[0].dt, "h": scenes[0].h,
+                       "graph": not args.no_graph,
+                       "parallelism": f"scenes split over {world} GPUs by size" if world > 1 else "single GPU",
+                       "l2": "working set > L2 (~%d MB)" % int(n * (3 * 16 * 2 + 8 * 2 + 4 * 2 + 16 * 4 + 8 + 4 + 4 * scenes[0].nbr_cap + 4) / 1e6),
+                       "timed_steps": "steps %d..%d of every scene" % (start + 2, start + 1 + args.steps)},
+            "iters_per_step": {"mean_over_scenes": float(np.mean(per_scene)), "max_scene": float(np.max(per_scene)),
+                               "min_scene": float(np.min(per_scene)), "unconverged_steps": int(np.sum(unconv))},
+            "comparison": comparison,
+            "learned_training": train_info,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "alg_bytes_per_particle": ALG_BYTES[dom], "mean_launch_us": per_launch_s * 1e6},
+            "kernels": kernels, "kernels_steps": prof_steps,
+            "gpu_launches": int(launches * args.steps / prof_steps),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n_all * 40, "d2h_bytes_per_step": n_all * 44},
+            "clocks": clk,
+            "cpu_baseline": None,
+        }
+        print(json.dumps(out))
+    rep_.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.scene == "C3":
+        run_batch(args)
     else:
         run_ours(args)
 

@@ -269,6 +269,43 @@ int psb_mlp_train(psb_ctx* ctx, int32_t iters, int32_t batch, float lr, uint64_t
 int psb_mlp_forward(psb_ctx* ctx, const float* X, int32_t n, float* y);
 int psb_mlp_loss_grad(psb_ctx* ctx, const float* X, const float* T, int32_t n, float* loss, float* grad);
 
+/* Batched scenes: n_scenes independent scenes stepped together in one
+ * context, each sweep one kernel launch over every scene's particles. No
+ * counterpart in the reference, which steps one system per update
+ * (PciSphSystem.cpp:163-204).
+ * Every scene is CONFIG-profile PCISPH, and all share h, mass, rho0, dt, mu,
+ * k, gravity, spacing, skin, xsph, cell, wall_k, wall_c, particle_radius,
+ * eta, min_iters, max_iters, nbr_cap and warm_start; their boxes, grids
+ * (grid_min, dims) and particle counts (n_max) differ. The particles are
+ * concatenated in scene order: ids [0, n_max of scene 0) are scene 0, the
+ * next n_max of scene 1 are scene 1, and so on; psb_upload takes exactly the
+ * total and psb_download returns it in the same order.
+ * Each scene gets its own grid and key range, its own convergence test and
+ * corrector iteration count, and its own walls: its results are those it has
+ * when stepped alone, bit for bit. The corrector loop runs on the device (a
+ * one-block kernel tests each scene after every density pass and retires
+ * the converged ones), so a step never waits on the host.
+ * psb_step_stats of a batch: iters = the most corrections any scene took,
+ * converged = all scenes converged, err = the max over scenes per pass. */
+int psb_create_batch(const psb_scene* scenes, int32_t n_scenes, psb_ctx** out);
+/* Scenes in the context (1 for psb_create) and the first particle id of each
+ * (first: n_scenes + 1 entries, the last one the total; may be NULL). */
+int psb_batch_layout(const psb_ctx* ctx, int32_t* n_scenes, int64_t* first);
+/* Per-scene results (arrays of n_scenes, any may be NULL): the last step's
+ * corrections, converged flag and final density-pass max error; and, since
+ * the last upload, corrections summed over steps and the count of steps
+ * that ended at max_iters unconverged (-1 for a single-scene context). */
+int psb_batch_stats(psb_ctx* ctx, int32_t* iters, int32_t* converged, double* err_final, int64_t* iters_total,
+                    int64_t* unconverged_steps);
+/* CUDA-graph stepping (batches only): on, each step after the first since an
+ * upload is one cudaGraphLaunch of the whole step, grid rebuild, warm start,
+ * the corrector as a conditional while node (cudaGraphCondTypeWhile) and the
+ * commit. Graphs are captured on first use, one per state buffer parity,
+ * and released by psb_set_graph(ctx, 0) and psb_destroy. Steps that record
+ * training data or run with profiling on are launched kernel by kernel;
+ * both ways launch the same kernels in the same order. */
+int psb_set_graph(psb_ctx* ctx, int32_t on);
+
 const char* psb_status_string(int32_t status);
 const char* psb_last_error(const psb_ctx* ctx);
 int32_t psb_abi_version(void);

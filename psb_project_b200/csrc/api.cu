@@ -91,6 +91,8 @@ struct psb_ctx {
     int hist_blocks = 0, key_bits = 0;
     int sorted = -1;          // buffer holding the last sorted keys, -1: none
     int sorted_n = 0;
+    int stale = -1;           // after an upload: the previous particle set's sorted keys, whose cells
+    int stale_n = 0;          // the next build clears (-1: none)
     uint32_t* cell_start = nullptr;
     uint32_t* cell_end = nullptr;
     size_t ncells = 0;
@@ -132,6 +134,25 @@ struct psb_ctx {
     int32_t* mc_tri = nullptr;
     long long iso_cap = 0, mc_cube_cap = 0, mc_edge_cap = 0, mc_scratch_cap = 0, mc_vert_cap = 0, mc_tri_cap = 0;
     bool mc_table = false;
+    // batched scenes (psb_create_batch); a single scene has nscenes == 1 and batch == false
+    bool batch = false;
+    int nscenes = 1;
+    std::vector<int64_t> first{0, 0};        // first particle id of each scene, then the total
+    std::vector<psb::SceneGeom> geom;
+    psb::SceneGeom* d_scenes = nullptr;
+    uint16_t* d_slot_scene = nullptr;
+    uint8_t* d_active = nullptr;
+    unsigned long long* d_err_scene = nullptr;    // the current density pass, per scene
+    unsigned long long* d_err_sh = nullptr;       // (PSB_MAX_ITERS + 1) x nscenes, per pass and scene
+    int* d_loop = nullptr;                        // device loop words (batch.cu)
+    int* h_loop = nullptr;                        // pinned mirrors
+    unsigned long long* h_err_sh = nullptr;
+    // CUDA-graph stepping (batches)
+    bool graph_on = false;
+    cudaGraphExec_t gexec[2] = {};                // one per state buffer parity (cs)
+    int graph_sorted = -1;                        // the sort's result buffer, fixed by the key width
+    cudaStream_t cap_main = nullptr;              // captures the step (the legacy stream cannot be captured)
+    cudaStream_t cap_stream = nullptr;            // captures the while node's body
     // host mirrors
     unsigned long long* h_err = nullptr;
     int* h_flags = nullptr;
@@ -198,6 +219,12 @@ void free_all(psb_ctx* c) {
     cudaFree(c->iso); cudaFree(c->mc_cube); cudaFree(c->mc_edge); cudaFree(c->mc_scratch); cudaFree(c->mc_vert);
     cudaFree(c->mc_tri);
     cudaFreeHost(c->h_err); cudaFreeHost(c->h_flags);
+    cudaFree(c->d_scenes); cudaFree(c->d_slot_scene); cudaFree(c->d_active); cudaFree(c->d_err_scene);
+    cudaFree(c->d_err_sh); cudaFree(c->d_loop);
+    cudaFreeHost(c->h_loop); cudaFreeHost(c->h_err_sh);
+    for (auto& g : c->gexec) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+    if (c->cap_main) cudaStreamDestroy(c->cap_main);
 }
 
 int validate(const psb_scene* s, std::string& why) {
@@ -381,8 +408,10 @@ int build(psb_ctx* c, bool keep_p = false, bool features = false) {
     Params P = c->P;
     P.n = c->n;
     const int n = c->n;
-    if (c->sorted >= 0)
-        timed(c, "reset_cells", [&] { psb::launch_reset_cells(st, c->sorted_n, c->keys[c->sorted], c->cell_start); });
+    const int rs = c->sorted >= 0 ? c->sorted : c->stale;       // cells occupied by the previous sort
+    const int rn = c->sorted >= 0 ? c->sorted_n : c->stale_n;
+    if (rs >= 0) timed(c, "reset_cells", [&] { psb::launch_reset_cells(st, rn, c->keys[rs], c->cell_start); });
+    c->stale = -1;
     cudaMemsetAsync(c->flags, 0, 8 * sizeof(int), st);
     timed(c, "cell_keys", [&] {
         psb::launch_cell_keys(st, P, c->pos[c->cs], c->ids[c->cr], c->keys[0], c->vals[0], &c->flags[4]);
@@ -429,7 +458,188 @@ int read_flags(psb_ctx* c) {
     return PSB_OK;
 }
 
+// ---- batched scenes -------------------------------------------------------
+
+// The corrector of a batch: k_batch_begin, then {density pass, decision,
+// pressure-force pass} until every scene has converged or max_iters passes
+// have run. The predictions stay in xs[0]: the config profile's pressure-
+// force pass reads the start positions, never x*, so it updates x* in place.
+// capture: enqueue the loop as a while node of the graph being captured on
+// the context's stream; else drive it from the host, one 4-byte read per pass.
+int batch_corrector(psb_ctx* c, const Params& P, int s, int r, bool capture) {
+    cudaStream_t st = c->stream;
+    const int S = c->nscenes;
+    const int max_it = c->sc.max_iters;
+    psb::launch_batch_begin(st, S, max_it, c->d_active, c->d_err_scene, c->d_err_sh, (PSB_MAX_ITERS + 1) * S,
+                            c->d_loop);
+    if (max_it == 0) return PSB_OK;
+    auto body = [&](cudaStream_t bs, cudaGraphConditionalHandle h, int set_handle) {
+        timed(c, "pci_density", [&] {
+            psb::launch_pci_density(bs, P, c->xs[0], c->rp[r], c->nbr_count, c->nbr_list, c->rpc, nullptr);
+        });
+        timed(c, "batch_decide", [&] {
+            psb::launch_batch_decide(bs, S, c->sc.min_iters, max_it, c->sc.eta, c->d_active, c->d_err_scene,
+                                     c->d_err_sh, c->d_loop, h, set_handle);
+        });
+        timed(c, "pci_force_predict", [&] {
+            psb::launch_pci_force_predict(bs, P, c->pos[s], c->vap[s], c->fnp, c->xs[1], c->rpc, c->nbr_count,
+                                          c->nbr_list, c->xs[0], c->vs, c->rp[r]);
+        });
+    };
+    if (!capture) {
+        for (int k = 0; k < max_it; ++k) {
+            body(st, 0, 0);
+            PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->h_loop + 1, c->d_loop + 1, sizeof(int), cudaMemcpyDeviceToHost, st),
+                               "loop"));
+            PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "sync"));
+            if (!c->h_loop[1]) break;
+        }
+        return PSB_OK;
+    }
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    PSB_TRY(cuda_check(c, cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd), "capture info"));
+    cudaGraphConditionalHandle h;
+    PSB_TRY(cuda_check(c, cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault), "conditional handle"));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    PSB_TRY(cuda_check(c, cudaGraphAddNode(&node, g, deps, nd, &np), "while node"));
+    cudaGraph_t body_graph = np.conditional.phGraph_out[0];
+    PSB_TRY(cuda_check(c, cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
+                       "capture dependencies"));
+    PSB_TRY(cuda_check(c, cudaStreamBeginCaptureToGraph(c->cap_stream, body_graph, nullptr, nullptr, 0,
+                                                        cudaStreamCaptureModeThreadLocal), "body capture"));
+    body(c->cap_stream, h, 1);
+    cudaGraph_t ended = nullptr;
+    return cuda_check(c, cudaStreamEndCapture(c->cap_stream, &ended), "body capture");
+}
+
+// One batch step, enqueued on the context's stream (or captured from it).
+int enqueue_batch_step(psb_ctx* c, bool capture) {
+    const bool collect = c->collect_stride > 0;
+    const int mode = c->sc.warm_start;
+    PSB_TRY(build(c, mode != PSB_WARM_ZERO || collect, mode == PSB_WARM_LEARNED || collect));
+    cudaStream_t st = c->stream;
+    Params P = c->P;
+    P.n = c->n;
+    const int s = c->cs, r = c->cr;
+    if (mode == PSB_WARM_LEARNED) {
+        timed(c, "mlp_infer", [&] { psb::launch_mlp_infer(st, c->n, c->feats, c->mlp_wbf, c->p_scale, c->rp[r]); });
+    } else if (mode == PSB_WARM_ZERO && collect) {
+        psb::launch_zero_pressure(st, c->n, c->rp[r]);
+    }
+    timed(c, "pci_init", [&] {
+        psb::launch_pci_init(st, P, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list,
+                             mode == PSB_WARM_ZERO ? 0 : 1, c->fnp, c->xs[0], c->vs);
+    });
+    PSB_TRY(batch_corrector(c, P, s, r, capture));
+    const float4* v_commit = c->vs;
+    if (P.xsph_k != 0.f) {
+        timed(c, "xsph", [&] { psb::launch_xsph(st, P, c->xs[0], c->vs, c->nbr_count, c->nbr_list, c->xs[1]); });
+        v_commit = c->xs[1];
+    }
+    timed(c, "pci_commit", [&] {
+        psb::launch_pci_commit(st, P, c->xs[0], v_commit, c->rpc, c->sc.max_iters > 0, c->pos[s], c->vel[s], c->vap[s],
+                               c->rp[r]);
+    });
+    return cuda_check(c, cudaGetLastError(), "launch");
+}
+
+// Captures the step from the current state parity into c->gexec[c->cs], on
+// the context's own capture stream (nothing runs; the graph is launched on
+// the caller's stream, which may be the legacy one).
+int capture_batch_step(psb_ctx* c) {
+    const int p = c->cs;
+    cudaStream_t user = c->stream;
+    cudaStream_t st = c->cap_main;
+    PSB_TRY(cuda_check(c, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture"));
+    const int saved_cs = c->cs, saved_cr = c->cr, saved_sorted = c->sorted, saved_stale = c->stale;
+    c->stream = st;
+    const int rc = enqueue_batch_step(c, true);
+    c->stream = user;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    // capturing ran none of it: the host state is the one before the step
+    c->graph_sorted = c->sorted;
+    c->cs = saved_cs; c->cr = saved_cr; c->sorted = saved_sorted; c->stale = saved_stale;
+    if (rc != PSB_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rc != PSB_OK ? rc : cuda_check(c, e, "capture");
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&c->gexec[p], g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) { c->gexec[p] = nullptr; return cuda_check(c, ei, "graph instantiate"); }
+    return PSB_OK;
+}
+
+int step_batch(psb_ctx* c, bool last) {
+    cudaStream_t st = c->stream;
+    const int S = c->nscenes;
+    const bool collect = c->collect_stride > 0;
+    // a graph holds the reset of the previous sort's cells: there must be one
+    // (after an upload, the set before it), of the same size
+    const int prev_n = c->sorted >= 0 ? c->sorted_n : (c->stale >= 0 ? c->stale_n : -1);
+    const bool graph = c->graph_on && !collect && !c->prof.on && prev_n == c->n;
+    if (graph) {
+        if (!c->gexec[c->cs]) PSB_TRY(capture_batch_step(c));
+        PSB_TRY(cuda_check(c, cudaGraphLaunch(c->gexec[c->cs], st), "graph launch"));
+        // what build() records of the step it enqueues
+        c->sorted = c->graph_sorted;
+        c->sorted_n = c->n;
+        c->stale = -1;
+        c->cs ^= 1;
+        c->cr ^= 1;
+        c->built = true;
+    } else {
+        PSB_TRY(enqueue_batch_step(c, false));
+    }
+    c->stats.steps += 1;
+    if (!last && !collect) return PSB_OK;
+    // per-scene results of this step
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->h_loop, c->d_loop, sizeof(int) * (2 + 4 * (size_t)S), cudaMemcpyDeviceToHost,
+                                          st), "loop"));
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->h_err_sh, c->d_err_sh, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S,
+                                          cudaMemcpyDeviceToHost, st), "err"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "sync"));
+    int iters = 0, all_conv = 1;
+    for (int k = 0; k < S; ++k) {
+        iters = std::max(iters, c->h_loop[2 + k]);
+        all_conv &= c->h_loop[2 + S + k];
+    }
+    c->stats.iters = iters;
+    c->stats.converged = all_conv;
+    if (collect && all_conv) {
+        const int stride = c->collect_stride;
+        const int offset = (int)(c->collect_steps % stride);
+        const int rows = offset < c->n ? (c->n - offset + stride - 1) / stride : 0;
+        psb::launch_collect(st, c->n, stride, offset, c->ds_rows, c->ds_cap, c->feats, c->rp[c->cr], c->p_scale, c->ds_X,
+                            c->ds_T);
+        c->ds_rows += (uint64_t)rows;
+        c->collect_steps += 1;
+    }
+    if (!last) return PSB_OK;
+    PSB_TRY(read_flags(c));
+    for (int i = 0; i <= PSB_MAX_ITERS; ++i) {
+        double m = 0.0;
+        for (int k = 0; k < S; ++k) {
+            const unsigned long long e = c->h_err_sh[(size_t)i * S + k];
+            if (e) m = std::max(m, psb::unorder_double(e));
+        }
+        c->stats.err[i] = m;
+    }
+    if (!all_conv) return fail(c, PSB_ENOCONV, "corrector loop reached max_iters above eta in a scene of the batch");
+    return PSB_OK;
+}
+
 int step_once(psb_ctx* c, bool last) {
+    if (c->batch) return step_batch(c, last);
     const bool need_prev_p = !c->P.ref && c->P.pci && (c->sc.warm_start != PSB_WARM_ZERO || c->collect_stride > 0);
     const bool features = !c->P.ref && c->P.pci && (c->sc.warm_start == PSB_WARM_LEARNED || c->collect_stride > 0);
     PSB_TRY(build(c, need_prev_p, features));
@@ -547,14 +757,12 @@ const char* psb_status_string(int32_t status) {
 
 const char* psb_last_error(const psb_ctx* c) { return c ? c->err.c_str() : ""; }
 
-int psb_create(const psb_scene* scene, psb_ctx** out) {
-    if (!out) return PSB_EINVAL;
-    *out = nullptr;
-    std::string why;
-    if (validate(scene, why) != PSB_OK) {
-        std::fprintf(stderr, "psb_create: %s\n", why.c_str());
-        return PSB_EINVAL;
-    }
+}  // extern "C"
+
+namespace {
+
+// Context and device buffers for `scene` (validated) over `ncells` grid cells.
+int create_impl(const psb_scene* scene, size_t ncells, psb_ctx** out) {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -567,7 +775,7 @@ int psb_create(const psb_scene* scene, psb_ctx** out) {
     c->P = derive(c->sc);
     c->n_max = scene->n_max;
     c->cap = c->P.cap;
-    c->ncells = (size_t)scene->dims[0] * scene->dims[1] * scene->dims[2];
+    c->ncells = ncells;
     c->key_bits = bits_for(c->ncells);
     c->hist_blocks = psb::radix_blocks(c->n_max);
     cudaGetDevice(&c->device);
@@ -623,6 +831,133 @@ int psb_create(const psb_scene* scene, psb_ctx** out) {
                                    (double)scene->gravity[2] * scene->gravity[2]);
         c->p_scale = (float)(scene->rho0 * (g > 0 ? g : 9.81) * 0.1);
     }
+    c->first = {0, (int64_t)scene->n_max};
+    *out = c;
+    return PSB_OK;
+}
+
+// The parameters every scene of a batch must share; returns the first that
+// differs from scene 0, or nullptr.
+const char* batch_mismatch(const psb_scene& a, const psb_scene& b) {
+    if (a.h != b.h) return "h";
+    if (a.mass != b.mass) return "mass";
+    if (a.rho0 != b.rho0) return "rho0";
+    if (a.k != b.k) return "k";
+    if (a.mu != b.mu) return "mu";
+    if (a.sigma != b.sigma || a.l != b.l) return "sigma/l";
+    if (a.dt != b.dt) return "dt";
+    for (int i = 0; i < 3; ++i)
+        if (a.gravity[i] != b.gravity[i]) return "gravity";
+    if (a.particle_radius != b.particle_radius) return "particle_radius";
+    if (a.cell != b.cell) return "cell";
+    if (a.profile != b.profile || a.method != b.method) return "profile/method";
+    if (a.min_iters != b.min_iters || a.max_iters != b.max_iters || a.eta != b.eta) return "min_iters/max_iters/eta";
+    if (a.wall_k != b.wall_k || a.wall_c != b.wall_c) return "wall_k/wall_c";
+    if (a.nbr_cap != b.nbr_cap) return "nbr_cap";
+    if (a.warm_start != b.warm_start) return "warm_start";
+    if (a.spacing != b.spacing || a.skin != b.skin || a.xsph != b.xsph) return "spacing/skin/xsph";
+    return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int psb_create(const psb_scene* scene, psb_ctx** out) {
+    if (!out) return PSB_EINVAL;
+    *out = nullptr;
+    std::string why;
+    if (validate(scene, why) != PSB_OK) {
+        std::fprintf(stderr, "psb_create: %s\n", why.c_str());
+        return PSB_EINVAL;
+    }
+    return create_impl(scene, (size_t)scene->dims[0] * scene->dims[1] * scene->dims[2], out);
+}
+
+int psb_create_batch(const psb_scene* scenes, int32_t n_scenes, psb_ctx** out) {
+    if (!out) return PSB_EINVAL;
+    *out = nullptr;
+    auto bad = [](const std::string& msg) {
+        std::fprintf(stderr, "psb_create_batch: %s\n", msg.c_str());
+        return PSB_EINVAL;
+    };
+    if (!scenes || n_scenes < 1 || n_scenes > 65535) return bad("need 1 <= n_scenes <= 65535 scenes");
+    std::string why;
+    int64_t total = 0;
+    size_t cells = 0;
+    for (int s = 0; s < n_scenes; ++s) {
+        if (validate(&scenes[s], why) != PSB_OK) return bad("scene " + std::to_string(s) + ": " + why);
+        if (const char* f = batch_mismatch(scenes[0], scenes[s]))
+            return bad("scene " + std::to_string(s) + " differs from scene 0 in " + f);
+        total += scenes[s].n_max;
+        cells += (size_t)scenes[s].dims[0] * scenes[s].dims[1] * scenes[s].dims[2];
+    }
+    if (scenes[0].profile != PSB_PROFILE_CONFIG || scenes[0].method != PSB_PCISPH)
+        return bad("batches are config-profile PCISPH scenes");
+    if (total > 0x7fffffff) return bad("more than 2^31 - 1 particles in all");
+    if ((double)cells >= 4294967295.0) return bad("too many grid cells in all (>= 2^32 - 1)");
+    psb_scene u = scenes[0];
+    u.n_max = (int32_t)total;
+    psb_ctx* c = nullptr;
+    PSB_TRY(create_impl(&u, cells, &c));
+    const int S = n_scenes;
+    c->batch = true;
+    c->nscenes = S;
+    c->first.assign(S + 1, 0);
+    c->geom.resize(S);
+    std::vector<uint16_t> slot_scene((size_t)total);
+    uint32_t base = 0;
+    for (int s = 0; s < S; ++s) {
+        const psb_scene& sc = scenes[s];
+        psb::SceneGeom& G = c->geom[s];
+        G.bx0 = sc.box_min[0]; G.by0 = sc.box_min[1]; G.bz0 = sc.box_min[2];
+        G.bx1 = sc.box_max[0]; G.by1 = sc.box_max[1]; G.bz1 = sc.box_max[2];
+        // as derive() forms the single scene's bounds
+        G.wlo_x = sc.box_min[0] + sc.particle_radius; G.wlo_y = sc.box_min[1] + sc.particle_radius;
+        G.wlo_z = sc.box_min[2] + sc.particle_radius;
+        G.whi_x = sc.box_max[0] - sc.particle_radius; G.whi_y = sc.box_max[1] - sc.particle_radius;
+        G.whi_z = sc.box_max[2] - sc.particle_radius;
+        G.g.gx = sc.grid_min[0]; G.g.gy = sc.grid_min[1]; G.g.gz = sc.grid_min[2];
+        G.g.cell = sc.cell;
+        G.g.nx = sc.dims[0]; G.g.ny = sc.dims[1]; G.g.nz = sc.dims[2];
+        G.cell_base = base;
+        base += (uint32_t)((size_t)sc.dims[0] * sc.dims[1] * sc.dims[2]);
+        G.first = (int)c->first[s];
+        G.count = sc.n_max;
+        c->first[s + 1] = c->first[s] + sc.n_max;
+        std::fill(slot_scene.begin() + c->first[s], slot_scene.begin() + c->first[s + 1], (uint16_t)s);
+    }
+    int rc = PSB_OK;
+    if (!rc) rc = dalloc(c, &c->d_scenes, S);
+    if (!rc) rc = dalloc(c, &c->d_slot_scene, (size_t)total);
+    if (!rc) rc = dalloc(c, &c->d_active, S);
+    if (!rc) rc = dalloc(c, &c->d_err_scene, S);
+    if (!rc) rc = dalloc(c, &c->d_err_sh, (size_t)(PSB_MAX_ITERS + 1) * S);
+    if (!rc) rc = dalloc(c, &c->d_loop, 2 + 4 * (size_t)S);
+    if (!rc && cudaMallocHost((void**)&c->h_loop, sizeof(int) * (2 + 4 * (size_t)S)) != cudaSuccess) rc = PSB_ENOMEM;
+    if (!rc && cudaMallocHost((void**)&c->h_err_sh, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S) != cudaSuccess)
+        rc = PSB_ENOMEM;
+    if (!rc) rc = cuda_check(c, cudaMemcpy(c->d_scenes, c->geom.data(), sizeof(psb::SceneGeom) * S, cudaMemcpyHostToDevice), "geom");
+    if (!rc) rc = cuda_check(c, cudaMemcpy(c->d_slot_scene, slot_scene.data(), 2 * (size_t)total, cudaMemcpyHostToDevice), "slots");
+    if (!rc) rc = cuda_check(c, cudaMemset(c->d_loop, 0, sizeof(int) * (2 + 4 * (size_t)S)), "loop");
+    if (!rc) rc = cuda_check(c, cudaMemset(c->d_active, 1, S), "active");
+    if (!rc) rc = cuda_check(c, cudaMemset(c->d_err_scene, 0, sizeof(unsigned long long) * S), "err");
+    if (!rc) rc = cuda_check(c, cudaMemset(c->d_err_sh, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S), "err");
+    if (!rc) rc = cuda_check(c, cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking), "stream");
+    if (!rc) rc = cuda_check(c, cudaStreamCreateWithFlags(&c->cap_main, cudaStreamNonBlocking), "stream");
+    if (rc) {
+        std::fprintf(stderr, "psb_create_batch: %s\n", c->err.c_str());
+        free_all(c);
+        delete c;
+        return rc;
+    }
+    std::memset(c->h_loop, 0, sizeof(int) * (2 + 4 * (size_t)S));
+    std::memset(c->h_err_sh, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S);
+    c->P.scenes = c->d_scenes;
+    c->P.slot_scene = c->d_slot_scene;
+    c->P.active = c->d_active;
+    c->P.err_scene = c->d_err_scene;
+    c->P.nscenes = S;
     *out = c;
     return PSB_OK;
 }
@@ -644,20 +979,23 @@ int psb_set_stream(psb_ctx* c, void* stream) {
 }
 
 static int upload_common(psb_ctx* c, int32_t n) {
-    // forget the previous particle set: clear its occupied cells
+    // forget the previous particle set; the next build clears its cells
     if (c->sorted >= 0) {
-        psb::launch_reset_cells(c->stream, c->sorted_n, c->keys[c->sorted], c->cell_start);
+        c->stale = c->sorted;
+        c->stale_n = c->sorted_n;
         c->sorted = -1;
     }
     c->n = n;
     c->cs = c->cr = 0;
     c->uploaded = true;
     c->built = false;
+    if (c->batch) cudaMemsetAsync(c->d_loop, 0, sizeof(int) * (2 + 4 * (size_t)c->nscenes), c->stream);
     return PSB_OK;
 }
 
 int psb_upload(psb_ctx* c, int32_t n, const float* pos, const float* vel, const float* vel_half, const float* pressure) {
     if (!c || n <= 0 || n > c->n_max || !pos) return fail(c, PSB_EINVAL, "psb_upload: bad n or NULL pos");
+    if (c->batch && n != c->n_max) return fail(c, PSB_EINVAL, "psb_upload: a batch takes all its scenes' particles");
     cudaSetDevice(c->device);
     upload_common(c, n);
     cudaStream_t st = c->stream;
@@ -676,6 +1014,7 @@ int psb_upload(psb_ctx* c, int32_t n, const float* pos, const float* vel, const 
 int psb_upload_aos_f64(psb_ctx* c, int32_t n, const double* pos, const double* vel, const double* vel_half,
                        int32_t on_device) {
     if (!c || n <= 0 || n > c->n_max || !pos) return fail(c, PSB_EINVAL, "psb_upload_aos_f64: bad n or NULL pos");
+    if (c->batch && n != c->n_max) return fail(c, PSB_EINVAL, "psb_upload_aos_f64: a batch takes all its scenes' particles");
     cudaSetDevice(c->device);
     upload_common(c, n);
     cudaStream_t st = c->stream;
@@ -881,6 +1220,7 @@ int psb_presolve(psb_ctx* c, int32_t iters) {
     P.n = c->n;
     const int s = c->cs, r = c->cr;
     cudaMemsetAsync(c->err_hist, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1), st);
+    if (c->batch) cudaMemsetAsync(c->d_active, 1, c->nscenes, st);     // every scene takes every pass
     timed(c, "pci_init", [&] {
         psb::launch_pci_init(st, P, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list, 1, c->fnp,
                              c->xs[0], c->vs);
@@ -934,6 +1274,7 @@ int iso_on_device(psb_ctx* c, const psb_iso_grid* g, double level, psb::IsoParam
     if (!g) return fail(c, PSB_EINVAL, "iso grid is NULL");
     if (!c->uploaded) return fail(c, PSB_ESTATE, "iso field before psb_upload");
     if (c->P.dem) return fail(c, PSB_EINVAL, "iso field: SPH scenes only");
+    if (c->batch) return fail(c, PSB_EINVAL, "iso field: single-scene contexts only");
     long long nn = 1;
     for (int a = 0; a < 3; ++a) {
         if (g->dims[a] < 2 || !(g->spacing[a] > 0) || !std::isfinite(g->origin[a]))
@@ -1077,6 +1418,61 @@ int psb_read_field(psb_ctx* c, int32_t field, void* dst, size_t bytes) {
     PSB_TRY(cuda_check(c, cudaMemcpyAsync(dst, src, need, cudaMemcpyDeviceToHost, st), "read_field"));
     PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "read_field"));
     return cuda_check(c, cudaGetLastError(), "read_field");
+}
+
+int psb_batch_layout(const psb_ctx* c, int32_t* n_scenes, int64_t* first) {
+    if (!c) return PSB_EINVAL;
+    if (n_scenes) *n_scenes = c->nscenes;
+    if (first) std::copy(c->first.begin(), c->first.end(), first);
+    return PSB_OK;
+}
+
+int psb_batch_stats(psb_ctx* c, int32_t* iters, int32_t* converged, double* err_final, int64_t* iters_total,
+                    int64_t* unconverged_steps) {
+    if (!c) return PSB_EINVAL;
+    const int S = c->nscenes;
+    if (!c->batch) {
+        if (iters) iters[0] = c->stats.iters;
+        if (converged) converged[0] = c->stats.converged;
+        if (err_final) err_final[0] = c->stats.iters >= 0 && c->stats.iters <= PSB_MAX_ITERS ? c->stats.err[c->stats.iters] : 0.0;
+        if (iters_total) iters_total[0] = c->stats.iters_total;
+        if (unconverged_steps) unconverged_steps[0] = -1;
+        return PSB_OK;
+    }
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->h_loop, c->d_loop, sizeof(int) * (2 + 4 * (size_t)S), cudaMemcpyDeviceToHost,
+                                          st), "loop"));
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->h_err_sh, c->d_err_sh, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S,
+                                          cudaMemcpyDeviceToHost, st), "err"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "sync"));
+    for (int k = 0; k < S; ++k) {
+        const int it = c->h_loop[2 + k];
+        if (iters) iters[k] = it;
+        if (converged) converged[k] = c->h_loop[2 + S + k];
+        if (err_final) {
+            // the last density pass: at index it if converged there, else it - 1
+            const int last = c->h_loop[2 + S + k] ? it : it - 1;
+            const unsigned long long e = last >= 0 && last <= PSB_MAX_ITERS ? c->h_err_sh[(size_t)last * S + k] : 0ull;
+            err_final[k] = e ? psb::unorder_double(e) : 0.0;
+        }
+        if (iters_total) iters_total[k] = c->h_loop[2 + 2 * S + k];
+        if (unconverged_steps) unconverged_steps[k] = c->h_loop[2 + 3 * S + k];
+    }
+    return PSB_OK;
+}
+
+int psb_set_graph(psb_ctx* c, int32_t on) {
+    if (!c) return PSB_EINVAL;
+    if (!c->batch) return fail(c, PSB_EINVAL, "psb_set_graph: batches only (psb_create_batch)");
+    cudaSetDevice(c->device);
+    if (!on) {
+        cudaStreamSynchronize(c->stream);
+        for (auto& g : c->gexec)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+    c->graph_on = on != 0;
+    return PSB_OK;
 }
 
 int psb_get_stats(psb_ctx* c, psb_step_stats* out) {

@@ -37,19 +37,24 @@ __global__ void k_reset_cells(int n, const uint32_t* __restrict__ sorted_keys, u
 }
 
 // Cell key of every particle, written at its id so that a stable sort of
-// the id-ordered keys yields (cell, id) order.
+// the id-ordered keys yields (cell, id) order. A batch gives each scene its
+// own grid and a block of keys after the previous scene's, so the sort keeps
+// every scene in its own contiguous slot range, in the order it has alone.
+template <bool BATCH>
 __global__ void k_cell_keys(Params P, const float4* __restrict__ pos, const int* __restrict__ ids,
                             uint32_t* __restrict__ keys_by_id, uint32_t* __restrict__ slot_by_id,
                             int* __restrict__ clamped) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= P.n) return;
     const float4 p = pos[s];
+    const Grid g = BATCH ? P.scenes[P.slot_scene[s]].g : P.g;
+    const uint32_t base = BATCH ? P.scenes[P.slot_scene[s]].cell_base : 0u;
     int c = 0;
-    const int i = cell_coord(p.x, P.g.gx, P.g.cell, P.g.nx, c);
-    const int j = cell_coord(p.y, P.g.gy, P.g.cell, P.g.ny, c);
-    const int k = cell_coord(p.z, P.g.gz, P.g.cell, P.g.nz, c);
+    const int i = cell_coord(p.x, g.gx, g.cell, g.nx, c);
+    const int j = cell_coord(p.y, g.gy, g.cell, g.ny, c);
+    const int k = cell_coord(p.z, g.gz, g.cell, g.nz, c);
     const int id = ids[s];
-    keys_by_id[id] = (uint32_t)i + (uint32_t)j * (uint32_t)P.g.nx + (uint32_t)k * (uint32_t)P.g.nx * (uint32_t)P.g.ny;
+    keys_by_id[id] = base + (uint32_t)i + (uint32_t)j * (uint32_t)g.nx + (uint32_t)k * (uint32_t)g.nx * (uint32_t)g.ny;
     slot_by_id[id] = (uint32_t)s;
     const unsigned ballot = __ballot_sync(__activemask(), c);
     if (ballot && (threadIdx.x & 31) == __ffs(ballot) - 1) atomicAdd(clamped, __popc(ballot));
@@ -199,7 +204,8 @@ __device__ __forceinline__ bool exact_neighbor(float4 a, float4 b, double h) {
 // One thread per sorted particle. The three cells of a grid row are
 // adjacent in sorted order, so each of the nine rows is one contiguous slot
 // range; candidates are visited in increasing slot order and the list is
-// sorted.
+// sorted. In a batch the walk stays inside the particle's scene's grid.
+template <bool BATCH>
 __global__ void __launch_bounds__(kBlock) k_build_nbr(Params P, const float4* __restrict__ pos,
                                                       const uint32_t* __restrict__ keys,
                                                       const uint32_t* __restrict__ cell_start,
@@ -207,18 +213,21 @@ __global__ void __launch_bounds__(kBlock) k_build_nbr(Params P, const float4* __
                                                       int* __restrict__ list, int* __restrict__ flags) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = t < P.n;       // every lane stays for the warp reductions below
-    const int n = P.n, nx = P.g.nx, ny = P.g.ny, nz = P.g.nz;
+    const int n = P.n;
     int cnt = 0;
     if (valid) {
+        const Grid g = BATCH ? P.scenes[P.slot_scene[t]].g : P.g;
+        const uint32_t base = BATCH ? P.scenes[P.slot_scene[t]].cell_base : 0u;
+        const int nx = g.nx, ny = g.ny, nz = g.nz;
         const float4 pi = pos[t];
-        const uint32_t key = keys[t];
+        const uint32_t key = keys[t] - base;
         const int ci = (int)(key % (uint32_t)nx);
         const int cj = (int)((key / (uint32_t)nx) % (uint32_t)ny);
         const int ck = (int)(key / ((uint32_t)nx * (uint32_t)ny));
         const int a0 = max(ci - 1, 0), a1 = min(ci + 1, nx - 1);
         for (int k = max(ck - 1, 0); k <= min(ck + 1, nz - 1); ++k) {
             for (int j = max(cj - 1, 0); j <= min(cj + 1, ny - 1); ++j) {
-                const uint32_t row = (uint32_t)j * (uint32_t)nx + (uint32_t)k * (uint32_t)nx * (uint32_t)ny;
+                const uint32_t row = base + (uint32_t)j * (uint32_t)nx + (uint32_t)k * (uint32_t)nx * (uint32_t)ny;
                 uint32_t lo = kEmpty, hi = 0;
                 for (int a = a0; a <= a1; ++a) {
                     const uint32_t s = cell_start[row + a];
@@ -270,7 +279,9 @@ void launch_reset_cells(cudaStream_t st, int n, const uint32_t* sorted_keys, uin
 
 void launch_cell_keys(cudaStream_t st, const Params& P, const float4* pos, const int* ids, uint32_t* keys_by_id,
                       uint32_t* slot_by_id, int* clamped) {
-    if (P.n > 0) k_cell_keys<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, ids, keys_by_id, slot_by_id, clamped);
+    if (P.n <= 0) return;
+    if (P.scenes) k_cell_keys<true><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, ids, keys_by_id, slot_by_id, clamped);
+    else k_cell_keys<false><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, ids, keys_by_id, slot_by_id, clamped);
 }
 
 int radix_blocks(int n) { return (n + kTile - 1) / kTile; }
@@ -299,7 +310,10 @@ void launch_reorder(cudaStream_t st, int n, const uint32_t* keys, const uint32_t
 
 void launch_build_nbr(cudaStream_t st, const Params& P, const float4* pos, const uint32_t* keys,
                       const uint32_t* cell_start, const uint32_t* cell_end, int* counts, int* list, int* flags) {
-    if (P.n > 0) k_build_nbr<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, keys, cell_start, cell_end, counts, list, flags);
+    if (P.n <= 0) return;
+    if (P.scenes)
+        k_build_nbr<true><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, keys, cell_start, cell_end, counts, list, flags);
+    else k_build_nbr<false><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, keys, cell_start, cell_end, counts, list, flags);
 }
 
 }  // namespace psb

@@ -27,6 +27,16 @@ struct Grid {
     int nx, ny, nz;
 };
 
+// One scene of a batch: its box and its own grid. Every other constant is
+// shared by the batch's scenes and lives in Params.
+struct SceneGeom {
+    float bx0, by0, bz0, bx1, by1, bz1;              // faces (ghost walls, wall distance)
+    float wlo_x, wlo_y, wlo_z, whi_x, whi_y, whi_z;  // projection bounds (faces -/+ particle radius)
+    Grid g;                                          // the scene's grid; its cells are keys cell_base + i + j nx + k nx ny
+    uint32_t cell_base;
+    int first, count;                                // its particles: sorted slots [first, first + count)
+};
+
 // Uniform per-scene constants, FP32 in normalised form (q = r^2/h^2, u = r/h)
 // so that no intermediate leaves FP32 range; derived on the host in FP64.
 struct Params {
@@ -63,6 +73,13 @@ struct Params {
     int ref;            // reference profile
     int pci;            // PCISPH (else WCSPH)
     int surface;        // surface tension on
+    // Batched scenes (kernels instantiated with BATCH = true read these; the
+    // box and grid fields above then go unused):
+    const SceneGeom* scenes;          // per scene
+    const uint16_t* slot_scene;       // scene of each sorted slot (scenes occupy contiguous slot ranges)
+    const uint8_t* active;            // corrector: scenes still iterating
+    unsigned long long* err_scene;    // corrector: per-scene max compression error of the pass (ordered)
+    int nscenes;
 };
 
 // ---- launchers (grid.cu) -------------------------------------------------
@@ -100,6 +117,15 @@ void launch_xsph(cudaStream_t st, const Params& P, const float4* xs, const float
                  const int* list, float4* vs_out);
 void launch_dem_step(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
                      const int* list, float4* pos_out, float4* vel_out, float4* vap_out, float4* force);
+
+// ---- batched scenes: the corrector loop on the device (batch.cu) ---------------
+// loop: [0] pass index, [1] continue, [2, 2 + S) corrections, [2 + S, 2 + 2S) converged,
+// [2 + 2S, 2 + 3S) corrections summed over steps, [2 + 3S, 2 + 4S) unconverged steps
+void launch_batch_begin(cudaStream_t st, int S, int max_it, uint8_t* active, unsigned long long* err_scene,
+                        unsigned long long* err_hist, int hist_len, int* loop);
+void launch_batch_decide(cudaStream_t st, int S, int min_it, int max_it, double eta, uint8_t* active,
+                         unsigned long long* err_scene, unsigned long long* err_hist, int* loop,
+                         cudaGraphConditionalHandle handle, int set_handle);
 
 // ---- iso field and marching cubes (mc.cu) ----------------------------------------
 constexpr int kMcMaxTri = 10;       // at most 12 active edges in loops of >= 3: 12 - 2 triangles

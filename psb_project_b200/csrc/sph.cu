@@ -51,19 +51,50 @@ __device__ __forceinline__ float density_deviation(const Params& P, const Kahan&
 
 __device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
 
+// The box faces that bound particle t (slot t): the scene's own (kernel
+// parameters, read where used) or, in a batch, its scene's table entry.
+template <bool BATCH> struct Faces;
+template <> struct Faces<false> {
+    const Params& P;
+    __device__ __forceinline__ float x0() const { return P.bx0; }
+    __device__ __forceinline__ float y0() const { return P.by0; }
+    __device__ __forceinline__ float z0() const { return P.bz0; }
+    __device__ __forceinline__ float x1() const { return P.bx1; }
+    __device__ __forceinline__ float y1() const { return P.by1; }
+    __device__ __forceinline__ float z1() const { return P.bz1; }
+};
+template <> struct Faces<true> {
+    const SceneGeom* G;
+    __device__ __forceinline__ float x0() const { return G->bx0; }
+    __device__ __forceinline__ float y0() const { return G->by0; }
+    __device__ __forceinline__ float z0() const { return G->bz0; }
+    __device__ __forceinline__ float x1() const { return G->bx1; }
+    __device__ __forceinline__ float y1() const { return G->by1; }
+    __device__ __forceinline__ float z1() const { return G->bz1; }
+};
+template <bool BATCH>
+__device__ __forceinline__ Faces<BATCH> faces_of(const Params& P, int t);
+template <>
+__device__ __forceinline__ Faces<false> faces_of<false>(const Params& P, int) { return Faces<false>{P}; }
+template <>
+__device__ __forceinline__ Faces<true> faces_of<true>(const Params& P, int t) {
+    return Faces<true>{P.scenes + P.slot_scene[t]};
+}
+
 // Penalty walls (config profile): a = K*depth - C*v along each axis on which
 // x lies outside the box (a state uploaded outside it; the projection below
 // keeps stepped particles inside).
-template <bool REF>
-__device__ __forceinline__ float3 wall_accel(const Params& P, float4 x, float4 v) {
+template <bool REF, bool BATCH = false>
+__device__ __forceinline__ float3 wall_accel(const Params& P, int t, float4 x, float4 v) {
     float3 a = make_float3(0.f, 0.f, 0.f);
     if (REF) return a;
-    if (x.x < P.bx0) a.x += P.wall_k * (P.bx0 - x.x) - P.wall_c * v.x;
-    if (x.x > P.bx1) a.x += -P.wall_k * (x.x - P.bx1) - P.wall_c * v.x;
-    if (x.y < P.by0) a.y += P.wall_k * (P.by0 - x.y) - P.wall_c * v.y;
-    if (x.y > P.by1) a.y += -P.wall_k * (x.y - P.by1) - P.wall_c * v.y;
-    if (x.z < P.bz0) a.z += P.wall_k * (P.bz0 - x.z) - P.wall_c * v.z;
-    if (x.z > P.bz1) a.z += -P.wall_k * (x.z - P.bz1) - P.wall_c * v.z;
+    const auto F = faces_of<BATCH>(P, t);
+    if (x.x < F.x0()) a.x += P.wall_k * (F.x0() - x.x) - P.wall_c * v.x;
+    if (x.x > F.x1()) a.x += -P.wall_k * (x.x - F.x1()) - P.wall_c * v.x;
+    if (x.y < F.y0()) a.y += P.wall_k * (F.y0() - x.y) - P.wall_c * v.y;
+    if (x.y > F.y1()) a.y += -P.wall_k * (x.y - F.y1()) - P.wall_c * v.y;
+    if (x.z < F.z0()) a.z += P.wall_k * (F.z0() - x.z) - P.wall_c * v.z;
+    if (x.z > F.z1()) a.z += -P.wall_k * (x.z - F.z1()) - P.wall_c * v.z;
     return a;
 }
 
@@ -81,15 +112,16 @@ __device__ __forceinline__ float3 wall_accel(const Params& P, float4 x, float4 v
 __device__ __forceinline__ float comp(float4 v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
 __device__ __forceinline__ float gcomp(const Params& P, int a) { return a == 0 ? P.gx : (a == 1 ? P.gy : P.gz); }
 
-__device__ __forceinline__ unsigned near_walls(const Params& P, float4 x) {
+template <class F_>
+__device__ __forceinline__ unsigned near_walls(const Params& P, const F_& F, float4 x) {
     unsigned w = 0u, n = 0u;
     auto push = [&](unsigned axis, unsigned lower) { w |= (axis | (lower << 2)) << (2u + 3u * n); ++n; };
-    if (x.x - P.bx0 < P.hf) push(0u, 1u);
-    else if (P.bx1 - x.x < P.hf) push(0u, 0u);
-    if (x.y - P.by0 < P.hf) push(1u, 1u);
-    else if (P.by1 - x.y < P.hf) push(1u, 0u);
-    if (x.z - P.bz0 < P.hf) push(2u, 1u);
-    else if (P.bz1 - x.z < P.hf) push(2u, 0u);
+    if (x.x - F.x0() < P.hf) push(0u, 1u);
+    else if (F.x1() - x.x < P.hf) push(0u, 0u);
+    if (x.y - F.y0() < P.hf) push(1u, 1u);
+    else if (F.y1() - x.y < P.hf) push(1u, 0u);
+    if (x.z - F.z0() < P.hf) push(2u, 1u);
+    else if (F.z1() - x.z < P.hf) push(2u, 0u);
     return w | n;
 }
 
@@ -98,13 +130,14 @@ __device__ __forceinline__ unsigned near_walls(const Params& P, float4 x) {
 // clamped at 0 so that a particle pushed through the face still sees its
 // ghosts on the wall side (unclamped, its own ghost would push it further
 // out). False if x_j is h or more inside.
-__device__ __forceinline__ bool reflect(const Params& P, unsigned w, int k, float4 xi, float4 xj, float3& r,
-                                        float& dp) {
+template <class F_>
+__device__ __forceinline__ bool reflect(const Params& P, const F_& F, unsigned w, int k, float4 xi, float4 xj,
+                                        float3& r, float& dp) {
     const unsigned f = (w >> (2 + 3 * k)) & 7u;
     const int a = (int)(f & 3u);
     const bool lower = (f >> 2) != 0u;
-    const float plane = lower ? (a == 0 ? P.bx0 : (a == 1 ? P.by0 : P.bz0))
-                              : (a == 0 ? P.bx1 : (a == 1 ? P.by1 : P.bz1));
+    const float plane = lower ? (a == 0 ? F.x0() : (a == 1 ? F.y0() : F.z0()))
+                              : (a == 0 ? F.x1() : (a == 1 ? F.y1() : F.z1()));
     const float nrm = lower ? 1.f : -1.f;
     const float dj = fmaxf(nrm * (comp(xj, a) - plane), 0.f);
     if (dj >= P.hf) return false;
@@ -117,24 +150,27 @@ __device__ __forceinline__ bool reflect(const Params& P, unsigned w, int k, floa
 
 // x_i minus the ghost of x_j across the faces in `mask`; false if a face of
 // the set is h or more from x_j. dp: the ghost's hydrostatic pressure offset.
-__device__ __forceinline__ bool ghost_delta(const Params& P, unsigned w, int mask, float4 xi, float4 xj, float3& r,
-                                            float& dp) {
+template <class F_>
+__device__ __forceinline__ bool ghost_delta(const Params& P, const F_& F, unsigned w, int mask, float4 xi,
+                                            float4 xj, float3& r, float& dp) {
     r = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
     dp = 0.f;
-    if ((mask & 1) && !reflect(P, w, 0, xi, xj, r, dp)) return false;
-    if ((mask & 2) && !reflect(P, w, 1, xi, xj, r, dp)) return false;
-    if ((mask & 4) && !reflect(P, w, 2, xi, xj, r, dp)) return false;
+    if ((mask & 1) && !reflect(P, F, w, 0, xi, xj, r, dp)) return false;
+    if ((mask & 2) && !reflect(P, F, w, 1, xi, xj, r, dp)) return false;
+    if ((mask & 4) && !reflect(P, F, w, 2, xi, xj, r, dp)) return false;
     return true;
 }
 
 // The ghosts of neighbour x_j (one per non-empty subset of the near faces).
 // Density: adds (1-q)^3 of each ghost within h.
-__device__ __forceinline__ void ghost_density_pair(const Params& P, unsigned w, float4 xi, float4 xj, Kahan& acc) {
+template <class F_>
+__device__ __forceinline__ void ghost_density_pair(const Params& P, const F_& F, unsigned w, float4 xi, float4 xj,
+                                                   Kahan& acc) {
     const int nm = 1 << (w & 3u);
     for (int mask = 1; mask < nm; ++mask) {
         float3 r;
         float dp;
-        if (!ghost_delta(P, w, mask, xi, xj, r, dp)) continue;
+        if (!ghost_delta(P, F, w, mask, xi, xj, r, dp)) continue;
         const float q = (r.x * r.x + r.y * r.y + r.z * r.z) * P.inv_h2;
         if (q >= 1.f) continue;
         const float wq = 1.f - q;
@@ -144,14 +180,15 @@ __device__ __forceinline__ void ghost_density_pair(const Params& P, unsigned w, 
 
 // Pressure: adds (pV_i + pV_ghost) (1-u)^2 x^ of each ghost within h, the
 // ghost carrying p_j continued hydrostatically across its faces.
-__device__ __forceinline__ void ghost_pressure_pair(const Params& P, unsigned w, float4 xi, float4 xj, float pVi,
-                                                    float pj, float3& ap) {
+template <class F_>
+__device__ __forceinline__ void ghost_pressure_pair(const Params& P, const F_& F, unsigned w, float4 xi, float4 xj,
+                                                    float pVi, float pj, float3& ap) {
     const float ir0 = 1.f / (P.rho0 * P.rho0);
     const int nm = 1 << (w & 3u);
     for (int mask = 1; mask < nm; ++mask) {
         float3 r;
         float dp;
-        if (!ghost_delta(P, w, mask, xi, xj, r, dp)) continue;
+        if (!ghost_delta(P, F, w, mask, xi, xj, r, dp)) continue;
         const float r2 = r.x * r.x + r.y * r.y + r.z * r.z;
         if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) continue;
         const float rinv = rsqrtf(r2);
@@ -165,21 +202,25 @@ __device__ __forceinline__ void ghost_pressure_pair(const Params& P, unsigned w,
 // particles within h of a face take (the walls are evaluated at xi). Kept
 // out of the main walk: a per-neighbour wall test there slows every
 // particle more than the separate walk costs the few near the faces.
+template <bool BATCH = false>
 __device__ __forceinline__ void ghost_density(const Params& P, int t, float4 xi, const float4* __restrict__ pos,
                                               const int* __restrict__ list, int cnt, Kahan& acc) {
-    const unsigned wall = near_walls(P, xi);
+    const auto F = faces_of<BATCH>(P, t);
+    const unsigned wall = near_walls(P, F, xi);
     if (!(wall & 3u)) return;
-    for (int c = 0; c < cnt; ++c) ghost_density_pair(P, wall, xi, pos[list[(size_t)c * P.n + t]], acc);
+    for (int c = 0; c < cnt; ++c) ghost_density_pair(P, F, wall, xi, pos[list[(size_t)c * P.n + t]], acc);
 }
 
+template <bool BATCH = false>
 __device__ __forceinline__ void ghost_pressure(const Params& P, int t, float4 xi, float pVi,
                                                const float4* __restrict__ pos, const float* __restrict__ pj_of,
                                                int pj_stride, const int* __restrict__ list, int cnt, float3& ap) {
-    const unsigned wall = near_walls(P, xi);
+    const auto F = faces_of<BATCH>(P, t);
+    const unsigned wall = near_walls(P, F, xi);
     if (!(wall & 3u)) return;
     for (int c = 0; c < cnt; ++c) {
         const int j = list[(size_t)c * P.n + t];
-        ghost_pressure_pair(P, wall, xi, pos[j], pVi, pj_of[(size_t)j * pj_stride], ap);
+        ghost_pressure_pair(P, F, wall, xi, pos[j], pVi, pj_of[(size_t)j * pj_stride], ap);
     }
 }
 
@@ -191,14 +232,20 @@ __device__ __forceinline__ void ghost_pressure(const Params& P, int t, float4 xi
 // behind a face meets its ghost at distance 0, which exerts no force, and
 // its density error could not be corrected). Config WCSPH keeps the penalty
 // walls its scene states.
-__device__ __forceinline__ void box_project(const Params& P, float3& x, float3& v) {
+template <bool BATCH = false>
+__device__ __forceinline__ void box_project(const Params& P, int t, float3& x, float3& v) {
+    float wlo_x = P.wlo_x, wlo_y = P.wlo_y, wlo_z = P.wlo_z, whi_x = P.whi_x, whi_y = P.whi_y, whi_z = P.whi_z;
+    if (BATCH) {
+        const SceneGeom* G = P.scenes + P.slot_scene[t];
+        wlo_x = G->wlo_x; wlo_y = G->wlo_y; wlo_z = G->wlo_z; whi_x = G->whi_x; whi_y = G->whi_y; whi_z = G->whi_z;
+    }
     float3 pI = x, nI = make_float3(0.f, 0.f, 0.f);
-    if (x.x >= P.whi_x) { pI.x = P.whi_x; nI.x = -1.f; }
-    if (x.y >= P.whi_y) { pI.y = P.whi_y; nI.y = -1.f; }
-    if (x.z >= P.whi_z) { pI.z = P.whi_z; nI.z = -1.f; }
-    if (x.x <= P.wlo_x) { pI.x = P.wlo_x; nI.x = 1.f; }
-    if (x.y <= P.wlo_y) { pI.y = P.wlo_y; nI.y = 1.f; }
-    if (x.z <= P.wlo_z) { pI.z = P.wlo_z; nI.z = 1.f; }
+    if (x.x >= whi_x) { pI.x = whi_x; nI.x = -1.f; }
+    if (x.y >= whi_y) { pI.y = whi_y; nI.y = -1.f; }
+    if (x.z >= whi_z) { pI.z = whi_z; nI.z = -1.f; }
+    if (x.x <= wlo_x) { pI.x = wlo_x; nI.x = 1.f; }
+    if (x.y <= wlo_y) { pI.y = wlo_y; nI.y = 1.f; }
+    if (x.z <= wlo_z) { pI.z = wlo_z; nI.z = 1.f; }
     const float l2 = nI.x * nI.x + nI.y * nI.y + nI.z * nI.z;
     if (l2 > 0.f) {
         const float il = rsqrtf(l2);
@@ -223,7 +270,7 @@ __device__ __forceinline__ void box_project(const Params& P, float3& x, float3& 
 //   f3 previous-step pressure / p_scale
 //   f4 distance to the nearest box face / h, capped at 1
 //   f5 k_grad |sum (1-u)^2 x^| h / rho0 (density-gradient magnitude)
-template <bool REF, bool FEAT>
+template <bool REF, bool FEAT, bool BATCH>
 __global__ void __launch_bounds__(kBlock) k_density_x(Params P, const float4* __restrict__ pos,
                                                       const float4* __restrict__ vel, const int* __restrict__ counts,
                                                       const int* __restrict__ list, float2* __restrict__ rp,
@@ -257,7 +304,7 @@ __global__ void __launch_bounds__(kBlock) k_density_x(Params P, const float4* __
             div += s * ((vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz);
         }
     }
-    if (!REF) ghost_density(P, t, xi, pos, list, cnt, acc);
+    if (!REF) ghost_density<BATCH>(P, t, xi, pos, list, cnt, acc);
     const float drho = density_deviation(P, acc);
     const float rho = P.rho0 + drho;
     float p;
@@ -273,10 +320,11 @@ __global__ void __launch_bounds__(kBlock) k_density_x(Params P, const float4* __
     }
     if (FEAT) {
         div *= -P.k_grad / P.rho0;
+        const auto F = faces_of<BATCH>(P, t);
         float dwall = P.hf;
-        dwall = fminf(dwall, fminf(xi.x - P.bx0, P.bx1 - xi.x));
-        dwall = fminf(dwall, fminf(xi.y - P.by0, P.by1 - xi.y));
-        dwall = fminf(dwall, fminf(xi.z - P.bz0, P.bz1 - xi.z));
+        dwall = fminf(dwall, fminf(xi.x - F.x0(), F.x1() - xi.x));
+        dwall = fminf(dwall, fminf(xi.y - F.y0(), F.y1() - xi.y));
+        dwall = fminf(dwall, fminf(xi.z - F.z0(), F.z1() - xi.z));
         float* f = feats + (size_t)t * 8;
         f[0] = (float)counts[t] * (1.f / 32.f);
         f[1] = (rho - P.dt * rho * div - P.rho0) / P.rho0 * 100.f;
@@ -298,7 +346,7 @@ struct PairSums {
     float fs;       // sum (1-q)(3-7q) / rho_j           (times -k_surf: surface term)
 };
 
-template <bool REF, bool WITH_PRESSURE>
+template <bool REF, bool WITH_PRESSURE, bool BATCH = false>
 __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi, float4 vi, float2 rpi,
                                               const float4* __restrict__ pos, const float4* __restrict__ vel,
                                               const float2* __restrict__ rp, const int* __restrict__ counts,
@@ -341,7 +389,7 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
         }
     }
     if (WITH_PRESSURE && !REF)
-        ghost_pressure(P, t, xi, pVi, pos, (const float*)rp + 1, 2, list, cnt, S.ap);
+        ghost_pressure<BATCH>(P, t, xi, pVi, pos, (const float*)rp + 1, 2, list, cnt, S.ap);
     return S;
 }
 
@@ -378,13 +426,13 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params P, const float4* 
     const PairSums S = pair_sums<REF, true>(P, t, xi, vi, rpi, pos, vel, rp, counts, list);
     const float3 f = nonpressure_force<REF>(P, S, rpi.x);
     fnp[t] = make_float4(f.x, f.y, f.z, 0.f);
-    const float3 aw = wall_accel<REF>(P, xi, vh);
+    const float3 aw = wall_accel<REF>(P, t, xi, vh);
     const float ir = 1.f / rpi.x;
     const float3 a = make_float3(f.x * ir + P.k_grad * S.ap.x + aw.x, f.y * ir + P.k_grad * S.ap.y + aw.y,
                                  f.z * ir + P.k_grad * S.ap.z + aw.z);
     float3 v = make_float3(vh.x + a.x * P.dt, vh.y + a.y * P.dt, vh.z + a.z * P.dt);
     float3 x = make_float3(xi.x + v.x * P.dt, xi.y + v.y * P.dt, xi.z + v.z * P.dt);
-    if (REF) box_project(P, x, v);   // config WCSPH: penalty walls only
+    if (REF) box_project(P, t, x, v);   // config WCSPH: penalty walls only
     pos_out[t] = make_float4(x.x, x.y, x.z, 0.f);
     vap_out[t] = make_float4(v.x, v.y, v.z, 0.f);
     vel_out[t] = make_float4((vh.x + v.x) * 0.5f, (vh.y + v.y) * 0.5f, (vh.z + v.z) * 0.5f, 0.f);
@@ -392,7 +440,7 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params P, const float4* 
 
 // PCISPH set-up sweep: non-pressure forces at x (and, for a warm start, the
 // pressure acceleration of the carried pressure), then the first prediction.
-template <bool REF, bool WARM>
+template <bool REF, bool WARM, bool BATCH>
 __global__ void __launch_bounds__(kBlock) k_pci_init(Params P, const float4* __restrict__ pos,
                                                      const float4* __restrict__ vel, const float4* __restrict__ vap,
                                                      const float2* __restrict__ rp, const int* __restrict__ counts,
@@ -402,10 +450,10 @@ __global__ void __launch_bounds__(kBlock) k_pci_init(Params P, const float4* __r
     if (t >= P.n) return;
     const float4 xi = pos[t], vi = vel[t], vh = vap[t];
     const float2 rpi = rp[t];
-    const PairSums S = pair_sums<REF, WARM>(P, t, xi, vi, rpi, pos, vel, rp, counts, list);
+    const PairSums S = pair_sums<REF, WARM, BATCH>(P, t, xi, vi, rpi, pos, vel, rp, counts, list);
     const float3 f = nonpressure_force<REF>(P, S, rpi.x);
     fnp[t] = make_float4(f.x, f.y, f.z, 0.f);
-    const float3 aw = wall_accel<REF>(P, xi, vh);
+    const float3 aw = wall_accel<REF, BATCH>(P, t, xi, vh);
     const float ir = 1.f / rpi.x;
     const float ap = WARM ? P.k_grad : 0.f;
     const float3 a = make_float3(f.x * ir + ap * S.ap.x + aw.x, f.y * ir + ap * S.ap.y + aw.y,
@@ -417,14 +465,17 @@ __global__ void __launch_bounds__(kBlock) k_pci_init(Params P, const float4* __r
 
 // PCISPH density pass at x*: rho*, the gradient sums of the pressure
 // increment, the candidate pressure and the FP64 max compression error.
-template <bool REF>
+// Batch: scenes that have converged are left as they are, and the error is
+// the max over each scene (P.err_scene).
+template <bool REF, bool BATCH>
 __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* __restrict__ xs,
                                                         const float2* __restrict__ rp, const int* __restrict__ counts,
                                                         const int* __restrict__ list, float2* __restrict__ rpc,
                                                         unsigned long long* __restrict__ err_slot) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double err = -1e300;
-    if (t < P.n) {
+    const int sc = BATCH && t < P.n ? (int)P.slot_scene[t] : -1;
+    if (t < P.n && (!BATCH || P.active[sc])) {
         const float4 xi = xs[t];
         const int cnt = min(counts[t], P.cap);
         Kahan acc;
@@ -448,7 +499,7 @@ __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* 
                 T2 += g * g;
             }
         }
-        if (!REF) ghost_density(P, t, xi, xs, list, cnt, acc);
+        if (!REF) ghost_density<BATCH>(P, t, xi, xs, list, cnt, acc);
         const float drho = density_deviation(P, acc);
         const float rho = P.rho0 + drho;
         float p = rp[t].y;
@@ -460,15 +511,26 @@ __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* 
         rpc[t] = make_float2(rho, p);
         err = (double)drho / P.rho0_d;
     }
+    if constexpr (BATCH) {    // a warp inside one scene reduces first; one straddling two or more reduces per lane
+        const int sc0 = __shfl_sync(0xffffffffu, sc, 0);
+        if (__all_sync(0xffffffffu, sc == sc0 || sc < 0)) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
-    __shared__ double s_err[kBlock / 32];
-    if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = err;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double m = s_err[0];
-        for (int w = 1; w < kBlock / 32; ++w) m = fmax(m, s_err[w]);
-        if (m > -1e300) atomicMax(err_slot, order_double(m));
+            for (int o = 16; o > 0; o >>= 1) err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
+            if ((threadIdx.x & 31) == 0 && sc0 >= 0 && err > -1e300) atomicMax(&P.err_scene[sc0], order_double(err));
+        } else if (sc >= 0 && err > -1e300) {
+            atomicMax(&P.err_scene[sc], order_double(err));
+        }
+    } else {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
+        __shared__ double s_err[kBlock / 32];
+        if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = err;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double m = s_err[0];
+            for (int w = 1; w < kBlock / 32; ++w) m = fmax(m, s_err[w]);
+            if (m > -1e300) atomicMax(err_slot, order_double(m));
+        }
     }
 }
 
@@ -480,7 +542,7 @@ __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* 
 // fixed-point iteration in positions whose gain grows with p dt^2/h^2, and
 // with rho* in p/rho^2 the force feeds back on the density; under a 0.64 m
 // column either one makes the corrector diverge.
-template <bool REF>
+template <bool REF, bool BATCH>
 __global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const float4* __restrict__ pos,
                                                               const float4* __restrict__ vap,
                                                               const float4* __restrict__ fnp,
@@ -491,6 +553,7 @@ __global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const fl
                                                               float4* __restrict__ vs, float2* __restrict__ rp) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= P.n) return;
+    if (BATCH && !P.active[P.slot_scene[t]]) return;     // its scene has converged
     const float4* __restrict__ geo = REF ? xs : pos;
     const float4 xi = geo[t];
     const float2 ri = rpc[t];
@@ -513,9 +576,9 @@ __global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const fl
         const float s = (pVi + pVj) * om * om * rinv;
         acc.x += s * dx; acc.y += s * dy; acc.z += s * dz;
     }
-    if (!REF) ghost_pressure(P, t, xi, pVi, geo, (const float*)rpc + 1, 2, list, cnt, acc);
+    if (!REF) ghost_pressure<BATCH>(P, t, xi, pVi, geo, (const float*)rpc + 1, 2, list, cnt, acc);
     const float4 x0 = pos[t], vh = vap[t], f = fnp[t];
-    const float3 aw = wall_accel<REF>(P, x0, vh);
+    const float3 aw = wall_accel<REF, BATCH>(P, t, x0, vh);
     const float ir = 1.f / ri.x;
     const float3 a = make_float3(f.x * ir + P.k_grad * acc.x + aw.x, f.y * ir + P.k_grad * acc.y + aw.y,
                                  f.z * ir + P.k_grad * acc.z + aw.z);
@@ -526,6 +589,7 @@ __global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const fl
 }
 
 // Commit of the last prediction, walls, velocity interpolation.
+template <bool BATCH>
 __global__ void __launch_bounds__(kBlock) k_pci_commit(Params P, const float4* __restrict__ xs,
                                                        const float4* __restrict__ vs, const float2* __restrict__ rpc,
                                                        int have_density_pass, float4* __restrict__ pos,
@@ -535,7 +599,7 @@ __global__ void __launch_bounds__(kBlock) k_pci_commit(Params P, const float4* _
     if (t >= P.n) return;
     float3 x = f3(xs[t]), v = f3(vs[t]);
     const float4 vh = vap[t];
-    box_project(P, x, v);
+    box_project<BATCH>(P, t, x, v);
     pos[t] = make_float4(x.x, x.y, x.z, 0.f);
     vap[t] = make_float4(v.x, v.y, v.z, 0.f);
     vel[t] = make_float4((vh.x + v.x) * 0.5f, (vh.y + v.y) * 0.5f, (vh.z + v.z) * 0.5f, 0.f);
@@ -571,14 +635,17 @@ inline int grid_of(int n) { return (n + kBlock - 1) / kBlock; }
 
 }  // namespace
 
+// Kernels are specialised on the physics profile (REF) and on batching
+// (P.scenes set: per-scene boxes and convergence; config profile only).
 void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
                       const int* list, float2* rp, float* rho_x, int zero_p, float p_scale, float* feats) {
     if (P.n <= 0) return;
     const unsigned g = grid_of(P.n);
-    if (P.ref) k_density_x<true, false><<<g, kBlock, 0, st>>>(P, pos, vel, counts, list, rp, rho_x, zero_p, p_scale, feats);
-    else if (feats)
-        k_density_x<false, true><<<g, kBlock, 0, st>>>(P, pos, vel, counts, list, rp, rho_x, zero_p, p_scale, feats);
-    else k_density_x<false, false><<<g, kBlock, 0, st>>>(P, pos, vel, counts, list, rp, rho_x, zero_p, p_scale, feats);
+    auto go = [&](auto kernel) { kernel<<<g, kBlock, 0, st>>>(P, pos, vel, counts, list, rp, rho_x, zero_p, p_scale, feats); };
+    if (P.ref) go(k_density_x<true, false, false>);
+    else if (P.scenes) { if (feats) go(k_density_x<false, true, true>); else go(k_density_x<false, false, true>); }
+    else if (feats) go(k_density_x<false, true, false>);
+    else go(k_density_x<false, false, false>);
 }
 
 void launch_wcsph_force(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float4* vap,
@@ -598,32 +665,32 @@ void launch_pci_init(cudaStream_t st, const Params& P, const float4* pos, const 
                      float4* vs) {
     if (P.n <= 0) return;
     const dim3 g(grid_of(P.n));
-    if (P.ref) {
-        if (warm) k_pci_init<true, true><<<g, kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, fnp, xs, vs);
-        else k_pci_init<true, false><<<g, kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, fnp, xs, vs);
-    } else {
-        if (warm) k_pci_init<false, true><<<g, kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, fnp, xs, vs);
-        else k_pci_init<false, false><<<g, kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, fnp, xs, vs);
-    }
+    auto go = [&](auto kernel) { kernel<<<g, kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, fnp, xs, vs); };
+    if (P.ref) { if (warm) go(k_pci_init<true, true, false>); else go(k_pci_init<true, false, false>); }
+    else if (P.scenes) { if (warm) go(k_pci_init<false, true, true>); else go(k_pci_init<false, false, true>); }
+    else if (warm) go(k_pci_init<false, true, false>);
+    else go(k_pci_init<false, false, false>);
 }
 
 void launch_pci_density(cudaStream_t st, const Params& P, const float4* xs, const float2* rp, const int* counts,
                         const int* list, float2* rpc, unsigned long long* err_slot) {
     if (P.n <= 0) return;
-    if (P.ref) k_pci_density<true><<<grid_of(P.n), kBlock, 0, st>>>(P, xs, rp, counts, list, rpc, err_slot);
-    else k_pci_density<false><<<grid_of(P.n), kBlock, 0, st>>>(P, xs, rp, counts, list, rpc, err_slot);
+    auto go = [&](auto kernel) { kernel<<<grid_of(P.n), kBlock, 0, st>>>(P, xs, rp, counts, list, rpc, err_slot); };
+    if (P.ref) go(k_pci_density<true, false>);
+    else if (P.scenes) go(k_pci_density<false, true>);
+    else go(k_pci_density<false, false>);
 }
 
 void launch_pci_force_predict(cudaStream_t st, const Params& P, const float4* pos, const float4* vap,
                               const float4* fnp, const float4* xs, const float2* rpc, const int* counts,
                               const int* list, float4* xs_next, float4* vs, float2* rp) {
     if (P.n <= 0) return;
-    if (P.ref)
-        k_pci_force_predict<true><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vap, fnp, xs, rpc, counts, list, xs_next,
-                                                                   vs, rp);
-    else
-        k_pci_force_predict<false><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vap, fnp, xs, rpc, counts, list, xs_next,
-                                                                    vs, rp);
+    auto go = [&](auto kernel) {
+        kernel<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vap, fnp, xs, rpc, counts, list, xs_next, vs, rp);
+    };
+    if (P.ref) go(k_pci_force_predict<true, false>);
+    else if (P.scenes) go(k_pci_force_predict<false, true>);
+    else go(k_pci_force_predict<false, false>);
 }
 
 void launch_xsph(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const int* counts,
@@ -633,7 +700,10 @@ void launch_xsph(cudaStream_t st, const Params& P, const float4* xs, const float
 
 void launch_pci_commit(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const float2* rpc,
                        int have_density_pass, float4* pos, float4* vel, float4* vap, float2* rp) {
-    if (P.n > 0) k_pci_commit<<<grid_of(P.n), kBlock, 0, st>>>(P, xs, vs, rpc, have_density_pass, pos, vel, vap, rp);
+    if (P.n <= 0) return;
+    if (P.scenes)
+        k_pci_commit<true><<<grid_of(P.n), kBlock, 0, st>>>(P, xs, vs, rpc, have_density_pass, pos, vel, vap, rp);
+    else k_pci_commit<false><<<grid_of(P.n), kBlock, 0, st>>>(P, xs, vs, rpc, have_density_pass, pos, vel, vap, rp);
 }
 
 }  // namespace psb

@@ -1,6 +1,7 @@
 """Replica runs over several GPUs (one process per GPU): a single dam break
-is not partitioned, each rank steps its own scene, and the ranks only agree
-on the timing.
+is not partitioned, each rank steps its own scene (or, for a batch of
+independent scenes, its size-balanced share of them), and the ranks only
+agree on the timing.
 
   * every rank gets the same scene with its own lattice seed;
   * the timed region is bracketed by a barrier and the device
@@ -51,6 +52,22 @@ class Replicas:
             self.dist.barrier()
             self.dist.destroy_process_group()
             self.dist = None
+
+
+def assign_scenes(sizes, world: int):
+    """Size-balanced assignment of independent scenes to `world` ranks
+    (longest processing time first: each scene, largest first, goes to the
+    rank with the fewest particles so far; ties to the lower rank). Every
+    rank computes the same assignment from the same sizes, so the ranks need
+    no exchange. Returns, per rank, its scene indices in increasing order."""
+    order = sorted(range(len(sizes)), key=lambda i: (-int(sizes[i]), i))
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += int(sizes[i])
+    return [sorted(v) for v in out]
 
 
 def env_ranks():

@@ -37,7 +37,8 @@ EXPORTS = (
     "psb_profile_enable", "psb_profile_read", "psb_profile_reset", "psb_lattice", "psb_status_string",
     "psb_last_error", "psb_abi_version", "psb_sort_cells_noalloc", "psb_presolve", "psb_mlp_set_weights",
     "psb_mlp_get_weights", "psb_mlp_collect", "psb_mlp_dataset", "psb_mlp_train", "psb_mlp_forward",
-    "psb_mlp_loss_grad", "psb_iso_field", "psb_extract_surface",
+    "psb_mlp_loss_grad", "psb_iso_field", "psb_extract_surface", "psb_create_batch", "psb_batch_layout",
+    "psb_batch_stats", "psb_set_graph",
 )
 MLP_PARAMS = 4673       # PSB_MLP_PARAMS
 MLP_IN, MLP_H = 6, 64
@@ -120,6 +121,10 @@ def lib():
         "psb_iso_field": ([P, ctypes.POINTER(IsoGrid), P], ctypes.c_int),
         "psb_extract_surface": ([P, ctypes.POINTER(IsoGrid), ctypes.c_double, P, ctypes.POINTER(I64), P,
                                  ctypes.POINTER(I64)], ctypes.c_int),
+        "psb_create_batch": ([ctypes.POINTER(PsbScene), I32, ctypes.POINTER(P)], ctypes.c_int),
+        "psb_batch_layout": ([P, ctypes.POINTER(I32), P], ctypes.c_int),
+        "psb_batch_stats": ([P, P, P, P, P, P], ctypes.c_int),
+        "psb_set_graph": ([P, I32], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -273,6 +278,17 @@ class Simulation:
                     "psb_mlp_train")
         return loss.value
 
+    def mlp_fit(self, iters: int, batch: int, lr: float, chunks: int = 10, seed: int = 0) -> float:
+        """Adam on the collected pairs with a cosine-decayed learning rate:
+        `chunks` equal runs of psb_mlp_train, the k-th at
+        lr * (1 + cos(pi (k + 1/2) / chunks)) / 2. Adam's moments carry over
+        between the chunks. Returns the last chunk's loss."""
+        loss = float("nan")
+        for k in range(chunks):
+            lr_k = lr * 0.5 * (1.0 + np.cos(np.pi * (k + 0.5) / chunks))
+            loss = self.mlp_train(max(1, iters // chunks), batch, lr_k, seed=seed * 1000 + k)
+        return loss
+
     def mlp_forward(self, X) -> np.ndarray:
         X8 = np.zeros((X.shape[0], 8), np.float32)
         X8[:, :X.shape[1]] = X
@@ -357,3 +373,51 @@ class Simulation:
             res[buf.value.decode()] = (la.value, ms.value)
             i += 1
         return res
+
+
+class BatchSimulation(Simulation):
+    """One psb_ctx over many independent scenes (psb_create_batch): every
+    sweep is one launch over all of them, each scene converging on its own.
+    Particles are concatenated in scene order; `first[s]` is scene s's first
+    particle id and `first[-1]` the total."""
+
+    def __init__(self, scenes):
+        scenes = list(scenes)
+        self.scenes = scenes
+        self._cs = (PsbScene * len(scenes))(*[sc.to_c() for sc in scenes])
+        h = ctypes.c_void_p()
+        rc = lib().psb_create_batch(self._cs, len(scenes), ctypes.byref(h))
+        if rc != OK:
+            raise PsbError(rc, f"psb_create_batch: {lib().psb_status_string(rc).decode()}")
+        self._h = h
+        self.n = 0
+        self.first = self.layout()
+        self.scene = scenes[0].replace(n=int(self.first[-1]))
+
+    def layout(self) -> np.ndarray:
+        ns = ctypes.c_int32()
+        self._check(lib().psb_batch_layout(self._h, ctypes.byref(ns), None), "psb_batch_layout")
+        first = np.empty(ns.value + 1, np.int64)
+        self._check(lib().psb_batch_layout(self._h, ctypes.byref(ns), _ptr(first)), "psb_batch_layout")
+        return first
+
+    def batch_stats(self) -> dict:
+        """Per-scene arrays: iters, converged, err_final (last step), iters_total and
+        unconverged_steps (since the last upload)."""
+        S = len(self.scenes)
+        it, cv = np.empty(S, np.int32), np.empty(S, np.int32)
+        err, tot, unc = np.empty(S, np.float64), np.empty(S, np.int64), np.empty(S, np.int64)
+        self._check(lib().psb_batch_stats(self._h, _ptr(it), _ptr(cv), _ptr(err), _ptr(tot), _ptr(unc)),
+                    "psb_batch_stats")
+        return {"iters": it, "converged": cv, "err_final": err, "iters_total": tot, "unconverged_steps": unc}
+
+    def set_graph(self, on: bool = True):
+        self._check(lib().psb_set_graph(self._h, 1 if on else 0), "psb_set_graph")
+
+    def split(self, a: np.ndarray):
+        """Per-scene views of an array in particle-id order."""
+        return [a[self.first[s]:self.first[s + 1]] for s in range(len(self.scenes))]
+
+
+def batch_positions(scenes) -> np.ndarray:
+    return np.concatenate([scene_positions(sc) for sc in scenes])

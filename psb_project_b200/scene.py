@@ -329,6 +329,31 @@ def config_scene(name: str) -> Scene:
     raise ValueError(f"unknown scene {name!r}")
 
 
+def batch_scenes(n_scenes: int = 64, seed: int = 3, n_range=(4096, 131072), spacing: float = 0.01, h: float = 0.02,
+                 side=(1.0, 2.0), fill=(0.4, 0.7), dt: float = 5e-4, warm_start: int = WARM_LEARNED,
+                 jitter: float = 1e-4, steps: int = 300) -> List[Scene]:
+    """Independent PCISPH dam breaks for one batch (config C3): particle
+    counts log-uniform in n_range, each a lattice block at `spacing` in the
+    corner of its own box, its height `fill` of the box's, box sides uniform
+    in `side`; all drawn from `seed`. The block's footprint is square,
+    nx = nz = round(sqrt(N / ny)), so the count is N up to that rounding.
+    The scenes share every constant but their boxes and counts (a batch's
+    requirement); each has its own jitter seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(n_scenes):
+        target = math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))
+        box = tuple(float(round(v, 3)) for v in rng.uniform(side[0], side[1], 3))
+        f = rng.uniform(fill[0], fill[1])
+        ny = max(2, int(round(f * box[1] / spacing)))
+        nxz = max(2, int(round(math.sqrt(target / ny))))
+        nxz = min(nxz, int(box[0] / spacing) - 2, int(box[2] / spacing) - 2)
+        sc = dam_break((nxz, ny, nxz), spacing, box, h, dt=dt, seed=seed * 1000 + s, jitter=jitter, steps=steps,
+                       name=f"C3 scene {s}")
+        out.append(sc.replace(warm_start=warm_start))
+    return out
+
+
 def ref_scene(nxyz=(12, 10, 8), spacing=0.01, box=(0.3, 0.3, 0.3), h=0.02, method=PCISPH, dt=5e-4,
               seed=7, jitter=1e-4) -> Scene:
     """Small scene in the reference-compatible profile (parity tests)."""
