@@ -61,6 +61,10 @@ ALG_BYTES = {
     "wcsph_force": 228,       # forces 52 + integrate 80 + walls/interpolation 96
     "mlp_infer": 36,          # features 32 -> initial pressure 4
 }
+TUNE_KEYS = ("bucket", "nbr_block", "nbr_schedule", "density_block", "init_block", "pci_density_block", "force_block",
+             "xsph_block")
+
+
 # Kernels per timed group (radix_sort is 3 kernels per 8-bit pass).
 def _kernels_per_group(name: str, sort_passes: int) -> int:
     return 3 * sort_passes if name == "radix_sort" else 1
@@ -78,15 +82,23 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
     ap.add_argument("--presolve", type=int, default=256, help="initial-pressure corrector passes before the warm-up")
-    ap.add_argument("--train-steps", type=int, default=400, help="plain-PCISPH steps recorded for training (learned)")
+    ap.add_argument("--train-steps", type=int, default=None,
+                    help="plain-PCISPH steps recorded for training (learned; default 400, C3: 100)")
     ap.add_argument("--train-iters", type=int, default=10000, help="Adam steps (learned)")
     ap.add_argument("--train-batch", type=int, default=65536)
     ap.add_argument("--train-lr", type=float, default=3e-3, help="peak learning rate of the cosine schedule")
     ap.add_argument("--xsph", type=float, default=None, help="override the scene's XSPH velocity smoothing factor")
     ap.add_argument("--no-graph", action="store_true", help="C3: launch kernel by kernel instead of CUDA graphs")
-    ap.add_argument("--eval-steps", type=int, default=1000,
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch configuration)")
+    ap.add_argument("--eval-steps", type=int, default=None,
                     help="steps after the recorded ones over which the warm starts are compared (0: skip)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    c3 = args.scene == "C3"
+    if args.train_steps is None:
+        args.train_steps = 100 if c3 else 400
+    if args.eval_steps is None:
+        args.eval_steps = 300 if c3 else 1000   # C3: 300 steps of every scene
+    return args
 
 
 
@@ -257,9 +269,13 @@ def run_ours(args):
 
     max_over_ranks = rep_.max_over_ranks
 
+    tune = None       # the autotuner's choice, given to every context created after it
+
     def make(mode):
         s_ = P.Simulation(base.replace(warm_start=mode))
         s_.set_stream(stream.cuda_stream)
+        if tune is not None:
+            s_.tune_set(**{k: tune[k] for k in TUNE_KEYS})
         return s_
 
     # Set-up (untimed): the dam at rest with its initial pressure, then plain
@@ -320,6 +336,11 @@ def run_ours(args):
             s.profile(False)
         return max_over_ranks(e0.elapsed_time(e1)), iters, prof
 
+    # ---- autotuner (untimed): launch configuration for this size bucket ----------
+    if not args.no_tune:
+        restore(sim)
+        sim.step(2)
+        tune = sim.autotune(trials=5)
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
@@ -435,6 +456,7 @@ def run_ours(args):
                                "min": int(np.min(iters))},
             "comparison": comparison,
             "learned_training": train_info,
+            "autotune": tune,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None if traffic is None else traffic * n,
@@ -475,10 +497,14 @@ def run_batch(args):
         rep_.barrier()
         torch.cuda.synchronize()
 
+    tune = None       # the autotuner's choice, given to every context created after it
+
     def make(mode, graph=True):
         b = P.BatchSimulation([s.replace(warm_start=mode) for s in scenes])
         b.set_stream(stream.cuda_stream)
         b.set_graph(graph and not args.no_graph)
+        if tune is not None:
+            b.tune_set(**{k: tune[k] for k in TUNE_KEYS})
         return b
 
     # set-up (untimed): initial pressure, plain steps recorded for training, warm-up
@@ -535,6 +561,10 @@ def run_batch(args):
     sim = make(modes[args.warm_start])
     if weights is not None:
         sim.mlp_set_weights(weights)
+    if not args.no_tune:
+        restore(sim)
+        sim.step(2)
+        tune = sim.autotune(trials=5)
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
@@ -583,7 +613,11 @@ def run_batch(args):
     passes = (max(1, int(np.ceil(np.log2(sum(int(np.prod(s.dims)) for s in scenes))))) + 7) // 8
     launches = int(sum(l * _kernels_per_group(k, passes) for k, (l, _) in prof.items()))
     tot_ms = sum(v[1] for v in prof.values())
-    dom = max((k for k in prof if k in ALG_BYTES), key=lambda k: prof[k][1])
+    # the corrector passes skip the scenes that have converged, so their
+    # launches do not cover every particle: the roofline kernel is the
+    # costliest of the sweeps that do
+    partial = ("pci_density", "pci_force_predict")
+    dom = max((k for k in prof if k in ALG_BYTES and k not in partial), key=lambda k: prof[k][1])
     l_dom, ms_dom = prof[dom]
     per_launch_s = ms_dom / l_dom / 1e3
     achieved = ALG_BYTES[dom] * n / per_launch_s / 1e9
@@ -607,6 +641,7 @@ def run_batch(args):
                                "min_scene": float(np.min(per_scene)), "unconverged_steps": int(np.sum(unconv))},
             "comparison": comparison,
             "learned_training": train_info,
+            "autotune": tune,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                          "alg_bytes_per_particle": ALG_BYTES[dom], "mean_launch_us": per_launch_s * 1e6},

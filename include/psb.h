@@ -306,6 +306,39 @@ int psb_batch_stats(psb_ctx* ctx, int32_t* iters, int32_t* converged, double* er
  * both ways launch the same kernels in the same order. */
 int psb_set_graph(psb_ctx* ctx, int32_t on);
 
+/* Autotuner: the launch configuration of the neighbour build and the five
+ * gather sweeps (density at x, PCISPH set-up, density/pressure pass,
+ * pressure-force pass, XSPH), kept per size bucket, bucket = floor(log2 n)
+ * of the particle count (a batch's total). Candidates: block sizes 128, 256
+ * and 512, and for the neighbour build two cell schedules -- 0, each thread
+ * walks its own 27 cells; 1, the lanes of a warp that share a grid row walk
+ * it together, staging 32 candidates at a time in shared memory. Every
+ * candidate computes the same result bit for bit; only the time differs.
+ * No counterpart in the reference, whose launches are sized by
+ * computeGridSize with 256 threads (common.cu:102-107). */
+typedef struct psb_tune {
+    int32_t bucket;
+    int32_t nbr_block, nbr_schedule;
+    int32_t density_block, init_block, pci_density_block, force_block, xsph_block;
+    /* mean launch times (ms) of the choice and of the default (256 threads,
+     * schedule 0): neighbour build, density at x, set-up, density/pressure,
+     * pressure force, XSPH (0 where the scene has no such kernel) */
+    double ms[6];
+    double ms_default[6];
+} psb_tune;
+/* Times every candidate `trials` times (CUDA events, after one untimed
+ * launch) on the context's current particles -- after at least one step --
+ * and stores the fastest of each kernel for the current bucket; later steps
+ * at that bucket use it. The state (positions, velocities, densities,
+ * pressures) is left as it was; scratch buffers are recomputed next step.
+ * Captured step graphs are released (they are captured again). */
+int psb_autotune(psb_ctx* ctx, int32_t trials, psb_tune* out);
+/* Installs a table entry (t->bucket; block sizes 0/128/256/512, 0 = 256;
+ * schedule 0 or 1), e.g. one saved from an earlier run. */
+int psb_tune_set(psb_ctx* ctx, const psb_tune* t);
+/* The entry for `bucket` (block sizes 0 when the bucket has none). */
+int psb_tune_get(psb_ctx* ctx, int32_t bucket, psb_tune* out);
+
 const char* psb_status_string(int32_t status);
 const char* psb_last_error(const psb_ctx* ctx);
 int32_t psb_abi_version(void);

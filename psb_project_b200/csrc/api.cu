@@ -18,6 +18,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <map>
 
 #include "psb.h"
 #include "psb_internal.cuh"
@@ -147,6 +148,8 @@ struct psb_ctx {
     int* d_loop = nullptr;                        // device loop words (batch.cu)
     int* h_loop = nullptr;                        // pinned mirrors
     unsigned long long* h_err_sh = nullptr;
+    // autotuner: launch configuration per size bucket (floor(log2 n))
+    std::map<int, psb_tune> tune_table;
     // CUDA-graph stepping (batches)
     bool graph_on = false;
     cudaGraphExec_t gexec[2] = {};                // one per state buffer parity (cs)
@@ -978,6 +981,30 @@ int psb_set_stream(psb_ctx* c, void* stream) {
     return PSB_OK;
 }
 
+static int size_bucket(int64_t n) {
+    int b = 0;
+    while (b < 62 && ((int64_t)1 << (b + 1)) <= n) ++b;
+    return b;
+}
+
+// The launch configuration of the current particle count's bucket.
+static void apply_tune(psb_ctx* c) {
+    psb::Tune t{};
+    auto it = c->tune_table.find(size_bucket(c->n));
+    if (it != c->tune_table.end()) {
+        const psb_tune& e = it->second;
+        t = psb::Tune{e.nbr_block, e.nbr_schedule, e.density_block, e.init_block, e.pci_density_block, e.force_block,
+                      e.xsph_block};
+    }
+    c->P.tune = t;
+}
+
+static void release_graphs(psb_ctx* c) {
+    cudaStreamSynchronize(c->stream);
+    for (auto& g : c->gexec)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
 static int upload_common(psb_ctx* c, int32_t n) {
     // forget the previous particle set; the next build clears its cells
     if (c->sorted >= 0) {
@@ -989,6 +1016,7 @@ static int upload_common(psb_ctx* c, int32_t n) {
     c->cs = c->cr = 0;
     c->uploaded = true;
     c->built = false;
+    apply_tune(c);
     if (c->batch) cudaMemsetAsync(c->d_loop, 0, sizeof(int) * (2 + 4 * (size_t)c->nscenes), c->stream);
     return PSB_OK;
 }
@@ -1466,12 +1494,137 @@ int psb_set_graph(psb_ctx* c, int32_t on) {
     if (!c) return PSB_EINVAL;
     if (!c->batch) return fail(c, PSB_EINVAL, "psb_set_graph: batches only (psb_create_batch)");
     cudaSetDevice(c->device);
-    if (!on) {
-        cudaStreamSynchronize(c->stream);
-        for (auto& g : c->gexec)
-            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-    }
+    if (!on) release_graphs(c);
     c->graph_on = on != 0;
+    return PSB_OK;
+}
+
+static bool block_ok(int b) { return b == 0 || b == 128 || b == 256 || b == 512; }
+
+int psb_tune_set(psb_ctx* c, const psb_tune* t) {
+    if (!c || !t) return PSB_EINVAL;
+    if (t->bucket < 0 || t->bucket > 62 || !block_ok(t->nbr_block) || !block_ok(t->density_block) ||
+        !block_ok(t->init_block) || !block_ok(t->pci_density_block) || !block_ok(t->force_block) ||
+        !block_ok(t->xsph_block) || (t->nbr_schedule != 0 && t->nbr_schedule != 1))
+        return fail(c, PSB_EINVAL, "psb_tune_set: block sizes 0/128/256/512, schedule 0 or 1, bucket 0..62");
+    cudaSetDevice(c->device);
+    c->tune_table[t->bucket] = *t;
+    release_graphs(c);
+    apply_tune(c);
+    return PSB_OK;
+}
+
+int psb_tune_get(psb_ctx* c, int32_t bucket, psb_tune* out) {
+    if (!c || !out) return PSB_EINVAL;
+    auto it = c->tune_table.find(bucket);
+    if (it != c->tune_table.end()) { *out = it->second; return PSB_OK; }
+    std::memset(out, 0, sizeof(*out));
+    out->bucket = bucket;
+    return PSB_OK;
+}
+
+int psb_autotune(psb_ctx* c, int32_t trials, psb_tune* out) {
+    if (!c || trials < 1 || trials > 1000) return fail(c, PSB_EINVAL, "psb_autotune: trials in 1..1000");
+    if (!c->uploaded || !c->built || c->sorted < 0 || c->stats.steps < 1)
+        return fail(c, PSB_ESTATE, "psb_autotune: take a step first");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    const int n = c->n;
+    const int s = c->cs, r = c->cr;
+    const bool pci = c->P.pci && !c->P.dem;
+    const bool sph = !c->P.dem;
+    const bool feats = pci && !c->P.ref && (c->sc.warm_start == PSB_WARM_LEARNED || c->collect_stride > 0);
+    const int warm = (pci && (c->P.ref || c->sc.warm_start != PSB_WARM_ZERO)) ? 1 : 0;
+    // the pressure-force pass overwrites the carried pressures, the density
+    // pass the densities: keep them
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->stage, c->rp[r], sizeof(float2) * n, cudaMemcpyDeviceToDevice, st), "tune"));
+    if (c->batch) cudaMemsetAsync(c->d_active, 1, c->nscenes, st);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto time_it = [&](auto launch) {
+        launch();
+        cudaEventRecord(e0, st);
+        for (int i = 0; i < trials; ++i) launch();
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return (double)ms / trials;
+    };
+    const int blocks[3] = {128, 256, 512};
+    psb_tune best{};
+    best.bucket = size_bucket(n);
+    Params P = c->P;
+    P.n = n;
+    // one kernel at a time: every other kernel at its default
+    auto tune_one = [&](int which, auto launch) {
+        double best_ms = 1e300;
+        int best_b = 256, best_sched = 0;
+        const int nsched = which == 0 ? 2 : 1;
+        for (int sched = 0; sched < nsched; ++sched)
+            for (int b : blocks) {
+                Params Q = P;
+                Q.tune = psb::Tune{};
+                switch (which) {
+                    case 0: Q.tune.nbr_block = b; Q.tune.nbr_schedule = sched; break;
+                    case 1: Q.tune.density_block = b; break;
+                    case 2: Q.tune.init_block = b; break;
+                    case 3: Q.tune.pci_density_block = b; break;
+                    case 4: Q.tune.force_block = b; break;
+                    default: Q.tune.xsph_block = b; break;
+                }
+                const double ms = time_it([&] { launch(Q); });
+                if (b == 256 && sched == 0) best.ms_default[which] = ms;
+                if (ms < best_ms) { best_ms = ms; best_b = b; best_sched = sched; }
+            }
+        best.ms[which] = best_ms;
+        switch (which) {
+            case 0: best.nbr_block = best_b; best.nbr_schedule = best_sched; break;
+            case 1: best.density_block = best_b; break;
+            case 2: best.init_block = best_b; break;
+            case 3: best.pci_density_block = best_b; break;
+            case 4: best.force_block = best_b; break;
+            default: best.xsph_block = best_b; break;
+        }
+    };
+    tune_one(0, [&](const Params& Q) {
+        psb::launch_build_nbr(st, Q, c->pos[s], c->keys[c->sorted], c->cell_start, c->cell_end, c->nbr_count,
+                              c->nbr_list, c->flags);
+    });
+    if (sph)
+        tune_one(1, [&](const Params& Q) {
+            psb::launch_density_x(st, Q, c->pos[s], c->vel[s], c->nbr_count, c->nbr_list, c->rp[r], c->rho_x, 0,
+                                  c->p_scale, feats ? c->feats : nullptr);
+        });
+    if (pci) {
+        tune_one(2, [&](const Params& Q) {
+            psb::launch_pci_init(st, Q, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list, warm,
+                                 c->fnp, c->xs[0], c->vs);
+        });
+        tune_one(3, [&](const Params& Q) {
+            psb::launch_pci_density(st, Q, c->xs[0], c->rp[r], c->nbr_count, c->nbr_list, c->rpc, &c->err_hist[0]);
+        });
+        tune_one(4, [&](const Params& Q) {
+            psb::launch_pci_force_predict(st, Q, c->pos[s], c->vap[s], c->fnp, c->xs[0], c->rpc, c->nbr_count,
+                                          c->nbr_list, c->xs[1], c->vs, c->rp[r]);
+        });
+        tune_one(5, [&](const Params& Q) {
+            psb::launch_xsph(st, Q, c->xs[0], c->vs, c->nbr_count, c->nbr_list, c->xs[1]);
+        });
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->rp[r], c->stage, sizeof(float2) * n, cudaMemcpyDeviceToDevice, st), "tune"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "tune"));
+    PSB_TRY(cuda_check(c, cudaGetLastError(), "tune"));
+    // kernels a scene does not run keep the default
+    if (!sph) best.density_block = 0;
+    if (!pci) best.init_block = best.pci_density_block = best.force_block = best.xsph_block = 0;
+    c->tune_table[best.bucket] = best;
+    release_graphs(c);
+    apply_tune(c);
+    if (out) *out = best;
     return PSB_OK;
 }
 

@@ -201,17 +201,34 @@ __device__ __forceinline__ bool exact_neighbor(float4 a, float4 b, double h) {
     return __dsqrt_rn(d2) <= h;
 }
 
-// One thread per sorted particle. The three cells of a grid row are
-// adjacent in sorted order, so each of the nine rows is one contiguous slot
-// range; candidates are visited in increasing slot order and the list is
-// sorted. In a batch the walk stays inside the particle's scene's grid.
-template <bool BATCH>
-__global__ void __launch_bounds__(kBlock) k_build_nbr(Params P, const float4* __restrict__ pos,
-                                                      const uint32_t* __restrict__ keys,
-                                                      const uint32_t* __restrict__ cell_start,
-                                                      const uint32_t* __restrict__ cell_end, int* __restrict__ counts,
-                                                      int* __restrict__ list, int* __restrict__ flags) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+// flags[1]: max count, flags[2..3]: total pairs (64-bit); every lane of the
+// warp calls it.
+__device__ __forceinline__ void nbr_flags(int cnt, int* __restrict__ flags) {
+    int m = cnt;
+    unsigned long long tot = (unsigned long long)cnt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    }
+    if ((threadIdx.x & 31) == 0 && tot > 0) {
+        atomicMax(&flags[1], m);
+        atomicAdd((unsigned long long*)&flags[2], tot);
+    }
+}
+
+// Per-thread schedule: one thread per sorted particle. The three cells of a
+// grid row are adjacent in sorted order, so each of the nine rows is one
+// contiguous slot range; candidates are visited in increasing slot order and
+// the list is sorted. In a batch the walk stays inside the particle's
+// scene's grid.
+template <bool BATCH, int BS>
+__global__ void __launch_bounds__(BS) k_build_nbr(Params P, const float4* __restrict__ pos,
+                                                  const uint32_t* __restrict__ keys,
+                                                  const uint32_t* __restrict__ cell_start,
+                                                  const uint32_t* __restrict__ cell_end, int* __restrict__ counts,
+                                                  int* __restrict__ list, int* __restrict__ flags) {
+    const int t = blockIdx.x * BS + threadIdx.x;
     const bool valid = t < P.n;       // every lane stays for the warp reductions below
     const int n = P.n;
     int cnt = 0;
@@ -255,18 +272,107 @@ __global__ void __launch_bounds__(kBlock) k_build_nbr(Params P, const float4* __
         counts[t] = cnt;
         if (cnt > P.cap) atomicOr(&flags[0], 1);
     }
-    // flags[1]: max count, flags[2..3]: total pairs (64-bit)
-    int m = cnt;
-    unsigned long long tot = (unsigned long long)cnt;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-        tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    nbr_flags(cnt, flags);
+}
+
+// Warp-cooperative schedule (row tiles). The lanes of a warp whose particles
+// lie in the same grid row (same scene, j and k; consecutive sorted
+// particles mostly do) form a group and walk its nine neighbour rows
+// together. For each row the group's slot span -- the union of its lanes'
+// three-cell ranges, one contiguous run of cells -- is staged 32 candidates
+// at a time in shared memory, one coalesced load per lane, and each lane
+// tests the staged candidates that lie inside its own range, in slot order.
+// A lane therefore accepts the same candidates in the same order as in the
+// per-thread schedule; the gathers become one load per candidate per group
+// instead of one per candidate per lane.
+template <bool BATCH, int BS>
+__global__ void __launch_bounds__(BS) k_build_nbr_tile(Params P, const float4* __restrict__ pos,
+                                                       const uint32_t* __restrict__ keys,
+                                                       const uint32_t* __restrict__ cell_start,
+                                                       const uint32_t* __restrict__ cell_end,
+                                                       int* __restrict__ counts, int* __restrict__ list,
+                                                       int* __restrict__ flags) {
+    __shared__ float4 s_tile[BS];
+    float4* tile = s_tile + (threadIdx.x & ~31u);
+    const int lane = threadIdx.x & 31;
+    const int t = blockIdx.x * BS + threadIdx.x;
+    const bool valid = t < P.n;
+    const int n = P.n;
+    int cnt = 0;
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    int nx = 1, ny = 1, nz = 1, ci = 0, cj = 0, ck = 0;
+    uint32_t base = 0, rowkey = kEmpty;     // rowkey: the global key of cell (0, j, k) of the particle's row
+    if (valid) {
+        const Grid g = BATCH ? P.scenes[P.slot_scene[t]].g : P.g;
+        base = BATCH ? P.scenes[P.slot_scene[t]].cell_base : 0u;
+        nx = g.nx; ny = g.ny; nz = g.nz;
+        pi = pos[t];
+        const uint32_t key = keys[t] - base;
+        ci = (int)(key % (uint32_t)nx);
+        cj = (int)((key / (uint32_t)nx) % (uint32_t)ny);
+        ck = (int)(key / ((uint32_t)nx * (uint32_t)ny));
+        rowkey = keys[t] - (uint32_t)ci;
     }
-    if ((threadIdx.x & 31) == 0 && tot > 0) {
-        atomicMax(&flags[1], m);
-        atomicAdd((unsigned long long*)&flags[2], tot);
+    const int a0 = max(ci - 1, 0), a1 = min(ci + 1, nx - 1);
+    unsigned todo = __ballot_sync(0xffffffffu, valid);
+    while (todo) {
+        const int leader = __ffs(todo) - 1;
+        const uint32_t rk = __shfl_sync(0xffffffffu, rowkey, leader);
+        const unsigned grp = __ballot_sync(0xffffffffu, valid && rowkey == rk);
+        todo &= ~grp;
+        const bool mine = (grp >> lane) & 1u;
+        // the group shares scene, j, k and the grid: take them from the leader
+        const int gj = __shfl_sync(0xffffffffu, cj, leader), gk = __shfl_sync(0xffffffffu, ck, leader);
+        const int gnx = __shfl_sync(0xffffffffu, nx, leader), gny = __shfl_sync(0xffffffffu, ny, leader);
+        const int gnz = __shfl_sync(0xffffffffu, nz, leader);
+        const uint32_t gbase = __shfl_sync(0xffffffffu, base, leader);
+        for (int k = max(gk - 1, 0); k <= min(gk + 1, gnz - 1); ++k) {
+            for (int j = max(gj - 1, 0); j <= min(gj + 1, gny - 1); ++j) {
+                const uint32_t row = gbase + (uint32_t)j * (uint32_t)gnx + (uint32_t)k * (uint32_t)gnx * (uint32_t)gny;
+                uint32_t lo = kEmpty, hi = 0;
+                if (mine) {
+                    for (int a = a0; a <= a1; ++a) {
+                        const uint32_t s = cell_start[row + a];
+                        if (s != kEmpty) {
+                            if (lo == kEmpty) lo = s;
+                            hi = cell_end[row + a];
+                        }
+                    }
+                }
+                const uint32_t L = __reduce_min_sync(0xffffffffu, lo);
+                const uint32_t H = __reduce_max_sync(0xffffffffu, hi);
+                if (L == kEmpty) continue;
+                for (uint32_t q0 = L; q0 < H; q0 += 32u) {
+                    if (q0 + lane < H) tile[lane] = pos[q0 + lane];
+                    __syncwarp();
+                    if (mine && lo != kEmpty) {
+                        // this lane's part of the staged chunk [q0, q0 + 32): [c0, c1)
+                        const uint32_t c0 = lo > q0 ? lo - q0 : 0u;
+                        const uint32_t c1 = hi > q0 ? min(hi - q0, 32u) : 0u;
+                        for (uint32_t c = c0; c < c1; ++c) {
+                            const float4 pj = tile[c];
+                            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                            const float d2 = dx * dx + dy * dy + dz * dz;
+                            bool acc;
+                            if (d2 < P.h2_lo) acc = true;
+                            else if (d2 > P.h2_hi) acc = false;
+                            else acc = exact_neighbor(pi, pj, P.h);
+                            if (acc) {
+                                if (cnt < P.cap) list[(size_t)cnt * n + t] = (int)(q0 + c);
+                                ++cnt;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+        }
     }
+    if (valid) {
+        counts[t] = cnt;
+        if (cnt > P.cap) atomicOr(&flags[0], 1);
+    }
+    nbr_flags(cnt, flags);
 }
 
 inline int grid_of(int n) { return (n + kBlock - 1) / kBlock; }
@@ -311,9 +417,16 @@ void launch_reorder(cudaStream_t st, int n, const uint32_t* keys, const uint32_t
 void launch_build_nbr(cudaStream_t st, const Params& P, const float4* pos, const uint32_t* keys,
                       const uint32_t* cell_start, const uint32_t* cell_end, int* counts, int* list, int* flags) {
     if (P.n <= 0) return;
-    if (P.scenes)
-        k_build_nbr<true><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, keys, cell_start, cell_end, counts, list, flags);
-    else k_build_nbr<false><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, keys, cell_start, cell_end, counts, list, flags);
+    with_block(P.tune.nbr_block, [&](auto B) {
+        constexpr int BS = decltype(B)::value;
+        const unsigned g = (unsigned)((P.n + BS - 1) / BS);
+        auto go = [&](auto kernel) { kernel<<<g, BS, 0, st>>>(P, pos, keys, cell_start, cell_end, counts, list, flags); };
+        if (P.tune.nbr_schedule == 1) {
+            if (P.scenes) go(k_build_nbr_tile<true, BS>); else go(k_build_nbr_tile<false, BS>);
+        } else {
+            if (P.scenes) go(k_build_nbr<true, BS>); else go(k_build_nbr<false, BS>);
+        }
+    });
 }
 
 }  // namespace psb

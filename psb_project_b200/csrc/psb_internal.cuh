@@ -15,6 +15,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 
 namespace psb {
 
@@ -35,6 +36,15 @@ struct SceneGeom {
     Grid g;                                          // the scene's grid; its cells are keys cell_base + i + j nx + k nx ny
     uint32_t cell_base;
     int first, count;                                // its particles: sorted slots [first, first + count)
+};
+
+// Launch configuration of the tunable kernels, the autotuner's choice for a
+// size bucket: block sizes (128, 256 or 512; 0 = 256) and the neighbour
+// build's schedule (0: each thread walks its own 27 cells; 1: the lanes of a
+// warp that share a grid row walk it together, staging candidates in shared
+// memory). Every choice computes the same result bit for bit.
+struct Tune {
+    int nbr_block, nbr_schedule, density_block, init_block, pci_density_block, force_block, xsph_block;
 };
 
 // Uniform per-scene constants, FP32 in normalised form (q = r^2/h^2, u = r/h)
@@ -80,7 +90,16 @@ struct Params {
     const uint8_t* active;            // corrector: scenes still iterating
     unsigned long long* err_scene;    // corrector: per-scene max compression error of the pass (ordered)
     int nscenes;
+    Tune tune;
 };
+
+// Runs f(std::integral_constant<int, B>) with B the tuned block size.
+template <class F>
+inline void with_block(int bs, F&& f) {
+    if (bs == 128) f(std::integral_constant<int, 128>{});
+    else if (bs == 512) f(std::integral_constant<int, 512>{});
+    else f(std::integral_constant<int, 256>{});
+}
 
 // ---- launchers (grid.cu) -------------------------------------------------
 void launch_reset_cells(cudaStream_t st, int n, const uint32_t* sorted_keys, uint32_t* cell_start);

@@ -270,8 +270,8 @@ __device__ __forceinline__ void box_project(const Params& P, int t, float3& x, f
 //   f3 previous-step pressure / p_scale
 //   f4 distance to the nearest box face / h, capped at 1
 //   f5 k_grad |sum (1-u)^2 x^| h / rho0 (density-gradient magnitude)
-template <bool REF, bool FEAT, bool BATCH>
-__global__ void __launch_bounds__(kBlock) k_density_x(Params P, const float4* __restrict__ pos,
+template <bool REF, bool FEAT, bool BATCH, int BS>
+__global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __restrict__ pos,
                                                       const float4* __restrict__ vel, const int* __restrict__ counts,
                                                       const int* __restrict__ list, float2* __restrict__ rp,
                                                       float* __restrict__ rho_x, int zero_p, float p_scale,
@@ -440,8 +440,8 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params P, const float4* 
 
 // PCISPH set-up sweep: non-pressure forces at x (and, for a warm start, the
 // pressure acceleration of the carried pressure), then the first prediction.
-template <bool REF, bool WARM, bool BATCH>
-__global__ void __launch_bounds__(kBlock) k_pci_init(Params P, const float4* __restrict__ pos,
+template <bool REF, bool WARM, bool BATCH, int BS>
+__global__ void __launch_bounds__(BS) k_pci_init(Params P, const float4* __restrict__ pos,
                                                      const float4* __restrict__ vel, const float4* __restrict__ vap,
                                                      const float2* __restrict__ rp, const int* __restrict__ counts,
                                                      const int* __restrict__ list, float4* __restrict__ fnp,
@@ -467,8 +467,8 @@ __global__ void __launch_bounds__(kBlock) k_pci_init(Params P, const float4* __r
 // increment, the candidate pressure and the FP64 max compression error.
 // Batch: scenes that have converged are left as they are, and the error is
 // the max over each scene (P.err_scene).
-template <bool REF, bool BATCH>
-__global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* __restrict__ xs,
+template <bool REF, bool BATCH, int BS>
+__global__ void __launch_bounds__(BS) k_pci_density(Params P, const float4* __restrict__ xs,
                                                         const float2* __restrict__ rp, const int* __restrict__ counts,
                                                         const int* __restrict__ list, float2* __restrict__ rpc,
                                                         unsigned long long* __restrict__ err_slot) {
@@ -523,12 +523,12 @@ __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* 
     } else {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
-        __shared__ double s_err[kBlock / 32];
+        __shared__ double s_err[BS / 32];
         if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = err;
         __syncthreads();
         if (threadIdx.x == 0) {
             double m = s_err[0];
-            for (int w = 1; w < kBlock / 32; ++w) m = fmax(m, s_err[w]);
+            for (int w = 1; w < BS / 32; ++w) m = fmax(m, s_err[w]);
             if (m > -1e300) atomicMax(err_slot, order_double(m));
         }
     }
@@ -542,8 +542,8 @@ __global__ void __launch_bounds__(kBlock) k_pci_density(Params P, const float4* 
 // fixed-point iteration in positions whose gain grows with p dt^2/h^2, and
 // with rho* in p/rho^2 the force feeds back on the density; under a 0.64 m
 // column either one makes the corrector diverge.
-template <bool REF, bool BATCH>
-__global__ void __launch_bounds__(kBlock) k_pci_force_predict(Params P, const float4* __restrict__ pos,
+template <bool REF, bool BATCH, int BS>
+__global__ void __launch_bounds__(BS) k_pci_force_predict(Params P, const float4* __restrict__ pos,
                                                               const float4* __restrict__ vap,
                                                               const float4* __restrict__ fnp,
                                                               const float4* __restrict__ xs,
@@ -609,7 +609,8 @@ __global__ void __launch_bounds__(kBlock) k_pci_commit(Params P, const float4* _
 // XSPH velocity smoothing (Monaghan 1989) of the committed prediction,
 // config PCISPH: v_i + xsph sum_j (m/rho0) W_ij (v_j - v_i) over the list at
 // x*, W the poly6 kernel (m W = k_rho (1-q)^3). Positions are not moved.
-__global__ void __launch_bounds__(kBlock) k_xsph(Params P, const float4* __restrict__ xs,
+template <int BS>
+__global__ void __launch_bounds__(BS) k_xsph(Params P, const float4* __restrict__ xs,
                                                  const float4* __restrict__ vs, const int* __restrict__ counts,
                                                  const int* __restrict__ list, float4* __restrict__ vs_out) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -635,17 +636,25 @@ inline int grid_of(int n) { return (n + kBlock - 1) / kBlock; }
 
 }  // namespace
 
-// Kernels are specialised on the physics profile (REF) and on batching
-// (P.scenes set: per-scene boxes and convergence; config profile only).
+// Kernels are specialised on the physics profile (REF), on batching
+// (P.scenes set: per-scene boxes and convergence; config profile only) and
+// on the tuned block size.
+template <int BS>
+inline unsigned blocks_of(int n) { return (unsigned)((n + BS - 1) / BS); }
+
 void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
                       const int* list, float2* rp, float* rho_x, int zero_p, float p_scale, float* feats) {
     if (P.n <= 0) return;
-    const unsigned g = grid_of(P.n);
-    auto go = [&](auto kernel) { kernel<<<g, kBlock, 0, st>>>(P, pos, vel, counts, list, rp, rho_x, zero_p, p_scale, feats); };
-    if (P.ref) go(k_density_x<true, false, false>);
-    else if (P.scenes) { if (feats) go(k_density_x<false, true, true>); else go(k_density_x<false, false, true>); }
-    else if (feats) go(k_density_x<false, true, false>);
-    else go(k_density_x<false, false, false>);
+    with_block(P.tune.density_block, [&](auto B) {
+        constexpr int BS = decltype(B)::value;
+        auto go = [&](auto kernel) {
+            kernel<<<blocks_of<BS>(P.n), BS, 0, st>>>(P, pos, vel, counts, list, rp, rho_x, zero_p, p_scale, feats);
+        };
+        if (P.ref) go(k_density_x<true, false, false, BS>);
+        else if (P.scenes) { if (feats) go(k_density_x<false, true, true, BS>); else go(k_density_x<false, false, true, BS>); }
+        else if (feats) go(k_density_x<false, true, false, BS>);
+        else go(k_density_x<false, false, false, BS>);
+    });
 }
 
 void launch_wcsph_force(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float4* vap,
@@ -664,38 +673,52 @@ void launch_pci_init(cudaStream_t st, const Params& P, const float4* pos, const 
                      const float2* rp, const int* counts, const int* list, int warm, float4* fnp, float4* xs,
                      float4* vs) {
     if (P.n <= 0) return;
-    const dim3 g(grid_of(P.n));
-    auto go = [&](auto kernel) { kernel<<<g, kBlock, 0, st>>>(P, pos, vel, vap, rp, counts, list, fnp, xs, vs); };
-    if (P.ref) { if (warm) go(k_pci_init<true, true, false>); else go(k_pci_init<true, false, false>); }
-    else if (P.scenes) { if (warm) go(k_pci_init<false, true, true>); else go(k_pci_init<false, false, true>); }
-    else if (warm) go(k_pci_init<false, true, false>);
-    else go(k_pci_init<false, false, false>);
+    with_block(P.tune.init_block, [&](auto B) {
+        constexpr int BS = decltype(B)::value;
+        auto go = [&](auto kernel) {
+            kernel<<<blocks_of<BS>(P.n), BS, 0, st>>>(P, pos, vel, vap, rp, counts, list, fnp, xs, vs);
+        };
+        if (P.ref) { if (warm) go(k_pci_init<true, true, false, BS>); else go(k_pci_init<true, false, false, BS>); }
+        else if (P.scenes) { if (warm) go(k_pci_init<false, true, true, BS>); else go(k_pci_init<false, false, true, BS>); }
+        else if (warm) go(k_pci_init<false, true, false, BS>);
+        else go(k_pci_init<false, false, false, BS>);
+    });
 }
 
 void launch_pci_density(cudaStream_t st, const Params& P, const float4* xs, const float2* rp, const int* counts,
                         const int* list, float2* rpc, unsigned long long* err_slot) {
     if (P.n <= 0) return;
-    auto go = [&](auto kernel) { kernel<<<grid_of(P.n), kBlock, 0, st>>>(P, xs, rp, counts, list, rpc, err_slot); };
-    if (P.ref) go(k_pci_density<true, false>);
-    else if (P.scenes) go(k_pci_density<false, true>);
-    else go(k_pci_density<false, false>);
+    with_block(P.tune.pci_density_block, [&](auto B) {
+        constexpr int BS = decltype(B)::value;
+        auto go = [&](auto kernel) { kernel<<<blocks_of<BS>(P.n), BS, 0, st>>>(P, xs, rp, counts, list, rpc, err_slot); };
+        if (P.ref) go(k_pci_density<true, false, BS>);
+        else if (P.scenes) go(k_pci_density<false, true, BS>);
+        else go(k_pci_density<false, false, BS>);
+    });
 }
 
 void launch_pci_force_predict(cudaStream_t st, const Params& P, const float4* pos, const float4* vap,
                               const float4* fnp, const float4* xs, const float2* rpc, const int* counts,
                               const int* list, float4* xs_next, float4* vs, float2* rp) {
     if (P.n <= 0) return;
-    auto go = [&](auto kernel) {
-        kernel<<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vap, fnp, xs, rpc, counts, list, xs_next, vs, rp);
-    };
-    if (P.ref) go(k_pci_force_predict<true, false>);
-    else if (P.scenes) go(k_pci_force_predict<false, true>);
-    else go(k_pci_force_predict<false, false>);
+    with_block(P.tune.force_block, [&](auto B) {
+        constexpr int BS = decltype(B)::value;
+        auto go = [&](auto kernel) {
+            kernel<<<blocks_of<BS>(P.n), BS, 0, st>>>(P, pos, vap, fnp, xs, rpc, counts, list, xs_next, vs, rp);
+        };
+        if (P.ref) go(k_pci_force_predict<true, false, BS>);
+        else if (P.scenes) go(k_pci_force_predict<false, true, BS>);
+        else go(k_pci_force_predict<false, false, BS>);
+    });
 }
 
 void launch_xsph(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const int* counts,
                  const int* list, float4* vs_out) {
-    if (P.n > 0) k_xsph<<<grid_of(P.n), kBlock, 0, st>>>(P, xs, vs, counts, list, vs_out);
+    if (P.n <= 0) return;
+    with_block(P.tune.xsph_block, [&](auto B) {
+        constexpr int BS = decltype(B)::value;
+        k_xsph<BS><<<blocks_of<BS>(P.n), BS, 0, st>>>(P, xs, vs, counts, list, vs_out);
+    });
 }
 
 void launch_pci_commit(cudaStream_t st, const Params& P, const float4* xs, const float4* vs, const float2* rpc,

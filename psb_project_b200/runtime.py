@@ -38,7 +38,7 @@ EXPORTS = (
     "psb_last_error", "psb_abi_version", "psb_sort_cells_noalloc", "psb_presolve", "psb_mlp_set_weights",
     "psb_mlp_get_weights", "psb_mlp_collect", "psb_mlp_dataset", "psb_mlp_train", "psb_mlp_forward",
     "psb_mlp_loss_grad", "psb_iso_field", "psb_extract_surface", "psb_create_batch", "psb_batch_layout",
-    "psb_batch_stats", "psb_set_graph",
+    "psb_batch_stats", "psb_set_graph", "psb_autotune", "psb_tune_set", "psb_tune_get",
 )
 MLP_PARAMS = 4673       # PSB_MLP_PARAMS
 MLP_IN, MLP_H = 6, 64
@@ -51,6 +51,22 @@ class PsbStepStats(ctypes.Structure):
         ("clamped", ctypes.c_int32), ("nbr_total", ctypes.c_int64),
         ("err", ctypes.c_double * (PSB_MAX_ITERS + 1)), ("steps", ctypes.c_int64), ("iters_total", ctypes.c_int64),
     ]
+
+
+class PsbTune(ctypes.Structure):
+    """psb_tune: the autotuner's launch configuration for one size bucket."""
+    _fields_ = [("bucket", ctypes.c_int32), ("nbr_block", ctypes.c_int32), ("nbr_schedule", ctypes.c_int32),
+                ("density_block", ctypes.c_int32), ("init_block", ctypes.c_int32),
+                ("pci_density_block", ctypes.c_int32), ("force_block", ctypes.c_int32),
+                ("xsph_block", ctypes.c_int32), ("ms", ctypes.c_double * 6), ("ms_default", ctypes.c_double * 6)]
+
+    KERNELS = ("build_nbr", "density_x", "pci_init", "pci_density", "pci_force_predict", "xsph")
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_[:8]}
+        d["ms"] = dict(zip(self.KERNELS, list(self.ms)))
+        d["ms_default"] = dict(zip(self.KERNELS, list(self.ms_default)))
+        return d
 
 
 class IsoGrid(ctypes.Structure):
@@ -125,6 +141,9 @@ def lib():
         "psb_batch_layout": ([P, ctypes.POINTER(I32), P], ctypes.c_int),
         "psb_batch_stats": ([P, P, P, P, P, P], ctypes.c_int),
         "psb_set_graph": ([P, I32], ctypes.c_int),
+        "psb_autotune": ([P, I32, ctypes.POINTER(PsbTune)], ctypes.c_int),
+        "psb_tune_set": ([P, ctypes.POINTER(PsbTune)], ctypes.c_int),
+        "psb_tune_get": ([P, I32, ctypes.POINTER(PsbTune)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -354,6 +373,30 @@ class Simulation:
         s = PsbStepStats()
         self._check(lib().psb_get_stats(self._h, ctypes.byref(s)), "psb_get_stats")
         return s
+
+    # -- autotuner ---------------------------------------------------------------
+    def autotune(self, trials: int = 5) -> dict:
+        """Times the launch configurations on the current particles (after a
+        step) and keeps the fastest for this particle count's size bucket."""
+        t = PsbTune()
+        self._check(lib().psb_autotune(self._h, int(trials), ctypes.byref(t)), "psb_autotune")
+        return t.as_dict()
+
+    def tune_set(self, bucket: int, nbr_block=0, nbr_schedule=0, density_block=0, init_block=0,
+                 pci_density_block=0, force_block=0, xsph_block=0):
+        t = PsbTune(bucket=bucket, nbr_block=nbr_block, nbr_schedule=nbr_schedule, density_block=density_block,
+                    init_block=init_block, pci_density_block=pci_density_block, force_block=force_block,
+                    xsph_block=xsph_block)
+        self._check(lib().psb_tune_set(self._h, ctypes.byref(t)), "psb_tune_set")
+
+    def tune_get(self, bucket: int) -> dict:
+        t = PsbTune()
+        self._check(lib().psb_tune_get(self._h, int(bucket), ctypes.byref(t)), "psb_tune_get")
+        return t.as_dict()
+
+    @staticmethod
+    def size_bucket(n: int) -> int:
+        return int(n).bit_length() - 1
 
     def profile(self, on: bool = True):
         self._check(lib().psb_profile_enable(self._h, 1 if on else 0), "psb_profile_enable")
