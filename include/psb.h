@@ -327,7 +327,9 @@ typedef struct psb_tune {
     double ms_default[6];
 } psb_tune;
 /* Times every candidate `trials` times (CUDA events, after one untimed
- * launch) on the context's current particles -- after at least one step --
+ * launch, each timed launch after a 256 MB write that evicts L2, as in a
+ * step no kernel finds its own data in L2) on the context's current
+ * particles -- after at least one step --
  * and stores the fastest of each kernel for the current bucket; later steps
  * at that bucket use it. The state (positions, velocities, densities,
  * pressures) is left as it was; scratch buffers are recomputed next step.

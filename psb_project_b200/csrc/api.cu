@@ -798,7 +798,7 @@ int create_impl(const psb_scene* scene, size_t ncells, psb_ctx** out) {
     if (!rc) rc = dalloc(c, &c->cell_start, c->ncells);
     if (!rc) rc = dalloc(c, &c->cell_end, c->ncells);
     if (!rc) rc = dalloc(c, &c->nbr_count, n);
-    if (!rc) rc = dalloc(c, &c->nbr_list, n * (size_t)c->cap);
+    if (!rc) rc = dalloc(c, &c->nbr_list, psb::nbr_list_ints(n, c->cap));
     if (!rc) rc = dalloc(c, &c->fnp, n);
     if (!rc) rc = dalloc(c, &c->vs, n);
     if (!rc) rc = dalloc(c, &c->rpc, n);
@@ -1542,15 +1542,26 @@ int psb_autotune(psb_ctx* c, int32_t trials, psb_tune* out) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    // In a step every kernel finds the data its predecessor left in L2, not
+    // its own; back-to-back repeats would favour configurations that reuse a
+    // warm L2. Each timed launch follows a write of 256 MB (twice L2).
+    const size_t flush_bytes = (size_t)256 << 20;
+    void* flush = nullptr;
+    if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) { cudaGetLastError(); flush = nullptr; }
     auto time_it = [&](auto launch) {
         launch();
-        cudaEventRecord(e0, st);
-        for (int i = 0; i < trials; ++i) launch();
-        cudaEventRecord(e1, st);
-        cudaEventSynchronize(e1);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        return (double)ms / trials;
+        double total = 0.0;
+        for (int i = 0; i < trials; ++i) {
+            if (flush) cudaMemsetAsync(flush, i & 0xff, flush_bytes, st);
+            cudaEventRecord(e0, st);
+            launch();
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            total += ms;
+        }
+        return total / trials;
     };
     const int blocks[3] = {128, 256, 512};
     psb_tune best{};
@@ -1615,6 +1626,7 @@ int psb_autotune(psb_ctx* c, int32_t trials, psb_tune* out) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (flush) { cudaStreamSynchronize(st); cudaFree(flush); }
     PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->rp[r], c->stage, sizeof(float2) * n, cudaMemcpyDeviceToDevice, st), "tune"));
     PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "tune"));
     PSB_TRY(cuda_check(c, cudaGetLastError(), "tune"));

@@ -52,16 +52,14 @@ __global__ void __launch_bounds__(kBlock) k_dem_step(Params P, const float4* __r
     const float4 xa = pos[t], va = vel[t];
     float3 f = make_float3(P.gx * P.dem_mass, P.gy * P.dem_mass, P.gz * P.dem_mass);
     const int cnt = min(counts[t], P.cap);
-#pragma unroll 4
-    for (int c = 0; c < cnt; ++c) {
-        const int j = list[(size_t)c * P.n + t];
+    for_each_nbr(list, P.n, t, cnt, [&](const int j) {
         const float4 xb = pos[j];
         const float rx = xb.x - xa.x, ry = xb.y - xa.y, rz = xb.z - xa.z;
         const float d2 = rx * rx + ry * ry + rz * rz;
-        if (!(d2 > 0.f)) continue;
+        if (!(d2 > 0.f)) return;
         const float rinv = rsqrtf(d2);
         const float d = d2 * rinv;
-        if (!(d < P.dem_range)) continue;
+        if (!(d < P.dem_range)) return;
         const float nx = rx * rinv, ny = ry * rinv, nz = rz * rinv;
         if (REF) {
             // -k_s (R - d) n only: the dashpot, shear and attraction lines of
@@ -75,7 +73,7 @@ __global__ void __launch_bounds__(kBlock) k_dem_step(Params P, const float4* __r
             const float s = -P.dem_k * (P.dem_R - d) + P.dem_c * vn;
             f.x += s * nx; f.y += s * ny; f.z += s * nz;
         }
-    }
+    });
     const float im = P.dem_inv_mass;
     float3 v = make_float3(va.x + f.x * im * P.dt, va.y + f.y * im * P.dt, va.z + f.z * im * P.dt);
     const float3 vx = REF ? make_float3(va.x, va.y, va.z) : v;

@@ -208,7 +208,7 @@ __device__ __forceinline__ void ghost_density(const Params& P, int t, float4 xi,
     const auto F = faces_of<BATCH>(P, t);
     const unsigned wall = near_walls(P, F, xi);
     if (!(wall & 3u)) return;
-    for (int c = 0; c < cnt; ++c) ghost_density_pair(P, F, wall, xi, pos[list[(size_t)c * P.n + t]], acc);
+    for_each_nbr(list, P.n, t, cnt, [&](const int j) { ghost_density_pair(P, F, wall, xi, pos[j], acc); });
 }
 
 template <bool BATCH = false>
@@ -218,10 +218,9 @@ __device__ __forceinline__ void ghost_pressure(const Params& P, int t, float4 xi
     const auto F = faces_of<BATCH>(P, t);
     const unsigned wall = near_walls(P, F, xi);
     if (!(wall & 3u)) return;
-    for (int c = 0; c < cnt; ++c) {
-        const int j = list[(size_t)c * P.n + t];
+    for_each_nbr(list, P.n, t, cnt, [&](const int j) {
         ghost_pressure_pair(P, F, wall, xi, pos[j], pVi, pj_of[(size_t)j * pj_stride], ap);
-    }
+    });
 }
 
 // collisionBox (BoxCollision_Kernel.cu:7-34) with restitution 0: clamp into
@@ -285,14 +284,12 @@ __global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __rest
     float3 gr = make_float3(0.f, 0.f, 0.f);
     float4 vi = make_float4(0.f, 0.f, 0.f, 0.f);
     if (FEAT) vi = vel[t];
-#pragma unroll 4
-    for (int c = 0; c < cnt; ++c) {
-        const int j = list[(size_t)c * P.n + t];
+    for_each_nbr(list, P.n, t, cnt, [&](const int j) {
         const float4 xj = pos[j];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float r2 = dx * dx + dy * dy + dz * dz;
         const float q = r2 * P.inv_h2;
-        if (!REF && q >= 1.f) continue;
+        if (!REF && q >= 1.f) return;
         const float w = 1.f - q;
         acc.add(w * w * w);
         if (FEAT && r2 > 0.f) {
@@ -303,7 +300,7 @@ __global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __rest
             gr.x += s * dx; gr.y += s * dy; gr.z += s * dz;
             div += s * ((vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz);
         }
-    }
+    });
     if (!REF) ghost_density<BATCH>(P, t, xi, pos, list, cnt, acc);
     const float drho = density_deviation(P, acc);
     const float rho = P.rho0 + drho;
@@ -358,15 +355,13 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
     const float ir0 = 1.f / (P.rho0 * P.rho0);
     const float pVi = WITH_PRESSURE ? (REF ? rpi.y / (rpi.x * rpi.x) : rpi.y * ir0) : 0.f;
     const int cnt = min(counts[t], P.cap);
-#pragma unroll 4
-    for (int c = 0; c < cnt; ++c) {
-        const int j = list[(size_t)c * P.n + t];
+    for_each_nbr(list, P.n, t, cnt, [&](const int j) {
         const float4 xj = pos[j];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float r2 = dx * dx + dy * dy + dz * dz;
-        if (!(r2 > 0.f)) continue;
+        if (!(r2 > 0.f)) return;
         const float q = r2 * P.inv_h2;
-        if (!REF && q >= 1.f) continue;
+        if (!REF && q >= 1.f) return;
         const float4 vj = vel[j];
         const float2 rpj = rp[j];
         const float rinv = rsqrtf(r2);
@@ -387,7 +382,7 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
             const float sn = t1 * t1 * inv_rj;
             S.nrm.x += dx * sn; S.nrm.y += dy * sn; S.nrm.z += dz * sn;
         }
-    }
+    });
     if (WITH_PRESSURE && !REF)
         ghost_pressure<BATCH>(P, t, xi, pVi, pos, (const float*)rp + 1, 2, list, cnt, S.ap);
     return S;
@@ -481,13 +476,12 @@ __global__ void __launch_bounds__(BS) k_pci_density(Params P, const float4* __re
         Kahan acc;
         float3 T1 = make_float3(0.f, 0.f, 0.f);
         float T2 = 0.f;
-    #pragma unroll 4
-    for (int c = 0; c < cnt; ++c) {
-            const float4 xj = xs[list[(size_t)c * P.n + t]];
+        for_each_nbr(list, P.n, t, cnt, [&](const int j) {
+            const float4 xj = xs[j];
             const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
             const float r2 = dx * dx + dy * dy + dz * dz;
             const float q = r2 * P.inv_h2;
-            if (!REF && q >= 1.f) continue;
+            if (!REF && q >= 1.f) return;
             const float w = 1.f - q;
             acc.add(w * w * w);
             if (REF && r2 > 0.f) {
@@ -498,7 +492,7 @@ __global__ void __launch_bounds__(BS) k_pci_density(Params P, const float4* __re
                 T1.x += s * dx; T1.y += s * dy; T1.z += s * dz;
                 T2 += g * g;
             }
-        }
+        });
         if (!REF) ghost_density<BATCH>(P, t, xi, xs, list, cnt, acc);
         const float drho = density_deviation(P, acc);
         const float rho = P.rho0 + drho;
@@ -561,21 +555,19 @@ __global__ void __launch_bounds__(BS) k_pci_force_predict(Params P, const float4
     const float pVi = REF ? ri.y / (ri.x * ri.x) : ri.y * ir0;
     const int cnt = min(counts[t], P.cap);
     float3 acc = make_float3(0.f, 0.f, 0.f);
-#pragma unroll 4
-    for (int c = 0; c < cnt; ++c) {
-        const int j = list[(size_t)c * P.n + t];
+    for_each_nbr(list, P.n, t, cnt, [&](const int j) {
         const float4 xj = geo[j];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float r2 = dx * dx + dy * dy + dz * dz;
-        if (!(r2 > 0.f)) continue;
-        if (!REF && r2 * P.inv_h2 >= 1.f) continue;
+        if (!(r2 > 0.f)) return;
+        if (!REF && r2 * P.inv_h2 >= 1.f) return;
         const float2 rj = rpc[j];
         const float rinv = rsqrtf(r2);
         const float om = 1.f - r2 * rinv * P.inv_h;
         const float pVj = REF ? rj.y / (rj.x * rj.x) : rj.y * ir0;
         const float s = (pVi + pVj) * om * om * rinv;
         acc.x += s * dx; acc.y += s * dy; acc.z += s * dz;
-    }
+    });
     if (!REF) ghost_pressure<BATCH>(P, t, xi, pVi, geo, (const float*)rpc + 1, 2, list, cnt, acc);
     const float4 x0 = pos[t], vh = vap[t], f = fnp[t];
     const float3 aw = wall_accel<REF, BATCH>(P, t, x0, vh);
@@ -618,17 +610,15 @@ __global__ void __launch_bounds__(BS) k_xsph(Params P, const float4* __restrict_
     const float4 xi = xs[t], vi = vs[t];
     const int cnt = min(counts[t], P.cap);
     float3 dv = make_float3(0.f, 0.f, 0.f);
-#pragma unroll 4
-    for (int c = 0; c < cnt; ++c) {
-        const int j = list[(size_t)c * P.n + t];
+    for_each_nbr(list, P.n, t, cnt, [&](const int j) {
         const float4 xj = xs[j];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float q = (dx * dx + dy * dy + dz * dz) * P.inv_h2;
-        if (q >= 1.f) continue;
+        if (q >= 1.f) return;
         const float4 vj = vs[j];
         const float w = (1.f - q) * (1.f - q) * (1.f - q);
         dv.x += w * (vj.x - vi.x); dv.y += w * (vj.y - vi.y); dv.z += w * (vj.z - vi.z);
-    }
+    });
     vs_out[t] = make_float4(vi.x + P.xsph_k * dv.x, vi.y + P.xsph_k * dv.y, vi.z + P.xsph_k * dv.z, 0.f);
 }
 
