@@ -90,6 +90,9 @@ def parse():
     ap.add_argument("--xsph", type=float, default=None, help="override the scene's XSPH velocity smoothing factor")
     ap.add_argument("--no-graph", action="store_true", help="C3: launch kernel by kernel instead of CUDA graphs")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch configuration)")
+    ap.add_argument("--tune-cache", default=None,
+                    help="JSON cache of tuned launch configurations: a bucket found there is not tuned again; "
+                         "new results are added")
     ap.add_argument("--eval-steps", type=int, default=None,
                     help="steps after the recorded ones over which the warm starts are compared (0: skip)")
     args = ap.parse_args()
@@ -338,9 +341,7 @@ def run_ours(args):
 
     # ---- autotuner (untimed): launch configuration for this size bucket ----------
     if not args.no_tune:
-        restore(sim)
-        sim.step(2)
-        tune = sim.autotune(trials=5)
+        tune = tuned(sim, restore, args)
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
@@ -471,6 +472,25 @@ def run_ours(args):
     rep_.close()
 
 
+def tuned(sim, restore, args) -> dict:
+    """The launch configuration for the simulation's size bucket: from the
+    cache file when it has the bucket, else measured by the autotuner on the
+    restored state (and added to the cache)."""
+    bucket = sim.size_bucket(sim.scene.n)
+    if args.tune_cache and os.path.exists(args.tune_cache):
+        sim.load_tune(args.tune_cache)
+        t = sim.tune_get(bucket)
+        if any(t[k] for k in sim.TUNE_FIELDS):
+            t["source"] = args.tune_cache
+            return t
+    restore(sim)
+    sim.step(2)
+    t = sim.autotune(trials=5)
+    if args.tune_cache:
+        sim.save_tune(args.tune_cache)
+    return t
+
+
 def run_batch(args):
     """Config C3: 64 independent PCISPH dam breaks stepped as one batch
     (psb_create_batch), each step one CUDA-graph launch with the corrector a
@@ -562,9 +582,7 @@ def run_batch(args):
     if weights is not None:
         sim.mlp_set_weights(weights)
     if not args.no_tune:
-        restore(sim)
-        sim.step(2)
-        tune = sim.autotune(trials=5)
+        tune = tuned(sim, restore, args)
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)

@@ -341,6 +341,22 @@ int psb_tune_set(psb_ctx* ctx, const psb_tune* t);
 /* The entry for `bucket` (block sizes 0 when the bucket has none). */
 int psb_tune_get(psb_ctx* ctx, int32_t bucket, psb_tune* out);
 
+/* FP64 diagnostics of the current state: with the corrector's convergence
+ * reduction, the only FP64 arithmetic on the device. Each sum runs in FP64
+ * in a fixed order (per-block partial sums, then one pass over the blocks),
+ * so repeated calls give identical results. No counterpart in the reference.
+ * n_out = 1: over all particles; n_out = the number of scenes of a batch:
+ * one entry per scene. */
+typedef struct psb_diag {
+    double mass;                /* sum m */
+    double momentum[3];         /* sum m v, v the interpolated velocity */
+    double kinetic;             /* sum m |v|^2 / 2 */
+    double potential;           /* sum -m g.x, g the step's gravity */
+    double density_err_mean;    /* mean |rho - rho0| / rho0 over the last density pass */
+    double density_err_max;     /* max of the same */
+} psb_diag;
+int psb_diagnostics(psb_ctx* ctx, psb_diag* out, int32_t n_out);
+
 const char* psb_status_string(int32_t status);
 const char* psb_last_error(const psb_ctx* ctx);
 int32_t psb_abi_version(void);

@@ -148,6 +148,10 @@ struct psb_ctx {
     int* d_loop = nullptr;                        // device loop words (batch.cu)
     int* h_loop = nullptr;                        // pinned mirrors
     unsigned long long* h_err_sh = nullptr;
+    // FP64 diagnostics scratch (grown on demand)
+    double* diag_rows = nullptr;
+    double* diag_out = nullptr;
+    long long diag_rows_cap = 0, diag_out_cap = 0;
     // autotuner: launch configuration per size bucket (floor(log2 n))
     std::map<int, psb_tune> tune_table;
     // CUDA-graph stepping (batches)
@@ -224,6 +228,7 @@ void free_all(psb_ctx* c) {
     cudaFreeHost(c->h_err); cudaFreeHost(c->h_flags);
     cudaFree(c->d_scenes); cudaFree(c->d_slot_scene); cudaFree(c->d_active); cudaFree(c->d_err_scene);
     cudaFree(c->d_err_sh); cudaFree(c->d_loop);
+    cudaFree(c->diag_rows); cudaFree(c->diag_out);
     cudaFreeHost(c->h_loop); cudaFreeHost(c->h_err_sh);
     for (auto& g : c->gexec) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -1341,6 +1346,39 @@ int iso_on_device(psb_ctx* c, const psb_iso_grid* g, double level, psb::IsoParam
 }  // namespace
 
 extern "C" {
+
+int psb_diagnostics(psb_ctx* c, psb_diag* out, int32_t n_out) {
+    if (!c || !out) return PSB_EINVAL;
+    if (n_out != 1 && n_out != c->nscenes) return fail(c, PSB_EINVAL, "psb_diagnostics: n_out is 1 or the scene count");
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_diagnostics before psb_upload");
+    static_assert(sizeof(psb_diag) == sizeof(double) * psb::kDiagTerms, "psb_diag holds the diagnostic terms");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    PSB_TRY(grow(c, &c->diag_rows, &c->diag_rows_cap, (long long)psb::diag_rows(c->n) * psb::kDiagTerms));
+    PSB_TRY(grow(c, &c->diag_out, &c->diag_out_cap, (long long)n_out * psb::kDiagTerms));
+    const float g[3] = {c->P.gx, c->P.gy, c->P.gz};
+    for (int k = 0; k < n_out; ++k) {
+        const int first = n_out == 1 ? 0 : (int)c->first[k];
+        const int count = n_out == 1 ? c->n : (int)(c->first[k + 1] - c->first[k]);
+        psb::launch_diagnostics(st, first, count, c->sc.mass, c->sc.rho0, g, c->pos[c->cs], c->vel[c->cs],
+                                c->rp[c->cr], c->diag_rows, c->diag_out + (size_t)k * psb::kDiagTerms);
+    }
+    std::vector<double> h((size_t)n_out * psb::kDiagTerms);
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(h.data(), c->diag_out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st),
+                       "diagnostics"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "diagnostics"));
+    for (int k = 0; k < n_out; ++k) {
+        const double* r = &h[(size_t)k * psb::kDiagTerms];
+        const double count = n_out == 1 ? (double)c->n : (double)(c->first[k + 1] - c->first[k]);
+        out[k].mass = r[0];
+        out[k].momentum[0] = r[1]; out[k].momentum[1] = r[2]; out[k].momentum[2] = r[3];
+        out[k].kinetic = r[4];
+        out[k].potential = r[5];
+        out[k].density_err_mean = count > 0 ? r[6] / count : 0.0;
+        out[k].density_err_max = r[7];
+    }
+    return cuda_check(c, cudaGetLastError(), "diagnostics");
+}
 
 int psb_iso_field(psb_ctx* c, const psb_iso_grid* g, double* iso) {
     if (!c) return PSB_EINVAL;

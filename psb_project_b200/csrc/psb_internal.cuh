@@ -178,6 +178,13 @@ void launch_batch_decide(cudaStream_t st, int S, int min_it, int max_it, double 
                          unsigned long long* err_scene, unsigned long long* err_hist, int* loop,
                          cudaGraphConditionalHandle handle, int set_handle);
 
+// ---- FP64 diagnostics (diag.cu) -------------------------------------------------
+// terms: mass, momentum x/y/z, kinetic, potential, sum and max of |rho - rho0|/rho0
+constexpr int kDiagTerms = 8;
+int diag_rows(int count);
+void launch_diagnostics(cudaStream_t st, int first, int count, double mass, double rho0, const float g[3],
+                        const float4* pos, const float4* vel, const float2* rp, double* rows, double* out);
+
 // ---- iso field and marching cubes (mc.cu) ----------------------------------------
 constexpr int kMcMaxTri = 10;       // at most 12 active edges in loops of >= 3: 12 - 2 triangles
 struct IsoParams {

@@ -38,7 +38,7 @@ EXPORTS = (
     "psb_last_error", "psb_abi_version", "psb_sort_cells_noalloc", "psb_presolve", "psb_mlp_set_weights",
     "psb_mlp_get_weights", "psb_mlp_collect", "psb_mlp_dataset", "psb_mlp_train", "psb_mlp_forward",
     "psb_mlp_loss_grad", "psb_iso_field", "psb_extract_surface", "psb_create_batch", "psb_batch_layout",
-    "psb_batch_stats", "psb_set_graph", "psb_autotune", "psb_tune_set", "psb_tune_get",
+    "psb_batch_stats", "psb_set_graph", "psb_autotune", "psb_tune_set", "psb_tune_get", "psb_diagnostics",
 )
 MLP_PARAMS = 4673       # PSB_MLP_PARAMS
 MLP_IN, MLP_H = 6, 64
@@ -67,6 +67,18 @@ class PsbTune(ctypes.Structure):
         d["ms"] = dict(zip(self.KERNELS, list(self.ms)))
         d["ms_default"] = dict(zip(self.KERNELS, list(self.ms_default)))
         return d
+
+
+class PsbDiag(ctypes.Structure):
+    """psb_diag: FP64 mass, momentum and energy of the current state."""
+    _fields_ = [("mass", ctypes.c_double), ("momentum", ctypes.c_double * 3), ("kinetic", ctypes.c_double),
+                ("potential", ctypes.c_double), ("density_err_mean", ctypes.c_double),
+                ("density_err_max", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {"mass": self.mass, "momentum": list(self.momentum), "kinetic": self.kinetic,
+                "potential": self.potential, "density_err_mean": self.density_err_mean,
+                "density_err_max": self.density_err_max}
 
 
 class IsoGrid(ctypes.Structure):
@@ -144,6 +156,7 @@ def lib():
         "psb_autotune": ([P, I32, ctypes.POINTER(PsbTune)], ctypes.c_int),
         "psb_tune_set": ([P, ctypes.POINTER(PsbTune)], ctypes.c_int),
         "psb_tune_get": ([P, I32, ctypes.POINTER(PsbTune)], ctypes.c_int),
+        "psb_diagnostics": ([P, ctypes.POINTER(PsbDiag), I32], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -374,6 +387,16 @@ class Simulation:
         self._check(lib().psb_get_stats(self._h, ctypes.byref(s)), "psb_get_stats")
         return s
 
+    # -- diagnostics -------------------------------------------------------------
+    def diagnostics(self, per_scene: bool = False):
+        """FP64 mass, momentum, energies and density-error statistics (a list
+        with one dict per scene when per_scene, else one dict)."""
+        k = len(getattr(self, "scenes", [None])) if per_scene else 1
+        arr = (PsbDiag * k)()
+        self._check(lib().psb_diagnostics(self._h, arr, k), "psb_diagnostics")
+        out = [d.as_dict() for d in arr]
+        return out if per_scene else out[0]
+
     # -- autotuner ---------------------------------------------------------------
     def autotune(self, trials: int = 5) -> dict:
         """Times the launch configurations on the current particles (after a
@@ -397,6 +420,33 @@ class Simulation:
     @staticmethod
     def size_bucket(n: int) -> int:
         return int(n).bit_length() - 1
+
+    TUNE_FIELDS = ("nbr_block", "nbr_schedule", "density_block", "init_block", "pci_density_block", "force_block",
+                   "xsph_block")
+
+    def save_tune(self, path: str):
+        """Merges this context's tuned buckets into the JSON cache at `path`
+        ({bucket: {field: value}}), keeping the other buckets' entries."""
+        import json
+        table = {}
+        if os.path.exists(path):
+            with open(path) as f:
+                table = json.load(f)
+        for b in range(63):
+            t = self.tune_get(b)
+            if any(t[k] for k in self.TUNE_FIELDS):
+                table[str(b)] = {k: int(t[k]) for k in self.TUNE_FIELDS}
+        with open(path, "w") as f:
+            json.dump(table, f, indent=1, sort_keys=True)
+
+    def load_tune(self, path: str) -> int:
+        """Installs every bucket of the JSON cache at `path`; returns how many."""
+        import json
+        with open(path) as f:
+            table = json.load(f)
+        for b, e in table.items():
+            self.tune_set(int(b), **{k: int(e.get(k, 0)) for k in self.TUNE_FIELDS})
+        return len(table)
 
     def profile(self, on: bool = True):
         self._check(lib().psb_profile_enable(self._h, 1 if on else 0), "psb_profile_enable")

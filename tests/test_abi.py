@@ -39,16 +39,18 @@ def test_every_declared_symbol_is_exported():
 def test_struct_layout_matches_header(tmp_path):
     c = tmp_path / "layout.c"
     c.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "psb.h"\n'
-                 'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(psb_scene), offsetof(psb_scene, spacing),'
+                 'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(psb_scene), offsetof(psb_scene, spacing),'
                  ' sizeof(psb_step_stats), offsetof(psb_step_stats, iters_total), offsetof(psb_scene, dem_attraction),'
-                 ' sizeof(psb_iso_grid), offsetof(psb_iso_grid, scale), sizeof(psb_tune), offsetof(psb_tune, ms));'
+                 ' sizeof(psb_iso_grid), offsetof(psb_iso_grid, scale), sizeof(psb_tune), offsetof(psb_tune, ms),'
+                 ' sizeof(psb_diag), offsetof(psb_diag, density_err_max));'
                  ' return 0;}\n')
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(c), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     assert got == [ctypes.sizeof(PsbScene), PsbScene.spacing.offset, ctypes.sizeof(R.PsbStepStats),
                    R.PsbStepStats.iters_total.offset, PsbScene.dem_attraction.offset, ctypes.sizeof(R.IsoGrid),
-                   R.IsoGrid.scale.offset, ctypes.sizeof(R.PsbTune), R.PsbTune.ms.offset]
+                   R.IsoGrid.scale.offset, ctypes.sizeof(R.PsbTune), R.PsbTune.ms.offset,
+                   ctypes.sizeof(R.PsbDiag), R.PsbDiag.density_err_max.offset]
 
 
 def test_abi_version_and_status_strings():

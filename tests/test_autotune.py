@@ -113,3 +113,20 @@ def test_autotune_keeps_state_and_stores_choice():
         got = sim.download()
     for k in ("pos", "vel", "pressure"):
         assert np.array_equal(got[k], ref[k]), k
+
+
+@pytest.mark.gpu
+def test_tune_cache_round_trip(tmp_path):
+    sc = P.dam_break((10, 10, 8), 0.01, (0.3, 0.3, 0.3), 0.02, dt=5e-4, seed=25)
+    path = str(tmp_path / "tune.json")
+    b = Simulation.size_bucket(sc.n)
+    with P.Simulation(sc) as a:
+        a.tune_set(b, **CONFIGS[3])
+        a.tune_set(b + 3, **CONFIGS[0])
+        a.save_tune(path)
+    with P.Simulation(sc) as c:
+        assert c.load_tune(path) == 2
+        for bucket, cfg in ((b, CONFIGS[3]), (b + 3, CONFIGS[0])):
+            got = c.tune_get(bucket)
+            for k in Simulation.TUNE_FIELDS:
+                assert got[k] == cfg.get(k, 0), (bucket, k)
