@@ -96,11 +96,11 @@ def parse():
     ap.add_argument("--eval-steps", type=int, default=None,
                     help="steps after the recorded ones over which the warm starts are compared (0: skip)")
     args = ap.parse_args()
-    c3 = args.scene == "C3"
+    short = args.scene in ("C3", "C4")
     if args.train_steps is None:
-        args.train_steps = 100 if c3 else 400
+        args.train_steps = 100 if short else 400
     if args.eval_steps is None:
-        args.eval_steps = 300 if c3 else 1000   # C3: 300 steps of every scene
+        args.eval_steps = 300 if short else 1000   # C3, C4: 300 steps
     return args
 
 
@@ -673,12 +673,155 @@ def run_batch(args):
     rep_.close()
 
 
+C4_SPHERE = ((1.5, 0.21, 0.5), 0.2)     # centre (m), radius (m): in the path of the collapsing block
+
+
+def run_c4(args):
+    """Config C4: the 4,194,304-particle PCISPH dam break (eta 0.5 %) around a
+    static 0.2 m sphere sampled as boundary particles, learned warm start,
+    with the density colour field's iso-0.5 surface extracted on a 256^3
+    node grid every 10 steps (marching cubes on the GPU, the mesh copied to
+    the host). `value` counts particle-steps over the wall time of steps and
+    extractions together. Multi-GPU: replicas with their own seeds."""
+    import torch
+    import psb_project_b200 as P
+    from psb_project_b200 import replicas
+
+    rep_ = replicas.init("nccl")
+    rank, world, local = rep_.rank, rep_.world, rep_.local
+    torch.cuda.set_device(local)
+    modes = {"zero": P.WARM_ZERO, "previous": P.WARM_PREVIOUS, "learned": P.WARM_LEARNED}
+    base = P.config_scene("C4")
+    if world > 1:
+        base.blocks[0].seed = rep_.seed(base.blocks[0].seed)
+    sc = base.replace(warm_start=modes[args.warm_start])
+    n = sc.n
+    centre, radius = C4_SPHERE
+    bnd = P.sphere_shell(centre, radius, sc.spacing)
+    grid = P.iso_grid((0.0, 0.0, 0.0), tuple(b / 255.0 for b in sc.box_max), (256, 256, 256))
+    stream = torch.cuda.current_stream()
+    max_over_ranks = rep_.max_over_ranks
+    tune = None
+
+    def barrier():
+        rep_.barrier()
+        torch.cuda.synchronize()
+
+    def make(mode):
+        s_ = P.Simulation(base.replace(warm_start=mode))
+        s_.set_stream(stream.cuda_stream)
+        s_.set_boundary(bnd)
+        if tune is not None:
+            s_.tune_set(**{k: tune[k] for k in TUNE_KEYS})
+        return s_
+
+    gen = make(P.WARM_ZERO)
+    gen.upload(P.scene_positions(sc))
+    gen.presolve(args.presolve)
+    train_info, weights = None, None
+    if args.warm_start == "learned":
+        t0 = time.perf_counter()
+        gen.mlp_collect(stride=64, capacity=(args.train_steps + 1) * ((n + 63) // 64))
+        gen.step(args.train_steps)
+        gen.mlp_collect(0)
+        rows, _, _ = gen.mlp_dataset(fetch=False)
+        t1 = time.perf_counter()
+        gen.mlp_set_weights(P.mlp_init_weights(rank))
+        loss0 = gen.mlp_train(1, args.train_batch, 1e-3, seed=11)
+        loss = gen.mlp_fit(args.train_iters, args.train_batch, args.train_lr, chunks=10, seed=12)
+        weights = gen.mlp_get_weights()
+        train_info = {"recorded_steps": args.train_steps, "rows": int(rows), "adam_steps": args.train_iters // 10 * 10 + 1,
+                      "batch": args.train_batch, "lr": args.train_lr, "loss_first": loss0, "loss_last": loss,
+                      "record_s": round(t1 - t0, 2), "train_s": round(time.perf_counter() - t1, 2)}
+    gen.step(args.warmup)
+    snap = gen.download()
+    gen.close()
+    start = (args.train_steps if train_info else 0) + args.warmup + 1
+
+    def restore(s_):
+        s_.upload(snap["pos"], snap["vel"], snap["vel_half"], snap["pressure"])
+
+    sim = make(modes[args.warm_start])
+    if weights is not None:
+        sim.mlp_set_weights(weights)
+    if not args.no_tune:
+        tune = tuned(sim, restore, args)
+    vert = np.empty((16 << 20, 3), np.float32)
+    tri = np.empty((32 << 20, 3), np.int32)
+
+    def timed_run(s_, steps, mc_every):
+        restore(s_)
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        its, mesh = [], (0, 0)
+        e0.record(stream)
+        for k in range(steps):
+            s_.step(1)
+            its.append(s_.stats().iters)
+            if mc_every and (k + 1) % mc_every == 0:
+                mesh = s_.extract_surface_into(grid, 0.5, vert, tri)
+        e1.record(stream)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1)), np.asarray(its), mesh
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ms, its, mesh = timed_run(sim, args.steps, 10)
+    value = world * n * args.steps / (ms / 1e3)
+    ms_nomc, _, _ = timed_run(sim, args.steps, 0)
+    clk = clocks.stop()
+    diag = sim.diagnostics()
+    comparison = {}
+    if args.eval_steps > 0 and weights is not None:
+        comparison["steps"] = "%d..%d" % (start, start + args.eval_steps - 1)
+        for name, mode in (("learned", P.WARM_LEARNED), ("zero", P.WARM_ZERO)):
+            b = sim if mode == modes[args.warm_start] else make(mode)
+            if weights is not None:
+                b.mlp_set_weights(weights)
+            m_, it_, _ = timed_run(b, args.eval_steps, 0)
+            comparison[name] = {"iters_mean": float(it_.mean()), "iters_p50": float(np.median(it_)),
+                                "not_converged_steps": int(np.sum(it_ >= sc.max_iters)),
+                                "ms_per_step": m_ / args.eval_steps}
+            if b is not sim:
+                b.close()
+        z, l_ = comparison["zero"], comparison["learned"]
+        z["iters_ratio_over_learned"] = z["iters_mean"] / max(l_["iters_mean"], 1e-9)
+        z["time_ratio_over_learned"] = z["ms_per_step"] / l_["ms_per_step"]
+    sim.close()
+    if rank == 0:
+        mc_ms = (ms - ms_nomc) / max(1, args.steps // 10)
+        out = {
+            "metric": "particle-steps/s, 4M-particle PCISPH dam break with a sphere obstacle and MC every 10 steps (C4)",
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": sc.name + " + 0.2 m sphere obstacle + MC 256^3 every 10 steps", "particles": n,
+                       "boundary_particles": int(bnd.shape[0]), "sphere": {"centre": centre, "radius": radius},
+                       "eta": sc.eta, "warm_start": args.warm_start, "dt": sc.dt, "h": sc.h,
+                       "timed_steps": "steps %d..%d" % (start, start + args.steps - 1),
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "iters_per_step": {"mean": float(its.mean()), "p50": float(np.median(its)), "max": int(its.max())},
+            "mc": {"grid": [256, 256, 256], "level": 0.5, "ms_per_extraction": mc_ms, "vertices": int(mesh[0]),
+                   "triangles": int(mesh[1])},
+            "ms_per_step_without_mc": ms_nomc / args.steps,
+            "diagnostics_fp64": diag,
+            "comparison": comparison, "learned_training": train_info, "autotune": tune,
+            "clocks": clk,
+        }
+        print(json.dumps(out))
+    rep_.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.scene == "C3":
         run_batch(args)
+    elif args.scene == "C4":
+        run_c4(args)
     else:
         run_ours(args)
 

@@ -341,6 +341,19 @@ int psb_tune_set(psb_ctx* ctx, const psb_tune* t);
 /* The entry for `bucket` (block sizes 0 when the bucket has none). */
 int psb_tune_get(psb_ctx* ctx, int32_t bucket, psb_tune* out);
 
+/* Static boundary particles (CONFIG profile, single-scene SPH contexts),
+ * after Akinci et al. 2012: a solid obstacle sampled by n_bnd particles
+ * (pos: n_bnd x 3 floats, inside the grid). Each gets psi_b = rho0 /
+ * sum_k W(x_b - x_k) over the boundary particles; a fluid particle gains
+ * psi_b W in its density and psi_b p_i/rho0^2 gradW in its pressure force
+ * (its own pressure mirrored onto the solid); free slip. Sample a solid at
+ * least h thick (e.g. a shell of two lattice spacings). Replaces any earlier
+ * set; n_bnd = 0 removes it. No counterpart in the reference, whose
+ * obstacles are analytic collision objects (src/Kernel/Collision). */
+int psb_set_boundary(psb_ctx* ctx, int32_t n_bnd, const float* pos);
+/* psi_b (kg) of the current boundary set, in the order it was given. */
+int psb_boundary_psi(psb_ctx* ctx, float* psi);
+
 /* FP64 diagnostics of the current state: with the corrector's convergence
  * reduction, the only FP64 arithmetic on the device. Each sum runs in FP64
  * in a fixed order (per-block partial sums, then one pass over the blocks),

@@ -47,6 +47,8 @@ class OrcParams(ctypes.Structure):
         ("skin", ctypes.c_double), ("xsph", ctypes.c_double),
         ("dem_spring", ctypes.c_double), ("dem_damping", ctypes.c_double), ("dem_shear", ctypes.c_double),
         ("dem_attraction", ctypes.c_double),
+        ("n_bnd", ctypes.c_int32), ("bnd_pos", ctypes.c_void_p), ("bnd_psi", ctypes.c_void_p),
+        ("bnd_counts", ctypes.c_void_p), ("bnd_lists", ctypes.c_void_p), ("bnd_cap", ctypes.c_int32),
     ]
 
 
@@ -166,6 +168,10 @@ def lib():
         L.orc_marching_cubes.argtypes = [ctypes.POINTER(IsoGrid), P, ctypes.c_double, ctypes.c_int64, P, P,
                                          ctypes.c_int64, P, P]
         L.orc_marching_cubes.restype = ctypes.c_int
+        L.orc_boundary_psi.argtypes = [ctypes.POINTER(OrcParams), ctypes.c_int32, P, P]
+        L.orc_boundary_psi.restype = None
+        L.orc_pressure_force.argtypes = [ctypes.POINTER(OrcParams), P, P, P, P, P, ctypes.c_int32, P]
+        L.orc_pressure_force.restype = None
         _lib = L
     return _lib
 
@@ -241,6 +247,15 @@ def params(scene, *, float_state: bool = False, n: Optional[int] = None) -> OrcP
     return p
 
 
+def boundary_psi(scene, bpos) -> np.ndarray:
+    """Akinci volumes psi_b (kg) of a boundary sampling."""
+    bpos = np.ascontiguousarray(bpos, np.float64)
+    psi = np.empty(bpos.shape[0])
+    P = params(scene)
+    lib().orc_boundary_psi(ctypes.byref(P), bpos.shape[0], _ptr(bpos), _ptr(psi))
+    return psi
+
+
 def pci_delta(scene) -> float:
     P = params(scene)
     return lib().orc_pci_delta(ctypes.byref(P))
@@ -291,10 +306,16 @@ def density(scene, pos, counts, lists, clamp) -> np.ndarray:
 class OracleSim:
     """FP64 state in particle-id order, stepped by orc_step."""
 
-    def __init__(self, scene, pos, vel=None, vel_half=None, pressure=None, *, float_state=False):
+    def __init__(self, scene, pos, vel=None, vel_half=None, pressure=None, *, float_state=False, boundary=None):
         n = pos.shape[0]
         self.scene = scene
         self.P = params(scene, float_state=float_state, n=n)
+        if boundary is not None:      # static boundary particles (config profile)
+            self.bnd_pos = np.ascontiguousarray(boundary, np.float64)
+            self.bnd_psi = boundary_psi(scene, self.bnd_pos)
+            self.P.n_bnd = self.bnd_pos.shape[0]
+            self.P.bnd_pos = self.bnd_pos.ctypes.data
+            self.P.bnd_psi = self.bnd_psi.ctypes.data
         self.pos = np.ascontiguousarray(pos, np.float64).copy()
         self.vel = np.zeros((n, 3)) if vel is None else np.ascontiguousarray(vel, np.float64).copy()
         self.vel_half = np.zeros((n, 3)) if vel_half is None else np.ascontiguousarray(vel_half, np.float64).copy()

@@ -213,6 +213,86 @@ static int ghost(const orc_params* P, const walls_t* w, int mask, const double* 
     return 1;
 }
 
+/* ---- config-profile boundary particles (Akinci et al. 2012) ----------------
+ * A solid is sampled by particles b of volume psi_b / rho0, with psi_b =
+ * rho0 / sum_k W_bk over the boundary particles (eq. 5), so that a sparse or
+ * thin sampling still contributes a full kernel's worth of density. A fluid
+ * particle i gains sum_b psi_b W_ib in density (eq. 6) and the pressure force
+ * -m_i sum_b psi_b (p_i/rho0^2) gradW_ib (eq. 10 with the config profile's
+ * rho0 in place of rho_i): the fluid's own pressure mirrored onto the solid.
+ * Free slip: no viscous term. Brute force over all b: test sizes only. */
+static inline double poly6(double h, double d) { return (315 / (64 * PI_D * pow(h, 9))) * pow((h * h) - (d * d), 3); }
+
+void orc_boundary_psi(const orc_params* P, int32_t nb, const double* bpos, double* psi) {
+    const double h = P->h;
+#pragma omp parallel for schedule(static)
+    for (int32_t b = 0; b < nb; ++b) {
+        double s = 0.0;
+        for (int32_t k = 0; k < nb; ++k) {
+            const double dv[3] = {bpos[3 * b] - bpos[3 * k], bpos[3 * b + 1] - bpos[3 * k + 1],
+                                  bpos[3 * b + 2] - bpos[3 * k + 2]};
+            const double d = len3(dv);
+            if (d < h) s += poly6(h, d);
+        }
+        psi[b] = P->rho0 / s;
+    }
+}
+
+/* The boundary particles particle i interacts with: its list, built at the
+ * step's start positions within the list cut-off (as the fluid lists are),
+ * or all of them when no lists are set. */
+static inline int32_t bnd_count(const orc_params* P, int32_t i) {
+    return P->bnd_counts ? P->bnd_counts[i] : P->n_bnd;
+}
+static inline int32_t bnd_at(const orc_params* P, int32_t i, int32_t t) {
+    return P->bnd_counts ? P->bnd_lists[(size_t)i * P->bnd_cap + t] : t;
+}
+
+static double boundary_density(const orc_params* P, int32_t i, const double* x) {
+    double s = 0.0;
+    for (int32_t t = 0; t < bnd_count(P, i); ++t) {
+        const int32_t b = bnd_at(P, i, t);
+        const double dv[3] = {x[0] - P->bnd_pos[3 * b], x[1] - P->bnd_pos[3 * b + 1], x[2] - P->bnd_pos[3 * b + 2]};
+        const double d = len3(dv);
+        if (d < P->h) s += poly6(P->h, d) * P->bnd_psi[b];
+    }
+    return s;
+}
+
+/* Boundary lists at pos: every boundary particle within the list cut-off
+ * (1 + skin) h, inclusive, in index order. */
+static void build_bnd_lists(const orc_params* P, const double* pos, int32_t** counts_out, int32_t** lists_out,
+                            int32_t* cap_out) {
+    const int32_t n = P->n;
+    const double hl = P->profile == ORC_PROFILE_CONFIG ? P->h * (1.0 + P->skin) : P->h;
+    int32_t* counts = (int32_t*)calloc((size_t)n, sizeof(int32_t));
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+        int32_t c = 0;
+        for (int32_t b = 0; b < P->n_bnd; ++b) {
+            const double dv[3] = {pos[3 * i] - P->bnd_pos[3 * b], pos[3 * i + 1] - P->bnd_pos[3 * b + 1],
+                                  pos[3 * i + 2] - P->bnd_pos[3 * b + 2]};
+            if (len3(dv) <= hl) ++c;
+        }
+        counts[i] = c;
+    }
+    int32_t cap = 1;
+    for (int32_t i = 0; i < n; ++i) cap = counts[i] > cap ? counts[i] : cap;
+    int32_t* lists = (int32_t*)malloc(sizeof(int32_t) * (size_t)n * (size_t)cap);
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+        int32_t c = 0;
+        for (int32_t b = 0; b < P->n_bnd; ++b) {
+            const double dv[3] = {pos[3 * i] - P->bnd_pos[3 * b], pos[3 * i + 1] - P->bnd_pos[3 * b + 1],
+                                  pos[3 * i + 2] - P->bnd_pos[3 * b + 2]};
+            if (len3(dv) <= hl) lists[(size_t)i * cap + c++] = b;
+        }
+    }
+    *counts_out = counts;
+    *lists_out = lists;
+    *cap_out = cap;
+}
+
 /* Poly6 density term; reference form of compute_Density_PCI (PciSphSystem_Kernel.cu:79-81). */
 void orc_density(const orc_params* P, const double* pos, const int32_t* counts, const int32_t* list, int32_t cap,
                  int clamp, double* rho) {
@@ -239,6 +319,7 @@ void orc_density(const orc_params* P, const double* pos, const int32_t* counts, 
                     if (d >= h) continue;
                     s += (315 / (64 * PI_D * pow(h, 9))) * pow((h * h) - (d * d), 3) * m;
                 }
+            if (P->n_bnd > 0) s += boundary_density(P, i, &pos[3 * i]);
         }
         rho[i] = RND(P, s);
     }
@@ -341,9 +422,25 @@ static void pressure_forces(const orc_params* P, const double* pos, const double
                     const double sc = -45 * pow(h - d, 2) / a;
                     for (int e = 0; e < 3; ++e) acc[e] = acc[e] + (dv[e] * inv) * sc * (pV1 + pV2) * m;
                 }
+            for (int32_t tb = 0; tb < bnd_count(P, i); ++tb) {     /* boundary particles: p_i mirrored */
+                const int32_t b = bnd_at(P, i, tb);
+                const double dv[3] = {pos[3 * i] - P->bnd_pos[3 * b], pos[3 * i + 1] - P->bnd_pos[3 * b + 1],
+                                      pos[3 * i + 2] - P->bnd_pos[3 * b + 2]};
+                const double d = len3(dv);
+                if (!(d > 0) || d >= h) continue;
+                const double inv = 1.0 / d;
+                const double a = PI_D * pow(h, 6);
+                const double sc = -45 * pow(h - d, 2) / a;
+                for (int e = 0; e < 3; ++e) acc[e] = acc[e] + (dv[e] * inv) * sc * pV1 * P->bnd_psi[b];
+            }
         }
         for (int e = 0; e < 3; ++e) fp[3 * i + e] = acc[e] * (-rho[i]);
     }
+}
+
+void orc_pressure_force(const orc_params* P, const double* pos, const double* rho, const double* p,
+                        const int32_t* counts, const int32_t* list, int32_t cap, double* fp) {
+    pressure_forces(P, pos, rho, p, counts, list, cap, fp);
 }
 
 double orc_pci_delta(const orc_params* P) {
@@ -477,6 +574,16 @@ static int step_wcsph(const orc_params* P, orc_state* S, orc_stats* st, double* 
     int32_t* counts = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
     int32_t cap = 0;
     int32_t* list = build_lists(P, S->pos, counts, &cap, st);
+    /* boundary particles: lists at the start positions, like the fluid's */
+    orc_params Qb;
+    int32_t *bnd_counts = NULL, *bnd_lists = NULL;
+    if (P->n_bnd > 0) {
+        Qb = *P;
+        build_bnd_lists(P, S->pos, &bnd_counts, &bnd_lists, &Qb.bnd_cap);
+        Qb.bnd_counts = bnd_counts;
+        Qb.bnd_lists = bnd_lists;
+        P = &Qb;
+    }
     double* rho = S->rho;
     double* p = S->p;
     double* fnp = (double*)malloc(sizeof(double) * 3 * (size_t)n);
@@ -536,6 +643,8 @@ static int step_wcsph(const orc_params* P, orc_state* S, orc_stats* st, double* 
     if (nbr_counts) memcpy(nbr_counts, counts, sizeof(int32_t) * (size_t)n);
     if (st) { st->iters = 0; st->converged = 1; }
     free(counts); free(list); free(fnp); free(fp);
+    free(bnd_counts);
+    free(bnd_lists);
     return 0;
 }
 
@@ -546,6 +655,16 @@ static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double*
     int32_t* counts = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
     int32_t cap = 0;
     int32_t* list = build_lists(P, S->pos, counts, &cap, st);
+    /* boundary particles: lists at the start positions, like the fluid's */
+    orc_params Qb;
+    int32_t *bnd_counts = NULL, *bnd_lists = NULL;
+    if (P->n_bnd > 0) {
+        Qb = *P;
+        build_bnd_lists(P, S->pos, &bnd_counts, &bnd_lists, &Qb.bnd_cap);
+        Qb.bnd_counts = bnd_counts;
+        Qb.bnd_lists = bnd_lists;
+        P = &Qb;
+    }
     const size_t n3 = 3 * (size_t)n;
     double* rho = (double*)malloc(sizeof(double) * (size_t)n);
     double* fnp = (double*)malloc(sizeof(double) * n3);
@@ -640,6 +759,8 @@ static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double*
     if (nbr_counts) memcpy(nbr_counts, counts, sizeof(int32_t) * (size_t)n);
     if (st) { st->iters = k; st->converged = ref ? 1 : converged; }
     free(counts); free(list); free(rho); free(fnp); free(fp); free(xs); free(vs); free(aw);
+    free(bnd_counts);
+    free(bnd_lists);
     return 0;
 }
 

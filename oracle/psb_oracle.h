@@ -40,7 +40,26 @@ typedef struct orc_params {
     double skin;                    /* config: lists hold pairs within (1 + skin) h */
     double xsph;                    /* config PCISPH: XSPH velocity smoothing factor */
     double dem_spring, dem_damping, dem_shear, dem_attraction;   /* DEM contact law */
+    /* config profile: static boundary particles (Akinci et al. 2012) and
+     * their volumes psi_b (kg; orc_boundary_psi); n_bnd = 0: none */
+    int32_t n_bnd;
+    const double* bnd_pos;      /* n_bnd * 3 */
+    const double* bnd_psi;      /* n_bnd */
+    /* set by the step functions: each particle's boundary neighbours at the
+     * step's start positions (n x bnd_cap); NULL: every boundary particle */
+    const int32_t* bnd_counts;
+    const int32_t* bnd_lists;
+    int32_t bnd_cap;
 } orc_params;
+
+/* psi_b = rho0 / sum_k W(x_b - x_k) over the boundary particles within h
+ * (self included), W the poly6 kernel (Akinci et al. 2012, eq. 5). */
+void orc_boundary_psi(const orc_params* P, int32_t nb, const double* bpos, double* psi);
+
+/* Pressure force density (n x 3) at pos with the given densities and
+ * pressures, over the lists (n x cap), walls and boundary particles. */
+void orc_pressure_force(const orc_params* P, const double* pos, const double* rho, const double* p,
+                        const int32_t* counts, const int32_t* list, int32_t cap, double* fp);
 
 /* Config-profile PCISPH pressure factor delta = 1 / (beta (|sum gradW|^2 +
  * sum |gradW|^2)) over the neighbours of a particle in a filled cubic

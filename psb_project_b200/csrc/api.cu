@@ -148,6 +148,22 @@ struct psb_ctx {
     int* d_loop = nullptr;                        // device loop words (batch.cu)
     int* h_loop = nullptr;                        // pinned mirrors
     unsigned long long* h_err_sh = nullptr;
+    // static boundary particles (psb_set_boundary); bnd_n == 0: none
+    int bnd_n = 0, bnd_res = 0;
+    static constexpr int kBndCap = 64;
+    float4* bnd_raw = nullptr;
+    float4* bnd_sorted = nullptr;
+    int* bnd_ids = nullptr;
+    int* bnd_iota = nullptr;
+    float* bnd_w = nullptr;
+    uint32_t* bnd_keys[2] = {};
+    uint32_t* bnd_vals[2] = {};
+    uint32_t* bnd_hist = nullptr;
+    uint32_t* bnd_cs = nullptr;     // boundary cell ranges over the grid
+    uint32_t* bnd_ce = nullptr;
+    int* bnd_count = nullptr;       // per fluid slot
+    int* bnd_list = nullptr;
+    long long bnd_cap_alloc = 0;
     // FP64 diagnostics scratch (grown on demand)
     double* diag_rows = nullptr;
     double* diag_out = nullptr;
@@ -229,6 +245,9 @@ void free_all(psb_ctx* c) {
     cudaFree(c->d_scenes); cudaFree(c->d_slot_scene); cudaFree(c->d_active); cudaFree(c->d_err_scene);
     cudaFree(c->d_err_sh); cudaFree(c->d_loop);
     cudaFree(c->diag_rows); cudaFree(c->diag_out);
+    cudaFree(c->bnd_raw); cudaFree(c->bnd_sorted); cudaFree(c->bnd_ids); cudaFree(c->bnd_iota); cudaFree(c->bnd_w);
+    for (int i = 0; i < 2; ++i) { cudaFree(c->bnd_keys[i]); cudaFree(c->bnd_vals[i]); }
+    cudaFree(c->bnd_hist); cudaFree(c->bnd_cs); cudaFree(c->bnd_ce); cudaFree(c->bnd_count); cudaFree(c->bnd_list);
     cudaFreeHost(c->h_loop); cudaFreeHost(c->h_err_sh);
     for (auto& g : c->gexec) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -440,6 +459,11 @@ int build(psb_ctx* c, bool keep_p = false, bool features = false) {
         psb::launch_build_nbr(st, P, c->pos[c->cs], c->keys[res], c->cell_start, c->cell_end, c->nbr_count, c->nbr_list,
                               c->flags);
     });
+    if (c->bnd_n > 0)
+        timed(c, "build_bnd_nbr", [&] {
+            psb::launch_build_bnd_nbr(st, P, c->pos[c->cs], c->keys[res], c->bnd_cs, c->bnd_ce, c->bnd_count,
+                                      c->bnd_list, c->flags);
+        });
     if (!P.dem) {
         const int zero_p = !keep_p && P.pci && (P.ref || c->sc.warm_start == PSB_WARM_ZERO);
         // the learned warm start and its data collection take their inputs from this pass
@@ -1346,6 +1370,96 @@ int iso_on_device(psb_ctx* c, const psb_iso_grid* g, double level, psb::IsoParam
 }  // namespace
 
 extern "C" {
+
+int psb_set_boundary(psb_ctx* c, int32_t n_bnd, const float* pos) {
+    if (!c || n_bnd < 0 || (n_bnd > 0 && !pos)) return fail(c, PSB_EINVAL, "psb_set_boundary: bad argument");
+    if (n_bnd > 0 && (c->P.ref || c->P.dem || c->batch))
+        return fail(c, PSB_EINVAL, "psb_set_boundary: config-profile SPH, single-scene contexts only");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    release_graphs(c);
+    if (c->bnd_n > 0) {      // forget the previous set: clear its cells
+        psb::launch_reset_cells(st, c->bnd_n, c->bnd_keys[c->bnd_res], c->bnd_cs);
+        c->bnd_n = 0;
+    }
+    c->P.bnd = nullptr;
+    c->P.bnd_count = nullptr;
+    c->P.bnd_list = nullptr;
+    if (n_bnd == 0) return cuda_check(c, cudaGetLastError(), "psb_set_boundary");
+    const size_t nb = (size_t)n_bnd;
+    if (!c->bnd_cs) {
+        PSB_TRY(dalloc(c, &c->bnd_cs, c->ncells));
+        PSB_TRY(dalloc(c, &c->bnd_ce, c->ncells));
+        PSB_TRY(cuda_check(c, cudaMemset(c->bnd_cs, 0xFF, sizeof(uint32_t) * c->ncells), "boundary"));
+        PSB_TRY(dalloc(c, &c->bnd_count, (size_t)c->n_max));
+        PSB_TRY(dalloc(c, &c->bnd_list, psb::nbr_list_ints((size_t)c->n_max, psb_ctx::kBndCap)));
+    }
+    if ((long long)nb > c->bnd_cap_alloc) {
+        cudaStreamSynchronize(st);
+        cudaFree(c->bnd_raw); cudaFree(c->bnd_sorted); cudaFree(c->bnd_ids); cudaFree(c->bnd_iota); cudaFree(c->bnd_w);
+        for (int i = 0; i < 2; ++i) { cudaFree(c->bnd_keys[i]); cudaFree(c->bnd_vals[i]); }
+        cudaFree(c->bnd_hist);
+        c->bnd_cap_alloc = 0;
+        PSB_TRY(dalloc(c, &c->bnd_raw, nb));
+        PSB_TRY(dalloc(c, &c->bnd_sorted, nb));
+        PSB_TRY(dalloc(c, &c->bnd_ids, nb));
+        PSB_TRY(dalloc(c, &c->bnd_iota, nb));
+        PSB_TRY(dalloc(c, &c->bnd_w, nb));
+        for (int i = 0; i < 2; ++i) {
+            PSB_TRY(dalloc(c, &c->bnd_keys[i], nb));
+            PSB_TRY(dalloc(c, &c->bnd_vals[i], nb));
+        }
+        PSB_TRY(dalloc(c, &c->bnd_hist, (size_t)256 * psb::radix_blocks((int)nb) + 256));
+        c->bnd_cap_alloc = (long long)nb;
+    }
+    // positions through the staging buffer (n_max x 32 B), in chunks
+    float* stage = (float*)c->stage;
+    const size_t chunk = ((size_t)c->n_max * 32) / (3 * sizeof(float));
+    for (size_t off = 0; off < nb; off += chunk) {
+        const size_t m = std::min(chunk, nb - off);
+        PSB_TRY(cuda_check(c, cudaMemcpyAsync(stage, pos + 3 * off, sizeof(float) * 3 * m, cudaMemcpyHostToDevice, st),
+                           "boundary"));
+        k_pack3<<<blocks((int)m), psb::kBlock, 0, st>>>((int)m, stage, c->bnd_raw + off);
+    }
+    cudaMemsetAsync(c->flags, 0, 8 * sizeof(int), st);
+    c->bnd_res = psb::launch_bnd_prepare(st, c->P, n_bnd, c->bnd_raw, c->bnd_iota, c->bnd_keys, c->bnd_vals,
+                                         c->bnd_hist, psb::radix_blocks(n_bnd), c->key_bits, c->bnd_sorted, c->bnd_ids,
+                                         c->bnd_w, c->bnd_cs, c->bnd_ce, &c->flags[4]);
+    // the bounding box, grown by the list cut-off
+    float lo[3] = {pos[0], pos[1], pos[2]}, hi[3] = {pos[0], pos[1], pos[2]};
+    for (size_t i = 1; i < nb; ++i)
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], pos[3 * i + a]);
+            hi[a] = std::max(hi[a], pos[3 * i + a]);
+        }
+    const float grow_by = (float)(c->P.h * 1.001) + 1e-6f;
+    for (int a = 0; a < 3; ++a) { c->P.bnd_lo[a] = lo[a] - grow_by; c->P.bnd_hi[a] = hi[a] + grow_by; }
+    c->bnd_n = n_bnd;
+    c->P.bnd = c->bnd_sorted;
+    c->P.bnd_count = c->bnd_count;
+    c->P.bnd_list = c->bnd_list;
+    c->P.bnd_cap = psb_ctx::kBndCap;
+    c->built = false;
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->h_flags, c->flags, 8 * sizeof(int), cudaMemcpyDeviceToHost, st), "boundary"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "boundary"));
+    if (c->h_flags[4]) return fail(c, PSB_EINVAL, "psb_set_boundary: boundary particles outside the grid");
+    return cuda_check(c, cudaGetLastError(), "psb_set_boundary");
+}
+
+int psb_boundary_psi(psb_ctx* c, float* psi) {
+    if (!c || !psi) return PSB_EINVAL;
+    if (c->bnd_n == 0) return fail(c, PSB_ESTATE, "psb_boundary_psi: no boundary set");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    std::vector<float> w((size_t)c->bnd_n);
+    std::vector<int> ids((size_t)c->bnd_n);
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(w.data(), c->bnd_w, sizeof(float) * w.size(), cudaMemcpyDeviceToHost, st), "psi"));
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(ids.data(), c->bnd_ids, sizeof(int) * ids.size(), cudaMemcpyDeviceToHost, st),
+                       "psi"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "psi"));
+    for (int t = 0; t < c->bnd_n; ++t) psi[ids[t]] = (float)(w[t] * c->sc.mass);
+    return PSB_OK;
+}
 
 int psb_diagnostics(psb_ctx* c, psb_diag* out, int32_t n_out) {
     if (!c || !out) return PSB_EINVAL;

@@ -91,6 +91,15 @@ struct Params {
     unsigned long long* err_scene;    // corrector: per-scene max compression error of the pass (ordered)
     int nscenes;
     Tune tune;
+    // Static boundary particles (config profile; Akinci et al. 2012): sorted
+    // by cell, position in .xyz and psi_b / m in .w; per fluid slot its
+    // boundary neighbours within the list cut-off, stored in quads like the
+    // fluid list (bnd_cap slots). bnd_count == nullptr: no boundary.
+    const float4* bnd;
+    const int* bnd_count;
+    const int* bnd_list;
+    int bnd_cap;
+    float bnd_lo[3], bnd_hi[3];     // their bounding box grown by the list cut-off
 };
 
 // Runs f(std::integral_constant<int, B>) with B the tuned block size.
@@ -177,6 +186,20 @@ void launch_batch_begin(cudaStream_t st, int S, int max_it, uint8_t* active, uns
 void launch_batch_decide(cudaStream_t st, int S, int min_it, int max_it, double eta, uint8_t* active,
                          unsigned long long* err_scene, unsigned long long* err_hist, int* loop,
                          cudaGraphConditionalHandle handle, int set_handle);
+
+// ---- boundary particles (boundary.cu) ------------------------------------------
+// Sorts nb boundary particles by cell (stable on index), fills their cell
+// ranges and writes psi_b / m to .w of sorted[]: rho0 / (k_rho sum_k (1 -
+// q_bk)^3) over the boundary particles within h, self included. Returns the
+// buffer (0 or 1) of keys[] that holds the sorted keys.
+int launch_bnd_prepare(cudaStream_t st, const Params& P, int nb, const float4* raw, int* iota, uint32_t* keys[2],
+                       uint32_t* vals[2], uint32_t* hist, int hist_blocks, int key_bits, float4* sorted, int* ids,
+                       float* w, uint32_t* cell_start, uint32_t* cell_end, int* clamped);
+// Per fluid slot: the boundary particles within the list cut-off, from a
+// 27-cell walk of the boundary's cell ranges (none outside P.bnd_lo/hi);
+// flags[0] is set when a slot has more than P.bnd_cap.
+void launch_build_bnd_nbr(cudaStream_t st, const Params& P, const float4* pos, const uint32_t* keys,
+                          const uint32_t* bnd_start, const uint32_t* bnd_end, int* counts, int* list, int* flags);
 
 // ---- FP64 diagnostics (diag.cu) -------------------------------------------------
 // terms: mass, momentum x/y/z, kinetic, potential, sum and max of |rho - rho0|/rho0

@@ -223,6 +223,39 @@ __device__ __forceinline__ void ghost_pressure(const Params& P, int t, float4 xi
     });
 }
 
+// Boundary particles (config profile; boundary.cu): density psi_b W_ib, as
+// (psi_b / m) (1 - q)^3 inside the k_rho-scaled sum, and the mirrored
+// pressure term psi_b pV_i gradW_ib, as (psi_b / m) pV_i (1-u)^2 x^ inside
+// the k_grad-scaled sum. The positions are the step's start positions of
+// a static solid; x_i is the particle's current (or predicted) position.
+__device__ __forceinline__ void boundary_density(const Params& P, int t, float4 xi, Kahan& acc) {
+    if (!P.bnd_count) return;
+    const int cnt = min(P.bnd_count[t], P.bnd_cap);
+    for_each_nbr(P.bnd_list, P.n, t, cnt, [&](const int b) {
+        const float4 xb = P.bnd[b];
+        const float dx = xi.x - xb.x, dy = xi.y - xb.y, dz = xi.z - xb.z;
+        const float q = (dx * dx + dy * dy + dz * dz) * P.inv_h2;
+        if (q >= 1.f) return;
+        const float w = 1.f - q;
+        acc.add(xb.w * (w * w * w));
+    });
+}
+
+__device__ __forceinline__ void boundary_pressure(const Params& P, int t, float4 xi, float pVi, float3& ap) {
+    if (!P.bnd_count) return;
+    const int cnt = min(P.bnd_count[t], P.bnd_cap);
+    for_each_nbr(P.bnd_list, P.n, t, cnt, [&](const int b) {
+        const float4 xb = P.bnd[b];
+        const float dx = xi.x - xb.x, dy = xi.y - xb.y, dz = xi.z - xb.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) return;
+        const float rinv = rsqrtf(r2);
+        const float om = 1.f - r2 * rinv * P.inv_h;
+        const float sc = xb.w * pVi * om * om * rinv;
+        ap.x += sc * dx; ap.y += sc * dy; ap.z += sc * dz;
+    });
+}
+
 // collisionBox (BoxCollision_Kernel.cu:7-34) with restitution 0: clamp into
 // [Min+r, Max-r] (upper bounds tested first, lower bounds win), then remove
 // the velocity component along the normalised sum of wall normals. PCISPH
@@ -301,7 +334,10 @@ __global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __rest
             div += s * ((vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz);
         }
     });
-    if (!REF) ghost_density<BATCH>(P, t, xi, pos, list, cnt, acc);
+    if (!REF) {
+        ghost_density<BATCH>(P, t, xi, pos, list, cnt, acc);
+        if (!BATCH) boundary_density(P, t, xi, acc);
+    }
     const float drho = density_deviation(P, acc);
     const float rho = P.rho0 + drho;
     float p;
@@ -383,8 +419,10 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
             S.nrm.x += dx * sn; S.nrm.y += dy * sn; S.nrm.z += dz * sn;
         }
     });
-    if (WITH_PRESSURE && !REF)
+    if (WITH_PRESSURE && !REF) {
         ghost_pressure<BATCH>(P, t, xi, pVi, pos, (const float*)rp + 1, 2, list, cnt, S.ap);
+        if (!BATCH) boundary_pressure(P, t, xi, pVi, S.ap);
+    }
     return S;
 }
 
@@ -493,7 +531,10 @@ __global__ void __launch_bounds__(BS) k_pci_density(Params P, const float4* __re
                 T2 += g * g;
             }
         });
-        if (!REF) ghost_density<BATCH>(P, t, xi, xs, list, cnt, acc);
+        if (!REF) {
+            ghost_density<BATCH>(P, t, xi, xs, list, cnt, acc);
+            if (!BATCH) boundary_density(P, t, xi, acc);
+        }
         const float drho = density_deviation(P, acc);
         const float rho = P.rho0 + drho;
         float p = rp[t].y;
@@ -568,7 +609,10 @@ __global__ void __launch_bounds__(BS) k_pci_force_predict(Params P, const float4
         const float s = (pVi + pVj) * om * om * rinv;
         acc.x += s * dx; acc.y += s * dy; acc.z += s * dz;
     });
-    if (!REF) ghost_pressure<BATCH>(P, t, xi, pVi, geo, (const float*)rpc + 1, 2, list, cnt, acc);
+    if (!REF) {
+        ghost_pressure<BATCH>(P, t, xi, pVi, geo, (const float*)rpc + 1, 2, list, cnt, acc);
+        if (!BATCH) boundary_pressure(P, t, xi, pVi, acc);
+    }
     const float4 x0 = pos[t], vh = vap[t], f = fnp[t];
     const float3 aw = wall_accel<REF, BATCH>(P, t, x0, vh);
     const float ir = 1.f / ri.x;

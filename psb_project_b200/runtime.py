@@ -39,6 +39,7 @@ EXPORTS = (
     "psb_mlp_get_weights", "psb_mlp_collect", "psb_mlp_dataset", "psb_mlp_train", "psb_mlp_forward",
     "psb_mlp_loss_grad", "psb_iso_field", "psb_extract_surface", "psb_create_batch", "psb_batch_layout",
     "psb_batch_stats", "psb_set_graph", "psb_autotune", "psb_tune_set", "psb_tune_get", "psb_diagnostics",
+    "psb_set_boundary", "psb_boundary_psi",
 )
 MLP_PARAMS = 4673       # PSB_MLP_PARAMS
 MLP_IN, MLP_H = 6, 64
@@ -157,6 +158,8 @@ def lib():
         "psb_tune_set": ([P, ctypes.POINTER(PsbTune)], ctypes.c_int),
         "psb_tune_get": ([P, I32, ctypes.POINTER(PsbTune)], ctypes.c_int),
         "psb_diagnostics": ([P, ctypes.POINTER(PsbDiag), I32], ctypes.c_int),
+        "psb_set_boundary": ([P, I32, P], ctypes.c_int),
+        "psb_boundary_psi": ([P, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -359,6 +362,15 @@ class Simulation:
                                               _ptr(tri), ctypes.byref(nt)), "psb_extract_surface")
         return vert[:nv.value], tri[:nt.value]
 
+    def extract_surface_into(self, grid: IsoGrid, level: float, vert: np.ndarray, tri: np.ndarray):
+        """psb_extract_surface in one call into caller buffers (vert (V, 3)
+        float32, tri (T, 3) int32, both C-contiguous); returns (V, T) used."""
+        nv = ctypes.c_int64(vert.shape[0])
+        nt = ctypes.c_int64(tri.shape[0])
+        self._check(lib().psb_extract_surface(self._h, ctypes.byref(grid), float(level), _ptr(vert), ctypes.byref(nv),
+                                              _ptr(tri), ctypes.byref(nt)), "psb_extract_surface")
+        return nv.value, nt.value
+
     def download(self, out: Optional[dict] = None) -> dict:
         n = self.n
         o = out if out is not None else {
@@ -386,6 +398,19 @@ class Simulation:
         s = PsbStepStats()
         self._check(lib().psb_get_stats(self._h, ctypes.byref(s)), "psb_get_stats")
         return s
+
+    # -- boundary particles ------------------------------------------------------
+    def set_boundary(self, pos):
+        """Static boundary particles (config profile): positions (n_b, 3)."""
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        self._check(lib().psb_set_boundary(self._h, pos.shape[0], _ptr(pos) if pos.shape[0] else None),
+                    "psb_set_boundary")
+        self.n_bnd = pos.shape[0]
+
+    def boundary_psi(self) -> np.ndarray:
+        out = np.empty(self.n_bnd, np.float32)
+        self._check(lib().psb_boundary_psi(self._h, _ptr(out)), "psb_boundary_psi")
+        return out
 
     # -- diagnostics -------------------------------------------------------------
     def diagnostics(self, per_scene: bool = False):

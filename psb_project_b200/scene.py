@@ -354,6 +354,20 @@ def batch_scenes(n_scenes: int = 64, seed: int = 3, n_range=(4096, 131072), spac
     return out
 
 
+def sphere_shell(centre, radius: float, spacing: float, layers: int = 2) -> np.ndarray:
+    """Boundary particles of a solid sphere: the points of the cubic lattice
+    of this spacing (aligned on the centre) whose distance to the centre lies
+    in [radius - layers spacing, radius). A shell of two spacings covers the
+    kernel's reach h = 2 spacing from outside."""
+    c = np.asarray(centre, np.float64)
+    m = int(math.ceil(radius / spacing)) + 1
+    ax = np.arange(-m, m + 1) * spacing
+    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
+    d = np.sqrt(X ** 2 + Y ** 2 + Z ** 2)
+    sel = (d < radius) & (d >= radius - layers * spacing)
+    return (np.stack([X[sel], Y[sel], Z[sel]], 1) + c).astype(np.float32)
+
+
 def ref_scene(nxyz=(12, 10, 8), spacing=0.01, box=(0.3, 0.3, 0.3), h=0.02, method=PCISPH, dt=5e-4,
               seed=7, jitter=1e-4) -> Scene:
     """Small scene in the reference-compatible profile (parity tests)."""

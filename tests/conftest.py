@@ -3,9 +3,11 @@ import sys
 
 import pytest
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-if ROOT not in sys.path:
-    sys.path.insert(0, ROOT)
+TESTS = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(TESTS)
+for p in (ROOT, TESTS):      # the package and oracle; test modules that share helpers
+    if p not in sys.path:
+        sys.path.insert(0, p)
 
 
 def pytest_configure(config):

@@ -19,7 +19,8 @@ def numpy_diag(state, sc, g):
     rho = state["density"].astype(np.float64)
     err = np.abs(rho - sc.rho0) / sc.rho0
     return {"mass": m * len(v), "momentum": list(m * v.sum(0)), "kinetic": 0.5 * m * np.sum(v * v),
-            "potential": -m * np.sum(x @ np.asarray(g, np.float64)), "density_err_mean": err.mean(),
+            # the step's gravity is stored in FP32
+            "potential": -m * np.sum(x @ np.asarray(g, np.float32).astype(np.float64)), "density_err_mean": err.mean(),
             "density_err_max": err.max()}
 
 
