@@ -354,6 +354,58 @@ int psb_set_boundary(psb_ctx* ctx, int32_t n_bnd, const float* pos);
 /* psi_b (kg) of the current boundary set, in the order it was given. */
 int psb_boundary_psi(psb_ctx* ctx, float* psi);
 
+/* The scene the context was created with (for a batch: scene 0 with n_max
+ * the total), the particle count of the last upload (0 before one) and the
+ * steps taken; psb_set_step_count overwrites the step count (checkpoints). */
+int psb_context_info(const psb_ctx* ctx, psb_scene* scene, int32_t* n, int64_t* steps);
+int psb_set_step_count(psb_ctx* ctx, int64_t steps);
+
+/* ---- files --------------------------------------------------------------
+ * The reference front end's export formats, so files made here open where
+ * the reference's did. Numbers carry 9 significant digits (every float
+ * exactly); the reference's writers round to 6. Paths are host file names;
+ * each call returns PSB_EINVAL when the file cannot be written.
+ * Txt particles, replacing ParticleExporter_Txt::_export for SPH systems
+ * (ParticleExporter_Txt.cpp:27-33): "SPH <n>", then "-p x y z -m m -d rho"
+ * per particle (pos: n x 3 doubles; density: n floats). */
+int psb_write_txt(const char* path, int32_t n, const double* pos, double mass, const float* density);
+/* XML particles, replacing ParticleExporter_XML::_export_SPHParticles
+ * (ParticleExporter_XML.cpp:130-185): <Particles name="SPH System" dt count>,
+ * <Gravity X Y Z Amp/>, and per particle the SPH attributes (mass, radius,
+ * kernelParticles = its neighbour count, interactionRadius, restDensity,
+ * gasStiffness, threshold, surfaceTension, viscosity) with <position>,
+ * <velocity>, <velocityInterAv> (2 v - v+), <velocityInterAp> (v+) and
+ * <color> (0, 0, 1). nbr_count may be NULL (written as 0). */
+int psb_write_xml(const char* path, const psb_scene* scene, int32_t n, const double* pos, const double* vel,
+                  const double* vel_half, const int32_t* nbr_count);
+/* Mitsuba grid volume, replacing _exportData (UniformGrid.cu:266-300):
+ * "VOL", version 3, encoding 1 (float32), resolution, 1 channel, the box
+ * (bmin, bmax), then the field (dims[0] x dims[1] x dims[2] doubles, x
+ * fastest, as psb_iso_field returns it) as floats. reference_layout = 0:
+ * Mitsuba's order (x fastest); 1: the reference's file, which writes the z
+ * resolution for all three axes and z fastest, for cubic grids only. */
+int psb_write_vol(const char* path, const double* field, const int32_t dims[3], const float bmin[3], const float bmax[3],
+                  int32_t reference_layout);
+/* Wavefront OBJ of a triangle mesh (psb_extract_surface's output),
+ * replacing SurfaceSPH::exportOBJ (SurfaceSPH.cpp:234-276): v lines, vn
+ * lines (area-weighted vertex normals), then "f a//a b//b c//c" per
+ * triangle. The reference also swaps y and z and scales for its renderer,
+ * and skips the last triangle; these do neither. */
+int psb_write_obj(const char* path, const float* vertices, int64_t n_vertices, const int32_t* triangles,
+                  int64_t n_triangles);
+/* The context's current state through the writers above (a download first). */
+int psb_export_txt(psb_ctx* ctx, const char* path);
+int psb_export_xml(psb_ctx* ctx, const char* path);
+/* Checkpoints: the complete state a step continues from -- positions,
+ * interpolated and half-step velocities, the carried pressure (read by the
+ * warm starts), densities and the step count -- in particle-id order, with
+ * the scene. Loading into a context of the same scene (any n_max large
+ * enough) uploads it; stepping on gives bit for bit what the saved context
+ * gives. Loading into a different scene returns PSB_EINVAL. No counterpart
+ * in the reference, which restarts from its XML configuration only. */
+int psb_checkpoint_save(psb_ctx* ctx, const char* path);
+int psb_checkpoint_load(psb_ctx* ctx, const char* path);
+
 /* FP64 diagnostics of the current state: with the corrector's convergence
  * reduction, the only FP64 arithmetic on the device. Each sum runs in FP64
  * in a fixed order (per-block partial sums, then one pass over the blocks),

@@ -1792,6 +1792,20 @@ int psb_autotune(psb_ctx* c, int32_t trials, psb_tune* out) {
     return PSB_OK;
 }
 
+int psb_context_info(const psb_ctx* c, psb_scene* scene, int32_t* n, int64_t* steps) {
+    if (!c) return PSB_EINVAL;
+    if (scene) *scene = c->sc;
+    if (n) *n = c->uploaded ? c->n : 0;
+    if (steps) *steps = c->stats.steps;
+    return PSB_OK;
+}
+
+int psb_set_step_count(psb_ctx* c, int64_t steps) {
+    if (!c || steps < 0) return PSB_EINVAL;
+    c->stats.steps = steps;
+    return PSB_OK;
+}
+
 int psb_get_stats(psb_ctx* c, psb_step_stats* out) {
     if (!c || !out) return PSB_EINVAL;
     *out = c->stats;

@@ -39,7 +39,9 @@ EXPORTS = (
     "psb_mlp_get_weights", "psb_mlp_collect", "psb_mlp_dataset", "psb_mlp_train", "psb_mlp_forward",
     "psb_mlp_loss_grad", "psb_iso_field", "psb_extract_surface", "psb_create_batch", "psb_batch_layout",
     "psb_batch_stats", "psb_set_graph", "psb_autotune", "psb_tune_set", "psb_tune_get", "psb_diagnostics",
-    "psb_set_boundary", "psb_boundary_psi",
+    "psb_set_boundary", "psb_boundary_psi", "psb_context_info", "psb_set_step_count", "psb_write_txt",
+    "psb_write_xml", "psb_write_vol", "psb_write_obj", "psb_export_txt", "psb_export_xml", "psb_checkpoint_save",
+    "psb_checkpoint_load",
 )
 MLP_PARAMS = 4673       # PSB_MLP_PARAMS
 MLP_IN, MLP_H = 6, 64
@@ -160,6 +162,16 @@ def lib():
         "psb_diagnostics": ([P, ctypes.POINTER(PsbDiag), I32], ctypes.c_int),
         "psb_set_boundary": ([P, I32, P], ctypes.c_int),
         "psb_boundary_psi": ([P, P], ctypes.c_int),
+        "psb_context_info": ([P, ctypes.POINTER(PsbScene), ctypes.POINTER(I32), ctypes.POINTER(I64)], ctypes.c_int),
+        "psb_set_step_count": ([P, I64], ctypes.c_int),
+        "psb_write_txt": ([ctypes.c_char_p, I32, P, ctypes.c_double, P], ctypes.c_int),
+        "psb_write_xml": ([ctypes.c_char_p, ctypes.POINTER(PsbScene), I32, P, P, P, P], ctypes.c_int),
+        "psb_write_vol": ([ctypes.c_char_p, P, P, P, P, I32], ctypes.c_int),
+        "psb_write_obj": ([ctypes.c_char_p, P, I64, P, I64], ctypes.c_int),
+        "psb_export_txt": ([P, ctypes.c_char_p], ctypes.c_int),
+        "psb_export_xml": ([P, ctypes.c_char_p], ctypes.c_int),
+        "psb_checkpoint_save": ([P, ctypes.c_char_p], ctypes.c_int),
+        "psb_checkpoint_load": ([P, ctypes.c_char_p], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -208,6 +220,45 @@ def mlp_unpack(w: np.ndarray):
         out.append(w[o:o + k].reshape(shape))
         o += k
     return out
+
+
+def _status(rc: int, what: str):
+    if rc != OK:
+        raise PsbError(rc, f"{what}: {lib().psb_status_string(rc).decode()}")
+
+
+def write_txt(path: str, pos, mass: float, density):
+    """Txt particle file (the reference's ParticleExporter_Txt format)."""
+    pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+    rho = np.ascontiguousarray(density, np.float32)
+    _status(lib().psb_write_txt(path.encode(), pos.shape[0], _ptr(pos), float(mass), _ptr(rho)), "psb_write_txt")
+
+
+def write_xml(path: str, scene: Scene, pos, vel, vel_half, nbr_count=None):
+    """XML particle file (the reference's ParticleExporter_XML SPH format)."""
+    cv = lambda a: np.ascontiguousarray(a, np.float64).reshape(-1, 3)
+    pos, vel, vel_half = cv(pos), cv(vel), cv(vel_half)
+    nb = None if nbr_count is None else np.ascontiguousarray(nbr_count, np.int32)
+    sc = scene.to_c()
+    _status(lib().psb_write_xml(path.encode(), ctypes.byref(sc), pos.shape[0], _ptr(pos), _ptr(vel), _ptr(vel_half),
+                                _ptr(nb)), "psb_write_xml")
+
+
+def write_vol(path: str, field, dims, bmin, bmax, reference_layout: bool = False):
+    """Mitsuba grid volume of a node field (x fastest, as iso_field returns it)."""
+    f = np.ascontiguousarray(field, np.float64)
+    d = np.asarray(dims, np.int32)
+    lo = np.asarray(bmin, np.float32)
+    hi = np.asarray(bmax, np.float32)
+    _status(lib().psb_write_vol(path.encode(), _ptr(f), _ptr(d), _ptr(lo), _ptr(hi), 1 if reference_layout else 0),
+            "psb_write_vol")
+
+
+def write_obj(path: str, vertices, triangles):
+    """Wavefront OBJ of a triangle mesh, with area-weighted vertex normals."""
+    v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(triangles, np.int32).reshape(-1, 3)
+    _status(lib().psb_write_obj(path.encode(), _ptr(v), v.shape[0], _ptr(t), t.shape[0]), "psb_write_obj")
 
 
 def scene_positions(scene: Scene) -> np.ndarray:
@@ -411,6 +462,27 @@ class Simulation:
         out = np.empty(self.n_bnd, np.float32)
         self._check(lib().psb_boundary_psi(self._h, _ptr(out)), "psb_boundary_psi")
         return out
+
+    # -- files -------------------------------------------------------------------
+    def export_txt(self, path: str):
+        self._check(lib().psb_export_txt(self._h, path.encode()), "psb_export_txt")
+
+    def export_xml(self, path: str):
+        self._check(lib().psb_export_xml(self._h, path.encode()), "psb_export_xml")
+
+    def checkpoint_save(self, path: str):
+        self._check(lib().psb_checkpoint_save(self._h, path.encode()), "psb_checkpoint_save")
+
+    def checkpoint_load(self, path: str):
+        self._check(lib().psb_checkpoint_load(self._h, path.encode()), "psb_checkpoint_load")
+        n = ctypes.c_int32()
+        self._check(lib().psb_context_info(self._h, None, ctypes.byref(n), None), "psb_context_info")
+        self.n = n.value
+
+    def steps_taken(self) -> int:
+        st = ctypes.c_int64()
+        self._check(lib().psb_context_info(self._h, None, None, ctypes.byref(st)), "psb_context_info")
+        return st.value
 
     # -- diagnostics -------------------------------------------------------------
     def diagnostics(self, per_scene: bool = False):
