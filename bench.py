@@ -814,6 +814,85 @@ def run_c4(args):
     rep_.close()
 
 
+def run_c1(args):
+    """Config C1: the 262,144-particle PCISPH dam break (eta 1 %, dt 1e-3)
+    with 4,096 DEM spheres dropped from above it, coupled two ways through
+    boundary particles (psb_project_b200.FluidDemCoupling): each step the
+    fluid steps with the spheres as its boundary, its reaction on every
+    sphere is the spheres' external force, and the spheres step. `value`
+    counts fluid and sphere particle-steps over the device time of the
+    coupled steps, the per-step host exchange of sphere positions and forces
+    included (that exchange is also the `e2e` traffic). Multi-GPU: replicas."""
+    import torch
+    import psb_project_b200 as P
+    from psb_project_b200 import replicas
+
+    rep_ = replicas.init("nccl")
+    rank, world, local = rep_.rank, rep_.world, rep_.local
+    torch.cuda.set_device(local)
+    fl, sp = P.c1_scenes(seed=1 + (replicas.SEED_STRIDE * rank if world > 1 else 0))
+    stream = torch.cuda.current_stream()
+    fluid, balls = P.Simulation(fl), P.Simulation(sp)
+    for s_ in (fluid, balls):
+        s_.set_stream(stream.cuda_stream)
+    fluid.upload(P.scene_positions(fl))
+    fluid.presolve(args.presolve)
+    balls.upload(P.scene_positions(sp))
+    coupled = P.FluidDemCoupling(fluid, balls)
+    coupled.step(args.warmup)
+
+    def barrier():
+        rep_.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    iters = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        coupled.step(1)
+        iters.append(fluid.stats().iters)
+    e1.record(stream)
+    barrier()
+    ms = rep_.max_over_ranks(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    n_all = fl.n + sp.n
+    value = world * n_all * args.steps / (ms / 1e3)
+    fluid.profile(True)
+    balls.profile(True)
+    coupled.step(min(args.steps, 20))
+    prof = {("fluid:" + k): v for k, v in fluid.profile_read().items()}
+    prof.update({("dem:" + k): v for k, v in balls.profile_read().items()})
+    bpos = balls.download()["pos"]
+    in_fluid = int(np.sum(bpos[:, 1] < fl.blocks[0].nxyz[1] * fl.blocks[0].spacing))
+    diag = fluid.diagnostics()
+    fluid.close()
+    balls.close()
+    if rank == 0:
+        tot = sum(v[1] for v in prof.values())
+        out = {
+            "metric": "particle-steps/s, 262,144-particle PCISPH dam break coupled with 4,096 DEM spheres (C1)",
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": fl.name + " + " + sp.name, "fluid_particles": fl.n, "spheres": sp.n,
+                       "eta": fl.eta, "dt": fl.dt, "coupling": "spheres as boundary particles, two-way",
+                       "timed_steps": "steps %d..%d" % (args.warmup + 1, args.warmup + args.steps),
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "iters_per_step": {"mean": float(np.mean(iters)), "p50": float(np.median(iters)), "max": int(np.max(iters))},
+            "spheres_below_fluid_top_at_end": in_fluid,
+            "kernels": {k: {"launches": l, "ms": round(v, 3), "share": round(v / tot, 4)} for k, (l, v) in prof.items()},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 24 * sp.n, "d2h_bytes_per_step": 24 * sp.n},
+            "diagnostics_fp64": diag, "clocks": clk,
+        }
+        print(json.dumps(out))
+    rep_.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -822,6 +901,8 @@ def main():
         run_batch(args)
     elif args.scene == "C4":
         run_c4(args)
+    elif args.scene == "C1":
+        run_c1(args)
     else:
         run_ours(args)
 

@@ -234,8 +234,7 @@ int psb_lattice(const int32_t nxyz[3], double spacing, const double origin[3], d
  * (about 2.1 MB) until the process exits.
  * Limit: n <= PSB_NOALLOC_MAX_N; larger n returns PSB_EINVAL (with a message
  * on stderr). The first call on each device looks up the array's device
- * address, so make that first call before any stream capture begins. All
- * calls share the one array: calls that overlap on the GPU (other streams or
+ * address. All calls share the one array: calls that overlap on the GPU (other streams or
  * threads on the same device) race and corrupt each other's results. */
 #define PSB_NOALLOC_MAX_N 262144
 int psb_sort_cells_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
@@ -353,6 +352,18 @@ int psb_tune_get(psb_ctx* ctx, int32_t bucket, psb_tune* out);
 int psb_set_boundary(psb_ctx* ctx, int32_t n_bnd, const float* pos);
 /* psi_b (kg) of the current boundary set, in the order it was given. */
 int psb_boundary_psi(psb_ctx* ctx, float* psi);
+/* The force (N, n_bnd x 3, in the order given) the fluid exerts on each
+ * boundary particle after the last step: minus the mirrored-pressure forces
+ * the particle exerts on the fluid particles within h, from their committed
+ * positions and pressures. With DEM spheres as the boundary particles this
+ * is the fluid's side of a two-way coupling (C1). No counterpart in the
+ * reference, which has no fluid-solid coupling. */
+int psb_boundary_forces(psb_ctx* ctx, float* force);
+/* DEM contexts: an external force per sphere (N, n x 3 in particle-id
+ * order) added to gravity and contacts in every step until replaced; NULL
+ * removes it. Extends CudaSystem::update's force sum (CudaSystem.cpp:207-224),
+ * which has gravity and contacts only. */
+int psb_set_external_force(psb_ctx* ctx, const float* force);
 
 /* The scene the context was created with (for a batch: scene 0 with n_max
  * the total), the particle count of the last upload (0 before one) and the

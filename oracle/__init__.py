@@ -49,6 +49,7 @@ class OrcParams(ctypes.Structure):
         ("dem_attraction", ctypes.c_double),
         ("n_bnd", ctypes.c_int32), ("bnd_pos", ctypes.c_void_p), ("bnd_psi", ctypes.c_void_p),
         ("bnd_counts", ctypes.c_void_p), ("bnd_lists", ctypes.c_void_p), ("bnd_cap", ctypes.c_int32),
+        ("dem_ext", ctypes.c_void_p),
     ]
 
 
@@ -172,6 +173,8 @@ def lib():
         L.orc_boundary_psi.restype = None
         L.orc_pressure_force.argtypes = [ctypes.POINTER(OrcParams), P, P, P, P, P, ctypes.c_int32, P]
         L.orc_pressure_force.restype = None
+        L.orc_boundary_reaction.argtypes = [ctypes.POINTER(OrcParams), P, P, ctypes.c_int32, P, P, P]
+        L.orc_boundary_reaction.restype = None
         _lib = L
     return _lib
 
@@ -256,6 +259,18 @@ def boundary_psi(scene, bpos) -> np.ndarray:
     return psi
 
 
+def boundary_reaction(scene, pos, p, bpos) -> np.ndarray:
+    """The fluid's force on each boundary particle (nb, 3)."""
+    pos = np.ascontiguousarray(pos, np.float64)
+    p = np.ascontiguousarray(p, np.float64)
+    bpos = np.ascontiguousarray(bpos, np.float64)
+    psi = boundary_psi(scene, bpos)
+    out = np.zeros((bpos.shape[0], 3))
+    P = params(scene, n=pos.shape[0])
+    lib().orc_boundary_reaction(ctypes.byref(P), _ptr(pos), _ptr(p), bpos.shape[0], _ptr(bpos), _ptr(psi), _ptr(out))
+    return out
+
+
 def pci_delta(scene) -> float:
     P = params(scene)
     return lib().orc_pci_delta(ctypes.byref(P))
@@ -333,6 +348,15 @@ class OracleSim:
         if rc != 0:
             raise RuntimeError(f"orc_presolve failed: {rc}")
         return self.stats
+
+    def set_external_force(self, f):
+        """DEM: a per-sphere external force (n, 3) for the following steps (None: off)."""
+        if f is None:
+            self.ext = None
+            self.P.dem_ext = None
+        else:
+            self.ext = np.ascontiguousarray(f, np.float64).reshape(-1, 3)
+            self.P.dem_ext = self.ext.ctypes.data
 
     def step(self):
         S = OrcState(self.pos.ctypes.data, self.vel.ctypes.data, self.vel_half.ctypes.data,

@@ -438,6 +438,24 @@ static void pressure_forces(const orc_params* P, const double* pos, const double
     }
 }
 
+void orc_boundary_reaction(const orc_params* P, const double* pos, const double* p, int32_t nb, const double* bpos,
+                           const double* psi, double* out) {
+    const double h = P->h, m = P->mass, ir0 = 1.0 / (P->rho0 * P->rho0);
+#pragma omp parallel for schedule(static)
+    for (int32_t b = 0; b < nb; ++b) {
+        double F[3] = {0, 0, 0};
+        for (int32_t i = 0; i < P->n; ++i) {
+            const double dv[3] = {pos[3 * i] - bpos[3 * b], pos[3 * i + 1] - bpos[3 * b + 1],
+                                  pos[3 * i + 2] - bpos[3 * b + 2]};
+            const double d = len3(dv);
+            if (!(d > 0) || d >= h) continue;
+            const double g = 45 * pow(h - d, 2) / (PI_D * pow(h, 6));
+            for (int e = 0; e < 3; ++e) F[e] -= m * psi[b] * p[i] * ir0 * g * dv[e] / d;
+        }
+        for (int e = 0; e < 3; ++e) out[3 * b + e] = F[e];
+    }
+}
+
 void orc_pressure_force(const orc_params* P, const double* pos, const double* rho, const double* p,
                         const int32_t* counts, const int32_t* list, int32_t cap, double* fp) {
     pressure_forces(P, pos, rho, p, counts, list, cap, fp);
@@ -840,6 +858,8 @@ static int step_dem(const orc_params* P, orc_state* S, orc_stats* st, double* f_
     for (int32_t i = 0; i < n; ++i) {
         double* fi = &f[3 * (size_t)i];
         for (int e = 0; e < 3; ++e) fi[e] = 0.0 + (double)P->gravity[e] * P->mass;
+        if (P->dem_ext)
+            for (int e = 0; e < 3; ++e) fi[e] += P->dem_ext[3 * (size_t)i + e];
         for (int32_t t = 0; t < counts[i]; ++t) {
             const int32_t j = list[(size_t)i * cap + t];
             if (ref) dem_pair_ref(P, &S->pos[3 * i], &S->pos[3 * j], &S->vel[3 * i], &S->vel[3 * j], fi);

@@ -50,7 +50,16 @@ typedef struct orc_params {
     const int32_t* bnd_counts;
     const int32_t* bnd_lists;
     int32_t bnd_cap;
+    /* DEM: an external force per sphere (n * 3, N; NULL: none) */
+    const double* dem_ext;
 } orc_params;
+
+/* The force the fluid (n particles at pos with pressures p) exerts on each
+ * boundary particle: minus the sum over fluid particles i within h of
+ * m_i psi_b (p_i/rho0^2) 45 (h-d)^2/(pi h^6) (x_i - x_b)/d, the reaction to
+ * the mirrored-pressure force. Brute force; out: nb * 3. */
+void orc_boundary_reaction(const orc_params* P, const double* pos, const double* p, int32_t nb, const double* bpos,
+                           const double* psi, double* out);
 
 /* psi_b = rho0 / sum_k W(x_b - x_k) over the boundary particles within h
  * (self included), W the poly6 kernel (Akinci et al. 2012, eq. 5). */

@@ -148,6 +148,10 @@ struct psb_ctx {
     int* d_loop = nullptr;                        // device loop words (batch.cu)
     int* h_loop = nullptr;                        // pinned mirrors
     unsigned long long* h_err_sh = nullptr;
+    // DEM: external force per sphere (psb_set_external_force), id order
+    float4* ext_force = nullptr;
+    float4* bnd_force = nullptr;    // boundary reaction scratch (psb_boundary_forces)
+    long long bnd_force_cap = 0;
     // static boundary particles (psb_set_boundary); bnd_n == 0: none
     int bnd_n = 0, bnd_res = 0;
     static constexpr int kBndCap = 64;
@@ -248,6 +252,7 @@ void free_all(psb_ctx* c) {
     cudaFree(c->bnd_raw); cudaFree(c->bnd_sorted); cudaFree(c->bnd_ids); cudaFree(c->bnd_iota); cudaFree(c->bnd_w);
     for (int i = 0; i < 2; ++i) { cudaFree(c->bnd_keys[i]); cudaFree(c->bnd_vals[i]); }
     cudaFree(c->bnd_hist); cudaFree(c->bnd_cs); cudaFree(c->bnd_ce); cudaFree(c->bnd_count); cudaFree(c->bnd_list);
+    cudaFree(c->ext_force); cudaFree(c->bnd_force);
     cudaFreeHost(c->h_loop); cudaFreeHost(c->h_err_sh);
     for (auto& g : c->gexec) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -324,6 +329,7 @@ Params derive(const psb_scene& s) {
     P.k_rho = (float)(315.0 * m / (64.0 * pi * h * h * h));
     const double G = 45.0 / (pi * h * h * h * h);
     P.k_grad = (float)(m * G);
+    P.mass = (float)m;
     P.k_visc = (float)(s.mu * m * 45.0 / (pi * h * h * h * h * h));
     P.k_surf = (float)(945.0 * m / (32.0 * pi * h * h * h * h * h));
     P.ref = s.profile == PSB_PROFILE_REF;
@@ -683,6 +689,7 @@ int step_once(psb_ctx* c, bool last) {
     cudaMemsetAsync(c->err_hist, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1), st);
     if (P.dem) {
         const int o = s ^ 1;
+        P.slot_ids = c->ids[r];
         timed(c, "dem_step", [&] {
             psb::launch_dem_step(st, P, c->pos[s], c->vel[s], c->nbr_count, c->nbr_list, c->pos[o], c->vel[o], c->vap[o],
                                  c->fnp);
@@ -1444,6 +1451,51 @@ int psb_set_boundary(psb_ctx* c, int32_t n_bnd, const float* pos) {
     PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "boundary"));
     if (c->h_flags[4]) return fail(c, PSB_EINVAL, "psb_set_boundary: boundary particles outside the grid");
     return cuda_check(c, cudaGetLastError(), "psb_set_boundary");
+}
+
+int psb_boundary_forces(psb_ctx* c, float* force) {
+    if (!c || !force) return PSB_EINVAL;
+    if (c->bnd_n == 0) return fail(c, PSB_ESTATE, "psb_boundary_forces: no boundary set");
+    if (!c->built) return fail(c, PSB_ESTATE, "psb_boundary_forces: take a step first");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    PSB_TRY(grow(c, &c->bnd_force, &c->bnd_force_cap, (long long)c->bnd_n));
+    Params P = c->P;
+    P.n = c->n;
+    psb::launch_bnd_reaction(st, P, c->bnd_n, c->pos[c->cs], c->rp[c->cr], c->cell_start, c->cell_end, c->bnd_force);
+    std::vector<float4> f((size_t)c->bnd_n);
+    std::vector<int> ids((size_t)c->bnd_n);
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(f.data(), c->bnd_force, sizeof(float4) * f.size(), cudaMemcpyDeviceToHost, st),
+                       "boundary forces"));
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(ids.data(), c->bnd_ids, sizeof(int) * ids.size(), cudaMemcpyDeviceToHost, st),
+                       "boundary forces"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "boundary forces"));
+    for (int t = 0; t < c->bnd_n; ++t) {
+        float* o = force + 3 * (size_t)ids[t];
+        o[0] = f[t].x; o[1] = f[t].y; o[2] = f[t].z;
+    }
+    return cuda_check(c, cudaGetLastError(), "boundary forces");
+}
+
+int psb_set_external_force(psb_ctx* c, const float* force) {
+    if (!c) return PSB_EINVAL;
+    if (!c->P.dem) return fail(c, PSB_EINVAL, "psb_set_external_force: DEM contexts only");
+    cudaSetDevice(c->device);
+    release_graphs(c);
+    if (!force) {
+        c->P.ext_force = nullptr;
+        return PSB_OK;
+    }
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_set_external_force before psb_upload");
+    cudaStream_t st = c->stream;
+    if (!c->ext_force) PSB_TRY(dalloc(c, &c->ext_force, (size_t)c->n_max));
+    float* stage = (float*)c->stage;
+    const int n = c->n;
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(stage, force, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, st),
+                       "external force"));
+    k_pack3<<<blocks(n), psb::kBlock, 0, st>>>(n, stage, c->ext_force);
+    c->P.ext_force = c->ext_force;
+    return cuda_check(c, cudaGetLastError(), "external force");
 }
 
 int psb_boundary_psi(psb_ctx* c, float* psi) {

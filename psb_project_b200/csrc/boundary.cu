@@ -123,7 +123,58 @@ __global__ void __launch_bounds__(kBlock) k_build_bnd_nbr(Params P, const float4
     if (cnt > P.bnd_cap) atomicOr(&flags[0], 1);
 }
 
+// Boundary slot b: F_b = - sum_j m a_j^b over the fluid particles j within
+// h, a_j^b = k_grad (psi_b / m) pV_j (1-u)^2 x^_jb the mirrored-pressure
+// acceleration the boundary particle gives j (sph.cu, boundary_pressure).
+__global__ void __launch_bounds__(kBlock) k_bnd_reaction(Params P, int nb, const float4* __restrict__ fluid_pos,
+                                                         const float2* __restrict__ fluid_rp,
+                                                         const uint32_t* __restrict__ cell_start,
+                                                         const uint32_t* __restrict__ cell_end,
+                                                         float4* __restrict__ force) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const float4 xb = P.bnd[b];
+    const int nx = P.g.nx, ny = P.g.ny, nz = P.g.nz;
+    int c[3];
+    const float lo[3] = {P.g.gx, P.g.gy, P.g.gz};
+    const float x[3] = {xb.x, xb.y, xb.z};
+    const int dims[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; ++a) {
+        const double q = floor(((double)x[a] - (double)lo[a]) / (double)P.g.cell);
+        c[a] = q < 0.0 ? 0 : (q >= (double)dims[a] ? dims[a] - 1 : (int)q);
+    }
+    const float ir0 = 1.f / (P.rho0 * P.rho0);
+    float3 s = make_float3(0.f, 0.f, 0.f);
+    for (int k = max(c[2] - 1, 0); k <= min(c[2] + 1, nz - 1); ++k)
+        for (int j = max(c[1] - 1, 0); j <= min(c[1] + 1, ny - 1); ++j) {
+            const uint32_t row = (uint32_t)j * (uint32_t)nx + (uint32_t)k * (uint32_t)nx * (uint32_t)ny;
+            for (int a = max(c[0] - 1, 0); a <= min(c[0] + 1, nx - 1); ++a) {
+                const uint32_t q0 = cell_start[row + a];
+                if (q0 == kEmpty) continue;
+                const uint32_t q1 = cell_end[row + a];
+                for (uint32_t q = q0; q < q1; ++q) {
+                    const float4 xj = fluid_pos[q];
+                    const float dx = xj.x - xb.x, dy = xj.y - xb.y, dz = xj.z - xb.z;
+                    const float r2 = dx * dx + dy * dy + dz * dz;
+                    if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) continue;
+                    const float rinv = rsqrtf(r2);
+                    const float om = 1.f - r2 * rinv * P.inv_h;
+                    const float w = fluid_rp[q].y * ir0 * om * om * rinv;
+                    s.x += w * dx; s.y += w * dy; s.z += w * dz;
+                }
+            }
+        }
+    const float k = -P.mass * P.k_grad * xb.w;
+    force[b] = make_float4(k * s.x, k * s.y, k * s.z, 0.f);
+}
+
 }  // namespace
+
+void launch_bnd_reaction(cudaStream_t st, const Params& P, int nb, const float4* fluid_pos, const float2* fluid_rp,
+                         const uint32_t* cell_start, const uint32_t* cell_end, float4* force) {
+    if (nb > 0)
+        k_bnd_reaction<<<blocks_for(nb), kBlock, 0, st>>>(P, nb, fluid_pos, fluid_rp, cell_start, cell_end, force);
+}
 
 int launch_bnd_prepare(cudaStream_t st, const Params& P, int nb, const float4* raw, int* iota, uint32_t* keys[2],
                        uint32_t* vals[2], uint32_t* hist, int hist_blocks, int key_bits, float4* sorted, int* ids,

@@ -74,6 +74,10 @@ __global__ void __launch_bounds__(kBlock) k_dem_step(Params P, const float4* __r
             f.x += s * nx; f.y += s * ny; f.z += s * nz;
         }
     });
+    if (P.ext_force) {      // e.g. the fluid's reaction in a coupled run
+        const float4 e = P.ext_force[P.slot_ids[t]];
+        f.x += e.x; f.y += e.y; f.z += e.z;
+    }
     const float im = P.dem_inv_mass;
     float3 v = make_float3(va.x + f.x * im * P.dt, va.y + f.y * im * P.dt, va.z + f.z * im * P.dt);
     const float3 vx = REF ? make_float3(va.x, va.y, va.z) : v;

@@ -15,8 +15,7 @@
 // (about 2.1 MB) until the process exits. Host code cannot pass the array's
 // name to a kernel (it is a host-side stand-in, not a device address), so
 // the address is fetched with cudaGetSymbolAddress once per device, on the
-// first call made with that device current. That first call should be made
-// before any stream capture begins.
+// first call made with that device current.
 //
 // All calls share the one array and it keeps the last call's contents.
 // Nothing in it needs clearing: every pass writes its histogram block by

@@ -100,6 +100,11 @@ struct Params {
     const int* bnd_list;
     int bnd_cap;
     float bnd_lo[3], bnd_hi[3];     // their bounding box grown by the list cut-off
+    // DEM: an external force per sphere in particle-id order (N; nullptr:
+    // none), found through the id of each sorted slot
+    const float4* ext_force;
+    const int* slot_ids;
+    float mass;         // particle mass (FP32)
 };
 
 // Runs f(std::integral_constant<int, B>) with B the tuned block size.
@@ -195,6 +200,12 @@ void launch_batch_decide(cudaStream_t st, int S, int min_it, int max_it, double 
 int launch_bnd_prepare(cudaStream_t st, const Params& P, int nb, const float4* raw, int* iota, uint32_t* keys[2],
                        uint32_t* vals[2], uint32_t* hist, int hist_blocks, int key_bits, float4* sorted, int* ids,
                        float* w, uint32_t* cell_start, uint32_t* cell_end, int* clamped);
+// The force the fluid exerts on each sorted boundary particle: minus the sum
+// of the mirrored-pressure forces the particle exerts on the fluid within h,
+// from the fluid's positions and committed pressures (sorted slots, cell
+// ranges of the last build). Written as float4 per boundary slot.
+void launch_bnd_reaction(cudaStream_t st, const Params& P, int nb, const float4* fluid_pos, const float2* fluid_rp,
+                         const uint32_t* cell_start, const uint32_t* cell_end, float4* force);
 // Per fluid slot: the boundary particles within the list cut-off, from a
 // 27-cell walk of the boundary's cell ranges (none outside P.bnd_lo/hi);
 // flags[0] is set when a slot has more than P.bnd_cap.

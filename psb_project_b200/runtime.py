@@ -41,7 +41,7 @@ EXPORTS = (
     "psb_batch_stats", "psb_set_graph", "psb_autotune", "psb_tune_set", "psb_tune_get", "psb_diagnostics",
     "psb_set_boundary", "psb_boundary_psi", "psb_context_info", "psb_set_step_count", "psb_write_txt",
     "psb_write_xml", "psb_write_vol", "psb_write_obj", "psb_export_txt", "psb_export_xml", "psb_checkpoint_save",
-    "psb_checkpoint_load",
+    "psb_checkpoint_load", "psb_boundary_forces", "psb_set_external_force",
 )
 MLP_PARAMS = 4673       # PSB_MLP_PARAMS
 MLP_IN, MLP_H = 6, 64
@@ -172,6 +172,8 @@ def lib():
         "psb_export_xml": ([P, ctypes.c_char_p], ctypes.c_int),
         "psb_checkpoint_save": ([P, ctypes.c_char_p], ctypes.c_int),
         "psb_checkpoint_load": ([P, ctypes.c_char_p], ctypes.c_int),
+        "psb_boundary_forces": ([P, P], ctypes.c_int),
+        "psb_set_external_force": ([P, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -458,6 +460,20 @@ class Simulation:
                     "psb_set_boundary")
         self.n_bnd = pos.shape[0]
 
+    def boundary_forces(self) -> np.ndarray:
+        """The fluid's force (N) on each boundary particle after the last step, (n_b, 3)."""
+        out = np.empty((self.n_bnd, 3), np.float32)
+        self._check(lib().psb_boundary_forces(self._h, _ptr(out)), "psb_boundary_forces")
+        return out
+
+    def set_external_force(self, force):
+        """DEM: external force per sphere (n, 3) in N, id order; None removes it."""
+        if force is None:
+            self._check(lib().psb_set_external_force(self._h, None), "psb_set_external_force")
+            return
+        f = np.ascontiguousarray(force, np.float32).reshape(-1, 3)
+        self._check(lib().psb_set_external_force(self._h, _ptr(f)), "psb_set_external_force")
+
     def boundary_psi(self) -> np.ndarray:
         out = np.empty(self.n_bnd, np.float32)
         self._check(lib().psb_boundary_psi(self._h, _ptr(out)), "psb_boundary_psi")
@@ -611,3 +627,28 @@ class BatchSimulation(Simulation):
 
 def batch_positions(scenes) -> np.ndarray:
     return np.concatenate([scene_positions(sc) for sc in scenes])
+
+
+class FluidDemCoupling:
+    """Two-way coupling of a config-profile SPH context and a DEM context
+    (config C1): every DEM sphere is one boundary particle of the fluid, at
+    its centre. One coupled step: the fluid steps with the spheres' current
+    positions as its boundary; the fluid's reaction on each sphere
+    (psb_boundary_forces) becomes the spheres' external force; the spheres
+    step. The sphere positions and forces cross the host (12 B each way per
+    sphere per step)."""
+
+    def __init__(self, fluid: Simulation, spheres: Simulation):
+        self.fluid = fluid
+        self.spheres = spheres
+        self.last_force = None
+
+    def step(self, nsteps: int = 1) -> int:
+        rc = OK
+        for _ in range(nsteps):
+            self.fluid.set_boundary(self.spheres.read_field(FIELD_POS))
+            rc = max(rc, self.fluid.step(1))
+            self.last_force = self.fluid.boundary_forces()
+            self.spheres.set_external_force(self.last_force)
+            self.spheres.step(1)
+        return rc

@@ -354,6 +354,20 @@ def batch_scenes(n_scenes: int = 64, seed: int = 3, n_range=(4096, 131072), spac
     return out
 
 
+def c1_scenes(fluid_n=(64, 64, 64), dem_n=(16, 16, 16), seed: int = 1):
+    """Config C1: the 262,144-particle PCISPH dam break (2 x 1 x 1 m box,
+    dt = 1e-3) and 4,096 DEM spheres (radius 0.01 m, density 2500 kg/m^3,
+    k_n = 1e4 N/m, restitution 0.3) on a 16^3 lattice of spacing 0.021 m
+    above the fluid block, same box and time step. Returns (fluid, spheres);
+    smaller counts give the same set-up at test size."""
+    fluid = dam_break(fluid_n, 0.01, (2.0, 1.0, 1.0), 0.02, dt=1e-3, mass=1e-3, seed=seed, steps=500,
+                      name="C1 PCISPH dam break %d" % (fluid_n[0] * fluid_n[1] * fluid_n[2]))
+    top = fluid_n[1] * 0.01
+    spheres = dem_block(dem_n, 0.021, (0.1, top + 0.02, 0.1), (2.0, 1.0, 1.0), 0.01, density=2500.0, k_n=1e4,
+                        restitution=0.3, dt=1e-3, seed=seed + 100, name="C1 DEM spheres")
+    return fluid, spheres
+
+
 def sphere_shell(centre, radius: float, spacing: float, layers: int = 2) -> np.ndarray:
     """Boundary particles of a solid sphere: the points of the cubic lattice
     of this spacing (aligned on the centre) whose distance to the centre lies
