@@ -365,6 +365,66 @@ int psb_boundary_forces(psb_ctx* ctx, float* force);
  * which has gravity and contacts only. */
 int psb_set_external_force(psb_ctx* ctx, const float* force);
 
+/* Collision objects: the reference's ObjectCollision subclasses
+ * (src/Kernel/Collision/*; Collision::collide, Collision.cpp:44-49), applied
+ * in list order after each step's integrator and box walls, to the start
+ * position, the new position and the new velocity (the half-step velocity
+ * of the SPH systems, SphSystem.cpp:323-328; the velocity of DEM,
+ * CudaSystem.cpp:253-257) before the velocity interpolation. Each object
+ * follows its reference kernel as it executes:
+ *  PLANE     PlaneCollision_Kernel.cu:7-81. v[0..11] corners A, B, C, D,
+ *            v[12..14] normal N. A particle behind the plane and within the
+ *            quad's extent on the axes N does not lie along goes to where
+ *            its motion crossed the plane; the velocity loses (1 + r) of its
+ *            normal part, r = elast |x - x_contact| / (dt |v|). A particle
+ *            that did not move is left alone (the reference divides by 0).
+ *  SPHERE    SphereCollision_Kernel.cu:7-91 through its launcher
+ *            (SphereCollision.cu:9-16), which passes dt and the container
+ *            flag in each other's place: the sphere (origin v[0..2], radius
+ *            v[3]) always keeps particles inside it, and the restitution
+ *            divides by 1 (container = 1) or 0 (container = 0, refused here
+ *            when elast > 0: the reference's velocities become non-finite).
+ *  CYLINDER  CylinderCollision_Kernel.cu:4-103: a container along the unit
+ *            axis v[3..5] about v[0..2], radius v[6] less 0.04, length v[7],
+ *            restitution 0.3 whatever elast says.
+ *  MESH      MeshCollision_Kernel.cu:14-137: count faces, data = count x 12
+ *            floats (A, B, C, N); the nearest face whose plane the particle
+ *            is behind and whose triangle holds the contact point; elast is
+ *            not used (0).
+ *  HEIGHT    Linear/Gaussian/PeriodicHeightFieldCollision_Kernel.cu: inside
+ *            the footprint v[0..2] (min) .. v[3..5] (max) in x and z, a
+ *            particle below y = h(x, z) + min.y is lifted to it; normals by
+ *            central differences (step 0.01). h is the sum of count terms,
+ *            data = count x 6 floats {kind, c0, c1, c2, c3, c4}:
+ *              PSB_HEIGHT_LINEAR    c0 x + c1 z
+ *              PSB_HEIGHT_GAUSSIAN  c0 exp(-((x-c1)^2/(2 c3^2) + (z-c2)^2/(2 c4^2)))
+ *              PSB_HEIGHT_COSINE    c0 cos(c1 (x cos c2 + z sin c2) + c3)
+ *            One term gives the reference's linear or Gaussian field, cosine
+ *            terms its periodic field, a mix its combined field (evaluated
+ *            here at the new position; the reference evaluates a combined
+ *            field at the start position).
+ * Single-scene contexts, every method and profile. data is host memory,
+ * copied. Replaces any earlier list; n = 0 removes it. */
+#define PSB_MAX_COLLIDERS 32
+#define PSB_MAX_COLLIDER_ITEMS 1048576      /* mesh faces or height terms per object */
+enum {
+    PSB_COLLIDER_PLANE = 1,
+    PSB_COLLIDER_SPHERE = 2,
+    PSB_COLLIDER_CYLINDER = 3,
+    PSB_COLLIDER_MESH = 4,
+    PSB_COLLIDER_HEIGHT = 5
+};
+enum { PSB_HEIGHT_LINEAR = 1, PSB_HEIGHT_GAUSSIAN = 2, PSB_HEIGHT_COSINE = 3 };
+typedef struct psb_collider {
+    int32_t type;        /* PSB_COLLIDER_* */
+    int32_t container;   /* sphere: the reference's is_container */
+    float elast;
+    int32_t count;       /* mesh: faces; height: terms */
+    float v[16];
+    const float* data;   /* mesh faces or height terms (host) */
+} psb_collider;
+int psb_set_colliders(psb_ctx* ctx, const psb_collider* objs, int32_t n);
+
 /* The scene the context was created with (for a batch: scene 0 with n_max
  * the total), the particle count of the last upload (0 before one) and the
  * steps taken; psb_set_step_count overwrites the step count (checkpoints). */

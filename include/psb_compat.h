@@ -98,6 +98,40 @@ void interactionSystem(double* oldPos, double* oldVel, double* forces, double* i
  * [Min + r, Max - r], remove the velocity along the summed wall normals */
 void collisionSystem_Box_CUDA(double* newPos, double* oldVel, double* newVel, float radiusParticle, float dt,
                               int nbBodiesP, psb_vec3 Min, psb_vec3 Max, bool container, float elast);
+/* The other collision objects, on (oldPos, newPos, newVel) in FP64 with the
+ * float arithmetic of their kernels (the formulas and the behaviours they
+ * keep are those of psb_set_colliders in psb.h):
+ * PlaneCollision.cu:9-21 / PlaneCollision_Kernel.cu:7-81 */
+void collisionPlan_CUDA(double* oldPos, double* newPos, double* oldVel, double* newVel, psb_vec3 A, psb_vec3 B,
+                        psb_vec3 C, psb_vec3 D, psb_vec3 N, float elast, float dt, int nbBodiesP);
+/* SphereCollision.cu:9-16 / SphereCollision_Kernel.cu:7-91 */
+void collisionSystem_Sphere_CUDA(double* oldPos, double* newPos, double* oldVel, double* newVel, float radiusParticle,
+                                 float dt, int nbBodies, psb_vec3 origin, float radius, float elast, bool container);
+/* CylinderCollision.cu:9-19 / CylinderCollision_Kernel.cu:4-103 */
+void collisionCylinder_CUDA(double* newPos, double* newVel, float radiusParticle, float dt, int nbBodiesP,
+                            psb_vec3 center, psb_vec3 direction, double radius, double length, float elast,
+                            bool container);
+/* MeshCollision.cu:8-18 / MeshCollision_Kernel.cu:14-137: fA, fB, fC, fN are
+ * device float arrays of 3 nbFaces (corners and normals) */
+void collisionMesh_CUDA(double* oldPos, double* newPos, double* oldVel, double* newVel, float radiusParticle, float dt,
+                        unsigned int nbFaces, float* fA, float* fB, float* fC, float* fN, float elast, int nbBodiesP);
+/* LinearHeightFieldCollision.cu:9-20: h = a x + b z */
+void collisionSystem_Linear_HeightFieldCollision_CUDA(double* oldPos, double* newPos, double* oldVel, double* newVel,
+                                                      double radiusParticle, float dt, unsigned int nbBodiesP,
+                                                      double a, double b, psb_vec3 Min, psb_vec3 Max, float elast);
+/* GaussianHeightFieldCollision.cu:9-21: h = A exp(-((x-x0)^2/(2 p1^2) + (z-z0)^2/(2 p2^2))) */
+void collisionSystem_Gaussian_HeightFieldCollision_CUDA(double* oldPos, double* newPos, double* oldVel,
+                                                        double* newVel, double radiusParticle, float dt,
+                                                        unsigned int nbBodiesP, double A, double x0, double z0,
+                                                        double p1, double p2, psb_vec3 Min, psb_vec3 Max,
+                                                        float elast);
+/* PeriodicHeightFieldCollision.cu:9-21: h = sum_i A_i cos(k_i (x cos theta_i
+ * + z sin theta_i) + phi_i), the four arrays on the device */
+void collisionSystem_Periodic_HeightFieldCollision_CUDA(double* oldPos, double* newPos, double* oldVel,
+                                                        double* newVel, double radiusParticle, float dt,
+                                                        unsigned int nbBodiesP, unsigned int nbFunc, double* A,
+                                                        double* k, double* theta, double* phi, psb_vec3 Min,
+                                                        psb_vec3 Max, float elast);
 /* PciSphSystem.cu:8-68: density, non-pressure forces, three pressure
  * corrections and the final leap-frog with the reference's formulas, run by
  * the B200 kernels (psb_step, reference profile) on a context that this

@@ -50,7 +50,39 @@ class OrcParams(ctypes.Structure):
         ("n_bnd", ctypes.c_int32), ("bnd_pos", ctypes.c_void_p), ("bnd_psi", ctypes.c_void_p),
         ("bnd_counts", ctypes.c_void_p), ("bnd_lists", ctypes.c_void_p), ("bnd_cap", ctypes.c_int32),
         ("dem_ext", ctypes.c_void_p),
+        ("n_coll", ctypes.c_int32), ("coll", ctypes.c_void_p),
     ]
+
+
+class OrcCollider(ctypes.Structure):
+    """orc_collider: one collision object as its reference kernel executes."""
+    _fields_ = [("type", ctypes.c_int32), ("container", ctypes.c_int32), ("elast", ctypes.c_float),
+                ("count", ctypes.c_int32), ("v", ctypes.c_float * 16), ("faces", ctypes.c_void_p),
+                ("terms", ctypes.c_void_p)]
+
+
+class Colliders:
+    """An orc_collider array plus the face and term arrays it points to.
+    Each object: (type, v (<= 16 floats), elast, container, faces (F x 12
+    float32) or None, terms (T x 6 float64) or None)."""
+
+    def __init__(self, objs):
+        self.arr = (OrcCollider * max(1, len(objs)))()
+        self.keep = []
+        for i, (typ, v, elast, container, faces, terms) in enumerate(objs):
+            o = self.arr[i]
+            o.type, o.container, o.elast = int(typ), int(bool(container)), float(elast)
+            vv = list(v) + [0.0] * (16 - len(v))
+            o.v[:] = [float(x) for x in vv]
+            if faces is not None:
+                f = np.ascontiguousarray(faces, np.float32).reshape(-1, 12)
+                self.keep.append(f)
+                o.faces, o.count = f.ctypes.data, f.shape[0]
+            if terms is not None:
+                t = np.ascontiguousarray(terms, np.float64).reshape(-1, 6)
+                self.keep.append(t)
+                o.terms, o.count = t.ctypes.data, t.shape[0]
+        self.n = len(objs)
 
 
 class OrcState(ctypes.Structure):
@@ -175,6 +207,8 @@ def lib():
         L.orc_pressure_force.restype = None
         L.orc_boundary_reaction.argtypes = [ctypes.POINTER(OrcParams), P, P, ctypes.c_int32, P, P, P]
         L.orc_boundary_reaction.restype = None
+        L.orc_collide.argtypes = [ctypes.POINTER(OrcCollider), ctypes.c_int32, P, P, P, ctypes.c_float]
+        L.orc_collide.restype = ctypes.c_int32
         _lib = L
     return _lib
 
@@ -204,6 +238,9 @@ def ref_lib():
         L.ref_iso.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, P]
         L.ref_marching_cubes.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int64,
                                          P, P]
+        L.ref_collide.argtypes = [ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                  ctypes.c_float, P, ctypes.c_int, P, P]
+        L.ref_collide.restype = ctypes.c_int
         _ref = L
     return _ref
 
@@ -321,10 +358,15 @@ def density(scene, pos, counts, lists, clamp) -> np.ndarray:
 class OracleSim:
     """FP64 state in particle-id order, stepped by orc_step."""
 
-    def __init__(self, scene, pos, vel=None, vel_half=None, pressure=None, *, float_state=False, boundary=None):
+    def __init__(self, scene, pos, vel=None, vel_half=None, pressure=None, *, float_state=False, boundary=None,
+                 colliders=None):
         n = pos.shape[0]
         self.scene = scene
         self.P = params(scene, float_state=float_state, n=n)
+        if colliders:                 # collision objects after the box (Colliders or its object list)
+            self.coll = colliders if isinstance(colliders, Colliders) else Colliders(colliders)
+            self.P.n_coll = self.coll.n
+            self.P.coll = ctypes.addressof(self.coll.arr)
         if boundary is not None:      # static boundary particles (config profile)
             self.bnd_pos = np.ascontiguousarray(boundary, np.float64)
             self.bnd_psi = boundary_psi(scene, self.bnd_pos)
@@ -366,6 +408,38 @@ class OracleSim:
         if rc != 0:
             raise RuntimeError(f"orc_step failed: {rc}")
         return self.stats
+
+
+def collide(obj, old_pos, pos, vel, dt):
+    """One collision object (a Colliders entry tuple) on FP64 copies of
+    (pos, vel); returns (pos, vel, hits)."""
+    c = Colliders([obj])
+    x = np.ascontiguousarray(pos, np.float64).copy()
+    v = np.ascontiguousarray(vel, np.float64).copy()
+    xo = np.ascontiguousarray(old_pos, np.float64)
+    hits = lib().orc_collide(ctypes.byref(c.arr[0]), x.shape[0], _ptr(xo), _ptr(x), _ptr(v), ctypes.c_float(dt))
+    return x, v, hits
+
+
+def ref_collide(obj, old_pos, pos, vel, dt, particle_radius=0.0):
+    """The same object through the reference's own kernel on the CPU
+    (oracle/_ref); returns (pos, vel)."""
+    typ, v, elast, container, faces, terms = obj
+    x = np.ascontiguousarray(pos, np.float64).copy()
+    u = np.ascontiguousarray(vel, np.float64).copy()
+    xo = np.ascontiguousarray(old_pos, np.float64).copy()
+    vv = np.zeros(16, np.float32)
+    vv[:len(v)] = v
+    f = None if faces is None else np.ascontiguousarray(faces, np.float32).reshape(-1, 12)
+    t = None if terms is None else np.ascontiguousarray(terms, np.float64).reshape(-1, 6)
+    count = f.shape[0] if f is not None else (t.shape[0] if t is not None else 0)
+    L = ref_lib()
+    rc = L.ref_collide(int(typ), x.shape[0], _ptr(xo), _ptr(x), _ptr(u), ctypes.c_float(dt), ctypes.c_float(elast),
+                       int(bool(container)), ctypes.c_float(particle_radius), _ptr(vv), count,
+                       None if f is None else _ptr(f), None if t is None else _ptr(t))
+    if rc != 0:
+        raise RuntimeError(f"ref_collide failed: {rc}")
+    return x, u
 
 
 class RefSim:

@@ -21,6 +21,8 @@
  *   PCISPH pressure force . PciSphSystem_Kernel.cu:88-114
  *   PCISPH sequence ....... .../PCISPH/PciSphSystem.cu:8-68, PciSphSystem.cpp:163-204
  *   box walls ............. src/Kernel/Collision/BoxCollision/BoxCollision_Kernel.cu:7-34
+ *   collision objects ..... src/Kernel/Collision/* (see orc_collide), after the box,
+ *                           Collision.cpp:44-49
  *   DEM contacts .......... src/Kernel/System/SimpleSystem/CudaParticle_Kernel.cu:10-55 (as executed,
  *                           see dem_pair_ref), integrateEuler ParticleKernel.cu:12-20,
  *                           sequence CudaSystem.cpp:207-224
@@ -566,6 +568,259 @@ static void box_project(const orc_params* P, double* x, double* v) {
     }
 }
 
+/* ---- collision objects ------------------------------------------------------
+ * Each object as its reference kernel executes, FP64 where the reference is
+ * FP64 and float where it computes in float (float3 temporaries, powf):
+ *   plane ..... src/Kernel/Collision/PlaneCollision/PlaneCollision_Kernel.cu:7-81
+ *   sphere .... SphereCollision/SphereCollision_Kernel.cu:7-91 with the launch of
+ *               SphereCollision.cu:9-16, which hands the kernel dt as its
+ *               `container` and the container flag as its dt
+ *   cylinder .. CylinderCollision/CylinderCollision_Kernel.cu:4-103
+ *   mesh ...... MeshCollision/MeshCollision_Kernel.cu:14-137
+ *   heights ... HeightField/{Linear,Gaussian,Periodic}/*HeightFieldCollision_Kernel.cu
+ * A plane particle that did not move is left alone (the reference divides
+ * by zero there). Squares the reference takes with powf are float products. */
+
+static inline float fsqf(float a) { return a * a; }
+static inline double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static inline float dot3f(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+/* v -= (1 + r) (v.n) n, r float */
+static void coll_reflect(double* v, const double* n, float r) {
+    const double k = (double)(1.f + r) * dot3(v, n);
+    for (int e = 0; e < 3; ++e) v[e] = v[e] - k * n[e];
+}
+
+static float coll_restitution(float elast, float dt, const double* x, const double* xc, const double* v) {
+    const double lv = len3(v);
+    if (lv > 0 && elast > 0) {
+        const double d[3] = {x[0] - xc[0], x[1] - xc[1], x[2] - xc[2]};
+        return (float)((double)elast * len3(d) / ((double)dt * lv));
+    }
+    return 0.f;
+}
+
+static int coll_plane(const orc_collider* o, float dt, const double* xo, double* x, double* v) {
+    const float* q = o->v;
+    const float* N = q + 12;
+    float lo[3] = {100000.f, 100000.f, 100000.f}, hi[3] = {-100000.f, -100000.f, -100000.f};
+    for (int c = 0; c < 4; ++c)
+        for (int a = 0; a < 3; ++a) {
+            if (lo[a] >= q[3 * c + a]) lo[a] = q[3 * c + a];
+            if (hi[a] <= q[3 * c + a]) hi[a] = q[3 * c + a];
+        }
+    for (int a = 0; a < 3; ++a) {
+        const float s = 1.f - N[a];
+        const double xa = x[a] * (double)s;
+        if (!(xa <= (double)(hi[a] * s) && xa >= (double)(lo[a] * s))) return 0;
+    }
+    float p1[3], ao[3], dir[3];
+    for (int a = 0; a < 3; ++a) {
+        p1[a] = (float)(x[a] - (double)q[a]);
+        ao[a] = (float)((double)q[a] - xo[a]);
+        dir[a] = (float)(x[a] - xo[a]);
+    }
+    if (!(dot3f(p1, N) <= 0.f)) return 0;
+    const float ao_n = dot3f(ao, N);
+    const float dn = sqrtf(dot3f(dir, dir));
+    if (!(dn > 0.f)) return 0;
+    for (int a = 0; a < 3; ++a) dir[a] = dir[a] / dn;
+    const float t = ao_n / dot3f(dir, N);
+    double xc[3], n[3];
+    for (int a = 0; a < 3; ++a) xc[a] = xo[a] + (double)(t * dir[a]);
+    const float r = coll_restitution(o->elast, dt, x, xc, v);
+    const double nw[3] = {N[0], N[1], N[2]};
+    const double ln = len3(nw);
+    for (int a = 0; a < 3; ++a) n[a] = nw[a] / ln;
+    for (int a = 0; a < 3; ++a) x[a] = xc[a];
+    coll_reflect(v, n, r);
+    return 1;
+}
+
+static int coll_sphere(const orc_collider* o, float dt, double* x, double* v) {
+    const int inside = dt != 0.f;
+    const float dt_k = o->container ? 1.f : 0.f;
+    const double c[3] = {o->v[0], o->v[1], o->v[2]};
+    const double R = (double)o->v[3];
+    const double op[3] = {x[0] - c[0], x[1] - c[1], x[2] - c[2]};
+    const double d = len3(op);
+    double xc[3], n[3];
+    if ((inside && d == R) || (!inside && d == R)) {
+        const double rd = 1.0f / d;          /* double3.h operator/: times the reciprocal */
+        for (int a = 0; a < 3; ++a) { xc[a] = x[a]; n[a] = -op[a] * rd; }
+    } else if (inside && d > R) {
+        const double rd = 1.0f / d;
+        for (int a = 0; a < 3; ++a) xc[a] = c[a] + (op[a] * rd) * R;
+        const double w[3] = {c[0] - xc[0], c[1] - xc[1], c[2] - xc[2]};
+        const double rl = 1.0f / len3(w);
+        for (int a = 0; a < 3; ++a) n[a] = w[a] * rl;
+    } else {
+        return 0;
+    }
+    const float r = coll_restitution(o->elast, dt_k, x, xc, v);
+    const double ln = len3(n);
+    for (int a = 0; a < 3; ++a) n[a] = n[a] / ln;
+    for (int a = 0; a < 3; ++a) x[a] = xc[a];
+    coll_reflect(v, n, r);
+    return 1;
+}
+
+static double fdist3(const double* a, const double* b) {
+    return (double)sqrtf(fsqf((float)(a[0] - b[0])) + fsqf((float)(a[1] - b[1])) + fsqf((float)(a[2] - b[2])));
+}
+
+static int coll_cylinder(const orc_collider* o, float dt, double* x, double* v) {
+    const float* ce = o->v;
+    const float* di = o->v + 3;
+    const float rb = o->v[6], l = o->v[7];
+    double p1[3], p2[3], C[3], cd[3], xc[3] = {x[0], x[1], x[2]}, n[3];
+    for (int a = 0; a < 3; ++a) {
+        p1[a] = (double)(ce[a] + di[a] * (l / 2));
+        p2[a] = (double)(ce[a] - di[a] * (l / 2));
+        cd[a] = (double)ce[a];
+    }
+    C[0] = (double)ce[0] + x[0] * (double)di[0];
+    C[1] = (double)ce[1] + x[1] * (double)di[1];
+    C[2] = (double)ce[2] + x[2] * (double)di[0];    /* the reference's z takes direction.x */
+    const double margin = (double)rb - 0.04;
+    const float dl = sqrtf(fsqf(di[0]) + fsqf(di[1]) + fsqf(di[2]));
+    const double w[3] = {C[0] - x[0], C[1] - x[1], C[2] - x[2]};
+    const double lw = len3(w);
+    if (fdist3(cd, C) >= (double)(l / 2)) {
+        const int low = fdist3(p1, C) > fdist3(p2, C);   /* nearer the P2 end */
+        const double* pe = low ? p2 : p1;
+        double u[3];
+        for (int a = 0; a < 3; ++a) u[a] = low ? w[a] / lw : -w[a] / lw;
+        for (int a = 0; a < 3; ++a)
+            if (di[a] != 0.f) xc[a] = pe[a];
+        if (lw >= (double)rb)
+            for (int a = 0; a < 3; ++a)
+                if (di[a] == 0.f) xc[a] = low ? C[a] - margin * u[a] : C[a] + margin * u[a];
+        for (int a = 0; a < 3; ++a) n[a] = (double)(low ? di[a] : -di[a]) / (double)dl;
+    } else {
+        if (!(fdist3(C, x) >= (double)rb)) return 0;
+        for (int a = 0; a < 3; ++a) {
+            n[a] = -w[a] / lw;
+            xc[a] = C[a] + margin * n[a] * (double)(1.f - di[a]);
+        }
+    }
+    float r = 0.f;
+    const double lv = len3(v);
+    if (lv > 0 && dt > 0.f) {
+        const double d[3] = {x[0] - xc[0], x[1] - xc[1], x[2] - xc[2]};
+        r = (float)((double)0.3f * len3(d) / ((double)dt * lv));
+    }
+    for (int a = 0; a < 3; ++a) x[a] = xc[a];
+    coll_reflect(v, n, r);
+    return 1;
+}
+
+static int in_triangle(const float* A, const float* B, const float* Cc, const float* P) {
+    float u[3], w[3], p[3];
+    for (int a = 0; a < 3; ++a) { u[a] = B[a] - A[a]; w[a] = Cc[a] - A[a]; p[a] = P[a] - A[a]; }
+    const float uu = dot3f(u, u), uw = dot3f(u, w), ww = dot3f(w, w), pu = dot3f(p, u), pw = dot3f(p, w);
+    const float D = uw * uw - uu * ww;
+    const float s = (uw * pw - ww * pu) / D;
+    if (s < 0.f || s > 1.f) return 0;
+    const float t = (uw * pu - uu * pw) / D;
+    if (t < 0.f || (s + t) > 1.f) return 0;
+    return 1;
+}
+
+static int coll_mesh(const orc_collider* o, const double* xo, double* x, double* v) {
+    double best = 10000000, xb[3] = {x[0], x[1], x[2]}, nb[3] = {0, 0, 0};
+    int found = 0;
+    for (int32_t f = 0; f < o->count; ++f) {
+        const float* A = o->faces + 12 * (size_t)f;
+        const float* N = A + 9;
+        const double Nd[3] = {N[0], N[1], N[2]};
+        const double p1[3] = {x[0] - A[0], x[1] - A[1], x[2] - A[2]};
+        const double d1 = dot3(p1, Nd);
+        if (!(d1 <= 0)) continue;
+        const double dir0[3] = {xo[0] - x[0], xo[1] - x[1], xo[2] - x[2]};
+        const double dn = len3(dir0);
+        double xc[3];
+        if (d1 == 0 || dn <= 0 || d1 == -1) {
+            for (int a = 0; a < 3; ++a) xc[a] = x[a];
+        } else {
+            const double ao[3] = {A[0] - x[0], A[1] - x[1], A[2] - x[2]};
+            const double ao_n = dot3(ao, Nd);
+            const double dir[3] = {dir0[0] / dn, dir0[1] / dn, dir0[2] / dn};
+            const double t = ao_n / dot3(dir, Nd);
+            for (int a = 0; a < 3; ++a) xc[a] = xo[a] + t * dir[a];
+            const float pf[3] = {(float)xc[0], (float)xc[1], (float)xc[2]};
+            if (!in_triangle(A, A + 3, A + 6, pf)) continue;
+        }
+        const double dist = fdist3(x, xc);
+        if (dist <= best) {
+            best = dist;
+            for (int a = 0; a < 3; ++a) { xb[a] = xc[a]; nb[a] = Nd[a]; }
+            found = 1;
+        }
+    }
+    if (!found) return 0;
+    for (int a = 0; a < 3; ++a) x[a] = xb[a];
+    coll_reflect(v, nb, 0.f);
+    return 1;
+}
+
+static double height_of(const orc_collider* o, double x, double z) {
+    double y = 0;
+    for (int32_t i = 0; i < o->count; ++i) {
+        const double* c = o->terms + 6 * (size_t)i;
+        const int kind = (int)c[0];
+        if (kind == 1) y += c[1] * x + c[2] * z;
+        else if (kind == 2)
+            y += c[1] * exp(-((double)fsqf((float)(x - c[2])) / (2 * c[4] * c[4]) +
+                              (double)fsqf((float)(z - c[3])) / (2 * c[5] * c[5])));
+        else y += c[1] * cos(c[2] * (x * cos(c[3]) + z * sin(c[3])) + c[4]);
+    }
+    return y;
+}
+
+static int coll_height(const orc_collider* o, float dt, double* x, double* v) {
+    const float* q = o->v;
+    if (!(x[0] >= (double)q[0] && x[2] >= (double)q[2] && x[0] <= (double)q[3] && x[2] <= (double)q[5])) return 0;
+    const double y = height_of(o, x[0], x[2]) + (double)q[1];
+    if (!(y >= x[1])) return 0;
+    const double xc[3] = {x[0], y, x[2]};
+    const float r = coll_restitution(o->elast, dt, x, xc, v);
+    const double d = 0.01;
+    const double dpx = (height_of(o, xc[0] + d, xc[2]) - height_of(o, xc[0] - d, xc[2])) / (2 * d);
+    const double dpz = (height_of(o, xc[0], xc[2] + d) - height_of(o, xc[0], xc[2] - d)) / (2 * d);
+    const double nn = sqrt(dpx * dpx + 1.0 + dpz * dpz);
+    double n[3] = {-dpx / nn, 1.0 / nn, -dpz / nn};
+    const double ln = len3(n);
+    for (int a = 0; a < 3; ++a) n[a] = n[a] / ln;
+    x[1] = y;
+    coll_reflect(v, n, r);
+    return 1;
+}
+
+static int collide_one(const orc_collider* o, float dt, const double* xo, double* x, double* v) {
+    switch (o->type) {
+        case 1: return coll_plane(o, dt, xo, x, v);
+        case 2: return coll_sphere(o, dt, x, v);
+        case 3: return coll_cylinder(o, dt, x, v);
+        case 4: return coll_mesh(o, xo, x, v);
+        case 5: return coll_height(o, dt, x, v);
+        default: return 0;
+    }
+}
+
+int32_t orc_collide(const orc_collider* o, int32_t n, const double* old_pos, double* pos, double* vel, float dt) {
+    int32_t hits = 0;
+#pragma omp parallel for schedule(static) reduction(+ : hits)
+    for (int32_t i = 0; i < n; ++i)
+        hits += collide_one(o, dt, old_pos ? &old_pos[3 * i] : &pos[3 * i], &pos[3 * i], &vel[3 * i]);
+    return hits;
+}
+
+/* Every object of P's list on one particle, after the box. */
+static void collide_all(const orc_params* P, const double* xo, double* x, double* v) {
+    for (int32_t k = 0; k < P->n_coll; ++k) collide_one(&P->coll[k], P->dt, xo, x, v);
+}
+
 /* ---- steps ---------------------------------------------------------------- */
 
 static int32_t* build_lists(const orc_params* P, const double* pos, int32_t* counts, int32_t* cap_out, orc_stats* st) {
@@ -643,6 +898,7 @@ static int step_wcsph(const orc_params* P, orc_state* S, orc_stats* st, double* 
         double aw[3] = {0, 0, 0};
         if (!ref) wall_accel(P, x, vap, aw);
         const double vav[3] = {vap[0], vap[1], vap[2]};
+        const double xo[3] = {x[0], x[1], x[2]};
         const double inv = 1.0 / rho[i];
         for (int e = 0; e < 3; ++e) {
             /* internalForces accumulates visc + surf + press, then the force
@@ -652,6 +908,7 @@ static int step_wcsph(const orc_params* P, orc_state* S, orc_stats* st, double* 
             x[e] = RND(P, x[e] + vap[e] * dt);
         }
         if (ref) box_project(P, x, vap);   /* config WCSPH: penalty walls only */
+        collide_all(P, xo, x, vap);
         for (int e = 0; e < 3; ++e) {
             x[e] = RND(P, x[e]);
             vap[e] = RND(P, vap[e]);
@@ -765,8 +1022,10 @@ static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double*
         double* x = &S->pos[3 * i];
         double* vap = &S->vel_ap[3 * i];
         const double vav[3] = {vap[0], vap[1], vap[2]};
+        const double xo[3] = {x[0], x[1], x[2]};
         for (int e = 0; e < 3; ++e) { x[e] = xs[3 * i + e]; vap[e] = vs[3 * i + e]; }
         box_project(P, x, vap);
+        collide_all(P, xo, x, vap);
         for (int e = 0; e < 3; ++e) {
             x[e] = RND(P, x[e]);
             vap[e] = RND(P, vap[e]);
@@ -871,11 +1130,13 @@ static int step_dem(const orc_params* P, orc_state* S, orc_stats* st, double* f_
         double* x = &S->pos[3 * i];
         double* v = &S->vel[3 * i];
         const double v0[3] = {v[0], v[1], v[2]};
+        const double xo[3] = {x[0], x[1], x[2]};
         for (int e = 0; e < 3; ++e) {
             v[e] = RND(P, v[e] + (f[3 * i + e] / P->mass) * dt);
             x[e] = RND(P, x[e] + (ref ? v0[e] : v[e]) * dt);
         }
         box_project(P, x, v);    /* collisionBox on (pos, vel), CudaSystem::collide */
+        collide_all(P, xo, x, v);
         for (int e = 0; e < 3; ++e) {
             x[e] = RND(P, x[e]);
             v[e] = RND(P, v[e]);

@@ -52,7 +52,32 @@ typedef struct orc_params {
     int32_t bnd_cap;
     /* DEM: an external force per sphere (n * 3, N; NULL: none) */
     const double* dem_ext;
+    /* collision objects applied after the box walls, in order (orc_collide) */
+    int32_t n_coll;
+    const struct orc_collider* coll;
 } orc_params;
+
+/* One collision object of the reference (src/Kernel/Collision/*), as its
+ * kernel executes. type 1 plane, 2 sphere, 3 cylinder, 4 mesh, 5 height
+ * field; v[] as psb_collider's (include/psb.h). faces: count x 12 floats
+ * (A, B, C, N); terms: count x 6 doubles {kind, c0..c4}, kind 1 linear
+ * c0 x + c1 z, 2 Gaussian c0 exp(-((x-c1)^2/(2 c3^2) + (z-c2)^2/(2 c4^2)))
+ * with the squares in float as the reference's powf, 3 cosine
+ * c0 cos(c1 (x cos c2 + z sin c2) + c3). */
+typedef struct orc_collider {
+    int32_t type;
+    int32_t container;
+    float elast;
+    int32_t count;
+    float v[16];
+    const float* faces;
+    const double* terms;
+} orc_collider;
+
+/* Applies one object to n particles: old_pos the start positions (plane
+ * and mesh read them), pos and vel (n x 3) updated where the object acts.
+ * dt is the system's time step. Returns the number of particles moved. */
+int32_t orc_collide(const orc_collider* o, int32_t n, const double* old_pos, double* pos, double* vel, float dt);
 
 /* The force the fluid (n particles at pos with pressures p) exerts on each
  * boundary particle: minus the sum over fluid particles i within h of

@@ -54,6 +54,30 @@ void collisionBox(int nbBodies, double3* newPos, double3* oldVel, double3* newVe
                   float elast, bool container, float radiusParticles, float dt);
 void evaluate_force_constante(uint nbBodies, double3* accumForceBuff, double* mass, float3 direction, float amplitude);
 void integrateEuler(uint nbBodies, double3* newPos, double3* newVel, double3* forces, double* mass, float dt);
+/* The collision objects' kernels (src/Kernel/Collision/*), C++ linkage
+ * where their headers have no extern "C". */
+void collisionPlan(uint nbBodies, double3* newPos, double3* newVel, double3* oldPos, double3* oldVel, float3 A,
+                   float3 B, float3 C, float3 D, float3 N, float elast, float dt);
+void collisionSphere(uint nbBodies, double3* newPos, double3* newVel, double3* oldPos, double3* oldVel, float3 origin,
+                     float radius, float elast, bool container, float dt);
+void collisionCylinder(int nbBodies, double3* newPos, double3* newVel, float radiusParticle, float dt, float elast,
+                       bool container, float3 center, float baseRadius, float length, float3 direction);
+extern "C" void collisionTriangle(uint nbBodies, uint nbFaces, double3* newPos, double3* newVel, double3* oldPos,
+                                  double3* oldVel, float* AF, float* BF, float* CF, float* NF, float elast,
+                                  float radiusParticle, float dt);
+extern "C" void collisionSystem_Linear_HeightFieldCollision_Kernel(double3* newPos, double3* newVel,
+                                                                   double radiusParticle, float dt, uint nbBodiesP,
+                                                                   double a, double b, float3 min_, float3 max_,
+                                                                   float elast);
+extern "C" void collisionSystem_Gaussian_HeightFieldCollision_Kernel(double3* newPos, double3* newVel,
+                                                                     double radiusParticle, float dt, uint nbBodiesP,
+                                                                     double A, double x0, double z0, double p1,
+                                                                     double p2, float3 min_, float3 max_, float elast);
+extern "C" void collisionSystem_Periodic_HeightFieldCollision_Kernel(double3* newPos, double3* newVel,
+                                                                     double radiusParticle, float dt, uint nbBodiesP,
+                                                                     uint nbFunc, double* A, double* k, double* theta,
+                                                                     double* phi, float3 min_, float3 max_,
+                                                                     float elast);
 /* MarchingCube_Kernel.cu:36 (its header also defines the case tables, which
  * that file's object already holds) */
 extern "C" void polygonize_MarchingCube_Kernel(double4* grid, uint nbCellsX, uint nbCellsY, uint nbCellsZ,
@@ -440,6 +464,76 @@ int ref_marching_cubes(const double* nodes4, int nx, int ny, int nz, double leve
             }
     *nv = k;
     return k > cap ? -1 : 0;
+}
+
+/* One collision object on n particles, through the launch its reference
+ * launcher makes (PlaneCollision.cu:9-21, SphereCollision.cu:9-16 -- its
+ * argument order included, CylinderCollision.cu:9-19, MeshCollision.cu:8-18,
+ * Linear/Gaussian/PeriodicHeightFieldCollision.cu:9-21). v[] and the layouts
+ * of faces (count x 12 floats) and terms (count x 6 doubles) are
+ * orc_collider's. A height object is one linear term, one Gaussian term or
+ * cosine terms only (the reference's three kernels). */
+int ref_collide(int type, int n, double* old_pos, double* pos, double* vel, float dt, float elast, int container,
+                float particle_radius, const float* v, int count, const float* faces, const double* terms) {
+    if (n <= 0) return 0;
+    double3* np = (double3*)pos;
+    double3* nv = (double3*)vel;
+    double3* op = (double3*)old_pos;
+    auto f3 = [](const float* a) { return make_float3(a[0], a[1], a[2]); };
+    if (type == 1) {
+        launch1d(n, true, [&] { collisionPlan(n, np, nv, op, nv, f3(v), f3(v + 3), f3(v + 6), f3(v + 9), f3(v + 12), elast, dt); });
+    } else if (type == 2) {
+        const float3 O = f3(v);
+        const float radius = v[3];
+        const bool cont = container != 0;
+        launch1d(n, true, [&] { collisionSphere(n, np, nv, op, nv, O, radius, elast, dt, cont); });
+    } else if (type == 3) {
+        launch1d(n, true, [&] {
+            collisionCylinder(n, np, nv, particle_radius, dt, elast, container != 0, f3(v), v[6], v[7], f3(v + 3));
+        });
+    } else if (type == 4) {
+        std::vector<float> fa(3 * (size_t)count), fb(fa.size()), fc(fa.size()), fn(fa.size());
+        for (int f = 0; f < count; ++f)
+            for (int a = 0; a < 3; ++a) {
+                fa[3 * f + a] = faces[12 * f + a];
+                fb[3 * f + a] = faces[12 * f + 3 + a];
+                fc[3 * f + a] = faces[12 * f + 6 + a];
+                fn[3 * f + a] = faces[12 * f + 9 + a];
+            }
+        launch1d(n, true, [&] {
+            collisionTriangle(n, (uint)count, np, nv, op, nv, fa.data(), fb.data(), fc.data(), fn.data(), elast,
+                              particle_radius, dt);
+        });
+    } else if (type == 5) {
+        const float3 mn = f3(v), mx = f3(v + 3);
+        const int kind = (int)terms[0];
+        if (kind == 1 && count == 1) {
+            launch1d(n, true, [&] {
+                collisionSystem_Linear_HeightFieldCollision_Kernel(np, nv, particle_radius, dt, n, terms[1], terms[2],
+                                                                   mn, mx, elast);
+            });
+        } else if (kind == 2 && count == 1) {
+            launch1d(n, true, [&] {
+                collisionSystem_Gaussian_HeightFieldCollision_Kernel(np, nv, particle_radius, dt, n, terms[1],
+                                                                     terms[2], terms[3], terms[4], terms[5], mn, mx,
+                                                                     elast);
+            });
+        } else {
+            std::vector<double> A(count), k(count), th(count), ph(count);
+            for (int i = 0; i < count; ++i) {
+                if ((int)terms[6 * i] != 3) return -2;
+                A[i] = terms[6 * i + 1]; k[i] = terms[6 * i + 2]; th[i] = terms[6 * i + 3]; ph[i] = terms[6 * i + 4];
+            }
+            launch1d(n, true, [&] {
+                collisionSystem_Periodic_HeightFieldCollision_Kernel(np, nv, particle_radius, dt, n, (uint)count,
+                                                                     A.data(), k.data(), th.data(), ph.data(), mn,
+                                                                     mx, elast);
+            });
+        }
+    } else {
+        return -1;
+    }
+    return 0;
 }
 
 }  /* extern "C" */

@@ -22,6 +22,7 @@
 
 #include "psb.h"
 #include "psb_internal.cuh"
+#include "colliders.cuh"
 
 using psb::Params;
 
@@ -151,6 +152,10 @@ struct psb_ctx {
     // DEM: external force per sphere (psb_set_external_force), id order
     float4* ext_force = nullptr;
     float4* bnd_force = nullptr;    // boundary reaction scratch (psb_boundary_forces)
+    // collision objects (psb_set_colliders): the device list and each
+    // object's mesh faces or height terms
+    psb::Collider* d_coll = nullptr;
+    std::vector<float*> coll_data;
     long long bnd_force_cap = 0;
     // static boundary particles (psb_set_boundary); bnd_n == 0: none
     int bnd_n = 0, bnd_res = 0;
@@ -253,6 +258,8 @@ void free_all(psb_ctx* c) {
     for (int i = 0; i < 2; ++i) { cudaFree(c->bnd_keys[i]); cudaFree(c->bnd_vals[i]); }
     cudaFree(c->bnd_hist); cudaFree(c->bnd_cs); cudaFree(c->bnd_ce); cudaFree(c->bnd_count); cudaFree(c->bnd_list);
     cudaFree(c->ext_force); cudaFree(c->bnd_force);
+    cudaFree(c->d_coll);
+    for (float* d : c->coll_data) cudaFree(d);
     cudaFreeHost(c->h_loop); cudaFreeHost(c->h_err_sh);
     for (auto& g : c->gexec) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -694,6 +701,10 @@ int step_once(psb_ctx* c, bool last) {
             psb::launch_dem_step(st, P, c->pos[s], c->vel[s], c->nbr_count, c->nbr_list, c->pos[o], c->vel[o], c->vap[o],
                                  c->fnp);
         });
+        if (P.n_coll > 0)
+            timed(c, "colliders", [&] {
+                psb::launch_apply_colliders(st, P, c->pos[s], nullptr, c->pos[o], c->vel[o], c->vap[o]);
+            });
         c->cs = o;
         c->stats.iters = 0;
         c->stats.converged = 1;
@@ -703,6 +714,10 @@ int step_once(psb_ctx* c, bool last) {
             psb::launch_wcsph_force(st, P, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list,
                                     c->pos[o], c->vel[o], c->vap[o], c->fnp);
         });
+        if (P.n_coll > 0)
+            timed(c, "colliders", [&] {
+                psb::launch_apply_colliders(st, P, c->pos[s], c->vap[s], c->pos[o], c->vel[o], c->vap[o]);
+            });
         c->cs = o;
         c->stats.iters = 0;
         c->stats.converged = 1;
@@ -1496,6 +1511,112 @@ int psb_set_external_force(psb_ctx* c, const float* force) {
     k_pack3<<<blocks(n), psb::kBlock, 0, st>>>(n, stage, c->ext_force);
     c->P.ext_force = c->ext_force;
     return cuda_check(c, cudaGetLastError(), "external force");
+}
+
+namespace {
+
+// Why an object cannot be taken, or "".
+std::string collider_problem(const psb_collider& o) {
+    const int items = o.type == PSB_COLLIDER_MESH ? 12 : o.type == PSB_COLLIDER_HEIGHT ? 6 : 0;
+    for (float x : o.v)
+        if (!std::isfinite(x)) return "non-finite parameter";
+    if (!std::isfinite(o.elast)) return "non-finite elast";
+    switch (o.type) {
+        case PSB_COLLIDER_PLANE:
+        case PSB_COLLIDER_CYLINDER:
+            return "";
+        case PSB_COLLIDER_SPHERE:
+            if (!o.container && o.elast > 0.f)
+                return "a sphere with container = 0 and elast > 0 (the reference's restitution divides by zero)";
+            return "";
+        case PSB_COLLIDER_MESH:
+        case PSB_COLLIDER_HEIGHT:
+            if (o.count < 1 || o.count > PSB_MAX_COLLIDER_ITEMS || !o.data) return "count or data out of range";
+            for (long long i = 0; i < (long long)o.count * items; ++i)
+                if (!std::isfinite(o.data[i])) return "non-finite face or term";
+            if (o.type == PSB_COLLIDER_HEIGHT)
+                for (int i = 0; i < o.count; ++i) {
+                    const float k = o.data[6 * i];
+                    if (k != PSB_HEIGHT_LINEAR && k != PSB_HEIGHT_GAUSSIAN && k != PSB_HEIGHT_COSINE)
+                        return "unknown height term kind";
+                }
+            return "";
+        default:
+            return "unknown type";
+    }
+}
+
+void drop_colliders(psb_ctx* c) {
+    cudaFree(c->d_coll);
+    c->d_coll = nullptr;
+    for (float* d : c->coll_data) cudaFree(d);
+    c->coll_data.clear();
+    c->P.coll = nullptr;
+    c->P.n_coll = 0;
+}
+
+}  // namespace
+
+int psb_set_colliders(psb_ctx* c, const psb_collider* objs, int32_t n) {
+    if (!c) return PSB_EINVAL;
+    if (n < 0 || n > PSB_MAX_COLLIDERS || (n > 0 && !objs))
+        return fail(c, PSB_EINVAL, "psb_set_colliders: bad argument");
+    if (n > 0 && c->batch) return fail(c, PSB_EINVAL, "psb_set_colliders: single-scene contexts only");
+    for (int i = 0; i < n; ++i) {
+        const std::string why = collider_problem(objs[i]);
+        if (!why.empty()) return fail(c, PSB_EINVAL, "psb_set_colliders: object " + std::to_string(i) + ": " + why);
+    }
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    release_graphs(c);
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "colliders"));   // no step still reads the old list
+    drop_colliders(c);
+    if (n == 0) return PSB_OK;
+    std::vector<psb::Collider> h((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        const psb_collider& o = objs[i];
+        psb::Collider& d = h[(size_t)i];
+        d = psb::Collider{};
+        d.type = o.type;
+        d.flag = o.container ? 1 : 0;
+        d.elast = o.elast;
+        d.count = o.count;
+        std::memcpy(d.v, o.v, sizeof d.v);
+        if (o.type == PSB_COLLIDER_MESH || o.type == PSB_COLLIDER_HEIGHT) {
+            const size_t m = (size_t)o.count * (o.type == PSB_COLLIDER_MESH ? 12 : 6);
+            float* buf = nullptr;
+            int rc = dalloc(c, &buf, m);
+            if (rc == PSB_OK) {
+                c->coll_data.push_back(buf);
+                rc = cuda_check(c, cudaMemcpyAsync(buf, o.data, sizeof(float) * m, cudaMemcpyHostToDevice, st),
+                                "colliders");
+            }
+            if (rc != PSB_OK) {
+                cudaStreamSynchronize(st);
+                drop_colliders(c);
+                return rc;
+            }
+            if (o.type == PSB_COLLIDER_MESH) {
+                d.fa = buf; d.fb = buf + 3; d.fc = buf + 6; d.fn = buf + 9;
+                d.stride = 12;
+            } else {
+                d.terms = buf;
+            }
+        }
+    }
+    int rc = dalloc(c, &c->d_coll, (size_t)n);
+    if (rc == PSB_OK)
+        rc = cuda_check(c, cudaMemcpyAsync(c->d_coll, h.data(), sizeof(psb::Collider) * h.size(), cudaMemcpyHostToDevice,
+                                           st), "colliders");
+    if (rc == PSB_OK) rc = cuda_check(c, cudaStreamSynchronize(st), "colliders");
+    if (rc != PSB_OK) {
+        cudaStreamSynchronize(st);
+        drop_colliders(c);
+        return rc;
+    }
+    c->P.coll = c->d_coll;
+    c->P.n_coll = n;
+    return PSB_OK;
 }
 
 int psb_boundary_psi(psb_ctx* c, float* psi) {

@@ -49,6 +49,8 @@ struct Tune {
 
 // Uniform per-scene constants, FP32 in normalised form (q = r^2/h^2, u = r/h)
 // so that no intermediate leaves FP32 range; derived on the host in FP64.
+struct Collider;     // colliders.cuh
+
 struct Params {
     int n;
     int cap;            // neighbour slots per particle
@@ -105,6 +107,10 @@ struct Params {
     const float4* ext_force;
     const int* slot_ids;
     float mass;         // particle mass (FP32)
+    // Collision objects applied after the integrator and the box, in order
+    // (colliders.cuh); n_coll == 0: none. Single-scene contexts only.
+    const Collider* coll;
+    int n_coll;
 };
 
 // Runs f(std::integral_constant<int, B>) with B the tuned block size.
@@ -204,6 +210,12 @@ int launch_bnd_prepare(cudaStream_t st, const Params& P, int nb, const float4* r
 // of the mirrored-pressure forces the particle exerts on the fluid within h,
 // from the fluid's positions and committed pressures (sorted slots, cell
 // ranges of the last build). Written as float4 per boundary slot.
+// Collision objects on the integrator's output (WCSPH and DEM; the PCISPH
+// commit applies them itself). x_old: the step's start positions. vh_old
+// (WCSPH): the start half-step velocities, for v = (vh_old + vap)/2; null
+// (DEM): vel and vap both take the new velocity.
+void launch_apply_colliders(cudaStream_t st, const Params& P, const float4* x_old, const float4* vh_old, float4* pos,
+                            float4* vel, float4* vap);
 void launch_bnd_reaction(cudaStream_t st, const Params& P, int nb, const float4* fluid_pos, const float2* fluid_rp,
                          const uint32_t* cell_start, const uint32_t* cell_end, float4* force);
 // Per fluid slot: the boundary particles within the list cut-off, from a

@@ -27,6 +27,7 @@
 // predictor that writes x*, v* to separate buffers and leaves the state
 // alone; the final leap-frog is the last prediction committed.
 #include "psb_internal.cuh"
+#include "colliders.cuh"
 
 namespace psb {
 
@@ -624,8 +625,9 @@ __global__ void __launch_bounds__(BS) k_pci_force_predict(Params P, const float4
     rp[t] = ri;
 }
 
-// Commit of the last prediction, walls, velocity interpolation.
-template <bool BATCH>
+// Commit of the last prediction, walls, collision objects (COLL: the start
+// position pos[t] is read before it is overwritten), velocity interpolation.
+template <bool BATCH, bool COLL>
 __global__ void __launch_bounds__(kBlock) k_pci_commit(Params P, const float4* __restrict__ xs,
                                                        const float4* __restrict__ vs, const float2* __restrict__ rpc,
                                                        int have_density_pass, float4* __restrict__ pos,
@@ -636,6 +638,13 @@ __global__ void __launch_bounds__(kBlock) k_pci_commit(Params P, const float4* _
     float3 x = f3(xs[t]), v = f3(vs[t]);
     const float4 vh = vap[t];
     box_project<BATCH>(P, t, x, v);
+    if constexpr (COLL) {
+        const float4 x0 = pos[t];
+        coll::V3<float> cx{x.x, x.y, x.z}, cv{v.x, v.y, v.z};
+        coll::apply_colliders(P.coll, P.n_coll, P.dt, coll::V3<float>{x0.x, x0.y, x0.z}, cx, cv);
+        x = make_float3(cx.x, cx.y, cx.z);
+        v = make_float3(cv.x, cv.y, cv.z);
+    }
     pos[t] = make_float4(x.x, x.y, x.z, 0.f);
     vap[t] = make_float4(v.x, v.y, v.z, 0.f);
     vel[t] = make_float4((vh.x + v.x) * 0.5f, (vh.y + v.y) * 0.5f, (vh.z + v.z) * 0.5f, 0.f);
@@ -759,8 +768,10 @@ void launch_pci_commit(cudaStream_t st, const Params& P, const float4* xs, const
                        int have_density_pass, float4* pos, float4* vel, float4* vap, float2* rp) {
     if (P.n <= 0) return;
     if (P.scenes)
-        k_pci_commit<true><<<grid_of(P.n), kBlock, 0, st>>>(P, xs, vs, rpc, have_density_pass, pos, vel, vap, rp);
-    else k_pci_commit<false><<<grid_of(P.n), kBlock, 0, st>>>(P, xs, vs, rpc, have_density_pass, pos, vel, vap, rp);
+        k_pci_commit<true, false><<<grid_of(P.n), kBlock, 0, st>>>(P, xs, vs, rpc, have_density_pass, pos, vel, vap, rp);
+    else if (P.n_coll > 0)
+        k_pci_commit<false, true><<<grid_of(P.n), kBlock, 0, st>>>(P, xs, vs, rpc, have_density_pass, pos, vel, vap, rp);
+    else k_pci_commit<false, false><<<grid_of(P.n), kBlock, 0, st>>>(P, xs, vs, rpc, have_density_pass, pos, vel, vap, rp);
 }
 
 }  // namespace psb

@@ -41,7 +41,7 @@ EXPORTS = (
     "psb_batch_stats", "psb_set_graph", "psb_autotune", "psb_tune_set", "psb_tune_get", "psb_diagnostics",
     "psb_set_boundary", "psb_boundary_psi", "psb_context_info", "psb_set_step_count", "psb_write_txt",
     "psb_write_xml", "psb_write_vol", "psb_write_obj", "psb_export_txt", "psb_export_xml", "psb_checkpoint_save",
-    "psb_checkpoint_load", "psb_boundary_forces", "psb_set_external_force",
+    "psb_checkpoint_load", "psb_boundary_forces", "psb_set_external_force", "psb_set_colliders",
 )
 MLP_PARAMS = 4673       # PSB_MLP_PARAMS
 MLP_IN, MLP_H = 6, 64
@@ -174,6 +174,7 @@ def lib():
         "psb_checkpoint_load": ([P, ctypes.c_char_p], ctypes.c_int),
         "psb_boundary_forces": ([P, P], ctypes.c_int),
         "psb_set_external_force": ([P, P], ctypes.c_int),
+        "psb_set_colliders": ([P, P, I32], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -473,6 +474,17 @@ class Simulation:
             return
         f = np.ascontiguousarray(force, np.float32).reshape(-1, 3)
         self._check(lib().psb_set_external_force(self._h, _ptr(f)), "psb_set_external_force")
+
+    # -- collision objects --------------------------------------------------------
+    def set_colliders(self, objs):
+        """Collision objects (psb_project_b200.colliders), applied in order
+        after each step's box walls; [] removes them."""
+        from . import colliders as C
+        objs = list(objs)
+        arr = C.structs(objs)
+        self._check(lib().psb_set_colliders(self._h, ctypes.cast(arr, ctypes.c_void_p) if objs else None, len(objs)),
+                    "psb_set_colliders")
+        self._colliders = objs
 
     def boundary_psi(self) -> np.ndarray:
         out = np.empty(self.n_bnd, np.float32)
