@@ -425,6 +425,77 @@ typedef struct psb_collider {
 } psb_collider;
 int psb_set_colliders(psb_ctx* ctx, const psb_collider* objs, int32_t n);
 
+/* Emission mid-run (the reference's Emitters, src/Kernel/Emitters/*, and
+ * PCI_SPHSystem::emitParticles / _initialize(begin, N),
+ * PciSphSystem.cpp:50-160): particles appended at the end of the state
+ * (ids n .. n + k - 1) before a step's neighbour search, into the capacity
+ * the context was created with (the scene's n); nothing already resident
+ * moves or crosses the host. Appended particles start with density and
+ * pressure 0, the given velocity, and (SPH) a zero half-step velocity, as
+ * the reference's SPHParticle constructor sets (SphParticle.cpp:33-34); a
+ * DEM sphere's half-step velocity is its velocity. Single-scene contexts.
+ *
+ * psb_emit appends k particles from host arrays (vel, vel_half: NULL = 0);
+ * PSB_EINVAL when n + k exceeds the capacity. */
+int psb_emit(psb_ctx* ctx, int32_t k, const float* pos, const float* vel, const float* vel_half);
+
+/* Emitters that run inside psb_step: at the start of every step, each
+ * emitter whose emissions so far are fewer than `duration` appends one
+ * emission (Emitters::emitParticles, Emitters.cpp:49-58, in the order the
+ * emitters were added), all of them or none: a step whose emissions exceed
+ * the capacity returns PSB_EINVAL before it changes anything. Each type
+ * follows the reference's emitParticles:
+ *  BOX        EmitterBox.cpp:29-47: float lattice from center - size/2 to
+ *             center + size/2 (inclusive) in steps of 2 particle_radius, z
+ *             outer, x inner, offset by world. v: center(3), size(3), world(3)
+ *  SPHERE     EmitterSphere.cpp: rings of radius r = 0, rho, 2 rho, ... up
+ *             to sqrt(radius^2 - y^2) (y absolute, as the reference), angle
+ *             step acos(r / sqrt(r^2 + 2 rho^2)), layers y = center.y upward
+ *             then below in steps of rho = particle_radius. v: center(3), radius
+ *  CYLINDER   EmitterCylinder.cpp: the same rings up to the base radius,
+ *             angle step acos(r / sqrt(r^2 + rho^2)), layers from P2.y to
+ *             P1.y (P = center -/+ direction length/2). v: center(3),
+ *             direction(3), base radius, length
+ *  HEART      EmitterGirly.cpp: grid points of [-3, 3]^3 at 0.02 where
+ *             |(x^2 + 2 y^2 + z^2 - 1)^3 - x^2 z^3| <= 0.001 (its 9/4 and 9/80
+ *             are integer divisions)
+ *  ELLIPSOID  EmitterElipsoide.cpp: `count` particles at center + (x + a cos t
+ *             / 100, 0, z + b sin t / 100), x, z uniform in [-a/2, a/2],
+ *             [-b/2, b/2], t uniform in [0, 2 pi). v: center(3), a, b
+ *  MESH       EmitterMesh.cpp: per face, `count` particles at
+ *             (u A + v B + w C)/(u + v + w), u, v, w uniform in [0, 0.5).
+ *             data: n_faces x 9 floats (A, B, C), host memory, copied
+ * The random emitters draw from SplitMix64 on (seed, emission, particle,
+ * draw) in place of the reference's rand(). */
+enum {
+    PSB_EMITTER_BOX = 1,
+    PSB_EMITTER_SPHERE = 2,
+    PSB_EMITTER_CYLINDER = 3,
+    PSB_EMITTER_HEART = 4,
+    PSB_EMITTER_ELLIPSOID = 5,
+    PSB_EMITTER_MESH = 6
+};
+#define PSB_MAX_EMITTERS 16
+typedef struct psb_emitter {
+    int32_t type;            /* PSB_EMITTER_* */
+    int32_t duration;        /* emissions (the reference's durationTime) */
+    int32_t count;           /* ellipsoid: per emission; mesh: per face */
+    int32_t n_faces;         /* mesh */
+    float particle_radius;   /* the emitting system's particle radius */
+    float velocity[3];       /* velocityEmission */
+    float v[12];
+    const float* data;       /* mesh faces */
+    uint64_t seed;           /* random emitters */
+} psb_emitter;
+int psb_add_emitter(psb_ctx* ctx, const psb_emitter* e);
+/* Removes every emitter. */
+int psb_clear_emitters(psb_ctx* ctx);
+/* Host only (no context, no GPU): the positions emission number `emission`
+ * of this emitter produces, in emission order, at most cap of them (out:
+ * cap x 3 floats, may be NULL to count); *n receives the full count. The
+ * random emitters use the same draws as the device. */
+int psb_emitter_positions(const psb_emitter* e, int32_t emission, int64_t cap, float* out, int64_t* n);
+
 /* The scene the context was created with (for a batch: scene 0 with n_max
  * the total), the particle count of the last upload (0 before one) and the
  * steps taken; psb_set_step_count overwrites the step count (checkpoints). */

@@ -383,6 +383,25 @@ class OracleSim:
         self.nbr = np.zeros(n, np.int32)
         self.stats = OrcStats()
 
+    def append(self, pos, vel=None, vel_half=None):
+        """Particles appended at the end (ids n ..), density and pressure 0."""
+        pos = np.asarray(pos, np.float64).reshape(-1, 3)
+        k = pos.shape[0]
+        z3 = np.zeros((k, 3))
+        vel = z3 if vel is None else np.asarray(vel, np.float64).reshape(-1, 3)
+        vel_half = z3 if vel_half is None else np.asarray(vel_half, np.float64).reshape(-1, 3)
+        self.pos = np.ascontiguousarray(np.concatenate([self.pos, pos]))
+        self.vel = np.ascontiguousarray(np.concatenate([self.vel, vel]))
+        self.vel_half = np.ascontiguousarray(np.concatenate([self.vel_half, vel_half]))
+        self.rho = np.concatenate([self.rho, np.zeros(k)])
+        self.p = np.concatenate([self.p, np.zeros(k)])
+        self.rho_x = np.zeros(self.pos.shape[0])
+        self.f_np = np.zeros((self.pos.shape[0], 3))
+        self.nbr = np.zeros(self.pos.shape[0], np.int32)
+        self.P.n = self.pos.shape[0]
+        if getattr(self, "ext", None) is not None:
+            self.set_external_force(np.concatenate([self.ext, z3]))
+
     def presolve(self, iters):
         S = OrcState(self.pos.ctypes.data, self.vel.ctypes.data, self.vel_half.ctypes.data,
                      self.rho.ctypes.data, self.p.ctypes.data)
@@ -440,6 +459,150 @@ def ref_collide(obj, old_pos, pos, vel, dt, particle_radius=0.0):
     if rc != 0:
         raise RuntimeError(f"ref_collide failed: {rc}")
     return x, u
+
+
+# ---- emitters (src/Kernel/Emitters/*), restated --------------------------------
+# The reference's emitters need its Particle, SimulationData and GL geometry
+# classes, so they are restated here rather than compiled: each loop as its
+# emitParticles runs it, with its float and double types, and the C
+# library's math (Python's math module and numpy's float32 power call it).
+
+_M64 = (1 << 64) - 1
+
+
+def _splitmix64(x):
+    z = (x + 0x9E3779B97F4A7C15) & _M64
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def _uniform(seed, emission, particle, draw):
+    k = _splitmix64(seed ^ _splitmix64(((emission << 32) | draw) & _M64) ^ _splitmix64(particle + 1))
+    return (k >> 11) * (1.0 / 9007199254740992.0)
+
+
+def _box(v, rho):
+    f32 = np.float32
+    cx, cy, cz = (float(f32(t)) for t in v[:3])
+    sx, sy, sz = (f32(t) for t in v[3:6])
+    wx, wy, wz = (float(f32(t)) for t in v[6:9])
+    step = f32(rho) * f32(2)
+
+    def axis(c, sz_):
+        out, x = [], f32(c - float(sz_ / f32(2)))
+        while float(x) <= c + float(sz_ / f32(2)):
+            out.append(x)
+            x = f32(x + step)
+        return out
+    pts = []
+    for z in axis(cz, sz):
+        for y in axis(cy, sy):
+            for x in axis(cx, sx):
+                pts.append((f32(float(x) + wx), f32(float(y) + wy), f32(float(z) + wz)))
+    return np.array(pts, np.float32).reshape(-1, 3)
+
+
+def _ring(cx, cz, y, r, dtheta, pts):
+    import math
+    theta, theta_ap = 0.0, 1.0
+    while theta <= 2 * math.pi and theta_ap > 0:
+        pts.append((cx + r * math.cos(theta), y, cz + r * math.sin(theta)))
+        theta += dtheta
+        theta_ap = theta
+
+
+def _sphere(v, rho):
+    import math
+    f32 = np.float32
+    cx, cy, cz = (float(f32(t)) for t in v[:3])
+    R, rho = f32(v[3]), f32(rho)
+    RR, rr2 = float(R * R), float(f32(2) * rho * rho)
+    pts = []
+
+    def layer(y):
+        r = 0.0
+        while RR - y * y >= 0 and r <= math.sqrt(RR - y * y):
+            _ring(cx, cz, y, r, math.acos(r / math.sqrt(r * r + rr2)), pts)
+            r += float(rho)
+    y = cy
+    while y < cy + float(R):
+        layer(y)
+        y += float(rho)
+    y = cy - float(rho)
+    while y >= cy - float(R):
+        layer(y)
+        y -= float(rho)
+    return np.array(pts, np.float64).astype(np.float32).reshape(-1, 3)
+
+
+def _cylinder(v, rho):
+    import math
+    f32 = np.float32
+    cx, cy, cz = (float(f32(t)) for t in v[:3])
+    dy = float(f32(v[4]))
+    rb, half, rho = f32(v[6]), float(f32(v[7]) / f32(2)), f32(rho)
+    rr = float(rho * rho)
+    pts = []
+    y, top = cy - dy * half, cy + dy * half
+    while y < top:
+        r = 0.0
+        while r <= float(rb):
+            _ring(cx, cz, y, r, math.acos(r / math.sqrt(r * r + rr)), pts)
+            r += float(rho)
+        y += float(rho)
+    return np.array(pts, np.float64).astype(np.float32).reshape(-1, 3)
+
+
+def _heart():
+    vals, x = [], -3.0
+    while x <= 3.0:
+        vals.append(x)
+        x += 0.02
+    a = np.array(vals)
+    Y, Z = np.meshgrid(a, a, indexing="ij")
+    pts = []
+    for x in a:
+        arg = x * x + 2 * Y * Y + Z * Z - 1
+        res = np.power(arg.astype(np.float32), np.float32(3)).astype(np.float64) - x * x * Z * Z * Z
+        m = (res >= -0.001) & (res <= 0.001)
+        pts.append(np.stack([np.full(m.sum(), x), Y[m], Z[m]], 1))
+    return np.concatenate(pts).astype(np.float32)
+
+
+def emitter_positions(typ, v, particle_radius=0.0, count=0, faces=None, seed=0, emission=0) -> np.ndarray:
+    """One emission of an emitter (types as psb_emitter's), float32 (k, 3)."""
+    import math
+    f32 = np.float32
+    if typ == 1:
+        return _box(v, particle_radius)
+    if typ == 2:
+        return _sphere(v, particle_radius)
+    if typ == 3:
+        return _cylinder(v, particle_radius)
+    if typ == 4:
+        return _heart()
+    if typ == 5:
+        out = np.empty((count, 3), np.float32)
+        a, b = f32(v[3]), f32(v[4])
+        for i in range(count):
+            t = _uniform(seed, emission, i, 0) * 6.283185307179586
+            cxe, cze = float(a) * math.cos(t), float(b) * math.sin(t)
+            x = f32(float(-a / f32(2)) + _uniform(seed, emission, i, 1) * float(a))
+            z = f32(float(-b / f32(2)) + _uniform(seed, emission, i, 2) * float(b))
+            out[i] = (f32(float(f32(v[0])) + float(x) + cxe / 100), f32(v[1]), f32(float(f32(v[2])) + float(z) + cze / 100))
+        return out
+    if typ == 6:
+        F = np.asarray(faces, np.float32).reshape(-1, 9)
+        out = np.empty((count * F.shape[0], 3), np.float32)
+        for i in range(out.shape[0]):
+            w = [f32(_uniform(seed, emission, i, d) * 0.5) for d in range(3)]
+            s_ = float(w[0] + w[1] + w[2])
+            face = F[i // count].astype(np.float64)
+            for k in range(3):
+                out[i, k] = f32((float(w[0]) * face[k] + float(w[1]) * face[3 + k] + float(w[2]) * face[6 + k]) / s_)
+        return out
+    raise ValueError(typ)
 
 
 class RefSim:

@@ -21,8 +21,8 @@ OUT_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(OUT_DIR, "libpsb.so")
 OBJ_DIR = os.path.join(ROOT, "_build")
 
-CU_SOURCES = ["grid.cu", "sph.cu", "api.cu", "noalloc.cu", "mlp.cu", "dem.cu", "mc.cu", "compat.cu", "batch.cu", "diag.cu", "boundary.cu", "colliders.cu"]
-CPP_SOURCES = ["scene.cpp", "io.cpp"]
+CU_SOURCES = ["grid.cu", "sph.cu", "api.cu", "noalloc.cu", "mlp.cu", "dem.cu", "mc.cu", "compat.cu", "batch.cu", "diag.cu", "boundary.cu", "colliders.cu", "emit.cu"]
+CPP_SOURCES = ["scene.cpp", "io.cpp", "emitters.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr",

@@ -72,6 +72,16 @@ struct Profiler {
 
 }  // namespace
 
+// One emitter (psb_add_emitter): the deterministic types keep their
+// emission's positions on the device; the random ones keep mesh faces.
+struct EmitterRec {
+    psb_emitter e{};
+    float* d_list = nullptr;
+    float* d_faces = nullptr;
+    int64_t per = 0;      // particles per emission
+    int done = 0;         // emissions so far
+};
+
 struct psb_ctx {
     psb_scene sc{};
     Params P{};
@@ -156,6 +166,7 @@ struct psb_ctx {
     // object's mesh faces or height terms
     psb::Collider* d_coll = nullptr;
     std::vector<float*> coll_data;
+    std::vector<EmitterRec> emitters;     // psb_add_emitter, in order
     long long bnd_force_cap = 0;
     // static boundary particles (psb_set_boundary); bnd_n == 0: none
     int bnd_n = 0, bnd_res = 0;
@@ -260,6 +271,7 @@ void free_all(psb_ctx* c) {
     cudaFree(c->ext_force); cudaFree(c->bnd_force);
     cudaFree(c->d_coll);
     for (float* d : c->coll_data) cudaFree(d);
+    for (auto& e : c->emitters) { cudaFree(e.d_list); cudaFree(e.d_faces); }
     cudaFreeHost(c->h_loop); cudaFreeHost(c->h_err_sh);
     for (auto& g : c->gexec) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -683,8 +695,41 @@ int step_batch(psb_ctx* c, bool last) {
     return PSB_OK;
 }
 
+// The emissions due this step (Emitters::emitParticles before the
+// neighbour search, PciSphSystem.cpp:155-160): all of them, or none when
+// they exceed the capacity.
+int run_emitters(psb_ctx* c) {
+    int64_t need = 0;
+    for (const auto& e : c->emitters)
+        if (e.done < e.e.duration) need += e.per;
+    if (need == 0) return PSB_OK;
+    if ((int64_t)c->n + need > (int64_t)c->n_max)
+        return fail(c, PSB_EINVAL, "emitters: " + std::to_string(need) + " particles due, " +
+                                       std::to_string(c->n_max - c->n) + " free of the context's capacity");
+    cudaStream_t st = c->stream;
+    const int dem = c->P.dem ? 1 : 0;
+    for (auto& e : c->emitters) {
+        if (e.done >= e.e.duration) continue;
+        const int n0 = c->n, k = (int)e.per;
+        float4* pos = c->pos[c->cs] ;
+        if (e.d_list)
+            psb::launch_emit_list(st, n0, k, e.d_list, e.e.velocity, dem, pos, c->vel[c->cs], c->vap[c->cs],
+                                  c->ids[c->cr], c->rp[c->cr]);
+        else
+            psb::launch_emit_random(st, n0, k, e.e.type, e.e.count, (unsigned)e.done, e.e.seed, e.e.v, e.d_faces,
+                                    e.e.velocity, dem, pos, c->vel[c->cs], c->vap[c->cs], c->ids[c->cr],
+                                    c->rp[c->cr]);
+        if (c->P.ext_force) cudaMemsetAsync(c->ext_force + n0, 0, sizeof(float4) * (size_t)k, st);
+        c->n += k;
+        e.done += 1;
+    }
+    c->built = false;
+    return cuda_check(c, cudaGetLastError(), "emitters");
+}
+
 int step_once(psb_ctx* c, bool last) {
     if (c->batch) return step_batch(c, last);
+    if (!c->emitters.empty()) PSB_TRY(run_emitters(c));
     const bool need_prev_p = !c->P.ref && c->P.pci && (c->sc.warm_start != PSB_WARM_ZERO || c->collect_stride > 0);
     const bool features = !c->P.ref && c->P.pci && (c->sc.warm_start == PSB_WARM_LEARNED || c->collect_stride > 0);
     PSB_TRY(build(c, need_prev_p, features));
@@ -1556,6 +1601,92 @@ void drop_colliders(psb_ctx* c) {
 }
 
 }  // namespace
+
+int psb_emit(psb_ctx* c, int32_t k, const float* pos, const float* vel, const float* vel_half) {
+    if (!c) return PSB_EINVAL;
+    if (k <= 0 || !pos) return fail(c, PSB_EINVAL, "psb_emit: bad k or NULL pos");
+    if (c->batch) return fail(c, PSB_EINVAL, "psb_emit: single-scene contexts only");
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_emit before psb_upload");
+    if ((int64_t)c->n + k > (int64_t)c->n_max)
+        return fail(c, PSB_EINVAL, "psb_emit: " + std::to_string(k) + " particles, " +
+                                       std::to_string(c->n_max - c->n) + " free of the context's capacity");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    float* stage = (float*)c->stage;
+    const int n0 = c->n;
+    const float* vh = c->P.dem ? vel : vel_half;     // a DEM sphere's half-step velocity is its velocity
+    struct { const float* src; float4* dst; } parts[3] = {
+        {pos, c->pos[c->cs] + n0}, {vel, c->vel[c->cs] + n0}, {vh, c->vap[c->cs] + n0}};
+    for (auto& p : parts) {
+        if (p.src)
+            PSB_TRY(cuda_check(c, cudaMemcpyAsync(stage, p.src, sizeof(float) * 3 * (size_t)k, cudaMemcpyHostToDevice,
+                                                  st), "emit"));
+        k_pack3<<<blocks(k), psb::kBlock, 0, st>>>(k, p.src ? stage : nullptr, p.dst);
+    }
+    psb::launch_append_ids(st, n0, k, c->ids[c->cr], c->rp[c->cr]);
+    if (c->P.ext_force) cudaMemsetAsync(c->ext_force + n0, 0, sizeof(float4) * (size_t)k, st);
+    c->n += k;
+    c->built = false;
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "emit"));   // the host arrays are the caller's again
+    return cuda_check(c, cudaGetLastError(), "emit");
+}
+
+int psb_add_emitter(psb_ctx* c, const psb_emitter* e) {
+    if (!c) return PSB_EINVAL;
+    if (!e) return fail(c, PSB_EINVAL, "psb_add_emitter: NULL emitter");
+    if (c->batch) return fail(c, PSB_EINVAL, "psb_add_emitter: single-scene contexts only");
+    if ((int)c->emitters.size() >= PSB_MAX_EMITTERS) return fail(c, PSB_EINVAL, "psb_add_emitter: too many emitters");
+    if (e->duration < 0) return fail(c, PSB_EINVAL, "psb_add_emitter: negative duration");
+    for (float x : e->v)
+        if (!std::isfinite(x)) return fail(c, PSB_EINVAL, "psb_add_emitter: non-finite parameter");
+    for (float x : e->velocity)
+        if (!std::isfinite(x)) return fail(c, PSB_EINVAL, "psb_add_emitter: non-finite velocity");
+    const bool lattice = e->type == PSB_EMITTER_BOX || e->type == PSB_EMITTER_SPHERE ||
+                         e->type == PSB_EMITTER_CYLINDER;
+    if (lattice && !(e->particle_radius > 0.f))
+        return fail(c, PSB_EINVAL, "psb_add_emitter: particle_radius must be > 0");
+    int64_t per = 0;
+    if (psb_emitter_positions(e, 0, 0, nullptr, &per) != PSB_OK)
+        return fail(c, PSB_EINVAL, "psb_add_emitter: bad type, count or faces");
+    if (per > (int64_t)c->n_max) return fail(c, PSB_EINVAL, "psb_add_emitter: one emission exceeds the capacity");
+    cudaSetDevice(c->device);
+    EmitterRec r;
+    r.e = *e;
+    r.e.data = nullptr;
+    r.per = per;
+    const bool random = e->type == PSB_EMITTER_ELLIPSOID || e->type == PSB_EMITTER_MESH;
+    int rc = PSB_OK;
+    if (!random && per > 0) {
+        std::vector<float> xyz(3 * (size_t)per);
+        int64_t m = 0;
+        psb_emitter_positions(e, 0, per, xyz.data(), &m);
+        rc = dalloc(c, &r.d_list, xyz.size());
+        if (rc == PSB_OK)
+            rc = cuda_check(c, cudaMemcpy(r.d_list, xyz.data(), sizeof(float) * xyz.size(), cudaMemcpyHostToDevice),
+                            "emitter");
+    } else if (e->type == PSB_EMITTER_MESH && e->n_faces > 0) {
+        rc = dalloc(c, &r.d_faces, 9 * (size_t)e->n_faces);
+        if (rc == PSB_OK)
+            rc = cuda_check(c, cudaMemcpy(r.d_faces, e->data, sizeof(float) * 9 * (size_t)e->n_faces,
+                                          cudaMemcpyHostToDevice), "emitter");
+    }
+    if (rc != PSB_OK) {
+        cudaFree(r.d_list);
+        cudaFree(r.d_faces);
+        return rc;
+    }
+    c->emitters.push_back(r);
+    return PSB_OK;
+}
+
+int psb_clear_emitters(psb_ctx* c) {
+    if (!c) return PSB_EINVAL;
+    cudaSetDevice(c->device);
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "emitters"));
+    for (auto& e : c->emitters) { cudaFree(e.d_list); cudaFree(e.d_faces); }
+    c->emitters.clear();
+    return PSB_OK;
+}
 
 int psb_set_colliders(psb_ctx* c, const psb_collider* objs, int32_t n) {
     if (!c) return PSB_EINVAL;

@@ -216,6 +216,14 @@ int launch_bnd_prepare(cudaStream_t st, const Params& P, int nb, const float4* r
 // (DEM): vel and vap both take the new velocity.
 void launch_apply_colliders(cudaStream_t st, const Params& P, const float4* x_old, const float4* vh_old, float4* pos,
                             float4* vel, float4* vap);
+// Emission (emit.cu): k particles at slots and ids n0 .. n0 + k - 1, velocity
+// v, half-step velocity v (dem) or 0, density and pressure 0.
+void launch_emit_list(cudaStream_t st, int n0, int k, const float* xyz, const float* v, int dem, float4* pos,
+                      float4* vel, float4* vap, int* ids, float2* rp);
+void launch_emit_random(cudaStream_t st, int n0, int k, int type, int count, unsigned emission,
+                        unsigned long long seed, const float* params, const float* faces, const float* v, int dem,
+                        float4* pos, float4* vel, float4* vap, int* ids, float2* rp);
+void launch_append_ids(cudaStream_t st, int n0, int k, int* ids, float2* rp);
 void launch_bnd_reaction(cudaStream_t st, const Params& P, int nb, const float4* fluid_pos, const float2* fluid_rp,
                          const uint32_t* cell_start, const uint32_t* cell_end, float4* force);
 // Per fluid slot: the boundary particles within the list cut-off, from a

@@ -41,7 +41,8 @@ EXPORTS = (
     "psb_batch_stats", "psb_set_graph", "psb_autotune", "psb_tune_set", "psb_tune_get", "psb_diagnostics",
     "psb_set_boundary", "psb_boundary_psi", "psb_context_info", "psb_set_step_count", "psb_write_txt",
     "psb_write_xml", "psb_write_vol", "psb_write_obj", "psb_export_txt", "psb_export_xml", "psb_checkpoint_save",
-    "psb_checkpoint_load", "psb_boundary_forces", "psb_set_external_force", "psb_set_colliders",
+    "psb_checkpoint_load", "psb_boundary_forces", "psb_set_external_force", "psb_set_colliders", "psb_emit",
+    "psb_add_emitter", "psb_clear_emitters", "psb_emitter_positions",
 )
 MLP_PARAMS = 4673       # PSB_MLP_PARAMS
 MLP_IN, MLP_H = 6, 64
@@ -175,6 +176,10 @@ def lib():
         "psb_boundary_forces": ([P, P], ctypes.c_int),
         "psb_set_external_force": ([P, P], ctypes.c_int),
         "psb_set_colliders": ([P, P, I32], ctypes.c_int),
+        "psb_emit": ([P, I32, P, P, P], ctypes.c_int),
+        "psb_add_emitter": ([P, P], ctypes.c_int),
+        "psb_clear_emitters": ([P], ctypes.c_int),
+        "psb_emitter_positions": ([P, I32, ctypes.c_int64, P, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -332,7 +337,12 @@ class Simulation:
 
     def step(self, nsteps: int = 1, allow_noconv: bool = True) -> int:
         allow = (OK, ENOCONV) if allow_noconv else (OK,)
-        return self._check(lib().psb_step(self._h, int(nsteps)), "psb_step", allow)
+        rc = lib().psb_step(self._h, int(nsteps))
+        if getattr(self, "_emitting", False):      # emitters grow the particle count inside the step
+            n = ctypes.c_int32()
+            lib().psb_context_info(self._h, None, ctypes.byref(n), None)
+            self.n = n.value
+        return self._check(rc, "psb_step", allow)
 
     def presolve(self, iters: int):
         self._check(lib().psb_presolve(self._h, int(iters)), "psb_presolve")
@@ -474,6 +484,25 @@ class Simulation:
             return
         f = np.ascontiguousarray(force, np.float32).reshape(-1, 3)
         self._check(lib().psb_set_external_force(self._h, _ptr(f)), "psb_set_external_force")
+
+    # -- emission -----------------------------------------------------------------
+    def emit(self, pos, vel=None, vel_half=None):
+        """Appends particles (ids n .. n + k - 1) to the resident state."""
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32).reshape(-1, 3) for a in (vel, vel_half)]
+        self._check(lib().psb_emit(self._h, pos.shape[0], _ptr(pos), *[None if a is None else _ptr(a) for a in arrs]),
+                    "psb_emit")
+        self.n += pos.shape[0]
+
+    def add_emitter(self, e):
+        """An emitter (psb_project_b200.emitters) that runs inside step()."""
+        s = e.struct()
+        self._check(lib().psb_add_emitter(self._h, ctypes.byref(s)), "psb_add_emitter")
+        self._emitting = True
+
+    def clear_emitters(self):
+        self._check(lib().psb_clear_emitters(self._h), "psb_clear_emitters")
+        self._emitting = False
 
     # -- collision objects --------------------------------------------------------
     def set_colliders(self, objs):
