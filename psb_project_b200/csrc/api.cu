@@ -339,6 +339,12 @@ Params derive(const psb_scene& s) {
     // list cut-off: the reference's h, or (1 + skin) h in the config profile
     const double hl = s.profile == PSB_PROFILE_CONFIG ? h * (1.0 + s.skin) : h;
     P.h = hl;
+    // sqrt_rn is monotone, so {x >= 0 : sqrt_rn(x) <= h} is [0, X]: find X
+    // from h*h by single ulps with the host's correctly rounded sqrt
+    double X = hl * hl;
+    while (std::sqrt(X) > hl) X = std::nextafter(X, 0.0);
+    while (std::sqrt(std::nextafter(X, INFINITY)) <= hl) X = std::nextafter(X, INFINITY);
+    P.h2_exact = X;
     const float h2f = (float)(hl * hl);
     P.h2_lo = h2f * (1.f - 1e-5f);
     P.h2_hi = h2f * (1.f + 1e-5f);

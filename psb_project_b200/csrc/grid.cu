@@ -192,13 +192,15 @@ __global__ void k_reorder(int n, const uint32_t* __restrict__ keys, const uint32
 }
 
 // The reference's test, sqrt((dx*dx + dy*dy) + dz*dz) <= h with every
-// operation rounded separately in FP64 (double3.h:15-47).
-__device__ __forceinline__ bool exact_neighbor(float4 a, float4 b, double h) {
+// operation rounded separately in FP64 (double3.h:15-47). The correctly
+// rounded square root is monotone, so the test is d2 <= h2_exact, the
+// largest double whose root rounds to at most h (found on the host).
+__device__ __forceinline__ bool exact_neighbor(float4 a, float4 b, double h2_exact) {
     const double dx = __dsub_rn((double)a.x, (double)b.x);
     const double dy = __dsub_rn((double)a.y, (double)b.y);
     const double dz = __dsub_rn((double)a.z, (double)b.z);
     const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-    return __dsqrt_rn(d2) <= h;
+    return d2 <= h2_exact;
 }
 
 // flags[1]: max count, flags[2..3]: total pairs (64-bit); every lane of the
@@ -261,7 +263,7 @@ __global__ void __launch_bounds__(BS) k_build_nbr(Params P, const float4* __rest
                     bool acc;
                     if (d2 < P.h2_lo) acc = true;
                     else if (d2 > P.h2_hi) acc = false;
-                    else acc = exact_neighbor(pi, pj, P.h);
+                    else acc = exact_neighbor(pi, pj, P.h2_exact);
                     if (acc) {      // one 4-byte store per entry (buffering four in registers measured slower)
                         if (cnt < P.cap) list[nbr_index(cnt, n, t)] = (int)q;
                         ++cnt;
@@ -356,7 +358,7 @@ __global__ void __launch_bounds__(BS) k_build_nbr_tile(Params P, const float4* _
                             bool acc;
                             if (d2 < P.h2_lo) acc = true;
                             else if (d2 > P.h2_hi) acc = false;
-                            else acc = exact_neighbor(pi, pj, P.h);
+                            else acc = exact_neighbor(pi, pj, P.h2_exact);
                             if (acc) {
                                 if (cnt < P.cap) list[nbr_index(cnt, n, t)] = (int)(q0 + c);
                                 ++cnt;

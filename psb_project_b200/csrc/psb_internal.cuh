@@ -57,6 +57,7 @@ struct Params {
     Grid g;
     double h;           // list cut-off of the exact neighbour test sqrt(d.d) <= h in FP64
                         // (reference: h; config: (1 + skin) h)
+    double h2_exact;    // the largest double x with sqrt_rn(x) <= h: the same test as d.d <= h2_exact
     float h2_lo, h2_hi; // FP32 d^2 outside [h2_lo, h2_hi] is decided without the FP64 test
     float h2, inv_h, inv_h2;
     float k_rho;        // 315 m / (64 pi h^3):           rho = k_rho * sum (1-q)^3
