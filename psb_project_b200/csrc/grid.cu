@@ -244,6 +244,8 @@ __global__ void __launch_bounds__(BS) k_build_nbr(Params P, const float4* __rest
         const int cj = (int)((key / (uint32_t)nx) % (uint32_t)ny);
         const int ck = (int)(key / ((uint32_t)nx * (uint32_t)ny));
         const int a0 = max(ci - 1, 0), a1 = min(ci + 1, nx - 1);
+        int* wq = list + nbr_index(0, n, t);
+        const size_t qstride = (size_t)4 * (size_t)n;
         for (int k = max(ck - 1, 0); k <= min(ck + 1, nz - 1); ++k) {
             for (int j = max(cj - 1, 0); j <= min(cj + 1, ny - 1); ++j) {
                 const uint32_t row = base + (uint32_t)j * (uint32_t)nx + (uint32_t)k * (uint32_t)nx * (uint32_t)ny;
@@ -260,13 +262,14 @@ __global__ void __launch_bounds__(BS) k_build_nbr(Params P, const float4* __rest
                     const float4 pj = pos[q];
                     const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                     const float d2 = dx * dx + dy * dy + dz * dz;
-                    bool acc;
-                    if (d2 < P.h2_lo) acc = true;
-                    else if (d2 > P.h2_hi) acc = false;
-                    else acc = exact_neighbor(pi, pj, P.h2_exact);
-                    if (acc) {      // one 4-byte store per entry (buffering four in registers measured slower)
-                        if (cnt < P.cap) list[nbr_index(cnt, n, t)] = (int)q;
+                    // beyond the FP32 window: out with one compare; below it: in;
+                    // inside it: the reference's FP64 test
+                    if (d2 <= P.h2_hi && (d2 < P.h2_lo || exact_neighbor(pi, pj, P.h2_exact))) {
+                        // one 4-byte store per entry (buffering four in registers measured
+                        // slower); wq is entry cnt's quad, nbr_index(cnt, n, t) - (cnt & 3)
+                        if (cnt < P.cap) wq[cnt & 3] = (int)q;
                         ++cnt;
+                        if ((cnt & 3) == 0 && cnt < P.cap) wq += qstride;
                     }
                 }
             }
