@@ -241,15 +241,17 @@ int psb_sort_cells_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uin
                            uint32_t* vals_out, int32_t n, int32_t key_bits, void* stream);
 
 /* Learned warm start (CONFIG-profile PCISPH, warm_start = PSB_WARM_LEARNED):
- * a per-particle MLP 6 -> 64 -> 64 -> 1 (SiLU), BF16 weights and
+ * a per-particle MLP 7 -> 64 -> 64 -> 1 (SiLU), BF16 weights and
  * activations with FP32 accumulation, predicts each step's initial
  * pressure; the corrector still iterates to the same eta. No counterpart in
  * the reference, which starts every step from p = 0
  * (PciSphSystem_Kernel.cu:131). Parameters (FP32 master copy), in order:
- * W1[64][6], b1[64], W2[64][64], b2[64], W3[64], b3. Inputs: neighbour count,
+ * W1[64][7], b1[64], W2[64][64], b2[64], W3[64], b3. Inputs: neighbour count,
  * advected density, velocity divergence, previous pressure, wall distance,
- * density-gradient magnitude (scaled as in psb_project_b200/csrc/mlp.cu). */
-#define PSB_MLP_PARAMS 4673
+ * density-gradient magnitude, previous pressure smoothed with the poly6
+ * weights over the neighbours (scaled as in psb_project_b200/csrc/sph.cu,
+ * k_density_x). */
+#define PSB_MLP_PARAMS 4737
 #define PSB_MLP_FEATURE_STRIDE 8
 int psb_mlp_set_weights(psb_ctx* ctx, const float* w);
 int psb_mlp_get_weights(psb_ctx* ctx, float* w);
@@ -263,7 +265,7 @@ int psb_mlp_dataset(psb_ctx* ctx, int64_t* rows, float* X, float* T);
 /* `iters` Adam steps (lr, beta 0.9/0.999) on MSE over minibatches of `batch`
  * rows drawn from the recorded data; *loss = last minibatch loss. */
 int psb_mlp_train(psb_ctx* ctx, int32_t iters, int32_t batch, float lr, uint64_t seed, float* loss);
-/* Forward pass and loss gradient on host rows (X: n x 8, first 6 used; T: n
+/* Forward pass and loss gradient on host rows (X: n x 8, first 7 used; T: n
  * targets), for checking the GPU's arithmetic. */
 int psb_mlp_forward(psb_ctx* ctx, const float* X, int32_t n, float* y);
 int psb_mlp_loss_grad(psb_ctx* ctx, const float* X, const float* T, int32_t n, float* loss, float* grad);

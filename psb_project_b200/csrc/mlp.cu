@@ -33,7 +33,7 @@ namespace psb {
 
 namespace {
 
-constexpr int kIn = 6, kH = 64;
+constexpr int kIn = 7, kH = 64;
 constexpr int oW1 = 0, oB1 = oW1 + kH * kIn, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH, oB3 = oW3 + kH;
 static_assert(oB3 + 1 == kMlpParams, "parameter layout");
 
@@ -47,7 +47,7 @@ __device__ __forceinline__ float silu_grad(float z) {
 // ---- inference -----------------------------------------------------------------
 // Tensor-core inference: one warp evaluates 16 particles per pass with
 // mma.sync.m16n8k16 (BF16 inputs, FP32 accumulation). Layer 1 is a
-// [16 x 16] x [16 x 64] product (6 inputs, 10 zero pads), layer 2
+// [16 x 16] x [16 x 64] product (7 inputs, 9 zero pads), layer 2
 // [16 x 64] x [64 x 64]; the layer-1 accumulator fragments, rounded to BF16,
 // are exactly the A fragments of layer 2 (rows groupID and groupID + 8,
 // columns 2 tig + {0, 1} of each 8-wide tile). The output layer (64 -> 1) is
@@ -55,7 +55,7 @@ __device__ __forceinline__ float silu_grad(float z) {
 // Shared memory: W1 and W2 as BF16 pairs, rows padded to 36 words so that
 // the eight groups of a B-fragment load fall in distinct banks.
 constexpr int kW2Stride = 36;     // 32-bit words per padded 64-wide row
-constexpr int kW1Stride = 4;      // 8 BF16 per row (6 used)
+constexpr int kW1Stride = 4;      // 8 BF16 per row (7 used)
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(256) k_mlp_infer_mma(int n, const float* __res
     const int warps_total = gridDim.x * (blockDim.x >> 5);
     for (int tile = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tile * 16 < n; tile += warps_total) {
         const int r0 = tile * 16 + gid, r1 = r0 + 8;
-        // layer 1: A = features (cols 0..5 real)
+        // layer 1: A = features (cols 0..6 real)
         uint32_t a0 = 0u, a1 = 0u;
         {
             const int k = 2 * tig;
@@ -179,7 +179,7 @@ __device__ __forceinline__ float warp_sum(float v) {
 // One thread per sample: forward (activations kept in registers, the second
 // layer recomputed per unit), MSE loss, backward. Weight gradients are summed
 // over the warp with shuffles and added to `grad` once per warp.
-// Sample b of the batch is row sel[b] of (X, T) (X stride 8, features 0..5).
+// Sample b of the batch is row sel[b] of (X, T) (X stride 8, features 0..6).
 __global__ void __launch_bounds__(128) k_mlp_train(int batch, const float* __restrict__ X, const float* __restrict__ T,
                                                    const uint32_t* __restrict__ sel,
                                                    const __nv_bfloat16* __restrict__ w, float* __restrict__ grad,

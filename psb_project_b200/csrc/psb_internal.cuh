@@ -264,7 +264,7 @@ void launch_mc_emit(cudaStream_t st, const IsoParams& Q, const double* iso, cons
                     const uint32_t* tri_off, float* vert, int32_t* tris);
 
 // ---- learned warm start (mlp.cu) ---------------------------------------------------
-constexpr int kMlpParams = 4673;   // 6x64 + 64 + 64x64 + 64 + 64 + 1
+constexpr int kMlpParams = 4737;   // 7x64 + 64 + 64x64 + 64 + 64 + 1
 void launch_mlp_infer(cudaStream_t st, int n, const float* feats, const void* wbf, float p_scale, float2* rp);
 void launch_mlp_forward(cudaStream_t st, int n, const float* X, int stride, const void* wbf, float* y);
 void launch_mlp_grad(cudaStream_t st, int batch, const float* X, const float* T, const uint32_t* sel, const void* wbf,

@@ -296,13 +296,15 @@ __device__ __forceinline__ void box_project(const Params& P, int t, float3& x, f
 // PCISPH: keeps the carried pressure (warm start) or zeroes it.
 // FEAT (config PCISPH, learned warm start or data collection): the same
 // neighbour walk also sums the velocity divergence and density gradient and
-// writes the MLP's six inputs (feats, stride 8):
+// writes the MLP's seven inputs (feats, stride 8):
 //   f0 neighbour count / 32
 //   f1 advected density deviation (rho - dt rho div v - rho0)/rho0 * 100
 //   f2 div v * dt * 100, div v = -(k_grad/rho0) sum (1-u)^2 (v_j - v_i).x^
 //   f3 previous-step pressure / p_scale
 //   f4 distance to the nearest box face / h, capped at 1
 //   f5 k_grad |sum (1-u)^2 x^| h / rho0 (density-gradient magnitude)
+//   f6 sum W_ij p_j / sum W_ij / p_scale over the list, self included: the
+//      carried pressure smoothed with the poly6 weights
 template <bool REF, bool FEAT, bool BATCH, int BS>
 __global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __restrict__ pos,
                                                       const float4* __restrict__ vel, const int* __restrict__ counts,
@@ -314,7 +316,7 @@ __global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __rest
     const float4 xi = pos[t];
     const int cnt = min(counts[t], P.cap);
     Kahan acc;
-    float div = 0.f;
+    float div = 0.f, wp = 0.f, ws = 0.f;
     float3 gr = make_float3(0.f, 0.f, 0.f);
     float4 vi = make_float4(0.f, 0.f, 0.f, 0.f);
     if (FEAT) vi = vel[t];
@@ -325,7 +327,12 @@ __global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __rest
         const float q = r2 * P.inv_h2;
         if (!REF && q >= 1.f) return;
         const float w = 1.f - q;
-        acc.add(w * w * w);
+        const float w3 = w * w * w;
+        acc.add(w3);
+        if (FEAT) {     // carried pressures: this pass writes rp[j].y back unchanged
+            wp += w3 * rp[j].y;
+            ws += w3;
+        }
         if (FEAT && r2 > 0.f) {
             const float4 vj = vel[j];
             const float rinv = rsqrtf(r2);
@@ -366,6 +373,7 @@ __global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __rest
         f[3] = rp[t].y / p_scale;          // the carried pressure, before this pass replaces it
         f[4] = fmaxf(dwall, 0.f) * P.inv_h;
         f[5] = P.k_grad * sqrtf(gr.x * gr.x + gr.y * gr.y + gr.z * gr.z) * P.hf / P.rho0;
+        f[6] = ws > 0.f ? wp / ws / p_scale : 0.f;
     }
     rp[t] = make_float2(rho, p);
     rho_x[t] = rho;

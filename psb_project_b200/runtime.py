@@ -44,8 +44,8 @@ EXPORTS = (
     "psb_checkpoint_load", "psb_boundary_forces", "psb_set_external_force", "psb_set_colliders", "psb_emit",
     "psb_add_emitter", "psb_clear_emitters", "psb_emitter_positions",
 )
-MLP_PARAMS = 4673       # PSB_MLP_PARAMS
-MLP_IN, MLP_H = 6, 64
+MLP_PARAMS = 4737       # PSB_MLP_PARAMS
+MLP_IN, MLP_H = 7, 64
 NOALLOC_MAX_N = 262144   # PSB_NOALLOC_MAX_N
 
 

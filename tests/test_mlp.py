@@ -40,7 +40,7 @@ def torch_forward(w, X):
     W1, b1, W2, b2, W3, b3 = [torch.tensor(a, dtype=torch.float64, requires_grad=True) for a in P.mlp_unpack(w)]
     params = [W1, b1, W2, b2, W3, b3]
     Wq = [_RoundSTE.apply(p) for p in params]
-    x = bf16(torch.tensor(X[:, :6], dtype=torch.float64))
+    x = bf16(torch.tensor(X[:, :R.MLP_IN], dtype=torch.float64))
     h1 = _RoundSTE.apply(torch.nn.functional.silu(x @ Wq[0].T + Wq[1]))
     h2 = _RoundSTE.apply(torch.nn.functional.silu(h1 @ Wq[2].T + Wq[3]))
     y = h2 @ Wq[4] + Wq[5]
@@ -49,13 +49,14 @@ def torch_forward(w, X):
 
 def sample_features(n, seed):
     rng = np.random.default_rng(seed)
-    X = np.zeros((n, 6), np.float32)
+    X = np.zeros((n, R.MLP_IN), np.float32)
     X[:, 0] = rng.uniform(0.3, 1.3, n)
     X[:, 1] = rng.normal(0, 1.0, n)
     X[:, 2] = rng.normal(0, 0.5, n)
     X[:, 3] = rng.uniform(0, 6, n)
     X[:, 4] = rng.uniform(0, 1, n)
     X[:, 5] = rng.uniform(0, 3, n)
+    X[:, 6] = rng.uniform(0, 6, n)
     return X
 
 
