@@ -1390,12 +1390,16 @@ namespace {
 template <typename T>
 int grow(psb_ctx* c, T** p, long long* cap, long long need) {
     if (need <= *cap) return PSB_OK;
+    // geometric growth: a free and an allocation cost from a few to a few
+    // hundred milliseconds on a large context, and outputs such as a mesh
+    // grow a little with every call
+    const long long alloc = std::max(need, *cap + *cap / 2);
     cudaStreamSynchronize(c->stream);
     cudaFree(*p);
     *p = nullptr;
     *cap = 0;
-    PSB_TRY(dalloc(c, p, (size_t)need));
-    *cap = need;
+    PSB_TRY(dalloc(c, p, (size_t)alloc));
+    *cap = alloc;
     return PSB_OK;
 }
 
