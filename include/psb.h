@@ -241,7 +241,7 @@ int psb_sort_cells_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uin
                            uint32_t* vals_out, int32_t n, int32_t key_bits, void* stream);
 
 /* Learned warm start (CONFIG-profile PCISPH, warm_start = PSB_WARM_LEARNED):
- * a per-particle MLP 7 -> 64 -> 64 -> 1 (SiLU), BF16 weights and
+ * a per-particle MLP 7 -> 64 -> 64 -> 1 (ReLU), BF16 weights and
  * activations with FP32 accumulation, predicts each step's initial
  * pressure; the corrector still iterates to the same eta. No counterpart in
  * the reference, which starts every step from p = 0

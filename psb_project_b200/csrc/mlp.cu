@@ -1,6 +1,6 @@
 // mlp.cu -- learned pressure warm start for the PCISPH corrector.
 //
-// A per-particle MLP, 6 -> 64 -> 64 -> 1 with SiLU, predicts each step's
+// A per-particle MLP, 7 -> 64 -> 64 -> 1 with ReLU, predicts each step's
 // initial pressure so that the eta-controlled corrector (unchanged; it still
 // iterates to the same eta and judges convergence) starts closer to the
 // converged pressure. The reference has no counterpart: it starts every
@@ -14,6 +14,7 @@
 //   f3 previous-step pressure / p_scale
 //   f4 distance to the nearest box face / h, capped at 1
 //   f5 |sum m gradW_ij| * h / rho0 (density-gradient magnitude)
+//   f6 previous-step pressure smoothed with the poly6 weights / p_scale
 // Output y: initial pressure max(0, y) * p_scale, p_scale = rho0 |g| 0.1 m.
 //
 // Precision: weights and activations are BF16 (round-to-nearest-even at
@@ -38,11 +39,10 @@ constexpr int oW1 = 0, oB1 = oW1 + kH * kIn, oW2 = oB1 + kH, oB2 = oW2 + kH * kH
 static_assert(oB3 + 1 == kMlpParams, "parameter layout");
 
 __device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
-__device__ __forceinline__ float silu(float z) { return z / (1.f + expf(-z)); }
-__device__ __forceinline__ float silu_grad(float z) {
-    const float s = 1.f / (1.f + expf(-z));
-    return s * (1.f + z * (1.f - s));
-}
+// ReLU: exact, and free of the special-function unit (a SiLU's exponential
+// and reciprocal bounded the inference kernel)
+__device__ __forceinline__ float act(float z) { return fmaxf(z, 0.f); }
+__device__ __forceinline__ float act_grad(float z) { return z > 0.f ? 1.f : 0.f; }
 
 // ---- inference -----------------------------------------------------------------
 // Tensor-core inference: one warp evaluates 16 particles per pass with
@@ -70,9 +70,6 @@ __device__ __forceinline__ void mma_bf16(float* c, uint32_t a0, uint32_t a1, uin
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// SiLU with the fast exponential and division (a few ulps; the activations
-// are rounded to BF16 right after)
-__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.f + __expf(-z)); }
 
 // y_raw != nullptr: write the raw output y there (host-facing evaluation)
 // instead of the initial pressure max(0, y) p_scale into rp.
@@ -132,10 +129,10 @@ __global__ void __launch_bounds__(256) k_mlp_infer_mma(int n, const float* __res
         uint32_t h1[4][4];
 #pragma unroll
         for (int ks = 0; ks < 4; ++ks) {
-            h1[ks][0] = pack_bf16(silu_fast(z1[2 * ks][0]), silu_fast(z1[2 * ks][1]));
-            h1[ks][1] = pack_bf16(silu_fast(z1[2 * ks][2]), silu_fast(z1[2 * ks][3]));
-            h1[ks][2] = pack_bf16(silu_fast(z1[2 * ks + 1][0]), silu_fast(z1[2 * ks + 1][1]));
-            h1[ks][3] = pack_bf16(silu_fast(z1[2 * ks + 1][2]), silu_fast(z1[2 * ks + 1][3]));
+            h1[ks][0] = pack_bf16(act(z1[2 * ks][0]), act(z1[2 * ks][1]));
+            h1[ks][1] = pack_bf16(act(z1[2 * ks][2]), act(z1[2 * ks][3]));
+            h1[ks][2] = pack_bf16(act(z1[2 * ks + 1][0]), act(z1[2 * ks + 1][1]));
+            h1[ks][3] = pack_bf16(act(z1[2 * ks + 1][2]), act(z1[2 * ks + 1][3]));
         }
         float y0 = 0.f, y1 = 0.f;
 #pragma unroll
@@ -148,10 +145,10 @@ __global__ void __launch_bounds__(256) k_mlp_infer_mma(int n, const float* __res
                 mma_bf16(c, h1[ks][0], h1[ks][1], h1[ks][2], h1[ks][3], wrow[8 * ks + tig], wrow[8 * ks + 4 + tig]);
             // output layer on the BF16-rounded activations
             const float w30 = sW3[col], w31 = sW3[col + 1];
-            y0 = fmaf(w30, bf(silu_fast(c[0])), y0);
-            y0 = fmaf(w31, bf(silu_fast(c[1])), y0);
-            y1 = fmaf(w30, bf(silu_fast(c[2])), y1);
-            y1 = fmaf(w31, bf(silu_fast(c[3])), y1);
+            y0 = fmaf(w30, bf(act(c[0])), y0);
+            y0 = fmaf(w31, bf(act(c[1])), y0);
+            y1 = fmaf(w30, bf(act(c[2])), y1);
+            y1 = fmaf(w31, bf(act(c[3])), y1);
         }
         y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
         y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
@@ -200,14 +197,14 @@ __global__ void __launch_bounds__(128) k_mlp_train(int batch, const float* __res
         float z = sw[oB1 + j];
 #pragma unroll
         for (int k = 0; k < kIn; ++k) z = fmaf(sw[oW1 + j * kIn + k], x[k], z);
-        h1[j] = bf(silu(z));
+        h1[j] = bf(act(z));
     }
     float y = sw[oB3];
     for (int j = 0; j < kH; ++j) {
         float z = sw[oB2 + j];
 #pragma unroll
         for (int k = 0; k < kH; ++k) z = fmaf(sw[oW2 + j * kH + k], h1[k], z);
-        y = fmaf(sw[oW3 + j], bf(silu(z)), y);
+        y = fmaf(sw[oW3 + j], bf(act(z)), y);
     }
     const float e = valid ? y - T[row] : 0.f;
     const float dy = 2.f * e * inv_b;                     // d(mean e^2)/dy
@@ -222,8 +219,8 @@ __global__ void __launch_bounds__(128) k_mlp_train(int batch, const float* __res
         float z = sw[oB2 + j];
 #pragma unroll
         for (int k = 0; k < kH; ++k) z = fmaf(sw[oW2 + j * kH + k], h1[k], z);
-        const float h2 = bf(silu(z));
-        const float dz2 = dy * sw[oW3 + j] * silu_grad(z);
+        const float h2 = bf(act(z));
+        const float dz2 = dy * sw[oW3 + j] * act_grad(z);
         const float g3 = warp_sum(dy * h2);
         const float g2b = warp_sum(dz2);
         if ((threadIdx.x & 31) == 0) { atomicAdd(&grad[oW3 + j], g3); atomicAdd(&grad[oB2 + j], g2b); }
@@ -239,7 +236,7 @@ __global__ void __launch_bounds__(128) k_mlp_train(int batch, const float* __res
         float z = sw[oB1 + j];
 #pragma unroll
         for (int k = 0; k < kIn; ++k) z = fmaf(sw[oW1 + j * kIn + k], x[k], z);
-        const float dz1 = dh1[j] * silu_grad(z);
+        const float dz1 = dh1[j] * act_grad(z);
         const float g1b = warp_sum(dz1);
         if ((threadIdx.x & 31) == 0) atomicAdd(&grad[oB1 + j], g1b);
 #pragma unroll

@@ -4,8 +4,8 @@ reference, training on the GPU, and the warm start in the corrector loop.
 The reference computes in float64 with the GPU's storage rounding applied at
 the same points: weights, inputs and hidden activations rounded to BF16
 (round-to-nearest-even), the rounding's derivative taken as 1 (the GPU
-back-propagates through the stored BF16 activations). What remains is FP32
-accumulation and CUDA's expf against float64:
+back-propagates through the stored BF16 activations). The activation is
+ReLU, exact in both; what remains is FP32 accumulation against float64:
   * forward: 99% of outputs within 1e-4 of the output scale, all within 2e-2
     (an FP32 pre-activation a few ulp from a BF16 rounding boundary rounds
     the other way and moves the output by one BF16 step of one unit);
@@ -41,8 +41,8 @@ def torch_forward(w, X):
     params = [W1, b1, W2, b2, W3, b3]
     Wq = [_RoundSTE.apply(p) for p in params]
     x = bf16(torch.tensor(X[:, :R.MLP_IN], dtype=torch.float64))
-    h1 = _RoundSTE.apply(torch.nn.functional.silu(x @ Wq[0].T + Wq[1]))
-    h2 = _RoundSTE.apply(torch.nn.functional.silu(h1 @ Wq[2].T + Wq[3]))
+    h1 = _RoundSTE.apply(torch.nn.functional.relu(x @ Wq[0].T + Wq[1]))
+    h2 = _RoundSTE.apply(torch.nn.functional.relu(h1 @ Wq[2].T + Wq[3]))
     y = h2 @ Wq[4] + Wq[5]
     return y, params
 
