@@ -11,9 +11,8 @@
  * Each entry point names the reference interface it replaces (paths inside
  * the edarles/PSB_Project tree). The reference's system classes
  * (PCI_SPHSystem, SPHSystem) keep their class API; their update() bodies
- * call these functions instead of the reference launchers -- the
- * integration recipe, with the ctypes binding the Python tests use, is in
- * INTEGRATION.md.
+ * call these functions instead of the reference launchers. The Python
+ * package (psb_project_b200/runtime.py) binds the same functions with ctypes.
  */
 #ifndef PSB_H
 #define PSB_H
@@ -368,7 +367,7 @@ int psb_boundary_forces(psb_ctx* ctx, float* force);
 int psb_set_external_force(psb_ctx* ctx, const float* force);
 
 /* Collision objects: the reference's ObjectCollision subclasses
- * (src/Kernel/Collision/*; Collision::collide, Collision.cpp:44-49), applied
+ * (src/Kernel/Collision; Collision::collide, Collision.cpp:44-49), applied
  * in list order after each step's integrator and box walls, to the start
  * position, the new position and the new velocity (the half-step velocity
  * of the SPH systems, SphSystem.cpp:323-328; the velocity of DEM,
@@ -427,7 +426,7 @@ typedef struct psb_collider {
 } psb_collider;
 int psb_set_colliders(psb_ctx* ctx, const psb_collider* objs, int32_t n);
 
-/* Emission mid-run (the reference's Emitters, src/Kernel/Emitters/*, and
+/* Emission mid-run (the reference's Emitters, src/Kernel/Emitters, and
  * PCI_SPHSystem::emitParticles / _initialize(begin, N),
  * PciSphSystem.cpp:50-160): particles appended at the end of the state
  * (ids n .. n + k - 1) before a step's neighbour search, into the capacity
