@@ -2,7 +2,7 @@
 //
 // A per-particle MLP, 7 -> 64 -> 64 -> 1 with ReLU, predicts each step's
 // initial pressure so that the eta-controlled corrector (unchanged; it still
-// iterates to the same eta and judges convergence) starts closer to the
+// iterates to the same eta and decides convergence) starts closer to the
 // converged pressure. The reference has no counterpart: it starts every
 // step from p = 0 (PciSphSystem_Kernel.cu:131).
 //

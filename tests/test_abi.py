@@ -12,6 +12,8 @@ import pytest
 import oracle
 import psb_project_b200 as P
 from psb_project_b200 import runtime as R
+from psb_project_b200.colliders import PsbCollider
+from psb_project_b200.emitters import PsbEmitter
 from psb_project_b200.scene import PsbScene
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -43,6 +45,9 @@ def test_struct_layout_matches_header(tmp_path):
                  ' sizeof(psb_step_stats), offsetof(psb_step_stats, iters_total), offsetof(psb_scene, dem_attraction),'
                  ' sizeof(psb_iso_grid), offsetof(psb_iso_grid, scale), sizeof(psb_tune), offsetof(psb_tune, ms),'
                  ' sizeof(psb_diag), offsetof(psb_diag, density_err_max));'
+                 ' printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(psb_collider), offsetof(psb_collider, v),'
+                 ' offsetof(psb_collider, data), sizeof(psb_emitter), offsetof(psb_emitter, data),'
+                 ' offsetof(psb_emitter, seed));'
                  ' return 0;}\n')
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(c), "-o", str(exe)], check=True)
@@ -50,7 +55,9 @@ def test_struct_layout_matches_header(tmp_path):
     assert got == [ctypes.sizeof(PsbScene), PsbScene.spacing.offset, ctypes.sizeof(R.PsbStepStats),
                    R.PsbStepStats.iters_total.offset, PsbScene.dem_attraction.offset, ctypes.sizeof(R.IsoGrid),
                    R.IsoGrid.scale.offset, ctypes.sizeof(R.PsbTune), R.PsbTune.ms.offset,
-                   ctypes.sizeof(R.PsbDiag), R.PsbDiag.density_err_max.offset]
+                   ctypes.sizeof(R.PsbDiag), R.PsbDiag.density_err_max.offset,
+                   ctypes.sizeof(PsbCollider), PsbCollider.v.offset, PsbCollider.data.offset,
+                   ctypes.sizeof(PsbEmitter), PsbEmitter.data.offset, PsbEmitter.seed.offset]
 
 
 def test_abi_version_and_status_strings():
@@ -108,3 +115,17 @@ def test_every_compat_launcher_is_exported():
     out = subprocess.run(["nm", "-D", "--defined-only", R.LIB_PATH], capture_output=True, text=True).stdout
     for n in names:
         assert re.search(rf"\bT {n}\b", out), n
+
+
+@pytest.mark.parametrize("header", ["psb.h", "psb_compat.h"])
+@pytest.mark.parametrize("lang", [("gcc", "-std=c99", "c"), ("g++", "-std=c++17", "cpp")])
+def test_header_compiles_strictly(tmp_path, header, lang):
+    """The public headers build warning-free as C99 and C++17 under -pedantic,
+    as a C or C++ host would include them."""
+    cc, std, ext = lang
+    src = tmp_path / f"inc.{ext}"
+    src.write_text(f'#include "{header}"\n')
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    r = subprocess.run([cc, std, "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only",
+                        "-I", os.path.join(ROOT, "include"), "-I", cuda_inc, str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
