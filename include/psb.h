@@ -494,7 +494,12 @@ int psb_clear_emitters(psb_ctx* ctx);
 /* Host only (no context, no GPU): the positions emission number `emission`
  * of this emitter produces, in emission order, at most cap of them (out:
  * cap x 3 floats, may be NULL to count); *n receives the full count. The
- * random emitters use the same draws as the device. */
+ * random emitters use the same draws as the device. PSB_EINVAL (and
+ * psb_add_emitter the same) for an emitter whose loops would not end (a
+ * particle radius that is not positive, a value that is not finite, a step
+ * below the float or double resolution of the coordinates it advances) or
+ * whose emission could exceed 2^31 - 1 points; PSB_ENOMEM when the host
+ * allocation fails. */
 int psb_emitter_positions(const psb_emitter* e, int32_t emission, int64_t cap, float* out, int64_t* n);
 
 /* The scene the context was created with (for a batch: scene 0 with n_max

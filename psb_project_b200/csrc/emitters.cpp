@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <new>
 #include <vector>
 
 #include "psb.h"
@@ -90,33 +91,105 @@ void heart(std::vector<float>& out) {
             }
 }
 
+// The largest emission accepted: a context's particle count is an int32.
+constexpr double kMaxPoints = 2147483647.0;
+
+// True when adding `step` to any value of magnitude up to `mag` moves it by
+// at least three quarters of a step (the step exceeds two ulps there), so a
+// generator loop over that range advances.
+bool advances_f(double mag, float step) {
+    const float m = (float)std::fabs(mag);
+    return std::isfinite(m) && step > 2 * (std::nextafter(m, INFINITY) - m);
+}
+bool advances_d(double mag, double step) {
+    mag = std::fabs(mag);
+    return std::isfinite(mag) && step > 2 * (std::nextafter(mag, INFINITY) - mag);
+}
+bool all_finite(const float* v, int k) {
+    for (int i = 0; i < k; ++i)
+        if (!std::isfinite(v[i])) return false;
+    return true;
+}
+
+// Points on one ring of radius up to r with angular step atan(a / r), the
+// ring loop's bound (dtheta only grows as the radius shrinks).
+double ring_bound(double a, double r) { return 2 * M_PI / std::atan2(a, std::max(r, 0.0)) + 2; }
+
+// An upper bound on the positions one emission of `e` produces, or -1 when
+// the generator's loops would not end: a radius that is not positive, a value
+// that is not finite, or a step below the resolution of the coordinates it
+// advances. Every loop then advances by at least 3/4 of its step, which the
+// per-axis counts (2 extent / step + 2) allow for.
+double emission_bound(const psb_emitter& e) {
+    const float rho = e.particle_radius;
+    const bool rho_ok = rho > 0 && std::isfinite(rho);
+    switch (e.type) {
+        case PSB_EMITTER_BOX: {
+            const float step = rho * 2;
+            if (!rho_ok || !std::isfinite(step) || !all_finite(e.v, 9)) return -1;
+            double b = 1;
+            for (int a = 0; a < 3; ++a) {
+                const double c = e.v[a], s = e.v[3 + a];
+                if (!advances_f(std::fabs(c) + std::fabs(s), step)) return -1;
+                b *= 2 * std::max(s, 0.0) / step + 2;
+            }
+            return b;
+        }
+        case PSB_EMITTER_SPHERE: {
+            if (!rho_ok || !all_finite(e.v, 4)) return -1;
+            const double R = std::max((double)e.v[3], 0.0);
+            if (!advances_d(std::fabs((double)e.v[1]) + R + rho, rho)) return -1;
+            return 2 * (2 * R / rho + 2) * (2 * R / rho + 2) * ring_bound(std::sqrt(2.0) * rho, R);
+        }
+        case PSB_EMITTER_CYLINDER: {
+            if (!rho_ok || !all_finite(e.v, 8)) return -1;
+            const double half = std::fabs((double)e.v[4] * ((double)e.v[7] / 2));
+            const double rb = std::max((double)e.v[6], 0.0);
+            if (!advances_d(std::fabs((double)e.v[1]) + half, rho) || !advances_d(rb + rho, rho)) return -1;
+            return (4 * half / rho + 2) * (2 * rb / rho + 2) * ring_bound(rho, rb);
+        }
+        case PSB_EMITTER_HEART: return 301.0 * 301.0 * 301.0;
+        case PSB_EMITTER_ELLIPSOID: return e.count < 0 ? -1 : (double)e.count;
+        case PSB_EMITTER_MESH:
+            if (e.count < 0 || e.n_faces < 0 || (e.n_faces > 0 && !e.data)) return -1;
+            return (double)e.count * e.n_faces;
+        default: return -1;
+    }
+}
+
 }  // namespace
 
 extern "C" int psb_emitter_positions(const psb_emitter* e, int32_t emission, int64_t cap, float* out, int64_t* n) {
     if (!e || !n || cap < 0 || emission < 0) return PSB_EINVAL;
+    const double bound = emission_bound(*e);
+    if (!(bound >= 0 && bound <= kMaxPoints)) return PSB_EINVAL;
     std::vector<float> pos;
-    switch (e->type) {
-        case PSB_EMITTER_BOX: box(*e, pos); break;
-        case PSB_EMITTER_SPHERE: sphere(*e, pos); break;
-        case PSB_EMITTER_CYLINDER: cylinder(*e, pos); break;
-        case PSB_EMITTER_HEART: heart(pos); break;
-        case PSB_EMITTER_ELLIPSOID:
-            if (e->count < 0) return PSB_EINVAL;
-            pos.resize(3 * (size_t)e->count);
-            for (int64_t i = 0; i < e->count; ++i)
-                psb::emit::ellipsoid_point(e->v, e->seed, (uint32_t)emission, (uint64_t)i, &pos[3 * i]);
-            break;
-        case PSB_EMITTER_MESH: {
-            if (e->count < 0 || e->n_faces < 0 || (e->n_faces > 0 && !e->data)) return PSB_EINVAL;
-            const int64_t m = (int64_t)e->count * e->n_faces;
-            pos.resize(3 * (size_t)m);
-            for (int64_t i = 0; i < m; ++i)
-                psb::emit::mesh_point(e->data + 9 * (i / e->count), e->seed, (uint32_t)emission, (uint64_t)i,
-                                      &pos[3 * i]);
-            break;
+    try {
+        switch (e->type) {
+            case PSB_EMITTER_BOX: box(*e, pos); break;
+            case PSB_EMITTER_SPHERE: sphere(*e, pos); break;
+            case PSB_EMITTER_CYLINDER: cylinder(*e, pos); break;
+            case PSB_EMITTER_HEART: heart(pos); break;
+            case PSB_EMITTER_ELLIPSOID:
+                if (e->count < 0) return PSB_EINVAL;
+                pos.resize(3 * (size_t)e->count);
+                for (int64_t i = 0; i < e->count; ++i)
+                    psb::emit::ellipsoid_point(e->v, e->seed, (uint32_t)emission, (uint64_t)i, &pos[3 * i]);
+                break;
+            case PSB_EMITTER_MESH: {
+                if (e->count < 0 || e->n_faces < 0 || (e->n_faces > 0 && !e->data)) return PSB_EINVAL;
+                const int64_t m = (int64_t)e->count * e->n_faces;
+                pos.resize(3 * (size_t)m);
+                for (int64_t i = 0; i < m; ++i)
+                    psb::emit::mesh_point(e->data + 9 * (i / e->count), e->seed, (uint32_t)emission, (uint64_t)i,
+                                          &pos[3 * i]);
+                break;
+            }
+            default:
+                return PSB_EINVAL;
         }
-        default:
-            return PSB_EINVAL;
+    } catch (const std::bad_alloc&) {
+        return PSB_ENOMEM;
     }
     *n = (int64_t)(pos.size() / 3);
     if (out)

@@ -113,6 +113,36 @@ def test_bad_emitter_rejected():
         E.positions(E.Emitter(9, []))
 
 
+@pytest.mark.parametrize("bad", [
+    E.box([0, 0, 0], [0.1, 0.1, 0.1], 0.0),                   # step 0: the lattice loop would not advance
+    E.box([0, 0, 0], [0.1, 0.1, 0.1], -0.01),
+    E.box([0, 0, 0], [0.1, 0.1, 0.1], float("nan")),
+    E.box([0, 0, 0], [float("inf"), 0.1, 0.1], 0.01),
+    E.box([0, 0, 0], [0.1, float("nan"), 0.1], 0.01),
+    E.box([1e6, 0, 0], [0.1, 0.1, 0.1], 1e-3),               # step below a float ulp at 1e6
+    E.box([0, 0, 0], [10.0, 10.0, 10.0], 1e-3),              # 1.25e14 points
+    E.sphere([0, 0, 0], 0.5, 0.0),
+    E.sphere([0, 1e12, 0], 0.5, 1e-5),                       # step below a double ulp at 1e12
+    E.sphere([0, 0, 0], 100.0, 1e-3),
+    E.cylinder([0, 0, 0], [0, 1, 0], 0.2, 1.0, 0.0),
+    E.cylinder([0, 0, 0], [0, float("inf"), 0], 0.2, 1.0, 0.01),
+    E.cylinder([0, 0, 0], [0, 1, 0], 50.0, 50.0, 1e-3),
+    E.ellipsoid([0, 0, 0], 1.0, 1.0, -1),
+    E.mesh([[0, 0, 0], [1, 0, 0], [0, 0, 1]], [[0, 1, 2]] * 4096, 1 << 20),
+])
+def test_degenerate_emitter_rejected_without_generating(bad):
+    """Emitters whose generator loops would never end, or whose one emission
+    would pass the int32 particle count, fail with PSB_EINVAL at once."""
+    with pytest.raises(R.PsbError):
+        E.positions(bad)
+
+
+def test_bound_admits_the_ordinary_emitters():
+    for e in (E.box([0.3, 0.2, 0.1], [0.2, 0.1, 0.3], 0.005), E.sphere([0.1, 0.0, 0.2], 0.15, 0.01),
+              E.cylinder([0, 0.4, 0], [0, 1, 0], 0.1, 0.3, 0.01), E.box([5.0, 5.0, 5.0], [0.0, 0.0, 0.0], 0.01)):
+        assert E.positions(e).shape[0] >= 1
+
+
 # ---- GPU ---------------------------------------------------------------------------
 
 def _compare(got, ref, x0_pos, v_tol=3e-5):
