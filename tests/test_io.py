@@ -113,6 +113,32 @@ def test_obj_closed_mesh_normals(tmp_path):
         P.write_obj(path, v, np.array([[0, 1, 4]], np.int32))     # index out of range
 
 
+def test_writers_reject_bad_arguments(tmp_path):
+    """The host writers return PSB_EINVAL for negative counts, missing
+    arrays, out-of-range triangle indices, negative volume dimensions, the
+    reference's volume layout on a non-cubic grid, and a path that cannot be
+    opened."""
+    import ctypes
+    from psb_project_b200 import runtime as R
+    L = R.lib()
+    vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+    L.psb_write_txt.argtypes = [ctypes.c_char_p, i32, vp, ctypes.c_double, vp]
+    L.psb_write_obj.argtypes = [ctypes.c_char_p, vp, i64, vp, i64]
+    L.psb_write_vol.argtypes = [ctypes.c_char_p, vp, vp, vp, vp, i32]
+    txt, obj, vol = (str(tmp_path / f).encode() for f in ("a.txt", "a.obj", "a.vol"))
+    pos, rho = np.zeros((2, 3)), np.zeros(2, np.float32)
+    assert L.psb_write_txt(txt, -1, pos.ctypes.data, 1.0, rho.ctypes.data) == 1
+    assert L.psb_write_txt(txt, 2, None, 1.0, rho.ctypes.data) == 1
+    assert L.psb_write_txt(str(tmp_path / "no" / "a.txt").encode(), 2, pos.ctypes.data, 1.0, rho.ctypes.data) == 1
+    v, tri = np.zeros((3, 3), np.float32), np.array([[0, 1, 5]], np.int32)
+    assert L.psb_write_obj(obj, v.ctypes.data, 3, tri.ctypes.data, 1) == 1
+    assert L.psb_write_obj(obj, v.ctypes.data, -3, None, 0) == 1
+    b = np.zeros(3, np.float32)
+    assert L.psb_write_vol(vol, np.zeros(6).ctypes.data, np.array([2, 3, -1], np.int32).ctypes.data,
+                           b.ctypes.data, b.ctypes.data, 0) == 1
+    assert L.psb_write_vol(vol, np.zeros(24).ctypes.data, np.array([2, 3, 4], np.int32).ctypes.data,
+                           b.ctypes.data, b.ctypes.data, 1) == 1
+
 @pytest.mark.gpu
 def test_exports_match_download(tmp_path):
     sc = P.dam_break((10, 8, 6), 0.01, (0.3, 0.3, 0.3), 0.02, dt=5e-4, seed=41)
