@@ -1411,8 +1411,8 @@ int iso_on_device(psb_ctx* c, const psb_iso_grid* g, double level, psb::IsoParam
     if (c->batch) return fail(c, PSB_EINVAL, "iso field: single-scene contexts only");
     long long nn = 1;
     for (int a = 0; a < 3; ++a) {
-        if (g->dims[a] < 2 || !(g->spacing[a] > 0) || !std::isfinite(g->origin[a]))
-            return fail(c, PSB_EINVAL, "iso grid: dims >= 2, spacing > 0, finite origin");
+        if (g->dims[a] < 2 || !(g->spacing[a] > 0) || !std::isfinite(g->spacing[a]) || !std::isfinite(g->origin[a]))
+            return fail(c, PSB_EINVAL, "iso grid: dims >= 2, finite spacing > 0, finite origin");
         nn *= g->dims[a];
     }
     if (3 * nn + 1 >= (1LL << 30)) return fail(c, PSB_EINVAL, "iso grid: at most 2^30 / 3 nodes");
@@ -1424,8 +1424,20 @@ int iso_on_device(psb_ctx* c, const psb_iso_grid* g, double level, psb::IsoParam
     }
     Q.level = level;
     const double h = c->sc.h;
+    // Every node's particle-grid cell, widened by its ring, must fit the
+    // device's int cell coordinates, and the reference profile's ring
+    // floor(1 / scale) stays at 16 cells or fewer (the reference uses 0.65,
+    // one ring), so each node's walk is bounded.
+    const double corner[3] = {c->P.g.gx, c->P.g.gy, c->P.g.gz};
+    for (int a = 0; a < 3; ++a) {
+        const double lo = (g->origin[a] - corner[a]) / c->P.g.cell;
+        const double hi = (g->origin[a] + (g->dims[a] - 1) * g->spacing[a] - corner[a]) / c->P.g.cell;
+        if (!(std::fabs(lo) < 1073741824.0 && std::fabs(hi) < 1073741824.0))
+            return fail(c, PSB_EINVAL, "iso grid: nodes lie too far from the particle grid");
+    }
     if (c->P.ref) {
-        if (!(g->scale > 0)) return fail(c, PSB_EINVAL, "iso grid: reference profile needs scale > 0");
+        if (!(g->scale >= 0.0625 && std::isfinite(g->scale)))
+            return fail(c, PSB_EINVAL, "iso grid: reference profile needs a finite scale >= 1/16");
         Q.r = h / g->scale;
         Q.ring = (int)std::floor(1.0 / g->scale);
     } else {
