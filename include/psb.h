@@ -175,7 +175,8 @@ typedef struct psb_iso_grid {
     int32_t dims[3];
     double scale;               /* REF profile: evaluateIso's scale -- influence radius h/scale over
                                    floor(1/scale) rings of particle-grid cells (SurfaceSPH::extract
-                                   uses 0.65, SurfaceSPH.cpp:31) */
+                                   uses 0.65, SurfaceSPH.cpp:31); finite and >= 1/16, and
+                                   origin/spacing finite, or PSB_EINVAL */
 } psb_iso_grid;
 
 /* The iso field at every node of `grid`, at the current positions (the
