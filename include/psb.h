@@ -233,9 +233,14 @@ int psb_lattice(const int32_t nxyz[3], double spacing, const double origin[3], d
  * device array inside libpsb, held by every GPU that loads the library
  * (about 2.1 MB) until the process exits.
  * Limit: n <= PSB_NOALLOC_MAX_N; larger n returns PSB_EINVAL (with a message
- * on stderr). The first call on each device looks up the array's device
- * address. All calls share the one array: calls that overlap on the GPU (other streams or
- * threads on the same device) race and corrupt each other's results. */
+ * on stderr). Every call looks up the array's address on the current device
+ * (a host-side lookup), so the entry point stays valid after the host resets
+ * the device. Sorting in place (keys_out == keys_in and/or vals_out ==
+ * vals_in) is supported; any other overlap of the four ranges returns
+ * PSB_EINVAL. A CUDA error already pending when the call starts is left in
+ * place and the call returns PSB_ECUDA without running. All calls share the
+ * one array: calls that overlap on the GPU (other streams or threads on the
+ * same device) race and corrupt each other's results. */
 #define PSB_NOALLOC_MAX_N 262144
 int psb_sort_cells_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                            uint32_t* vals_out, int32_t n, int32_t key_bits, void* stream);

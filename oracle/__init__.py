@@ -20,7 +20,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libpsbref.so")
-REF_SRC = os.environ.get("PSB_REFERENCE_SRC", "/root/reference/src")
+# The reference tree's src/ directory, when it is present: PSB_REFERENCE_SRC,
+# else a reference checkout beside this repository (<repo>/../reference/src).
+REF_SRC = os.environ.get("PSB_REFERENCE_SRC") or os.path.join(os.path.dirname(HERE), os.pardir, "reference", "src")
 
 ORC_MAX_ITERS = 64
 

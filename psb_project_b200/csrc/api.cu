@@ -23,6 +23,7 @@
 #include "psb.h"
 #include "psb_internal.cuh"
 #include "colliders.cuh"
+#include "emitters.h"
 
 using psb::Params;
 
@@ -1667,10 +1668,17 @@ int psb_add_emitter(psb_ctx* c, const psb_emitter* e) {
                          e->type == PSB_EMITTER_CYLINDER;
     if (lattice && !(e->particle_radius > 0.f))
         return fail(c, PSB_EINVAL, "psb_add_emitter: particle_radius must be > 0");
-    int64_t per = 0;
-    if (psb_emitter_positions(e, 0, 0, nullptr, &per) != PSB_OK)
-        return fail(c, PSB_EINVAL, "psb_add_emitter: bad type, count or faces");
-    if (per > (int64_t)c->n_max) return fail(c, PSB_EINVAL, "psb_add_emitter: one emission exceeds the capacity");
+    // One generation, stopped at the context's free capacity: an emission
+    // that could never be appended is refused before it fills host memory.
+    const int64_t free_slots = (int64_t)c->n_max - c->n;
+    std::vector<float> xyz;
+    const int g = psb::emit::generate(*e, 0, free_slots, xyz);
+    if (g == PSB_EOVERFLOW_NBR)
+        return fail(c, PSB_EINVAL, "psb_add_emitter: one emission exceeds the " + std::to_string(free_slots) +
+                                       " free slots of the context's capacity");
+    if (g == PSB_ENOMEM) return fail(c, PSB_ENOMEM, "psb_add_emitter: host memory for the emission");
+    if (g != PSB_OK) return fail(c, PSB_EINVAL, "psb_add_emitter: bad type, count or faces");
+    const int64_t per = (int64_t)(xyz.size() / 3);
     cudaSetDevice(c->device);
     EmitterRec r;
     r.e = *e;
@@ -1679,9 +1687,6 @@ int psb_add_emitter(psb_ctx* c, const psb_emitter* e) {
     const bool random = e->type == PSB_EMITTER_ELLIPSOID || e->type == PSB_EMITTER_MESH;
     int rc = PSB_OK;
     if (!random && per > 0) {
-        std::vector<float> xyz(3 * (size_t)per);
-        int64_t m = 0;
-        psb_emitter_positions(e, 0, per, xyz.data(), &m);
         rc = dalloc(c, &r.d_list, xyz.size());
         if (rc == PSB_OK)
             rc = cuda_check(c, cudaMemcpy(r.d_list, xyz.data(), sizeof(float) * xyz.size(), cudaMemcpyHostToDevice),

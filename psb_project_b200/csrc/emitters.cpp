@@ -18,14 +18,23 @@
 
 namespace {
 
-void push(std::vector<float>& out, double x, double y, double z) {
-    out.push_back((float)x);
-    out.push_back((float)y);
-    out.push_back((float)z);
+// The positions of one emission, bounded: a push beyond `limit` points
+// stops the generator (TooMany) before the vector grows any further.
+struct TooMany {};
+struct Sink {
+    std::vector<float>& v;
+    size_t limit;
+};
+
+void push(Sink& out, double x, double y, double z) {
+    if (out.v.size() / 3 >= out.limit) throw TooMany{};
+    out.v.push_back((float)x);
+    out.v.push_back((float)y);
+    out.v.push_back((float)z);
 }
 
 // EmitterBox.cpp:29-47
-void box(const psb_emitter& e, std::vector<float>& out) {
+void box(const psb_emitter& e, Sink& out) {
     const double cx = e.v[0], cy = e.v[1], cz = e.v[2];
     const float sx = e.v[3], sy = e.v[4], sz = e.v[5];
     const double wx = e.v[6], wy = e.v[7], wz = e.v[8];
@@ -40,7 +49,7 @@ void box(const psb_emitter& e, std::vector<float>& out) {
 
 // One ring of radius r at height y: angles 0, dt, 2 dt, ... while <= 2 pi
 // (EmitterSphere.cpp / EmitterCylinder.cpp inner loop).
-void ring(double cx, double cz, double y, double r, double dtheta, std::vector<float>& out) {
+void ring(double cx, double cz, double y, double r, double dtheta, Sink& out) {
     double theta = 0, theta_ap = 1;
     while (theta <= 2 * M_PI && theta_ap > 0) {
         push(out, cx + r * cos(theta), y, cz + r * sin(theta));
@@ -50,7 +59,7 @@ void ring(double cx, double cz, double y, double r, double dtheta, std::vector<f
 }
 
 // EmitterSphere.cpp: layers from center.y up, then from center.y - rho down
-void sphere(const psb_emitter& e, std::vector<float>& out) {
+void sphere(const psb_emitter& e, Sink& out) {
     const double cx = e.v[0], cy = e.v[1], cz = e.v[2];
     const float R = e.v[3], rho = e.particle_radius;
     auto layer = [&](double y) {
@@ -65,7 +74,7 @@ void sphere(const psb_emitter& e, std::vector<float>& out) {
 }
 
 // EmitterCylinder.cpp
-void cylinder(const psb_emitter& e, std::vector<float>& out) {
+void cylinder(const psb_emitter& e, Sink& out) {
     const double cx = e.v[0], cy = e.v[1], cz = e.v[2];
     const double dy = e.v[4];
     const float rb = e.v[6], len = e.v[7], rho = e.particle_radius;
@@ -80,7 +89,7 @@ void cylinder(const psb_emitter& e, std::vector<float>& out) {
 }
 
 // EmitterGirly.cpp: the grid [-3, 3]^3 at 0.02, x outer, z inner
-void heart(std::vector<float>& out) {
+void heart(Sink& out) {
     const double eps = 0.001, step = 0.02;
     for (double x = -3.0; x <= 3.0; x += step)
         for (double y = -3.0; y <= 3.0; y += step)
@@ -159,38 +168,57 @@ double emission_bound(const psb_emitter& e) {
 
 }  // namespace
 
-extern "C" int psb_emitter_positions(const psb_emitter* e, int32_t emission, int64_t cap, float* out, int64_t* n) {
-    if (!e || !n || cap < 0 || emission < 0) return PSB_EINVAL;
-    const double bound = emission_bound(*e);
+namespace psb {
+namespace emit {
+
+int generate(const psb_emitter& e, int32_t emission, int64_t limit, std::vector<float>& pos) {
+    if (emission < 0 || limit < 0) return PSB_EINVAL;
+    const double bound = emission_bound(e);
     if (!(bound >= 0 && bound <= kMaxPoints)) return PSB_EINVAL;
-    std::vector<float> pos;
+    pos.clear();
+    if ((e.type == PSB_EMITTER_ELLIPSOID || e.type == PSB_EMITTER_MESH) && bound > (double)limit)
+        return PSB_EOVERFLOW_NBR;     // the count is exact for the random emitters: nothing to generate
+    Sink out{pos, (size_t)limit};
     try {
-        switch (e->type) {
-            case PSB_EMITTER_BOX: box(*e, pos); break;
-            case PSB_EMITTER_SPHERE: sphere(*e, pos); break;
-            case PSB_EMITTER_CYLINDER: cylinder(*e, pos); break;
-            case PSB_EMITTER_HEART: heart(pos); break;
+        switch (e.type) {
+            case PSB_EMITTER_BOX: box(e, out); break;
+            case PSB_EMITTER_SPHERE: sphere(e, out); break;
+            case PSB_EMITTER_CYLINDER: cylinder(e, out); break;
+            case PSB_EMITTER_HEART: heart(out); break;
             case PSB_EMITTER_ELLIPSOID:
-                if (e->count < 0) return PSB_EINVAL;
-                pos.resize(3 * (size_t)e->count);
-                for (int64_t i = 0; i < e->count; ++i)
-                    psb::emit::ellipsoid_point(e->v, e->seed, (uint32_t)emission, (uint64_t)i, &pos[3 * i]);
+                pos.resize(3 * (size_t)e.count);
+                for (int64_t i = 0; i < e.count; ++i)
+                    ellipsoid_point(e.v, e.seed, (uint32_t)emission, (uint64_t)i, &pos[3 * i]);
                 break;
             case PSB_EMITTER_MESH: {
-                if (e->count < 0 || e->n_faces < 0 || (e->n_faces > 0 && !e->data)) return PSB_EINVAL;
-                const int64_t m = (int64_t)e->count * e->n_faces;
+                const int64_t m = (int64_t)e.count * e.n_faces;
                 pos.resize(3 * (size_t)m);
                 for (int64_t i = 0; i < m; ++i)
-                    psb::emit::mesh_point(e->data + 9 * (i / e->count), e->seed, (uint32_t)emission, (uint64_t)i,
-                                          &pos[3 * i]);
+                    mesh_point(e.data + 9 * (i / e.count), e.seed, (uint32_t)emission, (uint64_t)i, &pos[3 * i]);
                 break;
             }
             default:
                 return PSB_EINVAL;
         }
+    } catch (const TooMany&) {
+        pos.clear();
+        return PSB_EOVERFLOW_NBR;
     } catch (const std::bad_alloc&) {
+        pos.clear();
         return PSB_ENOMEM;
     }
+    return PSB_OK;
+}
+
+}  // namespace emit
+}  // namespace psb
+
+extern "C" int psb_emitter_positions(const psb_emitter* e, int32_t emission, int64_t cap, float* out, int64_t* n) {
+    if (!e || !n || cap < 0 || emission < 0) return PSB_EINVAL;
+    std::vector<float> pos;
+    const int rc = psb::emit::generate(*e, emission, (int64_t)kMaxPoints, pos);
+    if (rc == PSB_EOVERFLOW_NBR) return PSB_EINVAL;
+    if (rc != PSB_OK) return rc;
     *n = (int64_t)(pos.size() / 3);
     if (out)
         for (int64_t i = 0; i < 3 * std::min<int64_t>(cap, *n); ++i) out[i] = pos[(size_t)i];

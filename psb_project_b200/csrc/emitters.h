@@ -9,6 +9,9 @@
 #pragma once
 #include <cmath>
 #include <cstdint>
+#include <vector>
+
+#include "psb.h"
 
 #ifdef __CUDACC__
 #define PSB_HD __host__ __device__
@@ -56,6 +59,12 @@ PSB_HD inline void mesh_point(const float* face, uint64_t seed, uint32_t e, uint
     for (int k = 0; k < 3; ++k)
         out[k] = (float)(((double)a * face[k] + (double)b * face[3 + k] + (double)c * face[6 + k]) / s);
 }
+
+// Host: the positions of one emission of e (xyz, stride 3) into pos, at
+// most `limit` points. PSB_EINVAL for an emitter whose loops cannot end or
+// whose bound passes 2^31 - 1 points, PSB_EOVERFLOW_NBR when the emission has
+// more than `limit` points (the generator stops there), PSB_ENOMEM.
+int generate(const psb_emitter& e, int32_t emission, int64_t limit, std::vector<float>& pos);
 
 }  // namespace emit
 }  // namespace psb

@@ -14,8 +14,10 @@
 // PSB_NOALLOC_MAX_N elements. Every GPU that loads the library holds it
 // (about 2.1 MB) until the process exits. Host code cannot pass the array's
 // name to a kernel (it is a host-side stand-in, not a device address), so
-// the address is fetched with cudaGetSymbolAddress once per device, on the
-// first call made with that device current.
+// every call looks the address up with cudaGetSymbolAddress on the current
+// device. The lookup is a host-side table read once the module is loaded;
+// not caching it keeps the address right after the host application resets
+// the device and the runtime loads the module again.
 //
 // All calls share the one array and it keeps the last call's contents.
 // Nothing in it needs clearing: every pass writes its histogram block by
@@ -23,9 +25,11 @@
 // before it is read. Calls that overlap on the GPU (different streams, or
 // different host threads on the same device) race on the array and corrupt
 // each other's results; the caller must serialise them.
+//
+// Sorting in place (keys_out == keys_in, vals_out == vals_in, or both) is
+// supported; any other overlap of the four ranges is refused.
 #include <cuda_runtime.h>
 #include <cstdio>
-#include <mutex>
 
 #include "psb.h"
 #include "psb_internal.cuh"
@@ -39,30 +43,30 @@ constexpr size_t kScratchWords = 2 * (size_t)kMaxN + 256 * (size_t)kMaxBlocks + 
 // keys ping-pong | values ping-pong | digit histogram (256 x tiles) | digit totals (256)
 static __device__ __align__(256) uint32_t g_sort_scratch[kScratchWords];
 
-constexpr int kMaxDevices = 64;
-uint32_t* g_scratch_addr[kMaxDevices] = {};
-std::mutex g_setup_mutex;
-
-// Device address of the scratch on the current device, fetched once.
+// Device address of the scratch on the current device.
 int scratch_for_current_device(uint32_t** out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-        std::fprintf(stderr, "psb_sort_cells_noalloc: no usable current device (%s)\n", cudaGetErrorString(e));
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
+    if (e != cudaSuccess || !p) {
+        std::fprintf(stderr, "psb_sort_cells_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
         return PSB_ECUDA;
     }
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_sort_scratch);
-        if (e != cudaSuccess || !p) {
-            std::fprintf(stderr, "psb_sort_cells_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
-                         cudaGetErrorString(e));
-            return PSB_ECUDA;
-        }
-        g_scratch_addr[dev] = (uint32_t*)p;
+    *out = (uint32_t*)p;
+    return PSB_OK;
+}
+
+// Whether the byte ranges [a, a + bytes) and [b, b + bytes) share a byte.
+bool overlap(const void* a, const void* b, size_t bytes) {
+    const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+    return x < y + bytes && y < x + bytes;
+}
+
+int copy(cudaStream_t st, uint32_t* dst, const uint32_t* src, int32_t n) {
+    const cudaError_t e = cudaMemcpyAsync(dst, src, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "psb_sort_cells_noalloc: copy failed: %s\n", cudaGetErrorString(e));
+        return PSB_ECUDA;
     }
-    *out = g_scratch_addr[dev];
     return PSB_OK;
 }
 
@@ -80,29 +84,46 @@ extern "C" int psb_sort_cells_noalloc(const uint32_t* keys_in, const uint32_t* v
         return PSB_EINVAL;
     }
     if (n == 0) return PSB_OK;
+    const size_t bytes = sizeof(uint32_t) * (size_t)n;
+    if (overlap(keys_out, vals_out, bytes) || overlap(keys_out, vals_in, bytes) || overlap(vals_out, keys_in, bytes) ||
+        (keys_out != keys_in && overlap(keys_out, keys_in, bytes)) ||
+        (vals_out != vals_in && overlap(vals_out, vals_in, bytes))) {
+        std::fprintf(stderr, "psb_sort_cells_noalloc: overlapping buffers (only keys_out == keys_in and "
+                             "vals_out == vals_in may alias)\n");
+        return PSB_EINVAL;
+    }
+    // An error left pending by an earlier call of the caller's is not this
+    // sort's: refuse to run and leave it for the caller to read.
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        std::fprintf(stderr, "psb_sort_cells_noalloc: a CUDA error is pending from before the call: %s\n",
+                     cudaGetErrorString(pending));
+        return PSB_ECUDA;
+    }
     uint32_t* scratch = nullptr;
-    const int rc = scratch_for_current_device(&scratch);
+    int rc = scratch_for_current_device(&scratch);
     if (rc != PSB_OK) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     uint32_t* tmp_keys = scratch;
     uint32_t* tmp_vals = scratch + kMaxN;
     uint32_t* hist = scratch + 2 * (size_t)kMaxN;
     // The sort ping-pongs between its two buffers starting from the first:
-    // copy the input into the caller's output, sort between output and
-    // scratch, and copy back if the last pass ended in the scratch.
-    cudaMemcpyAsync(keys_out, keys_in, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(vals_out, vals_in, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
+    // copy the input into the caller's output (unless it is the input),
+    // sort between output and scratch, and copy back if the last pass ended
+    // in the scratch.
+    if (keys_out != keys_in && (rc = copy(st, keys_out, keys_in, n)) != PSB_OK) return rc;
+    if (vals_out != vals_in && (rc = copy(st, vals_out, vals_in, n)) != PSB_OK) return rc;
     uint32_t* keys[2] = {keys_out, tmp_keys};
     uint32_t* vals[2] = {vals_out, tmp_vals};
     const int res = psb::radix_sort(st, n, key_bits, keys, vals, hist, kMaxBlocks);
-    if (res == 1) {
-        cudaMemcpyAsync(keys_out, tmp_keys, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
-        cudaMemcpyAsync(vals_out, tmp_vals, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
-    }
-    const cudaError_t e = cudaGetLastError();
+    const cudaError_t e = cudaGetLastError();     // the sort's launches
     if (e != cudaSuccess) {
         std::fprintf(stderr, "psb_sort_cells_noalloc: %s\n", cudaGetErrorString(e));
         return PSB_ECUDA;
+    }
+    if (res == 1) {
+        if ((rc = copy(st, keys_out, tmp_keys, n)) != PSB_OK) return rc;
+        if ((rc = copy(st, vals_out, tmp_vals, n)) != PSB_OK) return rc;
     }
     return PSB_OK;
 }

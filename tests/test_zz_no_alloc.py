@@ -36,13 +36,13 @@ def regular_path(sc):
                 sim.read_field(R.FIELD_SORTED_ID))
 
 
-def noalloc_sort(keys, vals, bits):
+def noalloc_sort(keys, vals, bits, in_place=False):
     import torch
     dev = torch.device("cuda", 0)
     k_in = torch.from_numpy(keys.view(np.int32)).to(dev)
     v_in = torch.from_numpy(vals.view(np.int32)).to(dev)
-    k_out = torch.full_like(k_in, -1)
-    v_out = torch.full_like(v_in, -1)
+    k_out = k_in if in_place else torch.full_like(k_in, -1)
+    v_out = v_in if in_place else torch.full_like(v_in, -1)
     stream = torch.cuda.current_stream(dev)
     vp = lambda t: ctypes.c_void_p(t.data_ptr())
     rc = R.lib().psb_sort_cells_noalloc(vp(k_in), vp(v_in), vp(k_out), vp(v_out), keys.shape[0], bits,
@@ -62,6 +62,29 @@ def test_noalloc_sort_matches_regular_path_twice():
         assert rc == R.OK
         assert np.array_equal(k, sorted_keys)
         assert np.array_equal(v, sorted_ids.astype(np.uint32))
+
+
+def test_noalloc_sort_in_place():
+    """keys_out == keys_in and vals_out == vals_in: the sort runs in the
+    caller's buffers (the copy-in is skipped) and gives the same result."""
+    pytest.importorskip("torch")
+    sc = P.config_scene("C0")
+    keys_by_id, sorted_keys, sorted_ids = regular_path(sc)
+    rc, k, v = noalloc_sort(keys_by_id, np.arange(sc.n, dtype=np.uint32), key_bits(sc), in_place=True)
+    assert rc == R.OK
+    assert np.array_equal(k, sorted_keys)
+    assert np.array_equal(v, sorted_ids.astype(np.uint32))
+
+
+def test_noalloc_sort_rejects_partial_overlap():
+    """Outputs that overlap an input other than itself, or each other, are
+    refused before anything runs (the pointers are never dereferenced)."""
+    L = R.lib()
+    n = 1024
+    a, b = ctypes.c_void_p(1 << 20), ctypes.c_void_p((1 << 20) + 64)
+    c, d = ctypes.c_void_p(1 << 24), ctypes.c_void_p(1 << 26)
+    assert L.psb_sort_cells_noalloc(a, c, b, d, n, 20, None) == R.EINVAL     # keys_out overlaps keys_in
+    assert L.psb_sort_cells_noalloc(a, c, d, d, n, 20, None) == R.EINVAL     # keys_out == vals_out
 
 
 def test_noalloc_sort_rejects_sizes_beyond_its_scratch():
