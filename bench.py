@@ -80,7 +80,11 @@ def parse():
     ap.add_argument("--warm-start", choices=["zero", "previous", "learned"], default="learned",
                     help="zero: plain PCISPH (each step's corrector starts from p = 0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-steps", type=int, default=1)
+    ap.add_argument("--cpu-sample-steps", type=int, default=20)
+    ap.add_argument("--mlp", choices=["silu6", "relu7"], default="silu6",
+                    help="the learned warm start's network: silu6, the configured 6-input SiLU network, or relu7")
+    ap.add_argument("--no-variant", action="store_true",
+                    help="learned: do not train and compare the other network")
     ap.add_argument("--presolve", type=int, default=256, help="initial-pressure corrector passes before the warm-up")
     ap.add_argument("--train-steps", type=int, default=None,
                     help="plain-PCISPH steps recorded for training (learned; default 400, C3: 100)")
@@ -88,7 +92,7 @@ def parse():
     ap.add_argument("--train-batch", type=int, default=65536)
     ap.add_argument("--train-lr", type=float, default=3e-3, help="peak learning rate of the cosine schedule")
     ap.add_argument("--xsph", type=float, default=None, help="override the scene's XSPH velocity smoothing factor")
-    ap.add_argument("--no-graph", action="store_true", help="C3: launch kernel by kernel instead of CUDA graphs")
+    ap.add_argument("--no-graph", action="store_true", help="launch kernel by kernel instead of CUDA graphs")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch configuration)")
     ap.add_argument("--tune-cache", default=None,
                     help="JSON cache of tuned launch configurations: a bucket found there is not tuned again; "
@@ -193,20 +197,59 @@ def ncu_traffic():
         return {}
 
 
-def cpu_baseline_port(sc, snap, steps: int) -> dict:
+def cpu_baseline_port(sc, snap, steps: int, weights=None, arch: int = 0) -> dict:
     """The FP64 oracle (a C port of the same method, OpenMP on every host
     core) on a bounded sample: `steps` steps of the same scene from the same
-    state the GPU's timed steps start from."""
+    state the GPU's timed steps start from. With the learned warm start each
+    step's initial pressure comes from the same network on the CPU (FP64
+    features, BF16 rounding points) and the oracle's corrector starts there."""
     import oracle
-    sim = oracle.OracleSim(sc, snap["pos"], snap["vel"], snap["vel_half"], snap["pressure"])
+    import psb_project_b200 as P
+    learned = weights is not None and sc.warm_start == P.WARM_LEARNED
+    osc = sc.replace(warm_start=P.WARM_PREVIOUS) if learned else sc
+    sim = oracle.OracleSim(osc, snap["pos"], snap["vel"], snap["vel_half"], snap["pressure"])
     t0 = time.perf_counter()
     iters = []
     for _ in range(steps):
+        if learned:
+            sim.p[:] = oracle.learned_pressure(sc, sim.pos, sim.vel, sim.p, weights, arch)
         iters.append(sim.step().iters)
     dt = time.perf_counter() - t0
+    start = "learned warm start (CPU features and network)" if learned else \
+        {P.WARM_ZERO: "zero start", P.WARM_PREVIOUS: "previous-pressure start"}.get(sc.warm_start, "")
     return {"value": sc.n * steps / dt, "unit": UNIT, "cores": host_cores(), "kind": "port",
-            "sample": f"{steps} step(s) of the {sc.n:,}-particle scene from the GPU's timed start state "
-                      f"({sum(iters)} corrections), FP64 oracle, {host_cores()} threads on {cpu_model()}"}
+            "iters_per_step": iters,
+            "sample": f"{steps} steps of the {sc.n:,}-particle scene from the GPU's timed start state, {start} "
+                      f"({sum(iters)} corrections, {np.mean(iters):.2f} per step), FP64 oracle, "
+                      f"{host_cores()} threads on {cpu_model()}"}
+
+
+def oracle_error(sim, sc, snap) -> dict:
+    """The error of one GPU step against the FP64 oracle on the same state:
+    the first step from the timed start state, through the C ABI; the oracle
+    starts its corrector from the GPU's own initial pressure (the warm
+    start's output, psb_warm_start), so both run the same method on the same
+    inputs. Errors are relative: density element-wise, pressure and
+    velocity to the field's max, position to the step's largest
+    displacement."""
+    import oracle
+    import psb_project_b200 as P
+    sim.upload(snap["pos"], snap["vel"], snap["vel_half"], snap["pressure"])
+    _, p0 = sim.warm_start()
+    sim.step(1)
+    out = sim.download()
+    sg = sim.stats()
+    orc = oracle.OracleSim(sc.replace(warm_start=P.WARM_PREVIOUS), snap["pos"], snap["vel"], snap["vel_half"], p0)
+    so = orc.step()
+    rel = lambda a, b: float(np.max(np.abs(np.asarray(a, np.float64) - b)) / max(float(np.max(np.abs(b))), 1e-300))
+    disp = float(np.max(np.abs(orc.pos - snap["pos"])))
+    return {"density": float(np.max(np.abs(out["density"] - orc.rho) / orc.rho)),
+            "pressure": rel(out["pressure"], orc.p), "velocity": rel(out["vel"], orc.vel),
+            "position": float(np.max(np.abs(out["pos"] - orc.pos))) / max(disp, 1e-300),
+            "iters_gpu": int(sg.iters), "iters_oracle": int(so.iters),
+            "sample": "first step from the timed start state, FP32 GPU against the FP64 oracle from the same "
+                      "initial pressure; density element-wise, pressure and velocity relative to the field max, "
+                      "position relative to the step's largest displacement"}
 
 
 def run_reference(args):
@@ -273,12 +316,20 @@ def run_ours(args):
     max_over_ranks = rep_.max_over_ranks
 
     tune = None       # the autotuner's choice, given to every context created after it
+    archs = {"silu6": P.runtime.MLP_SILU6, "relu7": P.runtime.MLP_RELU7}
+    arch = archs[args.mlp]
+    weights = {}      # trained networks by name
 
-    def make(mode):
+    def make(mode, net=None, graph=True):
         s_ = P.Simulation(base.replace(warm_start=mode))
         s_.set_stream(stream.cuda_stream)
+        if net is not None:
+            s_.mlp_set_arch(archs[net])
+            s_.mlp_set_weights(weights[net])
         if tune is not None:
             s_.tune_set(**{k: tune[k] for k in TUNE_KEYS})
+        if graph and pcisph_cfg and not args.no_graph:
+            s_.set_graph(True)
         return s_
 
     # Set-up (untimed): the dam at rest with its initial pressure, then plain
@@ -286,33 +337,39 @@ def run_ours(args):
     # training targets), then the warm-up. The timed passes all restart from
     # the snapshot taken after it.
     pcisph_cfg = sc.method == P.PCISPH and sc.profile == P.PROFILE_CONFIG
-    gen = make(P.WARM_ZERO)
+    gen = make(P.WARM_ZERO, graph=False)
     gen.upload(P.scene_positions(sc))
     if pcisph_cfg and args.presolve > 0:
         gen.presolve(args.presolve)      # initial pressure of the dam at rest
     train_info = None
-    weights = None
-    if sc.warm_start == P.WARM_LEARNED:
+    learned = sc.warm_start == P.WARM_LEARNED
+    nets = [args.mlp] + ([] if args.no_variant else [k for k in archs if k != args.mlp])
+    if learned:
+        # plain PCISPH steps record (features, converged pressure); the 7-input
+        # network's features include the 6-input one's, so one recording serves both
         t0 = time.perf_counter()
+        gen.mlp_set_arch(P.runtime.MLP_RELU7)
         gen.mlp_collect(stride=64, capacity=max(1, (args.train_steps + 1) * ((n + 63) // 64)))
         gen.step(args.train_steps)
         gen.mlp_collect(0)
         rows, _, _ = gen.mlp_dataset(fetch=False)
-        t1 = time.perf_counter()
-        gen.mlp_set_weights(P.mlp_init_weights(rank))
-        loss0 = gen.mlp_train(1, args.train_batch, 1e-3, seed=11)
-        loss = gen.mlp_fit(args.train_iters, args.train_batch, args.train_lr, chunks=10, seed=12)
-        weights = gen.mlp_get_weights()
-        train_info = {"recorded_steps": args.train_steps, "rows": int(rows), "adam_steps": args.train_iters // 10 * 10 + 1,
-                      "batch": args.train_batch, "lr": args.train_lr, "schedule": "cosine, 10 chunks",
-                      "loss_first": loss0, "loss_last": loss,
-                      "record_s": round(t1 - t0, 2), "train_s": round(time.perf_counter() - t1, 2)}
+        train_info = {"recorded_steps": args.train_steps, "rows": int(rows), "record_s": round(time.perf_counter() - t0, 2),
+                      "adam_steps": args.train_iters // 10 * 10 + 1, "batch": args.train_batch, "lr": args.train_lr,
+                      "schedule": "cosine, 10 chunks", "networks": {}}
+        for net in nets:
+            t1 = time.perf_counter()
+            gen.mlp_set_arch(archs[net])
+            gen.mlp_set_weights(P.mlp_init_weights(rank, archs[net]))
+            loss0 = gen.mlp_train(1, args.train_batch, 1e-3, seed=11)
+            loss = gen.mlp_fit(args.train_iters, args.train_batch, args.train_lr, chunks=10, seed=12)
+            weights[net] = gen.mlp_get_weights()
+            train_info["networks"][net] = {"params": int(weights[net].size), "loss_first": loss0, "loss_last": loss,
+                                           "train_s": round(time.perf_counter() - t1, 2)}
+        train_info["train_s"] = train_info["networks"][args.mlp]["train_s"]
     gen.step(args.warmup)
     snap = gen.download()
     gen.close()
-    sim = make(sc.warm_start)
-    if weights is not None:
-        sim.mlp_set_weights(weights)
+    sim = make(sc.warm_start, args.mlp if learned else None)
     barrier()
 
     def restore(s):
@@ -403,14 +460,19 @@ def run_ours(args):
             (args.train_steps if train_info else 0) + args.warmup + 1,
             (args.train_steps if train_info else 0) + args.warmup + args.eval_steps)
         comparison[args.warm_start] = eval_pass(sim)
-        for name, mode in (("zero", P.WARM_ZERO), ("previous", P.WARM_PREVIOUS)):
-            if mode == sc.warm_start:
+        if learned:
+            comparison[args.warm_start]["network"] = args.mlp
+        others = [("zero", P.WARM_ZERO, None), ("previous", P.WARM_PREVIOUS, None)]
+        if learned:
+            others += [("learned_" + net, P.WARM_LEARNED, net) for net in nets[1:]]
+        for name, mode, net in others:
+            if mode == sc.warm_start and net is None:
                 continue
-            other = make(mode)
+            other = make(mode, net)
             comparison[name] = eval_pass(other)
             other.close()
         this = comparison[args.warm_start]
-        for name in ("zero", "previous"):
+        for name, _, _ in others:
             if name in comparison and name != args.warm_start:
                 o = comparison[name]
                 o["iters_ratio_over_" + args.warm_start] = o["iters_mean"] / max(this["iters_mean"], 1e-9)
@@ -429,13 +491,19 @@ def run_ours(args):
     kernels = {k: {"launches": l, "ms": round(v, 3), "share": round(v / tot_ms, 4)} for k, (l, v) in prof.items()}
 
     cpu = None
+    err = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            # the FP64 port has no MLP: it runs the previous-pressure warm start
-            cpu_sc = sc.replace(warm_start=P.WARM_PREVIOUS) if sc.warm_start == P.WARM_LEARNED else sc
-            cpu = cpu_baseline_port(cpu_sc, snap, args.cpu_sample_steps)
+            cpu = cpu_baseline_port(sc, snap, args.cpu_sample_steps, weights.get(args.mlp), arch)
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": host_cores(), "kind": "port", "sample": f"failed: {ex}"}
+        if pcisph_cfg:
+            try:
+                probe = make(sc.warm_start, args.mlp if learned else None, graph=False)
+                err = oracle_error(probe, sc, snap)
+                probe.close()
+            except Exception as ex:
+                err = {"failed": str(ex)}
 
     if rank == 0:
         out = {
@@ -444,7 +512,8 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": sc.name, "particles": n, "eta": sc.eta, "min_iters": sc.min_iters,
                        "max_iters": sc.max_iters, "warm_start": args.warm_start, "dt": sc.dt, "h": sc.h,
-                       "xsph": sc.xsph,
+                       "xsph": sc.xsph, "network": args.mlp if learned else None,
+                       "graph": pcisph_cfg and not args.no_graph,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "working set > L2 (state, lists and scratch ~%d MB per GPU)"
                              % int(n * (3 * 16 * 2 + 8 * 2 + 4 * 2 + 16 * 4 + 8 + 4 + 4 * sc.nbr_cap + 4) / 1e6),
@@ -467,6 +536,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "clocks": clk,
             "cpu_baseline": cpu,
+            "oracle_error": err,
         }
         print(json.dumps(out))
     rep_.close()

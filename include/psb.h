@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PSB_ABI_VERSION 1
+#define PSB_ABI_VERSION 2
 
 /* Status codes. The reference's launchers return void and never check
  * (src/common.cu:63-66); every call here returns one of these. */
@@ -246,18 +246,42 @@ int psb_sort_cells_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uin
                            uint32_t* vals_out, int32_t n, int32_t key_bits, void* stream);
 
 /* Learned warm start (CONFIG-profile PCISPH, warm_start = PSB_WARM_LEARNED):
- * a per-particle MLP 7 -> 64 -> 64 -> 1 (ReLU), BF16 weights and
- * activations with FP32 accumulation, predicts each step's initial
- * pressure; the corrector still iterates to the same eta. No counterpart in
- * the reference, which starts every step from p = 0
- * (PciSphSystem_Kernel.cu:131). Parameters (FP32 master copy), in order:
- * W1[64][7], b1[64], W2[64][64], b2[64], W3[64], b3. Inputs: neighbour count,
+ * a per-particle MLP with BF16 weights and activations and FP32
+ * accumulation predicts each step's initial pressure; the corrector still
+ * iterates to the same eta. No counterpart in the reference, which starts
+ * every step from p = 0 (PciSphSystem_Kernel.cu:131). Two networks:
+ *   PSB_MLP_SILU6 (the default): 6 -> 64 -> 64 -> 1, SiLU, 4,673 parameters;
+ *   PSB_MLP_RELU7: 7 -> 64 -> 64 -> 1, ReLU, 4,737 parameters.
+ * Parameters (FP32 master copy), in order: W1[64][n_in], b1[64],
+ * W2[64][64], b2[64], W3[64], b3. Inputs, in order: neighbour count,
  * advected density, velocity divergence, previous pressure, wall distance,
- * density-gradient magnitude, previous pressure smoothed with the poly6
- * weights over the neighbours (scaled as in psb_project_b200/csrc/sph.cu,
- * k_density_x). */
-#define PSB_MLP_PARAMS 4737
+ * density-gradient magnitude (the six of PSB_MLP_SILU6), and for
+ * PSB_MLP_RELU7 the previous pressure smoothed with the poly6 weights over
+ * the neighbours (scaled as in psb_project_b200/csrc/sph.cu, k_density_x).
+ * Feature rows are PSB_MLP_FEATURE_STRIDE floats; the network reads the
+ * first n_in. */
+#define PSB_MLP_SILU6 0
+#define PSB_MLP_RELU7 1
+#define PSB_MLP_PARAMS 4737          /* the larger network's count: a buffer of this size fits either */
+#define PSB_MLP_PARAMS_SILU6 4673
 #define PSB_MLP_FEATURE_STRIDE 8
+/* Selects the network; clears the weights and the optimiser state (set new
+ * weights before stepping with the learned start or training). */
+int psb_mlp_set_arch(psb_ctx* ctx, int32_t arch);
+/* The context's network, its input count and its parameter count (any
+ * pointer may be NULL). */
+int psb_mlp_info(const psb_ctx* ctx, int32_t* arch, int32_t* n_inputs, int32_t* n_params);
+/* The first half of a step, without stepping: rebuilds the grid and lists
+ * at the current state and returns, in particle-id order, the warm start's
+ * inputs (features: n rows of PSB_MLP_FEATURE_STRIDE floats, the first
+ * n_in set) and the initial pressure the next psb_step starts its
+ * corrector from (pressure: n floats; the network's prediction with
+ * PSB_WARM_LEARNED, the carried pressure with PSB_WARM_PREVIOUS, 0 with
+ * PSB_WARM_ZERO). Either pointer may be NULL. The state is unchanged, so a
+ * psb_step that follows starts from exactly these values. Single
+ * config-profile PCISPH contexts only. */
+int psb_warm_start(psb_ctx* ctx, float* features, float* pressure);
+/* The weights of the context's network (psb_mlp_info's n_params floats). */
 int psb_mlp_set_weights(psb_ctx* ctx, const float* w);
 int psb_mlp_get_weights(psb_ctx* ctx, float* w);
 /* Record (features, converged pressure / p_scale) of every stride-th particle
@@ -303,13 +327,16 @@ int psb_batch_layout(const psb_ctx* ctx, int32_t* n_scenes, int64_t* first);
  * that ended at max_iters unconverged (-1 for a single-scene context). */
 int psb_batch_stats(psb_ctx* ctx, int32_t* iters, int32_t* converged, double* err_final, int64_t* iters_total,
                     int64_t* unconverged_steps);
-/* CUDA-graph stepping (batches only): on, each step after the first since an
- * upload is one cudaGraphLaunch of the whole step, grid rebuild, warm start,
- * the corrector as a conditional while node (cudaGraphCondTypeWhile) and the
+/* CUDA-graph stepping (batches and config-profile PCISPH scenes; other
+ * scenes return PSB_EINVAL): on, each step after the first since an upload
+ * is one cudaGraphLaunch of the whole step, grid rebuild, warm start, the
+ * corrector as a conditional while node (cudaGraphCondTypeWhile) and the
  * commit. Graphs are captured on first use, one per state buffer parity,
- * and released by psb_set_graph(ctx, 0) and psb_destroy. Steps that record
- * training data or run with profiling on are launched kernel by kernel;
- * both ways launch the same kernels in the same order. */
+ * recaptured after emissions change the particle count, and released by
+ * psb_set_graph(ctx, 0) and psb_destroy. Steps that record training data,
+ * emit particles or run with profiling on are launched kernel by kernel,
+ * the corrector deciding on the device with one 4-byte read per pass; both
+ * ways launch the same kernels in the same order. */
 int psb_set_graph(psb_ctx* ctx, int32_t on);
 
 /* Autotuner: the launch configuration of the neighbour build and the five

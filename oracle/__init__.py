@@ -161,12 +161,18 @@ def ref_marching_cubes(g: IsoGrid, iso, level) -> np.ndarray:
     """The reference's polygonize kernel on the same nodes: triangle corners
     (3 per triangle) in cell order, shape (3T, 3)."""
     nodes4 = np.concatenate([grid_nodes(g), np.asarray(iso, np.float64)[:, None]], 1)
-    nodes4 = np.ascontiguousarray(nodes4)
+    return ref_polygonize(nodes4, g.dims, level)
+
+
+def ref_polygonize(nodes4, dims, level) -> np.ndarray:
+    """polygonize_MarchingCube_Kernel over nodes (x, y, z, value), x fastest:
+    triangle corners (3 per triangle) in cell order, shape (3T, 3)."""
+    nodes4 = np.ascontiguousarray(nodes4, np.float64)
     cap = 16 * nodes4.shape[0] + 64
     out = np.zeros((cap, 3))
     nv = ctypes.c_int64(0)
-    rc = ref_lib().ref_marching_cubes(_ptr(nodes4), int(g.dims[0]), int(g.dims[1]), int(g.dims[2]), float(level),
-                                      cap, _ptr(out), ctypes.byref(nv))
+    rc = ref_lib().ref_marching_cubes(_ptr(nodes4), int(dims[0]), int(dims[1]), int(dims[2]), float(level), cap,
+                                      _ptr(out), ctypes.byref(nv))
     if rc != 0:
         raise RuntimeError("ref_marching_cubes: capacity")
     return out[:nv.value]
@@ -189,6 +195,8 @@ def lib():
         L.orc_neighbors.restype = ctypes.c_int64
         L.orc_density.argtypes = [ctypes.POINTER(OrcParams), P, P, P, ctypes.c_int32, ctypes.c_int, P]
         L.orc_density.restype = None
+        L.orc_features.argtypes = [ctypes.POINTER(OrcParams), P, P, P, P]
+        L.orc_features.restype = None
         L.orc_step.argtypes = [ctypes.POINTER(OrcParams), ctypes.POINTER(OrcState), ctypes.POINTER(OrcStats), P, P, P]
         L.orc_step.restype = ctypes.c_int
         L.orc_presolve.argtypes = [ctypes.POINTER(OrcParams), ctypes.POINTER(OrcState), ctypes.c_int32,
@@ -243,6 +251,13 @@ def ref_lib():
         L.ref_collide.argtypes = [ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_float, ctypes.c_float, ctypes.c_int,
                                   ctypes.c_float, P, ctypes.c_int, P, P]
         L.ref_collide.restype = ctypes.c_int
+        F = ctypes.c_float
+        L.ref_densities_forces.argtypes = [P]
+        L.ref_vertex_normals.argtypes = [P, P, ctypes.c_int, F, P]
+        L.ref_force_trochoid.argtypes = [ctypes.c_int, P, P, P, F, F, F, F, F, F]
+        L.ref_force_constant.argtypes = [ctypes.c_int, P, P, P, F]
+        L.ref_mc_grid.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.c_double, F, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, P]
         _ref = L
     return _ref
 
@@ -355,6 +370,67 @@ def density(scene, pos, counts, lists, clamp) -> np.ndarray:
     lib().orc_density(ctypes.byref(P), _ptr(pos), _ptr(np.ascontiguousarray(counts, np.int32)), _ptr(lists),
                       lists.shape[1], 1 if clamp else 0, _ptr(rho))
     return rho
+
+
+def features(scene, pos, vel, p_prev, boundary=None) -> np.ndarray:
+    """Inputs of the learned warm start at the state (pos, vel, carried
+    pressure p_prev), (n, 7) in id order (orc_features; FP64)."""
+    pos = np.ascontiguousarray(pos, np.float64)
+    vel = np.ascontiguousarray(vel, np.float64)
+    p_prev = np.ascontiguousarray(p_prev, np.float64)
+    P = params(scene, n=pos.shape[0])
+    keep = []
+    if boundary is not None:
+        bpos = np.ascontiguousarray(boundary, np.float64)
+        psi = boundary_psi(scene, bpos)
+        keep += [bpos, psi]
+        P.n_bnd, P.bnd_pos, P.bnd_psi = bpos.shape[0], bpos.ctypes.data, psi.ctypes.data
+    out = np.empty((pos.shape[0], 7), np.float64)
+    lib().orc_features(ctypes.byref(P), _ptr(pos), _ptr(vel), _ptr(p_prev), _ptr(out))
+    return out
+
+
+def _bf16(a) -> np.ndarray:
+    """Round float32 values to bfloat16 (nearest, ties to even), kept as float32."""
+    a = np.ascontiguousarray(a, np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+def mlp_forward(w, X, n_in, activation) -> np.ndarray:
+    """The warm-start network y(X) on the CPU, FP64 arithmetic on the
+    library's BF16 rounding points: inputs, weights and both hidden layers'
+    activations rounded to BF16. w: the FP32 parameter vector (W1 [64 x
+    n_in], b1, W2 [64 x 64], b2, w3 [64], b3); activation "silu" or "relu".
+    Returns (y, h1, h2) with the hidden activations for error bounds."""
+    w = _bf16(np.asarray(w, np.float32)).astype(np.float64)
+    H = 64
+    o = 0
+    W1 = w[o:o + H * n_in].reshape(H, n_in); o += H * n_in
+    b1 = w[o:o + H]; o += H
+    W2 = w[o:o + H * H].reshape(H, H); o += H * H
+    b2 = w[o:o + H]; o += H
+    w3 = w[o:o + H]; o += H
+    b3 = w[o]
+    act = (lambda z: z / (1.0 + np.exp(-z))) if activation == "silu" else (lambda z: np.maximum(z, 0.0))
+    x = _bf16(np.asarray(X, np.float32)[:, :n_in]).astype(np.float64)
+    h1 = _bf16(act(x @ W1.T + b1)).astype(np.float64)
+    h2 = _bf16(act(h1 @ W2.T + b2)).astype(np.float64)
+    return h2 @ w3 + b3, h1, h2
+
+
+def learned_pressure(scene, pos, vel, p_prev, w, arch) -> np.ndarray:
+    """The learned warm start's initial pressure on the CPU: the FP64
+    features (orc_features) through the network (mlp_forward) with the
+    library's BF16 rounding points, max(0, y) p_scale. arch 0: 6 inputs,
+    SiLU; 1: 7 inputs, ReLU (the library's PSB_MLP_SILU6, PSB_MLP_RELU7)."""
+    F = features(scene, pos, vel, p_prev)
+    n_in, act = (6, "silu") if arch == 0 else (7, "relu")
+    y, _, _ = mlp_forward(w, F.astype(np.float32), n_in, act)
+    g = float(np.linalg.norm(np.asarray(scene.gravity, np.float64)))
+    p_scale = scene.rho0 * (g if g > 0 else 9.81) * 0.1
+    return np.maximum(0.0, y) * p_scale
 
 
 class OracleSim:
@@ -607,6 +683,32 @@ def emitter_positions(typ, v, particle_radius=0.0, count=0, faces=None, seed=0, 
     raise ValueError(typ)
 
 
+def ref_force_constant(accum, mass, direction, amplitude):
+    """evaluate_ForceExt_Constante (ForceExt.cu:24-34) on a copy of accum."""
+    acc = np.ascontiguousarray(accum, np.float64).copy()
+    d = np.asarray(direction, np.float32)
+    ref_lib().ref_force_constant(len(mass), _ptr(acc), _ptr(np.ascontiguousarray(mass, np.float64)), _ptr(d),
+                                 np.float32(amplitude))
+    return acc
+
+
+def ref_force_trochoid(pos, accum, mass, A, k, theta, w, phi, t):
+    """evaluate_ForceExt_Trochoide (ForceExt.cu:37-52) on a copy of accum."""
+    acc = np.ascontiguousarray(accum, np.float64).copy()
+    ref_lib().ref_force_trochoid(len(mass), _ptr(np.ascontiguousarray(pos, np.float64)), _ptr(acc),
+                                 _ptr(np.ascontiguousarray(mass, np.float64)), A, k, theta, w, phi, t)
+    return acc
+
+
+def ref_mc_grid(centre, l, w, d, cell, dims):
+    """createGrid_MarchingCube_CUDA's node centres, (nodes, 4) with value 0."""
+    nx, ny, nz = (int(v) for v in dims)
+    out = np.zeros((nx * ny * nz, 4), np.float64)
+    c = np.asarray(centre, np.float64)
+    ref_lib().ref_mc_grid(_ptr(c), l, w, d, np.float32(cell), nx, ny, nz, _ptr(out))
+    return out
+
+
 class RefSim:
     """The reference's kernels on the CPU, AoS double state (oracle/_ref)."""
 
@@ -700,6 +802,25 @@ class RefSim:
                                       s.particle_radius, _ptr(bmin), _ptr(bmax))
         if rc != 0:
             raise RuntimeError(f"ref_dem_update: {rc}")
+
+    def densities_forces(self):
+        """evaluate_densities_forces (SphSystem.cu:27-43) at the current
+        positions: density, pressure, f_press, f_visc, f_surf, normals, f_accum."""
+        rc = ref_lib().ref_densities_forces(self.h)
+        if rc != 0:
+            raise RuntimeError(f"ref_densities_forces: {rc}")
+        return {k: self.get(k, w) for k, w in (("density", 1), ("pressure", 1), ("f_press", 3), ("f_visc", 3),
+                                                ("f_surf", 3), ("normals", 3), ("f_accum", 3))}
+
+    def vertex_normals(self, verts, scale=1.0):
+        """computeNormales_Vertex_CUDA at the vertices (n, 3), with the
+        current densities."""
+        verts = np.ascontiguousarray(verts, np.float64)
+        out = np.zeros_like(verts)
+        rc = ref_lib().ref_vertex_normals(self.h, _ptr(verts), verts.shape[0], np.float32(scale), _ptr(out))
+        if rc != 0:
+            raise RuntimeError(f"ref_vertex_normals: {rc}")
+        return out
 
     def wcsph_update(self, collide=True):
         s = self.scene

@@ -1041,6 +1041,81 @@ static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double*
     return 0;
 }
 
+/* Inputs of the learned pressure warm start (config-profile PCISPH) at the
+ * step's start positions, seven per particle. The reference has no
+ * counterpart: every reference step starts from p = 0
+ * (PciSphSystem_Kernel.cu:131). Sums run over the neighbour list (self
+ * included, pairs with r >= h dropped); rho is the density at x with the
+ * wall ghosts and boundary particles, as the step computes it.
+ *   f0 neighbour count / 32
+ *   f1 advected density deviation (rho - dt rho div v - rho0) / rho0 * 100
+ *   f2 div v * dt * 100, div v = (1/rho0) sum_j m (v_j - v_i) . gradW_ij
+ *   f3 previous pressure / p_scale
+ *   f4 distance to the nearest box face / h, in [0, 1]
+ *   f5 |sum_j m gradW_ij| * h / rho0
+ *   f6 sum_j W_ij p_j / sum_j W_ij / p_scale (poly6 weights, 0 if none)
+ * with gradW the spiky gradient -45/(pi h^6) (h - r)^2 x_ij/r and p_scale
+ * = rho0 |g| 0.1 m (|g| = 9.81 when gravity is zero). */
+void orc_features(const orc_params* P, const double* pos, const double* vel, const double* p_prev, double* out) {
+    const int32_t n = P->n;
+    int32_t* counts = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+    int32_t cap = 0;
+    int32_t* list = build_lists(P, pos, counts, &cap, NULL);
+    orc_params Qb;
+    int32_t *bnd_counts = NULL, *bnd_lists = NULL;
+    if (P->n_bnd > 0) {
+        Qb = *P;
+        build_bnd_lists(P, pos, &bnd_counts, &bnd_lists, &Qb.bnd_cap);
+        Qb.bnd_counts = bnd_counts;
+        Qb.bnd_lists = bnd_lists;
+        P = &Qb;
+    }
+    double* rho = (double*)malloc(sizeof(double) * (size_t)n);
+    orc_density(P, pos, counts, list, cap, 1, rho);
+    const double h = P->h, m = P->mass, rho0 = P->rho0, dt = (double)P->dt;
+    const double G = 45.0 / (PI_D * pow(h, 6));
+    const double g = sqrt((double)P->gravity[0] * P->gravity[0] + (double)P->gravity[1] * P->gravity[1] +
+                          (double)P->gravity[2] * P->gravity[2]);
+    const double p_scale = rho0 * (g > 0 ? g : 9.81) * 0.1;
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+        const double* xi = &pos[3 * i];
+        double div = 0.0, gr[3] = {0, 0, 0}, wp = 0.0, ws = 0.0;
+        for (int32_t t = 0; t < counts[i]; ++t) {
+            const int32_t j = list[(size_t)i * cap + t];
+            const double d[3] = {xi[0] - pos[3 * j], xi[1] - pos[3 * j + 1], xi[2] - pos[3 * j + 2]};
+            const double r = len3(d);
+            if (r >= h) continue;
+            const double w = (h * h - r * r) / (h * h);
+            wp += w * w * w * p_prev[j];
+            ws += w * w * w;
+            if (r > 0) {
+                const double gw = -G * (h - r) * (h - r) / r;     /* gradW_ij = gw * d */
+                for (int e = 0; e < 3; ++e) {
+                    div += m * (vel[3 * j + e] - vel[3 * i + e]) * gw * d[e];
+                    gr[e] += m * gw * d[e];
+                }
+            }
+        }
+        div /= rho0;
+        double dwall = h;
+        for (int e = 0; e < 3; ++e) {
+            const double lo = xi[e] - (double)P->box_min[e], hi = (double)P->box_max[e] - xi[e];
+            dwall = lo < dwall ? lo : dwall;
+            dwall = hi < dwall ? hi : dwall;
+        }
+        double* f = &out[7 * (size_t)i];
+        f[0] = counts[i] / 32.0;
+        f[1] = (rho[i] - dt * rho[i] * div - rho0) / rho0 * 100.0;
+        f[2] = div * dt * 100.0;
+        f[3] = p_prev[i] / p_scale;
+        f[4] = (dwall > 0 ? dwall : 0.0) / h;
+        f[5] = len3(gr) * h / rho0;
+        f[6] = ws > 0 ? wp / ws / p_scale : 0.0;
+    }
+    free(counts); free(list); free(rho); free(bnd_counts); free(bnd_lists);
+}
+
 int orc_presolve(const orc_params* P, orc_state* S, int32_t iters, orc_stats* st) {
     /* The state is saved and restored around one warm-started step with
      * exactly `iters` corrections; only the pressure is kept. */

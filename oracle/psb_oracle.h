@@ -151,6 +151,10 @@ void orc_density(const orc_params* P, const double* pos, const int32_t* counts, 
  * force density, the neighbour counts. */
 int orc_step(const orc_params* P, orc_state* S, orc_stats* st, double* rho_x, double* f_np, int32_t* nbr_counts);
 
+/* Inputs of the learned warm start at pos (config PCISPH), 7 per particle
+ * in id order: see psb_oracle.c for the definitions. */
+void orc_features(const orc_params* P, const double* pos, const double* vel, const double* p_prev, double* out);
+
 /* Initial-pressure solve (PCISPH): `iters` corrector passes at eta = 0 with
  * positions and velocities restored afterwards; only S->p changes. */
 int orc_presolve(const orc_params* P, orc_state* S, int32_t iters, orc_stats* st);

@@ -53,6 +53,8 @@ thread_local dim3 gridDim;
 void collisionBox(int nbBodies, double3* newPos, double3* oldVel, double3* newVel, float3 Min, float3 Max,
                   float elast, bool container, float radiusParticles, float dt);
 void evaluate_force_constante(uint nbBodies, double3* accumForceBuff, double* mass, float3 direction, float amplitude);
+void evaluate_force_trochoide(uint nbBodies, double3* position, double3* accumForceBuff, double* mass, float A, float k,
+                              float theta, float w, float phi, float t);
 void integrateEuler(uint nbBodies, double3* newPos, double3* newVel, double3* forces, double* mass, float dt);
 /* The collision objects' kernels (src/Kernel/Collision/*), C++ linkage
  * where their headers have no extern "C". */
@@ -83,6 +85,8 @@ extern "C" void collisionSystem_Periodic_HeightFieldCollision_Kernel(double3* ne
 extern "C" void polygonize_MarchingCube_Kernel(double4* grid, uint nbCellsX, uint nbCellsY, uint nbCellsZ,
                                                double isoLevel, int* nbIndex, double3* vertexs, double3* normales,
                                                int* indexs);
+extern "C" void createGrid_MarchingCube_Kernel(double4* grid, double3 center, double l, double w, double d,
+                                               float sizeCell, uint nbPosX, uint nbPosY, uint nbPosZ, int* m_nbIndex);
 
 namespace {
 
@@ -418,6 +422,66 @@ int ref_dem_update(ref_sim* s, float dt, const float* gravity_dir, float gravity
                          0.f, true, particle_radius, dt);
         });
     }
+    return 0;
+}
+
+/* evaluate_densities_forces (SphSystem.cu:27-43): densityEvaluation then
+ * internalForces over the lists of the current positions (grid rebuilt). */
+int ref_densities_forces(ref_sim* s) {
+    int rc = ref_search(s);
+    if (rc) return rc;
+    const uint n = s->n;
+    partVoisine v{s->nb_count.data(), s->nb_list.data()};
+    double3* pos = (double3*)s->pos.data();
+    launch1d(n, true, [&] {
+        densityEvaluation(pos, s->mass.data(), s->radius.data(), s->k.data(), s->rho0.data(), n, s->density.data(),
+                          s->pressure.data(), v);
+    });
+    launch1d(n, true, [&] {
+        internalForces(pos, (double3*)s->vel.data(), s->mass.data(), s->density.data(), s->pressure.data(),
+                       s->radius.data(), s->mu.data(), s->threshold.data(), s->sigma.data(), (double3*)s->normals.data(), n,
+                       (double3*)s->f_press.data(), (double3*)s->f_visc.data(), (double3*)s->f_surf.data(),
+                       (double3*)s->f_accum.data(), v);
+    });
+    return 0;
+}
+
+/* computeNormales_Vertex_CUDA -> computeNormales_Vertexs_Kernel
+ * (UniformGridKernel.cu:141-190) at nV vertices (xyz), grid rebuilt at the
+ * current positions, with the particles' current densities. */
+int ref_vertex_normals(ref_sim* s, const double* posV, int nV, float scale, double* normals) {
+    int rc = ref_search(s);
+    if (rc) return rc;
+    UniformGrid* g = &s->grid;
+    launch1d((unsigned)nV, true, [&] {
+        computeNormales_Vertexs_Kernel((double3*)posV, (double3*)normals, scale, nV, g->Min, g->sizeCell, g->nbCellsX,
+                                       g->nbCellsY, g->nbCellsZ, g->nbParticles, g->indexParticles,
+                                       (double3*)s->pos.data(), s->radius.data(), s->mass.data(), s->density.data(), s->n);
+    });
+    return 0;
+}
+
+/* evaluate_ForceExt_Trochoide (ForceExt.cu:37-52) on n particles. */
+int ref_force_trochoid(int n, double* pos, double* accum, double* mass, float A, float k, float theta, float w, float phi,
+                       float t) {
+    launch1d((unsigned)n, true, [&] { evaluate_force_trochoide(n, (double3*)pos, (double3*)accum, mass, A, k, theta, w, phi, t); });
+    return 0;
+}
+
+/* evaluate_ForceExt_Constante (ForceExt.cu:24-34) on n particles. */
+int ref_force_constant(int n, double* accum, double* mass, const float* dir, float amp) {
+    const float3 d = make_float3(dir[0], dir[1], dir[2]);
+    launch1d((unsigned)n, true, [&] { evaluate_force_constante(n, (double3*)accum, mass, d, amp); });
+    return 0;
+}
+
+/* createGrid_MarchingCube_CUDA (MarchingCube.cu:12-28): node centres as double4. */
+int ref_mc_grid(const double* centre, double l, double w, double d, float cell, int nx, int ny, int nz, double* nodes4) {
+    std::vector<int> nb((size_t)nx * ny * nz, 0);
+    launch_cells(nx, ny, nz, [&] {
+        createGrid_MarchingCube_Kernel((double4*)nodes4, make_double3(centre[0], centre[1], centre[2]), l, w, d, cell,
+                                       nx, ny, nz, nb.data());
+    });
     return 0;
 }
 

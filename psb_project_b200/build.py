@@ -21,7 +21,11 @@ OUT_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(OUT_DIR, "libpsb.so")
 OBJ_DIR = os.path.join(ROOT, "_build")
 
-CU_SOURCES = ["grid.cu", "sph.cu", "api.cu", "noalloc.cu", "mlp.cu", "dem.cu", "mc.cu", "compat.cu", "batch.cu", "diag.cu", "boundary.cu", "colliders.cu", "emit.cu"]
+CU_SOURCES = ["grid.cu", "sph.cu", "api.cu", "noalloc.cu", "mlp.cu", "dem.cu", "mc.cu", "compat.cu", "compat_sph.cu",
+              "batch.cu", "diag.cu", "boundary.cu", "colliders.cu", "emit.cu"]
+# Per-file additions: the reference-signature FP64 kernels keep separate
+# multiplies and adds, as the reference's own kernels compiled for the host do.
+CU_EXTRA_FLAGS = {"compat_sph.cu": ["-fmad=false"]}
 CPP_SOURCES = ["scene.cpp", "io.cpp", "emitters.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -56,14 +60,14 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(OBJ_DIR, exist_ok=True)
     inc = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    headers.append(os.path.join(ROOT, "include", "psb.h"))
+    headers += [os.path.join(ROOT, "include", "psb.h"), os.path.join(ROOT, "include", "psb_compat.h")]
     objs = []
     nvcc = _nvcc()
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ_DIR, src + ".o")
         if force or _stale(o, [s] + headers):
-            cmd = [nvcc] + NVCC_FLAGS + inc + ["-Xptxas", "-v", "-c", s, "-o", o]
+            cmd = [nvcc] + NVCC_FLAGS + CU_EXTRA_FLAGS.get(src, []) + inc + ["-Xptxas", "-v", "-c", s, "-o", o]
             r = _run(cmd)
             if verbose:
                 sys.stderr.write(r.stderr)

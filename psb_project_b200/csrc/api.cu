@@ -130,6 +130,7 @@ struct psb_ctx {
     void* mlp_wbf = nullptr;  // BF16 copy used by the kernels
     int mlp_step = 0;
     bool mlp_set = false;
+    int mlp_arch = PSB_MLP_SILU6;   // the network (psb_mlp_set_arch)
     float p_scale = 1.f;
     float* ds_X = nullptr;    // recorded rows x 8
     float* ds_T = nullptr;
@@ -195,6 +196,8 @@ struct psb_ctx {
     bool graph_on = false;
     cudaGraphExec_t gexec[2] = {};                // one per state buffer parity (cs)
     int graph_sorted = -1;                        // the sort's result buffer, fixed by the key width
+    int graph_n = -1;                             // the particle count the graphs were captured for
+    int64_t iters_total_base = 0;                 // single scene: corrections before the loop words' sums
     cudaStream_t cap_main = nullptr;              // captures the step (the legacy stream cannot be captured)
     cudaStream_t cap_stream = nullptr;            // captures the while node's body
     // host mirrors
@@ -447,6 +450,14 @@ __global__ void k_scatter_rp(int n, const int* __restrict__ ids, const float2* _
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) dst[ids[t]] = comp ? rp[t].y : rp[t].x;
 }
+__global__ void k_scatter_rows8(int n, const int* __restrict__ ids, const float* __restrict__ src, float* __restrict__ dst) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float4* s = reinterpret_cast<const float4*>(src) + 2 * (size_t)t;
+    float4* d = reinterpret_cast<float4*>(dst) + 2 * (size_t)ids[t];
+    d[0] = s[0];
+    d[1] = s[1];
+}
 __global__ void k_scatter_u32(int n, const int* __restrict__ ids, const uint32_t* __restrict__ src, uint32_t* __restrict__ dst) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) dst[ids[t]] = src[t];
@@ -502,7 +513,7 @@ int build(psb_ctx* c, bool keep_p = false, bool features = false) {
         float* feats = features ? c->feats : nullptr;
         timed(c, "density_x", [&] {
             psb::launch_density_x(st, P, c->pos[c->cs], c->vel[c->cs], c->nbr_count, c->nbr_list, c->rp[c->cr], c->rho_x,
-                                  zero_p, c->p_scale, feats);
+                                  zero_p, c->p_scale, feats, psb::mlp_inputs(c->mlp_arch));
         });
     }
     c->built = true;
@@ -522,11 +533,13 @@ int read_flags(psb_ctx* c) {
     return PSB_OK;
 }
 
-// ---- batched scenes -------------------------------------------------------
+void release_graphs(psb_ctx* c);
 
-// The corrector of a batch: k_batch_begin, then {density pass, decision,
-// pressure-force pass} until every scene has converged or max_iters passes
-// have run. The predictions stay in xs[0]: the config profile's pressure-
+// ---- the corrector loop on the device: batches and config-profile PCISPH ---
+
+// The corrector of a batch (or of one config-profile PCISPH scene, a batch
+// of one): k_batch_begin, then {density pass, decision, pressure-force pass}
+// until every scene has converged or max_iters passes have run. The predictions stay in xs[0]: the config profile's pressure-
 // force pass reads the start positions, never x*, so it updates x* in place.
 // capture: enqueue the loop as a while node of the graph being captured on
 // the context's stream; else drive it from the host, one 4-byte read per pass.
@@ -539,7 +552,8 @@ int batch_corrector(psb_ctx* c, const Params& P, int s, int r, bool capture) {
     if (max_it == 0) return PSB_OK;
     auto body = [&](cudaStream_t bs, cudaGraphConditionalHandle h, int set_handle) {
         timed(c, "pci_density", [&] {
-            psb::launch_pci_density(bs, P, c->xs[0], c->rp[r], c->nbr_count, c->nbr_list, c->rpc, nullptr);
+            psb::launch_pci_density(bs, P, c->xs[0], c->rp[r], c->nbr_count, c->nbr_list, c->rpc,
+                                    c->batch ? nullptr : c->d_err_scene);
         });
         timed(c, "batch_decide", [&] {
             psb::launch_batch_decide(bs, S, c->sc.min_iters, max_it, c->sc.eta, c->d_active, c->d_err_scene,
@@ -584,17 +598,23 @@ int batch_corrector(psb_ctx* c, const Params& P, int s, int r, bool capture) {
     return cuda_check(c, cudaStreamEndCapture(c->cap_stream, &ended), "body capture");
 }
 
-// One batch step, enqueued on the context's stream (or captured from it).
-int enqueue_batch_step(psb_ctx* c, bool capture) {
+// One step of a batch, or of a single config-profile PCISPH scene, enqueued
+// on the context's stream (or captured from it). A single scene's pressure-
+// force pass reads the decision's active word and does nothing once the
+// scene has converged, as a batch's retired scenes do.
+int enqueue_loop_step(psb_ctx* c, bool capture) {
     const bool collect = c->collect_stride > 0;
     const int mode = c->sc.warm_start;
     PSB_TRY(build(c, mode != PSB_WARM_ZERO || collect, mode == PSB_WARM_LEARNED || collect));
     cudaStream_t st = c->stream;
     Params P = c->P;
     P.n = c->n;
+    if (!c->batch) P.active = c->d_active;
     const int s = c->cs, r = c->cr;
     if (mode == PSB_WARM_LEARNED) {
-        timed(c, "mlp_infer", [&] { psb::launch_mlp_infer(st, c->n, c->feats, c->mlp_wbf, c->p_scale, c->rp[r]); });
+        timed(c, "mlp_infer", [&] {
+            psb::launch_mlp_infer(st, c->mlp_arch, c->n, c->feats, c->mlp_wbf, c->p_scale, c->rp[r]);
+        });
     } else if (mode == PSB_WARM_ZERO && collect) {
         psb::launch_zero_pressure(st, c->n, c->rp[r]);
     }
@@ -618,14 +638,14 @@ int enqueue_batch_step(psb_ctx* c, bool capture) {
 // Captures the step from the current state parity into c->gexec[c->cs], on
 // the context's own capture stream (nothing runs; the graph is launched on
 // the caller's stream, which may be the legacy one).
-int capture_batch_step(psb_ctx* c) {
+int capture_loop_step(psb_ctx* c) {
     const int p = c->cs;
     cudaStream_t user = c->stream;
     cudaStream_t st = c->cap_main;
     PSB_TRY(cuda_check(c, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture"));
     const int saved_cs = c->cs, saved_cr = c->cr, saved_sorted = c->sorted, saved_stale = c->stale;
     c->stream = st;
-    const int rc = enqueue_batch_step(c, true);
+    const int rc = enqueue_loop_step(c, true);
     c->stream = user;
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(st, &g);
@@ -640,10 +660,11 @@ int capture_batch_step(psb_ctx* c) {
     const cudaError_t ei = cudaGraphInstantiate(&c->gexec[p], g, 0);
     cudaGraphDestroy(g);
     if (ei != cudaSuccess) { c->gexec[p] = nullptr; return cuda_check(c, ei, "graph instantiate"); }
+    c->graph_n = c->n;
     return PSB_OK;
 }
 
-int step_batch(psb_ctx* c, bool last) {
+int step_loop(psb_ctx* c, bool last) {
     cudaStream_t st = c->stream;
     const int S = c->nscenes;
     const bool collect = c->collect_stride > 0;
@@ -652,7 +673,8 @@ int step_batch(psb_ctx* c, bool last) {
     const int prev_n = c->sorted >= 0 ? c->sorted_n : (c->stale >= 0 ? c->stale_n : -1);
     const bool graph = c->graph_on && !collect && !c->prof.on && prev_n == c->n;
     if (graph) {
-        if (!c->gexec[c->cs]) PSB_TRY(capture_batch_step(c));
+        if (c->graph_n != c->n) release_graphs(c);       // emissions changed the particle count
+        if (!c->gexec[c->cs]) PSB_TRY(capture_loop_step(c));
         PSB_TRY(cuda_check(c, cudaGraphLaunch(c->gexec[c->cs], st), "graph launch"));
         // what build() records of the step it enqueues
         c->sorted = c->graph_sorted;
@@ -662,7 +684,7 @@ int step_batch(psb_ctx* c, bool last) {
         c->cr ^= 1;
         c->built = true;
     } else {
-        PSB_TRY(enqueue_batch_step(c, false));
+        PSB_TRY(enqueue_loop_step(c, false));
     }
     c->stats.steps += 1;
     if (!last && !collect) return PSB_OK;
@@ -679,6 +701,7 @@ int step_batch(psb_ctx* c, bool last) {
     }
     c->stats.iters = iters;
     c->stats.converged = all_conv;
+    if (!c->batch) c->stats.iters_total = c->iters_total_base + c->h_loop[2 + 2 * S];
     if (collect && all_conv) {
         const int stride = c->collect_stride;
         const int offset = (int)(c->collect_steps % stride);
@@ -735,8 +758,9 @@ int run_emitters(psb_ctx* c) {
 }
 
 int step_once(psb_ctx* c, bool last) {
-    if (c->batch) return step_batch(c, last);
+    if (c->batch) return step_loop(c, last);
     if (!c->emitters.empty()) PSB_TRY(run_emitters(c));
+    if (c->P.pci && !c->P.ref) return step_loop(c, last);     // config PCISPH: the corrector decides on the device
     const bool need_prev_p = !c->P.ref && c->P.pci && (c->sc.warm_start != PSB_WARM_ZERO || c->collect_stride > 0);
     const bool features = !c->P.ref && c->P.pci && (c->sc.warm_start == PSB_WARM_LEARNED || c->collect_stride > 0);
     PSB_TRY(build(c, need_prev_p, features));
@@ -774,67 +798,33 @@ int step_once(psb_ctx* c, bool last) {
         c->stats.iters = 0;
         c->stats.converged = 1;
     } else {
-        const int mode = P.ref ? PSB_WARM_ZERO : c->sc.warm_start;
-        const bool collect = !P.ref && c->collect_stride > 0;
-        if (mode == PSB_WARM_LEARNED) {
-            timed(c, "mlp_infer", [&] { psb::launch_mlp_infer(st, c->n, c->feats, c->mlp_wbf, c->p_scale, c->rp[r]); });
-        } else if (mode == PSB_WARM_ZERO && collect) {
-            psb::launch_zero_pressure(st, c->n, c->rp[r]);   // features kept the previous pressure
-        }
-        const int warm = mode == PSB_WARM_ZERO ? 0 : 1;
+        // reference-profile PCISPH: exactly three corrections from p = 0
+        // (PciSphSystem.cu:30-61), no host round trip
         timed(c, "pci_init", [&] {
-            psb::launch_pci_init(st, P, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list, warm,
+            psb::launch_pci_init(st, P, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list, 0,
                                  c->fnp, c->xs[0], c->vs);
         });
-        const int min_it = P.ref ? 3 : c->sc.min_iters;
-        const int max_it = P.ref ? 3 : c->sc.max_iters;
-        int xi = 0, k = 0, passes = 0;
-        converged = P.ref ? 1 : 0;
-        for (;;) {
-            if (k >= max_it) break;
+        constexpr int kRefIters = 3;
+        int xi = 0;
+        for (int k = 0; k < kRefIters; ++k) {
             timed(c, "pci_density", [&] {
                 psb::launch_pci_density(st, P, c->xs[xi], c->rp[r], c->nbr_count, c->nbr_list, c->rpc, &c->err_hist[k]);
             });
-            ++passes;
-            if (!P.ref) {
-                PSB_TRY(cuda_check(c, cudaMemcpyAsync(&c->h_err[k], &c->err_hist[k], 8, cudaMemcpyDeviceToHost, st), "err"));
-                PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "sync"));
-                if (k >= min_it && psb::unorder_double(c->h_err[k]) <= c->sc.eta) { converged = 1; break; }
-            }
             timed(c, "pci_force_predict", [&] {
                 psb::launch_pci_force_predict(st, P, c->pos[s], c->vap[s], c->fnp, c->xs[xi], c->rpc, c->nbr_count,
                                               c->nbr_list, c->xs[xi ^ 1], c->vs, c->rp[r]);
             });
             xi ^= 1;
-            ++k;
-        }
-        const float4* v_commit = c->vs;
-        if (P.xsph_k != 0.f) {     // the other prediction buffer is free now
-            timed(c, "xsph", [&] {
-                psb::launch_xsph(st, P, c->xs[xi], c->vs, c->nbr_count, c->nbr_list, c->xs[xi ^ 1]);
-            });
-            v_commit = c->xs[xi ^ 1];
         }
         timed(c, "pci_commit", [&] {
-            psb::launch_pci_commit(st, P, c->xs[xi], v_commit, c->rpc, passes > 0, c->pos[s], c->vel[s], c->vap[s],
-                                   c->rp[r]);
+            psb::launch_pci_commit(st, P, c->xs[xi], c->vs, c->rpc, 1, c->pos[s], c->vel[s], c->vap[s], c->rp[r]);
         });
-        if (collect && converged) {
-            const int stride = c->collect_stride;
-            const int offset = (int)(c->collect_steps % stride);
-            const int rows = offset < c->n ? (c->n - offset + stride - 1) / stride : 0;
-            psb::launch_collect(st, c->n, stride, offset, c->ds_rows, c->ds_cap, c->feats, c->rp[r], c->p_scale, c->ds_X,
-                                c->ds_T);
-            c->ds_rows += (uint64_t)rows;
-            c->collect_steps += 1;
-        }
-        iters = k;
+        iters = kRefIters;
         c->stats.iters = iters;
         c->stats.converged = converged;
-        if (last || !P.ref) {
+        if (last)
             PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->h_err, c->err_hist, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1),
                                                   cudaMemcpyDeviceToHost, st), "err"));
-        }
     }
     c->stats.steps += 1;
     c->stats.iters_total += iters;
@@ -843,9 +833,6 @@ int step_once(psb_ctx* c, bool last) {
         PSB_TRY(read_flags(c));
         for (int i = 0; i <= PSB_MAX_ITERS; ++i)
             c->stats.err[i] = (P.pci && c->h_err[i]) ? psb::unorder_double(c->h_err[i]) : 0.0;
-        if (P.pci && !converged) return fail(c, PSB_ENOCONV, "corrector loop reached max_iters above eta");
-    } else if (P.pci && !P.ref && !converged) {
-        // keep going; the status is reported by the last step of the call
     }
     return PSB_OK;
 }
@@ -965,6 +952,30 @@ const char* batch_mismatch(const psb_scene& a, const psb_scene& b) {
     return nullptr;
 }
 
+// The device-side corrector's words for S scenes (batch.cu), their pinned
+// mirrors, and the streams a CUDA-graph capture runs on.
+int alloc_loop(psb_ctx* c, int S) {
+    int rc = PSB_OK;
+    if (!rc) rc = dalloc(c, &c->d_active, S);
+    if (!rc) rc = dalloc(c, &c->d_err_scene, S);
+    if (!rc) rc = dalloc(c, &c->d_err_sh, (size_t)(PSB_MAX_ITERS + 1) * S);
+    if (!rc) rc = dalloc(c, &c->d_loop, 2 + 4 * (size_t)S);
+    if (!rc && cudaMallocHost((void**)&c->h_loop, sizeof(int) * (2 + 4 * (size_t)S)) != cudaSuccess) rc = PSB_ENOMEM;
+    if (!rc && cudaMallocHost((void**)&c->h_err_sh, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S) != cudaSuccess)
+        rc = PSB_ENOMEM;
+    if (!rc) rc = cuda_check(c, cudaMemset(c->d_loop, 0, sizeof(int) * (2 + 4 * (size_t)S)), "loop");
+    if (!rc) rc = cuda_check(c, cudaMemset(c->d_active, 1, S), "active");
+    if (!rc) rc = cuda_check(c, cudaMemset(c->d_err_scene, 0, sizeof(unsigned long long) * S), "err");
+    if (!rc) rc = cuda_check(c, cudaMemset(c->d_err_sh, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S), "err");
+    if (!rc) rc = cuda_check(c, cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking), "stream");
+    if (!rc) rc = cuda_check(c, cudaStreamCreateWithFlags(&c->cap_main, cudaStreamNonBlocking), "stream");
+    if (!rc) {
+        std::memset(c->h_loop, 0, sizeof(int) * (2 + 4 * (size_t)S));
+        std::memset(c->h_err_sh, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S);
+    }
+    return rc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -977,7 +988,16 @@ int psb_create(const psb_scene* scene, psb_ctx** out) {
         std::fprintf(stderr, "psb_create: %s\n", why.c_str());
         return PSB_EINVAL;
     }
-    return create_impl(scene, (size_t)scene->dims[0] * scene->dims[1] * scene->dims[2], out);
+    PSB_TRY(create_impl(scene, (size_t)scene->dims[0] * scene->dims[1] * scene->dims[2], out));
+    psb_ctx* c = *out;
+    if (const int rc = alloc_loop(c, 1)) {
+        std::fprintf(stderr, "psb_create: %s\n", c->err.c_str());
+        free_all(c);
+        delete c;
+        *out = nullptr;
+        return rc;
+    }
+    return PSB_OK;
 }
 
 int psb_create_batch(const psb_scene* scenes, int32_t n_scenes, psb_ctx** out) {
@@ -1036,29 +1056,15 @@ int psb_create_batch(const psb_scene* scenes, int32_t n_scenes, psb_ctx** out) {
     int rc = PSB_OK;
     if (!rc) rc = dalloc(c, &c->d_scenes, S);
     if (!rc) rc = dalloc(c, &c->d_slot_scene, (size_t)total);
-    if (!rc) rc = dalloc(c, &c->d_active, S);
-    if (!rc) rc = dalloc(c, &c->d_err_scene, S);
-    if (!rc) rc = dalloc(c, &c->d_err_sh, (size_t)(PSB_MAX_ITERS + 1) * S);
-    if (!rc) rc = dalloc(c, &c->d_loop, 2 + 4 * (size_t)S);
-    if (!rc && cudaMallocHost((void**)&c->h_loop, sizeof(int) * (2 + 4 * (size_t)S)) != cudaSuccess) rc = PSB_ENOMEM;
-    if (!rc && cudaMallocHost((void**)&c->h_err_sh, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S) != cudaSuccess)
-        rc = PSB_ENOMEM;
     if (!rc) rc = cuda_check(c, cudaMemcpy(c->d_scenes, c->geom.data(), sizeof(psb::SceneGeom) * S, cudaMemcpyHostToDevice), "geom");
     if (!rc) rc = cuda_check(c, cudaMemcpy(c->d_slot_scene, slot_scene.data(), 2 * (size_t)total, cudaMemcpyHostToDevice), "slots");
-    if (!rc) rc = cuda_check(c, cudaMemset(c->d_loop, 0, sizeof(int) * (2 + 4 * (size_t)S)), "loop");
-    if (!rc) rc = cuda_check(c, cudaMemset(c->d_active, 1, S), "active");
-    if (!rc) rc = cuda_check(c, cudaMemset(c->d_err_scene, 0, sizeof(unsigned long long) * S), "err");
-    if (!rc) rc = cuda_check(c, cudaMemset(c->d_err_sh, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S), "err");
-    if (!rc) rc = cuda_check(c, cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking), "stream");
-    if (!rc) rc = cuda_check(c, cudaStreamCreateWithFlags(&c->cap_main, cudaStreamNonBlocking), "stream");
+    if (!rc) rc = alloc_loop(c, S);
     if (rc) {
         std::fprintf(stderr, "psb_create_batch: %s\n", c->err.c_str());
         free_all(c);
         delete c;
         return rc;
     }
-    std::memset(c->h_loop, 0, sizeof(int) * (2 + 4 * (size_t)S));
-    std::memset(c->h_err_sh, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S);
     c->P.scenes = c->d_scenes;
     c->P.slot_scene = c->d_slot_scene;
     c->P.active = c->d_active;
@@ -1102,11 +1108,17 @@ static void apply_tune(psb_ctx* c) {
     c->P.tune = t;
 }
 
-static void release_graphs(psb_ctx* c) {
+}  // extern "C"
+
+namespace {
+void release_graphs(psb_ctx* c) {
     cudaStreamSynchronize(c->stream);
     for (auto& g : c->gexec)
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
+}  // namespace
+
+extern "C" {
 
 static int upload_common(psb_ctx* c, int32_t n) {
     // forget the previous particle set; the next build clears its cells
@@ -1120,7 +1132,8 @@ static int upload_common(psb_ctx* c, int32_t n) {
     c->uploaded = true;
     c->built = false;
     apply_tune(c);
-    if (c->batch) cudaMemsetAsync(c->d_loop, 0, sizeof(int) * (2 + 4 * (size_t)c->nscenes), c->stream);
+    if (!c->batch) c->iters_total_base = c->stats.iters_total;    // the loop words' sums restart at 0
+    cudaMemsetAsync(c->d_loop, 0, sizeof(int) * (2 + 4 * (size_t)c->nscenes), c->stream);
     return PSB_OK;
 }
 
@@ -1226,13 +1239,36 @@ int psb_step(psb_ctx* c, int32_t nsteps) {
     return status;
 }
 
+int psb_mlp_set_arch(psb_ctx* c, int32_t arch) {
+    if (!c) return PSB_EINVAL;
+    if (arch != PSB_MLP_SILU6 && arch != PSB_MLP_RELU7) return fail(c, PSB_EINVAL, "psb_mlp_set_arch: unknown network");
+    cudaSetDevice(c->device);
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "arch"));
+    c->mlp_arch = arch;
+    c->mlp_set = false;          // the weights of the other network mean nothing here
+    c->mlp_step = 0;
+    PSB_TRY(cuda_check(c, cudaMemset(c->mlp_w, 0, sizeof(float) * psb::kMlpParams), "arch"));
+    PSB_TRY(cuda_check(c, cudaMemset(c->mlp_wbf, 0, 2 * psb::kMlpParams), "arch"));
+    release_graphs(c);
+    return PSB_OK;
+}
+
+int psb_mlp_info(const psb_ctx* c, int32_t* arch, int32_t* n_inputs, int32_t* n_params) {
+    if (!c) return PSB_EINVAL;
+    if (arch) *arch = c->mlp_arch;
+    if (n_inputs) *n_inputs = psb::mlp_inputs(c->mlp_arch);
+    if (n_params) *n_params = psb::mlp_params(c->mlp_arch);
+    return PSB_OK;
+}
+
 int psb_mlp_set_weights(psb_ctx* c, const float* w) {
     if (!c || !w) return PSB_EINVAL;
     cudaSetDevice(c->device);
-    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->mlp_w, w, sizeof(float) * psb::kMlpParams, cudaMemcpyHostToDevice, c->stream), "weights"));
+    const int np = psb::mlp_params(c->mlp_arch);
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->mlp_w, w, sizeof(float) * np, cudaMemcpyHostToDevice, c->stream), "weights"));
     cudaMemsetAsync(c->mlp_m1, 0, sizeof(float) * psb::kMlpParams, c->stream);
     cudaMemsetAsync(c->mlp_m2, 0, sizeof(float) * psb::kMlpParams, c->stream);
-    psb::launch_to_bf16(c->stream, c->mlp_w, c->mlp_wbf);
+    psb::launch_to_bf16(c->stream, np, c->mlp_w, c->mlp_wbf);
     c->mlp_step = 0;
     c->mlp_set = true;
     PSB_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "weights"));
@@ -1242,7 +1278,8 @@ int psb_mlp_set_weights(psb_ctx* c, const float* w) {
 int psb_mlp_get_weights(psb_ctx* c, float* w) {
     if (!c || !w) return PSB_EINVAL;
     cudaSetDevice(c->device);
-    PSB_TRY(cuda_check(c, cudaMemcpyAsync(w, c->mlp_w, sizeof(float) * psb::kMlpParams, cudaMemcpyDeviceToHost, c->stream), "weights"));
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(w, c->mlp_w, sizeof(float) * psb::mlp_params(c->mlp_arch), cudaMemcpyDeviceToHost,
+                                          c->stream), "weights"));
     return cuda_check(c, cudaStreamSynchronize(c->stream), "weights");
 }
 
@@ -1292,9 +1329,12 @@ int psb_mlp_train(psb_ctx* c, int32_t iters, int32_t batch, float lr, uint64_t s
     }
     for (int it = 0; it < iters; ++it) {
         psb::launch_mlp_sample(st, batch, rows, seed + 0x100000001ull * (uint64_t)(c->mlp_step + 1), c->sel);
-        timed(c, "mlp_train", [&] { psb::launch_mlp_grad(st, batch, c->ds_X, c->ds_T, c->sel, c->mlp_wbf, c->mlp_grad, c->mlp_loss); });
+        timed(c, "mlp_train", [&] {
+            psb::launch_mlp_grad(st, c->mlp_arch, batch, c->ds_X, c->ds_T, c->sel, c->mlp_wbf, c->mlp_grad, c->mlp_loss);
+        });
         ++c->mlp_step;
-        psb::launch_adam(st, c->mlp_w, c->mlp_grad, c->mlp_m1, c->mlp_m2, c->mlp_wbf, lr, c->mlp_step);
+        psb::launch_adam(st, psb::mlp_params(c->mlp_arch), c->mlp_w, c->mlp_grad, c->mlp_m1, c->mlp_m2, c->mlp_wbf, lr,
+                         c->mlp_step);
     }
     if (loss) {
         PSB_TRY(cuda_check(c, cudaMemcpyAsync(loss, c->mlp_loss, sizeof(float), cudaMemcpyDeviceToHost, st), "loss"));
@@ -1314,12 +1354,13 @@ static int mlp_host_call(psb_ctx* c, const float* X, const float* T, int32_t n, 
     if (!rc) rc = cuda_check(c, cudaMemcpyAsync(dX, X, sizeof(float) * 8 * n, cudaMemcpyHostToDevice, st), "mlp");
     if (!rc && T) rc = cuda_check(c, cudaMemcpyAsync(dT, T, sizeof(float) * n, cudaMemcpyHostToDevice, st), "mlp");
     if (!rc && y) {
-        psb::launch_mlp_forward(st, n, dX, 8, c->mlp_wbf, dy);
+        psb::launch_mlp_forward(st, c->mlp_arch, n, dX, c->mlp_wbf, dy);
         rc = cuda_check(c, cudaMemcpyAsync(y, dy, sizeof(float) * n, cudaMemcpyDeviceToHost, st), "mlp");
     }
     if (!rc && grad) {
-        psb::launch_mlp_grad(st, n, dX, dT, nullptr, c->mlp_wbf, c->mlp_grad, c->mlp_loss);
-        rc = cuda_check(c, cudaMemcpyAsync(grad, c->mlp_grad, sizeof(float) * psb::kMlpParams, cudaMemcpyDeviceToHost, st), "mlp");
+        psb::launch_mlp_grad(st, c->mlp_arch, n, dX, dT, nullptr, c->mlp_wbf, c->mlp_grad, c->mlp_loss);
+        rc = cuda_check(c, cudaMemcpyAsync(grad, c->mlp_grad, sizeof(float) * psb::mlp_params(c->mlp_arch),
+                                           cudaMemcpyDeviceToHost, st), "mlp");
         if (!rc && loss) rc = cuda_check(c, cudaMemcpyAsync(loss, c->mlp_loss, sizeof(float), cudaMemcpyDeviceToHost, st), "mlp");
     }
     if (!rc) rc = cuda_check(c, cudaStreamSynchronize(st), "mlp");
@@ -1381,6 +1422,45 @@ int psb_build_neighbors(psb_ctx* c) {
     if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_build_neighbors before psb_upload");
     cudaSetDevice(c->device);
     PSB_TRY(build(c));
+    return read_flags(c);
+}
+
+int psb_warm_start(psb_ctx* c, float* features, float* pressure) {
+    if (!c) return PSB_EINVAL;
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_warm_start before psb_upload");
+    if (c->batch || !c->P.pci || c->P.ref)
+        return fail(c, PSB_EINVAL, "psb_warm_start: single config-profile PCISPH scenes only");
+    cudaSetDevice(c->device);
+    const int mode = c->sc.warm_start;
+    if (mode == PSB_WARM_LEARNED && !c->mlp_set) return fail(c, PSB_ESTATE, "psb_warm_start: no network weights set");
+    PSB_TRY(build(c, /*keep_p=*/true, /*features=*/true));
+    cudaStream_t st = c->stream;
+    const int n = c->n;
+    const int* ids = c->ids[c->cr];
+    float* stage = (float*)c->stage;
+    if (features) {
+        k_scatter_rows8<<<blocks(n), psb::kBlock, 0, st>>>(n, ids, c->feats, stage);
+        PSB_TRY(cuda_check(c, cudaMemcpyAsync(features, stage, sizeof(float) * 8 * (size_t)n, cudaMemcpyDeviceToHost, st),
+                           "warm_start"));
+        PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "warm_start"));
+    }
+    if (pressure) {
+        if (mode == PSB_WARM_ZERO) {
+            std::memset(pressure, 0, sizeof(float) * (size_t)n);
+        } else {
+            // the learned guess goes to the corrector's scratch: the carried
+            // pressure, an input of the next step, stays in place
+            const float2* src = c->rp[c->cr];
+            if (mode == PSB_WARM_LEARNED) {
+                psb::launch_mlp_infer(st, c->mlp_arch, n, c->feats, c->mlp_wbf, c->p_scale, c->rpc);
+                src = c->rpc;
+            }
+            k_scatter_rp<<<blocks(n), psb::kBlock, 0, st>>>(n, ids, src, 1, stage);
+            PSB_TRY(cuda_check(c, cudaMemcpyAsync(pressure, stage, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, st),
+                               "warm_start"));
+        }
+    }
+    PSB_TRY(cuda_check(c, cudaGetLastError(), "warm_start"));
     return read_flags(c);
 }
 
@@ -1975,7 +2055,8 @@ int psb_batch_stats(psb_ctx* c, int32_t* iters, int32_t* converged, double* err_
 
 int psb_set_graph(psb_ctx* c, int32_t on) {
     if (!c) return PSB_EINVAL;
-    if (!c->batch) return fail(c, PSB_EINVAL, "psb_set_graph: batches only (psb_create_batch)");
+    if (!c->batch && !(c->P.pci && !c->P.ref))
+        return fail(c, PSB_EINVAL, "psb_set_graph: batches and config-profile PCISPH scenes only");
     cudaSetDevice(c->device);
     if (!on) release_graphs(c);
     c->graph_on = on != 0;
@@ -2089,7 +2170,7 @@ int psb_autotune(psb_ctx* c, int32_t trials, psb_tune* out) {
     if (sph)
         tune_one(1, [&](const Params& Q) {
             psb::launch_density_x(st, Q, c->pos[s], c->vel[s], c->nbr_count, c->nbr_list, c->rp[r], c->rho_x, 0,
-                                  c->p_scale, feats ? c->feats : nullptr);
+                                  c->p_scale, feats ? c->feats : nullptr, psb::mlp_inputs(c->mlp_arch));
         });
     if (pci) {
         tune_one(2, [&](const Params& Q) {

@@ -28,6 +28,7 @@
 // is closed wherever the field is.
 #include <cuda_runtime.h>
 #include <cmath>
+#include <cstdio>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -280,6 +281,45 @@ __global__ void k_mc_triangles(IsoParams Q, const double* __restrict__ iso, cons
             tris[3 * ((size_t)base + t) + k] = (int32_t)edge_off[global_edge(Q, x, y, z, c_tri[cs][3 * t + k])];
 }
 
+// polygonize_MarchingCube_Kernel (MarchingCube_Kernel.cu:36-139) on the
+// reference's layout: nodes are double4 (x, y, z, value); every cube with a
+// triangle appends its triangles' vertices, three per triangle, to its own
+// `slots` vertex slots (vertex[c * slots + k], index[c * slots + k] = k) and
+// counts them in count[c], which it reads first (the reference accumulates).
+// Vertices are interpolated on the cube's edges in the reference's corner
+// order; a cube whose slots would overflow stops and raises *overflow.
+__global__ void k_mc_polygonize_slots(const double* __restrict__ node4, int nx, int ny, int nz, double level,
+                                      int* __restrict__ count, double* __restrict__ vertex, int* __restrict__ index,
+                                      int slots, int* __restrict__ overflow) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (long long)nx * ny * nz) return;
+    const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((long long)nx * ny));
+    if (x + 1 >= nx || y + 1 >= ny || z + 1 >= nz) return;
+    long long corner[8];
+    int cs = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        corner[k] = (x + c_corner[k][0]) + (long long)(y + c_corner[k][1]) * nx +
+                    (long long)(z + c_corner[k][2]) * nx * ny;
+        if (node4[4 * corner[k] + 3] <= level) cs |= 1 << k;
+    }
+    const int nt = c_ntri[cs];
+    if (nt == 0) return;
+    int m = count[c];
+    for (int t = 0; t < nt; ++t)
+        for (int v = 0; v < 3; ++v) {
+            if (m < 0 || m >= slots) { *overflow = 1; count[c] = m; return; }
+            const int e = c_tri[cs][3 * t + v];
+            const long long a = corner[c_edge[e][0]], b = corner[c_edge[e][1]];
+            const double va = node4[4 * a + 3], vb = node4[4 * b + 3];
+            double* out = vertex + 3 * ((size_t)c * slots + m);
+            for (int d = 0; d < 3; ++d) out[d] = interp(level, va, vb, node4[4 * a + d], node4[4 * b + d]);
+            index[(size_t)c * slots + m] = m;
+            ++m;
+        }
+    count[c] = m;
+}
+
 // ---- exclusive scan of uint32 (three-level, 1024 items per block) ------------
 constexpr int kScanThreads = 256, kScanItems = 4, kScanTile = kScanThreads * kScanItems;
 
@@ -318,6 +358,26 @@ __global__ void k_scan_add(long long n, uint32_t* __restrict__ data, const uint3
 inline unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
+
+void launch_mc_polygonize_slots(cudaStream_t st, const double* node4, int nx, int ny, int nz, double level, int* count,
+                                double* vertex, int* index, int slots) {
+    static int* d_overflow = nullptr;
+    if (!d_overflow && cudaMalloc((void**)&d_overflow, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        d_overflow = nullptr;
+    }
+    int* flag = d_overflow;
+    if (!flag) return;
+    cudaMemsetAsync(flag, 0, sizeof(int), st);
+    const long long nn = (long long)nx * ny * nz;
+    k_mc_polygonize_slots<<<blocks_for(nn, 256), 256, 0, st>>>(node4, nx, ny, nz, level, count, vertex, index, slots,
+                                                               flag);
+    int h = 0;
+    cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    if (h) std::fprintf(stderr, "polygonize_MarchingCube_CUDA: a cell needed more than %d vertex slots (stopped there)\n",
+                        slots);
+}
 
 void mc_upload_table(cudaStream_t st) {
     static uint8_t ntri[256];

@@ -169,9 +169,10 @@ void launch_build_nbr(cudaStream_t st, const Params& P, const float4* pos, const
                       const uint32_t* cell_start, const uint32_t* cell_end, int* counts, int* list, int* flags);
 
 // ---- launchers (sph.cu) ---------------------------------------------------
+// feats != nullptr: also the warm start's inputs f0 .. f(nfeat - 1), nfeat 6 or 7.
 void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
                       const int* list, float2* rp, float* rho_x, int zero_p, float p_scale = 1.f,
-                      float* feats = nullptr);
+                      float* feats = nullptr, int nfeat = 7);
 void launch_wcsph_force(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const float4* vap,
                         const float2* rp, const int* counts, const int* list, float4* pos_out, float4* vel_out,
                         float4* vap_out, float4* fnp);
@@ -262,16 +263,24 @@ void launch_mc_classify(cudaStream_t st, const IsoParams& Q, const double* iso, 
                         uint32_t* edge_flag);
 void launch_mc_emit(cudaStream_t st, const IsoParams& Q, const double* iso, const uint32_t* edge_off,
                     const uint32_t* tri_off, float* vert, int32_t* tris);
+// The reference's polygonizer layout (compat): double4 nodes, per-cube vertex
+// slots and counts; synchronous, reports a slot overflow on stderr.
+void launch_mc_polygonize_slots(cudaStream_t st, const double* node4, int nx, int ny, int nz, double level, int* count,
+                                double* vertex, int* index, int slots);
 
 // ---- learned warm start (mlp.cu) ---------------------------------------------------
-constexpr int kMlpParams = 4737;   // 7x64 + 64 + 64x64 + 64 + 64 + 1
-void launch_mlp_infer(cudaStream_t st, int n, const float* feats, const void* wbf, float p_scale, float2* rp);
-void launch_mlp_forward(cudaStream_t st, int n, const float* X, int stride, const void* wbf, float* y);
-void launch_mlp_grad(cudaStream_t st, int batch, const float* X, const float* T, const uint32_t* sel, const void* wbf,
-                     float* grad, float* loss);
+// Networks (psb.h PSB_MLP_*): arch 0 6 -> 64 -> 64 -> 1 SiLU, arch 1 7 -> 64 -> 64 -> 1 ReLU.
+constexpr int kMlpParams = 4737;   // the larger network's parameters: 7x64 + 64 + 64x64 + 64 + 64 + 1
+int mlp_inputs(int arch);
+int mlp_params(int arch);
+void launch_mlp_infer(cudaStream_t st, int arch, int n, const float* feats, const void* wbf, float p_scale, float2* rp);
+void launch_mlp_forward(cudaStream_t st, int arch, int n, const float* X, const void* wbf, float* y);
+void launch_mlp_grad(cudaStream_t st, int arch, int batch, const float* X, const float* T, const uint32_t* sel,
+                     const void* wbf, float* grad, float* loss);
 void launch_mlp_sample(cudaStream_t st, int batch, uint64_t size, uint64_t seed, uint32_t* sel);
-void launch_adam(cudaStream_t st, float* w, const float* grad, float* m1, float* m2, void* wbf, float lr, int step);
-void launch_to_bf16(cudaStream_t st, const float* w, void* wbf);
+void launch_adam(cudaStream_t st, int np, float* w, const float* grad, float* m1, float* m2, void* wbf, float lr,
+                 int step);
+void launch_to_bf16(cudaStream_t st, int np, const float* w, void* wbf);
 void launch_collect(cudaStream_t st, int n, int stride, int offset, uint64_t base, uint64_t cap, const float* feats,
                     const float2* rp, float p_scale, float* X, float* T);
 void launch_zero_pressure(cudaStream_t st, int n, float2* rp);

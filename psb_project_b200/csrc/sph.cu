@@ -294,9 +294,9 @@ __device__ __forceinline__ void box_project(const Params& P, int t, float3& x, f
 // SphKernel.cu:25; config: Tait, p = k rho0/7 ((rho/rho0)^7 - 1), written as
 // k rho0/7 d (1 + x + ... + x^6) with x = 1 + d to avoid cancellation).
 // PCISPH: keeps the carried pressure (warm start) or zeroes it.
-// FEAT (config PCISPH, learned warm start or data collection): the same
+// NF (config PCISPH, learned warm start or data collection): the same
 // neighbour walk also sums the velocity divergence and density gradient and
-// writes the MLP's seven inputs (feats, stride 8):
+// writes the MLP's first NF inputs (6 or 7; feats, stride 8, the rest 0):
 //   f0 neighbour count / 32
 //   f1 advected density deviation (rho - dt rho div v - rho0)/rho0 * 100
 //   f2 div v * dt * 100, div v = -(k_grad/rho0) sum (1-u)^2 (v_j - v_i).x^
@@ -305,12 +305,13 @@ __device__ __forceinline__ void box_project(const Params& P, int t, float3& x, f
 //   f5 k_grad |sum (1-u)^2 x^| h / rho0 (density-gradient magnitude)
 //   f6 sum W_ij p_j / sum W_ij / p_scale over the list, self included: the
 //      carried pressure smoothed with the poly6 weights
-template <bool REF, bool FEAT, bool BATCH, int BS>
+template <bool REF, int NF, bool BATCH, int BS>
 __global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __restrict__ pos,
                                                       const float4* __restrict__ vel, const int* __restrict__ counts,
                                                       const int* __restrict__ list, float2* __restrict__ rp,
                                                       float* __restrict__ rho_x, int zero_p, float p_scale,
                                                       float* __restrict__ feats) {
+    constexpr bool FEAT = NF > 0, SMOOTH_P = NF > 6;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= P.n) return;
     const float4 xi = pos[t];
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __rest
         const float w = 1.f - q;
         const float w3 = w * w * w;
         acc.add(w3);
-        if (FEAT) {     // carried pressures: this pass writes rp[j].y back unchanged
+        if (SMOOTH_P) {     // carried pressures: this pass writes rp[j].y back unchanged
             wp += w3 * rp[j].y;
             ws += w3;
         }
@@ -366,14 +367,13 @@ __global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __rest
         dwall = fminf(dwall, fminf(xi.x - F.x0(), F.x1() - xi.x));
         dwall = fminf(dwall, fminf(xi.y - F.y0(), F.y1() - xi.y));
         dwall = fminf(dwall, fminf(xi.z - F.z0(), F.z1() - xi.z));
-        float* f = feats + (size_t)t * 8;
-        f[0] = (float)counts[t] * (1.f / 32.f);
-        f[1] = (rho - P.dt * rho * div - P.rho0) / P.rho0 * 100.f;
-        f[2] = div * P.dt * 100.f;
-        f[3] = rp[t].y / p_scale;          // the carried pressure, before this pass replaces it
-        f[4] = fmaxf(dwall, 0.f) * P.inv_h;
-        f[5] = P.k_grad * sqrtf(gr.x * gr.x + gr.y * gr.y + gr.z * gr.z) * P.hf / P.rho0;
-        f[6] = ws > 0.f ? wp / ws / p_scale : 0.f;
+        float4* f = reinterpret_cast<float4*>(feats + (size_t)t * 8);     // two 16-byte stores
+        f[0] = make_float4((float)counts[t] * (1.f / 32.f), (rho - P.dt * rho * div - P.rho0) / P.rho0 * 100.f,
+                           div * P.dt * 100.f,
+                           rp[t].y / p_scale);     // the carried pressure, before this pass replaces it
+        f[1] = make_float4(fmaxf(dwall, 0.f) * P.inv_h,
+                           P.k_grad * sqrtf(gr.x * gr.x + gr.y * gr.y + gr.z * gr.z) * P.hf / P.rho0,
+                           SMOOTH_P && ws > 0.f ? wp / ws / p_scale : 0.f, 0.f);
     }
     rp[t] = make_float2(rho, p);
     rho_x[t] = rho;
@@ -598,6 +598,7 @@ __global__ void __launch_bounds__(BS) k_pci_force_predict(Params P, const float4
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= P.n) return;
     if (BATCH && !P.active[P.slot_scene[t]]) return;     // its scene has converged
+    if (!BATCH && P.active && !P.active[0]) return;      // single scene, corrector decided on the device: converged
     const float4* __restrict__ geo = REF ? xs : pos;
     const float4 xi = geo[t];
     const float2 ri = rpc[t];
@@ -693,18 +694,24 @@ inline int grid_of(int n) { return (n + kBlock - 1) / kBlock; }
 template <int BS>
 inline unsigned blocks_of(int n) { return (unsigned)((n + BS - 1) / BS); }
 
+
 void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
-                      const int* list, float2* rp, float* rho_x, int zero_p, float p_scale, float* feats) {
+                      const int* list, float2* rp, float* rho_x, int zero_p, float p_scale, float* feats, int nfeat) {
     if (P.n <= 0) return;
     with_block(P.tune.density_block, [&](auto B) {
         constexpr int BS = decltype(B)::value;
         auto go = [&](auto kernel) {
             kernel<<<blocks_of<BS>(P.n), BS, 0, st>>>(P, pos, vel, counts, list, rp, rho_x, zero_p, p_scale, feats);
         };
-        if (P.ref) go(k_density_x<true, false, false, BS>);
-        else if (P.scenes) { if (feats) go(k_density_x<false, true, true, BS>); else go(k_density_x<false, false, true, BS>); }
-        else if (feats) go(k_density_x<false, true, false, BS>);
-        else go(k_density_x<false, false, false, BS>);
+        const int nf = feats ? (nfeat > 6 ? 7 : 6) : 0;
+        if (P.ref) go(k_density_x<true, 0, false, BS>);
+        else if (P.scenes) {
+            if (nf == 7) go(k_density_x<false, 7, true, BS>);
+            else if (nf == 6) go(k_density_x<false, 6, true, BS>);
+            else go(k_density_x<false, 0, true, BS>);
+        } else if (nf == 7) go(k_density_x<false, 7, false, BS>);
+        else if (nf == 6) go(k_density_x<false, 6, false, BS>);
+        else go(k_density_x<false, 0, false, BS>);
     });
 }
 
@@ -741,7 +748,9 @@ void launch_pci_density(cudaStream_t st, const Params& P, const float4* xs, cons
     if (P.n <= 0) return;
     with_block(P.tune.pci_density_block, [&](auto B) {
         constexpr int BS = decltype(B)::value;
-        auto go = [&](auto kernel) { kernel<<<blocks_of<BS>(P.n), BS, 0, st>>>(P, xs, rp, counts, list, rpc, err_slot); };
+        auto go = [&](auto kernel) {
+            kernel<<<blocks_of<BS>(P.n), BS, 0, st>>>(P, xs, rp, counts, list, rpc, err_slot);
+        };
         if (P.ref) go(k_pci_density<true, false, BS>);
         else if (P.scenes) go(k_pci_density<false, true, BS>);
         else go(k_pci_density<false, false, BS>);

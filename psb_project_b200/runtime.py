@@ -42,10 +42,13 @@ EXPORTS = (
     "psb_set_boundary", "psb_boundary_psi", "psb_context_info", "psb_set_step_count", "psb_write_txt",
     "psb_write_xml", "psb_write_vol", "psb_write_obj", "psb_export_txt", "psb_export_xml", "psb_checkpoint_save",
     "psb_checkpoint_load", "psb_boundary_forces", "psb_set_external_force", "psb_set_colliders", "psb_emit",
-    "psb_add_emitter", "psb_clear_emitters", "psb_emitter_positions",
+    "psb_add_emitter", "psb_clear_emitters", "psb_emitter_positions", "psb_mlp_set_arch", "psb_mlp_info",
+    "psb_warm_start",
 )
-MLP_PARAMS = 4737       # PSB_MLP_PARAMS
-MLP_IN, MLP_H = 7, 64
+MLP_SILU6, MLP_RELU7 = 0, 1   # PSB_MLP_SILU6 (the configured network), PSB_MLP_RELU7
+MLP_PARAMS = 4737       # PSB_MLP_PARAMS: the larger network's count
+MLP_H = 64
+MLP_INPUTS = {MLP_SILU6: 6, MLP_RELU7: 7}
 NOALLOC_MAX_N = 262144   # PSB_NOALLOC_MAX_N
 
 
@@ -144,6 +147,9 @@ def lib():
         "psb_sort_cells_noalloc": ([P, P, P, P, I32, I32, P], ctypes.c_int),
         "psb_presolve": ([P, I32], ctypes.c_int),
         "psb_mlp_set_weights": ([P, P], ctypes.c_int),
+        "psb_mlp_set_arch": ([P, I32], ctypes.c_int),
+        "psb_mlp_info": ([P, P, P, P], ctypes.c_int),
+        "psb_warm_start": ([P, P, P], ctypes.c_int),
         "psb_mlp_get_weights": ([P, P], ctypes.c_int),
         "psb_mlp_collect": ([P, I32, I64], ctypes.c_int),
         "psb_mlp_dataset": ([P, ctypes.POINTER(I64), P, P], ctypes.c_int),
@@ -206,13 +212,18 @@ def lattice(nxyz, spacing, origin, jitter, seed, id0=0) -> np.ndarray:
     return out
 
 
-def mlp_init_weights(seed: int = 0) -> np.ndarray:
-    """He-uniform initial weights in the psb_mlp layout: W1[64][6], b1[64],
+def mlp_params(arch: int = MLP_SILU6) -> int:
+    """Parameter count of a network: 64 n_in + 64 + 64 x 64 + 64 + 64 + 1."""
+    return MLP_H * MLP_INPUTS[arch] + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1
+
+
+def mlp_init_weights(seed: int = 0, arch: int = MLP_SILU6) -> np.ndarray:
+    """He-uniform initial weights in the psb_mlp layout: W1[64][n_in], b1[64],
     W2[64][64], b2[64], W3[64], b3 (biases zero)."""
     rng = np.random.default_rng(seed)
-    w = np.zeros(MLP_PARAMS, np.float32)
+    w = np.zeros(mlp_params(arch), np.float32)
     o = 0
-    for fan_in, fan_out in ((MLP_IN, MLP_H), (MLP_H, MLP_H), (MLP_H, 1)):
+    for fan_in, fan_out in ((MLP_INPUTS[arch], MLP_H), (MLP_H, MLP_H), (MLP_H, 1)):
         lim = np.sqrt(6.0 / fan_in)
         w[o:o + fan_in * fan_out] = rng.uniform(-lim, lim, fan_in * fan_out) * (0.5 if fan_out == 1 else 1.0)
         o += fan_in * fan_out + fan_out
@@ -220,10 +231,12 @@ def mlp_init_weights(seed: int = 0) -> np.ndarray:
 
 
 def mlp_unpack(w: np.ndarray):
-    """(W1, b1, W2, b2, W3, b3) views of a flat parameter vector."""
+    """(W1, b1, W2, b2, W3, b3) views of a flat parameter vector (either
+    network: the input count follows from the length)."""
+    n_in = (len(w) - (MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1)) // MLP_H
     o = 0
     out = []
-    for shape in ((MLP_H, MLP_IN), (MLP_H,), (MLP_H, MLP_H), (MLP_H,), (MLP_H,), (1,)):
+    for shape in ((MLP_H, n_in), (MLP_H,), (MLP_H, MLP_H), (MLP_H,), (MLP_H,), (1,)):
         k = int(np.prod(shape))
         out.append(w[o:o + k].reshape(shape))
         o += k
@@ -348,15 +361,35 @@ class Simulation:
         self._check(lib().psb_presolve(self._h, int(iters)), "psb_presolve")
 
     # -- learned warm start -------------------------------------------------------
+    def mlp_set_arch(self, arch: int):
+        """Selects the network (MLP_SILU6, the configured one and the default,
+        or MLP_RELU7); clears its weights."""
+        self._check(lib().psb_mlp_set_arch(self._h, int(arch)), "psb_mlp_set_arch")
+
+    def mlp_info(self) -> dict:
+        a, ni, npar = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._check(lib().psb_mlp_info(self._h, ctypes.byref(a), ctypes.byref(ni), ctypes.byref(npar)), "psb_mlp_info")
+        return {"arch": a.value, "n_inputs": ni.value, "n_params": npar.value}
+
     def mlp_set_weights(self, w):
         w = np.ascontiguousarray(w, np.float32)
-        assert w.shape == (MLP_PARAMS,)
+        if w.shape != (self.mlp_info()["n_params"],):
+            raise ValueError(f"weights of shape {w.shape} for a network of {self.mlp_info()['n_params']} parameters")
         self._check(lib().psb_mlp_set_weights(self._h, _ptr(w)), "psb_mlp_set_weights")
 
     def mlp_get_weights(self) -> np.ndarray:
-        w = np.empty(MLP_PARAMS, np.float32)
+        w = np.empty(self.mlp_info()["n_params"], np.float32)
         self._check(lib().psb_mlp_get_weights(self._h, _ptr(w)), "psb_mlp_get_weights")
         return w
+
+    def warm_start(self):
+        """(features (n, 8), initial pressure (n,)) of the next step, id
+        order, without stepping (psb_warm_start)."""
+        n = self.n
+        F = np.empty((n, 8), np.float32)
+        p = np.empty(n, np.float32)
+        self._check(lib().psb_warm_start(self._h, _ptr(F), _ptr(p)), "psb_warm_start")
+        return F, p
 
     def mlp_collect(self, stride: int, capacity: int = 1 << 22):
         self._check(lib().psb_mlp_collect(self._h, int(stride), int(capacity)), "psb_mlp_collect")
@@ -399,7 +432,7 @@ class Simulation:
         X8 = np.zeros((X.shape[0], 8), np.float32)
         X8[:, :X.shape[1]] = X
         T = np.ascontiguousarray(T, np.float32)
-        g = np.empty(MLP_PARAMS, np.float32)
+        g = np.empty(self.mlp_info()["n_params"], np.float32)
         loss = ctypes.c_float()
         self._check(lib().psb_mlp_loss_grad(self._h, _ptr(X8), _ptr(T), X.shape[0], ctypes.byref(loss), _ptr(g)),
                     "psb_mlp_loss_grad")
@@ -605,6 +638,11 @@ class Simulation:
     def profile(self, on: bool = True):
         self._check(lib().psb_profile_enable(self._h, 1 if on else 0), "psb_profile_enable")
 
+    def set_graph(self, on: bool = True):
+        """CUDA-graph stepping (batches and config-profile PCISPH scenes): each
+        step one cudaGraphLaunch, the corrector a device-side while loop."""
+        self._check(lib().psb_set_graph(self._h, 1 if on else 0), "psb_set_graph")
+
     def profile_reset(self):
         self._check(lib().psb_profile_reset(self._h), "psb_profile_reset")
 
@@ -657,9 +695,6 @@ class BatchSimulation(Simulation):
         self._check(lib().psb_batch_stats(self._h, _ptr(it), _ptr(cv), _ptr(err), _ptr(tot), _ptr(unc)),
                     "psb_batch_stats")
         return {"iters": it, "converged": cv, "err_final": err, "iters_total": tot, "unconverged_steps": unc}
-
-    def set_graph(self, on: bool = True):
-        self._check(lib().psb_set_graph(self._h, 1 if on else 0), "psb_set_graph")
 
     def split(self, a: np.ndarray):
         """Per-scene views of an array in particle-id order."""

@@ -62,7 +62,7 @@ def test_struct_layout_matches_header(tmp_path):
 
 def test_abi_version_and_status_strings():
     L = R.lib()
-    assert L.psb_abi_version() == 1
+    assert L.psb_abi_version() == 2
     assert L.psb_status_string(0) == b"ok"
     assert L.psb_status_string(3) == b"neighbour list overflow"
     assert L.psb_status_string(99) == b"unknown status"

@@ -170,3 +170,40 @@ def test_graph_after_reupload_equals_eager():
     for key in ("pos", "vel", "pressure"):
         assert np.array_equal(res[0][0][key], res[1][0][key]), key
     assert np.array_equal(res[0][1], res[1][1])
+
+
+def run_single_graph(sc, steps, weights, presolve, graph):
+    with P.Simulation(sc) as sim:
+        if weights is not None:
+            sim.mlp_set_weights(weights)
+        sim.set_graph(graph)
+        sim.upload(P.scene_positions(sc))
+        if presolve:
+            sim.presolve(presolve)
+        its, errs = [], []
+        for _ in range(steps):
+            sim.step(1)
+            st = sim.stats()
+            its.append(st.iters)
+            errs.append([st.err[k] for k in range(st.iters + 1)])
+        out = sim.download()
+        out["iters_total"] = sim.stats().iters_total
+        return out, its, errs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("warm", ["zero", "learned"])
+def test_single_scene_graph_equals_eager(warm):
+    """A config-profile PCISPH scene stepped as one CUDA graph per step
+    (the corrector a device-side while node) gives the kernel-by-kernel
+    result bit for bit, with the same corrections and error history."""
+    mode = P.WARM_ZERO if warm == "zero" else P.WARM_LEARNED
+    sc = small_batch(1, warm_start=mode, seed=21)[0]
+    w = P.mlp_init_weights(7) if warm == "learned" else None
+    eager, it_e, err_e = run_single_graph(sc, 12, w, 8, graph=False)
+    graph, it_g, err_g = run_single_graph(sc, 12, w, 8, graph=True)
+    for key in ("pos", "vel", "vel_half", "pressure", "density"):
+        assert np.array_equal(eager[key], graph[key]), key
+    assert it_e == it_g and err_e == err_g
+    assert eager["iters_total"] == graph["iters_total"] == sum(it_e)
+    assert max(it_e) >= 3

@@ -148,8 +148,14 @@ class Vec3(ctypes.Structure):
     _fields_ = [("e", ctypes.c_double * 3)]
 
 
+# The launchers take the reference's Vector3 by value; its user-provided
+# copy constructor makes the C++ ABI pass it through a hidden pointer, so a
+# C caller (ctypes here) passes a pointer to the three doubles.
+PV3 = ctypes.POINTER(Vec3)
+
+
 def _v3(a):
-    return Vec3((ctypes.c_double * 3)(*[float(t) for t in a]))
+    return ctypes.pointer(Vec3((ctypes.c_double * 3)(*[float(t) for t in a])))
 
 
 def _compat(lib, name, spec, xo, x, v, dt, torch):
@@ -162,15 +168,15 @@ def _compat(lib, name, spec, xo, x, v, dt, torch):
     keep = []
     if typ == C.PLANE:
         f = lib.collisionPlan_CUDA
-        f.argtypes = [V, V, V, V, Vec3, Vec3, Vec3, Vec3, Vec3, fl, fl, I]
+        f.argtypes = [V, V, V, V, PV3, PV3, PV3, PV3, PV3, fl, fl, I]
         f(p(to), p(tx), p(tv), p(tv), *[_v3(vv[3 * k:3 * k + 3]) for k in range(5)], elast, dt, len(x))
     elif typ == C.SPHERE:
         f = lib.collisionSystem_Sphere_CUDA
-        f.argtypes = [V, V, V, V, fl, fl, I, Vec3, fl, fl, ctypes.c_bool]
+        f.argtypes = [V, V, V, V, fl, fl, I, PV3, fl, fl, ctypes.c_bool]
         f(p(to), p(tx), p(tv), p(tv), 0.01, dt, len(x), _v3(vv[:3]), vv[3], elast, bool(container))
     elif typ == C.CYLINDER:
         f = lib.collisionCylinder_CUDA
-        f.argtypes = [V, V, fl, fl, I, Vec3, Vec3, ctypes.c_double, ctypes.c_double, fl, ctypes.c_bool]
+        f.argtypes = [V, V, fl, fl, I, PV3, PV3, ctypes.c_double, ctypes.c_double, fl, ctypes.c_bool]
         f(p(tx), p(tv), 0.01, dt, len(x), _v3(vv[:3]), _v3(vv[3:6]), vv[6], vv[7], elast, True)
     elif typ == C.MESH:
         F = np.asarray(faces, np.float32).reshape(-1, 12)
@@ -184,17 +190,17 @@ def _compat(lib, name, spec, xo, x, v, dt, torch):
         mn, mx = _v3(vv[:3]), _v3(vv[3:6])
         if T.shape[0] == 1 and T[0, 0] == C.HEIGHT_LINEAR:
             f = lib.collisionSystem_Linear_HeightFieldCollision_CUDA
-            f.argtypes = [V, V, V, V, ctypes.c_double, fl, U, ctypes.c_double, ctypes.c_double, Vec3, Vec3, fl]
+            f.argtypes = [V, V, V, V, ctypes.c_double, fl, U, ctypes.c_double, ctypes.c_double, PV3, PV3, fl]
             f(p(to), p(tx), p(tv), p(tv), 0.01, dt, len(x), T[0, 1], T[0, 2], mn, mx, elast)
         elif T.shape[0] == 1 and T[0, 0] == C.HEIGHT_GAUSSIAN:
             f = lib.collisionSystem_Gaussian_HeightFieldCollision_CUDA
-            f.argtypes = [V, V, V, V, ctypes.c_double, fl, U] + [ctypes.c_double] * 5 + [Vec3, Vec3, fl]
+            f.argtypes = [V, V, V, V, ctypes.c_double, fl, U] + [ctypes.c_double] * 5 + [PV3, PV3, fl]
             f(p(to), p(tx), p(tv), p(tv), 0.01, dt, len(x), *[float(c) for c in T[0, 1:6]], mn, mx, elast)
         else:
             cols = [d(T[:, k]) for k in (1, 2, 3, 4)]
             keep += cols
             f = lib.collisionSystem_Periodic_HeightFieldCollision_CUDA
-            f.argtypes = [V, V, V, V, ctypes.c_double, fl, U, U, V, V, V, V, Vec3, Vec3, fl]
+            f.argtypes = [V, V, V, V, ctypes.c_double, fl, U, U, V, V, V, V, PV3, PV3, fl]
             f(p(to), p(tx), p(tv), p(tv), 0.01, dt, len(x), T.shape[0], *[p(t) for t in cols], mn, mx, elast)
     f.restype = None
     torch.cuda.synchronize()

@@ -57,7 +57,10 @@ def L():
     lib.interpolateSPHVelocities.argtypes = [V, V, V, V, I]
     lib.integrateSystem.argtypes = [V, V, V, V, V, V, D, I, I]
     lib.interactionSystem.argtypes = [V, V, V, V, V, V, V, V, PartVoisine, I]
-    lib.collisionSystem_Box_CUDA.argtypes = [V, V, V, ctypes.c_float, ctypes.c_float, I, Vec3, Vec3, ctypes.c_bool,
+    # Vector3 by value reaches the callee through a hidden pointer (its copy
+    # constructor is user-provided): a C caller passes the pointer
+    PV3 = ctypes.POINTER(Vec3)
+    lib.collisionSystem_Box_CUDA.argtypes = [V, V, V, ctypes.c_float, ctypes.c_float, I, PV3, PV3, ctypes.c_bool,
                                              ctypes.c_float]
     lib.pci_SPH_update.argtypes = [V] * 19 + [D, PartVoisine, V, V, V, V, V, ctypes.c_float, ctypes.c_uint]
     for f in ("createGrid", "_finalizeGrid", "reinitCells", "storeParticles", "searchNeighbooring",
@@ -134,7 +137,8 @@ def test_elementwise_launchers():
     bx = rng.uniform(-0.2, 1.2, (n, 3))
     d4 = {k: dev(a) for k, a in dict(x=bx, v=v).items()}
     lo, hi = Vec3((ctypes.c_double * 3)(0, 0, 0)), Vec3((ctypes.c_double * 3)(1, 1, 1))
-    lib.collisionSystem_Box_CUDA(ptr(d4["x"]), None, ptr(d4["v"]), 0.1, dtf, n, lo, hi, True, 0.0)
+    lib.collisionSystem_Box_CUDA(ptr(d4["x"]), None, ptr(d4["v"]), 0.1, dtf, n, ctypes.byref(lo), ctypes.byref(hi),
+                                 True, 0.0)
     xw, vw = bx.copy(), v.copy()
     r = np.float32(0.1)
     for i in range(n):

@@ -1,0 +1,116 @@
+"""GPU parity at the configured sizes and over trajectories.
+
+  * The 1,048,576-particle PCISPH dam break (the headline scene): one step
+    of the config method from a pre-solved rest state, through the C ABI,
+    against the FP64 oracle on the same FP32 state. Cell keys, the stable
+    (cell, id) order and the neighbour counts are bit-exact; densities
+    within 1e-5 element-wise; the non-pressure force density within 1e-5 of
+    its max; pressure and velocities within 1e-4 of their max (the floor of
+    an FP32 corrector: every correction adds delta (rho* - rho0), and the
+    FP32 rounding of the predicted positions x* alone moves rho* by ~1e-4
+    kg/m^3, ~1e-5 of the pressure scale per correction); positions within
+    4 float ulps plus 1e-5 of the displacement. The iteration count agrees
+    unless the deciding error sits within 2e-6 of eta.
+  * 50-step PCISPH trajectories, reference and config profile, against the
+    FP64 oracle from the same start: before the flow turns chaotic the
+    positions stay within 1e-4 of the distance travelled (the reference's
+    three fixed corrections), and, for the eta loop, whose FP32 and FP64
+    decisions may differ by one correction on a step, within 1e-3 of it.
+The state sizes here are the configured ones; the oracle runs on every host
+thread.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import psb_project_b200 as P
+from psb_project_b200 import runtime as R
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_norm(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def on_bound(sc, x):
+    x = np.asarray(x, np.float64)
+    lo = (np.asarray(sc.box_min, np.float32) + np.float32(sc.particle_radius)).astype(np.float64)
+    hi = (np.asarray(sc.box_max, np.float32) - np.float32(sc.particle_radius)).astype(np.float64)
+    return np.any((x == lo) | (x == hi), axis=1)
+
+
+def test_c2_full_scene_step_matches_oracle():
+    sc = P.config_scene("C2").replace(warm_start=P.WARM_PREVIOUS)
+    assert sc.n == 1_048_576
+    pos = P.scene_positions(sc)
+    with P.Simulation(sc) as sim:
+        sim.upload(pos)
+        sim.presolve(64)
+        start = sim.download()
+        # grid at the start state: keys, order, neighbour counts
+        sim.build_neighbors()
+        pos64 = start["pos"].astype(np.float64)
+        keys = oracle.cell_keys(sc, pos64)
+        perm = oracle.sort_perm(keys)
+        counts, _ = oracle.neighbors(sc, pos64, with_lists=False)
+        assert np.array_equal(sim.read_field(R.FIELD_CELL_KEY), keys)
+        assert np.array_equal(sim.read_field(R.FIELD_SORTED_ID), perm)
+        assert np.array_equal(sim.read_field(R.FIELD_NBR_COUNT), counts)
+        # one step of the eta loop
+        sim.step(1)
+        out = sim.download()
+        sg = sim.stats()
+        fnp = sim.read_field(R.FIELD_FORCE_NP)
+        rho_x = sim.read_field(R.FIELD_DENSITY_X)
+    orc = oracle.OracleSim(sc, start["pos"], start["vel"], start["vel_half"], start["pressure"], float_state=True)
+    so = orc.step()
+    assert np.array_equal(orc.nbr, counts)
+    assert np.max(np.abs(rho_x - orc.rho_x) / orc.rho_x) <= 1e-5
+    assert rel_norm(fnp, orc.f_np) <= 1e-5
+    for k in range(min(so.iters, sg.iters) + 1):
+        assert abs(sg.err[k] - so.err[k]) <= 1e-5, (k, sg.err[k], so.err[k])
+    if sg.iters != so.iters:
+        k = min(sg.iters, so.iters)
+        assert abs(so.err[k] - sc.eta) <= 2e-6, (sg.iters, so.iters, so.err[k])
+        return
+    assert np.max(np.abs(out["density"] - orc.rho) / orc.rho) <= 1e-5
+    assert rel_norm(out["pressure"], orc.p) <= 1e-4
+    keep = on_bound(sc, out["pos"]) == on_bound(sc, orc.pos)
+    assert (~keep).sum() <= 0.002 * sc.n
+    assert rel_norm(out["vel_half"][keep], orc.vel_half[keep]) <= 1e-4
+    assert rel_norm(out["vel"][keep], orc.vel[keep]) <= 1e-4
+    disp = np.max(np.abs(orc.pos - start["pos"]))
+    err = np.max(np.abs(out["pos"].astype(np.float64) - orc.pos))
+    assert err <= 4 * float(np.spacing(np.float32(np.max(np.abs(orc.pos))))) + 1e-5 * disp, (err, disp)
+
+
+@pytest.mark.parametrize("profile", ["ref", "config"])
+def test_trajectory_50_steps_pcisph(profile):
+    if profile == "ref":
+        sc = P.ref_scene()
+        tol = 1e-4
+    else:
+        sc = P.dam_break((24, 20, 16), 0.005, (0.5, 0.4, 0.3), 0.01, dt=1e-3, seed=11)
+        tol = 1e-3
+    pos = P.scene_positions(sc)
+    with P.Simulation(sc) as sim:
+        sim.upload(pos)
+        its_g = []
+        for _ in range(50):
+            sim.step(1)
+            its_g.append(sim.stats().iters)
+        out = sim.download()
+    orc = oracle.OracleSim(sc, pos)
+    its_o = [orc.step().iters for _ in range(50)]
+    travel = np.max(np.abs(orc.pos - pos))
+    err = np.max(np.abs(out["pos"] - orc.pos))
+    assert travel > 10 * sc.h * 0.01, travel        # the block has moved
+    assert err <= tol * travel + 4 * float(np.spacing(np.float32(1.0))), (err, travel)
+    assert rel_norm(out["vel"], orc.vel) <= 10 * tol
+    if profile == "ref":
+        assert its_g == its_o == [3] * 50
+    else:
+        assert sum(abs(a - b) for a, b in zip(its_g, its_o)) <= 5, (its_g, its_o)
