@@ -75,7 +75,10 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--impl", choices=["ours", "reference", "reference-cuda"], default="ours",
+                    help="reference: the reference's kernels as host code on every core; reference-cuda: its own "
+                         "CUDA path (kernels and PCISPH launcher compiled for this GPU), beside this build on the "
+                         "same physics")
     ap.add_argument("--scene", default="C2")
     ap.add_argument("--warm-start", choices=["zero", "previous", "learned"], default="learned",
                     help="zero: plain PCISPH (each step's corrector starts from p = 0)")
@@ -972,10 +975,77 @@ def run_c1(args):
     rep_.close()
 
 
+def run_reference_cuda(args):
+    """The reference's own CUDA path on this GPU: its kernel files and its
+    pci_SPH_update launcher compiled unchanged for sm_100a
+    (oracle/_ref/libpsbref_cuda.so), stepped through PCI_SPHSystem::update's
+    (or SPHSystem::update's, C0) call sequence, with the reference's physics
+    (three fixed corrections, FP64). Timed on the device over the reference's
+    own work (the guards that refuse out-of-bounds steps are not timed).
+    Beside it, this build on the same physics (reference profile, same scene
+    and start), device-timed the same way. Rank 0 only."""
+    from psb_project_b200.replicas import env_ranks
+    rank, world, _ = env_ranks()
+    if rank != 0:
+        return
+    import oracle
+    import torch
+    import psb_project_b200 as P
+    sc = P.config_scene(args.scene)
+    method = P.WCSPH if sc.method == P.WCSPH else P.PCISPH
+    sc_ref = P.dam_break(sc.blocks[0].nxyz, sc.blocks[0].spacing, sc.box_max, sc.h, method=method,
+                         profile=P.PROFILE_REF, dt=sc.dt, mass=sc.mass, seed=sc.blocks[0].seed)
+    name = "reference-cuda"
+    if not oracle.refcuda_available():
+        print(json.dumps({"impl": name, "unavailable": "oracle/_ref/libpsbref_cuda.so (the reference's CUDA files "
+                          "compiled for this GPU) is not present: build() compiles it where the reference tree "
+                          "exists"}))
+        return
+    pos = oracle.scene_positions(sc_ref).astype(np.float64)
+    ref = oracle.RefCudaSim(sc_ref, pos)
+    stepf = ref.pcisph_update if method == P.PCISPH else ref.wcsph_update
+    try:
+        for _ in range(args.warmup):
+            stepf()
+        t0 = time.perf_counter()
+        ms = [stepf() for _ in range(args.steps)]
+        wall = time.perf_counter() - t0
+    except RuntimeError as ex:
+        print(json.dumps({"impl": name, "unavailable": f"the reference's step was refused by the guard: {ex}"}))
+        return
+    value = sc_ref.n * args.steps / (sum(ms) / 1e3)
+    # this build on the same physics from the same start
+    stream = torch.cuda.current_stream()
+    with P.Simulation(sc_ref) as sim:
+        sim.set_stream(stream.cuda_stream)
+        sim.upload(pos.astype(np.float32))
+        sim.step(args.warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ours_ms = e0.elapsed_time(e1)
+    ours = sc_ref.n * args.steps / (ours_ms / 1e3)
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": name, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sum(ms) / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{sc.name}: reference physics ({'3 fixed corrections' if method == P.PCISPH else 'WCSPH'})",
+                   "particles": sc_ref.n, "dt": sc_ref.dt, "parallelism": "single GPU"},
+        "wall_ms_per_step": wall * 1e3 / args.steps,
+        "same_physics_this_build": {"value": ours, "ms_per_step": ours_ms / args.steps, "dtype": "f32",
+                                    "ratio_over_reference": ours / value},
+    }))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.impl == "reference-cuda":
+        run_reference_cuda(args)
     elif args.scene == "C3":
         run_batch(args)
     elif args.scene == "C4":

@@ -20,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libpsbref.so")
+REFCUDA_PATH = os.path.join(HERE, "_ref", "libpsbref_cuda.so")
 # The reference tree's src/ directory, when it is present: PSB_REFERENCE_SRC,
 # else a reference checkout beside this repository (<repo>/../reference/src).
 REF_SRC = os.environ.get("PSB_REFERENCE_SRC") or os.path.join(os.path.dirname(HERE), os.pardir, "reference", "src")
@@ -32,6 +33,7 @@ def build(with_reference: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
     if with_reference and os.path.isdir(REF_SRC):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_SRC={REF_SRC}"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "refcuda", f"REF_SRC={REF_SRC}"], check=True)
 
 
 class OrcParams(ctypes.Structure):
@@ -707,6 +709,106 @@ def ref_mc_grid(centre, l, w, d, cell, dims):
     c = np.asarray(centre, np.float64)
     ref_lib().ref_mc_grid(_ptr(c), l, w, d, np.float32(cell), nx, ny, nz, _ptr(out))
     return out
+
+
+def refcuda_available() -> bool:
+    return os.path.exists(REFCUDA_PATH)
+
+
+_refcuda = None
+
+
+def refcuda_lib():
+    """The reference's own CUDA path (oracle/_ref/libpsbref_cuda.so)."""
+    global _refcuda
+    if _refcuda is None:
+        if not refcuda_available():
+            raise FileNotFoundError(f"{REFCUDA_PATH} is not built (make -C oracle refcuda)")
+        L = ctypes.CDLL(REFCUDA_PATH)
+        P, F = ctypes.c_void_p, ctypes.c_float
+        L.rc_create.argtypes = [ctypes.c_int, P, F, P]
+        L.rc_create.restype = P
+        L.rc_destroy.argtypes = [P]
+        L.rc_set.argtypes = [P, ctypes.c_char_p, P]
+        L.rc_get.argtypes = [P, ctypes.c_char_p, P]
+        L.rc_neighbors.argtypes = [P, P]
+        L.rc_error.argtypes = [P]
+        L.rc_error.restype = ctypes.c_char_p
+        L.rc_pcisph_update.argtypes = [P, F, ctypes.c_double, F, P, P, ctypes.POINTER(F)]
+        L.rc_wcsph_update.argtypes = [P, F, P, F, F, P, P, ctypes.POINTER(F)]
+        _refcuda = L
+    return _refcuda
+
+
+class RefCudaSim:
+    """The reference's kernels and its PCISPH launcher compiled for the GPU,
+    on the reference's device layouts (AoS double), behind our guards: a
+    step that would write past the reference's arrays is refused."""
+
+    def __init__(self, scene, pos, vel=None, vel_half=None):
+        L = refcuda_lib()
+        n = pos.shape[0]
+        self.n, self.scene = n, scene
+        gmin = np.asarray(scene.grid_min, np.float32)
+        dims = np.asarray(scene.dims, np.int32)
+        self.h = L.rc_create(n, _ptr(gmin), scene.cell, _ptr(dims))
+        if not self.h:
+            raise RuntimeError("rc_create failed")
+        z3 = np.zeros((n, 3))
+        p = np.ascontiguousarray(pos, np.float64)
+        v = z3 if vel is None else np.ascontiguousarray(vel, np.float64)
+        vh = z3 if vel_half is None else np.ascontiguousarray(vel_half, np.float64)
+        for name, arr in (("pos", p), ("pos_old", p), ("r_pos", p), ("r_pos_old", p), ("vel", v), ("vel_old", v),
+                          ("vel_ap", vh), ("vel_av", vh), ("r_vel_ap", vh), ("r_vel_av", vh)):
+            self.set(name, arr)
+        ones = np.ones(n)
+        for name, val in (("mass", scene.mass), ("radius", scene.h), ("rho0", scene.rho0), ("k", scene.k),
+                          ("mu", scene.mu), ("sigma", scene.sigma), ("l", scene.l)):
+            self.set(name, ones * val)
+        self.box = (np.asarray(scene.box_min, np.float32), np.asarray(scene.box_max, np.float32))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            refcuda_lib().rc_destroy(self.h)
+            self.h = None
+
+    def set(self, name, arr):
+        arr = np.ascontiguousarray(arr, np.float64)
+        if refcuda_lib().rc_set(self.h, name.encode(), _ptr(arr)) != 0:
+            raise KeyError(name)
+
+    def get(self, name, width):
+        out = np.empty((self.n, width) if width > 1 else self.n, np.float64)
+        if refcuda_lib().rc_get(self.h, name.encode(), _ptr(out)) != 0:
+            raise KeyError(name)
+        return out
+
+    def neighbors(self):
+        c = np.empty(self.n, np.int32)
+        refcuda_lib().rc_neighbors(self.h, _ptr(c))
+        return c
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what}: {rc} ({refcuda_lib().rc_error(self.h).decode()})")
+
+    def pcisph_update(self, threshold=10.0) -> float:
+        """PCI_SPHSystem::update through the reference's pci_SPH_update; returns
+        the reference's device milliseconds of the step."""
+        ms = ctypes.c_float()
+        s = self.scene
+        self._check(refcuda_lib().rc_pcisph_update(self.h, s.dt, threshold, s.particle_radius, _ptr(self.box[0]),
+                                                   _ptr(self.box[1]), ctypes.byref(ms)), "rc_pcisph_update")
+        return ms.value
+
+    def wcsph_update(self) -> float:
+        ms = ctypes.c_float()
+        s = self.scene
+        g = np.asarray([0.0, -1.0, 0.0], np.float32)
+        self._check(refcuda_lib().rc_wcsph_update(self.h, s.dt, _ptr(g), np.float32(9.81), s.particle_radius,
+                                                  _ptr(self.box[0]), _ptr(self.box[1]), ctypes.byref(ms)),
+                    "rc_wcsph_update")
+        return ms.value
 
 
 class RefSim:
