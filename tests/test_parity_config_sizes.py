@@ -5,11 +5,15 @@
     against the FP64 oracle on the same FP32 state. Cell keys, the stable
     (cell, id) order and the neighbour counts are bit-exact; densities
     within 1e-5 element-wise; the non-pressure force density within 1e-5 of
-    its max; pressure and velocities within 1e-4 of their max (the floor of
-    an FP32 corrector: every correction adds delta (rho* - rho0), and the
-    FP32 rounding of the predicted positions x* alone moves rho* by ~1e-4
-    kg/m^3, ~1e-5 of the pressure scale per correction); positions within
-    4 float ulps plus 1e-5 of the displacement. The iteration count agrees
+    its max; pressure within 1e-4 of its max (the floor of an FP32
+    corrector: every correction adds delta (rho* - rho0), and the FP32
+    rounding of the predicted positions x* alone moves rho* by ~1e-4
+    kg/m^3, ~1e-5 of the pressure scale per correction); velocities within
+    1e-4 of their max plus the pressure error's own effect: an error of 1e-4
+    p_max that varies from particle to particle accelerates a particle by up
+    to 1e-4 p_max / (rho0 s) over dt (s the lattice spacing), which dominates
+    when the column starts at rest and the velocities are still small;
+    positions within 4 float ulps plus 1e-5 of the displacement. The iteration count agrees
     unless the deciding error sits within 2e-6 of eta.
   * 50-step PCISPH trajectories, reference and config profile, against the
     FP64 oracle from the same start: before the flow turns chaotic the
@@ -80,8 +84,11 @@ def test_c2_full_scene_step_matches_oracle():
     assert rel_norm(out["pressure"], orc.p) <= 1e-4
     keep = on_bound(sc, out["pos"]) == on_bound(sc, orc.pos)
     assert (~keep).sum() <= 0.002 * sc.n
-    assert rel_norm(out["vel_half"][keep], orc.vel_half[keep]) <= 1e-4
-    assert rel_norm(out["vel"][keep], orc.vel[keep]) <= 1e-4
+    dv = 1e-4 * np.max(np.abs(orc.p)) / (sc.rho0 * sc.blocks[0].spacing) * sc.dt
+    for key in ("vel_half", "vel"):
+        ref = getattr(orc, key)[keep]
+        err = np.max(np.abs(out[key][keep] - ref))
+        assert err <= 1e-4 * np.max(np.abs(ref)) + dv, (key, err, np.max(np.abs(ref)), dv)
     disp = np.max(np.abs(orc.pos - start["pos"]))
     err = np.max(np.abs(out["pos"].astype(np.float64) - orc.pos))
     assert err <= 4 * float(np.spacing(np.float32(np.max(np.abs(orc.pos))))) + 1e-5 * disp, (err, disp)
