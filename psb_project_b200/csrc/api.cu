@@ -352,6 +352,16 @@ Params derive(const psb_scene& s) {
     const float h2f = (float)(hl * hl);
     P.h2_lo = h2f * (1.f - 1e-5f);
     P.h2_hi = h2f * (1.f + 1e-5f);
+    {   // cell pruning bound: the window's top plus the error a face
+        // distance can carry, (d + e)^2 - d^2 <= 2 cell e + e^2 with e an
+        // ulp of the grid's largest coordinate (taken four times)
+        double big = 0.0;
+        for (int a = 0; a < 3; ++a)
+            big = std::max(big, std::max(std::fabs((double)s.grid_min[a]),
+                                         std::fabs((double)s.grid_min[a] + (double)s.dims[a] * (double)s.cell)));
+        const double e = 4.0 * (std::nextafter((float)big, INFINITY) - (float)big);
+        P.prune2 = std::nextafter((float)((double)P.h2_hi + 2.0 * (double)s.cell * e + e * e), INFINITY);
+    }
     P.h2 = h2f;
     P.inv_h = (float)(1.0 / h);
     P.inv_h2 = (float)(1.0 / (h * h));
@@ -471,6 +481,13 @@ int bits_for(size_t ncells) {
     return b;
 }
 
+// Whether the density pass at x is folded into the neighbour build: one
+// config-profile PCISPH scene with the per-thread cell walk (the row-tile
+// schedule, batches, the reference profile, WCSPH and DEM keep the two sweeps).
+bool fused_density(const psb_ctx* c, const Params& P) {
+    return !c->batch && P.pci && !P.ref && !P.dem && P.tune.nbr_schedule == 0;
+}
+
 // Grid, sort, reorder, neighbour lists, density at x. keep_p: leave the
 // carried pressure in place even where the scene starts every step from 0.
 int build(psb_ctx* c, bool keep_p = false, bool features = false) {
@@ -498,23 +515,32 @@ int build(psb_ctx* c, bool keep_p = false, bool features = false) {
     c->cr = nr;
     c->sorted = res;
     c->sorted_n = n;
-    timed(c, "build_nbr", [&] {
-        psb::launch_build_nbr(st, P, c->pos[c->cs], c->keys[res], c->cell_start, c->cell_end, c->nbr_count, c->nbr_list,
-                              c->flags);
-    });
+    // boundary lists first: the density at x reads them
     if (c->bnd_n > 0)
         timed(c, "build_bnd_nbr", [&] {
             psb::launch_build_bnd_nbr(st, P, c->pos[c->cs], c->keys[res], c->bnd_cs, c->bnd_ce, c->bnd_count,
                                       c->bnd_list, c->flags);
         });
-    if (!P.dem) {
-        const int zero_p = !keep_p && P.pci && (P.ref || c->sc.warm_start == PSB_WARM_ZERO);
-        // the learned warm start and its data collection take their inputs from this pass
-        float* feats = features ? c->feats : nullptr;
-        timed(c, "density_x", [&] {
-            psb::launch_density_x(st, P, c->pos[c->cs], c->vel[c->cs], c->nbr_count, c->nbr_list, c->rp[c->cr], c->rho_x,
-                                  zero_p, c->p_scale, feats, psb::mlp_inputs(c->mlp_arch));
+    const int zero_p = !keep_p && P.pci && (P.ref || c->sc.warm_start == PSB_WARM_ZERO);
+    // the learned warm start and its data collection take their inputs from the density pass at x
+    float* feats = features ? c->feats : nullptr;
+    const int nfeat = psb::mlp_inputs(c->mlp_arch);
+    if (fused_density(c, P)) {
+        timed(c, "build_nbr", [&] {
+            psb::launch_build_density(st, P, c->pos[c->cs], c->vel[c->cs], c->keys[res], c->cell_start, c->cell_end,
+                                      c->nbr_count, c->nbr_list, c->flags, c->rp[c->cr], c->rho_x, zero_p, c->p_scale,
+                                      feats, nfeat);
         });
+    } else {
+        timed(c, "build_nbr", [&] {
+            psb::launch_build_nbr(st, P, c->pos[c->cs], c->keys[res], c->cell_start, c->cell_end, c->nbr_count,
+                                  c->nbr_list, c->flags);
+        });
+        if (!P.dem)
+            timed(c, "density_x", [&] {
+                psb::launch_density_x(st, P, c->pos[c->cs], c->vel[c->cs], c->nbr_count, c->nbr_list, c->rp[c->cr],
+                                      c->rho_x, zero_p, c->p_scale, feats, nfeat);
+            });
     }
     c->built = true;
     return cuda_check(c, cudaGetLastError(), "launch");
@@ -2163,9 +2189,24 @@ int psb_autotune(psb_ctx* c, int32_t trials, psb_tune* out) {
             default: best.xsph_block = best_b; break;
         }
     };
+    // The neighbour build: where the density pass at x folds into the
+    // per-thread build, schedule 0 is that fused kernel and schedule 1 the
+    // row-tile build followed by the density pass (at its default block),
+    // so that the two are timed for the same work.
     tune_one(0, [&](const Params& Q) {
+        if (fused_density(c, Q)) {
+            psb::launch_build_density(st, Q, c->pos[s], c->vel[s], c->keys[c->sorted], c->cell_start, c->cell_end,
+                                      c->nbr_count, c->nbr_list, c->flags, c->rp[r], c->rho_x, 0, c->p_scale,
+                                      feats ? c->feats : nullptr, psb::mlp_inputs(c->mlp_arch));
+            return;
+        }
         psb::launch_build_nbr(st, Q, c->pos[s], c->keys[c->sorted], c->cell_start, c->cell_end, c->nbr_count,
                               c->nbr_list, c->flags);
+        Params D = Q;
+        D.tune.nbr_schedule = 0;
+        if (sph && fused_density(c, D))
+            psb::launch_density_x(st, Q, c->pos[s], c->vel[s], c->nbr_count, c->nbr_list, c->rp[r], c->rho_x, 0,
+                                  c->p_scale, feats ? c->feats : nullptr, psb::mlp_inputs(c->mlp_arch));
     });
     if (sph)
         tune_one(1, [&](const Params& Q) {

@@ -191,34 +191,6 @@ __global__ void k_reorder(int n, const uint32_t* __restrict__ keys, const uint32
     if (t == n - 1 || keys[t + 1] != k) cell_end[k] = (uint32_t)t + 1u;
 }
 
-// The reference's test, sqrt((dx*dx + dy*dy) + dz*dz) <= h with every
-// operation rounded separately in FP64 (double3.h:15-47). The correctly
-// rounded square root is monotone, so the test is d2 <= h2_exact, the
-// largest double whose root rounds to at most h (found on the host).
-__device__ __forceinline__ bool exact_neighbor(float4 a, float4 b, double h2_exact) {
-    const double dx = __dsub_rn((double)a.x, (double)b.x);
-    const double dy = __dsub_rn((double)a.y, (double)b.y);
-    const double dz = __dsub_rn((double)a.z, (double)b.z);
-    const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-    return d2 <= h2_exact;
-}
-
-// flags[1]: max count, flags[2..3]: total pairs (64-bit); every lane of the
-// warp calls it.
-__device__ __forceinline__ void nbr_flags(int cnt, int* __restrict__ flags) {
-    int m = cnt;
-    unsigned long long tot = (unsigned long long)cnt;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-        tot += __shfl_xor_sync(0xffffffffu, tot, o);
-    }
-    if ((threadIdx.x & 31) == 0 && tot > 0) {
-        atomicMax(&flags[1], m);
-        atomicAdd((unsigned long long*)&flags[2], tot);
-    }
-}
-
 // Per-thread schedule: one thread per sorted particle. The three cells of a
 // grid row are adjacent in sorted order, so each of the nine rows is one
 // contiguous slot range; candidates are visited in increasing slot order and
@@ -235,45 +207,15 @@ __global__ void __launch_bounds__(BS) k_build_nbr(Params P, const float4* __rest
     const int n = P.n;
     int cnt = 0;
     if (valid) {
-        const Grid g = BATCH ? P.scenes[P.slot_scene[t]].g : P.g;
-        const uint32_t base = BATCH ? P.scenes[P.slot_scene[t]].cell_base : 0u;
-        const int nx = g.nx, ny = g.ny, nz = g.nz;
-        const float4 pi = pos[t];
-        const uint32_t key = keys[t] - base;
-        const int ci = (int)(key % (uint32_t)nx);
-        const int cj = (int)((key / (uint32_t)nx) % (uint32_t)ny);
-        const int ck = (int)(key / ((uint32_t)nx * (uint32_t)ny));
-        const int a0 = max(ci - 1, 0), a1 = min(ci + 1, nx - 1);
         int* wq = list + nbr_index(0, n, t);
         const size_t qstride = (size_t)4 * (size_t)n;
-        for (int k = max(ck - 1, 0); k <= min(ck + 1, nz - 1); ++k) {
-            for (int j = max(cj - 1, 0); j <= min(cj + 1, ny - 1); ++j) {
-                const uint32_t row = base + (uint32_t)j * (uint32_t)nx + (uint32_t)k * (uint32_t)nx * (uint32_t)ny;
-                uint32_t lo = kEmpty, hi = 0;
-                for (int a = a0; a <= a1; ++a) {
-                    const uint32_t s = cell_start[row + a];
-                    if (s != kEmpty) {
-                        if (lo == kEmpty) lo = s;
-                        hi = cell_end[row + a];
-                    }
-                }
-                if (lo == kEmpty) continue;
-                for (uint32_t q = lo; q < hi; ++q) {
-                    const float4 pj = pos[q];
-                    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                    const float d2 = dx * dx + dy * dy + dz * dz;
-                    // beyond the FP32 window: out with one compare; below it: in;
-                    // inside it: the reference's FP64 test
-                    if (d2 <= P.h2_hi && (d2 < P.h2_lo || exact_neighbor(pi, pj, P.h2_exact))) {
-                        // one 4-byte store per entry (buffering four in registers measured
-                        // slower); wq is entry cnt's quad, nbr_index(cnt, n, t) - (cnt & 3)
-                        if (cnt < P.cap) wq[cnt & 3] = (int)q;
-                        ++cnt;
-                        if ((cnt & 3) == 0 && cnt < P.cap) wq += qstride;
-                    }
-                }
-            }
-        }
+        walk_neighbours<BATCH>(P, t, pos[t], pos, keys, cell_start, cell_end, [&](uint32_t q, float4) {
+            // one 4-byte store per entry (buffering four in registers measured
+            // slower); wq is entry cnt's quad, nbr_index(cnt, n, t) - (cnt & 3)
+            if (cnt < P.cap) wq[cnt & 3] = (int)q;
+            ++cnt;
+            if ((cnt & 3) == 0 && cnt < P.cap) wq += qstride;
+        });
         counts[t] = cnt;
         if (cnt > P.cap) atomicOr(&flags[0], 1);
     }
@@ -357,7 +299,7 @@ __global__ void __launch_bounds__(BS) k_build_nbr_tile(Params P, const float4* _
                         for (uint32_t c = c0; c < c1; ++c) {
                             const float4 pj = tile[c];
                             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                            const float d2 = dx * dx + dy * dy + dz * dz;
+                            const float d2 = dist2(dx, dy, dz);
                             bool acc;
                             if (d2 < P.h2_lo) acc = true;
                             else if (d2 > P.h2_hi) acc = false;

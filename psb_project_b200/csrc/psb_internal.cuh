@@ -59,6 +59,7 @@ struct Params {
                         // (reference: h; config: (1 + skin) h)
     double h2_exact;    // the largest double x with sqrt_rn(x) <= h: the same test as d.d <= h2_exact
     float h2_lo, h2_hi; // FP32 d^2 outside [h2_lo, h2_hi] is decided without the FP64 test
+    float prune2;       // a cell whose FP32 face-distance bound (squared) exceeds this holds no neighbour
     float h2, inv_h, inv_h2;
     float k_rho;        // 315 m / (64 pi h^3):           rho = k_rho * sum (1-q)^3
     float k_grad;       // 45 m / (pi h^4):               a_p = k_grad * sum (pV_i+pV_j)(1-u)^2 x^
@@ -154,6 +155,100 @@ __device__ __forceinline__ void for_each_nbr(const int* __restrict__ list, int n
     }
 }
 
+// |d|^2 of a pair in FP32 with the multiply-adds written out, so that every
+// kernel that tests or weights the same pair rounds it the same way.
+__device__ __forceinline__ float dist2(float dx, float dy, float dz) {
+    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
+
+// The reference's test, sqrt((dx*dx + dy*dy) + dz*dz) <= h with every
+// operation rounded separately in FP64 (double3.h:15-47). The correctly
+// rounded square root is monotone, so the test is d2 <= h2_exact, the
+// largest double whose root rounds to at most h (found on the host).
+__device__ __forceinline__ bool exact_neighbor(float4 a, float4 b, double h2_exact) {
+    const double dx = __dsub_rn((double)a.x, (double)b.x);
+    const double dy = __dsub_rn((double)a.y, (double)b.y);
+    const double dz = __dsub_rn((double)a.z, (double)b.z);
+    const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    return d2 <= h2_exact;
+}
+
+// flags[1]: max count, flags[2..3]: total pairs (64-bit); every lane of the
+// warp calls it.
+__device__ __forceinline__ void nbr_flags(int cnt, int* __restrict__ flags) {
+    int m = cnt;
+    unsigned long long tot = (unsigned long long)cnt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    }
+    if ((threadIdx.x & 31) == 0 && tot > 0) {
+        atomicMax(&flags[1], m);
+        atomicAdd((unsigned long long*)&flags[2], tot);
+    }
+}
+
+// The 27-cell walk of sorted particle t (one thread per particle): the three
+// cells of a grid row are adjacent in sorted order, so each of the nine rows
+// is one contiguous slot range, and accept(slot, position) runs for every
+// candidate within the list cut-off in increasing slot order, row by row --
+// the list order. In a batch the walk stays inside the particle's scene's
+// grid. Candidates beyond the FP32 window are out with one compare, those
+// below it in; inside it the reference's FP64 test decides.
+// Cells that cannot hold a neighbour are not walked: the distance from the
+// particle to the faces of its own cell bounds, from below, its distance to
+// everything in the next cell that way (particles clamped into the border
+// cells lie beyond them), so a row, or the outer cell of a row, whose bound
+// exceeds the list cut-off by the FP32 window's margin is skipped. That
+// leaves about three quarters of the 27 cells, and the list is unchanged.
+template <bool BATCH, class F>
+__device__ __forceinline__ void walk_neighbours(const Params& P, int t, float4 pi, const float4* __restrict__ pos,
+                                                const uint32_t* __restrict__ keys,
+                                                const uint32_t* __restrict__ cell_start,
+                                                const uint32_t* __restrict__ cell_end, F&& accept) {
+    const Grid g = BATCH ? P.scenes[P.slot_scene[t]].g : P.g;
+    const uint32_t base = BATCH ? P.scenes[P.slot_scene[t]].cell_base : 0u;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const uint32_t key = keys[t] - base;
+    const int ci = (int)(key % (uint32_t)nx);
+    const int cj = (int)((key / (uint32_t)nx) % (uint32_t)ny);
+    const int ck = (int)(key / ((uint32_t)nx * (uint32_t)ny));
+    // distances to the own cell's lower and upper faces on each axis, FP32:
+    // a face fma(i, cell, corner) is off by at most half an ulp of the largest
+    // coordinate, which P.prune2 (the cut-off plus 4 cell ulp) absorbs
+    const float lx = fmaxf(pi.x - fmaf((float)ci, g.cell, g.gx), 0.f), hx = fmaxf(fmaf((float)(ci + 1), g.cell, g.gx) - pi.x, 0.f);
+    const float ly = fmaxf(pi.y - fmaf((float)cj, g.cell, g.gy), 0.f), hy = fmaxf(fmaf((float)(cj + 1), g.cell, g.gy) - pi.y, 0.f);
+    const float lz = fmaxf(pi.z - fmaf((float)ck, g.cell, g.gz), 0.f), hz = fmaxf(fmaf((float)(ck + 1), g.cell, g.gz) - pi.z, 0.f);
+    const float bound = P.prune2;
+    const bool xlo = ci > 0 && lx * lx <= bound, xhi = ci + 1 < nx && hx * hx <= bound;
+    for (int k = max(ck - 1, 0); k <= min(ck + 1, nz - 1); ++k) {
+        const float dz = k < ck ? lz : (k > ck ? hz : 0.f);
+        for (int j = max(cj - 1, 0); j <= min(cj + 1, ny - 1); ++j) {
+            const float dy = j < cj ? ly : (j > cj ? hy : 0.f);
+            const float dyz = dy * dy + dz * dz;
+            if (dyz > bound) continue;
+            const int a0 = xlo && lx * lx + dyz <= bound ? ci - 1 : ci;
+            const int a1 = xhi && hx * hx + dyz <= bound ? ci + 1 : ci;
+            const uint32_t row = base + (uint32_t)j * (uint32_t)nx + (uint32_t)k * (uint32_t)nx * (uint32_t)ny;
+            uint32_t lo = kEmpty, hi = 0;
+            for (int a = a0; a <= a1; ++a) {
+                const uint32_t s = cell_start[row + a];
+                if (s != kEmpty) {
+                    if (lo == kEmpty) lo = s;
+                    hi = cell_end[row + a];
+                }
+            }
+            if (lo == kEmpty) continue;
+            for (uint32_t q = lo; q < hi; ++q) {
+                const float4 pj = pos[q];
+                const float d2 = dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z);
+                if (d2 <= P.h2_hi && (d2 < P.h2_lo || exact_neighbor(pi, pj, P.h2_exact))) accept(q, pj);
+            }
+        }
+    }
+}
+
 // ---- launchers (grid.cu) -------------------------------------------------
 void launch_reset_cells(cudaStream_t st, int n, const uint32_t* sorted_keys, uint32_t* cell_start);
 void launch_cell_keys(cudaStream_t st, const Params& P, const float4* pos, const int* ids, uint32_t* keys_by_id,
@@ -167,6 +262,12 @@ void launch_reorder(cudaStream_t st, int n, const uint32_t* keys, const uint32_t
                     float4* vap2, float2* rp2, int* ids2, uint32_t* cell_start, uint32_t* cell_end);
 void launch_build_nbr(cudaStream_t st, const Params& P, const float4* pos, const uint32_t* keys,
                       const uint32_t* cell_start, const uint32_t* cell_end, int* counts, int* list, int* flags);
+// (sph.cu) The per-thread neighbour build of one config-profile scene with the
+// density pass at x folded in: lists, counts and flags as launch_build_nbr,
+// then density, pressure and features as launch_density_x.
+void launch_build_density(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const uint32_t* keys,
+                          const uint32_t* cell_start, const uint32_t* cell_end, int* counts, int* list, int* flags,
+                          float2* rp, float* rho_x, int zero_p, float p_scale, float* feats, int nfeat);
 
 // ---- launchers (sph.cu) ---------------------------------------------------
 // feats != nullptr: also the warm start's inputs f0 .. f(nfeat - 1), nfeat 6 or 7.

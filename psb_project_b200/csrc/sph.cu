@@ -172,7 +172,7 @@ __device__ __forceinline__ void ghost_density_pair(const Params& P, const F_& F,
         float3 r;
         float dp;
         if (!ghost_delta(P, F, w, mask, xi, xj, r, dp)) continue;
-        const float q = (r.x * r.x + r.y * r.y + r.z * r.z) * P.inv_h2;
+        const float q = dist2(r.x, r.y, r.z) * P.inv_h2;
         if (q >= 1.f) continue;
         const float wq = 1.f - q;
         acc.add(wq * wq * wq);
@@ -190,7 +190,7 @@ __device__ __forceinline__ void ghost_pressure_pair(const Params& P, const F_& F
         float3 r;
         float dp;
         if (!ghost_delta(P, F, w, mask, xi, xj, r, dp)) continue;
-        const float r2 = r.x * r.x + r.y * r.y + r.z * r.z;
+        const float r2 = dist2(r.x, r.y, r.z);
         if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) continue;
         const float rinv = rsqrtf(r2);
         const float om = 1.f - r2 * rinv * P.inv_h;
@@ -235,7 +235,7 @@ __device__ __forceinline__ void boundary_density(const Params& P, int t, float4 
     for_each_nbr(P.bnd_list, P.n, t, cnt, [&](const int b) {
         const float4 xb = P.bnd[b];
         const float dx = xi.x - xb.x, dy = xi.y - xb.y, dz = xi.z - xb.z;
-        const float q = (dx * dx + dy * dy + dz * dz) * P.inv_h2;
+        const float q = dist2(dx, dy, dz) * P.inv_h2;
         if (q >= 1.f) return;
         const float w = 1.f - q;
         acc.add(xb.w * (w * w * w));
@@ -248,7 +248,7 @@ __device__ __forceinline__ void boundary_pressure(const Params& P, int t, float4
     for_each_nbr(P.bnd_list, P.n, t, cnt, [&](const int b) {
         const float4 xb = P.bnd[b];
         const float dx = xi.x - xb.x, dy = xi.y - xb.y, dz = xi.z - xb.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float r2 = dist2(dx, dy, dz);
         if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) return;
         const float rinv = rsqrtf(r2);
         const float om = 1.f - r2 * rinv * P.inv_h;
@@ -305,32 +305,33 @@ __device__ __forceinline__ void box_project(const Params& P, int t, float3& x, f
 //   f5 k_grad |sum (1-u)^2 x^| h / rho0 (density-gradient magnitude)
 //   f6 sum W_ij p_j / sum W_ij / p_scale over the list, self included: the
 //      carried pressure smoothed with the poly6 weights
-template <bool REF, int NF, bool BATCH, int BS>
-__global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __restrict__ pos,
-                                                      const float4* __restrict__ vel, const int* __restrict__ counts,
-                                                      const int* __restrict__ list, float2* __restrict__ rp,
-                                                      float* __restrict__ rho_x, int zero_p, float p_scale,
-                                                      float* __restrict__ feats) {
-    constexpr bool FEAT = NF > 0, SMOOTH_P = NF > 6;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= P.n) return;
-    const float4 xi = pos[t];
-    const int cnt = min(counts[t], P.cap);
+// The sums of the density pass at x for one particle, pair by pair in list
+// order; shared by the density sweep and by the neighbour build that
+// computes the density as it accepts each neighbour, so that both give the
+// same bits.
+template <bool REF, int NF>
+struct DensityX {
+    static constexpr bool FEAT = NF > 0, SMOOTH_P = NF > 6;
     Kahan acc;
     float div = 0.f, wp = 0.f, ws = 0.f;
     float3 gr = make_float3(0.f, 0.f, 0.f);
     float4 vi = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (FEAT) vi = vel[t];
-    for_each_nbr(list, P.n, t, cnt, [&](const int j) {
-        const float4 xj = pos[j];
+
+    __device__ __forceinline__ void begin(const float4* __restrict__ vel, int t) {
+        if (FEAT) vi = vel[t];
+    }
+    // neighbour j at xj (r2 = dist2 of xi - xj); rp[j].y is the carried
+    // pressure, which the pass writes back unchanged
+    __device__ __forceinline__ void pair(const Params& P, float4 xi, float4 xj, int j, const float4* __restrict__ vel,
+                                         const float2* __restrict__ rp) {
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float r2 = dist2(dx, dy, dz);
         const float q = r2 * P.inv_h2;
         if (!REF && q >= 1.f) return;
         const float w = 1.f - q;
         const float w3 = w * w * w;
         acc.add(w3);
-        if (SMOOTH_P) {     // carried pressures: this pass writes rp[j].y back unchanged
+        if (SMOOTH_P) {
             wp += w3 * rp[j].y;
             ws += w3;
         }
@@ -342,41 +343,106 @@ __global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __rest
             gr.x += s * dx; gr.y += s * dy; gr.z += s * dz;
             div += s * ((vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz);
         }
-    });
-    if (!REF) {
-        ghost_density<BATCH>(P, t, xi, pos, list, cnt, acc);
-        if (!BATCH) boundary_density(P, t, xi, acc);
     }
-    const float drho = density_deviation(P, acc);
-    const float rho = P.rho0 + drho;
-    float p;
-    if (P.pci) {
-        p = zero_p ? 0.f : rp[t].y;
-    } else if (REF) {
-        p = P.eos_k * drho;
-    } else {
-        const float d = drho / P.rho0;
-        const float x = 1.f + d;
-        const float s = 1.f + x * (1.f + x * (1.f + x * (1.f + x * (1.f + x * (1.f + x)))));
-        p = P.eos_k * d * s;
+    // wall ghosts and boundary particles (config), then density, pressure
+    // (EOS, or the carried / zeroed PCISPH pressure) and the features
+    template <bool BATCH>
+    __device__ __forceinline__ void finish(const Params& P, int t, float4 xi, const float4* __restrict__ pos,
+                                           const int* __restrict__ list, int cnt, int count, float2* __restrict__ rp,
+                                           float* __restrict__ rho_x, int zero_p, float p_scale,
+                                           float* __restrict__ feats) {
+        if (!REF) {
+            ghost_density<BATCH>(P, t, xi, pos, list, cnt, acc);
+            if (!BATCH) boundary_density(P, t, xi, acc);
+        }
+        const float drho = density_deviation(P, acc);
+        const float rho = P.rho0 + drho;
+        float p;
+        if (P.pci) {
+            p = zero_p ? 0.f : rp[t].y;
+        } else if (REF) {
+            p = P.eos_k * drho;
+        } else {
+            const float d = drho / P.rho0;
+            const float x = 1.f + d;
+            const float s = 1.f + x * (1.f + x * (1.f + x * (1.f + x * (1.f + x * (1.f + x)))));
+            p = P.eos_k * d * s;
+        }
+        if (FEAT) {
+            div *= -P.k_grad / P.rho0;
+            const auto F = faces_of<BATCH>(P, t);
+            float dwall = P.hf;
+            dwall = fminf(dwall, fminf(xi.x - F.x0(), F.x1() - xi.x));
+            dwall = fminf(dwall, fminf(xi.y - F.y0(), F.y1() - xi.y));
+            dwall = fminf(dwall, fminf(xi.z - F.z0(), F.z1() - xi.z));
+            float4* f = reinterpret_cast<float4*>(feats + (size_t)t * 8);     // two 16-byte stores
+            f[0] = make_float4((float)count * (1.f / 32.f), (rho - P.dt * rho * div - P.rho0) / P.rho0 * 100.f,
+                               div * P.dt * 100.f,
+                               rp[t].y / p_scale);     // the carried pressure, before this pass replaces it
+            f[1] = make_float4(fmaxf(dwall, 0.f) * P.inv_h,
+                               P.k_grad * sqrtf(gr.x * gr.x + gr.y * gr.y + gr.z * gr.z) * P.hf / P.rho0,
+                               SMOOTH_P && ws > 0.f ? wp / ws / p_scale : 0.f, 0.f);
+        }
+        rp[t] = make_float2(rho, p);
+        rho_x[t] = rho;
     }
-    if (FEAT) {
-        div *= -P.k_grad / P.rho0;
-        const auto F = faces_of<BATCH>(P, t);
-        float dwall = P.hf;
-        dwall = fminf(dwall, fminf(xi.x - F.x0(), F.x1() - xi.x));
-        dwall = fminf(dwall, fminf(xi.y - F.y0(), F.y1() - xi.y));
-        dwall = fminf(dwall, fminf(xi.z - F.z0(), F.z1() - xi.z));
-        float4* f = reinterpret_cast<float4*>(feats + (size_t)t * 8);     // two 16-byte stores
-        f[0] = make_float4((float)counts[t] * (1.f / 32.f), (rho - P.dt * rho * div - P.rho0) / P.rho0 * 100.f,
-                           div * P.dt * 100.f,
-                           rp[t].y / p_scale);     // the carried pressure, before this pass replaces it
-        f[1] = make_float4(fmaxf(dwall, 0.f) * P.inv_h,
-                           P.k_grad * sqrtf(gr.x * gr.x + gr.y * gr.y + gr.z * gr.z) * P.hf / P.rho0,
-                           SMOOTH_P && ws > 0.f ? wp / ws / p_scale : 0.f, 0.f);
+};
+
+template <bool REF, int NF, bool BATCH, int BS>
+__global__ void __launch_bounds__(BS) k_density_x(Params P, const float4* __restrict__ pos,
+                                                      const float4* __restrict__ vel, const int* __restrict__ counts,
+                                                      const int* __restrict__ list, float2* __restrict__ rp,
+                                                      float* __restrict__ rho_x, int zero_p, float p_scale,
+                                                      float* __restrict__ feats) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const float4 xi = pos[t];
+    const int count = counts[t];
+    const int cnt = min(count, P.cap);
+    DensityX<REF, NF> D;
+    D.begin(vel, t);
+    for_each_nbr(list, P.n, t, cnt, [&](const int j) { D.pair(P, xi, pos[j], j, vel, rp); });
+    D.template finish<BATCH>(P, t, xi, pos, list, cnt, count, rp, rho_x, zero_p, p_scale, feats);
+}
+
+// The neighbour build of one scene (config profile) with the density pass
+// at x folded in: the 27-cell walk of each particle (walk_neighbours) writes
+// its list and, for every neighbour it accepts, adds that pair's density and
+// feature terms -- the same terms in the same order as k_density_x over the
+// finished list -- so the step saves one sweep over the lists. The ghost
+// and boundary terms then walk the list this thread has just written.
+template <int NF, int BS>
+__global__ void __launch_bounds__(BS) k_build_density(Params P, const float4* __restrict__ pos,
+                                                          const float4* __restrict__ vel,
+                                                          const uint32_t* __restrict__ keys,
+                                                          const uint32_t* __restrict__ cell_start,
+                                                          const uint32_t* __restrict__ cell_end,
+                                                          int* __restrict__ counts, int* __restrict__ list,
+                                                          int* __restrict__ flags, float2* __restrict__ rp,
+                                                          float* __restrict__ rho_x, int zero_p, float p_scale,
+                                                          float* __restrict__ feats) {
+    const int t = blockIdx.x * BS + threadIdx.x;
+    const bool valid = t < P.n;     // every lane stays for the warp reductions below
+    int cnt = 0;
+    if (valid) {
+        const float4 pi = pos[t];
+        DensityX<false, NF> D;
+        D.begin(vel, t);
+        int* wq = list + nbr_index(0, P.n, t);
+        const size_t qstride = (size_t)4 * (size_t)P.n;
+        walk_neighbours<false>(P, t, pi, pos, keys, cell_start, cell_end, [&](uint32_t q, float4 pj) {
+            if (cnt < P.cap) {
+                wq[cnt & 3] = (int)q;
+                D.pair(P, pi, pj, (int)q, vel, rp);
+            }
+            ++cnt;
+            if ((cnt & 3) == 0 && cnt < P.cap) wq += qstride;
+        });
+        counts[t] = cnt;
+        if (cnt > P.cap) atomicOr(&flags[0], 1);
+        D.template finish<false>(P, t, pi, pos, list, min(cnt, P.cap), cnt, rp, rho_x, zero_p, p_scale, feats);
     }
-    rp[t] = make_float2(rho, p);
-    rho_x[t] = rho;
+    nbr_flags(cnt, flags);
 }
 
 // Viscosity (+ reference surface tension) and, when with_pressure, the
@@ -403,7 +469,7 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
     for_each_nbr(list, P.n, t, cnt, [&](const int j) {
         const float4 xj = pos[j];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float r2 = dist2(dx, dy, dz);
         if (!(r2 > 0.f)) return;
         const float q = r2 * P.inv_h2;
         if (!REF && q >= 1.f) return;
@@ -526,7 +592,7 @@ __global__ void __launch_bounds__(BS) k_pci_density(Params P, const float4* __re
         for_each_nbr(list, P.n, t, cnt, [&](const int j) {
             const float4 xj = xs[j];
             const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-            const float r2 = dx * dx + dy * dy + dz * dz;
+            const float r2 = dist2(dx, dy, dz);
             const float q = r2 * P.inv_h2;
             if (!REF && q >= 1.f) return;
             const float w = 1.f - q;
@@ -609,7 +675,7 @@ __global__ void __launch_bounds__(BS) k_pci_force_predict(Params P, const float4
     for_each_nbr(list, P.n, t, cnt, [&](const int j) {
         const float4 xj = geo[j];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float r2 = dist2(dx, dy, dz);
         if (!(r2 > 0.f)) return;
         if (!REF && r2 * P.inv_h2 >= 1.f) return;
         const float2 rj = rpc[j];
@@ -675,7 +741,7 @@ __global__ void __launch_bounds__(BS) k_xsph(Params P, const float4* __restrict_
     for_each_nbr(list, P.n, t, cnt, [&](const int j) {
         const float4 xj = xs[j];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float q = (dx * dx + dy * dy + dz * dz) * P.inv_h2;
+        const float q = dist2(dx, dy, dz) * P.inv_h2;
         if (q >= 1.f) return;
         const float4 vj = vs[j];
         const float w = (1.f - q) * (1.f - q) * (1.f - q);
@@ -712,6 +778,23 @@ void launch_density_x(cudaStream_t st, const Params& P, const float4* pos, const
         } else if (nf == 7) go(k_density_x<false, 7, false, BS>);
         else if (nf == 6) go(k_density_x<false, 6, false, BS>);
         else go(k_density_x<false, 0, false, BS>);
+    });
+}
+
+void launch_build_density(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const uint32_t* keys,
+                          const uint32_t* cell_start, const uint32_t* cell_end, int* counts, int* list, int* flags,
+                          float2* rp, float* rho_x, int zero_p, float p_scale, float* feats, int nfeat) {
+    if (P.n <= 0) return;
+    with_block(P.tune.nbr_block, [&](auto B) {
+        constexpr int BS = decltype(B)::value;
+        auto go = [&](auto kernel) {
+            kernel<<<blocks_of<BS>(P.n), BS, 0, st>>>(P, pos, vel, keys, cell_start, cell_end, counts, list, flags, rp,
+                                                      rho_x, zero_p, p_scale, feats);
+        };
+        const int nf = feats ? (nfeat > 6 ? 7 : 6) : 0;
+        if (nf == 7) go(k_build_density<7, BS>);
+        else if (nf == 6) go(k_build_density<6, BS>);
+        else go(k_build_density<0, BS>);
     });
 }
 
