@@ -70,6 +70,20 @@ def _kernels_per_group(name: str, sort_passes: int) -> int:
     return 3 * sort_passes if name == "radix_sort" else 1
 
 
+CORRECTOR_KERNELS = ("batch_begin", "pci_density", "batch_decide", "pci_force_predict")
+
+
+def corrector_launches(prof: dict, steps: int, sort_passes: int, persistent: bool) -> int:
+    """Kernel launches of `steps` steps from a per-kernel profile taken with
+    the launches corrector; the persistent corrector replaces its four kinds
+    of kernel with one launch per step."""
+    total = sum(l * _kernels_per_group(k, sort_passes) for k, (l, _) in prof.items())
+    if persistent:
+        total -= sum(prof[k][0] for k in CORRECTOR_KERNELS if k in prof)
+        total += steps
+    return int(total)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -96,6 +110,9 @@ def parse():
     ap.add_argument("--train-lr", type=float, default=3e-3, help="peak learning rate of the cosine schedule")
     ap.add_argument("--xsph", type=float, default=None, help="override the scene's XSPH velocity smoothing factor")
     ap.add_argument("--no-graph", action="store_true", help="launch kernel by kernel instead of CUDA graphs")
+    ap.add_argument("--corrector", choices=["launches", "persistent", "both"], default="both",
+                    help="the corrector loop: three kernels per correction, one cooperative launch per step, or "
+                         "both timed and the faster one reported (config-profile PCISPH and C3)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch configuration)")
     ap.add_argument("--tune-cache", default=None,
                     help="JSON cache of tuned launch configurations: a bucket found there is not tuned again; "
@@ -323,6 +340,8 @@ def run_ours(args):
     arch = archs[args.mlp]
     weights = {}      # trained networks by name
 
+    corr_mode = None  # the faster corrector, given to every context created after it is known
+
     def make(mode, net=None, graph=True):
         s_ = P.Simulation(base.replace(warm_start=mode))
         s_.set_stream(stream.cuda_stream)
@@ -333,6 +352,8 @@ def run_ours(args):
             s_.tune_set(**{k: tune[k] for k in TUNE_KEYS})
         if graph and pcisph_cfg and not args.no_graph:
             s_.set_graph(True)
+        if pcisph_cfg and corr_mode is not None:
+            s_.set_corrector(corr_mode)
         return s_
 
     # Set-up (untimed): the dam at rest with its initial pressure, then plain
@@ -405,11 +426,29 @@ def run_ours(args):
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    # ---- device-resident timing -------------------------------------------------
-    ms_max, iters, _ = device_pass(sim)
+    # ---- device-resident timing, each corrector mode (same steps, same snapshot) ----
+    modes_c = {"launches": P.CORRECTOR_LAUNCHES, "persistent": P.CORRECTOR_PERSISTENT}
+    chosen = [args.corrector] if args.corrector != "both" or not pcisph_cfg else ["launches", "persistent"]
+    if not pcisph_cfg:
+        chosen = ["launches"]
+    corr = {}
+    for name in chosen:
+        if pcisph_cfg:
+            sim.set_corrector(modes_c[name])
+        ms_c, it_c, _ = device_pass(sim)
+        corr[name] = {"ms_per_step": ms_c / args.steps, "value": world * n * args.steps / (ms_c / 1e3),
+                      "iters_mean": float(np.mean(it_c)), "ms": ms_c, "iters": it_c}
+    best = min(corr, key=lambda k: corr[k]["ms"])
+    ms_max, iters = corr[best]["ms"], corr[best]["iters"]
     value = world * n * args.steps / (ms_max / 1e3)
     # ---- per-kernel timing: the same K steps with CUDA events around every launch ----
+    # (the launches corrector: its passes are separate kernels)
+    if pcisph_cfg:
+        sim.set_corrector(P.CORRECTOR_LAUNCHES)
     _, _, prof = device_pass(sim, profile=True)
+    if pcisph_cfg:
+        corr_mode = modes_c[best]
+        sim.set_corrector(corr_mode)
     # ---- end to end through the C ABI with host buffers ------------------------------
     pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
     h = {"pos": pin((n, 3)), "vel": pin((n, 3)), "vel_half": pin((n, 3)), "density": pin((n,)), "pressure": pin((n,))}
@@ -483,7 +522,7 @@ def run_ours(args):
     sim.close()
 
     passes = (max(1, int(np.ceil(np.log2(np.prod(sc.dims))))) + 7) // 8
-    launches = int(sum(l * _kernels_per_group(k, passes) for k, (l, _) in prof.items()))
+    launches = corrector_launches(prof, args.steps, passes, best == "persistent")
     tot_ms = sum(v[1] for v in prof.values())
     dom = max((k for k in prof if k in ALG_BYTES), key=lambda k: prof[k][1])
     l_dom, ms_dom = prof[dom]
@@ -516,7 +555,7 @@ def run_ours(args):
             "config": {"workload": sc.name, "particles": n, "eta": sc.eta, "min_iters": sc.min_iters,
                        "max_iters": sc.max_iters, "warm_start": args.warm_start, "dt": sc.dt, "h": sc.h,
                        "xsph": sc.xsph, "network": args.mlp if learned else None,
-                       "graph": pcisph_cfg and not args.no_graph,
+                       "graph": pcisph_cfg and not args.no_graph, "corrector": best,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "working set > L2 (state, lists and scratch ~%d MB per GPU)"
                              % int(n * (3 * 16 * 2 + 8 * 2 + 4 * 2 + 16 * 4 + 8 + 4 + 4 * sc.nbr_cap + 4) / 1e6),
@@ -527,6 +566,7 @@ def run_ours(args):
             "iters_per_step": {"mean": float(np.mean(iters)), "p50": float(np.median(iters)),
                                "p95": float(np.percentile(iters, 95)), "max": int(np.max(iters)),
                                "min": int(np.min(iters))},
+            "corrector_modes": {k: {kk: v[kk] for kk in ("ms_per_step", "value", "iters_mean")} for k, v in corr.items()},
             "comparison": comparison,
             "learned_training": train_info,
             "autotune": tune,
@@ -592,12 +632,16 @@ def run_batch(args):
 
     tune = None       # the autotuner's choice, given to every context created after it
 
+    corr_mode = None  # the faster corrector, given to every context created after it is known
+
     def make(mode, graph=True):
         b = P.BatchSimulation([s.replace(warm_start=mode) for s in scenes])
         b.set_stream(stream.cuda_stream)
         b.set_graph(graph and not args.no_graph)
         if tune is not None:
             b.tune_set(**{k: tune[k] for k in TUNE_KEYS})
+        if corr_mode is not None:
+            b.set_corrector(corr_mode)
         return b
 
     # set-up (untimed): initial pressure, plain steps recorded for training, warm-up
@@ -659,9 +703,21 @@ def run_batch(args):
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    ms_max, per_scene, unconv, _ = timed_pass(sim, args.steps)
+    modes_c = {"launches": P.CORRECTOR_LAUNCHES, "persistent": P.CORRECTOR_PERSISTENT}
+    chosen = ["launches", "persistent"] if args.corrector == "both" else [args.corrector]
+    corr = {}
+    for name in chosen:
+        sim.set_corrector(modes_c[name])
+        ms_c, ps_c, unc_c, _ = timed_pass(sim, args.steps)
+        corr[name] = {"ms_per_step": ms_c / args.steps, "value": n_all * args.steps / (ms_c / 1e3),
+                      "iters_mean": float(np.mean(ps_c)), "ms": ms_c, "per_scene": ps_c, "unconv": unc_c}
+    best = min(corr, key=lambda k: corr[k]["ms"])
+    ms_max, per_scene, unconv = corr[best]["ms"], corr[best]["per_scene"], corr[best]["unconv"]
     value = n_all * args.steps / (ms_max / 1e3)
+    sim.set_corrector(P.CORRECTOR_LAUNCHES)      # per-kernel profile: the passes as separate kernels
     _, _, _, prof = timed_pass(sim, min(args.steps, 20), profile=True)
+    corr_mode = modes_c[best]
+    sim.set_corrector(corr_mode)
     # end to end: host buffers in and out every step
     pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
     h = {"pos": pin((n, 3)), "vel": pin((n, 3)), "vel_half": pin((n, 3)), "density": pin((n,)), "pressure": pin((n,))}
@@ -702,7 +758,8 @@ def run_batch(args):
     sim.close()
 
     passes = (max(1, int(np.ceil(np.log2(sum(int(np.prod(s.dims)) for s in scenes))))) + 7) // 8
-    launches = int(sum(l * _kernels_per_group(k, passes) for k, (l, _) in prof.items()))
+    prof_steps = min(args.steps, 20)
+    launches = corrector_launches(prof, prof_steps, passes, best == "persistent")
     tot_ms = sum(v[1] for v in prof.values())
     # the corrector passes skip the scenes that have converged, so their
     # launches do not cover every particle: the roofline kernel is the
@@ -714,7 +771,6 @@ def run_batch(args):
     achieved = ALG_BYTES[dom] * n / per_launch_s / 1e9
     peak, peak_kind = peaks()
     kernels = {k: {"launches": l, "ms": round(v, 3), "share": round(v / tot_ms, 4)} for k, (l, v) in prof.items()}
-    prof_steps = min(args.steps, 20)
     if rank == 0:
         out = {
             "metric": "particle-steps/s, 64 batched PCISPH dam breaks at eta=1% (C3)", "value": value, "unit": UNIT,
@@ -724,12 +780,13 @@ def run_batch(args):
             "config": {"workload": "C3: 64 PCISPH dam breaks, N log-uniform in [4096, 131072], seed 3",
                        "particles": n_all, "scenes": len(all_scenes), "scenes_on_rank0": len(scenes),
                        "eta": scenes[0].eta, "warm_start": args.warm_start, "dt": scenes[0].dt, "h": scenes[0].h,
-                       "graph": not args.no_graph,
+                       "graph": not args.no_graph, "corrector": best,
                        "parallelism": f"scenes split over {world} GPUs by size" if world > 1 else "single GPU",
                        "l2": "working set > L2 (~%d MB)" % int(n * (3 * 16 * 2 + 8 * 2 + 4 * 2 + 16 * 4 + 8 + 4 + 4 * scenes[0].nbr_cap + 4) / 1e6),
                        "timed_steps": "steps %d..%d of every scene" % (start + 2, start + 1 + args.steps)},
             "iters_per_step": {"mean_over_scenes": float(np.mean(per_scene)), "max_scene": float(np.max(per_scene)),
                                "min_scene": float(np.min(per_scene)), "unconverged_steps": int(np.sum(unconv))},
+            "corrector_modes": {k: {kk: v[kk] for kk in ("ms_per_step", "value", "iters_mean")} for k, v in corr.items()},
             "comparison": comparison,
             "learned_training": train_info,
             "autotune": tune,

@@ -339,14 +339,29 @@ int psb_batch_stats(psb_ctx* ctx, int32_t* iters, int32_t* converged, double* er
  * ways launch the same kernels in the same order. */
 int psb_set_graph(psb_ctx* ctx, int32_t on);
 
+/* The corrector loop of batches and config-profile PCISPH scenes (others
+ * return PSB_EINVAL). PSB_CORRECTOR_LAUNCHES (the default): three kernels
+ * per correction, {density pass, decision, pressure-force pass}, repeated by
+ * the graph's while node or by the host. PSB_CORRECTOR_PERSISTENT: the whole
+ * loop in one cooperative launch of one resident wave of blocks, grid-wide
+ * barriers in place of the kernel boundaries. Both run the same passes in
+ * the same order on the same data: the results are bit-identical. */
+#define PSB_CORRECTOR_LAUNCHES 0
+#define PSB_CORRECTOR_PERSISTENT 1
+int psb_set_corrector(psb_ctx* ctx, int32_t mode);
+
 /* Autotuner: the launch configuration of the neighbour build and the five
  * gather sweeps (density at x, PCISPH set-up, density/pressure pass,
  * pressure-force pass, XSPH), kept per size bucket, bucket = floor(log2 n)
  * of the particle count (a batch's total). Candidates: block sizes 128, 256
- * and 512, and for the neighbour build two cell schedules -- 0, each thread
- * walks its own 27 cells; 1, the lanes of a warp that share a grid row walk
- * it together, staging 32 candidates at a time in shared memory. Every
- * candidate computes the same result bit for bit; only the time differs.
+ * and 512, and for the neighbour build three cell schedules -- 0, each
+ * thread walks its own 27 cells; 1, the lanes of a warp that share a grid
+ * row walk it together, staging 32 candidates at a time in shared memory;
+ * 2, schedule 0 with the density pass at x (and the network's inputs) folded
+ * into the same walk (single config-profile PCISPH scenes; elsewhere it runs
+ * as 0). Where the fold is possible, schedules 0 and 1 are timed together
+ * with the separate density pass. Every candidate computes the same result
+ * bit for bit; only the time differs.
  * No counterpart in the reference, whose launches are sized by
  * computeGridSize with 256 threads (common.cu:102-107). */
 typedef struct psb_tune {

@@ -194,6 +194,7 @@ struct psb_ctx {
     std::map<int, psb_tune> tune_table;
     // CUDA-graph stepping (batches)
     bool graph_on = false;
+    int corrector = PSB_CORRECTOR_LAUNCHES;       // the corrector loop: kernel per pass, or one persistent launch
     cudaGraphExec_t gexec[2] = {};                // one per state buffer parity (cs)
     int graph_sorted = -1;                        // the sort's result buffer, fixed by the key width
     int graph_n = -1;                             // the particle count the graphs were captured for
@@ -481,12 +482,11 @@ int bits_for(size_t ncells) {
     return b;
 }
 
-// Whether the density pass at x is folded into the neighbour build: one
-// config-profile PCISPH scene with the per-thread cell walk (the row-tile
-// schedule, batches, the reference profile, WCSPH and DEM keep the two sweeps).
-bool fused_density(const psb_ctx* c, const Params& P) {
-    return !c->batch && P.pci && !P.ref && !P.dem && P.tune.nbr_schedule == 0;
-}
+// Whether the density pass at x is folded into the neighbour build
+// (schedule 2): one config-profile PCISPH scene; batches, the reference
+// profile, WCSPH and DEM run schedule 2 as schedule 0.
+bool can_fuse_density(const psb_ctx* c, const Params& P) { return !c->batch && P.pci && !P.ref && !P.dem; }
+bool fused_density(const psb_ctx* c, const Params& P) { return can_fuse_density(c, P) && P.tune.nbr_schedule == 2; }
 
 // Grid, sort, reorder, neighbour lists, density at x. keep_p: leave the
 // carried pressure in place even where the scene starts every step from 0.
@@ -573,8 +573,19 @@ int batch_corrector(psb_ctx* c, const Params& P, int s, int r, bool capture) {
     cudaStream_t st = c->stream;
     const int S = c->nscenes;
     const int max_it = c->sc.max_iters;
-    psb::launch_batch_begin(st, S, max_it, c->d_active, c->d_err_scene, c->d_err_sh, (PSB_MAX_ITERS + 1) * S,
-                            c->d_loop);
+    if (c->corrector == PSB_CORRECTOR_PERSISTENT && max_it > 0) {     // begins the loop itself
+        cudaError_t e = cudaSuccess;
+        timed(c, "corrector_persistent", [&] {
+            e = psb::launch_corrector_persistent(st, P, c->pos[s], c->vap[s], c->fnp, c->xs[0], c->rp[r], c->rpc,
+                                                 c->nbr_count, c->nbr_list, c->vs, S, c->sc.min_iters, max_it,
+                                                 c->sc.eta, c->d_active, c->d_err_scene, c->d_err_sh, c->d_loop);
+        });
+        return cuda_check(c, e, "persistent corrector");
+    }
+    timed(c, "batch_begin", [&] {
+        psb::launch_batch_begin(st, S, max_it, c->d_active, c->d_err_scene, c->d_err_sh, (PSB_MAX_ITERS + 1) * S,
+                                c->d_loop);
+    });
     if (max_it == 0) return PSB_OK;
     auto body = [&](cudaStream_t bs, cudaGraphConditionalHandle h, int set_handle) {
         timed(c, "pci_density", [&] {
@@ -2089,13 +2100,30 @@ int psb_set_graph(psb_ctx* c, int32_t on) {
     return PSB_OK;
 }
 
+int psb_set_corrector(psb_ctx* c, int32_t mode) {
+    if (!c) return PSB_EINVAL;
+    if (!c->batch && !(c->P.pci && !c->P.ref))
+        return fail(c, PSB_EINVAL, "psb_set_corrector: batches and config-profile PCISPH scenes only");
+    if (mode != PSB_CORRECTOR_LAUNCHES && mode != PSB_CORRECTOR_PERSISTENT)
+        return fail(c, PSB_EINVAL, "psb_set_corrector: unknown mode " + std::to_string(mode));
+    cudaSetDevice(c->device);
+    if (mode == PSB_CORRECTOR_PERSISTENT) {
+        int coop = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
+        if (!coop) return fail(c, PSB_ECUDA, "psb_set_corrector: the device has no cooperative launch");
+    }
+    if (mode != c->corrector) release_graphs(c);
+    c->corrector = mode;
+    return PSB_OK;
+}
+
 static bool block_ok(int b) { return b == 0 || b == 128 || b == 256 || b == 512; }
 
 int psb_tune_set(psb_ctx* c, const psb_tune* t) {
     if (!c || !t) return PSB_EINVAL;
     if (t->bucket < 0 || t->bucket > 62 || !block_ok(t->nbr_block) || !block_ok(t->density_block) ||
         !block_ok(t->init_block) || !block_ok(t->pci_density_block) || !block_ok(t->force_block) ||
-        !block_ok(t->xsph_block) || (t->nbr_schedule != 0 && t->nbr_schedule != 1))
+        !block_ok(t->xsph_block) || t->nbr_schedule < 0 || t->nbr_schedule > 2)
         return fail(c, PSB_EINVAL, "psb_tune_set: block sizes 0/128/256/512, schedule 0 or 1, bucket 0..62");
     cudaSetDevice(c->device);
     c->tune_table[t->bucket] = *t;
@@ -2162,7 +2190,7 @@ int psb_autotune(psb_ctx* c, int32_t trials, psb_tune* out) {
     auto tune_one = [&](int which, auto launch) {
         double best_ms = 1e300;
         int best_b = 256, best_sched = 0;
-        const int nsched = which == 0 ? 2 : 1;
+        const int nsched = which == 0 ? (can_fuse_density(c, P) ? 3 : 2) : 1;
         for (int sched = 0; sched < nsched; ++sched)
             for (int b : blocks) {
                 Params Q = P;
@@ -2189,10 +2217,10 @@ int psb_autotune(psb_ctx* c, int32_t trials, psb_tune* out) {
             default: best.xsph_block = best_b; break;
         }
     };
-    // The neighbour build: where the density pass at x folds into the
-    // per-thread build, schedule 0 is that fused kernel and schedule 1 the
-    // row-tile build followed by the density pass (at its default block),
-    // so that the two are timed for the same work.
+    // The neighbour build. Where the density pass at x can fold into it,
+    // every schedule is timed with that pass: schedules 0 and 1 followed by
+    // the separate pass (at its default block), schedule 2 the fused kernel,
+    // so that all three do the same work.
     tune_one(0, [&](const Params& Q) {
         if (fused_density(c, Q)) {
             psb::launch_build_density(st, Q, c->pos[s], c->vel[s], c->keys[c->sorted], c->cell_start, c->cell_end,
@@ -2202,11 +2230,12 @@ int psb_autotune(psb_ctx* c, int32_t trials, psb_tune* out) {
         }
         psb::launch_build_nbr(st, Q, c->pos[s], c->keys[c->sorted], c->cell_start, c->cell_end, c->nbr_count,
                               c->nbr_list, c->flags);
-        Params D = Q;
-        D.tune.nbr_schedule = 0;
-        if (sph && fused_density(c, D))
-            psb::launch_density_x(st, Q, c->pos[s], c->vel[s], c->nbr_count, c->nbr_list, c->rp[r], c->rho_x, 0,
+        if (can_fuse_density(c, Q)) {
+            Params D = Q;
+            D.tune = psb::Tune{};
+            psb::launch_density_x(st, D, c->pos[s], c->vel[s], c->nbr_count, c->nbr_list, c->rp[r], c->rho_x, 0,
                                   c->p_scale, feats ? c->feats : nullptr, psb::mlp_inputs(c->mlp_arch));
+        }
     });
     if (sph)
         tune_one(1, [&](const Params& Q) {

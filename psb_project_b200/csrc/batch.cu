@@ -24,27 +24,13 @@ namespace {
 
 constexpr int kLoopThreads = 256;
 
-// Start of a step's corrector. With max_iters = 0 no pass runs and every
-// scene ends unconverged with no corrections, as a single scene does.
 __global__ void __launch_bounds__(kLoopThreads) k_batch_begin(int S, int max_it, uint8_t* __restrict__ active,
                                                              unsigned long long* __restrict__ err_scene,
                                                              unsigned long long* __restrict__ err_hist, int hist_len,
                                                              int* __restrict__ loop) {
-    for (int s = threadIdx.x; s < S; s += blockDim.x) {
-        active[s] = 1;
-        err_scene[s] = 0ull;
-        loop[2 + s] = 0;
-        loop[2 + S + s] = 0;
-        if (max_it == 0) loop[2 + 3 * S + s] += 1;
-    }
-    for (int i = threadIdx.x; i < hist_len; i += blockDim.x) err_hist[i] = 0ull;
-    if (threadIdx.x == 0) { loop[0] = 0; loop[1] = 1; }
+    corrector_begin(S, max_it, active, err_scene, err_hist, hist_len, loop);
 }
 
-// After density pass k. A scene converges when k >= min_iters and its error
-// is at most eta (the host loop's test, in FP64 on the same value). A scene
-// that has not converged takes the pressure-force pass; if that pass is its
-// max_iters-th, it stops after it, unconverged, with max_iters corrections.
 __global__ void __launch_bounds__(kLoopThreads) k_batch_decide(int S, int min_it, int max_it, double eta,
                                                               uint8_t* __restrict__ active,
                                                               unsigned long long* __restrict__ err_scene,
@@ -52,35 +38,8 @@ __global__ void __launch_bounds__(kLoopThreads) k_batch_decide(int S, int min_it
                                                               int* __restrict__ loop,
                                                               cudaGraphConditionalHandle handle, int set_handle) {
     __shared__ int any;
-    if (threadIdx.x == 0) any = 0;
-    __syncthreads();
-    const int k = loop[0];
-    for (int s = threadIdx.x; s < S; s += blockDim.x) {
-        if (!active[s]) continue;
-        const unsigned long long e = err_scene[s];
-        if (k < PSB_MAX_ITERS + 1) err_hist[(size_t)k * S + s] = e;
-        err_scene[s] = 0ull;
-        if (k >= min_it && e != 0ull && unorder_double(e) <= eta) {
-            active[s] = 0;
-            loop[2 + s] = k;
-            loop[2 + S + s] = 1;
-            loop[2 + 2 * S + s] += k;
-        } else if (k + 1 >= max_it) {
-            loop[2 + s] = k + 1;          // last pass; stays active for it
-            loop[2 + 2 * S + s] += k + 1;
-            loop[2 + 3 * S + s] += 1;
-        } else {
-            any = 1;
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        // k + 1 < max_it <= PSB_MAX_ITERS whenever any is set: the loop ends
-        const int cont = any && k + 1 < max_it && k + 1 <= PSB_MAX_ITERS;
-        loop[0] = k + 1;
-        loop[1] = cont;
-        if (set_handle) cudaGraphSetConditional(handle, cont ? 1u : 0u);
-    }
+    const int cont = corrector_decide(S, min_it, max_it, eta, active, err_scene, err_hist, loop, &any);
+    if (threadIdx.x == 0 && set_handle) cudaGraphSetConditional(handle, cont ? 1u : 0u);
 }
 
 }  // namespace

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <type_traits>
+#include "psb.h"
 
 namespace psb {
 
@@ -300,6 +301,14 @@ void launch_batch_begin(cudaStream_t st, int S, int max_it, uint8_t* active, uns
 void launch_batch_decide(cudaStream_t st, int S, int min_it, int max_it, double eta, uint8_t* active,
                          unsigned long long* err_scene, unsigned long long* err_hist, int* loop,
                          cudaGraphConditionalHandle handle, int set_handle);
+// The whole corrector loop of a config-profile scene or batch as one
+// cooperative launch (begin, then {density pass, decision, pressure-force
+// pass} until the decision ends it). Returns the launch's error.
+cudaError_t launch_corrector_persistent(cudaStream_t st, const Params& P, const float4* pos, const float4* vap,
+                                        const float4* fnp, float4* xs, float2* rp, float2* rpc, const int* counts,
+                                        const int* list, float4* vs, int S, int min_it, int max_it, double eta,
+                                        uint8_t* active, unsigned long long* err_scene, unsigned long long* err_hist,
+                                        int* loop);
 
 // ---- boundary particles (boundary.cu) ------------------------------------------
 // Sorts nb boundary particles by cell (stable on index), fills their cell
@@ -406,5 +415,63 @@ __host__ __device__ inline double unorder_double(unsigned long long u) {
 #endif
     return v;
 }
+
+// Start of a step's corrector, run by one block. With max_iters = 0 no pass
+// runs and every scene ends unconverged with no corrections, as a single
+// scene does.
+__device__ inline void corrector_begin(int S, int max_it, uint8_t* active, unsigned long long* err_scene,
+                                       unsigned long long* err_hist, int hist_len, int* loop) {
+    for (int s = threadIdx.x; s < S; s += blockDim.x) {
+        active[s] = 1;
+        err_scene[s] = 0ull;
+        loop[2 + s] = 0;
+        loop[2 + S + s] = 0;
+        if (max_it == 0) loop[2 + 3 * S + s] += 1;
+    }
+    for (int i = threadIdx.x; i < hist_len; i += blockDim.x) err_hist[i] = 0ull;
+    if (threadIdx.x == 0) { loop[0] = 0; loop[1] = 1; }
+}
+
+// After density pass k, run by one block (every thread calls it; any is a
+// shared word). A scene converges when k >= min_iters and its error is at
+// most eta (the host loop's test, in FP64 on the same value). A scene that
+// has not converged takes the pressure-force pass; if that pass is its
+// max_iters-th, it stops after it, unconverged, with max_iters corrections.
+// Returns (to every thread) whether another pass follows.
+__device__ inline int corrector_decide(int S, int min_it, int max_it, double eta, uint8_t* active,
+                                       unsigned long long* err_scene, unsigned long long* err_hist, int* loop,
+                                       int* any) {
+    if (threadIdx.x == 0) *any = 0;
+    __syncthreads();
+    const int k = loop[0];
+    for (int s = threadIdx.x; s < S; s += blockDim.x) {
+        if (!active[s]) continue;
+        const unsigned long long e = err_scene[s];
+        if (k < PSB_MAX_ITERS + 1) err_hist[(size_t)k * S + s] = e;
+        err_scene[s] = 0ull;
+        if (k >= min_it && e != 0ull && unorder_double(e) <= eta) {
+            active[s] = 0;
+            loop[2 + s] = k;
+            loop[2 + S + s] = 1;
+            loop[2 + 2 * S + s] += k;
+        } else if (k + 1 >= max_it) {
+            loop[2 + s] = k + 1;          // last pass; stays active for it
+            loop[2 + 2 * S + s] += k + 1;
+            loop[2 + 3 * S + s] += 1;
+        } else {
+            *any = 1;
+        }
+    }
+    __syncthreads();
+    // k + 1 < max_it <= PSB_MAX_ITERS whenever any is set: the loop ends
+    const int cont = *any && k + 1 < max_it && k + 1 <= PSB_MAX_ITERS;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        loop[0] = k + 1;
+        loop[1] = cont;
+    }
+    return cont;
+}
+
 
 }  // namespace psb

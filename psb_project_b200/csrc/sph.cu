@@ -26,8 +26,13 @@
 // The reference's predict/restore passes (PciSphSystem.cu:30-61) become a
 // predictor that writes x*, v* to separate buffers and leaves the state
 // alone; the final leap-frog is the last prediction committed.
+#include <algorithm>
+#include <cooperative_groups.h>
+
 #include "psb_internal.cuh"
 #include "colliders.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace psb {
 
@@ -575,53 +580,58 @@ __global__ void __launch_bounds__(BS) k_pci_init(Params P, const float4* __restr
 // increment, the candidate pressure and the FP64 max compression error.
 // Batch: scenes that have converged are left as they are, and the error is
 // the max over each scene (P.err_scene).
-template <bool REF, bool BATCH, int BS>
-__global__ void __launch_bounds__(BS) k_pci_density(Params P, const float4* __restrict__ xs,
-                                                        const float2* __restrict__ rp, const int* __restrict__ counts,
-                                                        const int* __restrict__ list, float2* __restrict__ rpc,
-                                                        unsigned long long* __restrict__ err_slot) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    double err = -1e300;
-    const int sc = BATCH && t < P.n ? (int)P.slot_scene[t] : -1;
-    if (t < P.n && (!BATCH || P.active[sc])) {
-        const float4 xi = xs[t];
-        const int cnt = min(counts[t], P.cap);
-        Kahan acc;
-        float3 T1 = make_float3(0.f, 0.f, 0.f);
-        float T2 = 0.f;
-        for_each_nbr(list, P.n, t, cnt, [&](const int j) {
-            const float4 xj = xs[j];
-            const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-            const float r2 = dist2(dx, dy, dz);
-            const float q = r2 * P.inv_h2;
-            if (!REF && q >= 1.f) return;
-            const float w = 1.f - q;
-            acc.add(w * w * w);
-            if (REF && r2 > 0.f) {
-                const float rinv = rsqrtf(r2);
-                const float om = 1.f - r2 * rinv * P.inv_h;
-                const float g = om * om;
-                const float s = g * rinv;
-                T1.x += s * dx; T1.y += s * dy; T1.z += s * dz;
-                T2 += g * g;
-            }
-        });
-        if (!REF) {
-            ghost_density<BATCH>(P, t, xi, xs, list, cnt, acc);
-            if (!BATCH) boundary_density(P, t, xi, acc);
+// The density pass for sorted particle t (t < P.n, its scene still
+// iterating): rho* and the candidate pressure into rpc[t]; returns the
+// compression error (rho* - rho0)/rho0 in FP64.
+template <bool REF, bool BATCH, class F4, class F2, class F2o>
+__device__ __forceinline__ double pci_density_at(const Params& P, int t, F4 xs, F2 rp, const int* __restrict__ counts,
+                                                 const int* __restrict__ list, F2o rpc) {
+    const float4 xi = xs[t];
+    const int cnt = min(counts[t], P.cap);
+    Kahan acc;
+    float3 T1 = make_float3(0.f, 0.f, 0.f);
+    float T2 = 0.f;
+    for_each_nbr(list, P.n, t, cnt, [&](const int j) {
+        const float4 xj = xs[j];
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float r2 = dist2(dx, dy, dz);
+        const float q = r2 * P.inv_h2;
+        if (!REF && q >= 1.f) return;
+        const float w = 1.f - q;
+        acc.add(w * w * w);
+        if (REF && r2 > 0.f) {
+            const float rinv = rsqrtf(r2);
+            const float om = 1.f - r2 * rinv * P.inv_h;
+            const float g = om * om;
+            const float s = g * rinv;
+            T1.x += s * dx; T1.y += s * dy; T1.z += s * dz;
+            T2 += g * g;
         }
-        const float drho = density_deviation(P, acc);
-        const float rho = P.rho0 + drho;
-        float p = rp[t].y;
-        if (REF) {              // per-particle factor, compressed particles only
-            if (drho > 0.f && T2 > 0.f) p += P.k_press * drho / (T1.x * T1.x + T1.y * T1.y + T1.z * T1.z + T2);
-        } else {                // prototype factor, every particle, p >= 0
-            p = fmaxf(0.f, p + P.k_delta * drho);
-        }
-        rpc[t] = make_float2(rho, p);
-        err = (double)drho / P.rho0_d;
+    });
+    if (!REF) {
+        ghost_density<BATCH>(P, t, xi, xs, list, cnt, acc);
+        if (!BATCH) boundary_density(P, t, xi, acc);
     }
-    if constexpr (BATCH) {    // a warp inside one scene reduces first; one straddling two or more reduces per lane
+    const float drho = density_deviation(P, acc);
+    const float rho = P.rho0 + drho;
+    float p = rp[t].y;
+    if (REF) {              // per-particle factor, compressed particles only
+        if (drho > 0.f && T2 > 0.f) p += P.k_press * drho / (T1.x * T1.x + T1.y * T1.y + T1.z * T1.z + T2);
+    } else {                // prototype factor, every particle, p >= 0
+        p = fmaxf(0.f, p + P.k_delta * drho);
+    }
+    rpc[t] = make_float2(rho, p);
+    return (double)drho / P.rho0_d;
+}
+
+// The max of the pass's errors. Batch: per scene (P.err_scene); a warp
+// inside one scene reduces first, one straddling two or more reduces per
+// lane; sc = the slot's scene, -1 for none. Single scene: per block, one
+// ordered-integer atomic max into err_slot. Every thread of the block calls it.
+template <bool BATCH, int BS>
+__device__ __forceinline__ void reduce_error(const Params& P, int sc, double err, unsigned long long* err_slot,
+                                             double* s_err) {
+    if constexpr (BATCH) {
         const int sc0 = __shfl_sync(0xffffffffu, sc, 0);
         if (__all_sync(0xffffffffu, sc == sc0 || sc < 0)) {
 #pragma unroll
@@ -633,7 +643,6 @@ __global__ void __launch_bounds__(BS) k_pci_density(Params P, const float4* __re
     } else {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
-        __shared__ double s_err[BS / 32];
         if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = err;
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -641,7 +650,75 @@ __global__ void __launch_bounds__(BS) k_pci_density(Params P, const float4* __re
             for (int w = 1; w < BS / 32; ++w) m = fmax(m, s_err[w]);
             if (m > -1e300) atomicMax(err_slot, order_double(m));
         }
+        __syncthreads();
     }
+}
+
+// PCISPH density pass at x*: rho*, the gradient sums of the pressure
+// increment, the candidate pressure and the FP64 max compression error.
+// Batch: scenes that have converged are left as they are, and the error is
+// the max over each scene (P.err_scene).
+template <bool REF, bool BATCH, int BS>
+__global__ void __launch_bounds__(BS) k_pci_density(Params P, const float4* __restrict__ xs,
+                                                        const float2* __restrict__ rp, const int* __restrict__ counts,
+                                                        const int* __restrict__ list, float2* __restrict__ rpc,
+                                                        unsigned long long* __restrict__ err_slot) {
+    __shared__ double s_err[BS / 32];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double err = -1e300;
+    const int sc = BATCH && t < P.n ? (int)P.slot_scene[t] : -1;
+    if (t < P.n && (!BATCH || P.active[sc])) err = pci_density_at<REF, BATCH>(P, t, xs, rp, counts, list, rpc);
+    reduce_error<BATCH, BS>(P, sc, err, err_slot, s_err);
+}
+
+// PCISPH pressure-force pass fused with the next prediction; commits the
+// candidate pressure. Reference profile: at the predicted positions x*, with
+// p/rho*^2 (PciSphSystem_Kernel.cu:88-114 runs on the predicted state).
+// Config profile: at the step's start positions x, with p/rho0^2. That keeps
+// the corrector a linear iteration in p: at x*, x* = x + dt^2 a(x*) is a
+// fixed-point iteration in positions whose gain grows with p dt^2/h^2, and
+// with rho* in p/rho^2 the force feeds back on the density; under a 0.64 m
+// column either one makes the corrector diverge.
+// The pressure-force pass for sorted particle t (t < P.n, its scene still
+// iterating): the next prediction into xs_next[t] and vs[t], and the
+// candidate pressure committed to rp[t].
+template <bool REF, bool BATCH, class F4, class F2>
+__device__ __forceinline__ void pci_force_at(const Params& P, int t, const float4* __restrict__ pos,
+                                             const float4* __restrict__ vap, const float4* __restrict__ fnp, F4 xs,
+                                             F2 rpc, const int* __restrict__ counts, const int* __restrict__ list,
+                                             float4* xs_next, float4* vs, float2* rp) {
+    const float4 xi = REF ? xs[t] : pos[t];
+    const float2 ri = rpc[t];
+    const float ir0 = 1.f / (P.rho0 * P.rho0);
+    const float pVi = REF ? ri.y / (ri.x * ri.x) : ri.y * ir0;
+    const int cnt = min(counts[t], P.cap);
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    for_each_nbr(list, P.n, t, cnt, [&](const int j) {
+        const float4 xj = REF ? xs[j] : pos[j];
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float r2 = dist2(dx, dy, dz);
+        if (!(r2 > 0.f)) return;
+        if (!REF && r2 * P.inv_h2 >= 1.f) return;
+        const float2 rj = rpc[j];
+        const float rinv = rsqrtf(r2);
+        const float om = 1.f - r2 * rinv * P.inv_h;
+        const float pVj = REF ? rj.y / (rj.x * rj.x) : rj.y * ir0;
+        const float s = (pVi + pVj) * om * om * rinv;
+        acc.x += s * dx; acc.y += s * dy; acc.z += s * dz;
+    });
+    if (!REF) {
+        ghost_pressure<BATCH>(P, t, xi, pVi, pos, (const float*)&rpc[0] + 1, 2, list, cnt, acc);
+        if (!BATCH) boundary_pressure(P, t, xi, pVi, acc);
+    }
+    const float4 x0 = pos[t], vh = vap[t], f = fnp[t];
+    const float3 aw = wall_accel<REF, BATCH>(P, t, x0, vh);
+    const float ir = 1.f / ri.x;
+    const float3 a = make_float3(f.x * ir + P.k_grad * acc.x + aw.x, f.y * ir + P.k_grad * acc.y + aw.y,
+                                 f.z * ir + P.k_grad * acc.z + aw.z);
+    const float3 v = make_float3(vh.x + a.x * P.dt, vh.y + a.y * P.dt, vh.z + a.z * P.dt);
+    vs[t] = make_float4(v.x, v.y, v.z, 0.f);
+    xs_next[t] = make_float4(x0.x + v.x * P.dt, x0.y + v.y * P.dt, x0.z + v.z * P.dt, 0.f);
+    rp[t] = ri;
 }
 
 // PCISPH pressure-force pass fused with the next prediction; commits the
@@ -665,39 +742,65 @@ __global__ void __launch_bounds__(BS) k_pci_force_predict(Params P, const float4
     if (t >= P.n) return;
     if (BATCH && !P.active[P.slot_scene[t]]) return;     // its scene has converged
     if (!BATCH && P.active && !P.active[0]) return;      // single scene, corrector decided on the device: converged
-    const float4* __restrict__ geo = REF ? xs : pos;
-    const float4 xi = geo[t];
-    const float2 ri = rpc[t];
-    const float ir0 = 1.f / (P.rho0 * P.rho0);
-    const float pVi = REF ? ri.y / (ri.x * ri.x) : ri.y * ir0;
-    const int cnt = min(counts[t], P.cap);
-    float3 acc = make_float3(0.f, 0.f, 0.f);
-    for_each_nbr(list, P.n, t, cnt, [&](const int j) {
-        const float4 xj = geo[j];
-        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float r2 = dist2(dx, dy, dz);
-        if (!(r2 > 0.f)) return;
-        if (!REF && r2 * P.inv_h2 >= 1.f) return;
-        const float2 rj = rpc[j];
-        const float rinv = rsqrtf(r2);
-        const float om = 1.f - r2 * rinv * P.inv_h;
-        const float pVj = REF ? rj.y / (rj.x * rj.x) : rj.y * ir0;
-        const float s = (pVi + pVj) * om * om * rinv;
-        acc.x += s * dx; acc.y += s * dy; acc.z += s * dz;
-    });
-    if (!REF) {
-        ghost_pressure<BATCH>(P, t, xi, pVi, geo, (const float*)rpc + 1, 2, list, cnt, acc);
-        if (!BATCH) boundary_pressure(P, t, xi, pVi, acc);
+    pci_force_at<REF, BATCH>(P, t, pos, vap, fnp, xs, rpc, counts, list, xs_next, vs, rp);
+}
+
+// The whole corrector loop of a config-profile scene or batch in one
+// cooperative launch: every block strides over the particles, and grid-wide
+// barriers separate {density pass, decision, pressure-force pass} as kernel
+// boundaries do in the graph. Block 0 takes the decision (the batch's rule,
+// corrector_decide). The arrays that the passes write and the next pass
+// reads (x*, the pressures, the decision's words) are read through plain
+// pointers here, not the read-only path: the barrier's acquire makes other
+// blocks' writes visible to ordinary loads. Same passes, same order, same
+// arithmetic as the graph's loop: the results are bit-identical.
+// Five resident blocks of 256 per SM (at most 48 registers, no spills),
+// the occupancy of the separate pressure-force pass.
+template <bool BATCH, int BS>
+__global__ void __launch_bounds__(BS, 5) k_corrector_persistent(Params P, const float4* __restrict__ pos,
+                                                                 const float4* __restrict__ vap,
+                                                                 const float4* __restrict__ fnp, float4* xs, float2* rp,
+                                                                 float2* rpc, const int* __restrict__ counts,
+                                                                 const int* __restrict__ list, float4* vs,
+                                                                 unsigned long long* err_slot, int S, int min_it,
+                                                                 int max_it, double eta, uint8_t* active,
+                                                                 unsigned long long* err_scene,
+                                                                 unsigned long long* err_hist, int* loop) {
+    cg::grid_group grid = cg::this_grid();
+    __shared__ double s_err[BS / 32];
+    __shared__ int s_any;
+    const long long stride = (long long)gridDim.x * BS;
+    if (blockIdx.x == 0) corrector_begin(S, max_it, active, err_scene, err_hist, (PSB_MAX_ITERS + 1) * S, loop);
+    grid.sync();
+    for (int pass = 0; pass < max_it; ++pass) {
+        // density pass (warp-uniform bounds: the reduction is warp-synchronous)
+        double emax = -1e300;
+        for (long long base = (long long)blockIdx.x * BS; base < P.n; base += stride) {
+            const int t = (int)(base + threadIdx.x);
+            double err = -1e300;
+            const int sc = BATCH && t < P.n ? (int)P.slot_scene[t] : -1;
+            const volatile uint8_t* act = active;
+            if (t < P.n && (!BATCH || act[sc])) err = pci_density_at<false, BATCH>(P, t, (const float4*)xs, (const float2*)rp, counts, list, rpc);
+            if (BATCH) reduce_error<true, BS>(P, sc, err, err_slot, s_err);
+            else emax = fmax(emax, err);
+        }
+        if (!BATCH) reduce_error<false, BS>(P, -1, emax, err_slot, s_err);
+        grid.sync();
+        if (blockIdx.x == 0) corrector_decide(S, min_it, max_it, eta, active, err_scene, err_hist, loop, &s_any);
+        grid.sync();
+        const int cont = *(volatile int*)&loop[1];
+        // pressure-force pass and the next prediction, x* in place
+        for (long long base = (long long)blockIdx.x * BS; base < P.n; base += stride) {
+            const int t = (int)(base + threadIdx.x);
+            if (t >= P.n) continue;
+            const volatile uint8_t* act = active;
+            if (!act[BATCH ? (int)P.slot_scene[t] : 0]) continue;
+            pci_force_at<false, BATCH>(P, t, pos, vap, fnp, (const float4*)xs, (const float2*)rpc, counts, list, xs,
+                                       vs, rp);
+        }
+        if (!cont) break;
+        grid.sync();
     }
-    const float4 x0 = pos[t], vh = vap[t], f = fnp[t];
-    const float3 aw = wall_accel<REF, BATCH>(P, t, x0, vh);
-    const float ir = 1.f / ri.x;
-    const float3 a = make_float3(f.x * ir + P.k_grad * acc.x + aw.x, f.y * ir + P.k_grad * acc.y + aw.y,
-                                 f.z * ir + P.k_grad * acc.z + aw.z);
-    const float3 v = make_float3(vh.x + a.x * P.dt, vh.y + a.y * P.dt, vh.z + a.z * P.dt);
-    vs[t] = make_float4(v.x, v.y, v.z, 0.f);
-    xs_next[t] = make_float4(x0.x + v.x * P.dt, x0.y + v.y * P.dt, x0.z + v.z * P.dt, 0.f);
-    rp[t] = ri;
 }
 
 // Commit of the last prediction, walls, collision objects (COLL: the start
@@ -840,6 +943,39 @@ void launch_pci_density(cudaStream_t st, const Params& P, const float4* xs, cons
     });
 }
 
+cudaError_t launch_corrector_persistent(cudaStream_t st, const Params& P, const float4* pos, const float4* vap,
+                                        const float4* fnp, float4* xs, float2* rp, float2* rpc, const int* counts,
+                                        const int* list, float4* vs, int S, int min_it, int max_it, double eta,
+                                        uint8_t* active, unsigned long long* err_scene, unsigned long long* err_hist,
+                                        int* loop) {
+    constexpr int BS = 256;
+    auto go = [&](auto kernel) -> cudaError_t {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, BS, 0);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+        // every block resident at once (the grid barrier needs it), no more
+        // blocks than the particles fill
+        const long long need = ((long long)P.n + BS - 1) / BS;
+        const int grid = (int)std::max(1LL, std::min<long long>((long long)per_sm * sms, need));
+        unsigned long long* err_slot = err_scene;
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(BS);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, kernel, P, pos, vap, fnp, xs, rp, rpc, counts, list, vs, err_slot, S, min_it,
+                                  max_it, eta, active, err_scene, err_hist, loop);
+    };
+    if (P.ref) return cudaErrorInvalidValue;
+    return P.scenes ? go(k_corrector_persistent<true, BS>) : go(k_corrector_persistent<false, BS>);
+}
 void launch_pci_force_predict(cudaStream_t st, const Params& P, const float4* pos, const float4* vap,
                               const float4* fnp, const float4* xs, const float2* rpc, const int* counts,
                               const int* list, float4* xs_next, float4* vs, float2* rp) {

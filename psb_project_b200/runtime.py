@@ -38,7 +38,7 @@ EXPORTS = (
     "psb_last_error", "psb_abi_version", "psb_sort_cells_noalloc", "psb_presolve", "psb_mlp_set_weights",
     "psb_mlp_get_weights", "psb_mlp_collect", "psb_mlp_dataset", "psb_mlp_train", "psb_mlp_forward",
     "psb_mlp_loss_grad", "psb_iso_field", "psb_extract_surface", "psb_create_batch", "psb_batch_layout",
-    "psb_batch_stats", "psb_set_graph", "psb_autotune", "psb_tune_set", "psb_tune_get", "psb_diagnostics",
+    "psb_batch_stats", "psb_set_graph", "psb_set_corrector", "psb_autotune", "psb_tune_set", "psb_tune_get", "psb_diagnostics",
     "psb_set_boundary", "psb_boundary_psi", "psb_context_info", "psb_set_step_count", "psb_write_txt",
     "psb_write_xml", "psb_write_vol", "psb_write_obj", "psb_export_txt", "psb_export_xml", "psb_checkpoint_save",
     "psb_checkpoint_load", "psb_boundary_forces", "psb_set_external_force", "psb_set_colliders", "psb_emit",
@@ -46,6 +46,7 @@ EXPORTS = (
     "psb_warm_start",
 )
 MLP_SILU6, MLP_RELU7 = 0, 1   # PSB_MLP_SILU6 (the configured network), PSB_MLP_RELU7
+CORRECTOR_LAUNCHES, CORRECTOR_PERSISTENT = 0, 1   # PSB_CORRECTOR_*
 MLP_PARAMS = 4737       # PSB_MLP_PARAMS: the larger network's count
 MLP_H = 64
 MLP_INPUTS = {MLP_SILU6: 6, MLP_RELU7: 7}
@@ -163,6 +164,7 @@ def lib():
         "psb_batch_layout": ([P, ctypes.POINTER(I32), P], ctypes.c_int),
         "psb_batch_stats": ([P, P, P, P, P, P], ctypes.c_int),
         "psb_set_graph": ([P, I32], ctypes.c_int),
+        "psb_set_corrector": ([P, I32], ctypes.c_int),
         "psb_autotune": ([P, I32, ctypes.POINTER(PsbTune)], ctypes.c_int),
         "psb_tune_set": ([P, ctypes.POINTER(PsbTune)], ctypes.c_int),
         "psb_tune_get": ([P, I32, ctypes.POINTER(PsbTune)], ctypes.c_int),
@@ -642,6 +644,12 @@ class Simulation:
         """CUDA-graph stepping (batches and config-profile PCISPH scenes): each
         step one cudaGraphLaunch, the corrector a device-side while loop."""
         self._check(lib().psb_set_graph(self._h, 1 if on else 0), "psb_set_graph")
+
+    def set_corrector(self, mode: int = CORRECTOR_PERSISTENT):
+        """The corrector loop (batches and config-profile PCISPH scenes):
+        CORRECTOR_LAUNCHES, three kernels per correction, or
+        CORRECTOR_PERSISTENT, the whole loop in one cooperative launch."""
+        self._check(lib().psb_set_corrector(self._h, int(mode)), "psb_set_corrector")
 
     def profile_reset(self):
         self._check(lib().psb_profile_reset(self._h), "psb_profile_reset")

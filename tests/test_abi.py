@@ -38,6 +38,16 @@ def test_every_declared_symbol_is_exported():
         assert re.search(rf"\bT {n}\b", out), n
 
 
+def test_header_constants_match_bindings():
+    src = open(HEADER).read()
+    defs = dict(re.findall(r"^#define\s+(PSB_\w+)\s+(\d+)\b", src, flags=re.M))
+    assert int(defs["PSB_MLP_SILU6"]) == R.MLP_SILU6 and int(defs["PSB_MLP_RELU7"]) == R.MLP_RELU7
+    assert int(defs["PSB_CORRECTOR_LAUNCHES"]) == R.CORRECTOR_LAUNCHES
+    assert int(defs["PSB_CORRECTOR_PERSISTENT"]) == R.CORRECTOR_PERSISTENT
+    assert int(defs["PSB_MLP_PARAMS"]) == R.mlp_params(R.MLP_RELU7)
+    assert int(defs["PSB_MLP_PARAMS_SILU6"]) == R.mlp_params(R.MLP_SILU6)
+
+
 def test_struct_layout_matches_header(tmp_path):
     c = tmp_path / "layout.c"
     c.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "psb.h"\n'

@@ -4,10 +4,12 @@ bucket.
 The known answer: every candidate computes the same result bit for bit.
 One thread still handles one particle and sums its list in the same
 order; the row-tile schedule of the neighbour build accepts the same
-candidates in the same slot order as the per-thread walk. So a scene
-stepped under any configuration -- block sizes 128/256/512, either
-neighbour schedule -- must end in exactly the default's state, in both
-physics profiles and in a batch. The tuner itself must leave the state
+candidates in the same slot order as the per-thread walk; the fused
+schedule computes the density at x (and the network's inputs) with the
+separate pass's pair arithmetic in the same order. So a scene stepped under
+any configuration -- block sizes 128/256/512, any neighbour schedule -- must
+end in exactly the default's state, in both physics profiles and in a
+batch (where the fused schedule runs as the per-thread walk). The tuner itself must leave the state
 untouched and store its choice for the bucket.
 """
 import numpy as np
@@ -23,6 +25,8 @@ CONFIGS = [
          xsph_block=512),
     dict(nbr_block=256, nbr_schedule=1),
     dict(nbr_block=512, nbr_schedule=0, density_block=128, force_block=512),
+    dict(nbr_block=128, nbr_schedule=2),
+    dict(nbr_block=512, nbr_schedule=2, density_block=128, force_block=128),
 ]
 
 
@@ -63,7 +67,7 @@ def test_configs_bit_identical_config_profile(cfg):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("cfg", [0, 1])
+@pytest.mark.parametrize("cfg", [0, 1, 4])
 def test_configs_bit_identical_reference_profile(cfg):
     sc = P.ref_scene(seed=22, jitter=2e-3)
     same(run(sc, 4), run(sc, 4, CONFIGS[cfg]))
@@ -74,7 +78,7 @@ def test_configs_bit_identical_batch():
     scenes = P.batch_scenes(n_scenes=4, seed=23, n_range=(300, 2500), side=(0.3, 0.5), dt=5e-4)
     w = P.mlp_init_weights(4)
     outs = []
-    for tune in (None, CONFIGS[1]):
+    for tune in (None, CONFIGS[1], CONFIGS[5]):
         with P.BatchSimulation(scenes) as b:
             b.mlp_set_weights(w)
             b.set_graph(True)
@@ -83,9 +87,10 @@ def test_configs_bit_identical_batch():
             b.upload(P.batch_positions(scenes))
             b.step(5)
             outs.append((b.download(), b.batch_stats()["iters_total"]))
-    for k in ("pos", "vel", "pressure"):
-        assert np.array_equal(outs[0][0][k], outs[1][0][k]), k
-    assert np.array_equal(outs[0][1], outs[1][1])
+    for o in outs[1:]:
+        for k in ("pos", "vel", "pressure"):
+            assert np.array_equal(outs[0][0][k], o[0][k]), k
+        assert np.array_equal(outs[0][1], o[1])
 
 
 @pytest.mark.gpu
@@ -106,7 +111,7 @@ def test_autotune_keeps_state_and_stores_choice():
         assert t["bucket"] == Simulation.size_bucket(sc.n)
         for k in ("nbr_block", "density_block", "init_block", "pci_density_block", "force_block", "xsph_block"):
             assert t[k] in (128, 256, 512), (k, t[k])
-        assert t["nbr_schedule"] in (0, 1)
+        assert t["nbr_schedule"] in (0, 1, 2)
         assert all(t["ms"][k] > 0 and t["ms"][k] <= t["ms_default"][k] for k in t["ms"])
         assert sim.tune_get(t["bucket"])["force_block"] == t["force_block"]
         sim.step(3)

@@ -77,11 +77,12 @@ def run_single(sc, steps, weights=None, presolve=0):
         return sim.download(), iters
 
 
-def run_batch(scenes, steps, weights=None, presolve=0, graph=False):
+def run_batch(scenes, steps, weights=None, presolve=0, graph=False, corrector=P.CORRECTOR_LAUNCHES):
     with P.BatchSimulation(scenes) as b:
         if weights is not None:
             b.mlp_set_weights(weights)
         b.set_graph(graph)
+        b.set_corrector(corrector)
         b.upload(P.batch_positions(scenes))
         if presolve:
             b.presolve(presolve)
@@ -172,11 +173,12 @@ def test_graph_after_reupload_equals_eager():
     assert np.array_equal(res[0][1], res[1][1])
 
 
-def run_single_graph(sc, steps, weights, presolve, graph):
+def run_single_graph(sc, steps, weights, presolve, graph, corrector=P.CORRECTOR_LAUNCHES):
     with P.Simulation(sc) as sim:
         if weights is not None:
             sim.mlp_set_weights(weights)
         sim.set_graph(graph)
+        sim.set_corrector(corrector)
         sim.upload(P.scene_positions(sc))
         if presolve:
             sim.presolve(presolve)
@@ -207,3 +209,54 @@ def test_single_scene_graph_equals_eager(warm):
     assert it_e == it_g and err_e == err_g
     assert eager["iters_total"] == graph["iters_total"] == sum(it_e)
     assert max(it_e) >= 3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graph", [False, True])
+def test_persistent_corrector_equals_launches(graph):
+    """The corrector loop as one cooperative launch (grid-wide barriers for
+    the kernel boundaries) gives the three-kernels-per-pass loop's batch bit
+    for bit: same corrections per scene, same error history, same state;
+    stepped eagerly and captured in the step's graph."""
+    scenes = small_batch(6, warm_start=P.WARM_LEARNED, seed=31)
+    w = P.mlp_init_weights(5)
+    ref, it_r, _, st_r = run_batch(scenes, 10, w, presolve=8, graph=graph)
+    got, it_p, _, st_p = run_batch(scenes, 10, w, presolve=8, graph=graph, corrector=P.CORRECTOR_PERSISTENT)
+    for key in ("pos", "vel", "vel_half", "pressure", "density"):
+        assert np.array_equal(ref[key], got[key]), key
+    assert np.array_equal(it_r, it_p)
+    assert np.array_equal(st_r["iters_total"], st_p["iters_total"])
+    assert np.array_equal(st_r["err_final"], st_p["err_final"])
+    assert it_r.max() >= 3 and len(set(it_r[-1])) >= 2      # scenes retired at different passes
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graph", [False, True])
+def test_single_scene_persistent_corrector_equals_launches(graph):
+    sc = small_batch(1, warm_start=P.WARM_ZERO, seed=32)[0]
+    ref, it_r, err_r = run_single_graph(sc, 10, None, 8, graph=graph)
+    got, it_p, err_p = run_single_graph(sc, 10, None, 8, graph=graph, corrector=P.CORRECTOR_PERSISTENT)
+    for key in ("pos", "vel", "vel_half", "pressure", "density"):
+        assert np.array_equal(ref[key], got[key]), key
+    assert it_r == it_p and err_r == err_p
+    assert ref["iters_total"] == got["iters_total"] == sum(it_r)
+
+
+@pytest.mark.gpu
+def test_persistent_corrector_max_iters_and_modes():
+    # eta unreachable in 3 passes: every scene stops at max_iters, as the launches do
+    scenes = [s.replace(eta=1e-9, min_iters=1, max_iters=3) for s in small_batch(3, seed=33)]
+    with P.BatchSimulation(scenes) as b:
+        b.set_corrector(P.CORRECTOR_PERSISTENT)
+        b.upload(P.batch_positions(scenes))
+        rc = b.step(3)
+        st = b.batch_stats()
+        with pytest.raises(P.runtime.PsbError):
+            b.set_corrector(7)
+    assert rc == P.runtime.ENOCONV
+    assert list(st["iters"]) == [3, 3, 3] and list(st["converged"]) == [0, 0, 0]
+    assert list(st["unconverged_steps"]) == [3, 3, 3]
+    ref = P.ref_scene()
+    with P.Simulation(ref) as sim:                # the reference profile keeps its host loop
+        with pytest.raises(P.runtime.PsbError):
+            sim.set_corrector(P.CORRECTOR_PERSISTENT)

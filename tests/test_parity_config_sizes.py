@@ -2,19 +2,28 @@
 
   * The 1,048,576-particle PCISPH dam break (the headline scene): one step
     of the config method from a pre-solved rest state, through the C ABI,
-    against the FP64 oracle on the same FP32 state. Cell keys, the stable
-    (cell, id) order and the neighbour counts are bit-exact; densities
-    within 1e-5 element-wise; the non-pressure force density within 1e-5 of
-    its max; pressure within 1e-4 of its max (the floor of an FP32
-    corrector: every correction adds delta (rho* - rho0), and the FP32
-    rounding of the predicted positions x* alone moves rho* by ~1e-4
-    kg/m^3, ~1e-5 of the pressure scale per correction); velocities within
-    1e-4 of their max plus the pressure error's own effect: an error of 1e-4
-    p_max that varies from particle to particle accelerates a particle by up
-    to 1e-4 p_max / (rho0 s) over dt (s the lattice spacing), which dominates
-    when the column starts at rest and the velocities are still small;
-    positions within 4 float ulps plus 1e-5 of the displacement. The iteration count agrees
-    unless the deciding error sits within 2e-6 of eta.
+    against the FP64 oracle on the same FP32 state.
+      - Cell keys, the stable (cell, id) order and the neighbour counts:
+        bit-exact.
+      - The density at x: 1e-5 element-wise. The non-pressure force
+        density: 1e-5 of its max.
+      - Pressure: 1e-4 of its max, the floor of an FP32 corrector. Every
+        correction adds delta (rho* - rho0), and the FP32 rounding of the
+        predicted positions x* alone moves rho* by ~1e-4 kg/m^3, ~1e-5 of
+        the pressure scale per correction.
+      - Velocities: 1e-4 of their max plus the pressure error's own effect,
+        dv. An error of 1e-4 p_max that varies from particle to particle
+        accelerates a particle by up to 1e-4 p_max / (rho0 s) over dt (s
+        the lattice spacing). It dominates when the column starts at rest
+        and the velocities are still small.
+      - The corrected density rho*: 1e-5 element-wise plus the effect of
+        that velocity error. rho* is evaluated at the last prediction x*,
+        which it moves by dx = dv dt. A pair distance then moves by at most
+        2 dx, and m |dW/dr| summed over a full poly6 neighbourhood is
+        315/64 rho0/h, so rho* moves by at most ~10 rho0 dx/h.
+      - Positions: 4 float ulps plus 1e-5 of the displacement.
+      - The iteration count agrees unless the deciding error sits within
+        2e-6 of eta.
   * 50-step PCISPH trajectories, reference and config profile, against the
     FP64 oracle from the same start: before the flow turns chaotic the
     positions stay within 1e-4 of the distance travelled (the reference's
@@ -80,11 +89,13 @@ def test_c2_full_scene_step_matches_oracle():
         k = min(sg.iters, so.iters)
         assert abs(so.err[k] - sc.eta) <= 2e-6, (sg.iters, so.iters, so.err[k])
         return
-    assert np.max(np.abs(out["density"] - orc.rho) / orc.rho) <= 1e-5
+    dv = 1e-4 * np.max(np.abs(orc.p)) / (sc.rho0 * sc.blocks[0].spacing) * sc.dt
+    drho = 10 * sc.rho0 * dv * sc.dt / sc.h
+    err = np.abs(out["density"] - orc.rho)
+    assert np.all(err <= 1e-5 * orc.rho + drho), (np.max(err - 1e-5 * orc.rho), drho)
     assert rel_norm(out["pressure"], orc.p) <= 1e-4
     keep = on_bound(sc, out["pos"]) == on_bound(sc, orc.pos)
     assert (~keep).sum() <= 0.002 * sc.n
-    dv = 1e-4 * np.max(np.abs(orc.p)) / (sc.rho0 * sc.blocks[0].spacing) * sc.dt
     for key in ("vel_half", "vel"):
         ref = getattr(orc, key)[keep]
         err = np.max(np.abs(out[key][keep] - ref))
