@@ -208,8 +208,12 @@ __device__ __forceinline__ void ghost_pressure_pair(const Params& P, const F_& F
 // particles within h of a face take (the walls are evaluated at xi). Kept
 // out of the main walk: a per-neighbour wall test there slows every
 // particle more than the separate walk costs the few near the faces.
+// The positions (ghost_density) and pressures (ghost_pressure) may be ones
+// that the persistent corrector rewrites between its passes, so they are
+// not declared __restrict__ here: a kernel whose own arguments are
+// restrict-qualified read-only arrays still gets read-only-cache loads.
 template <bool BATCH = false>
-__device__ __forceinline__ void ghost_density(const Params& P, int t, float4 xi, const float4* __restrict__ pos,
+__device__ __forceinline__ void ghost_density(const Params& P, int t, float4 xi, const float4* pos,
                                               const int* __restrict__ list, int cnt, Kahan& acc) {
     const auto F = faces_of<BATCH>(P, t);
     const unsigned wall = near_walls(P, F, xi);
@@ -219,7 +223,7 @@ __device__ __forceinline__ void ghost_density(const Params& P, int t, float4 xi,
 
 template <bool BATCH = false>
 __device__ __forceinline__ void ghost_pressure(const Params& P, int t, float4 xi, float pVi,
-                                               const float4* __restrict__ pos, const float* __restrict__ pj_of,
+                                               const float4* __restrict__ pos, const float* pj_of,
                                                int pj_stride, const int* __restrict__ list, int cnt, float3& ap) {
     const auto F = faces_of<BATCH>(P, t);
     const unsigned wall = near_walls(P, F, xi);

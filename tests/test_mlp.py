@@ -266,8 +266,10 @@ def test_learned_step_matches_oracle(arch):
     p0 for the state (and leaves the state as it is); the oracle's config
     PCISPH step with the previous-pressure start from p0 is then the same
     method. The network is trained briefly on the GPU so that p0 is a
-    realistic guess. Tolerances are the config-PCISPH step's (test_gpu_parity):
-    density 1e-5 element-wise, pressure and velocities 1e-4 of their max."""
+    realistic guess. The prediction p0 is compared with the oracle's network
+    first; the step's tolerances are the config-PCISPH step's
+    (test_gpu_parity): density 1e-5 element-wise, pressure and velocities
+    1e-4 of their max."""
     sc, snap = mid_dam_state()
     with P.Simulation(sc) as gen:
         gen.mlp_set_arch(arch)
@@ -282,11 +284,24 @@ def test_learned_step_matches_oracle(arch):
         sim.mlp_set_arch(arch)
         sim.mlp_set_weights(w)
         sim.upload(snap["pos"], snap["vel"], snap["vel_half"], snap["pressure"])
-        _, p0 = sim.warm_start()
+        F, p0 = sim.warm_start()
         sim.step(1)
         out = sim.download()
         sg = sim.stats()
     assert np.all(p0 >= 0) and np.max(p0) > 0
+    # the prediction itself: the oracle's network on the GPU's own inputs
+    # (the network arithmetic, the forward test's 99th-percentile bound) and
+    # on the oracle's FP64 inputs (the whole learned path; an input that
+    # differs by its 3e-5 tolerance can round to the neighbouring BF16 value)
+    n_in, act = R.MLP_INPUTS[arch], ("silu" if arch == R.MLP_SILU6 else "relu")
+    p_scale = sc.rho0 * float(np.linalg.norm(sc.gravity)) * 0.1
+    y, _, _ = oracle.mlp_forward(w, F, n_in, act)
+    ref_own = np.maximum(0.0, y) * p_scale
+    scale = float(np.max(ref_own))
+    assert np.quantile(np.abs(p0 - ref_own), 0.99) <= 3e-3 * scale
+    ref_full = oracle.learned_pressure(sc, snap["pos"], snap["vel"], snap["pressure"], w, arch)
+    d = np.abs(p0 - ref_full)
+    assert np.median(d) <= 1e-3 * scale and np.quantile(d, 0.99) <= 2e-2 * scale, (np.median(d), np.quantile(d, 0.99), scale)
     orc = oracle.OracleSim(sc, snap["pos"], snap["vel"], snap["vel_half"], p0, float_state=True)
     so = orc.step()
     for k in range(min(so.iters, sg.iters) + 1):
