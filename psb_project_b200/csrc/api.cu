@@ -353,16 +353,6 @@ Params derive(const psb_scene& s) {
     const float h2f = (float)(hl * hl);
     P.h2_lo = h2f * (1.f - 1e-5f);
     P.h2_hi = h2f * (1.f + 1e-5f);
-    {   // cell pruning bound: the window's top plus the error a face
-        // distance can carry, (d + e)^2 - d^2 <= 2 cell e + e^2 with e an
-        // ulp of the grid's largest coordinate (taken four times)
-        double big = 0.0;
-        for (int a = 0; a < 3; ++a)
-            big = std::max(big, std::max(std::fabs((double)s.grid_min[a]),
-                                         std::fabs((double)s.grid_min[a] + (double)s.dims[a] * (double)s.cell)));
-        const double e = 4.0 * (std::nextafter((float)big, INFINITY) - (float)big);
-        P.prune2 = std::nextafter((float)((double)P.h2_hi + 2.0 * (double)s.cell * e + e * e), INFINITY);
-    }
     P.h2 = h2f;
     P.inv_h = (float)(1.0 / h);
     P.inv_h2 = (float)(1.0 / (h * h));

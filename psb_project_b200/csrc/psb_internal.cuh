@@ -60,7 +60,6 @@ struct Params {
                         // (reference: h; config: (1 + skin) h)
     double h2_exact;    // the largest double x with sqrt_rn(x) <= h: the same test as d.d <= h2_exact
     float h2_lo, h2_hi; // FP32 d^2 outside [h2_lo, h2_hi] is decided without the FP64 test
-    float prune2;       // a cell whose FP32 face-distance bound (squared) exceeds this holds no neighbour
     float h2, inv_h, inv_h2;
     float k_rho;        // 315 m / (64 pi h^3):           rho = k_rho * sum (1-q)^3
     float k_grad;       // 45 m / (pi h^4):               a_p = k_grad * sum (pV_i+pV_j)(1-u)^2 x^
@@ -197,12 +196,6 @@ __device__ __forceinline__ void nbr_flags(int cnt, int* __restrict__ flags) {
 // the list order. In a batch the walk stays inside the particle's scene's
 // grid. Candidates beyond the FP32 window are out with one compare, those
 // below it in; inside it the reference's FP64 test decides.
-// Cells that cannot hold a neighbour are not walked: the distance from the
-// particle to the faces of its own cell bounds, from below, its distance to
-// everything in the next cell that way (particles clamped into the border
-// cells lie beyond them), so a row, or the outer cell of a row, whose bound
-// exceeds the list cut-off by the FP32 window's margin is skipped. That
-// leaves about three quarters of the 27 cells, and the list is unchanged.
 template <bool BATCH, class F>
 __device__ __forceinline__ void walk_neighbours(const Params& P, int t, float4 pi, const float4* __restrict__ pos,
                                                 const uint32_t* __restrict__ keys,
@@ -215,22 +208,13 @@ __device__ __forceinline__ void walk_neighbours(const Params& P, int t, float4 p
     const int ci = (int)(key % (uint32_t)nx);
     const int cj = (int)((key / (uint32_t)nx) % (uint32_t)ny);
     const int ck = (int)(key / ((uint32_t)nx * (uint32_t)ny));
-    // distances to the own cell's lower and upper faces on each axis, FP32:
-    // a face fma(i, cell, corner) is off by at most half an ulp of the largest
-    // coordinate, which P.prune2 (the cut-off plus 4 cell ulp) absorbs
-    const float lx = fmaxf(pi.x - fmaf((float)ci, g.cell, g.gx), 0.f), hx = fmaxf(fmaf((float)(ci + 1), g.cell, g.gx) - pi.x, 0.f);
-    const float ly = fmaxf(pi.y - fmaf((float)cj, g.cell, g.gy), 0.f), hy = fmaxf(fmaf((float)(cj + 1), g.cell, g.gy) - pi.y, 0.f);
-    const float lz = fmaxf(pi.z - fmaf((float)ck, g.cell, g.gz), 0.f), hz = fmaxf(fmaf((float)(ck + 1), g.cell, g.gz) - pi.z, 0.f);
-    const float bound = P.prune2;
-    const bool xlo = ci > 0 && lx * lx <= bound, xhi = ci + 1 < nx && hx * hx <= bound;
+    // Skipping the cells whose faces lie beyond the cut-off (a bound from the
+    // particle's distance to its own cell's faces) was measured: the lanes of
+    // a warp prune different cells, so the warp still walks their union, and
+    // the per-row bounds cost more than the skipped candidates save.
+    const int a0 = max(ci - 1, 0), a1 = min(ci + 1, nx - 1);
     for (int k = max(ck - 1, 0); k <= min(ck + 1, nz - 1); ++k) {
-        const float dz = k < ck ? lz : (k > ck ? hz : 0.f);
         for (int j = max(cj - 1, 0); j <= min(cj + 1, ny - 1); ++j) {
-            const float dy = j < cj ? ly : (j > cj ? hy : 0.f);
-            const float dyz = dy * dy + dz * dz;
-            if (dyz > bound) continue;
-            const int a0 = xlo && lx * lx + dyz <= bound ? ci - 1 : ci;
-            const int a1 = xhi && hx * hx + dyz <= bound ? ci + 1 : ci;
             const uint32_t row = base + (uint32_t)j * (uint32_t)nx + (uint32_t)k * (uint32_t)nx * (uint32_t)ny;
             uint32_t lo = kEmpty, hi = 0;
             for (int a = a0; a <= a1; ++a) {

@@ -38,21 +38,38 @@ namespace psb {
 
 namespace {
 
+// Every operation of the sums that several kernels compute for the same
+// pair (the corrector's passes in their own kernels and in the persistent
+// one, the density at x in its own sweep and inside the neighbour build) is
+// rounded explicitly: __fmul_rn/__fadd_rn/__fsub_rn are never contracted,
+// and __fmaf_rn is the one fused multiply-add, so the results do not depend
+// on where the compiler would otherwise fuse a product into a sum.
 struct Kahan {
     float s = 0.f, c = 0.f;     // sum and (negated) lost low part: true sum ~ s - c
     __device__ __forceinline__ void add(float x) {
-        const float y = x - c;
-        const float t = s + y;
-        c = (t - s) - y;
+        const float y = __fsub_rn(x, c);
+        const float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
         s = t;
     }
 };
+
+// (1 - q)^3 of a pair with q = r2 / h^2 (q < 1)
+__device__ __forceinline__ float poly6_w(float q) {
+    const float w = __fsub_rn(1.f, q);
+    return __fmul_rn(__fmul_rn(w, w), w);
+}
+
+// 1 - r/h of a pair, from r2 and its reciprocal square root
+__device__ __forceinline__ float spiky_om(const Params& P, float r2, float rinv) {
+    return __fmaf_rn(-__fmul_rn(r2, rinv), P.inv_h, 1.f);
+}
 
 // rho - rho0 = k_rho (s - c) - rho0 with the product's low part kept by the
 // FMA: the deviation, from which every pressure is computed, keeps its full
 // relative precision instead of the ~6e-5 absolute step of an FP32 density.
 __device__ __forceinline__ float density_deviation(const Params& P, const Kahan& a) {
-    return fmaf(P.k_rho, a.s, -P.rho0) - P.k_rho * a.c;
+    return __fsub_rn(__fmaf_rn(P.k_rho, a.s, -P.rho0), __fmul_rn(P.k_rho, a.c));
 }
 
 __device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
@@ -95,12 +112,16 @@ __device__ __forceinline__ float3 wall_accel(const Params& P, int t, float4 x, f
     float3 a = make_float3(0.f, 0.f, 0.f);
     if (REF) return a;
     const auto F = faces_of<BATCH>(P, t);
-    if (x.x < F.x0()) a.x += P.wall_k * (F.x0() - x.x) - P.wall_c * v.x;
-    if (x.x > F.x1()) a.x += -P.wall_k * (x.x - F.x1()) - P.wall_c * v.x;
-    if (x.y < F.y0()) a.y += P.wall_k * (F.y0() - x.y) - P.wall_c * v.y;
-    if (x.y > F.y1()) a.y += -P.wall_k * (x.y - F.y1()) - P.wall_c * v.y;
-    if (x.z < F.z0()) a.z += P.wall_k * (F.z0() - x.z) - P.wall_c * v.z;
-    if (x.z > F.z1()) a.z += -P.wall_k * (x.z - F.z1()) - P.wall_c * v.z;
+    // K * depth - C * v, depth > 0 on the outside
+    auto push = [&](float depth, float vel) {
+        return __fsub_rn(__fmul_rn(P.wall_k, depth), __fmul_rn(P.wall_c, vel));
+    };
+    if (x.x < F.x0()) a.x = __fadd_rn(a.x, push(__fsub_rn(F.x0(), x.x), v.x));
+    if (x.x > F.x1()) a.x = __fadd_rn(a.x, push(-__fsub_rn(x.x, F.x1()), v.x));
+    if (x.y < F.y0()) a.y = __fadd_rn(a.y, push(__fsub_rn(F.y0(), x.y), v.y));
+    if (x.y > F.y1()) a.y = __fadd_rn(a.y, push(-__fsub_rn(x.y, F.y1()), v.y));
+    if (x.z < F.z0()) a.z = __fadd_rn(a.z, push(__fsub_rn(F.z0(), x.z), v.z));
+    if (x.z > F.z1()) a.z = __fadd_rn(a.z, push(-__fsub_rn(x.z, F.z1()), v.z));
     return a;
 }
 
@@ -145,12 +166,12 @@ __device__ __forceinline__ bool reflect(const Params& P, const F_& F, unsigned w
     const float plane = lower ? (a == 0 ? F.x0() : (a == 1 ? F.y0() : F.z0()))
                               : (a == 0 ? F.x1() : (a == 1 ? F.y1() : F.z1()));
     const float nrm = lower ? 1.f : -1.f;
-    const float dj = fmaxf(nrm * (comp(xj, a) - plane), 0.f);
+    const float dj = fmaxf(__fmul_rn(nrm, __fsub_rn(comp(xj, a), plane)), 0.f);
     if (dj >= P.hf) return false;
-    const float di = fmaxf(nrm * (comp(xi, a) - plane), 0.f);
-    const float v = nrm * (di + dj);
+    const float di = fmaxf(__fmul_rn(nrm, __fsub_rn(comp(xi, a), plane)), 0.f);
+    const float v = __fmul_rn(nrm, __fadd_rn(di, dj));
     if (a == 0) r.x = v; else if (a == 1) r.y = v; else r.z = v;
-    dp += P.rho0 * (-gcomp(P, a) * nrm) * 2.f * dj;
+    dp = __fmaf_rn(__fmul_rn(__fmul_rn(P.rho0, __fmul_rn(-gcomp(P, a), nrm)), 2.f), dj, dp);
     return true;
 }
 
@@ -159,7 +180,7 @@ __device__ __forceinline__ bool reflect(const Params& P, const F_& F, unsigned w
 template <class F_>
 __device__ __forceinline__ bool ghost_delta(const Params& P, const F_& F, unsigned w, int mask, float4 xi,
                                             float4 xj, float3& r, float& dp) {
-    r = make_float3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
+    r = make_float3(__fsub_rn(xi.x, xj.x), __fsub_rn(xi.y, xj.y), __fsub_rn(xi.z, xj.z));
     dp = 0.f;
     if ((mask & 1) && !reflect(P, F, w, 0, xi, xj, r, dp)) return false;
     if ((mask & 2) && !reflect(P, F, w, 1, xi, xj, r, dp)) return false;
@@ -177,10 +198,9 @@ __device__ __forceinline__ void ghost_density_pair(const Params& P, const F_& F,
         float3 r;
         float dp;
         if (!ghost_delta(P, F, w, mask, xi, xj, r, dp)) continue;
-        const float q = dist2(r.x, r.y, r.z) * P.inv_h2;
+        const float q = __fmul_rn(dist2(r.x, r.y, r.z), P.inv_h2);
         if (q >= 1.f) continue;
-        const float wq = 1.f - q;
-        acc.add(wq * wq * wq);
+        acc.add(poly6_w(q));
     }
 }
 
@@ -189,18 +209,18 @@ __device__ __forceinline__ void ghost_density_pair(const Params& P, const F_& F,
 template <class F_>
 __device__ __forceinline__ void ghost_pressure_pair(const Params& P, const F_& F, unsigned w, float4 xi, float4 xj,
                                                     float pVi, float pj, float3& ap) {
-    const float ir0 = 1.f / (P.rho0 * P.rho0);
+    const float ir0 = 1.f / __fmul_rn(P.rho0, P.rho0);
     const int nm = 1 << (w & 3u);
     for (int mask = 1; mask < nm; ++mask) {
         float3 r;
         float dp;
         if (!ghost_delta(P, F, w, mask, xi, xj, r, dp)) continue;
         const float r2 = dist2(r.x, r.y, r.z);
-        if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) continue;
+        if (!(r2 > 0.f) || __fmul_rn(r2, P.inv_h2) >= 1.f) continue;
         const float rinv = rsqrtf(r2);
-        const float om = 1.f - r2 * rinv * P.inv_h;
-        const float sc = (pVi + (pj + dp) * ir0) * om * om * rinv;
-        ap.x += sc * r.x; ap.y += sc * r.y; ap.z += sc * r.z;
+        const float om = spiky_om(P, r2, rinv);
+        const float sc = __fmul_rn(__fmul_rn(__fmul_rn(__fmaf_rn(__fadd_rn(pj, dp), ir0, pVi), om), om), rinv);
+        ap.x = __fmaf_rn(sc, r.x, ap.x); ap.y = __fmaf_rn(sc, r.y, ap.y); ap.z = __fmaf_rn(sc, r.z, ap.z);
     }
 }
 
@@ -243,11 +263,10 @@ __device__ __forceinline__ void boundary_density(const Params& P, int t, float4 
     const int cnt = min(P.bnd_count[t], P.bnd_cap);
     for_each_nbr(P.bnd_list, P.n, t, cnt, [&](const int b) {
         const float4 xb = P.bnd[b];
-        const float dx = xi.x - xb.x, dy = xi.y - xb.y, dz = xi.z - xb.z;
-        const float q = dist2(dx, dy, dz) * P.inv_h2;
+        const float dx = __fsub_rn(xi.x, xb.x), dy = __fsub_rn(xi.y, xb.y), dz = __fsub_rn(xi.z, xb.z);
+        const float q = __fmul_rn(dist2(dx, dy, dz), P.inv_h2);
         if (q >= 1.f) return;
-        const float w = 1.f - q;
-        acc.add(xb.w * (w * w * w));
+        acc.add(__fmul_rn(xb.w, poly6_w(q)));
     });
 }
 
@@ -256,13 +275,13 @@ __device__ __forceinline__ void boundary_pressure(const Params& P, int t, float4
     const int cnt = min(P.bnd_count[t], P.bnd_cap);
     for_each_nbr(P.bnd_list, P.n, t, cnt, [&](const int b) {
         const float4 xb = P.bnd[b];
-        const float dx = xi.x - xb.x, dy = xi.y - xb.y, dz = xi.z - xb.z;
+        const float dx = __fsub_rn(xi.x, xb.x), dy = __fsub_rn(xi.y, xb.y), dz = __fsub_rn(xi.z, xb.z);
         const float r2 = dist2(dx, dy, dz);
-        if (!(r2 > 0.f) || r2 * P.inv_h2 >= 1.f) return;
+        if (!(r2 > 0.f) || __fmul_rn(r2, P.inv_h2) >= 1.f) return;
         const float rinv = rsqrtf(r2);
-        const float om = 1.f - r2 * rinv * P.inv_h;
-        const float sc = xb.w * pVi * om * om * rinv;
-        ap.x += sc * dx; ap.y += sc * dy; ap.z += sc * dz;
+        const float om = spiky_om(P, r2, rinv);
+        const float sc = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(xb.w, pVi), om), om), rinv);
+        ap.x = __fmaf_rn(sc, dx, ap.x); ap.y = __fmaf_rn(sc, dy, ap.y); ap.z = __fmaf_rn(sc, dz, ap.z);
     });
 }
 
@@ -597,12 +616,11 @@ __device__ __forceinline__ double pci_density_at(const Params& P, int t, F4 xs, 
     float T2 = 0.f;
     for_each_nbr(list, P.n, t, cnt, [&](const int j) {
         const float4 xj = xs[j];
-        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float dx = __fsub_rn(xi.x, xj.x), dy = __fsub_rn(xi.y, xj.y), dz = __fsub_rn(xi.z, xj.z);
         const float r2 = dist2(dx, dy, dz);
-        const float q = r2 * P.inv_h2;
+        const float q = __fmul_rn(r2, P.inv_h2);
         if (!REF && q >= 1.f) return;
-        const float w = 1.f - q;
-        acc.add(w * w * w);
+        acc.add(poly6_w(q));
         if (REF && r2 > 0.f) {
             const float rinv = rsqrtf(r2);
             const float om = 1.f - r2 * rinv * P.inv_h;
@@ -617,12 +635,12 @@ __device__ __forceinline__ double pci_density_at(const Params& P, int t, F4 xs, 
         if (!BATCH) boundary_density(P, t, xi, acc);
     }
     const float drho = density_deviation(P, acc);
-    const float rho = P.rho0 + drho;
+    const float rho = __fadd_rn(P.rho0, drho);
     float p = rp[t].y;
     if (REF) {              // per-particle factor, compressed particles only
         if (drho > 0.f && T2 > 0.f) p += P.k_press * drho / (T1.x * T1.x + T1.y * T1.y + T1.z * T1.z + T2);
     } else {                // prototype factor, every particle, p >= 0
-        p = fmaxf(0.f, p + P.k_delta * drho);
+        p = fmaxf(0.f, __fmaf_rn(P.k_delta, drho, p));
     }
     rpc[t] = make_float2(rho, p);
     return (double)drho / P.rho0_d;
@@ -693,22 +711,22 @@ __device__ __forceinline__ void pci_force_at(const Params& P, int t, const float
                                              float4* xs_next, float4* vs, float2* rp) {
     const float4 xi = REF ? xs[t] : pos[t];
     const float2 ri = rpc[t];
-    const float ir0 = 1.f / (P.rho0 * P.rho0);
-    const float pVi = REF ? ri.y / (ri.x * ri.x) : ri.y * ir0;
+    const float ir0 = 1.f / __fmul_rn(P.rho0, P.rho0);
+    const float pVi = REF ? ri.y / __fmul_rn(ri.x, ri.x) : __fmul_rn(ri.y, ir0);
     const int cnt = min(counts[t], P.cap);
     float3 acc = make_float3(0.f, 0.f, 0.f);
     for_each_nbr(list, P.n, t, cnt, [&](const int j) {
         const float4 xj = REF ? xs[j] : pos[j];
-        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float dx = __fsub_rn(xi.x, xj.x), dy = __fsub_rn(xi.y, xj.y), dz = __fsub_rn(xi.z, xj.z);
         const float r2 = dist2(dx, dy, dz);
         if (!(r2 > 0.f)) return;
-        if (!REF && r2 * P.inv_h2 >= 1.f) return;
+        if (!REF && __fmul_rn(r2, P.inv_h2) >= 1.f) return;
         const float2 rj = rpc[j];
         const float rinv = rsqrtf(r2);
-        const float om = 1.f - r2 * rinv * P.inv_h;
-        const float pVj = REF ? rj.y / (rj.x * rj.x) : rj.y * ir0;
-        const float s = (pVi + pVj) * om * om * rinv;
-        acc.x += s * dx; acc.y += s * dy; acc.z += s * dz;
+        const float om = spiky_om(P, r2, rinv);
+        const float pVj = REF ? rj.y / __fmul_rn(rj.x, rj.x) : __fmul_rn(rj.y, ir0);
+        const float s = __fmul_rn(__fmul_rn(__fmul_rn(__fadd_rn(pVi, pVj), om), om), rinv);
+        acc.x = __fmaf_rn(s, dx, acc.x); acc.y = __fmaf_rn(s, dy, acc.y); acc.z = __fmaf_rn(s, dz, acc.z);
     });
     if (!REF) {
         ghost_pressure<BATCH>(P, t, xi, pVi, pos, (const float*)&rpc[0] + 1, 2, list, cnt, acc);
@@ -717,11 +735,13 @@ __device__ __forceinline__ void pci_force_at(const Params& P, int t, const float
     const float4 x0 = pos[t], vh = vap[t], f = fnp[t];
     const float3 aw = wall_accel<REF, BATCH>(P, t, x0, vh);
     const float ir = 1.f / ri.x;
-    const float3 a = make_float3(f.x * ir + P.k_grad * acc.x + aw.x, f.y * ir + P.k_grad * acc.y + aw.y,
-                                 f.z * ir + P.k_grad * acc.z + aw.z);
-    const float3 v = make_float3(vh.x + a.x * P.dt, vh.y + a.y * P.dt, vh.z + a.z * P.dt);
+    auto accel = [&](float fc, float ac, float wc) {     // f/rho + k_grad sum + wall
+        return __fadd_rn(__fmaf_rn(P.k_grad, ac, __fmul_rn(fc, ir)), wc);
+    };
+    const float3 a = make_float3(accel(f.x, acc.x, aw.x), accel(f.y, acc.y, aw.y), accel(f.z, acc.z, aw.z));
+    const float3 v = make_float3(__fmaf_rn(a.x, P.dt, vh.x), __fmaf_rn(a.y, P.dt, vh.y), __fmaf_rn(a.z, P.dt, vh.z));
     vs[t] = make_float4(v.x, v.y, v.z, 0.f);
-    xs_next[t] = make_float4(x0.x + v.x * P.dt, x0.y + v.y * P.dt, x0.z + v.z * P.dt, 0.f);
+    xs_next[t] = make_float4(__fmaf_rn(v.x, P.dt, x0.x), __fmaf_rn(v.y, P.dt, x0.y), __fmaf_rn(v.z, P.dt, x0.z), 0.f);
     rp[t] = ri;
 }
 
