@@ -52,12 +52,19 @@ struct Kahan {
         c = __fsub_rn(__fsub_rn(t, s), y);
         s = t;
     }
+    // adds a * b with the product rounded only inside the sum (one FMA)
+    __device__ __forceinline__ void add_prod(float a, float b) {
+        const float y = __fmaf_rn(a, b, -c);
+        const float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+    }
 };
 
-// (1 - q)^3 of a pair with q = r2 / h^2 (q < 1)
-__device__ __forceinline__ float poly6_w(float q) {
+// Adds a pair's (1 - q)^3, q = r2 / h^2 < 1, as (1 - q)^2 times (1 - q).
+__device__ __forceinline__ void add_poly6(Kahan& acc, float q) {
     const float w = __fsub_rn(1.f, q);
-    return __fmul_rn(__fmul_rn(w, w), w);
+    acc.add_prod(__fmul_rn(w, w), w);
 }
 
 // 1 - r/h of a pair, from r2 and its reciprocal square root
@@ -200,7 +207,7 @@ __device__ __forceinline__ void ghost_density_pair(const Params& P, const F_& F,
         if (!ghost_delta(P, F, w, mask, xi, xj, r, dp)) continue;
         const float q = __fmul_rn(dist2(r.x, r.y, r.z), P.inv_h2);
         if (q >= 1.f) continue;
-        acc.add(poly6_w(q));
+        add_poly6(acc, q);
     }
 }
 
@@ -266,7 +273,8 @@ __device__ __forceinline__ void boundary_density(const Params& P, int t, float4 
         const float dx = __fsub_rn(xi.x, xb.x), dy = __fsub_rn(xi.y, xb.y), dz = __fsub_rn(xi.z, xb.z);
         const float q = __fmul_rn(dist2(dx, dy, dz), P.inv_h2);
         if (q >= 1.f) return;
-        acc.add(__fmul_rn(xb.w, poly6_w(q)));
+        const float w = __fsub_rn(1.f, q);
+        acc.add_prod(xb.w, __fmul_rn(__fmul_rn(w, w), w));
     });
 }
 
@@ -352,24 +360,28 @@ struct DensityX {
     // pressure, which the pass writes back unchanged
     __device__ __forceinline__ void pair(const Params& P, float4 xi, float4 xj, int j, const float4* __restrict__ vel,
                                          const float2* __restrict__ rp) {
-        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float dx = __fsub_rn(xi.x, xj.x), dy = __fsub_rn(xi.y, xj.y), dz = __fsub_rn(xi.z, xj.z);
         const float r2 = dist2(dx, dy, dz);
-        const float q = r2 * P.inv_h2;
+        const float q = __fmul_rn(r2, P.inv_h2);
         if (!REF && q >= 1.f) return;
-        const float w = 1.f - q;
-        const float w3 = w * w * w;
-        acc.add(w3);
+        const float w = __fsub_rn(1.f, q);
+        const float w2 = __fmul_rn(w, w);
+        const float w3 = __fmul_rn(w2, w);
+        acc.add_prod(w2, w);
         if (SMOOTH_P) {
-            wp += w3 * rp[j].y;
-            ws += w3;
+            wp = __fmaf_rn(w3, rp[j].y, wp);
+            ws = __fadd_rn(ws, w3);
         }
         if (FEAT && r2 > 0.f) {
             const float4 vj = vel[j];
             const float rinv = rsqrtf(r2);
-            const float om = 1.f - r2 * rinv * P.inv_h;
-            const float s = om * om * rinv;                  // (1-u)^2 / r
-            gr.x += s * dx; gr.y += s * dy; gr.z += s * dz;
-            div += s * ((vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz);
+            const float om = spiky_om(P, r2, rinv);
+            const float s = __fmul_rn(__fmul_rn(om, om), rinv);           // (1-u)^2 / r
+            gr.x = __fmaf_rn(s, dx, gr.x); gr.y = __fmaf_rn(s, dy, gr.y); gr.z = __fmaf_rn(s, dz, gr.z);
+            float d = __fmul_rn(__fsub_rn(vj.x, vi.x), dx);                  // (v_j - v_i) . (x_i - x_j)
+            d = __fmaf_rn(__fsub_rn(vj.y, vi.y), dy, d);
+            d = __fmaf_rn(__fsub_rn(vj.z, vi.z), dz, d);
+            div = __fmaf_rn(s, d, div);
         }
     }
     // wall ghosts and boundary particles (config), then density, pressure
@@ -384,7 +396,7 @@ struct DensityX {
             if (!BATCH) boundary_density(P, t, xi, acc);
         }
         const float drho = density_deviation(P, acc);
-        const float rho = P.rho0 + drho;
+        const float rho = __fadd_rn(P.rho0, drho);
         float p;
         if (P.pci) {
             p = zero_p ? 0.f : rp[t].y;
@@ -397,18 +409,19 @@ struct DensityX {
             p = P.eos_k * d * s;
         }
         if (FEAT) {
-            div *= -P.k_grad / P.rho0;
+            div = __fmul_rn(div, -P.k_grad / P.rho0);
             const auto F = faces_of<BATCH>(P, t);
             float dwall = P.hf;
             dwall = fminf(dwall, fminf(xi.x - F.x0(), F.x1() - xi.x));
             dwall = fminf(dwall, fminf(xi.y - F.y0(), F.y1() - xi.y));
             dwall = fminf(dwall, fminf(xi.z - F.z0(), F.z1() - xi.z));
             float4* f = reinterpret_cast<float4*>(feats + (size_t)t * 8);     // two 16-byte stores
-            f[0] = make_float4((float)count * (1.f / 32.f), (rho - P.dt * rho * div - P.rho0) / P.rho0 * 100.f,
-                               div * P.dt * 100.f,
+            const float adv = __fsub_rn(__fsub_rn(rho, __fmul_rn(__fmul_rn(P.dt, rho), div)), P.rho0);
+            const float grad = sqrtf(dist2(gr.x, gr.y, gr.z));
+            f[0] = make_float4((float)count * (1.f / 32.f), __fmul_rn(adv / P.rho0, 100.f),
+                               __fmul_rn(__fmul_rn(div, P.dt), 100.f),
                                rp[t].y / p_scale);     // the carried pressure, before this pass replaces it
-            f[1] = make_float4(fmaxf(dwall, 0.f) * P.inv_h,
-                               P.k_grad * sqrtf(gr.x * gr.x + gr.y * gr.y + gr.z * gr.z) * P.hf / P.rho0,
+            f[1] = make_float4(__fmul_rn(fmaxf(dwall, 0.f), P.inv_h), __fmul_rn(__fmul_rn(P.k_grad, grad), P.hf) / P.rho0,
                                SMOOTH_P && ws > 0.f ? wp / ws / p_scale : 0.f, 0.f);
         }
         rp[t] = make_float2(rho, p);
@@ -620,7 +633,7 @@ __device__ __forceinline__ double pci_density_at(const Params& P, int t, F4 xs, 
         const float r2 = dist2(dx, dy, dz);
         const float q = __fmul_rn(r2, P.inv_h2);
         if (!REF && q >= 1.f) return;
-        acc.add(poly6_w(q));
+        add_poly6(acc, q);
         if (REF && r2 > 0.f) {
             const float rinv = rsqrtf(r2);
             const float om = 1.f - r2 * rinv * P.inv_h;

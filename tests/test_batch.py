@@ -218,16 +218,16 @@ def test_persistent_corrector_equals_launches(graph):
     the kernel boundaries) gives the three-kernels-per-pass loop's batch bit
     for bit: same corrections per scene, same error history, same state;
     stepped eagerly and captured in the step's graph."""
-    scenes = small_batch(6, warm_start=P.WARM_LEARNED, seed=31)
-    w = P.mlp_init_weights(5)
-    ref, it_r, _, st_r = run_batch(scenes, 10, w, presolve=8, graph=graph)
-    got, it_p, _, st_p = run_batch(scenes, 10, w, presolve=8, graph=graph, corrector=P.CORRECTOR_PERSISTENT)
+    # eta 0.3%: the scenes need different numbers of corrections, so they retire at different passes
+    scenes = [s.replace(eta=3e-3) for s in small_batch(6, warm_start=P.WARM_PREVIOUS, seed=31)]
+    ref, it_r, _, st_r = run_batch(scenes, 10, None, presolve=8, graph=graph)
+    got, it_p, _, st_p = run_batch(scenes, 10, None, presolve=8, graph=graph, corrector=P.CORRECTOR_PERSISTENT)
     for key in ("pos", "vel", "vel_half", "pressure", "density"):
         assert np.array_equal(ref[key], got[key]), key
     assert np.array_equal(it_r, it_p)
     assert np.array_equal(st_r["iters_total"], st_p["iters_total"])
     assert np.array_equal(st_r["err_final"], st_p["err_final"])
-    assert it_r.max() >= 3 and len(set(it_r[-1])) >= 2      # scenes retired at different passes
+    assert any(len(set(row)) >= 2 for row in it_r)           # scenes retired at different passes
 
 
 @pytest.mark.gpu
