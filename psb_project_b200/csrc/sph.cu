@@ -38,12 +38,14 @@ namespace psb {
 
 namespace {
 
-// Every operation of the sums that several kernels compute for the same
-// pair (the corrector's passes in their own kernels and in the persistent
-// one, the density at x in its own sweep and inside the neighbour build) is
-// rounded explicitly: __fmul_rn/__fadd_rn/__fsub_rn are never contracted,
-// and __fmaf_rn is the one fused multiply-add, so the results do not depend
-// on where the compiler would otherwise fuse a product into a sum.
+// The sums that several kernels compute for the same pair (the corrector's
+// passes in their own kernels and in the persistent one, the density at x in
+// its own sweep and inside the neighbour build) round the same way in every
+// kernel: wherever a product feeds a sum, the operation is written out --
+// __fmaf_rn where the product is fused, __fmul_rn/__fadd_rn/__fsub_rn (never
+// contracted) where it is not. Plain * and + remain only where no fused
+// multiply-add can form (products of products, a sum feeding a product), so
+// the results do not depend on where the compiler would fuse.
 struct Kahan {
     float s = 0.f, c = 0.f;     // sum and (negated) lost low part: true sum ~ s - c
     __device__ __forceinline__ void add(float x) {
@@ -69,7 +71,7 @@ __device__ __forceinline__ void add_poly6(Kahan& acc, float q) {
 
 // 1 - r/h of a pair, from r2 and its reciprocal square root
 __device__ __forceinline__ float spiky_om(const Params& P, float r2, float rinv) {
-    return __fmaf_rn(-__fmul_rn(r2, rinv), P.inv_h, 1.f);
+    return __fmaf_rn(-(r2 * rinv), P.inv_h, 1.f);
 }
 
 // rho - rho0 = k_rho (s - c) - rho0 with the product's low part kept by the
@@ -737,8 +739,9 @@ __device__ __forceinline__ void pci_force_at(const Params& P, int t, const float
         const float2 rj = rpc[j];
         const float rinv = rsqrtf(r2);
         const float om = spiky_om(P, r2, rinv);
-        const float pVj = REF ? rj.y / __fmul_rn(rj.x, rj.x) : __fmul_rn(rj.y, ir0);
-        const float s = __fmul_rn(__fmul_rn(__fmul_rn(__fadd_rn(pVi, pVj), om), om), rinv);
+        // pV_i + pV_j (config: p_j / rho0^2 fused into the sum), then products only
+        const float pv = REF ? pVi + rj.y / (rj.x * rj.x) : __fmaf_rn(rj.y, ir0, pVi);
+        const float s = pv * om * om * rinv;
         acc.x = __fmaf_rn(s, dx, acc.x); acc.y = __fmaf_rn(s, dy, acc.y); acc.z = __fmaf_rn(s, dz, acc.z);
     });
     if (!REF) {

@@ -218,8 +218,10 @@ def test_persistent_corrector_equals_launches(graph):
     the kernel boundaries) gives the three-kernels-per-pass loop's batch bit
     for bit: same corrections per scene, same error history, same state;
     stepped eagerly and captured in the step's graph."""
-    # eta 0.3%: the scenes need different numbers of corrections, so they retire at different passes
-    scenes = [s.replace(eta=3e-3) for s in small_batch(6, warm_start=P.WARM_PREVIOUS, seed=31)]
+    # eta 0.1% from p = 0 with min_iters 1: the scenes need different numbers
+    # of corrections (the oracle takes 4 to 9 on the first step), so they
+    # retire at different passes
+    scenes = [s.replace(eta=1e-3, min_iters=1) for s in small_batch(6, warm_start=P.WARM_ZERO, seed=31)]
     ref, it_r, _, st_r = run_batch(scenes, 10, None, presolve=8, graph=graph)
     got, it_p, _, st_p = run_batch(scenes, 10, None, presolve=8, graph=graph, corrector=P.CORRECTOR_PERSISTENT)
     for key in ("pos", "vel", "vel_half", "pressure", "density"):
