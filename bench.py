@@ -217,22 +217,24 @@ def ncu_traffic():
         return {}
 
 
-def cpu_baseline_port(sc, snap, steps: int, weights=None, arch: int = 0) -> dict:
+def cpu_baseline_port(sc, snap, steps: int, weights=None, arch: int = 0, boundary=None) -> dict:
     """The FP64 oracle (a C port of the same method, OpenMP on every host
     core) on a bounded sample: `steps` steps of the same scene from the same
     state the GPU's timed steps start from. With the learned warm start each
     step's initial pressure comes from the same network on the CPU (FP64
-    features, BF16 rounding points) and the oracle's corrector starts there."""
+    features, BF16 rounding points) and the oracle's corrector starts there.
+    boundary: the scene's static boundary particles, if any."""
     import oracle
     import psb_project_b200 as P
     learned = weights is not None and sc.warm_start == P.WARM_LEARNED
     osc = sc.replace(warm_start=P.WARM_PREVIOUS) if learned else sc
-    sim = oracle.OracleSim(osc, snap["pos"], snap["vel"], snap["vel_half"], snap["pressure"])
+    bnd = None if boundary is None else np.asarray(boundary, np.float64)
+    sim = oracle.OracleSim(osc, snap["pos"], snap["vel"], snap["vel_half"], snap["pressure"], boundary=bnd)
     t0 = time.perf_counter()
     iters = []
     for _ in range(steps):
         if learned:
-            sim.p[:] = oracle.learned_pressure(sc, sim.pos, sim.vel, sim.p, weights, arch)
+            sim.p[:] = oracle.learned_pressure(sc, sim.pos, sim.vel, sim.p, weights, arch, bnd)
         iters.append(sim.step().iters)
     dt = time.perf_counter() - t0
     start = "learned warm start (CPU features and network)" if learned else \
@@ -242,6 +244,31 @@ def cpu_baseline_port(sc, snap, steps: int, weights=None, arch: int = 0) -> dict
             "sample": f"{steps} steps of the {sc.n:,}-particle scene from the GPU's timed start state, {start} "
                       f"({sum(iters)} corrections, {np.mean(iters):.2f} per step), FP64 oracle, "
                       f"{host_cores()} threads on {cpu_model()}"}
+
+
+def cpu_baseline_c1(fl, sp, fsnap, bsnap, steps: int) -> dict:
+    """C1 on the CPU: the FP64 oracle's fluid and DEM steps coupled as the
+    GPU couples them (the spheres as the fluid's boundary particles, the
+    fluid's reaction as the spheres' external force), from the state the
+    GPU's timed steps start from, OpenMP on every host core."""
+    import oracle
+    fluid = oracle.OracleSim(fl, fsnap["pos"], fsnap["vel"], fsnap["vel_half"], fsnap["pressure"],
+                             boundary=np.asarray(bsnap["pos"], np.float64))
+    balls = oracle.OracleSim(sp, bsnap["pos"], bsnap["vel"], bsnap["vel_half"])
+    t0 = time.perf_counter()
+    iters = []
+    for _ in range(steps):
+        fluid.bnd_pos[:] = balls.pos
+        fluid.bnd_psi[:] = oracle.boundary_psi(fl, fluid.bnd_pos)
+        iters.append(fluid.step().iters)
+        balls.set_external_force(oracle.boundary_reaction(fl, fluid.pos, fluid.p, fluid.bnd_pos))
+        balls.step()
+    dt = time.perf_counter() - t0
+    return {"value": (fl.n + sp.n) * steps / dt, "unit": UNIT, "cores": host_cores(), "kind": "port",
+            "iters_per_step": iters,
+            "sample": f"{steps} coupled steps of the {fl.n:,} fluid particles and {sp.n:,} spheres from the GPU's timed "
+                      f"start state ({np.mean(iters):.2f} corrections per step), FP64 oracle, {host_cores()} threads "
+                      f"on {cpu_model()}"}
 
 
 def oracle_error(sim, sc, snap) -> dict:
@@ -670,6 +697,7 @@ def run_batch(args):
                       "train_s": round(time.perf_counter() - t1, 2)}
     gen.step(args.warmup)
     snap = gen.download()
+    parts = {k: gen.split(snap[k]) for k in ("pos", "vel", "vel_half", "pressure")}
     gen.close()
     start = (args.train_steps if train_info else 0) + args.warmup + 1
 
@@ -775,6 +803,26 @@ def run_batch(args):
     achieved = ALG_BYTES[dom] * n / per_launch_s / 1e9
     peak, peak_kind = peaks()
     kernels = {k: {"launches": l, "ms": round(v, 3), "share": round(v / tot_ms, 4)} for k, (l, v) in prof.items()}
+    # CPU baseline: the oracle on the first scenes of this rank's share, up to
+    # ~150k particles, each from its own timed start state
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            done_n, secs, its, picked = 0, 0.0, [], 0
+            for s_i, sc_i in enumerate(scenes):
+                if done_n >= 150000:
+                    break
+                one = cpu_baseline_port(sc_i, {k: parts[k][s_i] for k in parts}, args.cpu_sample_steps, weights)
+                done_n += sc_i.n
+                secs += sc_i.n * args.cpu_sample_steps / one["value"]
+                its += one["iters_per_step"]
+                picked += 1
+            cpu = {"value": done_n * args.cpu_sample_steps / secs, "unit": UNIT, "cores": host_cores(), "kind": "port",
+                   "sample": f"{args.cpu_sample_steps} steps of each of the first {picked} scenes ({done_n:,} particles) "
+                             f"from their timed start states, {args.warm_start} start ({np.mean(its):.2f} corrections "
+                             f"per scene-step), FP64 oracle, {host_cores()} threads on {cpu_model()}"}
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": host_cores(), "kind": "port", "sample": f"failed: {ex}"}
     if rank == 0:
         out = {
             "metric": "particle-steps/s, 64 batched PCISPH dam breaks at eta=1% (C3)", "value": value, "unit": UNIT,
@@ -801,7 +849,7 @@ def run_batch(args):
             "gpu_launches": int(launches * args.steps / prof_steps),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n_all * 40, "d2h_bytes_per_step": n_all * 44},
             "clocks": clk,
-            "cpu_baseline": None,
+            "cpu_baseline": cpu,
         }
         print(json.dumps(out))
     rep_.close()
@@ -913,6 +961,25 @@ def run_c4(args):
     mc_total_ms = timed_run.mc_ms
     value = world * n * args.steps / (ms / 1e3)
     ms_nomc, its_nomc, _ = timed_run(sim, args.steps, 0)
+    # end to end through the C ABI: host buffers in and out every step, the
+    # extractions' meshes copied to the host as in the timed run
+    pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+    h = {"pos": pin((n, 3)), "vel": pin((n, 3)), "vel_half": pin((n, 3)), "density": pin((n,)), "pressure": pin((n,))}
+    for k in ("pos", "vel", "vel_half", "pressure"):
+        h[k][:] = snap[k]
+    barrier()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for k in range(args.steps):
+        sim.upload(h["pos"], h["vel"], h["vel_half"], h["pressure"])
+        sim.step(1)
+        sim.download(h)
+        if (k + 1) % 10 == 0:
+            sim.extract_surface_into(grid, 0.5, vert, tri)
+    e3.record(stream)
+    barrier()
+    e2e_value = world * n * args.steps / (max_over_ranks(e2.elapsed_time(e3)) / 1e3)
     clk = clocks.stop()
     diag = sim.diagnostics()
     comparison = {}
@@ -932,6 +999,14 @@ def run_c4(args):
         z["iters_ratio_over_learned"] = z["iters_mean"] / max(l_["iters_mean"], 1e-9)
         z["time_ratio_over_learned"] = z["ms_per_step"] / l_["ms_per_step"]
     sim.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # a 20-step sample of 4.2M particles would take minutes on the host:
+        # two steps, the same state and start
+        try:
+            cpu = cpu_baseline_port(sc, snap, min(args.cpu_sample_steps, 2), weights, 0, bnd)
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": host_cores(), "kind": "port", "sample": f"failed: {ex}"}
     if rank == 0:
         mc_ms = mc_total_ms / max(1, args.steps // 10)
         out = {
@@ -951,7 +1026,9 @@ def run_c4(args):
             "iters_per_step_without_mc": float(its_nomc.mean()),
             "diagnostics_fp64": diag,
             "comparison": comparison, "learned_training": train_info, "autotune": tune,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * 40, "d2h_bytes_per_step": n * 44},
             "clocks": clk,
+            "cpu_baseline": cpu,
         }
         print(json.dumps(out))
     rep_.close()
@@ -983,6 +1060,7 @@ def run_c1(args):
     balls.upload(P.scene_positions(sp))
     coupled = P.FluidDemCoupling(fluid, balls)
     coupled.step(args.warmup)
+    fsnap, bsnap = fluid.download(), balls.download()
 
     def barrier():
         rep_.barrier()
@@ -1015,6 +1093,12 @@ def run_c1(args):
     diag = fluid.diagnostics()
     fluid.close()
     balls.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_c1(fl, sp, fsnap, bsnap, args.cpu_sample_steps)
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": host_cores(), "kind": "port", "sample": f"failed: {ex}"}
     if rank == 0:
         tot = sum(v[1] for v in prof.values())
         out = {
@@ -1030,7 +1114,7 @@ def run_c1(args):
             "spheres_below_fluid_top_at_end": in_fluid,
             "kernels": {k: {"launches": l, "ms": round(v, 3), "share": round(v / tot, 4)} for k, (l, v) in prof.items()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 24 * sp.n, "d2h_bytes_per_step": 24 * sp.n},
-            "diagnostics_fp64": diag, "clocks": clk,
+            "diagnostics_fp64": diag, "clocks": clk, "cpu_baseline": cpu,
         }
         print(json.dumps(out))
     rep_.close()

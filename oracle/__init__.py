@@ -415,19 +415,21 @@ def mlp_forward(w, X, n_in, activation) -> np.ndarray:
     b2 = w[o:o + H]; o += H
     w3 = w[o:o + H]; o += H
     b3 = w[o]
-    act = (lambda z: z / (1.0 + np.exp(-z))) if activation == "silu" else (lambda z: np.maximum(z, 0.0))
+    # SiLU z sigma(z) written as z/2 (1 + tanh(z/2)), finite for every z
+    act = (lambda z: 0.5 * z * (1.0 + np.tanh(0.5 * z))) if activation == "silu" else (lambda z: np.maximum(z, 0.0))
     x = _bf16(np.asarray(X, np.float32)[:, :n_in]).astype(np.float64)
     h1 = _bf16(act(x @ W1.T + b1)).astype(np.float64)
     h2 = _bf16(act(h1 @ W2.T + b2)).astype(np.float64)
     return h2 @ w3 + b3, h1, h2
 
 
-def learned_pressure(scene, pos, vel, p_prev, w, arch) -> np.ndarray:
+def learned_pressure(scene, pos, vel, p_prev, w, arch, boundary=None) -> np.ndarray:
     """The learned warm start's initial pressure on the CPU: the FP64
     features (orc_features) through the network (mlp_forward) with the
     library's BF16 rounding points, max(0, y) p_scale. arch 0: 6 inputs,
-    SiLU; 1: 7 inputs, ReLU (the library's PSB_MLP_SILU6, PSB_MLP_RELU7)."""
-    F = features(scene, pos, vel, p_prev)
+    SiLU; 1: 7 inputs, ReLU (the library's PSB_MLP_SILU6, PSB_MLP_RELU7).
+    boundary: the static boundary particles' positions, if the scene has them."""
+    F = features(scene, pos, vel, p_prev, boundary)
     n_in, act = (6, "silu") if arch == 0 else (7, "relu")
     y, _, _ = mlp_forward(w, F.astype(np.float32), n_in, act)
     g = float(np.linalg.norm(np.asarray(scene.gravity, np.float64)))
