@@ -126,6 +126,7 @@ struct psb_ctx {
     float* mlp_m1 = nullptr;
     float* mlp_m2 = nullptr;
     float* mlp_grad = nullptr;
+    float* mlp_part = nullptr;    // per-block gradient partials (summed in block order)
     float* mlp_loss = nullptr;
     void* mlp_wbf = nullptr;  // BF16 copy used by the kernels
     int mlp_step = 0;
@@ -262,7 +263,7 @@ void free_all(psb_ctx* c) {
     cudaFree(c->hist); cudaFree(c->cell_start); cudaFree(c->cell_end); cudaFree(c->nbr_count);
     cudaFree(c->nbr_list); cudaFree(c->fnp); cudaFree(c->vs); cudaFree(c->rpc); cudaFree(c->rho_x);
     cudaFree(c->err_hist); cudaFree(c->flags); cudaFree(c->stage);
-    cudaFree(c->feats); cudaFree(c->mlp_w); cudaFree(c->mlp_m1); cudaFree(c->mlp_m2); cudaFree(c->mlp_grad);
+    cudaFree(c->feats); cudaFree(c->mlp_w); cudaFree(c->mlp_m1); cudaFree(c->mlp_m2); cudaFree(c->mlp_grad); cudaFree(c->mlp_part);
     cudaFree(c->mlp_loss); cudaFree(c->mlp_wbf); cudaFree(c->ds_X); cudaFree(c->ds_T); cudaFree(c->sel);
     cudaFree(c->iso); cudaFree(c->mc_cube); cudaFree(c->mc_edge); cudaFree(c->mc_scratch); cudaFree(c->mc_vert);
     cudaFree(c->mc_tri);
@@ -928,6 +929,7 @@ int create_impl(const psb_scene* scene, size_t ncells, psb_ctx** out) {
     if (!rc) rc = dalloc(c, &c->mlp_m1, psb::kMlpParams);
     if (!rc) rc = dalloc(c, &c->mlp_m2, psb::kMlpParams);
     if (!rc) rc = dalloc(c, &c->mlp_grad, psb::kMlpParams);
+    if (!rc) rc = dalloc(c, &c->mlp_part, psb::kMlpGradPartials);
     if (!rc) rc = dalloc(c, &c->mlp_loss, 1);
     if (!rc) rc = dalloc(c, (uint16_t**)&c->mlp_wbf, psb::kMlpParams);
     if (!rc && cudaMemset(c->mlp_w, 0, sizeof(float) * psb::kMlpParams) != cudaSuccess) rc = PSB_ECUDA;
@@ -1357,7 +1359,8 @@ int psb_mlp_train(psb_ctx* c, int32_t iters, int32_t batch, float lr, uint64_t s
     for (int it = 0; it < iters; ++it) {
         psb::launch_mlp_sample(st, batch, rows, seed + 0x100000001ull * (uint64_t)(c->mlp_step + 1), c->sel);
         timed(c, "mlp_train", [&] {
-            psb::launch_mlp_grad(st, c->mlp_arch, batch, c->ds_X, c->ds_T, c->sel, c->mlp_wbf, c->mlp_grad, c->mlp_loss);
+            psb::launch_mlp_grad(st, c->mlp_arch, batch, c->ds_X, c->ds_T, c->sel, c->mlp_wbf, c->mlp_part, c->mlp_grad,
+                                 c->mlp_loss);
         });
         ++c->mlp_step;
         psb::launch_adam(st, psb::mlp_params(c->mlp_arch), c->mlp_w, c->mlp_grad, c->mlp_m1, c->mlp_m2, c->mlp_wbf, lr,
@@ -1385,7 +1388,7 @@ static int mlp_host_call(psb_ctx* c, const float* X, const float* T, int32_t n, 
         rc = cuda_check(c, cudaMemcpyAsync(y, dy, sizeof(float) * n, cudaMemcpyDeviceToHost, st), "mlp");
     }
     if (!rc && grad) {
-        psb::launch_mlp_grad(st, c->mlp_arch, n, dX, dT, nullptr, c->mlp_wbf, c->mlp_grad, c->mlp_loss);
+        psb::launch_mlp_grad(st, c->mlp_arch, n, dX, dT, nullptr, c->mlp_wbf, c->mlp_part, c->mlp_grad, c->mlp_loss);
         rc = cuda_check(c, cudaMemcpyAsync(grad, c->mlp_grad, sizeof(float) * psb::mlp_params(c->mlp_arch),
                                            cudaMemcpyDeviceToHost, st), "mlp");
         if (!rc && loss) rc = cuda_check(c, cudaMemcpyAsync(loss, c->mlp_loss, sizeof(float), cudaMemcpyDeviceToHost, st), "mlp");

@@ -244,6 +244,7 @@ __global__ void __launch_bounds__(256) k_mlp_infer_mma(int n, const float* __res
 constexpr int kTrainWarps = 4;
 constexpr int kTrainRows = 16 * kTrainWarps;    // samples per block tile
 constexpr int kTRow = 72;                       // BF16 per padded row of a transposed activation tile
+constexpr int kPartStride = kMlpParams + 1;     // floats per block row of the gradient partials
 
 // Shared memory of the training kernel (dynamic): weight images, and per
 // tile the BF16 activations transposed (row = unit, column = sample), the
@@ -253,7 +254,7 @@ struct TrainSmem {
     uint32_t W2[kH * kRow];
     uint32_t W2T[kH * kRow];
     float B1[kH], B2[kH], W3[kH], B3;
-    float G[3 * kH + 2];                        // gradients of b1, b2, w3; b3; the loss
+    float G[kTrainWarps][3 * kH + 2];           // per warp: gradients of b1, b2, w3; b3; the loss
     __nv_bfloat16 H1T[kH * kTRow];              // h1[k][m]
     __nv_bfloat16 D2T[kH * kTRow];              // dz2[j][m]
     __nv_bfloat16 D1T[kH * kTRow];              // dz1[k][m]
@@ -274,19 +275,22 @@ __device__ __forceinline__ float row_sum(float v) {
 }
 
 // Mean-squared-error loss and its gradient over `batch` samples (sample b:
-// row sel[b] of X (stride 8) and T, or row b without sel). grad and loss
-// are accumulated (the caller clears them).
+// row sel[b] of X (stride 8) and T, or row b without sel). Each block
+// writes its partial sums -- every parameter's gradient at its layout
+// index, the loss at kMlpParams -- to its own row of `partial` (kPartStride
+// floats); k_grad_reduce adds the rows in block order. No atomics: the
+// gradient, and so the trained network, is the same bits on every run.
 template <int NIN, int ACT>
 __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_train_mma(int batch, const float* __restrict__ X,
                                                                   const float* __restrict__ T,
                                                                   const uint32_t* __restrict__ sel,
                                                                   const __nv_bfloat16* __restrict__ w,
-                                                                  float* __restrict__ grad, float* __restrict__ loss) {
+                                                                  float* __restrict__ partial) {
     using L = Layout<NIN>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
     stage_weights<NIN>(w, S.W1, S.W2, S.W2T, S.B1, S.B2, S.W3, &S.B3);
-    for (int i = threadIdx.x; i < 3 * kH + 2; i += blockDim.x) S.G[i] = 0.f;
+    for (int i = threadIdx.x; i < kTrainWarps * (3 * kH + 2); i += blockDim.x) (&S.G[0][0])[i] = 0.f;
     __syncthreads();
 
     const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3, wp = threadIdx.x >> 5;
@@ -345,9 +349,9 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_train_mma(int batch, c
                 const float d0 = dy0 * S.W3[col] * act_grad<ACT>(z2[nt][c]);
                 const float d1 = dy1 * S.W3[col] * act_grad<ACT>(z2[nt][2 + c]);
                 const float gb2 = row_sum(d0 + d1);
-                if (gid == 0) {
-                    atomicAdd(&S.G[2 * kH + col], gw3);
-                    atomicAdd(&S.G[kH + col], gb2);
+                if (gid == 0) {         // one lane per column in the warp
+                    S.G[wp][2 * kH + col] += gw3;
+                    S.G[wp][kH + col] += gb2;
                 }
                 z2[nt][c] = d0;
                 z2[nt][2 + c] = d1;
@@ -365,7 +369,7 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_train_mma(int batch, c
                 const float d0 = dh[nt][c] * act_grad<ACT>(z1[nt][c]);
                 const float d1 = dh[nt][2 + c] * act_grad<ACT>(z1[nt][2 + c]);
                 const float gb1 = row_sum(d0 + d1);
-                if (gid == 0) atomicAdd(&S.G[col], gb1);
+                if (gid == 0) S.G[wp][col] += gb1;
                 // the tile's operands of the weight-gradient products, transposed
                 S.H1T[col * kTRow + m0] = __float2bfloat16_rn(act<ACT>(z1[nt][c]));
                 S.H1T[col * kTRow + m1] = __float2bfloat16_rn(act<ACT>(z1[nt][2 + c]));
@@ -396,25 +400,28 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_train_mma(int batch, c
         }
         __syncthreads();
     }
-    // ---- one atomic add per parameter and block
+    // ---- the block's partial sums: the weight tiles straight from the
+    // accumulators (each parameter held by one lane), the rest summed over
+    // the warps in order
+    float* part = partial + (size_t)blockIdx.x * kPartStride;
     const int j0 = wp * 16;
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
         const int col = nt * 8 + 2 * tig;
-        atomicAdd(&grad[L::W2 + (j0 + gid) * kH + col], gW2[nt][0]);
-        atomicAdd(&grad[L::W2 + (j0 + gid) * kH + col + 1], gW2[nt][1]);
-        atomicAdd(&grad[L::W2 + (j0 + gid + 8) * kH + col], gW2[nt][2]);
-        atomicAdd(&grad[L::W2 + (j0 + gid + 8) * kH + col + 1], gW2[nt][3]);
+        part[L::W2 + (j0 + gid) * kH + col] = gW2[nt][0];
+        part[L::W2 + (j0 + gid) * kH + col + 1] = gW2[nt][1];
+        part[L::W2 + (j0 + gid + 8) * kH + col] = gW2[nt][2];
+        part[L::W2 + (j0 + gid + 8) * kH + col + 1] = gW2[nt][3];
     }
     {
         const int i = 2 * tig;
         if (i < NIN) {
-            atomicAdd(&grad[L::W1 + (j0 + gid) * NIN + i], gW1[0]);
-            atomicAdd(&grad[L::W1 + (j0 + gid + 8) * NIN + i], gW1[2]);
+            part[L::W1 + (j0 + gid) * NIN + i] = gW1[0];
+            part[L::W1 + (j0 + gid + 8) * NIN + i] = gW1[2];
         }
         if (i + 1 < NIN) {
-            atomicAdd(&grad[L::W1 + (j0 + gid) * NIN + i + 1], gW1[1]);
-            atomicAdd(&grad[L::W1 + (j0 + gid + 8) * NIN + i + 1], gW1[3]);
+            part[L::W1 + (j0 + gid) * NIN + i + 1] = gW1[1];
+            part[L::W1 + (j0 + gid + 8) * NIN + i + 1] = gW1[3];
         }
     }
 #pragma unroll
@@ -423,18 +430,49 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_train_mma(int batch, c
         g_loss += __shfl_xor_sync(0xffffffffu, g_loss, o);
     }
     if (lane == 0) {
-        atomicAdd(&S.G[3 * kH], g_b3);
-        atomicAdd(&S.G[3 * kH + 1], g_loss);
+        S.G[wp][3 * kH] = g_b3;
+        S.G[wp][3 * kH + 1] = g_loss;
     }
     __syncthreads();
+    auto warp_sum = [&](int i) {
+        float v = S.G[0][i];
+#pragma unroll
+        for (int q = 1; q < kTrainWarps; ++q) v += S.G[q][i];
+        return v;
+    };
     for (int i = threadIdx.x; i < kH; i += blockDim.x) {
-        atomicAdd(&grad[L::B1 + i], S.G[i]);
-        atomicAdd(&grad[L::B2 + i], S.G[kH + i]);
-        atomicAdd(&grad[L::W3 + i], S.G[2 * kH + i]);
+        part[L::B1 + i] = warp_sum(i);
+        part[L::B2 + i] = warp_sum(kH + i);
+        part[L::W3 + i] = warp_sum(2 * kH + i);
     }
     if (threadIdx.x == 0) {
-        atomicAdd(&grad[L::B3], S.G[3 * kH]);
-        atomicAdd(loss, S.G[3 * kH + 1]);
+        part[L::B3] = warp_sum(3 * kH);
+        part[kMlpParams] = warp_sum(3 * kH + 1);
+    }
+}
+
+// grad[p] (p < np) and the loss: the blocks' partial rows added in a fixed
+// order. Warp w of a block adds rows w, w + 8, ... for 32 consecutive
+// entries; the eight warp sums are then added in warp order.
+__global__ void __launch_bounds__(256) k_grad_reduce(int nblocks, int np, const float* __restrict__ partial,
+                                                     float* __restrict__ grad, float* __restrict__ loss) {
+    __shared__ float s[8][33];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int q = blockIdx.x * 32 + lane;                 // q == np: the loss
+    const int src = q < np ? q : kMlpParams;
+    float v = 0.f;
+    if (q <= np) {
+#pragma unroll 4
+        for (int b = w; b < nblocks; b += 8) v += partial[(size_t)b * kPartStride + src];
+    }
+    s[w][lane] = v;
+    __syncthreads();
+    if (w == 0 && q <= np) {
+        float t = s[0][lane];
+#pragma unroll
+        for (int k = 1; k < 8; ++k) t += s[k][lane];
+        if (q < np) grad[q] = t;
+        else *loss = t;
     }
 }
 
@@ -528,18 +566,22 @@ void launch_mlp_forward(cudaStream_t st, int arch, int n, const float* X, const 
 }
 
 void launch_mlp_grad(cudaStream_t st, int arch, int batch, const float* X, const float* T, const uint32_t* sel,
-                     const void* wbf, float* grad, float* loss) {
-    cudaMemsetAsync(grad, 0, sizeof(float) * kMlpParams, st);
-    cudaMemsetAsync(loss, 0, sizeof(float), st);
-    if (batch <= 0) return;
+                     const void* wbf, float* partial, float* grad, float* loss) {
+    if (batch <= 0) {
+        cudaMemsetAsync(grad, 0, sizeof(float) * kMlpParams, st);
+        cudaMemsetAsync(loss, 0, sizeof(float), st);
+        return;
+    }
     const int tiles = (batch + kTrainRows - 1) / kTrainRows;
-    const int blocks = std::min(tiles, 148 * 4);
+    const int blocks = std::min(tiles, kMlpGradBlocks);
     with_arch(arch, [&](auto nin, auto a) {
         auto kernel = k_mlp_train_mma<decltype(nin)::value, decltype(a)::value>;
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
-        kernel<<<blocks, kTrainWarps * 32, sizeof(TrainSmem), st>>>(batch, X, T, sel, (const __nv_bfloat16*)wbf, grad,
-                                                                    loss);
+        kernel<<<blocks, kTrainWarps * 32, sizeof(TrainSmem), st>>>(batch, X, T, sel, (const __nv_bfloat16*)wbf,
+                                                                    partial);
     });
+    const int np = mlp_params(arch);
+    k_grad_reduce<<<(np + 1 + 31) / 32, 256, 0, st>>>(blocks, np, partial, grad, loss);
 }
 
 void launch_mlp_sample(cudaStream_t st, int batch, uint64_t size, uint64_t seed, uint32_t* sel) {

@@ -369,8 +369,12 @@ int mlp_inputs(int arch);
 int mlp_params(int arch);
 void launch_mlp_infer(cudaStream_t st, int arch, int n, const float* feats, const void* wbf, float p_scale, float2* rp);
 void launch_mlp_forward(cudaStream_t st, int arch, int n, const float* X, const void* wbf, float* y);
+// Training blocks per minibatch (at most) and the gradient partials they
+// write: kMlpGradBlocks rows of kMlpParams + 1 floats (the caller's buffer).
+constexpr int kMlpGradBlocks = 148 * 4;
+constexpr size_t kMlpGradPartials = (size_t)kMlpGradBlocks * (kMlpParams + 1);
 void launch_mlp_grad(cudaStream_t st, int arch, int batch, const float* X, const float* T, const uint32_t* sel,
-                     const void* wbf, float* grad, float* loss);
+                     const void* wbf, float* partial, float* grad, float* loss);
 void launch_mlp_sample(cudaStream_t st, int batch, uint64_t size, uint64_t seed, uint32_t* sel);
 void launch_adam(cudaStream_t st, int np, float* w, const float* grad, float* m1, float* m2, void* wbf, float lr,
                  int step);

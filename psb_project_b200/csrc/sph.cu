@@ -362,6 +362,9 @@ struct DensityX {
     // pressure, which the pass writes back unchanged
     __device__ __forceinline__ void pair(const Params& P, float4 xi, float4 xj, int j, const float4* __restrict__ vel,
                                          const float2* __restrict__ rp) {
+        // the pair's other gathers issue with its position, ahead of the tests
+        const float4 vj = FEAT ? vel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float pj = SMOOTH_P ? rp[j].y : 0.f;
         const float dx = __fsub_rn(xi.x, xj.x), dy = __fsub_rn(xi.y, xj.y), dz = __fsub_rn(xi.z, xj.z);
         const float r2 = dist2(dx, dy, dz);
         const float q = __fmul_rn(r2, P.inv_h2);
@@ -371,11 +374,10 @@ struct DensityX {
         const float w3 = __fmul_rn(w2, w);
         acc.add_prod(w2, w);
         if (SMOOTH_P) {
-            wp = __fmaf_rn(w3, rp[j].y, wp);
+            wp = __fmaf_rn(w3, pj, wp);
             ws = __fadd_rn(ws, w3);
         }
         if (FEAT && r2 > 0.f) {
-            const float4 vj = vel[j];
             const float rinv = rsqrtf(r2);
             const float om = spiky_om(P, r2, rinv);
             const float s = __fmul_rn(__fmul_rn(om, om), rinv);           // (1-u)^2 / r
@@ -510,14 +512,14 @@ __device__ __forceinline__ PairSums pair_sums(const Params& P, int t, float4 xi,
     const float pVi = WITH_PRESSURE ? (REF ? rpi.y / (rpi.x * rpi.x) : rpi.y * ir0) : 0.f;
     const int cnt = min(counts[t], P.cap);
     for_each_nbr(list, P.n, t, cnt, [&](const int j) {
-        const float4 xj = pos[j];
+        const float4 xj = pos[j];       // the pair's three gathers, ahead of the tests
+        const float4 vj = vel[j];
+        const float2 rpj = rp[j];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float r2 = dist2(dx, dy, dz);
         if (!(r2 > 0.f)) return;
         const float q = r2 * P.inv_h2;
         if (!REF && q >= 1.f) return;
-        const float4 vj = vel[j];
-        const float2 rpj = rp[j];
         const float rinv = rsqrtf(r2);
         const float om = 1.f - r2 * rinv * P.inv_h;
         const float inv_rj = 1.f / rpj.x;
@@ -663,8 +665,9 @@ __device__ __forceinline__ double pci_density_at(const Params& P, int t, F4 xs, 
 
 // The max of the pass's errors. Batch: per scene (P.err_scene); a warp
 // inside one scene reduces first, one straddling two or more reduces per
-// lane; sc = the slot's scene, -1 for none. Single scene: per block, one
-// ordered-integer atomic max into err_slot. Every thread of the block calls it.
+// lane; sc = the slot's scene, -1 for none. Single scene (the persistent
+// corrector, once per block and pass): per block, one ordered-integer atomic
+// max into err_slot; every thread of the block calls it.
 template <bool BATCH, int BS>
 __device__ __forceinline__ void reduce_error(const Params& P, int sc, double err, unsigned long long* err_slot,
                                              double* s_err) {
@@ -695,17 +698,31 @@ __device__ __forceinline__ void reduce_error(const Params& P, int sc, double err
 // increment, the candidate pressure and the FP64 max compression error.
 // Batch: scenes that have converged are left as they are, and the error is
 // the max over each scene (P.err_scene).
+// Single scene: the max over each warp, then one ordered-integer atomic max
+// per warp (a reduction without return: the warp leaves at once). A block-
+// level reduction made the block's early warps wait at its barrier for the
+// slowest one, a third of the pass's stall cycles at 1M particles.
+template <bool BATCH, int BS>
+__device__ __forceinline__ void warp_max_error(const Params& P, int sc, double err, unsigned long long* err_slot) {
+    if constexpr (BATCH) {
+        reduce_error<true, BS>(P, sc, err, err_slot, nullptr);
+    } else {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
+        if ((threadIdx.x & 31) == 0 && err > -1e300) atomicMax(err_slot, order_double(err));
+    }
+}
+
 template <bool REF, bool BATCH, int BS>
 __global__ void __launch_bounds__(BS) k_pci_density(Params P, const float4* __restrict__ xs,
                                                         const float2* __restrict__ rp, const int* __restrict__ counts,
                                                         const int* __restrict__ list, float2* __restrict__ rpc,
                                                         unsigned long long* __restrict__ err_slot) {
-    __shared__ double s_err[BS / 32];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double err = -1e300;
     const int sc = BATCH && t < P.n ? (int)P.slot_scene[t] : -1;
     if (t < P.n && (!BATCH || P.active[sc])) err = pci_density_at<REF, BATCH>(P, t, xs, rp, counts, list, rpc);
-    reduce_error<BATCH, BS>(P, sc, err, err_slot, s_err);
+    warp_max_error<BATCH, BS>(P, sc, err, err_slot);
 }
 
 // PCISPH pressure-force pass fused with the next prediction; commits the
@@ -731,12 +748,14 @@ __device__ __forceinline__ void pci_force_at(const Params& P, int t, const float
     const int cnt = min(counts[t], P.cap);
     float3 acc = make_float3(0.f, 0.f, 0.f);
     for_each_nbr(list, P.n, t, cnt, [&](const int j) {
+        // both gathers of the pair issue before its distance test, so a pair
+        // costs one dependent load after the list, not two
         const float4 xj = REF ? xs[j] : pos[j];
+        const float2 rj = rpc[j];
         const float dx = __fsub_rn(xi.x, xj.x), dy = __fsub_rn(xi.y, xj.y), dz = __fsub_rn(xi.z, xj.z);
         const float r2 = dist2(dx, dy, dz);
         if (!(r2 > 0.f)) return;
         if (!REF && __fmul_rn(r2, P.inv_h2) >= 1.f) return;
-        const float2 rj = rpc[j];
         const float rinv = rsqrtf(r2);
         const float om = spiky_om(P, r2, rinv);
         // pV_i + pV_j (config: p_j / rho0^2 fused into the sum), then products only

@@ -188,6 +188,28 @@ def test_training_reduces_loss_on_a_known_function():
     assert last < 0.2 * first
 
 
+def test_training_is_reproducible():
+    """The whole learned pipeline -- record plain-PCISPH rows, then train --
+    run twice from the same state gives the same weights bit for bit: the
+    simulation sums in list order, the minibatches are drawn from a seeded
+    counter-based generator, and each block's gradient partials are added in
+    block order (no floating-point atomics)."""
+    sc = P.dam_break((24, 20, 16), 0.005, (0.5, 0.4, 0.3), 0.01, seed=11).replace(warm_start=P.WARM_PREVIOUS)
+    pos = P.scene_positions(sc)
+    runs = []
+    for _ in range(2):
+        with P.Simulation(sc) as sim:
+            sim.upload(pos)
+            sim.presolve(20)
+            sim.mlp_collect(stride=4, capacity=1 << 18)
+            sim.step(6)
+            sim.mlp_set_weights(P.mlp_init_weights(0))
+            loss = sim.mlp_train(200, 4096, 2e-3, seed=5)
+            runs.append((loss, sim.mlp_get_weights()))
+    assert runs[0][0] == runs[1][0]
+    assert np.array_equal(runs[0][1], runs[1][1])
+
+
 def test_learned_warm_start_beats_plain():
     """Collect (features, converged pressure) pairs from warm-started steps,
     train, then run the same steps learned and plain: the learned start must
