@@ -117,6 +117,8 @@ def parse():
     ap.add_argument("--tune-cache", default=None,
                     help="JSON cache of tuned launch configurations: a bucket found there is not tuned again; "
                          "new results are added")
+    ap.add_argument("--c1-no-whole-run", action="store_true",
+                    help="C1: skip the untimed runs of all configured steps (implicit and staggered coupling)")
     ap.add_argument("--eval-steps", type=int, default=None,
                     help="steps after the recorded ones over which the warm starts are compared (0: skip)")
     args = ap.parse_args()
@@ -248,21 +250,19 @@ def cpu_baseline_port(sc, snap, steps: int, weights=None, arch: int = 0, boundar
 
 def cpu_baseline_c1(fl, sp, fsnap, bsnap, steps: int) -> dict:
     """C1 on the CPU: the FP64 oracle's fluid and DEM steps coupled as the
-    GPU couples them (the spheres as the fluid's boundary particles, the
-    fluid's reaction as the spheres' external force), from the state the
-    GPU's timed steps start from, OpenMP on every host core."""
+    GPU couples them (the spheres as the fluid's boundary particles, their
+    motion solved inside the fluid's corrector, the reaction of its last
+    prediction as the spheres' external force), from the state the GPU's
+    timed steps start from, OpenMP on every host core."""
     import oracle
     fluid = oracle.OracleSim(fl, fsnap["pos"], fsnap["vel"], fsnap["vel_half"], fsnap["pressure"],
                              boundary=np.asarray(bsnap["pos"], np.float64))
     balls = oracle.OracleSim(sp, bsnap["pos"], bsnap["vel"], bsnap["vel_half"])
+    coupled = oracle.Coupling(fl, fluid, sp, balls, implicit=True)
     t0 = time.perf_counter()
     iters = []
     for _ in range(steps):
-        fluid.bnd_pos[:] = balls.pos
-        fluid.bnd_psi[:] = oracle.boundary_psi(fl, fluid.bnd_pos)
-        iters.append(fluid.step().iters)
-        balls.set_external_force(oracle.boundary_reaction(fl, fluid.pos, fluid.p, fluid.bnd_pos))
-        balls.step()
+        iters.append(coupled.step()[0].iters)
     dt = time.perf_counter() - t0
     return {"value": (fl.n + sp.n) * steps / dt, "unit": UNIT, "cores": host_cores(), "kind": "port",
             "iters_per_step": iters,
@@ -1109,6 +1109,33 @@ def run_c1(args):
     diag = fluid.diagnostics()
     fluid.close()
     balls.close()
+
+    def whole_run(implicit):
+        """The configured steps from the start, untimed: corrections per
+        window of 50 steps and where the spheres are."""
+        f_, b_ = P.Simulation(fl), P.Simulation(sp)
+        f_.upload(P.scene_positions(fl))
+        f_.presolve(args.presolve)
+        b_.upload(P.scene_positions(sp))
+        c_ = P.FluidDemCoupling(f_, b_, implicit=implicit)
+        its_, win = [], []
+        t_ = time.perf_counter()
+        for k in range(fl.steps):
+            c_.step(1)
+            its_.append(f_.stats().iters)
+            if (k + 1) % 50 == 0:
+                w = np.array(its_[-50:])
+                y = b_.download()["pos"][:, 1]
+                win.append({"steps": f"{k - 48}..{k + 1}", "iters_mean": float(w.mean()), "iters_p50": float(np.median(w)),
+                            "not_converged": int(np.count_nonzero(w >= fl.max_iters)), "spheres_y_mean": float(y.mean())})
+        f_.close()
+        b_.close()
+        a_ = np.array(its_)
+        return {"steps": fl.steps, "iters_mean": float(a_.mean()), "iters_p50": float(np.median(a_)),
+                "not_converged": int(np.count_nonzero(a_ >= fl.max_iters)), "wall_s": round(time.perf_counter() - t_, 1),
+                "windows": win}
+
+    runs = {"implicit": whole_run(True), "staggered": whole_run(False)} if not args.c1_no_whole_run else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -1128,6 +1155,8 @@ def run_c1(args):
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "iters_per_step": {"mean": float(np.mean(iters)), "p50": float(np.median(iters)), "max": int(np.max(iters))},
             "spheres_below_fluid_top_at_end": in_fluid,
+            "coupling": "implicit: the spheres' motion solved inside the fluid's corrector",
+            "whole_run": runs,
             "kernels": {k: {"launches": l, "ms": round(v, 3), "share": round(v / tot, 4)} for k, (l, v) in prof.items()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 24 * sp.n, "d2h_bytes_per_step": 24 * sp.n},
             "diagnostics_fp64": diag, "clocks": clk, "cpu_baseline": cpu,

@@ -408,6 +408,25 @@ int psb_boundary_psi(psb_ctx* ctx, float* psi);
  * is the fluid's side of a two-way coupling (C1). No counterpart in the
  * reference, which has no fluid-solid coupling. */
 int psb_boundary_forces(psb_ctx* ctx, float* force);
+/* Makes the current boundary set move with the pressure corrector (config
+ * PCISPH, single scene): the two-way fluid-solid coupling solved inside the
+ * step instead of staggered between steps. vel and force (n_bnd x 3, in the
+ * order the set was given) are each particle's velocity and its non-fluid
+ * force (N: gravity and contacts, e.g. psb_dem_forces) at the step's start;
+ * mass is each particle's mass (kg). Every prediction of the step then also
+ * predicts the boundary, x*_b = x_b + dt (v_b + dt (F_b + f_b) / m) with F_b
+ * the fluid's reaction at the pressures of that prediction, and the density
+ * passes see x*_b. After the step, psb_boundary_forces returns the F_b of the
+ * last prediction: a DEM step given it as its external force moves the
+ * spheres to that prediction (where no wall projects them). vel = NULL makes
+ * the boundary static again; psb_set_boundary always does. No counterpart in
+ * the reference, which has no fluid-solid coupling. */
+int psb_set_boundary_motion(psb_ctx* ctx, const float* vel, const float* force, float mass);
+/* DEM contexts: the force (N, n x 3 in particle-id order) the next step
+ * would apply to each sphere apart from the external one: gravity and the
+ * contacts at the current state (CudaSystem::update's force sum,
+ * CudaSystem.cpp:226-245). Nothing moves. */
+int psb_dem_forces(psb_ctx* ctx, float* force);
 /* DEM contexts: an external force per sphere (N, n x 3 in particle-id
  * order) added to gravity and contacts in every step until replaced; NULL
  * removes it. Extends CudaSystem::update's force sum (CudaSystem.cpp:207-224),

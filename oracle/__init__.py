@@ -55,6 +55,8 @@ class OrcParams(ctypes.Structure):
         ("bnd_counts", ctypes.c_void_p), ("bnd_lists", ctypes.c_void_p), ("bnd_cap", ctypes.c_int32),
         ("dem_ext", ctypes.c_void_p),
         ("n_coll", ctypes.c_int32), ("coll", ctypes.c_void_p),
+        ("bnd_vel", ctypes.c_void_p), ("bnd_fext", ctypes.c_void_p), ("bnd_inv_mass", ctypes.c_double),
+        ("bnd_pred", ctypes.c_void_p), ("bnd_force", ctypes.c_void_p),
     ]
 
 
@@ -501,6 +503,26 @@ class OracleSim:
             self.ext = np.ascontiguousarray(f, np.float64).reshape(-1, 3)
             self.P.dem_ext = self.ext.ctypes.data
 
+    def set_boundary_motion(self, vel, fext, mass):
+        """Config PCISPH: the boundary particles move with the corrector
+        (two-way coupling inside the step): their velocities and non-fluid
+        forces at the step's start (n_bnd, 3) and their mass; None: static.
+        After a step, bnd_pred holds the predicted boundary positions and
+        bnd_force the fluid's reaction they were predicted with."""
+        if vel is None:
+            self.P.bnd_vel = self.P.bnd_fext = self.P.bnd_pred = self.P.bnd_force = None
+            return
+        nb = self.bnd_pos.shape[0]
+        self.bnd_vel = np.ascontiguousarray(vel, np.float64).reshape(nb, 3).copy()
+        self.bnd_fext = np.ascontiguousarray(fext, np.float64).reshape(nb, 3).copy()
+        self.bnd_pred = np.zeros((nb, 3))
+        self.bnd_force = np.zeros((nb, 3))
+        self.P.bnd_vel = self.bnd_vel.ctypes.data
+        self.P.bnd_fext = self.bnd_fext.ctypes.data
+        self.P.bnd_inv_mass = 1.0 / float(mass)
+        self.P.bnd_pred = self.bnd_pred.ctypes.data
+        self.P.bnd_force = self.bnd_force.ctypes.data
+
     def step(self):
         S = OrcState(self.pos.ctypes.data, self.vel.ctypes.data, self.vel_half.ctypes.data,
                      self.rho.ctypes.data, self.p.ctypes.data)
@@ -509,6 +531,42 @@ class OracleSim:
         if rc != 0:
             raise RuntimeError(f"orc_step failed: {rc}")
         return self.stats
+
+
+def dem_forces(scene, pos, vel):
+    """DEM: gravity and contact force (n, 3) on each sphere at (pos, vel),
+    the force its next step applies apart from an external one (FP64)."""
+    probe = OracleSim(scene, np.array(pos, np.float64), np.array(vel, np.float64), np.array(vel, np.float64))
+    probe.step()
+    return probe.f_np.copy()
+
+
+class Coupling:
+    """The fluid-DEM coupled step (config C1) on FP64 oracle states, as the
+    library's FluidDemCoupling runs it: every sphere one boundary particle
+    of the fluid. implicit: the spheres move with the fluid's corrector
+    (set_boundary_motion) and then step with the reaction of its last
+    prediction; else the staggered exchange (the fluid steps with the
+    spheres held, then the spheres step with its reaction)."""
+
+    def __init__(self, fluid_scene, fluid, sphere_scene, spheres, implicit=True):
+        self.fs, self.fluid, self.ss, self.spheres, self.implicit = fluid_scene, fluid, sphere_scene, spheres, implicit
+
+    def step(self):
+        fl, sp = self.fluid, self.spheres
+        fl.bnd_pos[:] = sp.pos
+        fl.bnd_psi[:] = boundary_psi(self.fs, fl.bnd_pos)
+        if self.implicit:
+            fl.set_boundary_motion(sp.vel, dem_forces(self.ss, sp.pos, sp.vel), float(self.ss.mass))
+            st = fl.step()
+            force = fl.bnd_force.copy()
+        else:
+            fl.set_boundary_motion(None, None, None)
+            st = fl.step()
+            force = boundary_reaction(self.fs, fl.pos, fl.p, fl.bnd_pos)
+        sp.set_external_force(force)
+        sp.step()
+        return st, force
 
 
 def collide(obj, old_pos, pos, vel, dt):

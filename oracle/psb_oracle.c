@@ -923,6 +923,34 @@ static int step_wcsph(const orc_params* P, orc_state* S, orc_stats* st, double* 
     return 0;
 }
 
+/* Moving boundary (P->bnd_vel set): the fluid's reaction F_b on every
+ * boundary particle at pressures p, over the fluid's boundary lists at the
+ * start positions (in fluid-particle order, so the sums are deterministic),
+ * and the boundary prediction x*_b = x_b + dt (v_b + dt (F_b + f_b) / m_b).
+ * F_b = -sum_i m psi_b (p_i / rho0^2) 45 (h - d)^2 / (pi h^6) (x_i - x_b) / d,
+ * the reaction to the mirrored-pressure force (as orc_boundary_reaction). */
+static void move_boundary(const orc_params* P, const double* pos, const double* p, double* F, double* pred) {
+    const int32_t nb = P->n_bnd;
+    const double h = P->h, m = P->mass, ir0 = 1.0 / (P->rho0 * P->rho0), dt = (double)P->dt;
+    memset(F, 0, sizeof(double) * 3 * (size_t)nb);
+    for (int32_t i = 0; i < P->n; ++i) {
+        for (int32_t t = 0; t < bnd_count(P, i); ++t) {
+            const int32_t b = bnd_at(P, i, t);
+            const double dv[3] = {pos[3 * i] - P->bnd_pos[3 * b], pos[3 * i + 1] - P->bnd_pos[3 * b + 1],
+                                  pos[3 * i + 2] - P->bnd_pos[3 * b + 2]};
+            const double d = len3(dv);
+            if (!(d > 0) || d >= h) continue;
+            const double g = 45 * pow(h - d, 2) / (PI_D * pow(h, 6));
+            for (int e = 0; e < 3; ++e) F[3 * b + e] -= m * P->bnd_psi[b] * p[i] * ir0 * g * dv[e] / d;
+        }
+    }
+    for (int32_t b = 0; b < nb; ++b)
+        for (int e = 0; e < 3; ++e) {
+            const double v = P->bnd_vel[3 * b + e] + dt * (F[3 * b + e] + P->bnd_fext[3 * b + e]) * P->bnd_inv_mass;
+            pred[3 * b + e] = RND(P, P->bnd_pos[3 * b + e] + dt * RND(P, v));
+        }
+}
+
 static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double* rho_x, double* f_np, int32_t* nbr_counts) {
     if (st) memset(st, 0, sizeof(*st));
     const int32_t n = P->n;
@@ -959,6 +987,16 @@ static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double*
     }
     if (ref || !P->warm_start) memset(p, 0, sizeof(double) * (size_t)n);
     else pressure_forces(P, S->pos, rho, p, counts, list, cap, fp);   /* warm start: f_p of the initial guess at x */
+    /* moving boundary: the density passes see the predicted boundary */
+    const int moving = !ref && P->n_bnd > 0 && P->bnd_vel && P->bnd_pred && P->bnd_force;
+    orc_params Qm;
+    const orc_params* Pd = P;
+    if (moving) {
+        move_boundary(P, S->pos, p, P->bnd_force, P->bnd_pred);
+        Qm = *P;
+        Qm.bnd_pos = P->bnd_pred;
+        Pd = &Qm;
+    }
 
     const double dt = (double)P->dt;
     const int min_it = ref ? 3 : P->min_iters, max_it = ref ? 3 : P->max_iters;
@@ -976,7 +1014,7 @@ static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double*
         }
         if (k >= max_it) break;
         double* rs = (double*)malloc(sizeof(double) * (size_t)n);
-        orc_density(P, xs, counts, list, cap, !ref, rs);
+        orc_density(Pd, xs, counts, list, cap, !ref, rs);
         double err = 0.0;
         for (int32_t i = 0; i < n; ++i) {
             const double e = (rs[i] - P->rho0) / P->rho0;
@@ -993,6 +1031,7 @@ static int step_pcisph(const orc_params* P, orc_state* S, orc_stats* st, double*
          * fixed-point iteration that diverges once p dt^2/h^2 grows, as it
          * does under a 0.64 m column) */
         pressure_forces(P, ref ? xs : S->pos, rho, p, counts, list, cap, fp);
+        if (moving) move_boundary(P, S->pos, p, P->bnd_force, P->bnd_pred);
         k++;
     }
     /* config: XSPH smoothing of the committed velocity (Monaghan 1989),

@@ -55,6 +55,20 @@ typedef struct orc_params {
     /* collision objects applied after the box walls, in order (orc_collide) */
     int32_t n_coll;
     const struct orc_collider* coll;
+    /* config PCISPH, boundary particles that move with the corrector (two-
+     * way coupling solved inside the step): each one's velocity and its
+     * non-fluid force (gravity and contacts) at the step's start (n_bnd x 3)
+     * and 1/mass; bnd_vel == NULL: the boundary is static. Each prediction
+     * also predicts the boundary, x*_b = x_b + dt (v_b + dt (F_b + f_b) / m)
+     * with F_b the fluid's reaction at the current pressures (at the start
+     * positions, as the pressure force); the density passes see x*_b.
+     * Written by the step: bnd_pred the last predicted boundary positions,
+     * bnd_force the reaction F_b they were predicted with (n_bnd x 3). */
+    const double* bnd_vel;
+    const double* bnd_fext;
+    double bnd_inv_mass;
+    double* bnd_pred;
+    double* bnd_force;
 } orc_params;
 
 /* One collision object of the reference (src/Kernel/Collision/*), as its

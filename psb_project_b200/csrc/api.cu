@@ -187,6 +187,16 @@ struct psb_ctx {
     int* bnd_count = nullptr;       // per fluid slot
     int* bnd_list = nullptr;
     long long bnd_cap_alloc = 0;
+    // boundary moving with the corrector (psb_set_boundary_motion), per
+    // sorted boundary slot: velocity and non-fluid force at the step's start,
+    // the predicted positions and the reaction they were predicted with
+    bool bnd_moving = false;
+    float bnd_inv_mass = 0.f;
+    float4* bnd_vel = nullptr;
+    float4* bnd_fext = nullptr;
+    float4* bnd_pred = nullptr;
+    float4* bnd_react = nullptr;
+    long long bnd_motion_cap = 0;
     // FP64 diagnostics scratch (grown on demand)
     double* diag_rows = nullptr;
     double* diag_out = nullptr;
@@ -263,6 +273,7 @@ void free_all(psb_ctx* c) {
     cudaFree(c->hist); cudaFree(c->cell_start); cudaFree(c->cell_end); cudaFree(c->nbr_count);
     cudaFree(c->nbr_list); cudaFree(c->fnp); cudaFree(c->vs); cudaFree(c->rpc); cudaFree(c->rho_x);
     cudaFree(c->err_hist); cudaFree(c->flags); cudaFree(c->stage);
+    cudaFree(c->bnd_vel); cudaFree(c->bnd_fext); cudaFree(c->bnd_pred); cudaFree(c->bnd_react);
     cudaFree(c->feats); cudaFree(c->mlp_w); cudaFree(c->mlp_m1); cudaFree(c->mlp_m2); cudaFree(c->mlp_grad); cudaFree(c->mlp_part);
     cudaFree(c->mlp_loss); cudaFree(c->mlp_wbf); cudaFree(c->ds_X); cudaFree(c->ds_T); cudaFree(c->sel);
     cudaFree(c->iso); cudaFree(c->mc_cube); cudaFree(c->mc_edge); cudaFree(c->mc_scratch); cudaFree(c->mc_vert);
@@ -554,6 +565,15 @@ void release_graphs(psb_ctx* c);
 
 // ---- the corrector loop on the device: batches and config-profile PCISPH ---
 
+// A boundary moving with the corrector: its reaction at the committed
+// pressures rp[r] (fluid at the start positions pos[s]) and its prediction.
+void move_boundary(psb_ctx* c, cudaStream_t st, const Params& P, int s, int r) {
+    timed(c, "bnd_move", [&] {
+        psb::launch_bnd_move(st, P, c->bnd_n, c->pos[s], c->rp[r], c->cell_start, c->cell_end, c->bnd_vel, c->bnd_fext,
+                             c->bnd_inv_mass, c->bnd_pred, c->bnd_react);
+    });
+}
+
 // The corrector of a batch (or of one config-profile PCISPH scene, a batch
 // of one): k_batch_begin, then {density pass, decision, pressure-force pass}
 // until every scene has converged or max_iters passes have run. The predictions stay in xs[0]: the config profile's pressure-
@@ -564,7 +584,10 @@ int batch_corrector(psb_ctx* c, const Params& P, int s, int r, bool capture) {
     cudaStream_t st = c->stream;
     const int S = c->nscenes;
     const int max_it = c->sc.max_iters;
-    if (c->corrector == PSB_CORRECTOR_PERSISTENT && max_it > 0) {     // begins the loop itself
+    const bool moving = P.bnd_pred != nullptr;
+    // the persistent corrector has no pass that moves the boundary: a moving
+    // boundary takes the per-pass launches
+    if (c->corrector == PSB_CORRECTOR_PERSISTENT && max_it > 0 && !moving) {     // begins the loop itself
         cudaError_t e = cudaSuccess;
         timed(c, "corrector_persistent", [&] {
             e = psb::launch_corrector_persistent(st, P, c->pos[s], c->vap[s], c->fnp, c->xs[0], c->rp[r], c->rpc,
@@ -591,6 +614,9 @@ int batch_corrector(psb_ctx* c, const Params& P, int s, int r, bool capture) {
             psb::launch_pci_force_predict(bs, P, c->pos[s], c->vap[s], c->fnp, c->xs[1], c->rpc, c->nbr_count,
                                           c->nbr_list, c->xs[0], c->vs, c->rp[r]);
         });
+        // the boundary predicted with the pressures the fluid's prediction
+        // just used (once the scene has converged, the same pressures again)
+        if (moving) move_boundary(c, bs, P, s, r);
     };
     if (!capture) {
         for (int k = 0; k < max_it; ++k) {
@@ -639,6 +665,8 @@ int enqueue_loop_step(psb_ctx* c, bool capture) {
     P.n = c->n;
     if (!c->batch) P.active = c->d_active;
     const int s = c->cs, r = c->cr;
+    const bool moving = c->bnd_moving && c->bnd_n > 0;
+    if (moving) P.bnd_pred = c->bnd_pred;
     if (mode == PSB_WARM_LEARNED) {
         timed(c, "mlp_infer", [&] {
             psb::launch_mlp_infer(st, c->mlp_arch, c->n, c->feats, c->mlp_wbf, c->p_scale, c->rp[r]);
@@ -650,6 +678,7 @@ int enqueue_loop_step(psb_ctx* c, bool capture) {
         psb::launch_pci_init(st, P, c->pos[s], c->vel[s], c->vap[s], c->rp[r], c->nbr_count, c->nbr_list,
                              mode == PSB_WARM_ZERO ? 0 : 1, c->fnp, c->xs[0], c->vs);
     });
+    if (moving) move_boundary(c, st, P, s, r);     // the boundary's first prediction, with the initial pressure
     PSB_TRY(batch_corrector(c, P, s, r, capture));
     const float4* v_commit = c->vs;
     if (P.xsph_k != 0.f) {
@@ -1585,6 +1614,7 @@ int psb_set_boundary(psb_ctx* c, int32_t n_bnd, const float* pos) {
     c->P.bnd = nullptr;
     c->P.bnd_count = nullptr;
     c->P.bnd_list = nullptr;
+    c->bnd_moving = false;      // a new set is static until psb_set_boundary_motion
     if (n_bnd == 0) return cuda_check(c, cudaGetLastError(), "psb_set_boundary");
     const size_t nb = (size_t)n_bnd;
     if (!c->bnd_cs) {
@@ -1655,7 +1685,12 @@ int psb_boundary_forces(psb_ctx* c, float* force) {
     PSB_TRY(grow(c, &c->bnd_force, &c->bnd_force_cap, (long long)c->bnd_n));
     Params P = c->P;
     P.n = c->n;
-    psb::launch_bnd_reaction(st, P, c->bnd_n, c->pos[c->cs], c->rp[c->cr], c->cell_start, c->cell_end, c->bnd_force);
+    if (c->bnd_moving)      // the reaction the boundary's last prediction used
+        PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->bnd_force, c->bnd_react, sizeof(float4) * (size_t)c->bnd_n,
+                                              cudaMemcpyDeviceToDevice, st), "boundary forces"));
+    else
+        psb::launch_bnd_reaction(st, P, c->bnd_n, c->pos[c->cs], c->rp[c->cr], c->cell_start, c->cell_end,
+                                 c->bnd_force);
     std::vector<float4> f((size_t)c->bnd_n);
     std::vector<int> ids((size_t)c->bnd_n);
     PSB_TRY(cuda_check(c, cudaMemcpyAsync(f.data(), c->bnd_force, sizeof(float4) * f.size(), cudaMemcpyDeviceToHost, st),
@@ -1668,6 +1703,75 @@ int psb_boundary_forces(psb_ctx* c, float* force) {
         o[0] = f[t].x; o[1] = f[t].y; o[2] = f[t].z;
     }
     return cuda_check(c, cudaGetLastError(), "boundary forces");
+}
+
+int psb_set_boundary_motion(psb_ctx* c, const float* vel, const float* force, float mass) {
+    if (!c) return PSB_EINVAL;
+    cudaSetDevice(c->device);
+    release_graphs(c);
+    if (!vel) {
+        c->bnd_moving = false;
+        return PSB_OK;
+    }
+    if (!force || !(mass > 0.f) || !std::isfinite(mass))
+        return fail(c, PSB_EINVAL, "psb_set_boundary_motion: bad argument");
+    if (c->bnd_n == 0) return fail(c, PSB_ESTATE, "psb_set_boundary_motion: set the boundary first");
+    if (c->batch || !c->P.pci || c->P.ref || c->P.dem)
+        return fail(c, PSB_EINVAL, "psb_set_boundary_motion: config-profile PCISPH, single-scene contexts only");
+    cudaStream_t st = c->stream;
+    const int nb = c->bnd_n;
+    long long cap = c->bnd_motion_cap;
+    PSB_TRY(grow(c, &c->bnd_vel, &cap, (long long)nb));
+    cap = c->bnd_motion_cap;
+    PSB_TRY(grow(c, &c->bnd_fext, &cap, (long long)nb));
+    cap = c->bnd_motion_cap;
+    PSB_TRY(grow(c, &c->bnd_pred, &cap, (long long)nb));
+    cap = c->bnd_motion_cap;
+    PSB_TRY(grow(c, &c->bnd_react, &cap, (long long)nb));
+    c->bnd_motion_cap = cap;
+    // each array through the staging buffer into bnd_raw (input order),
+    // then into sorted boundary slots
+    float* stage = (float*)c->stage;
+    const size_t chunk = ((size_t)c->n_max * 32) / (3 * sizeof(float));
+    const float* src[2] = {vel, force};
+    float4* dst[2] = {c->bnd_vel, c->bnd_fext};
+    for (int a = 0; a < 2; ++a) {
+        for (size_t off = 0; off < (size_t)nb; off += chunk) {
+            const size_t m = std::min(chunk, (size_t)nb - off);
+            PSB_TRY(cuda_check(c, cudaMemcpyAsync(stage, src[a] + 3 * off, sizeof(float) * 3 * m, cudaMemcpyHostToDevice,
+                                                  st), "boundary motion"));
+            k_pack3<<<blocks((int)m), psb::kBlock, 0, st>>>((int)m, stage, c->bnd_pred + off);
+        }
+        psb::launch_bnd_gather4(st, nb, c->bnd_ids, c->bnd_pred, dst[a]);
+    }
+    c->bnd_inv_mass = 1.f / mass;
+    c->bnd_moving = true;
+    return cuda_check(c, cudaGetLastError(), "psb_set_boundary_motion");
+}
+
+int psb_dem_forces(psb_ctx* c, float* force) {
+    if (!c || !force) return PSB_EINVAL;
+    if (!c->P.dem) return fail(c, PSB_EINVAL, "psb_dem_forces: DEM contexts only");
+    if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_dem_forces before psb_upload");
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    PSB_TRY(build(c));
+    Params P = c->P;
+    P.n = c->n;
+    psb::launch_dem_forces(st, P, c->pos[c->cs], c->vel[c->cs], c->nbr_count, c->nbr_list, c->fnp);
+    PSB_TRY(read_flags(c));
+    std::vector<float4> f((size_t)c->n);
+    std::vector<int> ids((size_t)c->n);
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(f.data(), c->fnp, sizeof(float4) * f.size(), cudaMemcpyDeviceToHost, st),
+                       "dem forces"));
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(ids.data(), c->ids[c->cr], sizeof(int) * ids.size(), cudaMemcpyDeviceToHost,
+                                          st), "dem forces"));
+    PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "dem forces"));
+    for (int t = 0; t < c->n; ++t) {
+        float* o = force + 3 * (size_t)ids[t];
+        o[0] = f[t].x; o[1] = f[t].y; o[2] = f[t].z;
+    }
+    return cuda_check(c, cudaGetLastError(), "dem forces");
 }
 
 int psb_set_external_force(psb_ctx* c, const float* force) {

@@ -123,17 +123,13 @@ __global__ void __launch_bounds__(kBlock) k_build_bnd_nbr(Params P, const float4
     if (cnt > P.bnd_cap) atomicOr(&flags[0], 1);
 }
 
-// Boundary slot b: F_b = - sum_j m a_j^b over the fluid particles j within
-// h, a_j^b = k_grad (psi_b / m) pV_j (1-u)^2 x^_jb the mirrored-pressure
-// acceleration the boundary particle gives j (sph.cu, boundary_pressure).
-__global__ void __launch_bounds__(kBlock) k_bnd_reaction(Params P, int nb, const float4* __restrict__ fluid_pos,
-                                                         const float2* __restrict__ fluid_rp,
-                                                         const uint32_t* __restrict__ cell_start,
-                                                         const uint32_t* __restrict__ cell_end,
-                                                         float4* __restrict__ force) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
-    const float4 xb = P.bnd[b];
+// F_b = - sum_j m a_j^b over the fluid particles j within h of the
+// boundary particle at xb, a_j^b = k_grad (psi_b / m) pV_j (1-u)^2 x^_jb
+// the mirrored-pressure acceleration the boundary particle gives j (sph.cu,
+// boundary_pressure); the fluid's cells are walked around xb.
+__device__ float3 bnd_reaction_at(const Params& P, float4 xb, const float4* __restrict__ fluid_pos,
+                                  const float2* __restrict__ fluid_rp, const uint32_t* __restrict__ cell_start,
+                                  const uint32_t* __restrict__ cell_end) {
     const int nx = P.g.nx, ny = P.g.ny, nz = P.g.nz;
     int c[3];
     const float lo[3] = {P.g.gx, P.g.gy, P.g.gz};
@@ -165,10 +161,65 @@ __global__ void __launch_bounds__(kBlock) k_bnd_reaction(Params P, int nb, const
             }
         }
     const float k = -P.mass * P.k_grad * xb.w;
-    force[b] = make_float4(k * s.x, k * s.y, k * s.z, 0.f);
+    return make_float3(k * s.x, k * s.y, k * s.z);
+}
+
+// Boundary slot b's reaction at the fluid's state.
+__global__ void __launch_bounds__(kBlock) k_bnd_reaction(Params P, int nb, const float4* __restrict__ fluid_pos,
+                                                         const float2* __restrict__ fluid_rp,
+                                                         const uint32_t* __restrict__ cell_start,
+                                                         const uint32_t* __restrict__ cell_end,
+                                                         float4* __restrict__ force) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const float3 F = bnd_reaction_at(P, P.bnd[b], fluid_pos, fluid_rp, cell_start, cell_end);
+    force[b] = make_float4(F.x, F.y, F.z, 0.f);
+}
+
+// Moving boundary: the reaction at the committed pressures of the current
+// correction (the fluid at the step's start positions, as the config
+// pressure force) and the boundary's prediction with it. The velocity and
+// position updates are the DEM step's (v += (f + F) / m dt, x += v dt), so
+// the spheres' next positions are the last prediction's wherever no wall
+// projects them.
+__global__ void __launch_bounds__(kBlock) k_bnd_move(Params P, int nb, const float4* __restrict__ fluid_pos,
+                                                     const float2* __restrict__ fluid_rp,
+                                                     const uint32_t* __restrict__ cell_start,
+                                                     const uint32_t* __restrict__ cell_end,
+                                                     const float4* __restrict__ vel, const float4* __restrict__ fext,
+                                                     float inv_mass, float4* __restrict__ pred,
+                                                     float4* __restrict__ force) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const float4 xb = P.bnd[b];
+    const float3 F = bnd_reaction_at(P, xb, fluid_pos, fluid_rp, cell_start, cell_end);
+    const float4 v0 = vel[b], f = fext[b];
+    const float vx = v0.x + (f.x + F.x) * inv_mass * P.dt;
+    const float vy = v0.y + (f.y + F.y) * inv_mass * P.dt;
+    const float vz = v0.z + (f.z + F.z) * inv_mass * P.dt;
+    pred[b] = make_float4(xb.x + vx * P.dt, xb.y + vy * P.dt, xb.z + vz * P.dt, xb.w);
+    force[b] = make_float4(F.x, F.y, F.z, 0.f);
+}
+
+__global__ void k_gather4(int nb, const int* __restrict__ ids, const float4* __restrict__ src,
+                          float4* __restrict__ dst) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nb) dst[t] = src[ids[t]];
 }
 
 }  // namespace
+
+void launch_bnd_move(cudaStream_t st, const Params& P, int nb, const float4* fluid_pos, const float2* fluid_rp,
+                     const uint32_t* cell_start, const uint32_t* cell_end, const float4* vel, const float4* fext,
+                     float inv_mass, float4* pred, float4* force) {
+    if (nb > 0)
+        k_bnd_move<<<blocks_for(nb), kBlock, 0, st>>>(P, nb, fluid_pos, fluid_rp, cell_start, cell_end, vel, fext,
+                                                      inv_mass, pred, force);
+}
+
+void launch_bnd_gather4(cudaStream_t st, int nb, const int* ids, const float4* src, float4* dst) {
+    if (nb > 0) k_gather4<<<blocks_for(nb), kBlock, 0, st>>>(nb, ids, src, dst);
+}
 
 void launch_bnd_reaction(cudaStream_t st, const Params& P, int nb, const float4* fluid_pos, const float2* fluid_rp,
                          const uint32_t* cell_start, const uint32_t* cell_end, float4* force) {

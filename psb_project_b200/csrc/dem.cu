@@ -41,7 +41,9 @@ __device__ __forceinline__ void project_box(const Params& P, float3& x, float3& 
     }
 }
 
-template <bool REF>
+// STEP false: only the force without the external one (gravity and the
+// contacts), written to force; nothing moves.
+template <bool REF, bool STEP = true>
 __global__ void __launch_bounds__(kBlock) k_dem_step(Params P, const float4* __restrict__ pos,
                                                      const float4* __restrict__ vel, const int* __restrict__ counts,
                                                      const int* __restrict__ list, float4* __restrict__ pos_out,
@@ -74,6 +76,10 @@ __global__ void __launch_bounds__(kBlock) k_dem_step(Params P, const float4* __r
             f.x += s * nx; f.y += s * ny; f.z += s * nz;
         }
     });
+    if constexpr (!STEP) {
+        force[t] = make_float4(f.x, f.y, f.z, 0.f);
+        return;
+    }
     if (P.ext_force) {      // e.g. the fluid's reaction in a coupled run
         const float4 e = P.ext_force[P.slot_ids[t]];
         f.x += e.x; f.y += e.y; f.z += e.z;
@@ -100,6 +106,17 @@ void launch_dem_step(cudaStream_t st, const Params& P, const float4* pos, const 
         k_dem_step<true><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, counts, list, pos_out, vel_out, vap_out, force);
     else
         k_dem_step<false><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, counts, list, pos_out, vel_out, vap_out, force);
+}
+
+void launch_dem_forces(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
+                       const int* list, float4* force) {
+    if (P.n <= 0) return;
+    if (P.ref)
+        k_dem_step<true, false><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, counts, list, nullptr, nullptr, nullptr,
+                                                                 force);
+    else
+        k_dem_step<false, false><<<grid_of(P.n), kBlock, 0, st>>>(P, pos, vel, counts, list, nullptr, nullptr, nullptr,
+                                                                  force);
 }
 
 }  // namespace psb

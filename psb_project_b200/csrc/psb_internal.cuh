@@ -104,6 +104,11 @@ struct Params {
     const int* bnd_list;
     int bnd_cap;
     float bnd_lo[3], bnd_hi[3];     // their bounding box grown by the list cut-off
+    // Boundary particles that move with the corrector (two-way coupling
+    // solved inside the step): their predicted positions (psi_b / m in .w),
+    // which the corrector's density passes read in place of bnd; nullptr:
+    // the boundary is static.
+    const float4* bnd_pred;
     // DEM: an external force per sphere in particle-id order (N; nullptr:
     // none), found through the id of each sorted slot
     const float4* ext_force;
@@ -276,6 +281,10 @@ void launch_xsph(cudaStream_t st, const Params& P, const float4* xs, const float
                  const int* list, float4* vs_out);
 void launch_dem_step(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
                      const int* list, float4* pos_out, float4* vel_out, float4* vap_out, float4* force);
+// The force on each sphere (slot order) that the next step would apply
+// without its external force: gravity and the contacts; nothing moves.
+void launch_dem_forces(cudaStream_t st, const Params& P, const float4* pos, const float4* vel, const int* counts,
+                       const int* list, float4* force);
 
 // ---- batched scenes: the corrector loop on the device (batch.cu) ---------------
 // loop: [0] pass index, [1] continue, [2, 2 + S) corrections, [2 + S, 2 + 2S) converged,
@@ -322,6 +331,15 @@ void launch_emit_random(cudaStream_t st, int n0, int k, int type, int count, uns
 void launch_append_ids(cudaStream_t st, int n0, int k, int* ids, float2* rp);
 void launch_bnd_reaction(cudaStream_t st, const Params& P, int nb, const float4* fluid_pos, const float2* fluid_rp,
                          const uint32_t* cell_start, const uint32_t* cell_end, float4* force);
+// Moving boundary (sorted slots): the reaction F_b at the pressures in
+// fluid_rp (fluid at the step's start positions) into force, and the
+// prediction x*_b = x_b + dt (v_b + dt (F_b + f_b) / m) into pred (.w:
+// psi_b / m, from P.bnd).
+void launch_bnd_move(cudaStream_t st, const Params& P, int nb, const float4* fluid_pos, const float2* fluid_rp,
+                     const uint32_t* cell_start, const uint32_t* cell_end, const float4* vel, const float4* fext,
+                     float inv_mass, float4* pred, float4* force);
+// dst[t] = src[ids[t]] (boundary arrays from their input order to sorted slots)
+void launch_bnd_gather4(cudaStream_t st, int nb, const int* ids, const float4* src, float4* dst);
 // Per fluid slot: the boundary particles within the list cut-off, from a
 // 27-cell walk of the boundary's cell ranges (none outside P.bnd_lo/hi);
 // flags[0] is set when a slot has more than P.bnd_cap.

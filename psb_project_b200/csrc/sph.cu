@@ -267,11 +267,14 @@ __device__ __forceinline__ void ghost_pressure(const Params& P, int t, float4 xi
 // pressure term psi_b pV_i gradW_ib, as (psi_b / m) pV_i (1-u)^2 x^ inside
 // the k_grad-scaled sum. The positions are the step's start positions of
 // a static solid; x_i is the particle's current (or predicted) position.
-__device__ __forceinline__ void boundary_density(const Params& P, int t, float4 xi, Kahan& acc) {
+// bx: the boundary positions the density sees (P.bnd at the step's start
+// positions; in the corrector, P.bnd_pred where the boundary moves with it).
+__device__ __forceinline__ void boundary_density(const Params& P, int t, float4 xi, Kahan& acc,
+                                                 const float4* __restrict__ bx) {
     if (!P.bnd_count) return;
     const int cnt = min(P.bnd_count[t], P.bnd_cap);
     for_each_nbr(P.bnd_list, P.n, t, cnt, [&](const int b) {
-        const float4 xb = P.bnd[b];
+        const float4 xb = bx[b];
         const float dx = __fsub_rn(xi.x, xb.x), dy = __fsub_rn(xi.y, xb.y), dz = __fsub_rn(xi.z, xb.z);
         const float q = __fmul_rn(dist2(dx, dy, dz), P.inv_h2);
         if (q >= 1.f) return;
@@ -397,7 +400,7 @@ struct DensityX {
                                            float* __restrict__ feats) {
         if (!REF) {
             ghost_density<BATCH>(P, t, xi, pos, list, cnt, acc);
-            if (!BATCH) boundary_density(P, t, xi, acc);
+            if (!BATCH) boundary_density(P, t, xi, acc, P.bnd);
         }
         const float drho = density_deviation(P, acc);
         const float rho = __fadd_rn(P.rho0, drho);
@@ -649,7 +652,7 @@ __device__ __forceinline__ double pci_density_at(const Params& P, int t, F4 xs, 
     });
     if (!REF) {
         ghost_density<BATCH>(P, t, xi, xs, list, cnt, acc);
-        if (!BATCH) boundary_density(P, t, xi, acc);
+        if (!BATCH) boundary_density(P, t, xi, acc, P.bnd_pred ? P.bnd_pred : P.bnd);
     }
     const float drho = density_deviation(P, acc);
     const float rho = __fadd_rn(P.rho0, drho);

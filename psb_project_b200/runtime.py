@@ -43,7 +43,7 @@ EXPORTS = (
     "psb_write_xml", "psb_write_vol", "psb_write_obj", "psb_export_txt", "psb_export_xml", "psb_checkpoint_save",
     "psb_checkpoint_load", "psb_boundary_forces", "psb_set_external_force", "psb_set_colliders", "psb_emit",
     "psb_add_emitter", "psb_clear_emitters", "psb_emitter_positions", "psb_mlp_set_arch", "psb_mlp_info",
-    "psb_warm_start",
+    "psb_warm_start", "psb_set_boundary_motion", "psb_dem_forces",
 )
 MLP_SILU6, MLP_RELU7 = 0, 1   # PSB_MLP_SILU6 (the configured network), PSB_MLP_RELU7
 CORRECTOR_LAUNCHES, CORRECTOR_PERSISTENT = 0, 1   # PSB_CORRECTOR_*
@@ -183,6 +183,8 @@ def lib():
         "psb_checkpoint_load": ([P, ctypes.c_char_p], ctypes.c_int),
         "psb_boundary_forces": ([P, P], ctypes.c_int),
         "psb_set_external_force": ([P, P], ctypes.c_int),
+        "psb_set_boundary_motion": ([P, P, P, ctypes.c_float], ctypes.c_int),
+        "psb_dem_forces": ([P, P], ctypes.c_int),
         "psb_set_colliders": ([P, P, I32], ctypes.c_int),
         "psb_emit": ([P, I32, P, P, P], ctypes.c_int),
         "psb_add_emitter": ([P, P], ctypes.c_int),
@@ -512,6 +514,23 @@ class Simulation:
         self._check(lib().psb_boundary_forces(self._h, _ptr(out)), "psb_boundary_forces")
         return out
 
+    def set_boundary_motion(self, vel, force=None, mass: float = 0.0):
+        """The boundary set moves with the pressure corrector (config PCISPH):
+        velocities and non-fluid forces (n_b, 3) at the step's start and the
+        particles' mass; vel None makes it static again."""
+        if vel is None:
+            self._check(lib().psb_set_boundary_motion(self._h, None, None, 0.0), "psb_set_boundary_motion")
+            return
+        v = np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
+        f = np.ascontiguousarray(force, np.float32).reshape(-1, 3)
+        self._check(lib().psb_set_boundary_motion(self._h, _ptr(v), _ptr(f), float(mass)), "psb_set_boundary_motion")
+
+    def dem_forces(self) -> np.ndarray:
+        """DEM: gravity and contact force (n, 3) on each sphere at the current state, id order."""
+        out = np.empty((self.n, 3), np.float32)
+        self._check(lib().psb_dem_forces(self._h, _ptr(out)), "psb_dem_forces")
+        return out
+
     def set_external_force(self, force):
         """DEM: external force per sphere (n, 3) in N, id order; None removes it."""
         if force is None:
@@ -716,21 +735,39 @@ def batch_positions(scenes) -> np.ndarray:
 class FluidDemCoupling:
     """Two-way coupling of a config-profile SPH context and a DEM context
     (config C1): every DEM sphere is one boundary particle of the fluid, at
-    its centre. One coupled step: the fluid steps with the spheres' current
-    positions as its boundary; the fluid's reaction on each sphere
-    (psb_boundary_forces) becomes the spheres' external force; the spheres
-    step. The sphere positions and forces cross the host (12 B each way per
-    sphere per step)."""
+    its centre.
 
-    def __init__(self, fluid: Simulation, spheres: Simulation):
+    implicit (default): the spheres' motion is solved inside the fluid's
+    pressure corrector. The spheres' gravity and contact forces at the start
+    (psb_dem_forces) and their velocities go to the fluid
+    (psb_set_boundary_motion); every prediction of the fluid step then also
+    predicts the spheres with the fluid's reaction at that prediction's
+    pressures, so the pressures and the spheres' motion converge together.
+    The reaction of the last prediction is the spheres' external force in
+    their own step, which moves them to that prediction.
+
+    implicit=False: the staggered exchange -- the fluid steps with the
+    spheres held, then the spheres step with its reaction. Unstable once a
+    cloud of spheres as heavy as the fluid it displaces moves into the fluid
+    (the added-mass effect of explicit partitioned coupling).
+
+    Sphere positions, velocities and forces cross the host each step (12 B
+    per sphere for each)."""
+
+    def __init__(self, fluid: Simulation, spheres: Simulation, implicit: bool = True):
         self.fluid = fluid
         self.spheres = spheres
+        self.implicit = implicit
+        self.mass = float(spheres.scene.mass)
         self.last_force = None
 
     def step(self, nsteps: int = 1) -> int:
         rc = OK
         for _ in range(nsteps):
             self.fluid.set_boundary(self.spheres.read_field(FIELD_POS))
+            if self.implicit:
+                self.fluid.set_boundary_motion(self.spheres.read_field(FIELD_VEL), self.spheres.dem_forces(),
+                                               self.mass)
             rc = max(rc, self.fluid.step(1))
             self.last_force = self.fluid.boundary_forces()
             self.spheres.set_external_force(self.last_force)
