@@ -368,7 +368,9 @@ def run_ours(args):
         base = base.replace(xsph=args.xsph)
     if world > 1:       # replicas: same scene, own seed per rank
         base.blocks[0].seed = rep_.seed(base.blocks[0].seed)
-    sc = base.replace(warm_start=modes[args.warm_start])
+    # a warm start is a PCISPH corrector's; WCSPH (C0) has none
+    is_pci = base.method == P.PCISPH and base.profile == P.PROFILE_CONFIG
+    sc = base.replace(warm_start=modes[args.warm_start] if is_pci else P.WARM_ZERO)
     n = sc.n
     stream = torch.cuda.current_stream()
 

@@ -1530,15 +1530,20 @@ namespace {
 template <typename T>
 int grow(psb_ctx* c, T** p, long long* cap, long long need) {
     if (need <= *cap) return PSB_OK;
-    // geometric growth: a free and an allocation cost from a few to a few
-    // hundred milliseconds on a large context, and outputs such as a mesh
-    // grow a little with every call
+    // Geometric growth, from the device's stream-ordered pool: outputs such
+    // as a mesh grow a little with every call, and a cudaFree / cudaMalloc
+    // pair waits for the whole device -- on a 4M-particle context with its
+    // step graphs it measured 25-750 ms, against 4.4 ms for the extraction
+    // it served.
     const long long alloc = std::max(need, *cap + *cap / 2);
-    cudaStreamSynchronize(c->stream);
-    cudaFree(*p);
+    if (*p) cudaFreeAsync(*p, c->stream);
     *p = nullptr;
     *cap = 0;
-    PSB_TRY(dalloc(c, p, (size_t)alloc));
+    if (cudaMallocAsync((void**)p, sizeof(T) * (size_t)alloc, c->stream) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(c, PSB_ENOMEM, "cudaMallocAsync of " + std::to_string(sizeof(T) * (size_t)alloc) + " bytes failed");
+    }
     *cap = alloc;
     return PSB_OK;
 }
