@@ -197,6 +197,9 @@ struct psb_ctx {
     float4* bnd_pred = nullptr;
     float4* bnd_react = nullptr;
     long long bnd_motion_cap = 0;
+    // the context's own stream-ordered pool for the buffers that grow on
+    // demand (grow); it keeps freed memory for the next growth
+    cudaMemPool_t pool = nullptr;
     // FP64 diagnostics scratch (grown on demand)
     double* diag_rows = nullptr;
     double* diag_out = nullptr;
@@ -293,6 +296,7 @@ void free_all(psb_ctx* c) {
     for (auto& g : c->gexec) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     if (c->cap_main) cudaStreamDestroy(c->cap_main);
+    if (c->pool) cudaMemPoolDestroy(c->pool);
 }
 
 int validate(const psb_scene* s, std::string& why) {
@@ -1530,19 +1534,33 @@ namespace {
 template <typename T>
 int grow(psb_ctx* c, T** p, long long* cap, long long need) {
     if (need <= *cap) return PSB_OK;
-    // Geometric growth, from the device's stream-ordered pool: outputs such
-    // as a mesh grow a little with every call, and a cudaFree / cudaMalloc
-    // pair waits for the whole device -- on a 4M-particle context with its
-    // step graphs it measured 25-750 ms, against 4.4 ms for the extraction
-    // it served.
+    // Geometric growth, from the context's stream-ordered pool: outputs
+    // such as a mesh grow a little with every call, and a cudaFree /
+    // cudaMalloc pair waits for the whole device -- on a 4M-particle context
+    // with its step graphs it measured 25-750 ms, against 4.4 ms for the
+    // extraction it served.
     const long long alloc = std::max(need, *cap + *cap / 2);
+    if (!c->pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = c->device;
+        if (cudaMemPoolCreate(&c->pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            c->pool = nullptr;
+            return fail(c, PSB_ECUDA, "cudaMemPoolCreate failed");
+        }
+        uint64_t keep = UINT64_MAX;      // never hand freed memory back between growths
+        cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (*p) cudaFreeAsync(*p, c->stream);
     *p = nullptr;
     *cap = 0;
-    if (cudaMallocAsync((void**)p, sizeof(T) * (size_t)alloc, c->stream) != cudaSuccess) {
+    if (cudaMallocFromPoolAsync((void**)p, sizeof(T) * (size_t)alloc, c->pool, c->stream) != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
-        return fail(c, PSB_ENOMEM, "cudaMallocAsync of " + std::to_string(sizeof(T) * (size_t)alloc) + " bytes failed");
+        return fail(c, PSB_ENOMEM, "allocation of " + std::to_string(sizeof(T) * (size_t)alloc) + " bytes failed");
     }
     *cap = alloc;
     return PSB_OK;
