@@ -30,6 +30,7 @@ import pytest
 
 import oracle
 import psb_project_b200 as P
+from psb_project_b200 import runtime as R
 
 G = 9.81
 SETTLE = 200
@@ -256,3 +257,32 @@ def test_gpu_c1_implicit_spheres_sink_and_corrector_converges():
     assert np.isfinite(f["pos"]).all() and np.isfinite(f["vel"]).all() and np.isfinite(b["pos"]).all()
     assert b["pos"][:, 1].mean() < 16 * 0.01, b["pos"][:, 1].mean()
     assert np.count_nonzero(its >= fl.max_iters) <= 25, np.count_nonzero(its >= fl.max_iters)
+
+
+@pytest.mark.gpu
+def test_gpu_boundary_motion_and_dem_forces_refuse_bad_calls():
+    """psb_set_boundary_motion needs a boundary set, a positive finite mass
+    and a config-profile PCISPH single scene; psb_dem_forces a DEM context.
+    The refused calls change nothing: the context still steps."""
+    sc, pos, sph, centre = tank()
+    with P.Simulation(sc) as fluid, P.Simulation(sph) as ball:
+        fluid.upload(pos)
+        v = np.zeros((1, 3), np.float32)
+        with pytest.raises(R.PsbError) as e:
+            fluid.set_boundary_motion(v, v, 0.01)         # no boundary yet
+        assert e.value.status == R.ESTATE
+        fluid.set_boundary(centre[None])
+        for bad in (0.0, -1.0, float("nan"), float("inf")):
+            with pytest.raises(R.PsbError) as e:
+                fluid.set_boundary_motion(v, v, bad)
+            assert e.value.status == R.EINVAL
+        with pytest.raises(R.PsbError) as e:
+            fluid.dem_forces()                             # not a DEM context
+        assert e.value.status == R.EINVAL
+        ball.upload(centre[None])
+        f = ball.dem_forces()                              # gravity alone for one sphere
+        assert np.allclose(f, [[0.0, -G * float(sph.mass), 0.0]], rtol=1e-6)
+        fluid.set_boundary_motion(v, f, float(sph.mass))
+        fluid.set_boundary_motion(None)                    # static again
+        fluid.step(1)
+        assert fluid.stats().converged == 1
