@@ -126,7 +126,9 @@ enum {
 int psb_create(const psb_scene* scene, psb_ctx** out);
 int psb_destroy(psb_ctx* ctx);
 
-/* Launch all work on `stream` (a cudaStream_t); NULL = the legacy stream. */
+/* Launch all work on `stream` (a cudaStream_t); NULL = the legacy stream.
+ * Work later queued on the new stream waits for what the context had queued
+ * on the previous one. */
 int psb_set_stream(psb_ctx* ctx, void* stream);
 
 /* Replaces the particle upload of PCI_SPHSystem::_initialize

@@ -1147,8 +1147,21 @@ int psb_destroy(psb_ctx* c) {
 
 int psb_set_stream(psb_ctx* c, void* stream) {
     if (!c) return PSB_EINVAL;
+    cudaSetDevice(c->device);
     c->prof.resolve(c->stream);
-    c->stream = (cudaStream_t)stream;
+    const cudaStream_t next = (cudaStream_t)stream;
+    if (next != c->stream) {
+        // the new stream waits for the work already queued on the old one:
+        // the context's buffers, and the pool memory that grow() frees in
+        // stream order, may still be in use there
+        cudaEvent_t done;
+        PSB_TRY(cuda_check(c, cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "psb_set_stream"));
+        cudaError_t e = cudaEventRecord(done, c->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(next, done, 0);
+        cudaEventDestroy(done);
+        PSB_TRY(cuda_check(c, e, "psb_set_stream"));
+    }
+    c->stream = next;
     return PSB_OK;
 }
 
