@@ -133,7 +133,14 @@ int psb_set_stream(psb_ctx* ctx, void* stream);
 
 /* Replaces the particle upload of PCI_SPHSystem::_initialize
  * (PciSphSystem.cpp:68-138): host arrays, particle-id order, xyz stride 3.
- * vel/vel_half may be NULL (zero). pressure may be NULL (zero). */
+ * vel/vel_half may be NULL (zero). pressure may be NULL (zero).
+ * Asynchronous: the positions are copied on the context's stream, the other
+ * arrays on a copy stream of the context's own, and the next psb_step runs
+ * its grid, sort and neighbour build while they are still in flight (it
+ * waits for them before it first reads them). Every other call waits for
+ * them first. From pinned host memory the copies overlap that work and run
+ * after the call returns: keep the arrays unchanged until a call that waits
+ * for the device (psb_step, psb_download, psb_read_field) has returned. */
 int psb_upload(psb_ctx* ctx, int32_t n, const float* pos, const float* vel, const float* vel_half,
                const float* pressure);
 
@@ -144,7 +151,8 @@ int psb_upload_aos_f64(psb_ctx* ctx, int32_t n, const double* pos, const double*
                        int32_t on_device);
 
 /* Replaces the per-step device-to-host copies of interpolateVelocities
- * (SphSystem.cpp:337-345). Any pointer may be NULL. Blocks until done. */
+ * (SphSystem.cpp:337-345). Any pointer may be NULL. Blocks until done; the
+ * copy of each array overlaps the reordering of the next. */
 int psb_download(psb_ctx* ctx, float* pos, float* vel, float* vel_half, float* density, float* pressure);
 int psb_download_aos_f64(psb_ctx* ctx, double* pos, double* vel, double* vel_half, int32_t on_device);
 

@@ -79,7 +79,11 @@ def build(verbose: bool = False, force: bool = False) -> str:
             _run(["g++", "-O2", "-fPIC", "-ffp-contract=off", "-fopenmp", "-std=c++17"] + inc + ["-c", s, "-o", o])
         objs.append(o)
     if force or _stale(LIB, objs):
-        _run([nvcc, "-shared", "-o", LIB] + objs + ["-Xcompiler", "-fopenmp"])
+        # linked beside the library and renamed over it: a process that has
+        # the old file mapped keeps its pages instead of seeing them rewritten
+        tmp = LIB + f".{os.getpid()}.tmp"
+        _run([nvcc, "-shared", "-o", tmp] + objs + ["-Xcompiler", "-fopenmp"])
+        os.replace(tmp, LIB)
     return LIB
 
 

@@ -209,12 +209,23 @@ struct psb_ctx {
     // CUDA-graph stepping (batches)
     bool graph_on = false;
     int corrector = PSB_CORRECTOR_LAUNCHES;       // the corrector loop: kernel per pass, or one persistent launch
-    cudaGraphExec_t gexec[2] = {};                // one per state buffer parity (cs)
+    // one per state buffer parity (cs), plain [0, 1] and for the first step
+    // after an upload [2, 3] (its state gather waits for the upload's copies)
+    cudaGraphExec_t gexec[4] = {};
+    bool capture_split = false;                   // the kind of graph being captured
     int graph_sorted = -1;                        // the sort's result buffer, fixed by the key width
     int graph_n = -1;                             // the particle count the graphs were captured for
     int64_t iters_total_base = 0;                 // single scene: corrections before the loop words' sums
     cudaStream_t cap_main = nullptr;              // captures the step (the legacy stream cannot be captured)
     cudaStream_t cap_stream = nullptr;            // captures the while node's body
+    // psb_upload copies velocities and pressures on copy_st while the next
+    // step's grid and neighbour build run; ev_in marks them in place, and the
+    // step waits for it only where it gathers them (in_pending: not yet
+    // waited for on the context's stream)
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t ev_in = nullptr;
+    cudaEvent_t ev_tail = nullptr;                // orders one stream after another's queued work
+    bool in_pending = false;
     // host mirrors
     unsigned long long* h_err = nullptr;
     int* h_flags = nullptr;
@@ -257,6 +268,45 @@ void timed(psb_ctx* c, const char* name, F&& launch) {
     if (c->prof.pending.size() > 8192) c->prof.resolve(c->stream);
 }
 
+// Stream `to` runs after the work queued on `from` so far.
+int follow(psb_ctx* c, cudaStream_t from, cudaStream_t to) {
+    cudaError_t e = cudaEventRecord(c->ev_tail, from);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(to, c->ev_tail, 0);
+    return cuda_check(c, e, "stream order");
+}
+
+// The context's stream waits for the last upload's copies on the copy
+// stream. Every entry point runs it first, except psb_step, whose step waits
+// at the first kernel that reads those arrays (wait_inputs).
+void join_inputs(psb_ctx* c) {
+    if (!c->in_pending) return;
+    cudaStreamWaitEvent(c->stream, c->ev_in, 0);
+    c->in_pending = false;
+}
+
+void enter(psb_ctx* c) {
+    cudaSetDevice(c->device);
+    join_inputs(c);
+}
+
+bool capturing(cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    return cs == cudaStreamCaptureStatusActive;
+}
+
+// Inside a step, before the first kernel that reads the uploaded velocities
+// or pressures. A step being captured into a graph gets an external event
+// wait node: each launch of the graph then waits for the record of ev_in
+// that precedes it (the last upload's).
+void wait_inputs(psb_ctx* c, cudaStream_t st) {
+    if (capturing(st)) {
+        cudaStreamWaitEvent(st, c->ev_in, cudaEventWaitExternal);
+        return;
+    }
+    join_inputs(c);
+}
+
 template <typename T>
 int dalloc(psb_ctx* c, T** p, size_t count) {
     *p = nullptr;
@@ -296,6 +346,9 @@ void free_all(psb_ctx* c) {
     for (auto& g : c->gexec) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     if (c->cap_main) cudaStreamDestroy(c->cap_main);
+    if (c->copy_st) cudaStreamDestroy(c->copy_st);
+    if (c->ev_in) cudaEventDestroy(c->ev_in);
+    if (c->ev_tail) cudaEventDestroy(c->ev_tail);
     if (c->pool) cudaMemPoolDestroy(c->pool);
 }
 
@@ -455,6 +508,14 @@ __global__ void k_init_ids(int n, const float* __restrict__ pres, int* __restric
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) { ids[i] = i; rp[i] = make_float2(0.f, pres ? pres[i] : 0.f); }
 }
+__global__ void k_iota(int n, int* __restrict__ ids) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) ids[i] = i;
+}
+__global__ void k_init_rp(int n, const float* __restrict__ pres, float2* __restrict__ rp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) rp[i] = make_float2(0.f, pres ? pres[i] : 0.f);
+}
 __global__ void k_scatter3(int n, const int* __restrict__ ids, const float4* __restrict__ src, float* __restrict__ dst) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) { const int id = ids[t]; const float4 v = src[t]; dst[3 * id] = v.x; dst[3 * id + 1] = v.y; dst[3 * id + 2] = v.z; }
@@ -511,12 +572,32 @@ int build(psb_ctx* c, bool keep_p = false, bool features = false) {
     });
     int res = 0;
     timed(c, "radix_sort", [&] { res = psb::radix_sort(st, n, c->key_bits, c->keys, c->vals, c->hist, c->hist_blocks); });
-    const int ns = c->cs ^ 1, nr = c->cr ^ 1;
-    timed(c, "reorder", [&] {
-        psb::launch_reorder(st, n, c->keys[res], c->vals[res], c->pos[c->cs], c->vel[c->cs], c->vap[c->cs], c->rp[c->cr],
-                            c->ids[c->cr], c->pos[ns], c->vel[ns], c->vap[ns], c->rp[nr], c->ids[nr], c->cell_start,
-                            c->cell_end);
-    });
+    const int os = c->cs, orr = c->cr, ns = os ^ 1, nr = orr ^ 1;
+    // The first step after an upload gathers the positions first and the
+    // rest of the state after its neighbour build, once the upload's copies
+    // of it are in: they overlap the grid and the build. Other steps gather
+    // everything in one launch.
+    const bool split = capturing(st) ? c->capture_split : c->in_pending;
+    if (split) {
+        timed(c, "reorder", [&] {
+            psb::launch_reorder_pos(st, n, c->keys[res], c->vals[res], c->pos[os], c->ids[orr], c->pos[ns], c->ids[nr],
+                                    c->cell_start, c->cell_end);
+        });
+    } else {
+        timed(c, "reorder", [&] {
+            psb::launch_reorder(st, n, c->keys[res], c->vals[res], c->pos[os], c->vel[os], c->vap[os], c->rp[orr],
+                                c->ids[orr], c->pos[ns], c->vel[ns], c->vap[ns], c->rp[nr], c->ids[nr], c->cell_start,
+                                c->cell_end);
+        });
+    }
+    auto reorder_state = [&] {
+        if (!split) return;
+        wait_inputs(c, st);
+        timed(c, "reorder_state", [&] {
+            psb::launch_reorder_state(st, n, c->vals[res], c->vel[os], c->vap[os], c->rp[orr], c->vel[ns], c->vap[ns],
+                                      c->rp[nr]);
+        });
+    };
     c->cs = ns;
     c->cr = nr;
     c->sorted = res;
@@ -532,6 +613,7 @@ int build(psb_ctx* c, bool keep_p = false, bool features = false) {
     float* feats = features ? c->feats : nullptr;
     const int nfeat = psb::mlp_inputs(c->mlp_arch);
     if (fused_density(c, P)) {
+        reorder_state();
         timed(c, "build_nbr", [&] {
             psb::launch_build_density(st, P, c->pos[c->cs], c->vel[c->cs], c->keys[res], c->cell_start, c->cell_end,
                                       c->nbr_count, c->nbr_list, c->flags, c->rp[c->cr], c->rho_x, zero_p, c->p_scale,
@@ -542,6 +624,7 @@ int build(psb_ctx* c, bool keep_p = false, bool features = false) {
             psb::launch_build_nbr(st, P, c->pos[c->cs], c->keys[res], c->cell_start, c->cell_end, c->nbr_count,
                                   c->nbr_list, c->flags);
         });
+        reorder_state();
         if (!P.dem)
             timed(c, "density_x", [&] {
                 psb::launch_density_x(st, P, c->pos[c->cs], c->vel[c->cs], c->nbr_count, c->nbr_list, c->rp[c->cr],
@@ -699,8 +782,8 @@ int enqueue_loop_step(psb_ctx* c, bool capture) {
 // Captures the step from the current state parity into c->gexec[c->cs], on
 // the context's own capture stream (nothing runs; the graph is launched on
 // the caller's stream, which may be the legacy one).
-int capture_loop_step(psb_ctx* c) {
-    const int p = c->cs;
+int capture_loop_step(psb_ctx* c, int p) {
+    c->capture_split = p >= 2;
     cudaStream_t user = c->stream;
     cudaStream_t st = c->cap_main;
     PSB_TRY(cuda_check(c, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture"));
@@ -735,8 +818,10 @@ int step_loop(psb_ctx* c, bool last) {
     const bool graph = c->graph_on && !collect && !c->prof.on && prev_n == c->n;
     if (graph) {
         if (c->graph_n != c->n) release_graphs(c);       // emissions changed the particle count
-        if (!c->gexec[c->cs]) PSB_TRY(capture_loop_step(c));
-        PSB_TRY(cuda_check(c, cudaGraphLaunch(c->gexec[c->cs], st), "graph launch"));
+        const int gi = c->cs + (c->in_pending ? 2 : 0);
+        if (!c->gexec[gi]) PSB_TRY(capture_loop_step(c, gi));
+        PSB_TRY(cuda_check(c, cudaGraphLaunch(c->gexec[gi], st), "graph launch"));
+        c->in_pending = false;        // the graph waits for the upload's copies itself
         // what build() records of the step it enqueues
         c->sorted = c->graph_sorted;
         c->sorted_n = c->n;
@@ -956,7 +1041,8 @@ int create_impl(const psb_scene* scene, size_t ncells, psb_ctx** out) {
     if (!rc) rc = dalloc(c, &c->rho_x, n);
     if (!rc) rc = dalloc(c, &c->err_hist, PSB_MAX_ITERS + 1);
     if (!rc) rc = dalloc(c, &c->flags, 8);
-    if (!rc) rc = dalloc(c, (char**)&c->stage, n * 32);
+    // uploads and downloads stage every array at once: 3 x 12 + 2 x 4 bytes
+    if (!rc) rc = dalloc(c, (char**)&c->stage, n * 48);
     if (!rc) rc = dalloc(c, &c->feats, n * 8);
     if (!rc) rc = dalloc(c, &c->mlp_w, psb::kMlpParams);
     if (!rc) rc = dalloc(c, &c->mlp_m1, psb::kMlpParams);
@@ -1031,6 +1117,11 @@ int alloc_loop(psb_ctx* c, int S) {
     if (!rc) rc = cuda_check(c, cudaMemset(c->d_err_sh, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S), "err");
     if (!rc) rc = cuda_check(c, cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking), "stream");
     if (!rc) rc = cuda_check(c, cudaStreamCreateWithFlags(&c->cap_main, cudaStreamNonBlocking), "stream");
+    if (!rc) rc = cuda_check(c, cudaStreamCreateWithFlags(&c->copy_st, cudaStreamNonBlocking), "stream");
+    if (!rc) rc = cuda_check(c, cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming), "event");
+    if (!rc) rc = cuda_check(c, cudaEventCreateWithFlags(&c->ev_tail, cudaEventDisableTiming), "event");
+    // a step's graph waits on ev_in: give it a first, completed record
+    if (!rc) rc = cuda_check(c, cudaEventRecord(c->ev_in, c->copy_st), "event");
     if (!rc) {
         std::memset(c->h_loop, 0, sizeof(int) * (2 + 4 * (size_t)S));
         std::memset(c->h_err_sh, 0, sizeof(unsigned long long) * (PSB_MAX_ITERS + 1) * S);
@@ -1140,6 +1231,7 @@ int psb_destroy(psb_ctx* c) {
     if (!c) return PSB_EINVAL;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    if (c->copy_st) cudaStreamSynchronize(c->copy_st);
     free_all(c);
     delete c;
     return PSB_OK;
@@ -1147,7 +1239,7 @@ int psb_destroy(psb_ctx* c) {
 
 int psb_set_stream(psb_ctx* c, void* stream) {
     if (!c) return PSB_EINVAL;
-    cudaSetDevice(c->device);
+    enter(c);
     c->prof.resolve(c->stream);
     const cudaStream_t next = (cudaStream_t)stream;
     if (next != c->stream) {
@@ -1215,18 +1307,31 @@ static int upload_common(psb_ctx* c, int32_t n) {
 int psb_upload(psb_ctx* c, int32_t n, const float* pos, const float* vel, const float* vel_half, const float* pressure) {
     if (!c || n <= 0 || n > c->n_max || !pos) return fail(c, PSB_EINVAL, "psb_upload: bad n or NULL pos");
     if (c->batch && n != c->n_max) return fail(c, PSB_EINVAL, "psb_upload: a batch takes all its scenes' particles");
-    cudaSetDevice(c->device);
+    enter(c);
     upload_common(c, n);
-    cudaStream_t st = c->stream;
+    cudaStream_t st = c->stream, cp = c->copy_st;
     float* stage = (float*)c->stage;
-    const size_t b3 = sizeof(float) * 3 * (size_t)n;
-    struct { const float* src; float4* dst; } parts[3] = {{pos, c->pos[0]}, {vel, c->vel[0]}, {vel_half, c->vap[0]}};
+    const size_t n3 = 3 * (size_t)n;
+    // positions and ids on the context's stream: all that the next step's
+    // grid and neighbour build read
+    PSB_TRY(cuda_check(c, cudaMemcpyAsync(stage, pos, sizeof(float) * n3, cudaMemcpyHostToDevice, st), "upload"));
+    k_pack3<<<blocks(n), psb::kBlock, 0, st>>>(n, stage, c->pos[0]);
+    k_iota<<<blocks(n), psb::kBlock, 0, st>>>(n, c->ids[0]);
+    // the rest on the copy stream, behind the positions' copy (and whatever
+    // still reads the state buffers or the stage); the step gathers them
+    // after its neighbour build, waiting on ev_in
+    PSB_TRY(follow(c, st, cp));
+    float* region = stage + n3;
+    struct { const float* src; float4* dst; } parts[2] = {{vel, c->vel[0]}, {vel_half, c->vap[0]}};
     for (auto& p : parts) {
-        if (p.src) PSB_TRY(cuda_check(c, cudaMemcpyAsync(stage, p.src, b3, cudaMemcpyHostToDevice, st), "upload"));
-        k_pack3<<<blocks(n), psb::kBlock, 0, st>>>(n, p.src ? stage : nullptr, p.dst);
+        if (p.src) PSB_TRY(cuda_check(c, cudaMemcpyAsync(region, p.src, sizeof(float) * n3, cudaMemcpyHostToDevice, cp), "upload"));
+        k_pack3<<<blocks(n), psb::kBlock, 0, cp>>>(n, p.src ? region : nullptr, p.dst);
+        region += n3;
     }
-    if (pressure) PSB_TRY(cuda_check(c, cudaMemcpyAsync(stage, pressure, sizeof(float) * n, cudaMemcpyHostToDevice, st), "upload"));
-    k_init_ids<<<blocks(n), psb::kBlock, 0, st>>>(n, pressure ? stage : nullptr, c->ids[0], c->rp[0]);
+    if (pressure) PSB_TRY(cuda_check(c, cudaMemcpyAsync(region, pressure, sizeof(float) * n, cudaMemcpyHostToDevice, cp), "upload"));
+    k_init_rp<<<blocks(n), psb::kBlock, 0, cp>>>(n, pressure ? region : nullptr, c->rp[0]);
+    PSB_TRY(cuda_check(c, cudaEventRecord(c->ev_in, cp), "upload"));
+    c->in_pending = true;
     return cuda_check(c, cudaGetLastError(), "upload");
 }
 
@@ -1234,7 +1339,7 @@ int psb_upload_aos_f64(psb_ctx* c, int32_t n, const double* pos, const double* v
                        int32_t on_device) {
     if (!c || n <= 0 || n > c->n_max || !pos) return fail(c, PSB_EINVAL, "psb_upload_aos_f64: bad n or NULL pos");
     if (c->batch && n != c->n_max) return fail(c, PSB_EINVAL, "psb_upload_aos_f64: a batch takes all its scenes' particles");
-    cudaSetDevice(c->device);
+    enter(c);
     upload_common(c, n);
     cudaStream_t st = c->stream;
     double* stage = (double*)c->stage;
@@ -1258,31 +1363,39 @@ int psb_upload_aos_f64(psb_ctx* c, int32_t n, const double* pos, const double* v
 int psb_download(psb_ctx* c, float* pos, float* vel, float* vel_half, float* density, float* pressure) {
     if (!c) return PSB_EINVAL;
     if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_download before psb_upload");
-    cudaSetDevice(c->device);
-    cudaStream_t st = c->stream;
+    enter(c);
+    cudaStream_t st = c->stream, cp = c->copy_st;
     const int n = c->n;
-    float* stage = (float*)c->stage;
+    // each array is put in id order into a stage region of its own on the
+    // context's stream and copied out on the copy stream, so the copy of
+    // one overlaps the reordering of the next
+    float* region = (float*)c->stage;
     struct { float* dst; const float4* src; } v3[3] = {{pos, c->pos[c->cs]}, {vel, c->vel[c->cs]}, {vel_half, c->vap[c->cs]}};
     for (auto& p : v3) {
         if (!p.dst) continue;
-        k_scatter3<<<blocks(n), psb::kBlock, 0, st>>>(n, c->ids[c->cr], p.src, stage);
-        PSB_TRY(cuda_check(c, cudaMemcpyAsync(p.dst, stage, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st), "download"));
-        PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "download"));
+        k_scatter3<<<blocks(n), psb::kBlock, 0, st>>>(n, c->ids[c->cr], p.src, region);
+        PSB_TRY(follow(c, st, cp));
+        PSB_TRY(cuda_check(c, cudaMemcpyAsync(p.dst, region, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, cp), "download"));
+        region += 3 * (size_t)n;
     }
     struct { float* dst; int comp; } v1[2] = {{density, 0}, {pressure, 1}};
     for (auto& p : v1) {
         if (!p.dst) continue;
-        k_scatter_rp<<<blocks(n), psb::kBlock, 0, st>>>(n, c->ids[c->cr], c->rp[c->cr], p.comp, stage);
-        PSB_TRY(cuda_check(c, cudaMemcpyAsync(p.dst, stage, sizeof(float) * n, cudaMemcpyDeviceToHost, st), "download"));
-        PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "download"));
+        k_scatter_rp<<<blocks(n), psb::kBlock, 0, st>>>(n, c->ids[c->cr], c->rp[c->cr], p.comp, region);
+        PSB_TRY(follow(c, st, cp));
+        PSB_TRY(cuda_check(c, cudaMemcpyAsync(p.dst, region, sizeof(float) * n, cudaMemcpyDeviceToHost, cp), "download"));
+        region += n;
     }
-    return cuda_check(c, cudaGetLastError(), "download");
+    PSB_TRY(cuda_check(c, cudaGetLastError(), "download"));
+    // the context's stream also follows the copies (its next work may reuse the stage)
+    PSB_TRY(follow(c, cp, st));
+    return cuda_check(c, cudaStreamSynchronize(cp), "download");
 }
 
 int psb_download_aos_f64(psb_ctx* c, double* pos, double* vel, double* vel_half, int32_t on_device) {
     if (!c) return PSB_EINVAL;
     if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_download before psb_upload");
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     const int n = c->n;
     double* stage = (double*)c->stage;
@@ -1304,6 +1417,9 @@ int psb_step(psb_ctx* c, int32_t nsteps) {
     if (!c || nsteps < 0) return fail(c, PSB_EINVAL, "psb_step: bad argument");
     if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_step before psb_upload");
     cudaSetDevice(c->device);
+    // emitters write the state before the step's build, which otherwise
+    // waits for the last upload's copies itself
+    if (!c->emitters.empty()) join_inputs(c);
     int status = PSB_OK;
     for (int i = 0; i < nsteps; ++i) {
         const int rc = step_once(c, i == nsteps - 1);
@@ -1317,7 +1433,7 @@ int psb_step(psb_ctx* c, int32_t nsteps) {
 int psb_mlp_set_arch(psb_ctx* c, int32_t arch) {
     if (!c) return PSB_EINVAL;
     if (arch != PSB_MLP_SILU6 && arch != PSB_MLP_RELU7) return fail(c, PSB_EINVAL, "psb_mlp_set_arch: unknown network");
-    cudaSetDevice(c->device);
+    enter(c);
     PSB_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "arch"));
     c->mlp_arch = arch;
     c->mlp_set = false;          // the weights of the other network mean nothing here
@@ -1338,7 +1454,7 @@ int psb_mlp_info(const psb_ctx* c, int32_t* arch, int32_t* n_inputs, int32_t* n_
 
 int psb_mlp_set_weights(psb_ctx* c, const float* w) {
     if (!c || !w) return PSB_EINVAL;
-    cudaSetDevice(c->device);
+    enter(c);
     const int np = psb::mlp_params(c->mlp_arch);
     PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->mlp_w, w, sizeof(float) * np, cudaMemcpyHostToDevice, c->stream), "weights"));
     cudaMemsetAsync(c->mlp_m1, 0, sizeof(float) * psb::kMlpParams, c->stream);
@@ -1352,7 +1468,7 @@ int psb_mlp_set_weights(psb_ctx* c, const float* w) {
 
 int psb_mlp_get_weights(psb_ctx* c, float* w) {
     if (!c || !w) return PSB_EINVAL;
-    cudaSetDevice(c->device);
+    enter(c);
     PSB_TRY(cuda_check(c, cudaMemcpyAsync(w, c->mlp_w, sizeof(float) * psb::mlp_params(c->mlp_arch), cudaMemcpyDeviceToHost,
                                           c->stream), "weights"));
     return cuda_check(c, cudaStreamSynchronize(c->stream), "weights");
@@ -1360,7 +1476,7 @@ int psb_mlp_get_weights(psb_ctx* c, float* w) {
 
 int psb_mlp_collect(psb_ctx* c, int32_t stride, int64_t capacity) {
     if (!c || stride < 0 || (stride > 0 && capacity <= 0)) return fail(c, PSB_EINVAL, "psb_mlp_collect: bad argument");
-    cudaSetDevice(c->device);
+    enter(c);
     c->collect_stride = stride;
     if (stride == 0) return PSB_OK;
     if ((uint64_t)capacity != c->ds_cap) {
@@ -1379,7 +1495,7 @@ int psb_mlp_collect(psb_ctx* c, int32_t stride, int64_t capacity) {
 
 int psb_mlp_dataset(psb_ctx* c, int64_t* rows, float* X, float* T) {
     if (!c || !rows) return PSB_EINVAL;
-    cudaSetDevice(c->device);
+    enter(c);
     const uint64_t r = c->ds_rows < c->ds_cap ? c->ds_rows : c->ds_cap;
     *rows = (int64_t)r;
     if (X && r) PSB_TRY(cuda_check(c, cudaMemcpyAsync(X, c->ds_X, sizeof(float) * 8 * r, cudaMemcpyDeviceToHost, c->stream), "dataset"));
@@ -1392,7 +1508,7 @@ int psb_mlp_train(psb_ctx* c, int32_t iters, int32_t batch, float lr, uint64_t s
     const uint64_t rows = c->ds_rows < c->ds_cap ? c->ds_rows : c->ds_cap;
     if (rows == 0) return fail(c, PSB_ESTATE, "psb_mlp_train: no recorded data");
     if (!c->mlp_set) return fail(c, PSB_ESTATE, "psb_mlp_train: set initial weights first");
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     if (batch > c->sel_cap) {
         cudaStreamSynchronize(st);
@@ -1421,7 +1537,7 @@ int psb_mlp_train(psb_ctx* c, int32_t iters, int32_t batch, float lr, uint64_t s
 
 static int mlp_host_call(psb_ctx* c, const float* X, const float* T, int32_t n, float* y, float* loss, float* grad) {
     if (!c || !X || n <= 0) return fail(c, PSB_EINVAL, "psb_mlp: bad argument");
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     float *dX = nullptr, *dT = nullptr, *dy = nullptr;
     int rc = dalloc(c, &dX, (size_t)n * 8);
@@ -1461,7 +1577,7 @@ int psb_presolve(psb_ctx* c, int32_t iters) {
     if (!c || iters < 0) return fail(c, PSB_EINVAL, "psb_presolve: bad argument");
     if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_presolve before psb_upload");
     if (!c->P.pci || c->P.ref) return fail(c, PSB_EINVAL, "psb_presolve: config-profile PCISPH scenes only");
-    cudaSetDevice(c->device);
+    enter(c);
     PSB_TRY(build(c, /*keep_p=*/true));
     cudaStream_t st = c->stream;
     Params P = c->P;
@@ -1496,7 +1612,7 @@ int psb_presolve(psb_ctx* c, int32_t iters) {
 int psb_build_neighbors(psb_ctx* c) {
     if (!c) return PSB_EINVAL;
     if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_build_neighbors before psb_upload");
-    cudaSetDevice(c->device);
+    enter(c);
     PSB_TRY(build(c));
     return read_flags(c);
 }
@@ -1506,7 +1622,7 @@ int psb_warm_start(psb_ctx* c, float* features, float* pressure) {
     if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_warm_start before psb_upload");
     if (c->batch || !c->P.pci || c->P.ref)
         return fail(c, PSB_EINVAL, "psb_warm_start: single config-profile PCISPH scenes only");
-    cudaSetDevice(c->device);
+    enter(c);
     const int mode = c->sc.warm_start;
     if (mode == PSB_WARM_LEARNED && !c->mlp_set) return fail(c, PSB_ESTATE, "psb_warm_start: no network weights set");
     PSB_TRY(build(c, /*keep_p=*/true, /*features=*/true));
@@ -1621,7 +1737,7 @@ int iso_on_device(psb_ctx* c, const psb_iso_grid* g, double level, psb::IsoParam
         Q.inv_r2 = 1.0 / (h * h);
         Q.k_colour = 315.0 * c->sc.mass / (64.0 * 3.14159265358979323846 * h * h * h);
     }
-    cudaSetDevice(c->device);
+    enter(c);
     PSB_TRY(build(c, /*keep_p=*/true));
     PSB_TRY(grow(c, &c->iso, &c->iso_cap, nn));
     Params P = c->P;
@@ -1640,7 +1756,7 @@ int psb_set_boundary(psb_ctx* c, int32_t n_bnd, const float* pos) {
     if (!c || n_bnd < 0 || (n_bnd > 0 && !pos)) return fail(c, PSB_EINVAL, "psb_set_boundary: bad argument");
     if (n_bnd > 0 && (c->P.ref || c->P.dem || c->batch))
         return fail(c, PSB_EINVAL, "psb_set_boundary: config-profile SPH, single-scene contexts only");
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     release_graphs(c);
     if (c->bnd_n > 0) {      // forget the previous set: clear its cells
@@ -1716,7 +1832,7 @@ int psb_boundary_forces(psb_ctx* c, float* force) {
     if (!c || !force) return PSB_EINVAL;
     if (c->bnd_n == 0) return fail(c, PSB_ESTATE, "psb_boundary_forces: no boundary set");
     if (!c->built) return fail(c, PSB_ESTATE, "psb_boundary_forces: take a step first");
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     PSB_TRY(grow(c, &c->bnd_force, &c->bnd_force_cap, (long long)c->bnd_n));
     Params P = c->P;
@@ -1743,7 +1859,7 @@ int psb_boundary_forces(psb_ctx* c, float* force) {
 
 int psb_set_boundary_motion(psb_ctx* c, const float* vel, const float* force, float mass) {
     if (!c) return PSB_EINVAL;
-    cudaSetDevice(c->device);
+    enter(c);
     release_graphs(c);
     if (!vel) {
         c->bnd_moving = false;
@@ -1789,7 +1905,7 @@ int psb_dem_forces(psb_ctx* c, float* force) {
     if (!c || !force) return PSB_EINVAL;
     if (!c->P.dem) return fail(c, PSB_EINVAL, "psb_dem_forces: DEM contexts only");
     if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_dem_forces before psb_upload");
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     PSB_TRY(build(c));
     Params P = c->P;
@@ -1813,7 +1929,7 @@ int psb_dem_forces(psb_ctx* c, float* force) {
 int psb_set_external_force(psb_ctx* c, const float* force) {
     if (!c) return PSB_EINVAL;
     if (!c->P.dem) return fail(c, PSB_EINVAL, "psb_set_external_force: DEM contexts only");
-    cudaSetDevice(c->device);
+    enter(c);
     release_graphs(c);
     if (!force) {
         c->P.ext_force = nullptr;
@@ -1883,7 +1999,7 @@ int psb_emit(psb_ctx* c, int32_t k, const float* pos, const float* vel, const fl
     if ((int64_t)c->n + k > (int64_t)c->n_max)
         return fail(c, PSB_EINVAL, "psb_emit: " + std::to_string(k) + " particles, " +
                                        std::to_string(c->n_max - c->n) + " free of the context's capacity");
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     float* stage = (float*)c->stage;
     const int n0 = c->n;
@@ -1929,7 +2045,7 @@ int psb_add_emitter(psb_ctx* c, const psb_emitter* e) {
     if (g == PSB_ENOMEM) return fail(c, PSB_ENOMEM, "psb_add_emitter: host memory for the emission");
     if (g != PSB_OK) return fail(c, PSB_EINVAL, "psb_add_emitter: bad type, count or faces");
     const int64_t per = (int64_t)(xyz.size() / 3);
-    cudaSetDevice(c->device);
+    enter(c);
     EmitterRec r;
     r.e = *e;
     r.e.data = nullptr;
@@ -1958,7 +2074,7 @@ int psb_add_emitter(psb_ctx* c, const psb_emitter* e) {
 
 int psb_clear_emitters(psb_ctx* c) {
     if (!c) return PSB_EINVAL;
-    cudaSetDevice(c->device);
+    enter(c);
     PSB_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "emitters"));
     for (auto& e : c->emitters) { cudaFree(e.d_list); cudaFree(e.d_faces); }
     c->emitters.clear();
@@ -1974,7 +2090,7 @@ int psb_set_colliders(psb_ctx* c, const psb_collider* objs, int32_t n) {
         const std::string why = collider_problem(objs[i]);
         if (!why.empty()) return fail(c, PSB_EINVAL, "psb_set_colliders: object " + std::to_string(i) + ": " + why);
     }
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     release_graphs(c);
     PSB_TRY(cuda_check(c, cudaStreamSynchronize(st), "colliders"));   // no step still reads the old list
@@ -2030,7 +2146,7 @@ int psb_set_colliders(psb_ctx* c, const psb_collider* objs, int32_t n) {
 int psb_boundary_psi(psb_ctx* c, float* psi) {
     if (!c || !psi) return PSB_EINVAL;
     if (c->bnd_n == 0) return fail(c, PSB_ESTATE, "psb_boundary_psi: no boundary set");
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     std::vector<float> w((size_t)c->bnd_n);
     std::vector<int> ids((size_t)c->bnd_n);
@@ -2047,7 +2163,7 @@ int psb_diagnostics(psb_ctx* c, psb_diag* out, int32_t n_out) {
     if (n_out != 1 && n_out != c->nscenes) return fail(c, PSB_EINVAL, "psb_diagnostics: n_out is 1 or the scene count");
     if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_diagnostics before psb_upload");
     static_assert(sizeof(psb_diag) == sizeof(double) * psb::kDiagTerms, "psb_diag holds the diagnostic terms");
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     PSB_TRY(grow(c, &c->diag_rows, &c->diag_rows_cap, (long long)psb::diag_rows(c->n) * psb::kDiagTerms));
     PSB_TRY(grow(c, &c->diag_out, &c->diag_out_cap, (long long)n_out * psb::kDiagTerms));
@@ -2132,7 +2248,7 @@ int psb_extract_surface(psb_ctx* c, const psb_iso_grid* g, double level, float* 
 int psb_read_field(psb_ctx* c, int32_t field, void* dst, size_t bytes) {
     if (!c || !dst) return PSB_EINVAL;
     if (!c->uploaded) return fail(c, PSB_ESTATE, "psb_read_field before psb_upload");
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     const int n = c->n;
     const int* ids = c->ids[c->cr];
@@ -2200,7 +2316,7 @@ int psb_batch_stats(psb_ctx* c, int32_t* iters, int32_t* converged, double* err_
         if (unconverged_steps) unconverged_steps[0] = -1;
         return PSB_OK;
     }
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     PSB_TRY(cuda_check(c, cudaMemcpyAsync(c->h_loop, c->d_loop, sizeof(int) * (2 + 4 * (size_t)S), cudaMemcpyDeviceToHost,
                                           st), "loop"));
@@ -2227,7 +2343,7 @@ int psb_set_graph(psb_ctx* c, int32_t on) {
     if (!c) return PSB_EINVAL;
     if (!c->batch && !(c->P.pci && !c->P.ref))
         return fail(c, PSB_EINVAL, "psb_set_graph: batches and config-profile PCISPH scenes only");
-    cudaSetDevice(c->device);
+    enter(c);
     if (!on) release_graphs(c);
     c->graph_on = on != 0;
     return PSB_OK;
@@ -2239,7 +2355,7 @@ int psb_set_corrector(psb_ctx* c, int32_t mode) {
         return fail(c, PSB_EINVAL, "psb_set_corrector: batches and config-profile PCISPH scenes only");
     if (mode != PSB_CORRECTOR_LAUNCHES && mode != PSB_CORRECTOR_PERSISTENT)
         return fail(c, PSB_EINVAL, "psb_set_corrector: unknown mode " + std::to_string(mode));
-    cudaSetDevice(c->device);
+    enter(c);
     if (mode == PSB_CORRECTOR_PERSISTENT) {
         int coop = 0;
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
@@ -2258,7 +2374,7 @@ int psb_tune_set(psb_ctx* c, const psb_tune* t) {
         !block_ok(t->init_block) || !block_ok(t->pci_density_block) || !block_ok(t->force_block) ||
         !block_ok(t->xsph_block) || t->nbr_schedule < 0 || t->nbr_schedule > 2)
         return fail(c, PSB_EINVAL, "psb_tune_set: block sizes 0/128/256/512, schedule 0 or 1, bucket 0..62");
-    cudaSetDevice(c->device);
+    enter(c);
     c->tune_table[t->bucket] = *t;
     release_graphs(c);
     apply_tune(c);
@@ -2278,7 +2394,7 @@ int psb_autotune(psb_ctx* c, int32_t trials, psb_tune* out) {
     if (!c || trials < 1 || trials > 1000) return fail(c, PSB_EINVAL, "psb_autotune: trials in 1..1000");
     if (!c->uploaded || !c->built || c->sorted < 0 || c->stats.steps < 1)
         return fail(c, PSB_ESTATE, "psb_autotune: take a step first");
-    cudaSetDevice(c->device);
+    enter(c);
     cudaStream_t st = c->stream;
     const int n = c->n;
     const int s = c->cs, r = c->cr;

@@ -191,6 +191,36 @@ __global__ void k_reorder(int n, const uint32_t* __restrict__ keys, const uint32
     if (t == n - 1 || keys[t + 1] != k) cell_end[k] = (uint32_t)t + 1u;
 }
 
+// The same in two launches, for the first step after an upload: positions,
+// ids and cell ranges (all that the neighbour build reads) here, the rest
+// in k_reorder_state once the upload's copies of it are in.
+__global__ void k_reorder_pos(int n, const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                              const float4* __restrict__ pos, const int* __restrict__ ids, float4* __restrict__ pos2,
+                              int* __restrict__ ids2, uint32_t* __restrict__ cell_start,
+                              uint32_t* __restrict__ cell_end) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t s = vals[t];
+    pos2[t] = pos[s];
+    ids2[t] = ids[s];
+    const uint32_t k = keys[t];
+    if (t == 0 || keys[t - 1] != k) cell_start[k] = (uint32_t)t;
+    if (t == n - 1 || keys[t + 1] != k) cell_end[k] = (uint32_t)t + 1u;
+}
+
+// Gathers velocities, half-step velocities and (density, pressure) into
+// sorted order.
+__global__ void k_reorder_state(int n, const uint32_t* __restrict__ vals, const float4* __restrict__ vel,
+                                const float4* __restrict__ vap, const float2* __restrict__ rp,
+                                float4* __restrict__ vel2, float4* __restrict__ vap2, float2* __restrict__ rp2) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t s = vals[t];
+    vel2[t] = vel[s];
+    vap2[t] = vap[s];
+    rp2[t] = rp[s];
+}
+
 // Per-thread schedule: one thread per sorted particle. The three cells of a
 // grid row are adjacent in sorted order, so each of the nine rows is one
 // contiguous slot range; candidates are visited in increasing slot order and
@@ -359,6 +389,17 @@ void launch_reorder(cudaStream_t st, int n, const uint32_t* keys, const uint32_t
     if (n > 0)
         k_reorder<<<grid_of(n), kBlock, 0, st>>>(n, keys, vals, pos, vel, vap, rp, ids, pos2, vel2, vap2, rp2, ids2,
                                                  cell_start, cell_end);
+}
+
+void launch_reorder_pos(cudaStream_t st, int n, const uint32_t* keys, const uint32_t* vals, const float4* pos,
+                        const int* ids, float4* pos2, int* ids2, uint32_t* cell_start, uint32_t* cell_end) {
+    if (n > 0)
+        k_reorder_pos<<<grid_of(n), kBlock, 0, st>>>(n, keys, vals, pos, ids, pos2, ids2, cell_start, cell_end);
+}
+
+void launch_reorder_state(cudaStream_t st, int n, const uint32_t* vals, const float4* vel, const float4* vap,
+                          const float2* rp, float4* vel2, float4* vap2, float2* rp2) {
+    if (n > 0) k_reorder_state<<<grid_of(n), kBlock, 0, st>>>(n, vals, vel, vap, rp, vel2, vap2, rp2);
 }
 
 void launch_build_nbr(cudaStream_t st, const Params& P, const float4* pos, const uint32_t* keys,

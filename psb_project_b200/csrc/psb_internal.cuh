@@ -247,9 +247,16 @@ void launch_cell_keys(cudaStream_t st, const Params& P, const float4* pos, const
 // hist holds 256 * radix_blocks(n) + 256 words.
 int radix_sort(cudaStream_t st, int n, int bits, uint32_t* keys[2], uint32_t* vals[2], uint32_t* hist, int nblocks_cap);
 int radix_blocks(int n);
+// The whole state into sorted order, with the cell ranges; or in two
+// launches: positions, ids and cell ranges (what the neighbour build reads),
+// then the rest.
 void launch_reorder(cudaStream_t st, int n, const uint32_t* keys, const uint32_t* vals, const float4* pos,
                     const float4* vel, const float4* vap, const float2* rp, const int* ids, float4* pos2, float4* vel2,
                     float4* vap2, float2* rp2, int* ids2, uint32_t* cell_start, uint32_t* cell_end);
+void launch_reorder_pos(cudaStream_t st, int n, const uint32_t* keys, const uint32_t* vals, const float4* pos,
+                        const int* ids, float4* pos2, int* ids2, uint32_t* cell_start, uint32_t* cell_end);
+void launch_reorder_state(cudaStream_t st, int n, const uint32_t* vals, const float4* vel, const float4* vap,
+                          const float2* rp, float4* vel2, float4* vap2, float2* rp2);
 void launch_build_nbr(cudaStream_t st, const Params& P, const float4* pos, const uint32_t* keys,
                       const uint32_t* cell_start, const uint32_t* cell_end, int* counts, int* list, int* flags);
 // (sph.cu) The per-thread neighbour build of one config-profile scene with the
