@@ -51,8 +51,9 @@ UNIT = "particle-steps/s"
 ALG_BYTES = {
     "cell_keys": 24,          # pos 16 -> key + id 8
     "radix_sort": 16,         # one read + write of the (key, value) pairs
-    "reorder": 53,            # slot + key 8, pos + id 20 in and out, cell ranges 5
-    "reorder_state": 84,      # slot 4, vel, half-step vel, (rho, p) 40 in and out
+    "reorder": 77,            # pos, vel, pressure 36 in + 36 out, cell ranges 5
+    "reorder_pos": 53,        # after an upload: slot + key 8, pos + id 20 in and out, cell ranges 5
+    "reorder_state": 84,      # ... then slot 4, vel, half-step vel, (rho, p) 40 in and out
     "build_nbr": 24,          # pos 16 + key 4 -> count 4
     "density_x": 20,          # pos 16 -> rho 4 (learned: + vel 16, 8 features 32)
     "pci_init": 132,          # non-pressure forces 52 + first prediction 80

@@ -579,7 +579,7 @@ int build(psb_ctx* c, bool keep_p = false, bool features = false) {
     // everything in one launch.
     const bool split = capturing(st) ? c->capture_split : c->in_pending;
     if (split) {
-        timed(c, "reorder", [&] {
+        timed(c, "reorder_pos", [&] {
             psb::launch_reorder_pos(st, n, c->keys[res], c->vals[res], c->pos[os], c->ids[orr], c->pos[ns], c->ids[nr],
                                     c->cell_start, c->cell_end);
         });
