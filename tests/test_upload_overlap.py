@@ -13,7 +13,8 @@ the upload joined before the step:
   * steps straight after an upload, kernel by kernel and as CUDA graphs
     (a graph carries an event wait node that must wait for the upload made
     before each of its launches, including a graph captured earlier);
-  * a download, a field read and a stream switch straight after an upload.
+  * a download, a field read, a stream switch, a pressure pre-solve and an
+    emission straight after an upload.
 """
 import numpy as np
 import pytest
@@ -108,3 +109,32 @@ def test_stream_switch_after_upload(inputs):
         out = sim.download()
         sim.set_stream(0)
     assert_same([out], ref)
+
+
+def test_presolve_and_emission_after_upload(inputs):
+    """psb_presolve and psb_emit wait for the copies before they touch the state."""
+    sc, a = inputs
+    k = 4096
+    # a block of the lattice moved into the empty half of the box
+    extra = {"pos": a["pos"][:k] + np.float32([2.0, 0.0, 0.0]), "vel": a["vel"][:k]}
+
+    def run(join):
+        with P.Simulation(sc.replace(n=sc.n + k)) as sim:       # capacity for the emitted block
+            sim.upload(a["pos"], a["zero3"], a["zero3"], a["zero1"])
+            sim.step(1)
+            sim.upload(a["pos"], a["vel"], a["vel_half"], a["pressure"])
+            if join:
+                sim.download()
+            sim.presolve(2)
+            p = sim.read_field(R.FIELD_PRESSURE)
+            sim.upload(a["pos"], a["vel"], a["vel_half"], a["pressure"])
+            if join:
+                sim.download()
+            sim.emit(extra["pos"], extra["vel"])
+            sim.step(1)
+            return p, sim.download()
+
+    p_a, out_a = run(False)
+    p_b, out_b = run(True)
+    np.testing.assert_array_equal(p_a, p_b)
+    assert_same([out_a], [out_b])
